@@ -1,0 +1,323 @@
+"""Benchmark of the sparse-voxel-tree march on B200.
+
+Workload (one step = one frame): 1920x1080 over the 1024x256x1024 synthetic
+terrain (6-octave value noise, seed 7, water below y=64, 1% trees, ~3% glass
+in the top two surface layers; 1024 chunks of 64^3), camera 30 above the
+centre column looking +z, pitched -15 deg.  Frame A is rendered untimed; the
+timed frames use the camera moved half a voxel along x with FLAG_HIZ on.
+Every step marches the primary rays, one sun shadow ray per lit-facing hit
+and one water-refraction / glass-transmission ray per water / glass hit.
+
+Metric: Grays/s of primary + shadow rays (secondary rays are traced but not
+counted).  `value` is measured on device-resident inputs; `e2e` goes through
+the C ABI with host buffers (frame + chunk list + grid uploaded, visibility
+and shadow buffers read back every step).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Under torchrun every rank renders its own copy (replicas: the march does not
+shard a frame across GPUs); value is the total over ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Grays/s at 1080p (primary + shadow rays)"
+UNIT = "Grays/s"
+WORKLOAD = "1920x1080 frame over the 1024x256x1024 terrain (1024 chunks), Hi-Z frame moved 0.5 voxel"
+
+# algorithmic bytes per counted event (the layout's element sizes)
+BYTES = {"chunk_records": 96, "l1_fetches": 16, "leaf_fetches": 8, "attr_fetches": 4, "palette_decodes": 12,
+         "grid_lookups": 4}
+OUT_BYTES_PER_PIXEL = 8 + 4 + 8 + 4      # vis, shadow, secondary key, secondary t
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([s.strip() for s in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]
+                          and "Not" not in s[3 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def build_workload():
+    from voxelcraft_menu_b200 import world as W
+    rec = W.recipe_large_terrain()
+    w = W.World.generate(rec)
+    pools = w.pools()
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_HIZ
+    view_a = w.view(W.large_terrain_camera(rec, flags=flags))
+    view_b = w.view(W.large_terrain_camera(rec, flags=flags, dx=0.5))
+    return w, pools, view_a, view_b
+
+
+def oracle_rows(o, view, row0, rows):
+    """Time the oracle's frame (engine pass sequence) + shadow pass over tile
+    rows [row0, row0 + rows); returns (seconds, primary + shadow rays)."""
+    tx, ty = int(view.frame.tiles[0]), int(view.frame.tiles[1])
+    rows = min(rows, ty - row0)
+    width, height = int(view.frame.res[0]), int(view.frame.res[1])
+    tiles = (row0 * tx, (row0 + rows) * tx)
+    p0, p1 = row0 * 8 * width, min((row0 + rows) * 8, height) * width
+    t0 = time.perf_counter()
+    vis, _, _, tr = o.frame_vis(tiles=tiles, traffic=True)
+    _, tr2 = o.shadow(vis, pix=(p0, p1), traffic=True)
+    dt = time.perf_counter() - t0
+    return dt, tr["rays"] + tr2["rays"], p1 - p0
+
+
+def cpu_sample(view, pools, budget_s=12.0):
+    """The oracle (the engine's pass sequence restated on the CPU) over a
+    bounded band of tile rows of the same frame, on every host core."""
+    from oracle.oracle import Oracle
+    o = Oracle(view, *pools)
+    ty = int(view.frame.tiles[1])
+    t_total, rays, px, rows, row0 = 0.0, 0, 0, 2, ty // 2 - 8
+    while t_total < budget_s and row0 < ty:
+        dt, r, p = oracle_rows(o, view, row0, rows)
+        t_total += dt
+        rays += r
+        px += p
+        row0 += rows
+        rows *= 2
+    return {"value": rays / t_total / 1e9, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"oracle (engine pass sequence restated in C++, OpenMP) over the middle tile rows of the "
+                      f"same frame: {px} pixels, {rays} primary+shadow rays in {t_total:.1f}s"}
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    w, pools, va, vb = build_workload()
+    from oracle.oracle import Oracle
+    o = Oracle(vb, *pools)
+    ty = int(vb.frame.tiles[1])
+    rows = 8
+    row0 = ty // 2 - rows // 2
+    times, rays, px = [], 0, 0
+    for i in range(args.warmup + args.steps):
+        dt, r, p = oracle_rows(o, vb, row0, rows)
+        if i >= args.warmup:
+            times.append(dt)
+            rays, px = r, p
+    mean = float(np.mean(times))
+    value = rays / mean / 1e9
+    sample = f"oracle over {rows} middle tile rows per step ({px} pixels, {rays} primary+shadow rays)"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variant", type=int, default=-1, help="fused tile variant (-1: autotune)")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from voxelcraft_menu_b200.march import Marcher
+    from voxelcraft_menu_b200 import tuning
+
+    w, pools, va, vb = build_workload()
+    m = Marcher(1920, 1080, device=local)
+    # the library enqueues on torch's (non-default) current stream, so torch's
+    # CUDA events bracket exactly the march's launches
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    m._ck(m._L.vm_set_stream(m._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
+    m.upload_world(*pools)
+
+    # tile shape / CTAs per SM: autotuned on this frame unless fixed
+    if args.variant >= 0:
+        best = {"variant": args.variant, "ctas_per_sm": 0}
+    else:
+        best = tuning.autotune_single(m, vb, warm=va)
+    m.set_tuning(best["variant"], best["ctas_per_sm"])
+
+    # frame A then the timed frame B (Hi-Z of A carried over)
+    m.upload_view(va)
+    m.render()
+    m.upload_view(vb)
+    traffic = m.render_counted()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)   # > 126 MB L2
+
+    for _ in range(args.warmup):
+        m.render()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize(dev)
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        m.render()
+        ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms_step = float(np.mean(ms))
+    if world > 1:
+        t = torch.tensor([ms_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+        dist.barrier()
+
+    npix = 1920 * 1080
+    rays = traffic["rays_primary"] + traffic["rays_shadow"]
+    value = world * rays / (ms_step * 1e-3) / 1e9
+
+    # e2e through the C ABI with host buffers (pinned), per step: frame + chunk
+    # list + grid up, render, vis + shadow down
+    vis_h = torch.empty(npix, dtype=torch.int64).pin_memory()
+    sh_h = torch.empty(npix, dtype=torch.float32).pin_memory()
+    ch_h = torch.from_numpy(vb.chunks.view(np.uint8).copy()).pin_memory()
+    gr_h = torch.from_numpy(vb.grid.view(np.int32).copy()).pin_memory()
+    import ctypes as C
+    L = m._L
+
+    def e2e_step():
+        m._ck(L.vm_upload_chunks(m._h, C.c_void_p(ch_h.data_ptr()), len(vb.chunks), C.c_void_p(gr_h.data_ptr()),
+                                 vb.grid.size))
+        m._ck(L.vm_set_frame(m._h, C.byref(vb.frame)))
+        m._ck(L.vm_render(m._h))
+        m._ck(L.vm_read_vis(m._h, C.c_void_p(vis_h.data_ptr())))
+        m._ck(L.vm_read_shadow(m._h, C.c_void_p(sh_h.data_ptr())))
+
+    for _ in range(3):
+        e2e_step()
+    e_ms = []
+    for i in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        e2e_step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        e_ms.append(ev0.elapsed_time(ev1))
+    e2e_ms = float(np.mean(e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = vb.chunks.nbytes + vb.grid.nbytes + 352
+    d2h = npix * 12
+
+    algo_bytes = sum(traffic[k] * b for k, b in BYTES.items()) + npix * OUT_BYTES_PER_PIXEL
+    peak, peak_kind = peaks()
+    achieved = algo_bytes / (ms_step * 1e-3) / 1e9
+    stats = m.stats()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "resolution": [1920, 1080], "chunks": int(len(vb.chunks)),
+                       "tile": best, "l2": "flushed between timed steps (256 MB write)",
+                       "parallelism": f"replicas x{world}"},
+            "rays_per_step": {"primary": traffic["rays_primary"], "shadow": traffic["rays_shadow"],
+                              "secondary_uncounted": traffic["rays_secondary"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": algo_bytes, "dda_steps_per_launch": traffic["iters"],
+                         "bytes_per_dda_step": algo_bytes / max(traffic["iters"], 1)},
+            "e2e": {"value": world * rays / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+            "device_error": int(stats.device_error),
+        }
+        if not args.no_cpu:
+            line["cpu_baseline"] = cpu_sample(vb, pools)
+        print(json.dumps(line), flush=True)
+    m.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,151 @@
+/* voxmarch: the sparse-voxel-tree ray march of the voxel engine
+ * Vuk03-boop/voxelcraft-menu, as CUDA kernels for one B200 (sm_100a) behind a
+ * flat C ABI.
+ *
+ * The engine runs this path as wgpu compute passes inside Renderer::render
+ * (src/render/mod.rs:1593-1919).  Every call below replaces one piece of that
+ * host code, keeps the engine's buffer layouts byte for byte (vm_frame ==
+ * GpuFrame, vm_chunk == GpuChunk, inner / leaf / brick pools, chunk grid,
+ * 64-bit visibility keys) and is stream-ordered on the context's stream.
+ *
+ * Conventions
+ *  - Every call returns a vm_status; on error vm_last_error() has the text.
+ *  - Host arrays are read (or written) only during the call.  The context owns
+ *    all device buffers; vm_device_buffers() exposes them for zero-copy use.
+ *  - One context per host thread; no internal threads.
+ *  - Read calls synchronise the context's stream; all others only enqueue.
+ */
+#ifndef VOXMARCH_H
+#define VOXMARCH_H
+#include <stddef.h>
+#include <stdint.h>
+#include "../voxelcraft_menu_b200/csrc/vm_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum vm_status {
+  VM_OK = 0,
+  VM_E_INVALID = 1,        /* bad argument or malformed buffer */
+  VM_E_CAPACITY = 2,       /* pair list truncated: the engine's TRUNCATION_MARK (src/render/mod.rs:37,1957-1975) */
+  VM_E_TILE_OVERFLOW = 3,  /* tile index does not fit the 19-bit pair field: OVERSIZE_MARK (src/render/mod.rs:39,2047-2060) */
+  VM_E_ITER_CAP = 4,       /* informational: some march hit MAX_ITERS (common.wgsl:698-701); counted, not fatal */
+  VM_E_TIMEOUT = 5,        /* a bounded device wait gave up */
+  VM_E_CUDA = 6,           /* CUDA runtime error */
+  VM_E_NOT_READY = 7       /* call order: e.g. march before world / frame */
+} vm_status;
+
+typedef struct vm_ctx vm_ctx;
+
+typedef struct vm_caps {
+  uint32_t max_width, max_height;   /* largest frame this context renders */
+  uint32_t max_chunks;              /* largest chunk list (<= 8191 for the 13-bit field) */
+  uint32_t max_views;               /* largest batch (vm_batch_*) */
+  uint64_t max_batch_pixels;        /* total pixels of a batch */
+} vm_caps;
+
+/* Renderer::new (src/render/mod.rs:851): device buffers for one renderer. */
+int vm_create(int device_ordinal, const vm_caps* caps, vm_ctx** out);
+void vm_destroy(vm_ctx* ctx);
+const char* vm_last_error(const vm_ctx* ctx);
+/* Run on a caller stream (cudaStream_t as void*); NULL restores the context's own. */
+int vm_set_stream(vm_ctx* ctx, void* cuda_stream);
+
+/* Renderer::sync_world (src/render/mod.rs:1355-1396): replace the three pools.
+ * inners: n_inners x vec4<u32> (common.wgsl:100); leaves: n_leaves x vec2<u32>
+ * (common.wgsl:101); bricks: n_bricks x u32 (common.wgsl:102). */
+int vm_upload_world(vm_ctx* ctx, const uint32_t* inners, uint64_t n_inners, const uint32_t* leaves,
+                    uint64_t n_leaves, const uint32_t* bricks, uint64_t n_bricks);
+/* GpuMirror dirty-range upload (src/render/pools.rs): pool 0 inners, 1 leaves,
+ * 2 bricks; offset and count in that pool's elements; the pool grows if needed. */
+int vm_update_pool(vm_ctx* ctx, int pool, uint64_t offset, const uint32_t* data, uint64_t count);
+/* build_chunk_list's uploads (src/render/mod.rs:1555-1562): the chunk list
+ * (visible chunks first, then shadow-only ones) and the chunk grid. */
+int vm_upload_chunks(vm_ctx* ctx, const vm_chunk* chunks, uint32_t n_chunks, const uint32_t* grid, uint64_t grid_len);
+/* queue.write_buffer of GpuFrame (src/render/mod.rs:1707). */
+int vm_set_frame(vm_ctx* ctx, const vm_frame* frame);
+
+/* The engine's passes, one call per group of dispatches (src/render/mod.rs:1716-1851):
+ * vm_select   = clear vis / counters (hiz too unless FLAG_HIZ) + tile_select + finalize (1716-1749)
+ * vm_march    = march; with FLAG_HIZ also build_hiz, finalize_deferred,
+ *               recover_select, finalize_recover and the second march (1751-1794)
+ * vm_primary_shadow = primary_shadow (1824-1841), blocker distance per pixel
+ * vm_secondary      = one water-refraction / glass-transmission ray per hit
+ *                     (water_refract_leg resolve.wgsl:1029, shade_glass resolve.wgsl:1261) */
+int vm_select(vm_ctx* ctx);
+int vm_march(vm_ctx* ctx);
+int vm_primary_shadow(vm_ctx* ctx);
+int vm_secondary(vm_ctx* ctx);
+
+/* The same frame as vm_select + vm_march + vm_primary_shadow + vm_secondary
+ * in one fused, persistent kernel; identical vis / shadow / secondary output.
+ * hiz receives the final visibility's per-8x8-tile minimum. */
+int vm_render(vm_ctx* ctx);
+
+/* Tuning of vm_render and vm_batch_run: tile variant 0 = 8x8, 1 = 16x8,
+ * 2 = 16x16, 3 = 32x16 pixels per CTA; ctas_per_sm 0 = occupancy maximum. */
+int vm_set_tuning(vm_ctx* ctx, int tile_variant, int ctas_per_sm);
+
+/* Read-backs (synchronise the context's stream). */
+int vm_read_vis(vm_ctx* ctx, uint64_t* out);                 /* res.x*res.y keys (common.wgsl:1324) */
+int vm_read_hiz(vm_ctx* ctx, uint32_t* out);                 /* tiles.x*tiles.y */
+int vm_read_shadow(vm_ctx* ctx, float* out);                 /* blocker distance, 0 = lit */
+int vm_read_secondary(vm_ctx* ctx, uint64_t* key, float* t); /* see below */
+int vm_read_heatmap(vm_ctx* ctx, uint32_t* out);             /* FLAG_HEATMAP iteration sums (march.wgsl:51-53) */
+/* Expanded visibility: voxel index X*(Z*y + z) + x over the world box
+ * [origin, origin + dims), face = normal id (common.wgsl:387), t = hit_t
+ * (common.wgsl:1300).  Misses: voxel 0xFFFFFFFF, face 0xFF, t 0. */
+int vm_read_expanded(vm_ctx* ctx, const int32_t origin[3], const uint32_t dims[3], uint32_t* voxel, uint8_t* face,
+                     float* t);
+/* Hi-Z input of the next FLAG_HIZ frame (the engine keeps last frame's buffer). */
+int vm_write_hiz(vm_ctx* ctx, const uint32_t* hiz);
+
+/* secondary key: 0 = no secondary ray for the pixel; else bit 63 traced,
+ * bit 62 hit, bit 61 glass (else water), bits 37-39 normal, 24-36 chunk,
+ * 0-23 voxel (x<<16 | y<<8 | z); t = distance along the ray, max on a miss. */
+
+/* Renderer::pair_demand / march_stats (src/render/mod.rs:1948-2045). */
+typedef struct vm_stats {
+  uint32_t counters[8];     /* the engine's counters[0..5] after the last vm_march */
+  uint32_t pairs_selected, pairs_deferred, pairs_recovered, max_pairs;
+  uint32_t truncated;       /* 1 if any list exceeded max_pairs */
+  uint32_t device_error;    /* nonzero: a pool index was out of range (bit set per pool) */
+} vm_stats;
+int vm_stats_read(vm_ctx* ctx, vm_stats* out);
+
+/* Traffic counted by the instrumented fused kernel (one extra launch):
+ * chunk records, L1 / leaf / attribute fetches, palette decodes, grid
+ * lookups, DDA iterations, and rays of each kind. */
+typedef struct vm_traffic {
+  uint64_t chunk_records, l1_fetches, leaf_fetches, attr_fetches, palette_decodes, grid_lookups, iters;
+  uint64_t rays_primary, rays_shadow, rays_secondary;
+} vm_traffic;
+int vm_render_counted(vm_ctx* ctx, vm_traffic* out);
+
+/* Batched views: many frames (each with its own chunk list and grid) marched
+ * by one persistent work-stealing launch (vm_batch_run mode 0, replayed from
+ * a CUDA graph) or by one launch per view (mode 1, the baseline).  Views are
+ * packed in order; their outputs are concatenated in the batch buffers. */
+int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm_chunk* chunks,
+                 const uint32_t* chunk_counts, const uint32_t* grids, const uint32_t* grid_lens);
+int vm_batch_run(vm_ctx* ctx, int mode);
+int vm_batch_read(vm_ctx* ctx, uint64_t* vis, float* shadow);
+uint64_t vm_batch_pixels(const vm_ctx* ctx);
+
+/* Device pointers of the context's buffers (valid until the next upload that
+ * grows them), for zero-copy callers such as a torch binding. */
+typedef struct vm_device_ptrs {
+  void* vis; void* shadow; void* sec_key; void* sec_t; void* hiz;
+  void* batch_vis; void* batch_shadow;
+  void* stream;
+} vm_device_ptrs;
+int vm_device_buffers(vm_ctx* ctx, vm_device_ptrs* out);
+
+/* Synchronise the context's stream. */
+int vm_sync(vm_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1223 @@
+// ORACLE — test infrastructure only.
+//
+// A plain CPU restatement of the reference engine's WGSL ray march, used as the
+// checker for the CUDA path (tests, the smoke check and the timed CPU baseline
+// leg of bench.py).  Nothing in the product links or calls this file.
+//
+// The reference (Vuk03-boop/voxelcraft-menu) has no CPU march: its headless
+// modes run the same WGSL passes.  This file restates those passes line by line
+// in C++ with a fixed floating-point contract:
+//   * compiled with -ffp-contract=off (no FMA), IEEE division and sqrt;
+//   * normalize(v) = v / sqrt(dot(v, v)), dot evaluated left to right;
+//   * min/max follow IEEE minNum/maxNum (fminf/fmaxf);
+//   * float -> int conversions saturate (as WGSL and PTX cvt do).
+// The CUDA kernels are held to bit-exact agreement with this contract.
+//
+// Parity status: the reference's layout producers, key packing, pair word,
+// water-line predicate and camera rays are pinned to the reference's own tests
+// (tests/tree.rs, tests/full_march.rs, tests/emitter_gate.rs, tests/cutout.rs,
+// tests/pairs.rs, tests/waterline.rs, tests/camera.rs, tests/physics.rs);
+// the march outputs themselves are UNPINNED against the reference's GPU march,
+// which cannot run here (WGSL needs a graphics stack) and which has no golden
+// march outputs.  The hierarchical march is cross-checked against a restated
+// unit-voxel DDA (src/player.rs:334-393) on opaque worlds.
+//
+// Citations are paths inside the reference project.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cstdio>
+#include <vector>
+#include <algorithm>
+#include <atomic>
+#include <omp.h>
+
+#include "../voxelcraft_menu_b200/csrc/vm_types.h"
+
+namespace {
+
+// ----------------------------------------------------------------------------
+// error flag: any out-of-bounds pool access sets it (the oracle never reads
+// outside the buffers it was given).
+std::atomic<int> g_err{0};
+char g_err_msg[256];
+
+void set_err(const char* what, uint64_t idx, uint64_t n) {
+  int expect = 0;
+  if (g_err.compare_exchange_strong(expect, 1)) {
+    snprintf(g_err_msg, sizeof g_err_msg, "%s index %llu out of %llu", what,
+             (unsigned long long)idx, (unsigned long long)n);
+  }
+}
+
+struct V3 { float x, y, z; };
+struct I3 { int32_t x, y, z; };
+struct U3 { uint32_t x, y, z; };
+
+inline V3 v3(float x, float y, float z) { return {x, y, z}; }
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 mul(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline V3 muls(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 divs(V3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+inline V3 neg(V3 a) { return {-a.x, -a.y, -a.z}; }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline V3 vmin(V3 a, V3 b) { return {fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)}; }
+inline V3 vmax(V3 a, V3 b) { return {fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)}; }
+inline float comp(V3 a, uint32_t i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+inline int32_t comp(I3 a, uint32_t i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+inline void setc(I3& a, uint32_t i, int32_t v) { if (i == 0) a.x = v; else if (i == 1) a.y = v; else a.z = v; }
+inline bool compb(const bool* b, uint32_t i) { return b[i]; }
+inline float signf(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+inline V3 normalize(V3 v) { float l = sqrtf(dot(v, v)); return {v.x / l, v.y / l, v.z / l}; }
+inline float length(V3 v) { return sqrtf(dot(v, v)); }
+
+// saturating float -> i32 (WGSL conversion semantics; NaN -> 0)
+inline int32_t f2i(float x) {
+  if (x != x) return 0;
+  if (x >= 2147483648.0f) return INT32_MAX;
+  if (x <= -2147483648.0f) return INT32_MIN;
+  return (int32_t)x;
+}
+inline uint32_t f2u(float x) {
+  if (x != x || x <= 0.0f) return 0;
+  if (x >= 4294967296.0f) return UINT32_MAX;
+  return (uint32_t)x;
+}
+inline I3 floor_i(V3 p) { return {f2i(floorf(p.x)), f2i(floorf(p.y)), f2i(floorf(p.z))}; }
+
+inline V3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
+
+// ----------------------------------------------------------------------------
+struct World {
+  const vm_frame* f;
+  const vm_chunk* chunks; uint32_t n_chunks;
+  const uint32_t* inners; uint64_t n_inners;   // count of vec4<u32>
+  const uint32_t* leaves; uint64_t n_leaves;   // count of vec2<u32>
+  const uint32_t* bricks; uint64_t n_bricks;   // count of u32
+  const uint32_t* grid; uint64_t n_grid;
+};
+
+// per-thread counters of the traversal's memory traffic (for the roofline)
+struct Counters {
+  uint64_t chunk_records, l1_fetches, leaf_fetches, attr_fetches, palette_decodes,
+      grid_lookups, iters, march_calls, rays;
+};
+thread_local Counters* t_cnt = nullptr;
+inline void cnt_add(uint64_t Counters::*f, uint64_t v = 1) { if (t_cnt) t_cnt->*f += v; }
+
+struct U4 { uint32_t x, y, z, w; };
+struct U2 { uint32_t x, y; };
+
+inline U4 inner_at(const World& w, uint64_t i) {
+  if (i >= w.n_inners) { set_err("inners", i, w.n_inners); return {0, 0, 0, 0}; }
+  const uint32_t* p = w.inners + 4 * i;
+  return {p[0], p[1], p[2], p[3]};
+}
+inline U2 leaf_at(const World& w, uint64_t i) {
+  if (i >= w.n_leaves) { set_err("leaves", i, w.n_leaves); return {0, 0}; }
+  return {w.leaves[2 * i], w.leaves[2 * i + 1]};
+}
+inline uint32_t brick_at(const World& w, uint64_t i) {
+  if (i >= w.n_bricks) { set_err("bricks", i, w.n_bricks); return 0; }
+  return w.bricks[i];
+}
+inline const vm_chunk& chunk_at(const World& w, uint32_t ci) {
+  static const vm_chunk zero{};
+  if (ci >= w.n_chunks) { set_err("chunks", ci, w.n_chunks); return zero; }
+  return w.chunks[ci];
+}
+inline uint32_t grid_at(const World& w, uint64_t i) {
+  if (i >= w.n_grid) { set_err("grid", i, w.n_grid); return VM_NO_CHUNK; }
+  return w.grid[i];
+}
+
+// ---- tree helpers: common.wgsl:299-356 ----
+inline bool mask_has(U2 m, uint32_t bit) {
+  if (bit < 32u) return ((m.x >> bit) & 1u) != 0u;
+  return ((m.y >> (bit - 32u)) & 1u) != 0u;
+}
+inline uint32_t popc(uint32_t x) { return (uint32_t)__builtin_popcount(x); }
+inline uint32_t mask_below(U2 m, uint32_t bit) {
+  if (bit < 32u) return popc(m.x & ((1u << bit) - 1u));
+  if (bit == 32u) return popc(m.x);
+  return popc(m.x) + popc(m.y & ((1u << (bit - 32u)) - 1u));
+}
+inline uint32_t cell_bit(U3 c) { return c.x | (c.y << 2u) | (c.z << 4u); }
+inline U3 ushr(U3 a, uint32_t s) { return {a.x >> s, a.y >> s, a.z >> s}; }
+inline U3 uand(U3 a, uint32_t m) { return {a.x & m, a.y & m, a.z & m}; }
+
+// leaf_block: common.wgsl:320-334
+uint32_t leaf_block(const World& w, uint32_t entry, U3 v) {
+  if ((entry & VM_UNIFORM_BIT) != 0u) return entry & 0xFFFFu;
+  cnt_add(&Counters::palette_decodes);
+  uint32_t hdr = brick_at(w, entry);
+  uint32_t n = hdr & 0xFFu;
+  uint32_t bits = (hdr >> 8u) & 0xFFu;
+  uint32_t pal_words = (n + 1u) / 2u;
+  uint32_t vb = cell_bit(uand(v, 3u));
+  uint32_t bitpos = vb * bits;
+  uint32_t wd = brick_at(w, (uint64_t)entry + 1u + pal_words + (bitpos >> 5u));
+  uint32_t idx = (wd >> (bitpos & 31u)) & ((bits >= 32u ? 0u : (1u << bits)) - 1u);
+  uint32_t pw = brick_at(w, (uint64_t)entry + 1u + idx / 2u);
+  return (pw >> ((idx & 1u) * 16u)) & 0xFFFFu;
+}
+
+// leaf_attr: common.wgsl:336-348
+uint32_t leaf_attr(const World& w, uint32_t ci, U3 v) {
+  const vm_chunk& c = chunk_at(w, ci);
+  U2 root_mask{c.root[0], c.root[1]};
+  uint32_t l1b = cell_bit(ushr(v, 4u));
+  U4 l1;
+  if ((c.root[2] & VM_FULL_BIT) != 0u) {
+    l1 = {0xFFFFFFFFu, 0xFFFFFFFFu, VM_FULL_BIT, l1b * 64u};
+  } else {
+    l1 = inner_at(w, (uint64_t)(c.root[2] & VM_PTR_MASK) + mask_below(root_mask, l1b));
+  }
+  uint32_t lfb = cell_bit(uand(ushr(v, 2u), 3u));
+  return brick_at(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + mask_below(U2{l1.x, l1.y}, lfb));
+}
+
+// block_at: common.wgsl:350-356
+uint32_t block_at(const World& w, uint32_t ci, U3 v) {
+  const vm_chunk& c = chunk_at(w, ci);
+  if ((c.attr_flags & VM_ATTR_UNIFORM) != 0u) return c.attr_base;
+  return leaf_block(w, leaf_attr(w, ci, v), v);
+}
+
+// voxel_occupied: common.wgsl:912-940
+bool voxel_occupied(const World& w, uint32_t ci, I3 v) {
+  if (v.x < 0 || v.y < 0 || v.z < 0 || v.x > 63 || v.y > 63 || v.z > 63) return false;
+  const vm_chunk& c = chunk_at(w, ci);
+  U3 uv{(uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z};
+  U2 root_mask{c.root[0], c.root[1]};
+  uint32_t l1b = cell_bit(ushr(uv, 4u));
+  if (!mask_has(root_mask, l1b)) return false;
+  bool occupied = false;
+  if ((c.root[2] & VM_FULL_BIT) != 0u) {
+    occupied = true;
+  } else {
+    U4 l1 = inner_at(w, (uint64_t)(c.root[2] & VM_PTR_MASK) + mask_below(root_mask, l1b));
+    if ((l1.z & VM_FULL_BIT) != 0u) {
+      occupied = true;
+    } else {
+      U2 l1m{l1.x, l1.y};
+      uint32_t lfb = cell_bit(uand(ushr(uv, 2u), 3u));
+      if (mask_has(l1m, lfb)) {
+        U2 leaf = leaf_at(w, (uint64_t)(l1.z & VM_PTR_MASK) + mask_below(l1m, lfb));
+        occupied = mask_has(leaf, cell_bit(uand(uv, 3u)));
+      }
+    }
+  }
+  return occupied;
+}
+
+inline uint64_t grid_index(const World& w, I3 rel) {
+  const uint32_t* gd = w.f->grid_dim;
+  return (uint64_t)(uint32_t)rel.x + (uint64_t)(uint32_t)rel.y * gd[0] +
+         (uint64_t)(uint32_t)rel.z * gd[0] * gd[1];
+}
+inline bool grid_outside(const World& w, I3 rel) {
+  const uint32_t* gd = w.f->grid_dim;
+  return rel.x < 0 || rel.y < 0 || rel.z < 0 || rel.x >= (int32_t)gd[0] ||
+         rel.y >= (int32_t)gd[1] || rel.z >= (int32_t)gd[2];
+}
+
+// world_block_at: common.wgsl:266-277
+uint32_t world_block_at(const World& w, V3 p) {
+  I3 cell = floor_i(divs(p, 64.0f));
+  cell = {cell.x - w.f->grid_min[0], cell.y - w.f->grid_min[1], cell.z - w.f->grid_min[2]};
+  if (grid_outside(w, cell)) return 0u;
+  cnt_add(&Counters::grid_lookups);
+  uint32_t ci = grid_at(w, grid_index(w, cell));
+  if (ci == VM_NO_CHUNK) return 0u;
+  const vm_chunk& c = chunk_at(w, ci);
+  I3 v = floor_i(divs(sub(p, ld3(c.origin)), c.voxel_size));
+  if (v.x < 0 || v.y < 0 || v.z < 0 || v.x >= 64 || v.y >= 64 || v.z >= 64) return 0u;
+  if (!voxel_occupied(w, ci, v)) return 0u;
+  return block_at(w, ci, U3{(uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z});
+}
+
+// ray_dir: common.wgsl:358-368
+V3 ray_dir(const vm_frame& f, float px, float py) {
+  float ndc_x = ((px + f.jitter[0]) / (float)f.res[0]) * 2.0f - 1.0f;
+  float ndc_y = 1.0f - ((py + f.jitter[1]) / (float)f.res[1]) * 2.0f;
+  V3 v = add(add(ld3(f.cam_fwd), muls(ld3(f.cam_right), ndc_x * f.tan_half_fov * f.aspect)),
+             muls(ld3(f.cam_up), ndc_y * f.tan_half_fov));
+  V3 d = normalize(v);
+  V3 o;
+  o.x = fabsf(d.x) < 1e-6f ? 1e-6f * signf(d.x + 1e-9f) : d.x;
+  o.y = fabsf(d.y) < 1e-6f ? 1e-6f * signf(d.y + 1e-9f) : d.y;
+  o.z = fabsf(d.z) < 1e-6f ? 1e-6f * signf(d.z + 1e-9f) : d.z;
+  return o;
+}
+
+inline float fractf(float x) { return x - floorf(x); }
+
+// dither / ray_skips: common.wgsl:370-385
+bool ray_skips(const vm_frame& f, float fade, uint32_t px, uint32_t py) {
+  if (fade >= 1.0f) return false;
+  float p0 = (float)px + 5.588238f * (float)f.frame_index;
+  float p1 = (float)py;
+  float d = fractf(52.9829189f * fractf(p0 * 0.06711056f + p1 * 0.00583715f));
+  if (fade >= 0.0f) return d >= fade;
+  return d < -fade;
+}
+
+// normal_of: common.wgsl:387-398
+V3 normal_of(uint32_t id) {
+  if (id >= VM_NORMAL_CROSS_A) {
+    float s = id == VM_NORMAL_CROSS_B ? 1.0f : -1.0f;
+    return {0.70710678f, 0.0f, s * 0.70710678f};
+  }
+  uint32_t axis = id >> 1u;
+  float s = (id & 1u) == 1u ? 1.0f : -1.0f;
+  if (axis == 0u) return {s, 0.0f, 0.0f};
+  if (axis == 1u) return {0.0f, s, 0.0f};
+  return {0.0f, 0.0f, s};
+}
+
+// hash_u32: common.wgsl:1422-1430
+inline uint32_t hash_u32(uint32_t x) {
+  uint32_t h = x;
+  h ^= h >> 16u;
+  h *= 0x7feb352du;
+  h ^= h >> 15u;
+  h *= 0x846ca68bu;
+  h ^= h >> 16u;
+  return h;
+}
+
+// leaf_solid: common.wgsl:514-518
+bool leaf_solid(I3 wv, U3 m) {
+  int32_t qx = (int32_t)((uint32_t)wv.x * 4u + m.x);
+  int32_t qy = (int32_t)((uint32_t)wv.y * 4u + m.y);
+  int32_t qz = (int32_t)((uint32_t)wv.z * 4u + m.z);
+  uint32_t h = hash_u32(((uint32_t)qx * 73856093u) ^ ((uint32_t)qy * 19349663u) ^
+                        ((uint32_t)qz * 83492791u));
+  return (float)(h >> 8u) * (1.0f / 16777216.0f) < VM_LEAF_FILL;
+}
+
+// micro_entry: common.wgsl:520-528
+U3 micro_entry(U3 uc, V3 ro, V3 rd, float t, uint32_t axis, const bool* pos_dir, bool snap) {
+  V3 p = muls(sub(add(ro, muls(rd, t)), v3((float)uc.x, (float)uc.y, (float)uc.z)), 4.0f);
+  I3 m = floor_i(p);
+  m = {std::min(std::max(m.x, 0), 3), std::min(std::max(m.y, 0), 3), std::min(std::max(m.z, 0), 3)};
+  if (snap) setc(m, axis, pos_dir[axis] ? 0 : 3);
+  return {(uint32_t)m.x, (uint32_t)m.y, (uint32_t)m.z};
+}
+
+struct MicroHit { bool hit; float t; uint32_t normal; U3 micro; };
+
+// cutout_march: common.wgsl:537-577
+MicroHit cutout_march(I3 wv, U3 uc, V3 ro, V3 rd, float t_in, uint32_t axis_in,
+                      const bool* pos_dir, bool snap) {
+  MicroHit r{false, t_in, 0u, {0u, 0u, 0u}};
+  V3 base = v3((float)uc.x, (float)uc.y, (float)uc.z);
+  V3 inv = v3(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+  const float ms = 1.0f / 4.0f;
+  U3 me = micro_entry(uc, ro, rd, t_in, axis_in, pos_dir, snap);
+  I3 m{(int32_t)me.x, (int32_t)me.y, (int32_t)me.z};
+  float t = t_in;
+  uint32_t axis = axis_in;
+  for (uint32_t i = 0; i < 12u; ++i) {
+    if (m.x < 0 || m.y < 0 || m.z < 0 || m.x >= 4 || m.y >= 4 || m.z >= 4) return r;
+    if (leaf_solid(wv, U3{(uint32_t)m.x, (uint32_t)m.y, (uint32_t)m.z})) {
+      r.hit = true;
+      r.t = t;
+      r.normal = axis * 2u + (pos_dir[axis] ? 0u : 1u);
+      r.micro = {(uint32_t)m.x, (uint32_t)m.y, (uint32_t)m.z};
+      return r;
+    }
+    V3 bound = v3((float)(pos_dir[0] ? m.x + 1 : m.x), (float)(pos_dir[1] ? m.y + 1 : m.y),
+                  (float)(pos_dir[2] ? m.z + 1 : m.z));
+    V3 tn = mul(sub(add(base, muls(bound, ms)), ro), inv);
+    if (tn.x <= tn.y && tn.x <= tn.z) { t = tn.x; axis = 0u; }
+    else if (tn.y <= tn.z) { t = tn.y; axis = 1u; }
+    else { t = tn.z; axis = 2u; }
+    setc(m, axis, comp(m, axis) + (pos_dir[axis] ? 1 : -1));
+  }
+  return r;
+}
+
+inline bool is_tuft(uint32_t b) { return b == VM_TALL_GRASS || b == VM_GRASS_TALL || b == VM_REEDS; }
+inline bool is_cutout_id(uint32_t b) { return b == VM_LEAVES || b == VM_PINE_LEAVES; }
+inline bool casts_sun_shadow(uint32_t id) { return id != VM_GLOWSTONE; }  // common.wgsl:264
+
+struct Hit { bool hit; float t; uint32_t normal; U3 voxel; U3 micro; uint32_t iters; };
+
+// march_chunk: common.wgsl:579-910.  Foliage tufts (ids 18/24/25) are
+// transparent here: their cross quads need the atlas alpha (cross_quad,
+// common.wgsl:425-487), which has no device-buffer form in this build.
+Hit march_chunk(const World& w, uint32_t ci, V3 ro_w, V3 rd, float t_limit, bool skip_water,
+                bool skip_foliage, bool skip_glass, bool sun_ray) {
+  (void)skip_foliage;
+  Hit h{false, 0.0f, 0u, {0u, 0u, 0u}, {0u, 0u, 0u}, 0u};
+  cnt_add(&Counters::march_calls);
+  cnt_add(&Counters::chunk_records);
+  const vm_chunk& c = chunk_at(w, ci);
+  float vs = c.voxel_size;
+  V3 origin = ld3(c.origin);
+  V3 ro = divs(sub(ro_w, origin), vs);
+  V3 inv = v3(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+  V3 bmin = divs(sub(ld3(c.aabb_min), origin), vs);
+  V3 bmax = divs(sub(ld3(c.aabb_max), origin), vs);
+  V3 t0 = mul(sub(bmin, ro), inv);
+  V3 t1 = mul(sub(bmax, ro), inv);
+  V3 tmin3 = vmin(t0, t1);
+  V3 tmax3 = vmax(t0, t1);
+  float t_enter = fmaxf(fmaxf(tmin3.x, tmin3.y), tmin3.z);
+  float t_exit = fminf(fminf(tmax3.x, tmax3.y), tmax3.z);
+  float t_end = fminf(t_exit, t_limit / vs);
+  float t = fmaxf(t_enter, 0.0f);
+  if (t >= t_end) return h;
+  uint32_t axis;
+  if (tmin3.x >= tmin3.y && tmin3.x >= tmin3.z) axis = 0u;
+  else if (tmin3.y >= tmin3.z) axis = 1u;
+  else axis = 2u;
+  bool pos_dir[3] = {rd.x > 0.0f, rd.y > 0.0f, rd.z > 0.0f};
+  V3 pos = add(ro, muls(rd, t));
+  I3 cell = floor_i(pos);
+  if (t_enter > 0.0f) {
+    setc(cell, axis, pos_dir[axis] ? f2i(floorf(comp(bmin, axis))) : f2i(ceilf(comp(bmax, axis))) - 1);
+  }
+  cell = {std::min(std::max(cell.x, 0), 63), std::min(std::max(cell.y, 0), 63),
+          std::min(std::max(cell.z, 0), 63)};
+  U2 root_mask{c.root[0], c.root[1]};
+  uint32_t root_ptr = c.root[2] & VM_PTR_MASK;
+
+  bool water_aware = skip_water && (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
+  if (water_aware && (c.attr_flags & VM_ATTR_UNIFORM) != 0u) {
+    if (c.attr_base == VM_WATER) return h;
+    water_aware = false;
+  }
+  bool attr_uniform = (c.attr_flags & VM_ATTR_UNIFORM) != 0u;
+  bool foliage_aware = (c.attr_flags & VM_ATTR_HAS_FOLIAGE) != 0u;
+  if (foliage_aware && attr_uniform && !is_tuft(c.attr_base)) foliage_aware = false;
+  bool cutout_aware = (c.attr_flags & VM_ATTR_HAS_CUTOUT) != 0u && vs == 1.0f;
+  if (cutout_aware && attr_uniform && c.attr_base != VM_LEAVES && c.attr_base != VM_PINE_LEAVES)
+    cutout_aware = false;
+  bool glass_aware = skip_glass && (c.attr_flags & VM_ATTR_HAS_GLASS) != 0u;
+  if (glass_aware && attr_uniform) {
+    if (c.attr_base == VM_GLASS) return h;
+    glass_aware = false;
+  }
+  bool noncaster_aware = sun_ray && (c.attr_flags & VM_ATTR_HAS_EMITTER) != 0u;
+  if (noncaster_aware && attr_uniform && !casts_sun_shadow(c.attr_base)) return h;
+  bool water_interface = !skip_water && (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
+  bool attr_needed = (noncaster_aware && !attr_uniform) || (water_interface && !attr_uniform) ||
+                     water_aware || glass_aware || ((foliage_aware || cutout_aware) && !attr_uniform);
+
+  U2 trav_mask = root_mask;
+  if (water_aware) trav_mask = U2{c.dry_mask[0], c.dry_mask[1]};
+  bool root_full = (c.root[2] & VM_FULL_BIT) != 0u;
+  // SPEC_FULL_MARCH is on (its default), so the full-root short cut at
+  // common.wgsl:677-686 never fires.
+  if (trav_mask.x == 0u && trav_mask.y == 0u) return h;
+
+  uint32_t l1_cached = 0xFFFFFFFFu;
+  U4 l1{0u, 0u, 0u, 0u};
+  uint32_t leaf_cached = 0xFFFFFFFFu;
+  U2 leaf{0u, 0u};
+  uint32_t attr = 0u;
+  for (;;) {
+    h.iters += 1u;
+    cnt_add(&Counters::iters);
+    if (h.iters > VM_MAX_ITERS) break;
+    if (cell.x < 0 || cell.y < 0 || cell.z < 0 || cell.x > 63 || cell.y > 63 || cell.z > 63) break;
+    U3 uc{(uint32_t)cell.x, (uint32_t)cell.y, (uint32_t)cell.z};
+    int32_t skip = 16;
+    bool solid = false;
+    uint32_t l1b = cell_bit(ushr(uc, 4u));
+    if (mask_has(trav_mask, l1b)) {
+      if (l1b != l1_cached) {
+        l1_cached = l1b;
+        if (root_full) {
+          l1 = {0xFFFFFFFFu, 0xFFFFFFFFu, VM_FULL_BIT, (l1b * 64u) | 0xF0000000u};
+        } else {
+          cnt_add(&Counters::l1_fetches);
+          l1 = inner_at(w, (uint64_t)root_ptr + mask_below(root_mask, l1b));
+        }
+        leaf_cached = 0xFFFFFFFFu;
+      }
+      bool line_skip = false;
+      if (water_aware) {
+        uint32_t wl = l1.w >> 28u;
+        float ly = (float)(uc.y & 15u);
+        if (wl < 15u && ly > (float)wl) {
+          line_skip = rd.y >= 0.0f;
+          if (!line_skip) {
+            float hh = fmaxf(fabsf(rd.x), fabsf(rd.z));
+            if (hh > 1e-6f && (ly - (float)wl) > 16.0f * (fabsf(rd.y) / hh)) line_skip = true;
+          }
+        }
+      }
+      if (line_skip) {
+        skip = 16;
+      } else if ((l1.z & VM_FULL_BIT) != 0u) {
+        solid = true;
+        if (attr_needed) {
+          uint32_t lfb = cell_bit(uand(ushr(uc, 2u), 3u));
+          if (lfb != leaf_cached) {
+            leaf_cached = lfb;
+            cnt_add(&Counters::attr_fetches);
+            attr = brick_at(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + lfb);
+          }
+        }
+      } else {
+        U2 l1m{l1.x, l1.y};
+        uint32_t lfb = cell_bit(uand(ushr(uc, 2u), 3u));
+        if (mask_has(l1m, lfb)) {
+          if (lfb != leaf_cached) {
+            leaf_cached = lfb;
+            uint32_t li = mask_below(l1m, lfb);
+            cnt_add(&Counters::leaf_fetches);
+            leaf = leaf_at(w, (uint64_t)(l1.z & VM_PTR_MASK) + li);
+            if (attr_needed) {
+              cnt_add(&Counters::attr_fetches);
+              attr = brick_at(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + li);
+            }
+          }
+          uint32_t vb = cell_bit(uand(uc, 3u));
+          if (mask_has(leaf, vb)) {
+            solid = true;
+          } else {
+            uint32_t sh = vb & 42u;
+            uint32_t lo;
+            if (sh == 0u) lo = leaf.x;
+            else if (sh < 32u) lo = (leaf.x >> sh) | (leaf.y << (32u - sh));
+            else lo = leaf.y >> (sh - 32u);
+            skip = (lo & 0x00330033u) == 0u ? 2 : 1;
+          }
+        } else {
+          skip = 4;
+        }
+      }
+    } else {
+      uint32_t sh = l1b & 42u;
+      uint32_t rlo;
+      if (sh == 0u) rlo = trav_mask.x;
+      else if (sh < 32u) rlo = (trav_mask.x >> sh) | (trav_mask.y << (32u - sh));
+      else rlo = trav_mask.y >> (sh - 32u);
+      skip = (rlo & 0x00330033u) == 0u ? 32 : 16;
+    }
+    if (solid && noncaster_aware) {
+      uint32_t id = attr_uniform ? c.attr_base : leaf_block(w, attr, uc);
+      if (!casts_sun_shadow(id)) { solid = false; skip = 1; }
+    }
+    if (solid && water_interface) {
+      uint32_t id = attr_uniform ? c.attr_base : leaf_block(w, attr, uc);
+      if (id == VM_WATER) {
+        uint32_t nid = axis * 2u + (pos_dir[axis] ? 0u : 1u);
+        V3 outward = normal_of(nid);
+        V3 boundary = add(ro_w, muls(rd, t * vs));
+        if (world_block_at(w, add(boundary, muls(outward, 0.002f * vs))) == VM_WATER) {
+          solid = false;
+          skip = 1;
+        }
+      }
+    }
+    if (solid && water_aware) {
+      if (leaf_block(w, attr, uc) == VM_WATER) {
+        solid = false;
+        skip = (attr & VM_UNIFORM_BIT) != 0u ? 4 : 1;
+      }
+    }
+    if (solid && glass_aware) {
+      if (leaf_block(w, attr, uc) == VM_GLASS) {
+        solid = false;
+        skip = (attr & VM_UNIFORM_BIT) != 0u ? 4 : 1;
+      }
+    }
+    if (solid && foliage_aware) {
+      uint32_t bid = attr_uniform ? c.attr_base : leaf_block(w, attr, uc);
+      if (is_tuft(bid)) { solid = false; skip = 1; }
+    }
+    if (solid && cutout_aware) {
+      uint32_t bid = attr_uniform ? c.attr_base : leaf_block(w, attr, uc);
+      if (is_cutout_id(bid)) {
+        I3 wv{f2i(c.origin[0]) + (int32_t)uc.x, f2i(c.origin[1]) + (int32_t)uc.y,
+              f2i(c.origin[2]) + (int32_t)uc.z};
+        MicroHit q = cutout_march(wv, uc, ro, rd, t, axis, pos_dir, t > 0.0f);
+        if (q.hit) {
+          h.hit = true;
+          h.t = q.t * vs;
+          h.normal = q.normal;
+          h.voxel = uc;
+          h.micro = q.micro;
+          return h;
+        }
+        solid = false;
+        skip = 1;
+      }
+    }
+    if (solid) {
+      h.hit = true;
+      h.t = t * vs;
+      h.normal = axis * 2u + (pos_dir[axis] ? 0u : 1u);
+      h.voxel = uc;
+      h.micro = micro_entry(uc, ro, rd, t, axis, pos_dir, t > 0.0f);
+      return h;
+    }
+    I3 bmin_i{cell.x - (cell.x & (skip - 1)), cell.y - (cell.y & (skip - 1)), cell.z - (cell.z & (skip - 1))};
+    I3 bmax_i{bmin_i.x + skip, bmin_i.y + skip, bmin_i.z + skip};
+    V3 bounds = v3((float)(pos_dir[0] ? bmax_i.x : bmin_i.x), (float)(pos_dir[1] ? bmax_i.y : bmin_i.y),
+                   (float)(pos_dir[2] ? bmax_i.z : bmin_i.z));
+    V3 tn = mul(sub(bounds, ro), inv);
+    if (tn.x <= tn.y && tn.x <= tn.z) { t = tn.x; axis = 0u; }
+    else if (tn.y <= tn.z) { t = tn.y; axis = 1u; }
+    else { t = tn.z; axis = 2u; }
+    if (t >= t_end) break;
+    pos = add(ro, muls(rd, t));
+    cell = floor_i(pos);
+    setc(cell, axis, pos_dir[axis] ? comp(bmax_i, axis) : comp(bmin_i, axis) - 1);
+  }
+  return h;
+}
+
+// shadow_ray_t: common.wgsl:1156-1195
+float shadow_ray_t(const World& w, V3 ro, V3 rd, float max_dist) {
+  V3 inv = v3(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+  bool pos_dir[3] = {rd.x > 0.0f, rd.y > 0.0f, rd.z > 0.0f};
+  I3 cell = floor_i(divs(ro, 64.0f));
+  float t = 0.0f;
+  uint32_t last = VM_NO_CHUNK;
+  for (uint32_t i = 0; i < 24u; ++i) {
+    I3 rel{cell.x - w.f->grid_min[0], cell.y - w.f->grid_min[1], cell.z - w.f->grid_min[2]};
+    if (grid_outside(w, rel)) return -1.0f;
+    cnt_add(&Counters::grid_lookups);
+    uint32_t ci = grid_at(w, grid_index(w, rel));
+    if (ci != VM_NO_CHUNK && ci != last) {
+      last = ci;
+      Hit m = march_chunk(w, ci, ro, rd, max_dist, true, true, true, true);
+      if (m.hit) return m.t;
+    }
+    V3 bounds = muls(v3((float)(pos_dir[0] ? cell.x + 1 : cell.x), (float)(pos_dir[1] ? cell.y + 1 : cell.y),
+                        (float)(pos_dir[2] ? cell.z + 1 : cell.z)), 64.0f);
+    V3 tn = mul(sub(bounds, ro), inv);
+    uint32_t axis = 0u;
+    if (tn.x <= tn.y && tn.x <= tn.z) { t = tn.x; }
+    else if (tn.y <= tn.z) { t = tn.y; axis = 1u; }
+    else { t = tn.z; axis = 2u; }
+    if (t >= max_dist) return -1.0f;
+    setc(cell, axis, comp(cell, axis) + (pos_dir[axis] ? 1 : -1));
+  }
+  return -1.0f;
+}
+
+struct WorldHit { bool hit; float t; uint32_t normal; U3 voxel; uint32_t ci; };
+
+// trace_world: common.wgsl:1205-1253
+WorldHit trace_world(const World& w, V3 ro, V3 rd, float max_dist, bool skip_water) {
+  WorldHit out{false, max_dist, 0u, {0u, 0u, 0u}, VM_NO_CHUNK};
+  V3 dir;
+  dir.x = fabsf(rd.x) < 1e-6f ? 1e-6f * signf(rd.x + 1e-9f) : rd.x;
+  dir.y = fabsf(rd.y) < 1e-6f ? 1e-6f * signf(rd.y + 1e-9f) : rd.y;
+  dir.z = fabsf(rd.z) < 1e-6f ? 1e-6f * signf(rd.z + 1e-9f) : rd.z;
+  V3 inv = v3(1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z);
+  bool pos_dir[3] = {dir.x > 0.0f, dir.y > 0.0f, dir.z > 0.0f};
+  I3 cell = floor_i(divs(ro, 64.0f));
+  for (uint32_t i = 0; i < 16u; ++i) {
+    I3 rel{cell.x - w.f->grid_min[0], cell.y - w.f->grid_min[1], cell.z - w.f->grid_min[2]};
+    if (grid_outside(w, rel)) return out;
+    cnt_add(&Counters::grid_lookups);
+    uint32_t ci = grid_at(w, grid_index(w, rel));
+    V3 bounds = muls(v3((float)(pos_dir[0] ? cell.x + 1 : cell.x), (float)(pos_dir[1] ? cell.y + 1 : cell.y),
+                        (float)(pos_dir[2] ? cell.z + 1 : cell.z)), 64.0f);
+    V3 tn = mul(sub(bounds, ro), inv);
+    float t_exit = tn.x;
+    uint32_t axis = 0u;
+    if (tn.y < t_exit) { t_exit = tn.y; axis = 1u; }
+    if (tn.z < t_exit) { t_exit = tn.z; axis = 2u; }
+    if (ci != VM_NO_CHUNK) {
+      Hit h = march_chunk(w, ci, ro, rd, fminf(t_exit, max_dist), skip_water, false, true, false);
+      if (h.hit) {
+        out.hit = true; out.t = h.t; out.normal = h.normal; out.voxel = h.voxel; out.ci = ci;
+        return out;
+      }
+    }
+    if (t_exit >= max_dist) return out;
+    setc(cell, axis, comp(cell, axis) + (pos_dir[axis] ? 1 : -1));
+  }
+  return out;
+}
+
+// hit_t: common.wgsl:1300-1318
+float hit_t(const World& w, uint32_t ci, U3 v, U3 micro, uint32_t normal_id, V3 rd) {
+  const vm_chunk& c = chunk_at(w, ci);
+  const vm_frame& f = *w.f;
+  V3 box_min = add(ld3(c.origin), muls(v3((float)v.x, (float)v.y, (float)v.z), c.voxel_size));
+  if (normal_id >= VM_NORMAL_CROSS_A) {
+    if (normal_id == VM_NORMAL_CROSS_A)
+      return ((box_min.x - box_min.z) - (f.cam_pos[0] - f.cam_pos[2])) / (rd.x - rd.z);
+    return ((box_min.x + box_min.z + c.voxel_size) - (f.cam_pos[0] + f.cam_pos[2])) / (rd.x + rd.z);
+  }
+  uint32_t axis = normal_id >> 1u;
+  float ms = c.voxel_size / 4.0f;
+  uint32_t mi = axis == 0 ? micro.x : (axis == 1 ? micro.y : micro.z);
+  float plane = comp(box_min, axis) + (float)(mi + ((normal_id & 1u) == 1u ? 1u : 0u)) * ms;
+  return (plane - f.cam_pos[axis]) / comp(rd, axis);
+}
+
+// depth_key / make_key: common.wgsl:1320-1330
+inline uint32_t depth_key(const vm_frame& f, float t) {
+  float x = 1.0f - t / f.far_;
+  x = fminf(fmaxf(x, 0.0f), 1.0f);
+  return f2u(x * 16777215.0f);
+}
+inline uint64_t make_key(const vm_frame& f, float t, uint32_t normal, uint32_t ci, U3 v, U3 micro) {
+  uint64_t d = depth_key(f, t);
+  uint32_t bx = v.x | (micro.x << 6u), by = v.y | (micro.y << 6u), bz = v.z | (micro.z << 6u);
+  return (d << 40) | ((uint64_t)normal << 37) | ((uint64_t)ci << 24) |
+         (uint64_t)((bx << 16u) | (by << 8u) | bz);
+}
+
+// tile_select geometry: tile_select.wgsl:1-9
+inline bool box_outside(V3 bmin, V3 bmax, V3 n, V3 cam) {
+  V3 p{n.x > 0.0f ? bmax.x : bmin.x, n.y > 0.0f ? bmax.y : bmin.y, n.z > 0.0f ? bmax.z : bmin.z};
+  return dot(n, sub(p, cam)) < 0.0f;
+}
+inline float box_distance(V3 p, V3 bmin, V3 bmax) {
+  return length(vmax(vmax(sub(bmin, p), sub(p, bmax)), v3(0.0f, 0.0f, 0.0f)));
+}
+
+struct TileCull {
+  V3 n[4];
+  float reach;
+};
+
+// per-tile planes and reach: tile_select.wgsl:11-57
+TileCull tile_planes(const vm_frame& f, uint32_t tx, uint32_t ty) {
+  float x0 = (float)(tx * 8u), y0 = (float)(ty * 8u);
+  float x1 = x0 + 8.0f, y1 = y0 + 8.0f;
+  V3 d00 = ray_dir(f, x0, y0), d10 = ray_dir(f, x1, y0), d11 = ray_dir(f, x1, y1), d01 = ray_dir(f, x0, y1);
+  V3 center = ray_dir(f, (x0 + x1) * 0.5f, (y0 + y1) * 0.5f);
+  TileCull tc;
+  tc.n[0] = cross(d00, d10);
+  tc.n[1] = cross(d10, d11);
+  tc.n[2] = cross(d11, d01);
+  tc.n[3] = cross(d01, d00);
+  for (int i = 0; i < 4; ++i) if (!(dot(tc.n[i], center) >= 0.0f)) tc.n[i] = neg(tc.n[i]);
+  V3 cam = ld3(f.cam_pos);
+  float reach = f.far_;
+  const uint32_t both = VM_FLAG_UNDERWATER | VM_FLAG_WATER_FAR;
+  if ((f.flags & both) == both) {
+    float up = fmaxf(fmaxf(d00.y, d10.y), fmaxf(d11.y, d01.y));
+    float submerged = fmaxf(f.sea_level - cam.y, 0.0f);
+    float escape = 1e30f;
+    if (up > 0.0f) escape = submerged / up;
+    if (escape >= VM_WATER_FAR_DIST) {
+      reach = fminf(f.far_, VM_WATER_FAR_DIST);
+      float dep_far = submerged - up * VM_WATER_FAR_DIST;
+      if ((f.flags & VM_FLAG_WATER_DARK) != 0u && fminf(submerged, dep_far) >= VM_WATER_DARK_DEPTH)
+        reach = fminf(reach, VM_WATER_DARK_DIST);
+    }
+  }
+  tc.reach = reach;
+  return tc;
+}
+
+// refract per the WGSL builtin definition
+V3 refract(V3 e1, V3 e2, float e3) {
+  float d = dot(e2, e1);
+  float k = 1.0f - e3 * e3 * (1.0f - d * d);
+  if (k < 0.0f) return v3(0.0f, 0.0f, 0.0f);
+  return sub(muls(e1, e3), muls(e2, e3 * d + sqrtf(k)));
+}
+
+inline float smoothstep(float e0, float e1, float x) {
+  float t = fminf(fmaxf((x - e0) / (e1 - e0), 0.0f), 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+
+inline U3 key_voxel(uint64_t key) {
+  uint32_t low = (uint32_t)(key & 0xFFFFFFull);
+  return {(low >> 16u) & 63u, (low >> 8u) & 63u, low & 63u};
+}
+inline U3 key_micro(uint64_t key) {
+  uint32_t low = (uint32_t)(key & 0xFFFFFFull);
+  return {(low >> 22u) & 3u, (low >> 14u) & 3u, (low >> 6u) & 3u};
+}
+inline uint32_t key_ci(uint64_t key) { return (uint32_t)(key >> 24) & 0x1FFFu; }
+inline uint32_t key_nid(uint64_t key) { return (uint32_t)(key >> 37) & 7u; }
+
+}  // namespace
+
+// ============================================================================
+// C ABI of the oracle (loaded with ctypes by tests/ and bench.py)
+// ============================================================================
+extern "C" {
+
+typedef struct or_world {
+  const vm_frame* frame;
+  const vm_chunk* chunks; uint32_t n_chunks;
+  const uint32_t* inners; uint64_t n_inners;
+  const uint32_t* leaves; uint64_t n_leaves;
+  const uint32_t* bricks; uint64_t n_bricks;
+  const uint32_t* grid; uint64_t n_grid;
+} or_world;
+
+typedef struct or_hit {
+  uint32_t hit; float t; uint32_t normal; uint32_t voxel[3]; uint32_t micro[3]; uint32_t iters;
+} or_hit;
+
+typedef struct or_counters {
+  uint64_t chunk_records, l1_fetches, leaf_fetches, attr_fetches, palette_decodes, grid_lookups,
+      iters, march_calls, rays;
+} or_counters;
+
+static World mk(const or_world* o) {
+  World w;
+  w.f = o->frame; w.chunks = o->chunks; w.n_chunks = o->n_chunks;
+  w.inners = o->inners; w.n_inners = o->n_inners;
+  w.leaves = o->leaves; w.n_leaves = o->n_leaves;
+  w.bricks = o->bricks; w.n_bricks = o->n_bricks;
+  w.grid = o->grid; w.n_grid = o->n_grid;
+  return w;
+}
+
+int or_last_error(char* buf, int len) {
+  int e = g_err.load();
+  if (e && buf && len > 0) { strncpy(buf, g_err_msg, len - 1); buf[len - 1] = 0; }
+  return e;
+}
+void or_clear_error(void) { g_err.store(0); g_err_msg[0] = 0; }
+
+void or_ray_dir(const vm_frame* f, float px, float py, float* out) {
+  V3 d = ray_dir(*f, px, py);
+  out[0] = d.x; out[1] = d.y; out[2] = d.z;
+}
+
+int or_march_chunk(const or_world* o, uint32_t ci, const float* ro, const float* rd, float t_limit,
+                   uint32_t skip_water, uint32_t skip_foliage, uint32_t skip_glass, uint32_t sun_ray,
+                   or_hit* out) {
+  World w = mk(o);
+  Hit h = march_chunk(w, ci, ld3(ro), ld3(rd), t_limit, skip_water, skip_foliage, skip_glass, sun_ray);
+  out->hit = h.hit; out->t = h.t; out->normal = h.normal;
+  out->voxel[0] = h.voxel.x; out->voxel[1] = h.voxel.y; out->voxel[2] = h.voxel.z;
+  out->micro[0] = h.micro.x; out->micro[1] = h.micro.y; out->micro[2] = h.micro.z;
+  out->iters = h.iters;
+  return g_err.load();
+}
+
+float or_shadow_ray_t(const or_world* o, const float* ro, const float* rd, float max_dist) {
+  World w = mk(o);
+  return shadow_ray_t(w, ld3(ro), ld3(rd), max_dist);
+}
+
+int or_trace_world(const or_world* o, const float* ro, const float* rd, float max_dist,
+                   uint32_t skip_water, uint32_t* hit, float* t, uint32_t* normal, uint32_t* voxel,
+                   uint32_t* ci) {
+  World w = mk(o);
+  WorldHit h = trace_world(w, ld3(ro), ld3(rd), max_dist, skip_water);
+  *hit = h.hit; *t = h.t; *normal = h.normal;
+  voxel[0] = h.voxel.x; voxel[1] = h.voxel.y; voxel[2] = h.voxel.z; *ci = h.ci;
+  return g_err.load();
+}
+
+uint32_t or_block_at(const or_world* o, uint32_t ci, const uint32_t* v) {
+  World w = mk(o);
+  return block_at(w, ci, U3{v[0], v[1], v[2]});
+}
+
+uint32_t or_world_block_at(const or_world* o, const float* p) {
+  World w = mk(o);
+  return world_block_at(w, ld3(p));
+}
+
+uint64_t or_make_key(const vm_frame* f, float t, uint32_t normal, uint32_t ci, const uint32_t* v,
+                     const uint32_t* micro) {
+  return make_key(*f, t, normal, ci, U3{v[0], v[1], v[2]}, U3{micro[0], micro[1], micro[2]});
+}
+
+uint32_t or_depth_key(const vm_frame* f, float t) { return depth_key(*f, t); }
+
+uint32_t or_leaf_solid(const int32_t* wv, const uint32_t* m) {
+  return leaf_solid(I3{wv[0], wv[1], wv[2]}, U3{m[0], m[1], m[2]});
+}
+
+// The reference's frame: tile_select (+Hi-Z deferral) -> march every pair ->
+// [build_hiz -> recover_select -> march recovered] (src/render/mod.rs:1738-1794).
+// vis[] receives max() of every pair's key, exactly the atomicMax fold of the
+// reference.  hiz_in is the previous frame's tile buffer (read when FLAG_HIZ);
+// hiz_out receives this frame's build_hiz result (FLAG_HIZ) or zeros.
+// counters: [0] select count, [1] deferred, [2] recovered, [3] pairs marched,
+// [4] raw select, [5] raw recover (tile_select.wgsl:112-141).
+// Tiles [tile_begin, tile_end) are processed; pixels outside them are untouched.
+int or_frame(const or_world* o, const uint32_t* hiz_in, uint64_t* vis, uint32_t* hiz_out,
+             uint32_t* counters, uint32_t* dbg, uint32_t tile_begin, uint32_t tile_end,
+             int threads, or_counters* traffic) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  const uint32_t tiles_x = f.tiles[0];
+  const uint32_t n_tiles = f.tiles[0] * f.tiles[1];
+  if (tile_end > n_tiles) tile_end = n_tiles;
+  const bool use_hiz = (f.flags & VM_FLAG_HIZ) != 0u;
+  const bool underwater = (f.flags & VM_FLAG_UNDERWATER) != 0u;
+  const bool heat = (f.flags & VM_FLAG_HEATMAP) != 0u && dbg;
+  V3 cam = ld3(f.cam_pos);
+  uint64_t c_sel = 0, c_def = 0, c_rec = 0;
+  Counters total{};
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel reduction(+ : c_sel, c_def, c_rec)
+  {
+    Counters local{};
+    t_cnt = traffic ? &local : nullptr;
+    std::vector<uint32_t> sel, def;
+#pragma omp for schedule(dynamic, 4)
+    for (int64_t tid = tile_begin; tid < (int64_t)tile_end; ++tid) {
+      uint32_t tile_id = (uint32_t)tid;
+      uint32_t tx = tile_id % tiles_x, ty = tile_id / tiles_x;
+      TileCull tc = tile_planes(f, tx, ty);
+      uint32_t tile_far = use_hiz && hiz_in ? hiz_in[tile_id] : 0u;
+      sel.clear(); def.clear();
+      for (uint32_t ci = 0; ci < f.chunk_count; ++ci) {
+        const vm_chunk& c = chunk_at(w, ci);
+        if (ci == f.camera_chunk) { sel.push_back(ci); continue; }
+        V3 bmin = ld3(c.aabb_min), bmax = ld3(c.aabb_max);
+        if (box_outside(bmin, bmax, ld3(f.cam_fwd), cam)) continue;
+        bool out = false;
+        for (int i = 0; i < 4 && !out; ++i) out = box_outside(bmin, bmax, tc.n[i], cam);
+        if (out) continue;
+        float dmin = box_distance(cam, bmin, bmax);
+        if (dmin >= tc.reach) continue;
+        if (use_hiz && depth_key(f, dmin) < tile_far) { def.push_back(ci); continue; }
+        sel.push_back(ci);
+      }
+      c_sel += sel.size();
+      c_def += def.size();
+      auto march_list = [&](const std::vector<uint32_t>& list) {
+        for (uint32_t ci : list) {
+          const vm_chunk& c = chunk_at(w, ci);
+          for (uint32_t ly = 0; ly < 8u; ++ly)
+            for (uint32_t lx = 0; lx < 8u; ++lx) {
+              uint32_t px = tx * 8u + lx, py = ty * 8u + ly;
+              if (px >= f.res[0] || py >= f.res[1]) continue;
+              if (ray_skips(f, c.fade, px, py)) continue;
+              V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+              Hit h = march_chunk(w, ci, cam, rd, f.far_, underwater, false, false, false);
+              uint64_t pix = (uint64_t)py * f.res[0] + px;
+              if (h.hit) {
+                uint64_t k = make_key(f, h.t, h.normal, ci, h.voxel, h.micro);
+                if (k > vis[pix]) vis[pix] = k;
+              }
+              if (heat) dbg[pix] += h.iters;
+            }
+        }
+      };
+      // clear this tile's pixels
+      for (uint32_t ly = 0; ly < 8u; ++ly)
+        for (uint32_t lx = 0; lx < 8u; ++lx) {
+          uint32_t px = tx * 8u + lx, py = ty * 8u + ly;
+          if (px >= f.res[0] || py >= f.res[1]) continue;
+          vis[(uint64_t)py * f.res[0] + px] = 0;
+          cnt_add(&Counters::rays);
+          if (heat) dbg[(uint64_t)py * f.res[0] + px] = 0;
+        }
+      march_list(sel);
+      uint32_t hz = 0u;
+      if (use_hiz) {
+        // build_hiz: march.wgsl:57-76
+        uint32_t m = 0xFFFFFFFFu;
+        for (uint32_t ly = 0; ly < 8u; ++ly)
+          for (uint32_t lx = 0; lx < 8u; ++lx) {
+            uint32_t px = tx * 8u + lx, py = ty * 8u + ly;
+            uint32_t d = 0u;
+            if (px < f.res[0] && py < f.res[1]) d = (uint32_t)(vis[(uint64_t)py * f.res[0] + px] >> 40);
+            m = std::min(m, d);
+          }
+        hz = m;
+        // recover_select: tile_select.wgsl:94-110
+        std::vector<uint32_t> rec;
+        for (uint32_t ci : def) {
+          const vm_chunk& c = chunk_at(w, ci);
+          float dmin = box_distance(cam, ld3(c.aabb_min), ld3(c.aabb_max));
+          if (depth_key(f, dmin) >= hz) rec.push_back(ci);
+        }
+        c_rec += rec.size();
+        march_list(rec);
+      }
+      if (hiz_out) hiz_out[tile_id] = hz;
+    }
+    if (traffic) {
+#pragma omp critical
+      {
+        total.chunk_records += local.chunk_records; total.l1_fetches += local.l1_fetches;
+        total.leaf_fetches += local.leaf_fetches; total.attr_fetches += local.attr_fetches;
+        total.palette_decodes += local.palette_decodes; total.grid_lookups += local.grid_lookups;
+        total.iters += local.iters; total.march_calls += local.march_calls; total.rays += local.rays;
+      }
+    }
+    t_cnt = nullptr;
+  }
+  if (counters) {
+    uint32_t mp = f.max_pairs;
+    counters[1] = (uint32_t)c_def;
+    counters[2] = (uint32_t)c_rec;
+    counters[4] = (uint32_t)c_sel;
+    counters[3] = std::min<uint32_t>((uint32_t)c_sel, mp);
+    counters[5] = (uint32_t)c_rec;
+    counters[0] = use_hiz ? std::min<uint32_t>((uint32_t)c_rec, mp) : (uint32_t)c_sel;
+  }
+  if (traffic) {
+    traffic->chunk_records = total.chunk_records; traffic->l1_fetches = total.l1_fetches;
+    traffic->leaf_fetches = total.leaf_fetches; traffic->attr_fetches = total.attr_fetches;
+    traffic->palette_decodes = total.palette_decodes; traffic->grid_lookups = total.grid_lookups;
+    traffic->iters = total.iters; traffic->march_calls = total.march_calls; traffic->rays = total.rays;
+  }
+  return g_err.load();
+}
+
+// The per-tile pair list of tile_select for one tile (ascending chunk index),
+// for tests of the culling itself.  Returns the number written (<= cap).
+uint32_t or_tile_pairs(const or_world* o, uint32_t tile_id, const uint32_t* hiz_in, uint32_t* out,
+                       uint32_t cap, uint32_t* deferred, uint32_t dcap, uint32_t* n_def) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  TileCull tc = tile_planes(f, tile_id % f.tiles[0], tile_id / f.tiles[0]);
+  V3 cam = ld3(f.cam_pos);
+  const bool use_hiz = (f.flags & VM_FLAG_HIZ) != 0u;
+  uint32_t tile_far = use_hiz && hiz_in ? hiz_in[tile_id] : 0u;
+  uint32_t n = 0, nd = 0;
+  for (uint32_t ci = 0; ci < f.chunk_count; ++ci) {
+    const vm_chunk& c = chunk_at(w, ci);
+    if (ci == f.camera_chunk) { if (n < cap) out[n] = ci; ++n; continue; }
+    V3 bmin = ld3(c.aabb_min), bmax = ld3(c.aabb_max);
+    if (box_outside(bmin, bmax, ld3(f.cam_fwd), cam)) continue;
+    bool outb = false;
+    for (int i = 0; i < 4 && !outb; ++i) outb = box_outside(bmin, bmax, tc.n[i], cam);
+    if (outb) continue;
+    float dmin = box_distance(cam, bmin, bmax);
+    if (dmin >= tc.reach) continue;
+    if (use_hiz && depth_key(f, dmin) < tile_far) { if (nd < dcap) deferred[nd] = ci; ++nd; continue; }
+    if (n < cap) out[n] = ci;
+    ++n;
+  }
+  if (n_def) *n_def = nd;
+  return n;
+}
+
+// primary_shadow: shadow.wgsl:8-48 (per pixel blocker distance; 0 = lit).
+int or_primary_shadow(const or_world* o, const uint64_t* vis, float* out, uint64_t pix_begin,
+                      uint64_t pix_end, int threads, or_counters* traffic) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  uint64_t npix = (uint64_t)f.res[0] * f.res[1];
+  if (pix_end > npix) pix_end = npix;
+  const bool active = (f.flags & VM_FLAG_SHADOWS) != 0u && (f.flags & VM_FLAG_HEATMAP) == 0u &&
+                      f.daylight > 0.01f;
+  V3 sun = ld3(f.sun_dir);
+  V3 cam = ld3(f.cam_pos);
+  Counters total{};
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel
+  {
+    Counters local{};
+    t_cnt = traffic ? &local : nullptr;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t pi = (int64_t)pix_begin; pi < (int64_t)pix_end; ++pi) {
+      uint64_t pix = (uint64_t)pi;
+      float distance = 0.0f;
+      if (active) {
+        uint64_t key = vis[pix];
+        if (key != 0ull) {
+          uint32_t ci = key_ci(key);
+          U3 v = key_voxel(key);
+          uint32_t id = block_at(w, ci, v);
+          if (!(id == VM_WATER || id == VM_GLASS)) {
+            uint32_t nid = key_nid(key);
+            U3 micro = key_micro(key);
+            uint32_t px = (uint32_t)(pix % f.res[0]), py = (uint32_t)(pix / f.res[0]);
+            V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+            V3 n = normal_of(nid);
+            if (nid >= VM_NORMAL_CROSS_A && dot(n, rd) > 0.0f) n = neg(n);
+            if (dot(n, sun) > 0.0f) {
+              float t = hit_t(w, ci, v, micro, nid, rd);
+              V3 hit = add(cam, muls(rd, t));
+              float scale = chunk_at(w, ci).voxel_size;
+              if (t >= 0.0f) {
+                cnt_add(&Counters::rays); float blocker = shadow_ray_t(w, add(hit, muls(n, 0.02f * scale)), sun, f.shadow_dist);
+                if (blocker >= 0.0f) distance = fminf(fmaxf(blocker, 0.001f), 65504.0f);
+              }
+            }
+          }
+        }
+      }
+      out[pix] = distance;
+    }
+    if (traffic) {
+#pragma omp critical
+      {
+        total.chunk_records += local.chunk_records; total.l1_fetches += local.l1_fetches;
+        total.leaf_fetches += local.leaf_fetches; total.attr_fetches += local.attr_fetches;
+        total.palette_decodes += local.palette_decodes; total.grid_lookups += local.grid_lookups;
+        total.iters += local.iters; total.march_calls += local.march_calls; total.rays += local.rays;
+      }
+    }
+    t_cnt = nullptr;
+  }
+  if (traffic) {
+    traffic->chunk_records = total.chunk_records; traffic->l1_fetches = total.l1_fetches;
+    traffic->leaf_fetches = total.leaf_fetches; traffic->attr_fetches = total.attr_fetches;
+    traffic->palette_decodes = total.palette_decodes; traffic->grid_lookups = total.grid_lookups;
+    traffic->iters = total.iters; traffic->march_calls = total.march_calls; traffic->rays = total.rays;
+  }
+  return g_err.load();
+}
+
+// One water-refraction or glass-transmission secondary ray per visible hit:
+// water  -> water_refract_leg (resolve.wgsl:1029-1042), gated as water_sec /
+//           water_compose gate it (FLAG_WATER_REFRACT, refract_detail > 0,
+//           resolve.wgsl:1098,1524);
+// glass  -> shade_glass's transmission trace (resolve.wgsl:1261-1280).
+// sec_key: 0 = no secondary ray; else bit 63 = traced, bit 62 = hit, bit 61 =
+// glass (else water), bits 37-39 normal, 24-36 chunk, 0-23 voxel (x<<16|y<<8|z).
+// sec_t: hit distance along the secondary ray, or its max distance on a miss.
+int or_secondary(const or_world* o, const uint64_t* vis, uint64_t* sec_key, float* sec_t,
+                 uint64_t pix_begin, uint64_t pix_end, int threads) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  uint64_t npix = (uint64_t)f.res[0] * f.res[1];
+  if (pix_end > npix) pix_end = npix;
+  V3 cam = ld3(f.cam_pos);
+  const float inv_ior = 1.0f / VM_WATER_IOR;
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t pi = (int64_t)pix_begin; pi < (int64_t)pix_end; ++pi) {
+    uint64_t pix = (uint64_t)pi;
+    uint64_t out_key = 0ull;
+    float out_t = 0.0f;
+    uint64_t key = vis[pix];
+    if (key != 0ull) {
+      uint32_t ci = key_ci(key);
+      U3 v = key_voxel(key);
+      uint32_t id = block_at(w, ci, v);
+      bool water = id == VM_WATER, glass = id == VM_GLASS;
+      if (water || glass) {
+        uint32_t nid = key_nid(key);
+        U3 micro = key_micro(key);
+        uint32_t px = (uint32_t)(pix % f.res[0]), py = (uint32_t)(pix / f.res[0]);
+        V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+        float t = hit_t(w, ci, v, micro, nid, rd);
+        V3 hit = add(cam, muls(rd, t));
+        bool traced = false;
+        WorldHit h2{};
+        if (water) {
+          float detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, t);
+          if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && detail > 0.0f) {
+            V3 rdir = refract(rd, normal_of(nid), inv_ior);
+            V3 ro2 = add(hit, muls(rdir, VM_SURFACE_EPS));
+            h2 = trace_world(w, ro2, rdir, VM_WATER_REFRACT_DIST, true);
+            traced = true;
+          }
+        } else {
+          V3 ro2 = add(hit, muls(rd, VM_SURFACE_EPS));
+          h2 = trace_world(w, ro2, rd, fmaxf(VM_GLASS_TRANSMIT_DIST, f.far_), false);
+          traced = true;
+        }
+        if (traced) {
+          out_key = (1ull << 63) | (glass ? (1ull << 61) : 0ull);
+          if (h2.hit) {
+            out_key |= (1ull << 62) | ((uint64_t)h2.normal << 37) | ((uint64_t)h2.ci << 24) |
+                       (uint64_t)((h2.voxel.x << 16u) | (h2.voxel.y << 8u) | h2.voxel.z);
+          }
+          out_t = h2.t;
+        }
+      }
+    }
+    sec_key[pix] = out_key;
+    sec_t[pix] = out_t;
+  }
+  return g_err.load();
+}
+
+// Expanded visibility (voxel index, face, hit distance) from the raw keys:
+// voxel index = X*(Z*y + z) + x over the world box [origin, origin+dims),
+// face = the key's normal id, t = hit_t (common.wgsl:1300).  Misses give
+// voxel 0xFFFFFFFF, face 0xFF, t 0.
+int or_expand(const or_world* o, const uint64_t* vis, const int32_t* wmin, const uint32_t* wdim,
+              uint32_t* voxel, uint8_t* face, float* tout, int threads) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  uint64_t npix = (uint64_t)f.res[0] * f.res[1];
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(static)
+  for (int64_t pi = 0; pi < (int64_t)npix; ++pi) {
+    uint64_t key = vis[pi];
+    if (key == 0ull) { voxel[pi] = 0xFFFFFFFFu; face[pi] = 0xFF; tout[pi] = 0.0f; continue; }
+    uint32_t ci = key_ci(key);
+    U3 v = key_voxel(key);
+    U3 micro = key_micro(key);
+    uint32_t nid = key_nid(key);
+    const vm_chunk& c = chunk_at(w, ci);
+    int32_t vs = f2i(c.voxel_size);
+    int32_t wx = f2i(c.origin[0]) + (int32_t)v.x * vs - wmin[0];
+    int32_t wy = f2i(c.origin[1]) + (int32_t)v.y * vs - wmin[1];
+    int32_t wz = f2i(c.origin[2]) + (int32_t)v.z * vs - wmin[2];
+    voxel[pi] = (uint32_t)wx + wdim[0] * ((uint32_t)wz + wdim[2] * (uint32_t)wy);
+    face[pi] = (uint8_t)nid;
+    uint32_t px = (uint32_t)(pi % f.res[0]), py = (uint32_t)(pi / f.res[0]);
+    V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+    tout[pi] = hit_t(w, ci, v, micro, nid, rd);
+  }
+  return g_err.load();
+}
+
+// Block lookup through the chunk grid (lod-0 chunks), for the unit DDA below.
+static uint32_t grid_block(const World& w, int32_t x, int32_t y, int32_t z) {
+  I3 cell{x >> 6, y >> 6, z >> 6};
+  I3 rel{cell.x - w.f->grid_min[0], cell.y - w.f->grid_min[1], cell.z - w.f->grid_min[2]};
+  if (grid_outside(w, rel)) return 0u;
+  uint32_t ci = grid_at(w, grid_index(w, rel));
+  if (ci == VM_NO_CHUNK) return 0u;
+  const vm_chunk& c = chunk_at(w, ci);
+  I3 v{x - f2i(c.origin[0]), y - f2i(c.origin[1]), z - f2i(c.origin[2])};
+  if (!voxel_occupied(w, ci, v)) return 0u;
+  return block_at(w, ci, U3{(uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z});
+}
+
+uint32_t or_grid_block(const or_world* o, int32_t x, int32_t y, int32_t z) {
+  World w = mk(o);
+  return grid_block(w, x, y, z);
+}
+
+// Unit-voxel Amanatides-Woo walk over block lookups, restating Player::pick
+// (src/player.rs:334-393) with a caller-chosen step cap and reach.  A block
+// counts as solid when its id is nonzero.  Returns 1 and the block / entry
+// normal / distance on a hit.
+int or_pick(const or_world* o, const float* orig, const float* dir, uint32_t max_steps, float reach,
+            int32_t* block, int32_t* normal, float* dist) {
+  World w = mk(o);
+  V3 ro = ld3(orig), d = ld3(dir);
+  I3 cell = floor_i(ro);
+  I3 step{(int32_t)signf(d.x), (int32_t)signf(d.y), (int32_t)signf(d.z)};
+  V3 inv{fabsf(1.0f / d.x), fabsf(1.0f / d.y), fabsf(1.0f / d.z)};
+  V3 tmax{d.x > 0.0f ? ((float)cell.x + 1.0f - ro.x) * inv.x : (ro.x - (float)cell.x) * inv.x,
+          d.y > 0.0f ? ((float)cell.y + 1.0f - ro.y) * inv.y : (ro.y - (float)cell.y) * inv.y,
+          d.z > 0.0f ? ((float)cell.z + 1.0f - ro.z) * inv.z : (ro.z - (float)cell.z) * inv.z};
+  I3 nrm{0, 0, 0};
+  float t = 0.0f;
+  for (uint32_t i = 0; i < max_steps; ++i) {
+    if (grid_block(w, cell.x, cell.y, cell.z) != 0u) {
+      block[0] = cell.x; block[1] = cell.y; block[2] = cell.z;
+      normal[0] = nrm.x; normal[1] = nrm.y; normal[2] = nrm.z;
+      *dist = t;
+      return 1;
+    }
+    if (tmax.x < tmax.y && tmax.x < tmax.z) {
+      t = tmax.x; tmax.x += inv.x; cell.x += step.x; nrm = {-step.x, 0, 0};
+    } else if (tmax.y < tmax.z) {
+      t = tmax.y; tmax.y += inv.y; cell.y += step.y; nrm = {0, -step.y, 0};
+    } else {
+      t = tmax.z; tmax.z += inv.z; cell.z += step.z; nrm = {0, 0, -step.z};
+    }
+    if (t > reach) break;
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,317 @@
+"""Parity of the CUDA march with the oracle, through the C ABI.
+
+Bar: visibility keys, shadow blocker distances, secondary keys and distances,
+voxel indices and faces are compared bit for bit; hit distances are held to
+1e-5 relative (and are bit-exact here because both sides follow the same
+float contract)."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from voxelcraft_menu_b200 import world as W
+from voxelcraft_menu_b200.march import MarchError, Marcher, TILE_SHAPES
+from voxelcraft_menu_b200.world import Camera, Recipe, World
+
+pytestmark = pytest.mark.gpu
+
+T_RTOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def small():
+    w = World.generate(W.recipe_small_terrain())
+    pools = w.pools()
+    m = Marcher(1920, 1080)
+    m.upload_world(*pools)
+    return w, pools, m
+
+
+@pytest.fixture(scope="module")
+def large():
+    rec = W.recipe_large_terrain()
+    w = World.generate(rec)
+    pools = w.pools()
+    m = Marcher(1920, 1080)
+    m.upload_world(*pools)
+    return rec, w, pools, m
+
+
+def oracle_all(view, pools, hiz_in=None, tiles=None):
+    o = Oracle(view, *pools)
+    vis, hiz, ctr = o.frame_vis(hiz_in=hiz_in, tiles=tiles)
+    sh = o.shadow(vis)
+    sk, st = o.secondary(vis)
+    return o, vis, hiz, ctr, sh, sk, st
+
+
+def assert_same(got, want, what):
+    if not np.array_equal(got, want):
+        bad = np.flatnonzero(got != want)
+        raise AssertionError(f"{what}: {bad.size} of {got.size} differ; first at {bad[:5]}: "
+                             f"got {got[bad[:5]]}, want {want[bad[:5]]}")
+
+
+def test_engine_passes_match_the_oracle(small):
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera())
+    m.upload_view(v)
+    m.render_passes()
+    o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
+    assert_same(m.read_vis(), vis, "vis")
+    assert_same(m.read_shadow(), sh, "shadow")
+    gk, gt = m.read_secondary()
+    assert_same(gk, sk, "secondary key")
+    assert_same(gt, st, "secondary t")
+    s = m.stats()
+    assert s.device_error == 0
+    assert s.pairs_selected == ctr[4] and s.counters[3] == ctr[3]
+    assert (vis != 0).mean() > 0.3 and (sh > 0).any() and ((sk >> 63) & 1).any()
+
+
+@pytest.mark.parametrize("variant", sorted(TILE_SHAPES))
+def test_fused_kernel_matches_the_oracle(small, variant):
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera())
+    m.upload_view(v)
+    m.set_tuning(variant)
+    m.render()
+    o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
+    assert_same(m.read_vis(), vis, "vis")
+    assert_same(m.read_shadow(), sh, "shadow")
+    gk, gt = m.read_secondary()
+    assert_same(gk, sk, "secondary key")
+    assert_same(gt, st, "secondary t")
+    assert m.stats().device_error == 0
+    m.set_tuning(2)
+
+
+def test_expanded_outputs(small):
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera())
+    m.upload_view(v)
+    m.render()
+    o = Oracle(v, *pools)
+    vis, _, _ = o.frame_vis()
+    vox, face, t = m.read_expanded((0, 0, 0), (256, 128, 256))
+    ov, of, ot = o.expand(vis, (0, 0, 0), (256, 128, 256))
+    assert_same(vox, ov, "voxel index")
+    assert_same(face, of, "face")
+    hit = ov != 0xFFFFFFFF
+    assert np.all(np.abs(t[hit] - ot[hit]) <= T_RTOL * np.abs(ot[hit]))
+    # the voxel index names the block the key names
+    idx = np.flatnonzero(hit)[:: max(1, hit.sum() // 500)]
+    for i in idx:
+        x, rest = ov[i] % 256, ov[i] // 256
+        z, y = rest % 256, rest // 256
+        assert w.get_block(int(x), int(y), int(z)) != W.AIR
+
+
+def test_hiz_frames_match_the_oracle(small):
+    """Frame A, then frame B with the camera moved half a voxel, FLAG_HIZ on:
+    the engine's pass sequence keeps every counter of the oracle's."""
+    w, pools, m = small
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_HIZ
+    va = w.view(W.small_terrain_camera(flags=flags))
+    m.upload_view(va)
+    m.write_hiz(np.zeros(int(va.frame.tiles[0]) * int(va.frame.tiles[1]), np.uint32))
+    m.select(); m.march()
+    oa = Oracle(va, *pools)
+    vis_a, hiz_a, ctr_a = oa.frame_vis(hiz_in=np.zeros(oa.ntiles, np.uint32))
+    assert_same(m.read_vis(), vis_a, "vis A")
+    assert_same(m.read_hiz(), hiz_a, "hiz A")
+    cam_b = W.small_terrain_camera(flags=flags)
+    cam_b.pos = (cam_b.pos[0] + 0.5, cam_b.pos[1], cam_b.pos[2])
+    vb = w.view(cam_b)
+    m.upload_view(vb)
+    m.select(); m.march()
+    vis_b, hiz_b, ctr_b = Oracle(vb, *pools).frame_vis(hiz_in=hiz_a)
+    assert_same(m.read_vis(), vis_b, "vis B")
+    assert_same(m.read_hiz(), hiz_b, "hiz B")
+    s = m.stats()
+    assert s.pairs_deferred == ctr_b[1] > 0
+    assert s.pairs_recovered == ctr_b[5]
+    assert s.pairs_selected == ctr_b[4]
+    # and the fused kernel gives the same visibility
+    m.render()
+    assert_same(m.read_vis(), vis_b, "fused vis B")
+
+
+def test_heatmap_matches_the_oracle(small):
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera(flags=W.FLAG_HEATMAP))
+    m.upload_view(v)
+    m.select(); m.march()
+    vis, hiz, ctr, dbg = Oracle(v, *pools).frame_vis(heat=True)
+    assert_same(m.read_vis(), vis, "vis")
+    assert_same(m.read_heatmap(), dbg, "iteration heatmap")
+
+
+@pytest.mark.parametrize("res", [(1, 1), (7, 5), (333, 77), (64, 64), (129, 257)])
+def test_ragged_resolutions(small, res):
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera(width=res[0], height=res[1]))
+    m.upload_view(v)
+    o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
+    for variant in (0, 2, 3):
+        m.set_tuning(variant)
+        m.render()
+        assert_same(m.read_vis(), vis, f"fused {variant} vis")
+        assert_same(m.read_shadow(), sh, f"fused {variant} shadow")
+    m.set_tuning(2)
+    m.render_passes()
+    assert_same(m.read_vis(), vis, "passes vis")
+    assert_same(m.read_shadow(), sh, "passes shadow")
+
+
+@pytest.mark.parametrize("yaw,pitch,pos", [(0.0, -30.0, (30.0, 100.0, 130.0)), (200.0, -5.0, (200.0, 70.0, 200.0)),
+                                           (45.0, 60.0, (128.0, 66.0, 128.0)), (135.0, -89.0, (60.0, 95.0, 60.0))])
+def test_other_cameras(small, yaw, pitch, pos):
+    """Cameras looking up, down, along the axes, close to the water and inside
+    the terrain's bounding boxes (camera chunk path)."""
+    w, pools, m = small
+    v = w.view(Camera(pos=pos, yaw=math.radians(yaw), pitch=math.radians(pitch), width=320, height=200))
+    m.upload_view(v)
+    o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
+    m.render()
+    assert_same(m.read_vis(), vis, "fused vis")
+    assert_same(m.read_shadow(), sh, "fused shadow")
+    gk, gt = m.read_secondary()
+    assert_same(gk, sk, "fused secondary")
+    m.render_passes()
+    assert_same(m.read_vis(), vis, "passes vis")
+
+
+def test_underwater_camera(small):
+    w, pools, m = small
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_UNDERWATER | W.FLAG_WATER_FAR | W.FLAG_WATER_DARK
+    rec = W.recipe_small_terrain()
+    # find a column under water
+    for x in range(0, 256, 8):
+        h = W.surface_height(rec, x, 128)
+        if h < 58:
+            break
+    v = w.view(Camera(pos=(x + 0.5, 62.0, 128.5), pitch=math.radians(10.0), width=320, height=200, flags=flags))
+    assert v.frame.flags & W.FLAG_UNDERWATER
+    m.upload_view(v)
+    o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
+    m.render()
+    assert_same(m.read_vis(), vis, "fused vis")
+    m.render_passes()
+    assert_same(m.read_vis(), vis, "passes vis")
+    assert_same(m.read_shadow(), sh, "shadow")
+
+
+def test_empty_world_and_empty_view():
+    w = World()
+    d = np.zeros(64 ** 3, np.uint16)
+    w.insert_dense((0, 0, 0), d)
+    m = Marcher(64, 64)
+    m.upload_world(*w.pools())
+    v = w.view(Camera(pos=(10.0, 10.0, 10.0), width=64, height=64))
+    assert len(v.chunks) == 0
+    m.upload_view(v)
+    m.render()
+    assert not m.read_vis().any()
+    m.render_passes()
+    assert not m.read_vis().any()
+
+
+def test_large_world_reduced_resolution(large):
+    rec, w, pools, m = large
+    v = w.view(W.large_terrain_camera(rec, width=480, height=270))
+    m.upload_view(v)
+    o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
+    m.render()
+    assert_same(m.read_vis(), vis, "vis")
+    assert_same(m.read_shadow(), sh, "shadow")
+    gk, gt = m.read_secondary()
+    assert_same(gk, sk, "secondary key")
+    assert_same(gt, st, "secondary t")
+    glass = ((sk >> 63) & 1).astype(bool) & ((sk >> 61) & 1).astype(bool)
+    water = ((sk >> 63) & 1).astype(bool) & ~((sk >> 61) & 1).astype(bool)
+    assert glass.any() and water.any()
+
+
+def test_large_world_full_hd(large):
+    """1920x1080: fused kernel == engine pass sequence on the GPU over every
+    pixel, and == the oracle on a band of tiles."""
+    rec, w, pools, m = large
+    v = w.view(W.large_terrain_camera(rec))
+    m.upload_view(v)
+    m.render()
+    fv, fs = m.read_vis(), m.read_shadow()
+    fk, ft = m.read_secondary()
+    m.render_passes()
+    assert_same(m.read_vis(), fv, "vis fused vs passes")
+    assert_same(m.read_shadow(), fs, "shadow fused vs passes")
+    pk, pt = m.read_secondary()
+    assert_same(pk, fk, "secondary fused vs passes")
+    o = Oracle(v, *pools)
+    tx = int(v.frame.tiles[0])
+    rows = (60 * tx, 64 * tx)            # four tile rows across the horizon
+    vis, _, _ = o.frame_vis(tiles=rows)
+    px = (rows[0] * 64, rows[1] * 64)
+    sl = slice(60 * 8 * 1920, 64 * 8 * 1920)
+    assert_same(fv[sl], vis[sl], "vis band")
+    sh = o.shadow(np.where(np.arange(vis.size) < sl.stop, vis, 0), pix=(sl.start, sl.stop))
+    assert_same(fs[sl], sh[sl], "shadow band")
+
+
+def test_batch_matches_single_views(small):
+    w, pools, m = small
+    rng = np.random.default_rng(3)
+    views = []
+    for i in range(12):
+        res = int(rng.choice([32, 64, 128]))
+        pos = (float(rng.uniform(20, 236)), float(rng.uniform(90, 120)), float(rng.uniform(20, 236)))
+        views.append(w.view(Camera(pos=pos, yaw=float(rng.uniform(0, 6.28)), pitch=float(rng.uniform(-1.2, 0.3)),
+                                   fov_y=math.radians(90.0), width=res, height=res)))
+    views.append(w.view(W.small_terrain_camera()))
+    m.batch_set(views)
+    m.batch_run()
+    bv, bs = m.batch_read()
+    m.batch_run(per_view=True)
+    pv, ps = m.batch_read()
+    assert_same(pv, bv, "per-view vs persistent vis")
+    assert_same(ps, bs, "per-view vs persistent shadow")
+    off = 0
+    for v in views:
+        n = v.n_pixels
+        o = Oracle(v, *pools)
+        vis, _, _ = o.frame_vis()
+        sh = o.shadow(vis)
+        assert_same(bv[off:off + n], vis, "batch vis")
+        assert_same(bs[off:off + n], sh, "batch shadow")
+        off += n
+    m.batch_run()   # graph replay
+    bv2, _ = m.batch_read()
+    assert_same(bv2, bv, "graph replay")
+
+
+def test_invalid_frames_are_rejected(small):
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera())
+    m.upload_view(v)
+    f = v.frame
+    bad = type(f).from_buffer_copy(f)
+    bad.tiles[0] = 3
+    m.set_frame(bad)
+    with pytest.raises(MarchError) as e:
+        m.render()
+    assert e.value.code == 1
+    bad = type(f).from_buffer_copy(f)
+    bad.chunk_count = 100000
+    m.set_frame(bad)
+    with pytest.raises(MarchError):
+        m.select()
+    big = Marcher(8192, 4320)
+    big.upload_world(*pools)
+    vb = w.view(W.small_terrain_camera(width=8192, height=4320))
+    with pytest.raises(MarchError) as e:
+        big.upload_view(vb)
+        big.select()
+    assert e.value.code == 3, "tile index overflows the pair word"
+    big.close()
+    m.set_frame(f)

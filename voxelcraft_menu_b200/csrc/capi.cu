@@ -1,0 +1,712 @@
+// The C ABI of include/voxmarch.h: one context = one renderer's device state.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/voxmarch.h"
+#include "kernels.cuh"
+
+using vmk::FusedArgs;
+using vmk::ViewDesc;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct vm_ctx {
+  int device = 0;
+  int sms = 148;
+  cudaStream_t own = nullptr, stream = nullptr;
+  vm_caps caps{};
+  // world pools
+  DevBuf inners, leaves, bricks;
+  uint64_t n_inners = 0, n_leaves = 0, n_bricks = 0;
+  bool have_world = false;
+  // per-frame inputs
+  DevBuf chunks, grid;
+  uint32_t n_chunks = 0;
+  uint64_t grid_len = 0;
+  bool have_chunks = false;
+  vm_frame frame{};
+  bool have_frame = false;
+  // per-frame outputs and scratch
+  DevBuf vis, shadow, sec_key, sec_t, hiz, dbg, pairs, counters, err, work, dkmax, sufmax, traffic, expand;
+  // batch
+  DevBuf b_frames, b_views, b_views1, b_chunks, b_grids, b_vis, b_shadow, b_seck, b_sect, b_hiz, b_dkmax, b_sufmax;
+  std::vector<vm_frame> bh_frames;
+  std::vector<ViewDesc> bh_views;
+  std::vector<uint32_t> bh_counts;
+  std::vector<uint64_t> bh_grid_lens;
+  uint32_t b_n_views = 0, b_total_tiles = 0, b_n_chunks = 0;
+  uint64_t b_pixels = 0, b_grid_total = 0, b_hiz_total = 0;
+  bool b_underwater = false;
+  int b_layout_variant = -1;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  // tuning
+  int variant = vmk::FUSED_16x16;
+  int ctas_per_sm = 0;
+  std::string err_text;
+};
+
+namespace {
+
+int fail(vm_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err_text = buf;
+  return code;
+}
+
+int cuda_fail(vm_ctx* c, cudaError_t e, const char* what) {
+  return fail(c, VM_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                         \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+// grow a device buffer; keep_bytes of the old contents are copied over
+int ensure(vm_ctx* ctx, DevBuf& b, size_t bytes, size_t keep_bytes = 0) {
+  if (bytes <= b.bytes && b.p) return VM_OK;
+  size_t cap = std::max<size_t>(bytes, 256);
+  if (b.bytes) cap = std::max(cap, b.bytes + b.bytes / 2);
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, cap);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+  if (b.p) {
+    if (keep_bytes) {
+      e = cudaMemcpyAsync(p, b.p, std::min(keep_bytes, b.bytes), cudaMemcpyDeviceToDevice, ctx->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMemcpyAsync");
+    }
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(b.p);
+  }
+  b.p = p;
+  b.bytes = cap;
+  return VM_OK;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+void drop_graph(vm_ctx* ctx) {
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  ctx->graph_exec = nullptr;
+  ctx->graph = nullptr;
+}
+
+vmd::DevWorld dev_world(vm_ctx* ctx) {
+  vmd::DevWorld w;
+  w.chunks = (const vm_chunk*)ctx->chunks.p; w.n_chunks = ctx->n_chunks;
+  w.inners = (const uint4*)ctx->inners.p; w.n_inners = ctx->n_inners;
+  w.leaves = (const uint2*)ctx->leaves.p; w.n_leaves = ctx->n_leaves;
+  w.bricks = (const uint32_t*)ctx->bricks.p; w.n_bricks = ctx->n_bricks;
+  w.grid = (const uint32_t*)ctx->grid.p; w.n_grid = ctx->grid_len;
+  w.err = (uint32_t*)ctx->err.p;
+  return w;
+}
+
+// Checks shared by every frame entry point.
+int check_frame(vm_ctx* ctx, const vm_frame& f, uint32_t n_chunks, uint64_t grid_len) {
+  if (f.res[0] == 0 || f.res[1] == 0) return fail(ctx, VM_E_INVALID, "empty resolution");
+  if (f.tiles[0] != (f.res[0] + 7) / 8 || f.tiles[1] != (f.res[1] + 7) / 8)
+    return fail(ctx, VM_E_INVALID, "tiles (%u,%u) do not match res (%u,%u) in 8x8 tiles", f.tiles[0], f.tiles[1],
+                f.res[0], f.res[1]);
+  if ((uint64_t)f.tiles[0] * f.tiles[1] > VM_MAX_TILES)
+    return fail(ctx, VM_E_TILE_OVERFLOW, "tile index overflows the pair word: %u x %u tiles > %u", f.tiles[0],
+                f.tiles[1], VM_MAX_TILES);
+  if (f.chunk_count > n_chunks) return fail(ctx, VM_E_INVALID, "chunk_count %u > uploaded chunks %u", f.chunk_count, n_chunks);
+  if (n_chunks > VM_MAX_CHUNKS) return fail(ctx, VM_E_INVALID, "%u chunks exceed the 13-bit chunk field", n_chunks);
+  if (f.camera_chunk != VM_NO_CHUNK && f.camera_chunk >= f.chunk_count)
+    return fail(ctx, VM_E_INVALID, "camera_chunk %u outside the visible list", f.camera_chunk);
+  if ((uint64_t)f.grid_dim[0] * f.grid_dim[1] * f.grid_dim[2] > grid_len)
+    return fail(ctx, VM_E_INVALID, "grid_dim product exceeds the uploaded grid");
+  if (!(f.far_ > 0.0f)) return fail(ctx, VM_E_INVALID, "far must be positive");
+  if (f.sun_dir[0] == 0.0f || f.sun_dir[1] == 0.0f || f.sun_dir[2] == 0.0f)
+    return fail(ctx, VM_E_INVALID, "sun_dir components must be nonzero (the shadow DDA divides by them)");
+  if (f.max_pairs == 0 || f.max_pairs > 0x7FFFFFFFu) return fail(ctx, VM_E_INVALID, "max_pairs out of range");
+  return VM_OK;
+}
+
+int check_ready(vm_ctx* ctx) {
+  if (!ctx->have_world) return fail(ctx, VM_E_NOT_READY, "no world uploaded");
+  if (!ctx->have_chunks) return fail(ctx, VM_E_NOT_READY, "no chunk list uploaded");
+  if (!ctx->have_frame) return fail(ctx, VM_E_NOT_READY, "no frame set");
+  const vm_frame& f = ctx->frame;
+  if (f.res[0] > ctx->caps.max_width || f.res[1] > ctx->caps.max_height)
+    return fail(ctx, VM_E_INVALID, "frame %ux%u exceeds the context's %ux%u", f.res[0], f.res[1], ctx->caps.max_width,
+                ctx->caps.max_height);
+  return check_frame(ctx, f, ctx->n_chunks, ctx->grid_len);
+}
+
+uint32_t fused_grid(vm_ctx* ctx, int variant, bool underwater, bool count, uint32_t tiles) {
+  int per = ctx->ctas_per_sm > 0 ? ctx->ctas_per_sm : vmk::fused_max_ctas_per_sm(variant, underwater, count);
+  if (per <= 0) per = 1;
+  uint64_t g = (uint64_t)ctx->sms * (uint64_t)per;
+  return (uint32_t)std::min<uint64_t>(g, tiles);
+}
+
+FusedArgs base_args(vm_ctx* ctx) {
+  FusedArgs a;
+  memset(&a, 0, sizeof a);
+  a.inners = (const uint4*)ctx->inners.p; a.n_inners = ctx->n_inners;
+  a.leaves = (const uint2*)ctx->leaves.p; a.n_leaves = ctx->n_leaves;
+  a.bricks = (const uint32_t*)ctx->bricks.p; a.n_bricks = ctx->n_bricks;
+  a.err = (uint32_t*)ctx->err.p;
+  a.work = (uint32_t*)ctx->work.p;
+  return a;
+}
+
+// The single-view fused launch (frame and view descriptor by value).
+int enqueue_render(vm_ctx* ctx, bool count) {
+  const vm_frame& f = ctx->frame;
+  uint32_t tw, th;
+  vmk::fused_dims(ctx->variant, &tw, &th);
+  ViewDesc v;
+  memset(&v, 0, sizeof v);
+  v.n_chunks = ctx->n_chunks;
+  v.grid_len = (uint32_t)ctx->grid_len;
+  v.tiles_x = (f.res[0] + tw - 1) / tw;
+  v.tiles_y = (f.res[1] + th - 1) / th;
+  FusedArgs a = base_args(ctx);
+  a.frames = nullptr;
+  a.views = nullptr;
+  a.n_views = 1;
+  a.total_tiles = v.tiles_x * v.tiles_y;
+  a.chunks = (const vm_chunk*)ctx->chunks.p;
+  a.grids = (const uint32_t*)ctx->grid.p;
+  a.dkmax = (const uint32_t*)ctx->dkmax.p;
+  a.sufmax = (const uint32_t*)ctx->sufmax.p;
+  a.vis = (unsigned long long*)ctx->vis.p;
+  a.shadow = (float*)ctx->shadow.p;
+  a.sec_key = (unsigned long long*)ctx->sec_key.p;
+  a.sec_t = (float*)ctx->sec_t.p;
+  a.hiz = (uint32_t*)ctx->hiz.p;
+  a.traffic = (vmk::Traffic64*)ctx->traffic.p;
+  a.do_shadow = 1;
+  a.do_secondary = 1;
+  a.frame0 = f;
+  a.view0 = v;
+  CK(vmk::launch_chunk_bounds(nullptr, nullptr, 1, f, v, a.chunks, (uint32_t*)ctx->dkmax.p, (uint32_t*)ctx->sufmax.p,
+                              ctx->stream));
+  CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(uint32_t), ctx->stream));
+  const bool uw = (f.flags & VM_FLAG_UNDERWATER) != 0u;
+  CK(vmk::launch_fused(a, ctx->variant, uw, count, fused_grid(ctx, ctx->variant, uw, count, a.total_tiles), ctx->stream));
+  return VM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vm_create(int device_ordinal, const vm_caps* caps, vm_ctx** out) {
+  if (!out || !caps) return VM_E_INVALID;
+  *out = nullptr;
+  if (caps->max_width == 0 || caps->max_height == 0) return VM_E_INVALID;
+  vm_ctx* ctx = new vm_ctx();
+  ctx->device = device_ordinal;
+  ctx->caps = *caps;
+  if (ctx->caps.max_chunks == 0) ctx->caps.max_chunks = VM_MAX_CHUNKS;
+  cudaError_t e = cudaSetDevice(device_ordinal);
+  if (e != cudaSuccess) { delete ctx; return VM_E_CUDA; }
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device_ordinal);
+  e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete ctx; return VM_E_CUDA; }
+  ctx->stream = ctx->own;
+  const uint64_t npix = (uint64_t)caps->max_width * caps->max_height;
+  const uint64_t tiles = (uint64_t)((caps->max_width + 7) / 8) * ((caps->max_height + 7) / 8);
+  int rc = VM_OK;
+  rc |= ensure(ctx, ctx->vis, npix * 8);
+  rc |= ensure(ctx, ctx->shadow, npix * 4);
+  rc |= ensure(ctx, ctx->sec_key, npix * 8);
+  rc |= ensure(ctx, ctx->sec_t, npix * 4);
+  rc |= ensure(ctx, ctx->dbg, npix * 4);
+  rc |= ensure(ctx, ctx->expand, npix * 9);
+  rc |= ensure(ctx, ctx->hiz, tiles * 4);
+  rc |= ensure(ctx, ctx->counters, 64);
+  rc |= ensure(ctx, ctx->err, 64);
+  rc |= ensure(ctx, ctx->work, 64);
+  rc |= ensure(ctx, ctx->traffic, sizeof(vmk::Traffic64));
+  rc |= ensure(ctx, ctx->dkmax, (size_t)ctx->caps.max_chunks * 4);
+  rc |= ensure(ctx, ctx->sufmax, (size_t)ctx->caps.max_chunks * 4);
+  if (rc != VM_OK) { vm_destroy(ctx); return VM_E_CUDA; }
+  cudaMemsetAsync(ctx->hiz.p, 0, tiles * 4, ctx->stream);
+  cudaMemsetAsync(ctx->err.p, 0, 64, ctx->stream);
+  cudaMemsetAsync(ctx->counters.p, 0, 64, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  *out = ctx;
+  return VM_OK;
+}
+
+void vm_destroy(vm_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graph(ctx);
+  DevBuf* all[] = {&ctx->inners, &ctx->leaves, &ctx->bricks, &ctx->chunks, &ctx->grid, &ctx->vis, &ctx->shadow,
+                   &ctx->sec_key, &ctx->sec_t, &ctx->hiz, &ctx->dbg, &ctx->pairs, &ctx->counters, &ctx->err,
+                   &ctx->work, &ctx->dkmax, &ctx->sufmax, &ctx->traffic, &ctx->expand, &ctx->b_frames,
+                   &ctx->b_views, &ctx->b_views1, &ctx->b_chunks, &ctx->b_grids, &ctx->b_vis, &ctx->b_shadow,
+                   &ctx->b_seck, &ctx->b_sect, &ctx->b_hiz, &ctx->b_dkmax, &ctx->b_sufmax};
+  for (DevBuf* b : all) release(*b);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+}
+
+const char* vm_last_error(const vm_ctx* ctx) { return ctx ? ctx->err_text.c_str() : "null context"; }
+
+int vm_set_stream(vm_ctx* ctx, void* s) {
+  if (!ctx) return VM_E_INVALID;
+  ctx->stream = s ? (cudaStream_t)s : ctx->own;
+  drop_graph(ctx);
+  return VM_OK;
+}
+
+int vm_upload_world(vm_ctx* ctx, const uint32_t* inners, uint64_t n_inners, const uint32_t* leaves, uint64_t n_leaves,
+                    const uint32_t* bricks, uint64_t n_bricks) {
+  if (!ctx) return VM_E_INVALID;
+  if ((n_inners && !inners) || (n_leaves && !leaves) || (n_bricks && !bricks))
+    return fail(ctx, VM_E_INVALID, "null pool with nonzero size");
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = ensure(ctx, ctx->inners, std::max<uint64_t>(n_inners, 1) * 16))) return rc;
+  if ((rc = ensure(ctx, ctx->leaves, std::max<uint64_t>(n_leaves, 1) * 8))) return rc;
+  if ((rc = ensure(ctx, ctx->bricks, std::max<uint64_t>(n_bricks, 1) * 4))) return rc;
+  if (n_inners) CK(cudaMemcpyAsync(ctx->inners.p, inners, n_inners * 16, cudaMemcpyHostToDevice, ctx->stream));
+  if (n_leaves) CK(cudaMemcpyAsync(ctx->leaves.p, leaves, n_leaves * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if (n_bricks) CK(cudaMemcpyAsync(ctx->bricks.p, bricks, n_bricks * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->n_inners = n_inners;
+  ctx->n_leaves = n_leaves;
+  ctx->n_bricks = n_bricks;
+  ctx->have_world = true;
+  drop_graph(ctx);
+  return VM_OK;
+}
+
+int vm_update_pool(vm_ctx* ctx, int pool, uint64_t offset, const uint32_t* data, uint64_t count) {
+  if (!ctx || !data || pool < 0 || pool > 2) return VM_E_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  DevBuf* b = pool == 0 ? &ctx->inners : pool == 1 ? &ctx->leaves : &ctx->bricks;
+  uint64_t* n = pool == 0 ? &ctx->n_inners : pool == 1 ? &ctx->n_leaves : &ctx->n_bricks;
+  const size_t esz = pool == 0 ? 16 : pool == 1 ? 8 : 4;
+  const uint64_t end = offset + count;
+  int rc;
+  if ((rc = ensure(ctx, *b, end * esz, *n * esz))) return rc;
+  CK(cudaMemcpyAsync((char*)b->p + offset * esz, data, count * esz, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *n = std::max(*n, end);
+  ctx->have_world = true;
+  drop_graph(ctx);
+  return VM_OK;
+}
+
+int vm_upload_chunks(vm_ctx* ctx, const vm_chunk* chunks, uint32_t n_chunks, const uint32_t* grid, uint64_t grid_len) {
+  if (!ctx || (n_chunks && !chunks) || !grid || grid_len == 0) return VM_E_INVALID;
+  if (n_chunks > ctx->caps.max_chunks || n_chunks > VM_MAX_CHUNKS)
+    return fail(ctx, VM_E_INVALID, "%u chunks exceed the context capacity %u", n_chunks, ctx->caps.max_chunks);
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = ensure(ctx, ctx->chunks, std::max<uint32_t>(n_chunks, 1) * sizeof(vm_chunk)))) return rc;
+  if ((rc = ensure(ctx, ctx->grid, grid_len * 4))) return rc;
+  if (n_chunks) CK(cudaMemcpyAsync(ctx->chunks.p, chunks, (size_t)n_chunks * sizeof(vm_chunk), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->grid.p, grid, grid_len * 4, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->n_chunks = n_chunks;
+  ctx->grid_len = grid_len;
+  ctx->have_chunks = true;
+  return VM_OK;
+}
+
+int vm_set_frame(vm_ctx* ctx, const vm_frame* frame) {
+  if (!ctx || !frame) return VM_E_INVALID;
+  ctx->frame = *frame;
+  ctx->have_frame = true;
+  return VM_OK;
+}
+
+int vm_set_tuning(vm_ctx* ctx, int tile_variant, int ctas_per_sm) {
+  if (!ctx || tile_variant < 0 || tile_variant >= vmk::FUSED_VARIANTS || ctas_per_sm < 0) return VM_E_INVALID;
+  if (tile_variant != ctx->variant || ctas_per_sm != ctx->ctas_per_sm) drop_graph(ctx);
+  ctx->variant = tile_variant;
+  ctx->ctas_per_sm = ctas_per_sm;
+  return VM_OK;
+}
+
+int vm_select(vm_ctx* ctx) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  const vm_frame& f = ctx->frame;
+  const uint64_t npix = (uint64_t)f.res[0] * f.res[1];
+  const uint64_t tiles = (uint64_t)f.tiles[0] * f.tiles[1];
+  if ((rc = ensure(ctx, ctx->pairs, (size_t)f.max_pairs * 2 * 4))) return rc;
+  CK(cudaMemsetAsync(ctx->vis.p, 0, npix * 8, ctx->stream));
+  CK(cudaMemsetAsync(ctx->counters.p, 0, 32, ctx->stream));
+  if (f.flags & VM_FLAG_HEATMAP) CK(cudaMemsetAsync(ctx->dbg.p, 0, npix * 4, ctx->stream));
+  if (!(f.flags & VM_FLAG_HIZ)) CK(cudaMemsetAsync(ctx->hiz.p, 0, tiles * 4, ctx->stream));
+  const vmd::DevWorld w = dev_world(ctx);
+  CK(vmk::launch_tile_select(f, w, (const uint32_t*)ctx->hiz.p, (uint32_t*)ctx->pairs.p, (uint32_t*)ctx->counters.p,
+                             ctx->stream));
+  CK(vmk::launch_finalize(f, (uint32_t*)ctx->counters.p, false, ctx->stream));
+  return VM_OK;
+}
+
+int vm_march(vm_ctx* ctx) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->pairs.p) return fail(ctx, VM_E_NOT_READY, "vm_march before vm_select");
+  CK(cudaSetDevice(ctx->device));
+  const vm_frame& f = ctx->frame;
+  const vmd::DevWorld w = dev_world(ctx);
+  uint32_t* pairs = (uint32_t*)ctx->pairs.p;
+  uint32_t* ctr = (uint32_t*)ctx->counters.p;
+  unsigned long long* vis = (unsigned long long*)ctx->vis.p;
+  uint32_t* dbg = (f.flags & VM_FLAG_HEATMAP) ? (uint32_t*)ctx->dbg.p : nullptr;
+  CK(vmk::launch_march_pairs(f, w, pairs, ctr, vis, dbg, ctx->sms, ctx->stream));
+  if (f.flags & VM_FLAG_HIZ) {
+    CK(vmk::launch_build_hiz(f, vis, (uint32_t*)ctx->hiz.p, ctx->stream));
+    CK(vmk::launch_recover(f, w, pairs, ctr, (const uint32_t*)ctx->hiz.p, ctx->sms, ctx->stream));
+    CK(vmk::launch_finalize(f, ctr, true, ctx->stream));
+    CK(vmk::launch_march_pairs(f, w, pairs, ctr, vis, dbg, ctx->sms, ctx->stream));
+  }
+  return VM_OK;
+}
+
+int vm_primary_shadow(vm_ctx* ctx) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(vmk::launch_primary_shadow(ctx->frame, dev_world(ctx), (const unsigned long long*)ctx->vis.p, (float*)ctx->shadow.p,
+                                ctx->stream));
+  return VM_OK;
+}
+
+int vm_secondary(vm_ctx* ctx) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(vmk::launch_secondary(ctx->frame, dev_world(ctx), (const unsigned long long*)ctx->vis.p,
+                           (unsigned long long*)ctx->sec_key.p, (float*)ctx->sec_t.p, ctx->stream));
+  return VM_OK;
+}
+
+int vm_render(vm_ctx* ctx) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  return enqueue_render(ctx, false);
+}
+
+int vm_render_counted(vm_ctx* ctx, vm_traffic* out) {
+  if (!ctx || !out) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemsetAsync(ctx->traffic.p, 0, sizeof(vmk::Traffic64), ctx->stream));
+  if ((rc = enqueue_render(ctx, true))) return rc;
+  vmk::Traffic64 t;
+  CK(cudaMemcpyAsync(&t, ctx->traffic.p, sizeof t, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  out->chunk_records = t.chunk; out->l1_fetches = t.l1; out->leaf_fetches = t.leaf; out->attr_fetches = t.attr;
+  out->palette_decodes = t.pal; out->grid_lookups = t.grid; out->iters = t.iters;
+  out->rays_primary = t.rays_primary; out->rays_shadow = t.rays_shadow; out->rays_secondary = t.rays_secondary;
+  return VM_OK;
+}
+
+static int read_dev(vm_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (!dst) return fail(ctx, VM_E_INVALID, "null output");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return VM_OK;
+}
+
+int vm_read_vis(vm_ctx* ctx, uint64_t* out) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  return read_dev(ctx, out, ctx->vis.p, (size_t)ctx->frame.res[0] * ctx->frame.res[1] * 8);
+}
+int vm_read_hiz(vm_ctx* ctx, uint32_t* out) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  return read_dev(ctx, out, ctx->hiz.p, (size_t)ctx->frame.tiles[0] * ctx->frame.tiles[1] * 4);
+}
+int vm_write_hiz(vm_ctx* ctx, const uint32_t* hiz) {
+  if (!ctx || !ctx->have_frame || !hiz) return VM_E_NOT_READY;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(ctx->hiz.p, hiz, (size_t)ctx->frame.tiles[0] * ctx->frame.tiles[1] * 4, cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return VM_OK;
+}
+int vm_read_shadow(vm_ctx* ctx, float* out) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  return read_dev(ctx, out, ctx->shadow.p, (size_t)ctx->frame.res[0] * ctx->frame.res[1] * 4);
+}
+int vm_read_secondary(vm_ctx* ctx, uint64_t* key, float* t) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  const size_t n = (size_t)ctx->frame.res[0] * ctx->frame.res[1];
+  int rc = read_dev(ctx, key, ctx->sec_key.p, n * 8);
+  if (rc) return rc;
+  return read_dev(ctx, t, ctx->sec_t.p, n * 4);
+}
+int vm_read_heatmap(vm_ctx* ctx, uint32_t* out) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  return read_dev(ctx, out, ctx->dbg.p, (size_t)ctx->frame.res[0] * ctx->frame.res[1] * 4);
+}
+
+int vm_read_expanded(vm_ctx* ctx, const int32_t origin[3], const uint32_t dims[3], uint32_t* voxel, uint8_t* face,
+                     float* t) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (!origin || !dims || !voxel || !face || !t) return fail(ctx, VM_E_INVALID, "null argument");
+  CK(cudaSetDevice(ctx->device));
+  const vm_frame& f = ctx->frame;
+  const size_t n = (size_t)f.res[0] * f.res[1];
+  uint32_t* dv = (uint32_t*)ctx->expand.p;
+  float* dt = (float*)((char*)ctx->expand.p + n * 4);
+  uint8_t* df = (uint8_t*)((char*)ctx->expand.p + n * 8);
+  CK(vmk::launch_expand(f, dev_world(ctx), (const unsigned long long*)ctx->vis.p, origin[0], origin[1], origin[2], dims[0],
+                        dims[1], dims[2], dv, df, dt, ctx->stream));
+  CK(cudaMemcpyAsync(voxel, dv, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(t, dt, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(face, df, n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return VM_OK;
+}
+
+int vm_stats_read(vm_ctx* ctx, vm_stats* out) {
+  if (!ctx || !out) return VM_E_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  memset(out, 0, sizeof *out);
+  uint32_t c[8] = {0}, e = 0;
+  CK(cudaMemcpyAsync(c, ctx->counters.p, 32, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(&e, ctx->err.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  memcpy(out->counters, c, sizeof c);
+  out->pairs_selected = c[4];
+  out->pairs_deferred = c[1];
+  out->pairs_recovered = c[5];
+  out->max_pairs = ctx->frame.max_pairs;
+  out->truncated = (c[4] > out->max_pairs || c[1] > out->max_pairs || c[5] > out->max_pairs) ? 1u : 0u;
+  out->device_error = e;
+  return VM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batches
+// ---------------------------------------------------------------------------
+static int batch_layout(vm_ctx* ctx) {
+  // work items depend on the tile variant: rebuild descriptors when it changes
+  if (ctx->b_layout_variant == ctx->variant) return VM_OK;
+  uint32_t tw, th;
+  vmk::fused_dims(ctx->variant, &tw, &th);
+  std::vector<ViewDesc> single(ctx->b_n_views);
+  uint32_t tile = 0;
+  for (uint32_t v = 0; v < ctx->b_n_views; ++v) {
+    ViewDesc& d = ctx->bh_views[v];
+    const vm_frame& f = ctx->bh_frames[v];
+    d.tile_begin = tile;
+    d.tiles_x = (f.res[0] + tw - 1) / tw;
+    d.tiles_y = (f.res[1] + th - 1) / th;
+    tile += d.tiles_x * d.tiles_y;
+    single[v] = d;
+    single[v].tile_begin = 0;
+  }
+  ctx->b_total_tiles = tile;
+  CK(cudaMemcpyAsync(ctx->b_views.p, ctx->bh_views.data(), ctx->b_n_views * sizeof(ViewDesc), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(ctx->b_views1.p, single.data(), ctx->b_n_views * sizeof(ViewDesc), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->b_layout_variant = ctx->variant;
+  drop_graph(ctx);
+  return VM_OK;
+}
+
+int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm_chunk* chunks,
+                 const uint32_t* chunk_counts, const uint32_t* grids, const uint32_t* grid_lens) {
+  if (!ctx || n_views == 0 || !frames || !chunks || !chunk_counts || !grids || !grid_lens) return VM_E_INVALID;
+  if (!ctx->have_world) return fail(ctx, VM_E_NOT_READY, "no world uploaded");
+  if (ctx->caps.max_views && n_views > ctx->caps.max_views)
+    return fail(ctx, VM_E_INVALID, "%u views exceed the context capacity %u", n_views, ctx->caps.max_views);
+  CK(cudaSetDevice(ctx->device));
+  ctx->bh_frames.assign(frames, frames + n_views);
+  ctx->bh_views.assign(n_views, ViewDesc{});
+  uint64_t chunk_total = 0, grid_total = 0, pix = 0, hiz_total = 0;
+  const bool uw = (frames[0].flags & VM_FLAG_UNDERWATER) != 0u;
+  for (uint32_t v = 0; v < n_views; ++v) {
+    const vm_frame& f = frames[v];
+    int rc = check_frame(ctx, f, chunk_counts[v], grid_lens[v]);
+    if (rc) return fail(ctx, rc, "view %u: %s", v, ctx->err_text.c_str());
+    if (((f.flags & VM_FLAG_UNDERWATER) != 0u) != uw)
+      return fail(ctx, VM_E_INVALID, "views of one batch must agree on FLAG_UNDERWATER");
+    ViewDesc& d = ctx->bh_views[v];
+    d.chunk_off = (uint32_t)chunk_total;
+    d.n_chunks = chunk_counts[v];
+    d.grid_off = grid_total;
+    d.grid_len = grid_lens[v];
+    d.pix_off = pix;
+    d.hiz_off = (uint32_t)hiz_total;
+    chunk_total += chunk_counts[v];
+    grid_total += grid_lens[v];
+    pix += (uint64_t)f.res[0] * f.res[1];
+    hiz_total += (uint64_t)f.tiles[0] * f.tiles[1];
+  }
+  if (ctx->caps.max_batch_pixels && pix > ctx->caps.max_batch_pixels)
+    return fail(ctx, VM_E_INVALID, "batch of %llu pixels exceeds the context capacity", (unsigned long long)pix);
+  int rc = 0;
+  rc |= ensure(ctx, ctx->b_frames, n_views * sizeof(vm_frame));
+  rc |= ensure(ctx, ctx->b_views, n_views * sizeof(ViewDesc));
+  rc |= ensure(ctx, ctx->b_views1, n_views * sizeof(ViewDesc));
+  rc |= ensure(ctx, ctx->b_chunks, std::max<uint64_t>(chunk_total, 1) * sizeof(vm_chunk));
+  rc |= ensure(ctx, ctx->b_grids, grid_total * 4);
+  rc |= ensure(ctx, ctx->b_vis, pix * 8);
+  rc |= ensure(ctx, ctx->b_shadow, pix * 4);
+  rc |= ensure(ctx, ctx->b_seck, pix * 8);
+  rc |= ensure(ctx, ctx->b_sect, pix * 4);
+  rc |= ensure(ctx, ctx->b_hiz, hiz_total * 4);
+  rc |= ensure(ctx, ctx->b_dkmax, std::max<uint64_t>(chunk_total, 1) * 4);
+  rc |= ensure(ctx, ctx->b_sufmax, std::max<uint64_t>(chunk_total, 1) * 4);
+  if (rc) return VM_E_CUDA;
+  CK(cudaMemcpyAsync(ctx->b_frames.p, frames, n_views * sizeof(vm_frame), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->b_chunks.p, chunks, chunk_total * sizeof(vm_chunk), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->b_grids.p, grids, grid_total * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->b_n_views = n_views;
+  ctx->b_pixels = pix;
+  ctx->b_n_chunks = (uint32_t)chunk_total;
+  ctx->b_grid_total = grid_total;
+  ctx->b_hiz_total = hiz_total;
+  ctx->b_underwater = uw;
+  ctx->b_layout_variant = -1;
+  drop_graph(ctx);
+  return batch_layout(ctx);
+}
+
+static FusedArgs batch_args(vm_ctx* ctx) {
+  FusedArgs a = base_args(ctx);
+  a.frames = (const vm_frame*)ctx->b_frames.p;
+  a.views = (const ViewDesc*)ctx->b_views.p;
+  a.n_views = ctx->b_n_views;
+  a.total_tiles = ctx->b_total_tiles;
+  a.chunks = (const vm_chunk*)ctx->b_chunks.p;
+  a.grids = (const uint32_t*)ctx->b_grids.p;
+  a.dkmax = (const uint32_t*)ctx->b_dkmax.p;
+  a.sufmax = (const uint32_t*)ctx->b_sufmax.p;
+  a.vis = (unsigned long long*)ctx->b_vis.p;
+  a.shadow = (float*)ctx->b_shadow.p;
+  a.sec_key = (unsigned long long*)ctx->b_seck.p;
+  a.sec_t = (float*)ctx->b_sect.p;
+  a.hiz = (uint32_t*)ctx->b_hiz.p;
+  a.traffic = (vmk::Traffic64*)ctx->traffic.p;
+  a.do_shadow = 1;
+  a.do_secondary = 0;
+  return a;
+}
+
+static int enqueue_batch_persistent(vm_ctx* ctx) {
+  FusedArgs a = batch_args(ctx);
+  vm_frame dummy_f{};
+  ViewDesc dummy_v{};
+  CK(vmk::launch_chunk_bounds(a.frames, a.views, a.n_views, dummy_f, dummy_v, a.chunks, (uint32_t*)a.dkmax,
+                              (uint32_t*)a.sufmax, ctx->stream));
+  CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(uint32_t), ctx->stream));
+  CK(vmk::launch_fused(a, ctx->variant, ctx->b_underwater, false,
+                       fused_grid(ctx, ctx->variant, ctx->b_underwater, false, a.total_tiles), ctx->stream));
+  return VM_OK;
+}
+
+int vm_batch_run(vm_ctx* ctx, int mode) {
+  if (!ctx) return VM_E_INVALID;
+  if (ctx->b_n_views == 0) return fail(ctx, VM_E_NOT_READY, "no batch set");
+  CK(cudaSetDevice(ctx->device));
+  int rc = batch_layout(ctx);
+  if (rc) return rc;
+  if (mode == 0) {
+    if (!ctx->graph_exec) {
+      CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      rc = enqueue_batch_persistent(ctx);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+      ctx->graph = g;
+      CK(cudaGraphInstantiate(&ctx->graph_exec, g, 0));
+    }
+    CK(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+    return VM_OK;
+  }
+  if (mode == 1) {
+    // one launch sequence per view: bounds + counter reset + fused kernel
+    FusedArgs base = batch_args(ctx);
+    for (uint32_t v = 0; v < ctx->b_n_views; ++v) {
+      FusedArgs a = base;
+      const ViewDesc& d = ctx->bh_views[v];
+      a.frames = (const vm_frame*)ctx->b_frames.p + v;
+      a.views = (const ViewDesc*)ctx->b_views1.p + v;
+      a.n_views = 1;
+      a.total_tiles = d.tiles_x * d.tiles_y;
+      vm_frame dummy_f{};
+      ViewDesc dummy_v{};
+      CK(vmk::launch_chunk_bounds(a.frames, a.views, 1, dummy_f, dummy_v, a.chunks, (uint32_t*)a.dkmax,
+                                  (uint32_t*)a.sufmax, ctx->stream));
+      CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(uint32_t), ctx->stream));
+      CK(vmk::launch_fused(a, ctx->variant, ctx->b_underwater, false,
+                           fused_grid(ctx, ctx->variant, ctx->b_underwater, false, a.total_tiles), ctx->stream));
+    }
+    return VM_OK;
+  }
+  return fail(ctx, VM_E_INVALID, "unknown batch mode %d", mode);
+}
+
+int vm_batch_read(vm_ctx* ctx, uint64_t* vis, float* shadow) {
+  if (!ctx || ctx->b_n_views == 0) return VM_E_NOT_READY;
+  int rc = VM_OK;
+  if (vis) rc = read_dev(ctx, vis, ctx->b_vis.p, ctx->b_pixels * 8);
+  if (rc) return rc;
+  if (shadow) rc = read_dev(ctx, shadow, ctx->b_shadow.p, ctx->b_pixels * 4);
+  return rc;
+}
+
+uint64_t vm_batch_pixels(const vm_ctx* ctx) { return ctx ? ctx->b_pixels : 0; }
+
+int vm_device_buffers(vm_ctx* ctx, vm_device_ptrs* out) {
+  if (!ctx || !out) return VM_E_INVALID;
+  out->vis = ctx->vis.p; out->shadow = ctx->shadow.p; out->sec_key = ctx->sec_key.p; out->sec_t = ctx->sec_t.p;
+  out->hiz = ctx->hiz.p; out->batch_vis = ctx->b_vis.p; out->batch_shadow = ctx->b_shadow.p;
+  out->stream = (void*)ctx->stream;
+  return VM_OK;
+}
+
+int vm_sync(vm_ctx* ctx) {
+  if (!ctx) return VM_E_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return VM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,651 @@
+// Device-side traversal of the engine's 64-tree chunks, sm_100a.
+//
+// Numerical contract (shared with the CPU oracle so that results are
+// bit-identical): this translation unit is compiled with --fmad=false and IEEE
+// division / sqrt, floor/ceil are exact, float->int conversions saturate
+// (cvt.rzi), and min/max are IEEE minNum/maxNum.  Every function cites the
+// WGSL it re-implements (src/render/shaders/*.wgsl in the reference).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "vm_types.h"
+
+namespace vmd {
+
+// Device view of the world pools.  Every index computed from the data is
+// checked against the pool size; a bad index records an error code in *err
+// and reads element 0 instead, so malformed pools never fault.
+struct DevWorld {
+  const vm_chunk* chunks; uint32_t n_chunks;
+  const uint4* inners; uint64_t n_inners;
+  const uint2* leaves; uint64_t n_leaves;
+  const uint32_t* bricks; uint64_t n_bricks;
+  const uint32_t* grid; uint64_t n_grid;
+  uint32_t* err;
+};
+
+enum : uint32_t { ERR_CHUNK = 1u, ERR_INNER = 2u, ERR_LEAF = 4u, ERR_BRICK = 8u, ERR_GRID = 16u, ERR_LIST = 32u };
+
+__device__ __forceinline__ void flag(const DevWorld& w, uint32_t e) { atomicOr(w.err, e); }
+
+__device__ __forceinline__ uint4 ld_inner(const DevWorld& w, uint64_t i) {
+  if (i >= w.n_inners) { flag(w, ERR_INNER); i = 0; }
+  return __ldg(w.inners + i);
+}
+__device__ __forceinline__ uint2 ld_leaf(const DevWorld& w, uint64_t i) {
+  if (i >= w.n_leaves) { flag(w, ERR_LEAF); i = 0; }
+  return __ldg(w.leaves + i);
+}
+__device__ __forceinline__ uint32_t ld_brick(const DevWorld& w, uint64_t i) {
+  if (i >= w.n_bricks) { flag(w, ERR_BRICK); i = 0; }
+  return __ldg(w.bricks + i);
+}
+__device__ __forceinline__ uint32_t ld_grid(const DevWorld& w, uint64_t i) {
+  if (i >= w.n_grid) { flag(w, ERR_GRID); return VM_NO_CHUNK; }
+  return __ldg(w.grid + i);
+}
+
+// The march-relevant part of a GpuChunk, loaded with six 128-bit loads.
+struct Chunk {
+  float aabb_min[3]; float vs;
+  float aabb_max[3]; uint32_t lod;
+  float origin[3]; float fade;
+  uint32_t root[4];
+  uint32_t attr_base, attr_flags, light_base, light_flags;
+  uint32_t dry[2], res[2];
+};
+static_assert(sizeof(Chunk) == 96, "Chunk mirrors vm_chunk");
+
+__device__ __forceinline__ Chunk ld_chunk(const DevWorld& w, uint32_t ci) {
+  if (ci >= w.n_chunks) { flag(w, ERR_CHUNK); ci = 0; }
+  const uint4* p = reinterpret_cast<const uint4*>(w.chunks + ci);
+  Chunk c;
+  uint4* d = reinterpret_cast<uint4*>(&c);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) d[i] = __ldg(p + i);
+  return c;
+}
+
+struct F3 { float x, y, z; };
+__device__ __forceinline__ F3 f3(float x, float y, float z) { return {x, y, z}; }
+__device__ __forceinline__ F3 operator+(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ F3 operator-(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ F3 operator*(F3 a, F3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+__device__ __forceinline__ F3 operator*(F3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ F3 operator/(F3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ F3 neg(F3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ float dot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ F3 cross(F3 a, F3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ F3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
+__device__ __forceinline__ float comp(F3 a, uint32_t i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+__device__ __forceinline__ float signf(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+__device__ __forceinline__ float tiny_fix(float d) { return fabsf(d) < 1e-6f ? 1e-6f * signf(d + 1e-9f) : d; }
+__device__ __forceinline__ int32_t ffloor_i(float x) { return __float2int_rd(x); }
+__device__ __forceinline__ int32_t fceil_i(float x) { return __float2int_ru(x); }
+__device__ __forceinline__ uint32_t popc(uint32_t x) { return __popc(x); }
+
+__device__ __forceinline__ uint32_t cell_bit(uint32_t x, uint32_t y, uint32_t z) { return x | (y << 2) | (z << 4); }
+__device__ __forceinline__ bool mask_has(uint32_t lo, uint32_t hi, uint32_t bit) {
+  return bit < 32u ? ((lo >> bit) & 1u) != 0u : ((hi >> (bit - 32u)) & 1u) != 0u;
+}
+__device__ __forceinline__ uint32_t mask_below(uint32_t lo, uint32_t hi, uint32_t bit) {
+  // popcount of the mask bits strictly below `bit` (common.wgsl:306-314)
+  uint64_t m = ((uint64_t)hi << 32) | lo;
+  return (uint32_t)__popcll(m & ((1ull << bit) - 1ull));
+}
+// 2x2x2 sub-block occupancy test below base bit `sh` (common.wgsl:764-773,781-790)
+__device__ __forceinline__ bool block2_empty(uint32_t lo, uint32_t hi, uint32_t sh) {
+  uint64_t m = ((uint64_t)hi << 32) | lo;
+  return ((uint32_t)(m >> sh) & 0x00330033u) == 0u;
+}
+
+// ray_dir: common.wgsl:358-368
+__device__ __forceinline__ F3 ray_dir(const vm_frame& f, float px, float py) {
+  float ndc_x = ((px + f.jitter[0]) / (float)f.res[0]) * 2.0f - 1.0f;
+  float ndc_y = 1.0f - ((py + f.jitter[1]) / (float)f.res[1]) * 2.0f;
+  F3 v = (ld3(f.cam_fwd) + ld3(f.cam_right) * (ndc_x * f.tan_half_fov * f.aspect)) +
+         ld3(f.cam_up) * (ndc_y * f.tan_half_fov);
+  float l = sqrtf(dot(v, v));
+  F3 d = {v.x / l, v.y / l, v.z / l};
+  return {tiny_fix(d.x), tiny_fix(d.y), tiny_fix(d.z)};
+}
+
+// dither / ray_skips: common.wgsl:370-385
+__device__ __forceinline__ bool ray_skips(const vm_frame& f, float fade, uint32_t px, uint32_t py) {
+  if (fade >= 1.0f) return false;
+  float p0 = (float)px + 5.588238f * (float)f.frame_index;
+  float p1 = (float)py;
+  float x = p0 * 0.06711056f + p1 * 0.00583715f;
+  x = x - floorf(x);
+  float d = 52.9829189f * x;
+  d = d - floorf(d);
+  if (fade >= 0.0f) return d >= fade;
+  return d < -fade;
+}
+
+// normal_of: common.wgsl:387-398
+__device__ __forceinline__ F3 normal_of(uint32_t id) {
+  if (id >= VM_NORMAL_CROSS_A) {
+    float s = id == VM_NORMAL_CROSS_B ? 1.0f : -1.0f;
+    return {0.70710678f, 0.0f, s * 0.70710678f};
+  }
+  uint32_t axis = id >> 1u;
+  float s = (id & 1u) == 1u ? 1.0f : -1.0f;
+  if (axis == 0u) return {s, 0.0f, 0.0f};
+  if (axis == 1u) return {0.0f, s, 0.0f};
+  return {0.0f, 0.0f, s};
+}
+
+// hash_u32 / leaf_solid: common.wgsl:1422-1430, 514-518
+__device__ __forceinline__ uint32_t hash_u32(uint32_t h) {
+  h ^= h >> 16u; h *= 0x7feb352du; h ^= h >> 15u; h *= 0x846ca68bu; h ^= h >> 16u;
+  return h;
+}
+__device__ __forceinline__ bool leaf_solid(int32_t wx, int32_t wy, int32_t wz, uint32_t mx, uint32_t my, uint32_t mz) {
+  uint32_t qx = (uint32_t)wx * 4u + mx, qy = (uint32_t)wy * 4u + my, qz = (uint32_t)wz * 4u + mz;
+  uint32_t h = hash_u32((qx * 73856093u) ^ (qy * 19349663u) ^ (qz * 83492791u));
+  return (float)(h >> 8u) * (1.0f / 16777216.0f) < VM_LEAF_FILL;
+}
+
+// leaf_block: common.wgsl:320-334
+__device__ __forceinline__ uint32_t leaf_block(const DevWorld& w, uint32_t entry, uint32_t vx, uint32_t vy, uint32_t vz) {
+  if ((entry & VM_UNIFORM_BIT) != 0u) return entry & 0xFFFFu;
+  uint32_t hdr = ld_brick(w, entry);
+  uint32_t n = hdr & 0xFFu;
+  uint32_t bits = (hdr >> 8u) & 0xFFu;
+  uint32_t pal_words = (n + 1u) / 2u;
+  uint32_t vb = cell_bit(vx & 3u, vy & 3u, vz & 3u);
+  uint32_t bitpos = vb * bits;
+  uint32_t wd = ld_brick(w, (uint64_t)entry + 1u + pal_words + (bitpos >> 5u));
+  uint32_t idx = (wd >> (bitpos & 31u)) & ((bits >= 32u ? 0u : (1u << bits)) - 1u);
+  uint32_t pw = ld_brick(w, (uint64_t)entry + 1u + idx / 2u);
+  return (pw >> ((idx & 1u) * 16u)) & 0xFFFFu;
+}
+
+// leaf_attr + block_at: common.wgsl:336-356
+__device__ __forceinline__ uint32_t block_at(const DevWorld& w, const Chunk& c, uint32_t vx, uint32_t vy, uint32_t vz) {
+  if ((c.attr_flags & VM_ATTR_UNIFORM) != 0u) return c.attr_base;
+  uint32_t l1b = cell_bit(vx >> 4, vy >> 4, vz >> 4);
+  uint4 l1;
+  if ((c.root[2] & VM_FULL_BIT) != 0u) {
+    l1 = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, VM_FULL_BIT, l1b * 64u);
+  } else {
+    l1 = ld_inner(w, (uint64_t)(c.root[2] & VM_PTR_MASK) + mask_below(c.root[0], c.root[1], l1b));
+  }
+  uint32_t lfb = cell_bit((vx >> 2) & 3u, (vy >> 2) & 3u, (vz >> 2) & 3u);
+  uint32_t entry = ld_brick(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + mask_below(l1.x, l1.y, lfb));
+  return leaf_block(w, entry, vx, vy, vz);
+}
+
+// voxel_occupied: common.wgsl:912-940
+__device__ __forceinline__ bool voxel_occupied(const DevWorld& w, const Chunk& c, int32_t x, int32_t y, int32_t z) {
+  if (x < 0 || y < 0 || z < 0 || x > 63 || y > 63 || z > 63) return false;
+  uint32_t ux = x, uy = y, uz = z;
+  uint32_t l1b = cell_bit(ux >> 4, uy >> 4, uz >> 4);
+  if (!mask_has(c.root[0], c.root[1], l1b)) return false;
+  if ((c.root[2] & VM_FULL_BIT) != 0u) return true;
+  uint4 l1 = ld_inner(w, (uint64_t)(c.root[2] & VM_PTR_MASK) + mask_below(c.root[0], c.root[1], l1b));
+  if ((l1.z & VM_FULL_BIT) != 0u) return true;
+  uint32_t lfb = cell_bit((ux >> 2) & 3u, (uy >> 2) & 3u, (uz >> 2) & 3u);
+  if (!mask_has(l1.x, l1.y, lfb)) return false;
+  uint2 leaf = ld_leaf(w, (uint64_t)(l1.z & VM_PTR_MASK) + mask_below(l1.x, l1.y, lfb));
+  return mask_has(leaf.x, leaf.y, cell_bit(ux & 3u, uy & 3u, uz & 3u));
+}
+
+__device__ __forceinline__ bool grid_rel(const vm_frame& f, int32_t cx, int32_t cy, int32_t cz, uint64_t* idx) {
+  int32_t rx = cx - f.grid_min[0], ry = cy - f.grid_min[1], rz = cz - f.grid_min[2];
+  if (rx < 0 || ry < 0 || rz < 0 || rx >= (int32_t)f.grid_dim[0] || ry >= (int32_t)f.grid_dim[1] ||
+      rz >= (int32_t)f.grid_dim[2])
+    return false;
+  *idx = (uint64_t)(uint32_t)rx + (uint64_t)(uint32_t)ry * f.grid_dim[0] +
+         (uint64_t)(uint32_t)rz * f.grid_dim[0] * f.grid_dim[1];
+  return true;
+}
+
+// world_block_at: common.wgsl:266-277
+static __device__ __noinline__ uint32_t world_block_at(const DevWorld& w, const vm_frame& f, F3 p) {
+  uint64_t gi;
+  if (!grid_rel(f, ffloor_i(p.x / 64.0f), ffloor_i(p.y / 64.0f), ffloor_i(p.z / 64.0f), &gi)) return 0u;
+  uint32_t ci = ld_grid(w, gi);
+  if (ci == VM_NO_CHUNK) return 0u;
+  Chunk c = ld_chunk(w, ci);
+  int32_t vx = ffloor_i((p.x - c.origin[0]) / c.vs);
+  int32_t vy = ffloor_i((p.y - c.origin[1]) / c.vs);
+  int32_t vz = ffloor_i((p.z - c.origin[2]) / c.vs);
+  if (vx < 0 || vy < 0 || vz < 0 || vx >= 64 || vy >= 64 || vz >= 64) return 0u;
+  if (!voxel_occupied(w, c, vx, vy, vz)) return 0u;
+  return block_at(w, c, vx, vy, vz);
+}
+
+struct Hit {
+  bool hit; float t; uint32_t normal;
+  uint32_t vx, vy, vz;
+  uint32_t mx, my, mz;
+  uint32_t iters;
+};
+
+__device__ __forceinline__ bool is_tuft(uint32_t b) { return b == VM_TALL_GRASS || b == VM_GRASS_TALL || b == VM_REEDS; }
+__device__ __forceinline__ bool is_cutout_id(uint32_t b) { return b == VM_LEAVES || b == VM_PINE_LEAVES; }
+
+// micro_entry: common.wgsl:520-528
+__device__ __forceinline__ void micro_entry(uint32_t ux, uint32_t uy, uint32_t uz, F3 ro, F3 rd, float t, uint32_t axis,
+                                            bool px_, bool py_, bool pz_, bool snap, uint32_t* m) {
+  F3 p = ((ro + rd * t) - f3((float)ux, (float)uy, (float)uz)) * 4.0f;
+  int32_t a = min(max(ffloor_i(p.x), 0), 3), b = min(max(ffloor_i(p.y), 0), 3), c = min(max(ffloor_i(p.z), 0), 3);
+  if (snap) {
+    if (axis == 0) a = px_ ? 0 : 3;
+    else if (axis == 1) b = py_ ? 0 : 3;
+    else c = pz_ ? 0 : 3;
+  }
+  m[0] = a; m[1] = b; m[2] = c;
+}
+
+// cutout_march: common.wgsl:537-577
+static __device__ __noinline__ bool cutout_march(int32_t wx, int32_t wy, int32_t wz, uint32_t ux, uint32_t uy, uint32_t uz,
+                                          F3 ro, F3 rd, float t_in, uint32_t axis_in, bool pdx, bool pdy, bool pdz,
+                                          bool snap, float* t_out, uint32_t* n_out, uint32_t* m_out) {
+  F3 inv = {1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
+  const float ms = 1.0f / 4.0f;
+  uint32_t me[3];
+  micro_entry(ux, uy, uz, ro, rd, t_in, axis_in, pdx, pdy, pdz, snap, me);
+  int32_t m0 = me[0], m1 = me[1], m2 = me[2];
+  float t = t_in;
+  uint32_t axis = axis_in;
+  for (uint32_t i = 0; i < 12u; ++i) {
+    if (m0 < 0 || m1 < 0 || m2 < 0 || m0 >= 4 || m1 >= 4 || m2 >= 4) return false;
+    if (leaf_solid(wx, wy, wz, m0, m1, m2)) {
+      *t_out = t;
+      bool pd = axis == 0 ? pdx : (axis == 1 ? pdy : pdz);
+      *n_out = axis * 2u + (pd ? 0u : 1u);
+      m_out[0] = m0; m_out[1] = m1; m_out[2] = m2;
+      return true;
+    }
+    F3 bound = {(float)(pdx ? m0 + 1 : m0), (float)(pdy ? m1 + 1 : m1), (float)(pdz ? m2 + 1 : m2)};
+    F3 tn = ((f3((float)ux, (float)uy, (float)uz) + bound * ms) - ro) * inv;
+    if (tn.x <= tn.y && tn.x <= tn.z) { t = tn.x; axis = 0u; m0 += pdx ? 1 : -1; }
+    else if (tn.y <= tn.z) { t = tn.y; axis = 1u; m1 += pdy ? 1 : -1; }
+    else { t = tn.z; axis = 2u; m2 += pdz ? 1 : -1; }
+  }
+  return false;
+}
+
+// Ray state shared by a sequence of march_chunk calls on one ray.
+struct Ray {
+  F3 o, d, inv;
+  bool pdx, pdy, pdz;
+};
+__device__ __forceinline__ Ray make_ray(F3 o, F3 d) {
+  Ray r;
+  r.o = o; r.d = d;
+  r.inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+  r.pdx = d.x > 0.0f; r.pdy = d.y > 0.0f; r.pdz = d.z > 0.0f;
+  return r;
+}
+
+// march_chunk: common.wgsl:579-910.
+//   SKIP_WATER / SKIP_GLASS / SUN_RAY are the WGSL arguments of the same name
+//   (skip_foliage only gates the tuft cross-quad trace, which this build does
+//   not have: tufts are transparent, as in the oracle).
+//   COUNT enables the per-ray traffic counters used by the roofline.
+struct Traffic { uint32_t chunk, l1, leaf, attr, pal, grid, iters; };
+
+template <bool SKIP_WATER, bool SKIP_GLASS, bool SUN_RAY, bool COUNT>
+__device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f, const Chunk& c, const Ray& r,
+                                           float t_limit, Traffic* tr) {
+  Hit h;
+  h.hit = false; h.t = 0.0f; h.normal = 0u; h.vx = h.vy = h.vz = 0u; h.mx = h.my = h.mz = 0u; h.iters = 0u;
+  if (COUNT) tr->chunk++;
+  const float vs = c.vs;
+  const F3 origin = ld3(c.origin);
+  const F3 ro = (r.o - origin) / vs;
+  const F3 rd = r.d;
+  const F3 inv = r.inv;
+  const F3 bmin = (ld3(c.aabb_min) - origin) / vs;
+  const F3 bmax = (ld3(c.aabb_max) - origin) / vs;
+  const F3 t0 = (bmin - ro) * inv;
+  const F3 t1 = (bmax - ro) * inv;
+  const F3 tmin3 = {fminf(t0.x, t1.x), fminf(t0.y, t1.y), fminf(t0.z, t1.z)};
+  const F3 tmax3 = {fmaxf(t0.x, t1.x), fmaxf(t0.y, t1.y), fmaxf(t0.z, t1.z)};
+  const float t_enter = fmaxf(fmaxf(tmin3.x, tmin3.y), tmin3.z);
+  const float t_exit = fminf(fminf(tmax3.x, tmax3.y), tmax3.z);
+  const float t_end = fminf(t_exit, t_limit / vs);
+  float t = fmaxf(t_enter, 0.0f);
+  if (t >= t_end) return h;
+  uint32_t axis;
+  if (tmin3.x >= tmin3.y && tmin3.x >= tmin3.z) axis = 0u;
+  else if (tmin3.y >= tmin3.z) axis = 1u;
+  else axis = 2u;
+  const bool pdx = r.pdx, pdy = r.pdy, pdz = r.pdz;
+  F3 pos = ro + rd * t;
+  int32_t cx = ffloor_i(pos.x), cy = ffloor_i(pos.y), cz = ffloor_i(pos.z);
+  if (t_enter > 0.0f) {
+    if (axis == 0) cx = pdx ? ffloor_i(bmin.x) : fceil_i(bmax.x) - 1;
+    else if (axis == 1) cy = pdy ? ffloor_i(bmin.y) : fceil_i(bmax.y) - 1;
+    else cz = pdz ? ffloor_i(bmin.z) : fceil_i(bmax.z) - 1;
+  }
+  cx = min(max(cx, 0), 63); cy = min(max(cy, 0), 63); cz = min(max(cz, 0), 63);
+  const uint32_t root_lo = c.root[0], root_hi = c.root[1];
+  const uint32_t root_ptr = c.root[2] & VM_PTR_MASK;
+  const bool attr_uniform = (c.attr_flags & VM_ATTR_UNIFORM) != 0u;
+
+  bool water_aware = SKIP_WATER && (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
+  if (water_aware && attr_uniform) {
+    if (c.attr_base == VM_WATER) return h;
+    water_aware = false;
+  }
+  bool foliage_aware = (c.attr_flags & VM_ATTR_HAS_FOLIAGE) != 0u;
+  if (foliage_aware && attr_uniform && !is_tuft(c.attr_base)) foliage_aware = false;
+  bool cutout_aware = (c.attr_flags & VM_ATTR_HAS_CUTOUT) != 0u && vs == 1.0f;
+  if (cutout_aware && attr_uniform && c.attr_base != VM_LEAVES && c.attr_base != VM_PINE_LEAVES) cutout_aware = false;
+  bool glass_aware = SKIP_GLASS && (c.attr_flags & VM_ATTR_HAS_GLASS) != 0u;
+  if (glass_aware && attr_uniform) {
+    if (c.attr_base == VM_GLASS) return h;
+    glass_aware = false;
+  }
+  const bool noncaster_aware = SUN_RAY && (c.attr_flags & VM_ATTR_HAS_EMITTER) != 0u;
+  if (noncaster_aware && attr_uniform && c.attr_base == VM_GLOWSTONE) return h;
+  const bool water_interface = !SKIP_WATER && (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
+  const bool attr_needed = (noncaster_aware && !attr_uniform) || (water_interface && !attr_uniform) || water_aware ||
+                           glass_aware || ((foliage_aware || cutout_aware) && !attr_uniform);
+  const bool any_filter = noncaster_aware || water_interface || water_aware || glass_aware || foliage_aware || cutout_aware;
+
+  uint32_t trav_lo = root_lo, trav_hi = root_hi;
+  if (water_aware) { trav_lo = c.dry[0]; trav_hi = c.dry[1]; }
+  const bool root_full = (c.root[2] & VM_FULL_BIT) != 0u;
+  if (trav_lo == 0u && trav_hi == 0u) return h;
+
+  uint32_t l1_cached = 0xFFFFFFFFu;
+  uint4 l1 = make_uint4(0u, 0u, 0u, 0u);
+  uint32_t leaf_cached = 0xFFFFFFFFu;
+  uint2 leaf = make_uint2(0u, 0u);
+  uint32_t attr = 0u;
+  for (;;) {
+    h.iters += 1u;
+    if (COUNT) tr->iters++;
+    if (h.iters > VM_MAX_ITERS) break;
+    if ((uint32_t)cx > 63u || (uint32_t)cy > 63u || (uint32_t)cz > 63u) break;
+    const uint32_t ux = cx, uy = cy, uz = cz;
+    int32_t skip = 16;
+    bool solid = false;
+    const uint32_t l1b = cell_bit(ux >> 4, uy >> 4, uz >> 4);
+    if (mask_has(trav_lo, trav_hi, l1b)) {
+      if (l1b != l1_cached) {
+        l1_cached = l1b;
+        if (root_full) {
+          l1 = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, VM_FULL_BIT, (l1b * 64u) | 0xF0000000u);
+        } else {
+          if (COUNT) tr->l1++;
+          l1 = ld_inner(w, (uint64_t)root_ptr + mask_below(root_lo, root_hi, l1b));
+        }
+        leaf_cached = 0xFFFFFFFFu;
+      }
+      bool line_skip = false;
+      if (water_aware) {
+        const uint32_t wl = l1.w >> 28u;
+        const float ly = (float)(uy & 15u);
+        if (wl < 15u && ly > (float)wl) {
+          line_skip = rd.y >= 0.0f;
+          if (!line_skip) {
+            const float hh = fmaxf(fabsf(rd.x), fabsf(rd.z));
+            if (hh > 1e-6f && (ly - (float)wl) > 16.0f * (fabsf(rd.y) / hh)) line_skip = true;
+          }
+        }
+      }
+      const uint32_t lfb = cell_bit((ux >> 2) & 3u, (uy >> 2) & 3u, (uz >> 2) & 3u);
+      if (line_skip) {
+        skip = 16;
+      } else if ((l1.z & VM_FULL_BIT) != 0u) {
+        solid = true;
+        if (attr_needed && lfb != leaf_cached) {
+          leaf_cached = lfb;
+          if (COUNT) tr->attr++;
+          attr = ld_brick(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + lfb);
+        }
+      } else if (mask_has(l1.x, l1.y, lfb)) {
+        if (lfb != leaf_cached) {
+          leaf_cached = lfb;
+          const uint32_t li = mask_below(l1.x, l1.y, lfb);
+          if (COUNT) tr->leaf++;
+          leaf = ld_leaf(w, (uint64_t)(l1.z & VM_PTR_MASK) + li);
+          if (attr_needed) {
+            if (COUNT) tr->attr++;
+            attr = ld_brick(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + li);
+          }
+        }
+        const uint32_t vb = cell_bit(ux & 3u, uy & 3u, uz & 3u);
+        if (mask_has(leaf.x, leaf.y, vb)) solid = true;
+        else skip = block2_empty(leaf.x, leaf.y, vb & 42u) ? 2 : 1;
+      } else {
+        skip = 4;
+      }
+    } else {
+      skip = block2_empty(trav_lo, trav_hi, l1b & 42u) ? 32 : 16;
+    }
+    if (solid && any_filter) {
+      // block id of this voxel, decoded once for all filters below
+      uint32_t id = c.attr_base;
+      const bool need_id = !attr_uniform && (noncaster_aware || water_interface || water_aware || glass_aware ||
+                                             foliage_aware || cutout_aware);
+      if (need_id) {
+        if (COUNT && (attr & VM_UNIFORM_BIT) == 0u) tr->pal++;
+        id = leaf_block(w, attr, ux, uy, uz);
+      }
+      if (noncaster_aware && id == VM_GLOWSTONE) { solid = false; skip = 1; }
+      if (solid && water_interface && id == VM_WATER) {
+        const uint32_t nid = axis * 2u + ((axis == 0 ? pdx : (axis == 1 ? pdy : pdz)) ? 0u : 1u);
+        const F3 outward = normal_of(nid);
+        const F3 boundary = r.o + rd * (t * vs);
+        if (COUNT) tr->grid++;
+        if (world_block_at(w, f, boundary + outward * (0.002f * vs)) == VM_WATER) { solid = false; skip = 1; }
+      }
+      if (solid && water_aware && id == VM_WATER) { solid = false; skip = (attr & VM_UNIFORM_BIT) != 0u ? 4 : 1; }
+      if (solid && glass_aware && id == VM_GLASS) { solid = false; skip = (attr & VM_UNIFORM_BIT) != 0u ? 4 : 1; }
+      if (solid && foliage_aware && is_tuft(id)) { solid = false; skip = 1; }
+      if (solid && cutout_aware && is_cutout_id(id)) {
+        const int32_t wx = __float2int_rz(c.origin[0]) + (int32_t)ux;
+        const int32_t wy = __float2int_rz(c.origin[1]) + (int32_t)uy;
+        const int32_t wz = __float2int_rz(c.origin[2]) + (int32_t)uz;
+        float qt; uint32_t qn; uint32_t qm[3];
+        if (cutout_march(wx, wy, wz, ux, uy, uz, ro, rd, t, axis, pdx, pdy, pdz, t > 0.0f, &qt, &qn, qm)) {
+          h.hit = true; h.t = qt * vs; h.normal = qn;
+          h.vx = ux; h.vy = uy; h.vz = uz;
+          h.mx = qm[0]; h.my = qm[1]; h.mz = qm[2];
+          return h;
+        }
+        solid = false;
+        skip = 1;
+      }
+    }
+    if (solid) {
+      h.hit = true;
+      h.t = t * vs;
+      const bool pd = axis == 0 ? pdx : (axis == 1 ? pdy : pdz);
+      h.normal = axis * 2u + (pd ? 0u : 1u);
+      h.vx = ux; h.vy = uy; h.vz = uz;
+      uint32_t m[3];
+      micro_entry(ux, uy, uz, ro, rd, t, axis, pdx, pdy, pdz, t > 0.0f, m);
+      h.mx = m[0]; h.my = m[1]; h.mz = m[2];
+      return h;
+    }
+    const int32_t bx0 = cx - (cx & (skip - 1)), by0 = cy - (cy & (skip - 1)), bz0 = cz - (cz & (skip - 1));
+    const float bndx = (float)(pdx ? bx0 + skip : bx0);
+    const float bndy = (float)(pdy ? by0 + skip : by0);
+    const float bndz = (float)(pdz ? bz0 + skip : bz0);
+    const float tnx = (bndx - ro.x) * inv.x, tny = (bndy - ro.y) * inv.y, tnz = (bndz - ro.z) * inv.z;
+    if (tnx <= tny && tnx <= tnz) { t = tnx; axis = 0u; }
+    else if (tny <= tnz) { t = tny; axis = 1u; }
+    else { t = tnz; axis = 2u; }
+    if (t >= t_end) break;
+    pos = ro + rd * t;
+    cx = ffloor_i(pos.x); cy = ffloor_i(pos.y); cz = ffloor_i(pos.z);
+    if (axis == 0) cx = pdx ? bx0 + skip : bx0 - 1;
+    else if (axis == 1) cy = pdy ? by0 + skip : by0 - 1;
+    else cz = pdz ? bz0 + skip : bz0 - 1;
+  }
+  return h;
+}
+
+// shadow_ray_t: common.wgsl:1156-1195
+template <bool COUNT>
+__device__ __noinline__ float shadow_ray_t(const DevWorld& w, const vm_frame& f, F3 ro, F3 rd, float max_dist, Traffic* tr) {
+  const Ray r = make_ray(ro, rd);
+  int32_t cx = ffloor_i(ro.x / 64.0f), cy = ffloor_i(ro.y / 64.0f), cz = ffloor_i(ro.z / 64.0f);
+  uint32_t last = VM_NO_CHUNK;
+  for (uint32_t i = 0; i < 24u; ++i) {
+    uint64_t gi;
+    if (!grid_rel(f, cx, cy, cz, &gi)) return -1.0f;
+    if (COUNT) tr->grid++;
+    const uint32_t ci = ld_grid(w, gi);
+    if (ci != VM_NO_CHUNK && ci != last) {
+      last = ci;
+      const Chunk c = ld_chunk(w, ci);
+      const Hit m = march_chunk<true, true, true, COUNT>(w, f, c, r, max_dist, tr);
+      if (m.hit) return m.t;
+    }
+    const float bx = (float)(r.pdx ? cx + 1 : cx) * 64.0f;
+    const float by = (float)(r.pdy ? cy + 1 : cy) * 64.0f;
+    const float bz = (float)(r.pdz ? cz + 1 : cz) * 64.0f;
+    const float tnx = (bx - ro.x) * r.inv.x, tny = (by - ro.y) * r.inv.y, tnz = (bz - ro.z) * r.inv.z;
+    float t;
+    uint32_t axis = 0u;
+    if (tnx <= tny && tnx <= tnz) t = tnx;
+    else if (tny <= tnz) { t = tny; axis = 1u; }
+    else { t = tnz; axis = 2u; }
+    if (t >= max_dist) return -1.0f;
+    if (axis == 0) cx += r.pdx ? 1 : -1;
+    else if (axis == 1) cy += r.pdy ? 1 : -1;
+    else cz += r.pdz ? 1 : -1;
+  }
+  return -1.0f;
+}
+
+struct WorldHit { bool hit; float t; uint32_t normal; uint32_t vx, vy, vz; uint32_t ci; };
+
+// trace_world: common.wgsl:1205-1253
+template <bool SKIP_WATER, bool COUNT>
+__device__ __noinline__ WorldHit trace_world(const DevWorld& w, const vm_frame& f, F3 ro, F3 rd, float max_dist, Traffic* tr) {
+  WorldHit out;
+  out.hit = false; out.t = max_dist; out.normal = 0u; out.vx = out.vy = out.vz = 0u; out.ci = VM_NO_CHUNK;
+  const F3 dir = {tiny_fix(rd.x), tiny_fix(rd.y), tiny_fix(rd.z)};
+  const F3 inv = {1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z};
+  const bool pdx = dir.x > 0.0f, pdy = dir.y > 0.0f, pdz = dir.z > 0.0f;
+  const Ray r = make_ray(ro, rd);
+  int32_t cx = ffloor_i(ro.x / 64.0f), cy = ffloor_i(ro.y / 64.0f), cz = ffloor_i(ro.z / 64.0f);
+  for (uint32_t i = 0; i < 16u; ++i) {
+    uint64_t gi;
+    if (!grid_rel(f, cx, cy, cz, &gi)) return out;
+    if (COUNT) tr->grid++;
+    const uint32_t ci = ld_grid(w, gi);
+    const float bx = (float)(pdx ? cx + 1 : cx) * 64.0f;
+    const float by = (float)(pdy ? cy + 1 : cy) * 64.0f;
+    const float bz = (float)(pdz ? cz + 1 : cz) * 64.0f;
+    const float tnx = (bx - ro.x) * inv.x, tny = (by - ro.y) * inv.y, tnz = (bz - ro.z) * inv.z;
+    float t_exit = tnx;
+    uint32_t axis = 0u;
+    if (tny < t_exit) { t_exit = tny; axis = 1u; }
+    if (tnz < t_exit) { t_exit = tnz; axis = 2u; }
+    if (ci != VM_NO_CHUNK) {
+      const Chunk c = ld_chunk(w, ci);
+      const Hit h = march_chunk<SKIP_WATER, true, false, COUNT>(w, f, c, r, fminf(t_exit, max_dist), tr);
+      if (h.hit) {
+        out.hit = true; out.t = h.t; out.normal = h.normal;
+        out.vx = h.vx; out.vy = h.vy; out.vz = h.vz; out.ci = ci;
+        return out;
+      }
+    }
+    if (t_exit >= max_dist) return out;
+    if (axis == 0) cx += pdx ? 1 : -1;
+    else if (axis == 1) cy += pdy ? 1 : -1;
+    else cz += pdz ? 1 : -1;
+  }
+  return out;
+}
+
+// hit_t: common.wgsl:1300-1318
+__device__ __forceinline__ float hit_t(const vm_frame& f, const Chunk& c, uint32_t vx, uint32_t vy, uint32_t vz,
+                                       uint32_t mx, uint32_t my, uint32_t mz, uint32_t nid, F3 rd) {
+  const F3 box_min = ld3(c.origin) + f3((float)vx, (float)vy, (float)vz) * c.vs;
+  if (nid >= VM_NORMAL_CROSS_A) {
+    if (nid == VM_NORMAL_CROSS_A)
+      return ((box_min.x - box_min.z) - (f.cam_pos[0] - f.cam_pos[2])) / (rd.x - rd.z);
+    return ((box_min.x + box_min.z + c.vs) - (f.cam_pos[0] + f.cam_pos[2])) / (rd.x + rd.z);
+  }
+  const uint32_t axis = nid >> 1u;
+  const float ms = c.vs / 4.0f;
+  const uint32_t mi = axis == 0 ? mx : (axis == 1 ? my : mz);
+  const float plane = comp(box_min, axis) + (float)(mi + ((nid & 1u) == 1u ? 1u : 0u)) * ms;
+  return (plane - f.cam_pos[axis]) / comp(rd, axis);
+}
+
+// depth_key / make_key: common.wgsl:1320-1330
+__device__ __forceinline__ uint32_t depth_key(const vm_frame& f, float t) {
+  float x = 1.0f - t / f.far_;
+  x = fminf(fmaxf(x, 0.0f), 1.0f);
+  return __float2uint_rz(x * 16777215.0f);
+}
+__device__ __forceinline__ unsigned long long make_key(const vm_frame& f, const Hit& h, uint32_t ci) {
+  const unsigned long long d = depth_key(f, h.t);
+  const uint32_t bx = h.vx | (h.mx << 6), by = h.vy | (h.my << 6), bz = h.vz | (h.mz << 6);
+  return (d << 40) | ((unsigned long long)h.normal << 37) | ((unsigned long long)ci << 24) |
+         (unsigned long long)((bx << 16) | (by << 8) | bz);
+}
+
+// tile_select geometry: tile_select.wgsl:1-9
+__device__ __forceinline__ bool box_outside(F3 bmin, F3 bmax, F3 n, F3 cam) {
+  const F3 p = {n.x > 0.0f ? bmax.x : bmin.x, n.y > 0.0f ? bmax.y : bmin.y, n.z > 0.0f ? bmax.z : bmin.z};
+  return dot(n, p - cam) < 0.0f;
+}
+__device__ __forceinline__ float box_distance(F3 p, F3 bmin, F3 bmax) {
+  const F3 d = {fmaxf(fmaxf(bmin.x - p.x, p.x - bmax.x), 0.0f), fmaxf(fmaxf(bmin.y - p.y, p.y - bmax.y), 0.0f),
+                fmaxf(fmaxf(bmin.z - p.z, p.z - bmax.z), 0.0f)};
+  return sqrtf(dot(d, d));
+}
+
+struct TilePlanes { F3 n[4]; float reach; };
+
+// tile_select.wgsl:17-57 for the 8x8 tile whose top-left pixel is (x0i, y0i)
+__device__ __forceinline__ TilePlanes tile_planes(const vm_frame& f, uint32_t x0i, uint32_t y0i) {
+  const float x0 = (float)x0i, y0 = (float)y0i;
+  const float x1 = x0 + 8.0f, y1 = y0 + 8.0f;
+  const F3 d00 = ray_dir(f, x0, y0), d10 = ray_dir(f, x1, y0), d11 = ray_dir(f, x1, y1), d01 = ray_dir(f, x0, y1);
+  const F3 center = ray_dir(f, (x0 + x1) * 0.5f, (y0 + y1) * 0.5f);
+  TilePlanes tp;
+  tp.n[0] = cross(d00, d10);
+  tp.n[1] = cross(d10, d11);
+  tp.n[2] = cross(d11, d01);
+  tp.n[3] = cross(d01, d00);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) if (!(dot(tp.n[i], center) >= 0.0f)) tp.n[i] = neg(tp.n[i]);
+  float reach = f.far_;
+  const uint32_t both = VM_FLAG_UNDERWATER | VM_FLAG_WATER_FAR;
+  if ((f.flags & both) == both) {
+    const float up = fmaxf(fmaxf(d00.y, d10.y), fmaxf(d11.y, d01.y));
+    const float submerged = fmaxf(f.sea_level - f.cam_pos[1], 0.0f);
+    float escape = 1e30f;
+    if (up > 0.0f) escape = submerged / up;
+    if (escape >= VM_WATER_FAR_DIST) {
+      reach = fminf(f.far_, VM_WATER_FAR_DIST);
+      const float dep_far = submerged - up * VM_WATER_FAR_DIST;
+      if ((f.flags & VM_FLAG_WATER_DARK) != 0u && fminf(submerged, dep_far) >= VM_WATER_DARK_DEPTH)
+        reach = fminf(reach, VM_WATER_DARK_DIST);
+    }
+  }
+  tp.reach = reach;
+  return tp;
+}
+
+// refract per the WGSL builtin definition
+__device__ __forceinline__ F3 refract(F3 e1, F3 e2, float e3) {
+  const float d = dot(e2, e1);
+  const float k = 1.0f - e3 * e3 * (1.0f - d * d);
+  if (k < 0.0f) return f3(0.0f, 0.0f, 0.0f);
+  return e1 * e3 - e2 * (e3 * d + sqrtf(k));
+}
+__device__ __forceinline__ float smoothstep(float e0, float e1, float x) {
+  const float t = fminf(fmaxf((x - e0) / (e1 - e0), 0.0f), 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+
+}  // namespace vmd

@@ -1,0 +1,189 @@
+// Buffer layouts and constants of the sparse-voxel-tree march, shared by the
+// host code, the CUDA kernels and the CPU oracle.
+//
+// Every struct here is byte-for-byte the layout the engine uploads to its
+// wgpu compute pass, so a caller can hand the engine's own buffers over
+// unchanged:
+//   vm_frame  == GpuFrame  (src/render/mod.rs:399-459, asserts at 458-466;
+//                           WGSL side src/render/shaders/common.wgsl:1-78)
+//   vm_chunk  == GpuChunk  (src/render/mod.rs:469-488;
+//                           WGSL side common.wgsl:80-96)
+//   inner pool  = array<vec4<u32>>  (common.wgsl:100; Inner, src/voxel/geometry.rs:11-18)
+//   leaf pool   = array<vec2<u32>>  (common.wgsl:101; u64 leaf masks)
+//   brick pool  = array<u32>        (common.wgsl:102; src/voxel/attributes.rs)
+//   grid        = array<u32>        (common.wgsl:121; src/render/mod.rs:82-86)
+//   vis         = array<u64>        (common.wgsl:115; key packing common.wgsl:1320-1330)
+#pragma once
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct vm_frame {
+  float cam_pos[3];
+  float time;
+  float cam_fwd[3];
+  float tan_half_fov;
+  float cam_right[3];
+  float aspect;
+  float cam_up[3];
+  float far_;          /* `far` in the reference; renamed because of <windows.h> */
+  float sun_dir[3];
+  float daylight;
+  uint32_t res[2];
+  uint32_t tiles[2];
+  uint32_t chunk_count;
+  uint32_t camera_chunk;
+  uint32_t flags;
+  uint32_t max_pairs;
+  float fog_density;
+  float fog_falloff;
+  float shadow_dist;
+  float ambient;
+  float fog_scatter;
+  float fog_g;
+  float fog_height;
+  float mip_bias;
+  int32_t grid_min[3];
+  float sea_level;
+  uint32_t grid_dim[3];
+  float water_absorb;
+  float jitter[2];
+  float taa_feedback;
+  uint32_t frame_index;
+  float cloud_cover;
+  float cloud_height;
+  float cloud_scale;
+  float cloud_speed;
+  float godray_strength;
+  uint32_t godray_steps;
+  float godray_dist;
+  float cloud_shadow;
+  float tint_strength;
+  int32_t tint_seed;
+  float tint_freq_t;
+  float tint_freq_h;
+  float wave_amp;
+  float wave_scale;
+  float wave_speed;
+  float wave_reflect_slope;
+  float shaft_origin[2];
+  float shaft_texel;
+  float shaft_soft;
+  float cloud_patch;
+  float cloud_relief;
+  float haze_warm;
+  float zenith_deep;
+  float prev_view_proj[16];
+} vm_frame;
+
+typedef struct vm_chunk {
+  float aabb_min[3];
+  float voxel_size;
+  float aabb_max[3];
+  uint32_t lod;
+  float origin[3];
+  float fade;
+  uint32_t root[4];     /* Inner: mask lo, mask hi, run_ptr (bit31 FULL), leaf_prefix */
+  uint32_t attr_base;
+  uint32_t attr_flags;
+  uint32_t light_base;
+  uint32_t light_flags;
+  uint32_t dry_mask[2];
+  uint32_t reserved[2];
+} vm_chunk;
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#include <cstddef>
+static_assert(sizeof(vm_frame) == 352, "GpuFrame is 352 bytes (src/render/mod.rs:458)");
+static_assert(offsetof(vm_frame, res) == 80, "res offset");
+static_assert(offsetof(vm_frame, grid_min) == 144, "grid_min offset");
+static_assert(offsetof(vm_frame, grid_dim) == 160, "grid_dim offset");
+static_assert(offsetof(vm_frame, jitter) == 176, "jitter offset");
+static_assert(offsetof(vm_frame, cloud_cover) == 192, "src/render/mod.rs:460");
+static_assert(offsetof(vm_frame, godray_strength) == 208, "src/render/mod.rs:461");
+static_assert(offsetof(vm_frame, tint_strength) == 224, "src/render/mod.rs:462");
+static_assert(offsetof(vm_frame, wave_amp) == 240, "src/render/mod.rs:463");
+static_assert(offsetof(vm_frame, shaft_origin) == 256, "src/render/mod.rs:464");
+static_assert(offsetof(vm_frame, cloud_patch) == 272, "src/render/mod.rs:465");
+static_assert(offsetof(vm_frame, prev_view_proj) == 288, "src/render/mod.rs:466");
+static_assert(sizeof(vm_chunk) == 96, "GpuChunk is 96 bytes");
+static_assert(offsetof(vm_chunk, root) == 48, "root offset");
+static_assert(offsetof(vm_chunk, attr_base) == 64, "attr_base offset");
+static_assert(offsetof(vm_chunk, dry_mask) == 80, "dry_mask offset");
+#endif
+
+/* ---- constants (common.wgsl:138-263, src/render/mod.rs:20-39,82-86) ---- */
+#define VM_TILE 8u                    /* src/render/mod.rs:20 */
+#define VM_MAX_CHUNKS 8191u           /* src/render/mod.rs:21, 13-bit chunk field */
+#define VM_MAX_PAIRS_FLOOR (1u << 20) /* src/render/mod.rs:23 */
+#define VM_PAIRS_PER_TILE 16u         /* src/render/mod.rs:25 */
+#define VM_TILE_ID_BITS 19u           /* src/render/mod.rs:32 */
+#define VM_MAX_TILES (1u << 19)
+#define VM_GRID_X 32u                 /* src/render/mod.rs:82-84 */
+#define VM_GRID_Y 8u
+#define VM_GRID_Z 32u
+#define VM_NO_CHUNK 0xFFFFFFFFu
+#define VM_FULL_BIT 0x80000000u
+#define VM_PTR_MASK 0x7FFFFFFFu
+#define VM_UNIFORM_BIT 0x80000000u
+#define VM_PREFIX_MASK 0x0FFFFFFFu
+#define VM_MAX_ITERS 512u             /* common.wgsl:163 */
+
+#define VM_FLAG_HIZ 1u
+#define VM_FLAG_HEATMAP 2u
+#define VM_FLAG_SHADOWS 4u
+#define VM_FLAG_WATER_REFLECT 16u
+#define VM_FLAG_WATER_REFRACT 32u
+#define VM_FLAG_UNDERWATER 64u
+#define VM_FLAG_WATER_FAR 2097152u
+#define VM_FLAG_WATER_DARK 4194304u
+
+#define VM_ATTR_UNIFORM 1u
+#define VM_ATTR_HAS_WATER 2u
+#define VM_ATTR_HAS_FOLIAGE 4u
+#define VM_ATTR_HAS_CUTOUT 8u
+#define VM_ATTR_HAS_GLASS 16u
+#define VM_ATTR_HAS_EMITTER 32u
+
+/* block ids (src/block.rs:3-35) */
+#define VM_AIR 0u
+#define VM_STONE 1u
+#define VM_DIRT 2u
+#define VM_GRASS 3u
+#define VM_SAND 4u
+#define VM_GRAVEL 5u
+#define VM_LOG 6u
+#define VM_LEAVES 7u
+#define VM_PLANKS 8u
+#define VM_GLASS 10u
+#define VM_GLOWSTONE 11u
+#define VM_BEDROCK 12u
+#define VM_WATER 13u
+#define VM_PINE_LEAVES 16u
+#define VM_TALL_GRASS 18u
+#define VM_AMBER_LAMP 20u
+#define VM_AZURE_LAMP 21u
+#define VM_VERDANT_LAMP 22u
+#define VM_GRASS_TALL 24u
+#define VM_REEDS 25u
+#define VM_BLOCK_COUNT 26u
+
+/* WGSL override defaults that reach the march (common.wgsl:180-263) */
+#define VM_LEAF_FILL 0.62f
+#define VM_SURFACE_EPS 0.02f          /* common.wgsl:1258 */
+#define VM_WATER_IOR 1.333f           /* common.wgsl:1256 */
+#define VM_WATER_REFRACT_DIST 96.0f   /* resolve.wgsl:879 */
+#define VM_WATER_REFRACT_NEAR 96.0f   /* resolve.wgsl:873 */
+#define VM_WATER_REFRACT_FAR 192.0f   /* resolve.wgsl:874 */
+#define VM_GLASS_TRANSMIT_DIST 192.0f /* resolve.wgsl:886 */
+#define VM_WATER_FAR_DIST 128.0f      /* common.wgsl:165 */
+#define VM_WATER_DARK_DEPTH 15.0f     /* common.wgsl:167 */
+#define VM_WATER_DARK_DIST 64.0f      /* common.wgsl:172 */
+
+/* normal ids (common.wgsl:387-398) */
+#define VM_NORMAL_PY 3u
+#define VM_NORMAL_CROSS_A 6u
+#define VM_NORMAL_CROSS_B 7u

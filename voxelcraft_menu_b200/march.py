@@ -1,0 +1,256 @@
+"""The march behind the engine's renderer interface.
+
+`Renderer` mirrors the engine's `Renderer` for this path
+(src/render/mod.rs:747-2060): `sync_world`, `build_chunk_list`, `render` and
+the `march_stats` / `pair_demand` read-backs, each a thin call into the C ABI
+of include/voxmarch.h.  Every call raises `MarchError` when the library
+reports an error; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import native
+from .native import VmCaps, VmDevicePtrs, VmFrame, VmStats, VmTraffic, lib, ptr
+from .world import FLAG_HIZ, View, World
+
+VM_OK = 0
+STATUS = {0: "VM_OK", 1: "VM_E_INVALID", 2: "VM_E_CAPACITY", 3: "VM_E_TILE_OVERFLOW", 4: "VM_E_ITER_CAP",
+          5: "VM_E_TIMEOUT", 6: "VM_E_CUDA", 7: "VM_E_NOT_READY"}
+
+# fused tile variants (vm_set_tuning)
+TILE_8x8, TILE_16x8, TILE_16x16, TILE_32x16 = 0, 1, 2, 3
+TILE_SHAPES = {0: (8, 8), 1: (16, 8), 2: (16, 16), 3: (32, 16)}
+
+
+class MarchError(RuntimeError):
+    def __init__(self, code: int, text: str):
+        super().__init__(f"{STATUS.get(code, code)}: {text}")
+        self.code = code
+
+
+@dataclass
+class PairDemand:
+    """src/render/mod.rs:41-60"""
+    select: int
+    deferred: int
+    recover: int
+    cap: int
+
+    def overflowed(self) -> bool:
+        return self.select > self.cap or self.deferred > self.cap or self.recover > self.cap
+
+
+class Marcher:
+    """One vm_ctx: the device state of one renderer."""
+
+    def __init__(self, max_width: int, max_height: int, device: int = 0, max_chunks: int = 8191, max_views: int = 0,
+                 max_batch_pixels: int = 0):
+        self._L = lib()
+        caps = VmCaps(max_width, max_height, max_chunks, max_views, max_batch_pixels)
+        h = C.c_void_p()
+        rc = self._L.vm_create(device, C.byref(caps), C.byref(h))
+        if rc:
+            raise MarchError(rc, "vm_create failed (no CUDA device?)")
+        self._h = h
+        self.view: View | None = None
+
+    def close(self):
+        if self._h:
+            self._L.vm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc: int):
+        if rc != VM_OK:
+            raise MarchError(rc, self._L.vm_last_error(self._h).decode())
+
+    # -- inputs -------------------------------------------------------------
+    def upload_world(self, inners: np.ndarray, leaves: np.ndarray, bricks: np.ndarray):
+        i = np.ascontiguousarray(inners, np.uint32)
+        l = np.ascontiguousarray(leaves, np.uint32)
+        b = np.ascontiguousarray(bricks, np.uint32)
+        self._ck(self._L.vm_upload_world(self._h, ptr(i), i.size // 4, ptr(l), l.size // 2, ptr(b), b.size))
+
+    def update_pool(self, pool: int, offset: int, data: np.ndarray):
+        d = np.ascontiguousarray(data, np.uint32)
+        per = (4, 2, 1)[pool]
+        self._ck(self._L.vm_update_pool(self._h, pool, offset, ptr(d), d.size // per))
+
+    def upload_view(self, v: View):
+        ch = np.ascontiguousarray(v.chunks)
+        g = np.ascontiguousarray(v.grid, np.uint32)
+        self._ck(self._L.vm_upload_chunks(self._h, ptr(ch), len(ch), ptr(g), g.size))
+        self._ck(self._L.vm_set_frame(self._h, C.byref(v.frame)))
+        self.view = v
+
+    def set_frame(self, frame: VmFrame):
+        self._ck(self._L.vm_set_frame(self._h, C.byref(frame)))
+
+    def set_tuning(self, tile_variant: int = TILE_16x16, ctas_per_sm: int = 0):
+        self._ck(self._L.vm_set_tuning(self._h, tile_variant, ctas_per_sm))
+
+    # -- the engine's passes ------------------------------------------------------
+    def select(self):
+        self._ck(self._L.vm_select(self._h))
+
+    def march(self):
+        self._ck(self._L.vm_march(self._h))
+
+    def primary_shadow(self):
+        self._ck(self._L.vm_primary_shadow(self._h))
+
+    def secondary(self):
+        self._ck(self._L.vm_secondary(self._h))
+
+    def render_passes(self):
+        """tile_select .. march (+Hi-Z / recover) .. primary_shadow .. secondary"""
+        self.select()
+        self.march()
+        self.primary_shadow()
+        self.secondary()
+
+    def render(self):
+        """The fused persistent kernel: same outputs as render_passes()."""
+        self._ck(self._L.vm_render(self._h))
+
+    def render_counted(self) -> dict:
+        t = VmTraffic()
+        self._ck(self._L.vm_render_counted(self._h, C.byref(t)))
+        return {n: int(getattr(t, n)) for n, _ in VmTraffic._fields_}
+
+    def sync(self):
+        self._ck(self._L.vm_sync(self._h))
+
+    # -- outputs --------------------------------------------------------------
+    def _npix(self):
+        f = self.view.frame
+        return int(f.res[0]) * int(f.res[1])
+
+    def read_vis(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty(self._npix(), np.uint64) if out is None else out
+        self._ck(self._L.vm_read_vis(self._h, ptr(out)))
+        return out
+
+    def read_shadow(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty(self._npix(), np.float32) if out is None else out
+        self._ck(self._L.vm_read_shadow(self._h, ptr(out)))
+        return out
+
+    def read_secondary(self):
+        k = np.empty(self._npix(), np.uint64)
+        t = np.empty(self._npix(), np.float32)
+        self._ck(self._L.vm_read_secondary(self._h, ptr(k), ptr(t)))
+        return k, t
+
+    def read_hiz(self) -> np.ndarray:
+        f = self.view.frame
+        out = np.empty(int(f.tiles[0]) * int(f.tiles[1]), np.uint32)
+        self._ck(self._L.vm_read_hiz(self._h, ptr(out)))
+        return out
+
+    def write_hiz(self, hiz: np.ndarray):
+        h = np.ascontiguousarray(hiz, np.uint32)
+        self._ck(self._L.vm_write_hiz(self._h, ptr(h)))
+
+    def read_heatmap(self) -> np.ndarray:
+        out = np.empty(self._npix(), np.uint32)
+        self._ck(self._L.vm_read_heatmap(self._h, ptr(out)))
+        return out
+
+    def read_expanded(self, origin, dims):
+        n = self._npix()
+        vox = np.empty(n, np.uint32)
+        face = np.empty(n, np.uint8)
+        t = np.empty(n, np.float32)
+        o = np.asarray(origin, np.int32)
+        d = np.asarray(dims, np.uint32)
+        self._ck(self._L.vm_read_expanded(self._h, ptr(o), ptr(d), ptr(vox), ptr(face), ptr(t)))
+        return vox, face, t
+
+    def stats(self) -> VmStats:
+        s = VmStats()
+        self._ck(self._L.vm_stats_read(self._h, C.byref(s)))
+        return s
+
+    def pair_demand(self) -> PairDemand:
+        s = self.stats()
+        return PairDemand(s.pairs_selected, s.pairs_deferred, s.pairs_recovered, s.max_pairs)
+
+    def device_buffers(self) -> VmDevicePtrs:
+        p = VmDevicePtrs()
+        self._ck(self._L.vm_device_buffers(self._h, C.byref(p)))
+        return p
+
+    # -- batches -------------------------------------------------------------
+    def batch_set(self, views: list[View]):
+        frames = (VmFrame * len(views))(*[v.frame for v in views])
+        chunks = np.ascontiguousarray(np.concatenate([v.chunks for v in views]))
+        counts = np.array([len(v.chunks) for v in views], np.uint32)
+        grids = np.ascontiguousarray(np.concatenate([v.grid for v in views]).astype(np.uint32))
+        glens = np.array([v.grid.size for v in views], np.uint32)
+        self._ck(self._L.vm_batch_set(self._h, len(views), C.cast(frames, C.c_void_p), ptr(chunks), ptr(counts),
+                                      ptr(grids), ptr(glens)))
+        self.batch_views = views
+
+    def batch_run(self, per_view: bool = False):
+        self._ck(self._L.vm_batch_run(self._h, 1 if per_view else 0))
+
+    def batch_pixels(self) -> int:
+        return int(self._L.vm_batch_pixels(self._h))
+
+    def batch_read(self):
+        n = self.batch_pixels()
+        vis = np.empty(n, np.uint64)
+        sh = np.empty(n, np.float32)
+        self._ck(self._L.vm_batch_read(self._h, ptr(vis), ptr(sh)))
+        return vis, sh
+
+
+class Renderer:
+    """The engine's Renderer, reduced to this path (src/render/mod.rs:747)."""
+
+    def __init__(self, width: int, height: int, device: int = 0):
+        self.size = (width, height)
+        self.marcher = Marcher(width, height, device)
+        self.world = None
+        self._view = None
+
+    def sync_world(self, world: World):
+        """src/render/mod.rs:1355-1396"""
+        self.world = world
+        self.marcher.upload_world(*world.pools())
+
+    def build_chunk_list(self, cam) -> View:
+        """src/render/mod.rs:1447-1564"""
+        cam.width, cam.height = self.size
+        self._view = self.world.view(cam)
+        self.marcher.upload_view(self._view)
+        return self._view
+
+    def render(self, fused: bool = True):
+        """src/render/mod.rs:1593-1919 (march, Hi-Z, shadow and secondary passes)"""
+        if fused:
+            self.marcher.render()
+        else:
+            self.marcher.render_passes()
+
+    def pair_demand(self) -> PairDemand:
+        return self.marcher.pair_demand()
+
+    def march_stats(self) -> dict:
+        """src/render/mod.rs:1977-2045 over the FLAG_HEATMAP iteration buffer."""
+        it = self.marcher.read_heatmap().astype(np.int64)
+        touched = it[it > 0]
+        s = np.sort(touched)
+        pct = (lambda q: int(s[min(len(s) - 1, int(q * len(s)))]) if len(s) else 0)
+        return {"pixels": int(it.size), "iters": int(it.sum()), "worst": int(it.max(initial=0)),
+                "touched": int(touched.size), "p50": pct(0.5), "p90": pct(0.9), "p99": pct(0.99)}
