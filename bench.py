@@ -178,7 +178,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--variant", type=int, default=-1, help="fused tile variant (-1: autotune)")
+    ap.add_argument("--warps", type=int, default=0, help="primary kernel warps per block (0: autotune)")
+    ap.add_argument("--reg-level", type=int, default=0, help="primary kernel register level with --warps")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -207,11 +208,11 @@ def main():
     m.upload_world(*pools)
 
     # tile shape / CTAs per SM: autotuned on this frame unless fixed
-    if args.variant >= 0:
-        best = {"variant": args.variant, "ctas_per_sm": 0}
+    if args.warps > 0:
+        best = {"warps": args.warps, "reg_level": args.reg_level, "ctas_per_sm": 0}
     else:
         best = tuning.autotune_single(m, vb, warm=va)
-    m.set_tuning(best["variant"], best["ctas_per_sm"])
+    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"])
 
     # frame A then the timed frame B (Hi-Z of A carried over)
     m.upload_view(va)
@@ -297,8 +298,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "resolution": [1920, 1080], "chunks": int(len(vb.chunks)),
-                       "tile": best, "l2": "flushed between timed steps (256 MB write)",
+                       "tuning": best, "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"replicas x{world}"},
+            "work_per_step": traffic,
             "rays_per_step": {"primary": traffic["rays_primary"], "shadow": traffic["rays_shadow"],
                               "secondary_uncounted": traffic["rays_secondary"]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -307,7 +309,7 @@ def main():
                          "bytes_per_dda_step": algo_bytes / max(traffic["iters"], 1)},
             "e2e": {"value": world * rays / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 5 * args.steps,   # bounds, cull, primary, shadow, secondary per frame
             "clocks": clocks,
             "device_error": int(stats.device_error),
         }

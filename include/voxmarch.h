@@ -79,13 +79,16 @@ int vm_primary_shadow(vm_ctx* ctx);
 int vm_secondary(vm_ctx* ctx);
 
 /* The same frame as vm_select + vm_march + vm_primary_shadow + vm_secondary
- * in one fused, persistent kernel; identical vis / shadow / secondary output.
- * hiz receives the final visibility's per-8x8-tile minimum. */
+ * as a warp-independent wavefront pipeline (per-tile cull, front-to-back
+ * primary march with an exact early out, queued shadow and secondary rays);
+ * identical vis / shadow / secondary output.  hiz receives the final
+ * visibility's per-8x8-tile minimum. */
 int vm_render(vm_ctx* ctx);
 
-/* Tuning of vm_render and vm_batch_run: tile variant 0 = 8x8, 1 = 16x8,
- * 2 = 16x16, 3 = 32x16 pixels per CTA; ctas_per_sm 0 = occupancy maximum. */
-int vm_set_tuning(vm_ctx* ctx, int tile_variant, int ctas_per_sm);
+/* Tuning of vm_render and vm_batch_run's primary-ray kernel: warps per block
+ * (4 or 8), register budget (0 unconstrained, 1 about 80, 2 64 registers per
+ * thread) and resident blocks per SM (0 = occupancy maximum). */
+int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_sm);
 
 /* Read-backs (synchronise the context's stream). */
 int vm_read_vis(vm_ctx* ctx, uint64_t* out);                 /* res.x*res.y keys (common.wgsl:1324) */
@@ -120,6 +123,9 @@ int vm_stats_read(vm_ctx* ctx, vm_stats* out);
 typedef struct vm_traffic {
   uint64_t chunk_records, l1_fetches, leaf_fetches, attr_fetches, palette_decodes, grid_lookups, iters;
   uint64_t rays_primary, rays_shadow, rays_secondary;
+  uint64_t list_entries;    /* tile-list entries the primary rays examined */
+  uint64_t stage_iters[3];  /* DDA steps of the primary, shadow and secondary rays */
+  uint64_t stage_chunks[3]; /* chunk marches of the primary, shadow and secondary rays */
 } vm_traffic;
 int vm_render_counted(vm_ctx* ctx, vm_traffic* out);
 

@@ -11,7 +11,7 @@ import pytest
 
 from oracle.oracle import Oracle
 from voxelcraft_menu_b200 import world as W
-from voxelcraft_menu_b200.march import MarchError, Marcher, TILE_SHAPES
+from voxelcraft_menu_b200.march import PRIMARY_WARPS, MarchError, Marcher
 from voxelcraft_menu_b200.world import Camera, Recipe, World
 
 pytestmark = pytest.mark.gpu
@@ -70,12 +70,12 @@ def test_engine_passes_match_the_oracle(small):
     assert (vis != 0).mean() > 0.3 and (sh > 0).any() and ((sk >> 63) & 1).any()
 
 
-@pytest.mark.parametrize("variant", sorted(TILE_SHAPES))
-def test_fused_kernel_matches_the_oracle(small, variant):
+@pytest.mark.parametrize("warps,level,per_sm", [(4, 0, 0), (4, 1, 0), (4, 2, 1), (8, 0, 0), (8, 2, 0)])
+def test_pipeline_matches_the_oracle(small, warps, level, per_sm):
     w, pools, m = small
     v = w.view(W.small_terrain_camera())
     m.upload_view(v)
-    m.set_tuning(variant)
+    m.set_tuning(warps, level, per_sm)
     m.render()
     o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
     assert_same(m.read_vis(), vis, "vis")
@@ -84,7 +84,7 @@ def test_fused_kernel_matches_the_oracle(small, variant):
     assert_same(gk, sk, "secondary key")
     assert_same(gt, st, "secondary t")
     assert m.stats().device_error == 0
-    m.set_tuning(2)
+    m.set_tuning()
 
 
 def test_expanded_outputs(small):
@@ -154,12 +154,12 @@ def test_ragged_resolutions(small, res):
     v = w.view(W.small_terrain_camera(width=res[0], height=res[1]))
     m.upload_view(v)
     o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
-    for variant in (0, 2, 3):
-        m.set_tuning(variant)
+    for warps in PRIMARY_WARPS:
+        m.set_tuning(warps)
         m.render()
-        assert_same(m.read_vis(), vis, f"fused {variant} vis")
-        assert_same(m.read_shadow(), sh, f"fused {variant} shadow")
-    m.set_tuning(2)
+        assert_same(m.read_vis(), vis, f"pipeline {warps} warps vis")
+        assert_same(m.read_shadow(), sh, f"pipeline {warps} warps shadow")
+    m.set_tuning()
     m.render_passes()
     assert_same(m.read_vis(), vis, "passes vis")
     assert_same(m.read_shadow(), sh, "passes shadow")
@@ -252,10 +252,9 @@ def test_large_world_full_hd(large):
     tx = int(v.frame.tiles[0])
     rows = (60 * tx, 64 * tx)            # four tile rows across the horizon
     vis, _, _ = o.frame_vis(tiles=rows)
-    px = (rows[0] * 64, rows[1] * 64)
     sl = slice(60 * 8 * 1920, 64 * 8 * 1920)
     assert_same(fv[sl], vis[sl], "vis band")
-    sh = o.shadow(np.where(np.arange(vis.size) < sl.stop, vis, 0), pix=(sl.start, sl.stop))
+    sh = o.shadow(vis, pix=(sl.start, sl.stop))
     assert_same(fs[sl], sh[sl], "shadow band")
 
 

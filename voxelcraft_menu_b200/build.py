@@ -27,9 +27,9 @@ NVCC_FLAGS = ARCH + [
 ]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", f"-I{ROOT}", f"-I{CSRC}"]
 
-CU_SOURCES = ["kernels.cu", "capi.cu"]
+CU_SOURCES = ["kernels.cu", "pipeline.cu", "capi.cu"]
 CPP_SOURCES = ["world.cpp"]
-HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "world.h"]
+HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "ray_stages.cuh", "world.h"]
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:

@@ -10,7 +10,6 @@
 #include "../../include/voxmarch.h"
 #include "kernels.cuh"
 
-using vmk::FusedArgs;
 using vmk::ViewDesc;
 
 namespace {
@@ -40,21 +39,19 @@ struct vm_ctx {
   bool have_frame = false;
   // per-frame outputs and scratch
   DevBuf vis, shadow, sec_key, sec_t, hiz, dbg, pairs, counters, err, work, dkmax, sufmax, traffic, expand;
+  DevBuf tile_list, tile_count, shadow_q, sec_q;
   // batch
   DevBuf b_frames, b_views, b_views1, b_chunks, b_grids, b_vis, b_shadow, b_seck, b_sect, b_hiz, b_dkmax, b_sufmax;
+  DevBuf b_tile_list, b_tile_count, b_shadow_q, b_sec_q;
   std::vector<vm_frame> bh_frames;
   std::vector<ViewDesc> bh_views;
-  std::vector<uint32_t> bh_counts;
-  std::vector<uint64_t> bh_grid_lens;
-  uint32_t b_n_views = 0, b_total_tiles = 0, b_n_chunks = 0;
-  uint64_t b_pixels = 0, b_grid_total = 0, b_hiz_total = 0;
+  uint32_t b_n_views = 0, b_total_tiles = 0, b_n_chunks = 0, b_list_cap = 1;
+  uint64_t b_pixels = 0, b_grid_total = 0;
   bool b_underwater = false;
-  int b_layout_variant = -1;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
-  // tuning
-  int variant = vmk::FUSED_16x16;
-  int ctas_per_sm = 0;
+  // tuning of the primary kernel
+  vmk::PipeTuning tuning{4, 0, 0};
   std::string err_text;
 };
 
@@ -158,59 +155,55 @@ int check_ready(vm_ctx* ctx) {
   return check_frame(ctx, f, ctx->n_chunks, ctx->grid_len);
 }
 
-uint32_t fused_grid(vm_ctx* ctx, int variant, bool underwater, bool count, uint32_t tiles) {
-  int per = ctx->ctas_per_sm > 0 ? ctx->ctas_per_sm : vmk::fused_max_ctas_per_sm(variant, underwater, count);
-  if (per <= 0) per = 1;
-  uint64_t g = (uint64_t)ctx->sms * (uint64_t)per;
-  return (uint32_t)std::min<uint64_t>(g, tiles);
-}
+constexpr uint32_t LIST_CAP_MAX = 256;   // chunks stored per 8x8 tile before the march rescans
 
-FusedArgs base_args(vm_ctx* ctx) {
-  FusedArgs a;
+vmk::PipeArgs base_args(vm_ctx* ctx) {
+  vmk::PipeArgs a;
   memset(&a, 0, sizeof a);
   a.inners = (const uint4*)ctx->inners.p; a.n_inners = ctx->n_inners;
   a.leaves = (const uint2*)ctx->leaves.p; a.n_leaves = ctx->n_leaves;
   a.bricks = (const uint32_t*)ctx->bricks.p; a.n_bricks = ctx->n_bricks;
   a.err = (uint32_t*)ctx->err.p;
   a.work = (uint32_t*)ctx->work.p;
+  a.traffic = (vmk::Traffic64*)ctx->traffic.p;
+  a.do_shadow = 1;
+  a.do_secondary = 1;
+  a.px_per_lane = 1;
   return a;
 }
 
-// The single-view fused launch (frame and view descriptor by value).
+// The single-view pipeline (frame and view descriptor by value).
 int enqueue_render(vm_ctx* ctx, bool count) {
   const vm_frame& f = ctx->frame;
-  uint32_t tw, th;
-  vmk::fused_dims(ctx->variant, &tw, &th);
   ViewDesc v;
   memset(&v, 0, sizeof v);
   v.n_chunks = ctx->n_chunks;
   v.grid_len = (uint32_t)ctx->grid_len;
-  v.tiles_x = (f.res[0] + tw - 1) / tw;
-  v.tiles_y = (f.res[1] + th - 1) / th;
-  FusedArgs a = base_args(ctx);
+  v.tiles_x = f.tiles[0];
+  v.tiles_y = f.tiles[1];
+  vmk::PipeArgs a = base_args(ctx);
   a.frames = nullptr;
   a.views = nullptr;
   a.n_views = 1;
   a.total_tiles = v.tiles_x * v.tiles_y;
   a.chunks = (const vm_chunk*)ctx->chunks.p;
   a.grids = (const uint32_t*)ctx->grid.p;
-  a.dkmax = (const uint32_t*)ctx->dkmax.p;
-  a.sufmax = (const uint32_t*)ctx->sufmax.p;
+  a.dkmax = (uint32_t*)ctx->dkmax.p;
+  a.sufmax = (uint32_t*)ctx->sufmax.p;
+  a.tile_list = (uint16_t*)ctx->tile_list.p;
+  a.tile_count = (uint32_t*)ctx->tile_count.p;
+  a.list_cap = std::max(1u, std::min(f.chunk_count, LIST_CAP_MAX));
   a.vis = (unsigned long long*)ctx->vis.p;
   a.shadow = (float*)ctx->shadow.p;
   a.sec_key = (unsigned long long*)ctx->sec_key.p;
   a.sec_t = (float*)ctx->sec_t.p;
   a.hiz = (uint32_t*)ctx->hiz.p;
-  a.traffic = (vmk::Traffic64*)ctx->traffic.p;
-  a.do_shadow = 1;
-  a.do_secondary = 1;
+  a.shadow_q = (vmk::ShadowItem*)ctx->shadow_q.p;
+  a.sec_q = (vmk::SecItem*)ctx->sec_q.p;
   a.frame0 = f;
   a.view0 = v;
-  CK(vmk::launch_chunk_bounds(nullptr, nullptr, 1, f, v, a.chunks, (uint32_t*)ctx->dkmax.p, (uint32_t*)ctx->sufmax.p,
-                              ctx->stream));
-  CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(uint32_t), ctx->stream));
   const bool uw = (f.flags & VM_FLAG_UNDERWATER) != 0u;
-  CK(vmk::launch_fused(a, ctx->variant, uw, count, fused_grid(ctx, ctx->variant, uw, count, a.total_tiles), ctx->stream));
+  CK(vmk::launch_pipeline(a, ctx->tuning, uw, count, ctx->sms, ctx->stream));
   return VM_OK;
 }
 
@@ -245,9 +238,13 @@ int vm_create(int device_ordinal, const vm_caps* caps, vm_ctx** out) {
   rc |= ensure(ctx, ctx->counters, 64);
   rc |= ensure(ctx, ctx->err, 64);
   rc |= ensure(ctx, ctx->work, 64);
-  rc |= ensure(ctx, ctx->traffic, sizeof(vmk::Traffic64));
+  rc |= ensure(ctx, ctx->traffic, 3 * sizeof(vmk::Traffic64));
   rc |= ensure(ctx, ctx->dkmax, (size_t)ctx->caps.max_chunks * 4);
   rc |= ensure(ctx, ctx->sufmax, (size_t)ctx->caps.max_chunks * 4);
+  rc |= ensure(ctx, ctx->tile_list, tiles * LIST_CAP_MAX * 2);
+  rc |= ensure(ctx, ctx->tile_count, tiles * 4);
+  rc |= ensure(ctx, ctx->shadow_q, npix * sizeof(vmk::ShadowItem));
+  rc |= ensure(ctx, ctx->sec_q, npix * sizeof(vmk::SecItem));
   if (rc != VM_OK) { vm_destroy(ctx); return VM_E_CUDA; }
   cudaMemsetAsync(ctx->hiz.p, 0, tiles * 4, ctx->stream);
   cudaMemsetAsync(ctx->err.p, 0, 64, ctx->stream);
@@ -266,7 +263,9 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->sec_key, &ctx->sec_t, &ctx->hiz, &ctx->dbg, &ctx->pairs, &ctx->counters, &ctx->err,
                    &ctx->work, &ctx->dkmax, &ctx->sufmax, &ctx->traffic, &ctx->expand, &ctx->b_frames,
                    &ctx->b_views, &ctx->b_views1, &ctx->b_chunks, &ctx->b_grids, &ctx->b_vis, &ctx->b_shadow,
-                   &ctx->b_seck, &ctx->b_sect, &ctx->b_hiz, &ctx->b_dkmax, &ctx->b_sufmax};
+                   &ctx->b_seck, &ctx->b_sect, &ctx->b_hiz, &ctx->b_dkmax, &ctx->b_sufmax, &ctx->tile_list,
+                   &ctx->tile_count, &ctx->shadow_q, &ctx->sec_q, &ctx->b_tile_list, &ctx->b_tile_count,
+                   &ctx->b_shadow_q, &ctx->b_sec_q};
   for (DevBuf* b : all) release(*b);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
@@ -343,11 +342,16 @@ int vm_set_frame(vm_ctx* ctx, const vm_frame* frame) {
   return VM_OK;
 }
 
-int vm_set_tuning(vm_ctx* ctx, int tile_variant, int ctas_per_sm) {
-  if (!ctx || tile_variant < 0 || tile_variant >= vmk::FUSED_VARIANTS || ctas_per_sm < 0) return VM_E_INVALID;
-  if (tile_variant != ctx->variant || ctas_per_sm != ctx->ctas_per_sm) drop_graph(ctx);
-  ctx->variant = tile_variant;
-  ctx->ctas_per_sm = ctas_per_sm;
+int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_sm) {
+  if (!ctx) return VM_E_INVALID;
+  if (!(warps_per_block == 4 || warps_per_block == 8) || reg_level < 0 || reg_level > 2 || ctas_per_sm < 0)
+    return fail(ctx, VM_E_INVALID, "warps per block must be 4 or 8, register level 0..2, CTAs per SM >= 0");
+  if (warps_per_block != ctx->tuning.primary_warps || reg_level != ctx->tuning.reg_level ||
+      ctas_per_sm != ctx->tuning.ctas_per_sm)
+    drop_graph(ctx);
+  ctx->tuning.primary_warps = warps_per_block;
+  ctx->tuning.reg_level = reg_level;
+  ctx->tuning.ctas_per_sm = ctas_per_sm;
   return VM_OK;
 }
 
@@ -426,14 +430,22 @@ int vm_render_counted(vm_ctx* ctx, vm_traffic* out) {
   int rc = check_ready(ctx);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
-  CK(cudaMemsetAsync(ctx->traffic.p, 0, sizeof(vmk::Traffic64), ctx->stream));
+  CK(cudaMemsetAsync(ctx->traffic.p, 0, 3 * sizeof(vmk::Traffic64), ctx->stream));
   if ((rc = enqueue_render(ctx, true))) return rc;
-  vmk::Traffic64 t;
-  CK(cudaMemcpyAsync(&t, ctx->traffic.p, sizeof t, cudaMemcpyDeviceToHost, ctx->stream));
+  vmk::Traffic64 st[3];
+  CK(cudaMemcpyAsync(st, ctx->traffic.p, sizeof st, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  out->chunk_records = t.chunk; out->l1_fetches = t.l1; out->leaf_fetches = t.leaf; out->attr_fetches = t.attr;
-  out->palette_decodes = t.pal; out->grid_lookups = t.grid; out->iters = t.iters;
-  out->rays_primary = t.rays_primary; out->rays_shadow = t.rays_shadow; out->rays_secondary = t.rays_secondary;
+  memset(out, 0, sizeof *out);
+  for (const vmk::Traffic64& t : st) {
+    out->chunk_records += t.chunk; out->l1_fetches += t.l1; out->leaf_fetches += t.leaf; out->attr_fetches += t.attr;
+    out->palette_decodes += t.pal; out->grid_lookups += t.grid; out->iters += t.iters;
+    out->rays_primary += t.rays_primary; out->rays_shadow += t.rays_shadow; out->rays_secondary += t.rays_secondary;
+    out->list_entries += t.entries;
+  }
+  for (int s = 0; s < 3; ++s) {
+    out->stage_iters[s] = st[s].iters;
+    out->stage_chunks[s] = st[s].chunk;
+  }
   return VM_OK;
 }
 
@@ -519,34 +531,6 @@ int vm_stats_read(vm_ctx* ctx, vm_stats* out) {
 // ---------------------------------------------------------------------------
 // batches
 // ---------------------------------------------------------------------------
-static int batch_layout(vm_ctx* ctx) {
-  // work items depend on the tile variant: rebuild descriptors when it changes
-  if (ctx->b_layout_variant == ctx->variant) return VM_OK;
-  uint32_t tw, th;
-  vmk::fused_dims(ctx->variant, &tw, &th);
-  std::vector<ViewDesc> single(ctx->b_n_views);
-  uint32_t tile = 0;
-  for (uint32_t v = 0; v < ctx->b_n_views; ++v) {
-    ViewDesc& d = ctx->bh_views[v];
-    const vm_frame& f = ctx->bh_frames[v];
-    d.tile_begin = tile;
-    d.tiles_x = (f.res[0] + tw - 1) / tw;
-    d.tiles_y = (f.res[1] + th - 1) / th;
-    tile += d.tiles_x * d.tiles_y;
-    single[v] = d;
-    single[v].tile_begin = 0;
-  }
-  ctx->b_total_tiles = tile;
-  CK(cudaMemcpyAsync(ctx->b_views.p, ctx->bh_views.data(), ctx->b_n_views * sizeof(ViewDesc), cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(cudaMemcpyAsync(ctx->b_views1.p, single.data(), ctx->b_n_views * sizeof(ViewDesc), cudaMemcpyHostToDevice,
-                     ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  ctx->b_layout_variant = ctx->variant;
-  drop_graph(ctx);
-  return VM_OK;
-}
-
 int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm_chunk* chunks,
                  const uint32_t* chunk_counts, const uint32_t* grids, const uint32_t* grid_lens) {
   if (!ctx || n_views == 0 || !frames || !chunks || !chunk_counts || !grids || !grid_lens) return VM_E_INVALID;
@@ -556,7 +540,9 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
   CK(cudaSetDevice(ctx->device));
   ctx->bh_frames.assign(frames, frames + n_views);
   ctx->bh_views.assign(n_views, ViewDesc{});
-  uint64_t chunk_total = 0, grid_total = 0, pix = 0, hiz_total = 0;
+  std::vector<ViewDesc> single(n_views);
+  uint64_t chunk_total = 0, grid_total = 0, pix = 0, tiles = 0;
+  uint32_t max_vis = 1;
   const bool uw = (frames[0].flags & VM_FLAG_UNDERWATER) != 0u;
   for (uint32_t v = 0; v < n_views; ++v) {
     const vm_frame& f = frames[v];
@@ -570,14 +556,21 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
     d.grid_off = grid_total;
     d.grid_len = grid_lens[v];
     d.pix_off = pix;
-    d.hiz_off = (uint32_t)hiz_total;
+    d.tile_begin = (uint32_t)tiles;
+    d.tiles_x = f.tiles[0];
+    d.tiles_y = f.tiles[1];
+    single[v] = d;
+    single[v].tile_begin = 0;   // per-view launches index their own tile scratch from 0
     chunk_total += chunk_counts[v];
     grid_total += grid_lens[v];
     pix += (uint64_t)f.res[0] * f.res[1];
-    hiz_total += (uint64_t)f.tiles[0] * f.tiles[1];
+    tiles += (uint64_t)f.tiles[0] * f.tiles[1];
+    max_vis = std::max(max_vis, std::min(f.chunk_count, chunk_counts[v]));
   }
   if (ctx->caps.max_batch_pixels && pix > ctx->caps.max_batch_pixels)
     return fail(ctx, VM_E_INVALID, "batch of %llu pixels exceeds the context capacity", (unsigned long long)pix);
+  if (tiles > 0xFFFFFFFFull) return fail(ctx, VM_E_INVALID, "too many tiles in one batch");
+  const uint32_t cap = std::min(max_vis, LIST_CAP_MAX);
   int rc = 0;
   rc |= ensure(ctx, ctx->b_frames, n_views * sizeof(vm_frame));
   rc |= ensure(ctx, ctx->b_views, n_views * sizeof(ViewDesc));
@@ -588,71 +581,69 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
   rc |= ensure(ctx, ctx->b_shadow, pix * 4);
   rc |= ensure(ctx, ctx->b_seck, pix * 8);
   rc |= ensure(ctx, ctx->b_sect, pix * 4);
-  rc |= ensure(ctx, ctx->b_hiz, hiz_total * 4);
+  rc |= ensure(ctx, ctx->b_hiz, tiles * 4);
   rc |= ensure(ctx, ctx->b_dkmax, std::max<uint64_t>(chunk_total, 1) * 4);
   rc |= ensure(ctx, ctx->b_sufmax, std::max<uint64_t>(chunk_total, 1) * 4);
+  rc |= ensure(ctx, ctx->b_tile_list, tiles * cap * 2);
+  rc |= ensure(ctx, ctx->b_tile_count, tiles * 4);
+  rc |= ensure(ctx, ctx->b_shadow_q, pix * sizeof(vmk::ShadowItem));
+  rc |= ensure(ctx, ctx->b_sec_q, pix * sizeof(vmk::SecItem));
   if (rc) return VM_E_CUDA;
   CK(cudaMemcpyAsync(ctx->b_frames.p, frames, n_views * sizeof(vm_frame), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->b_chunks.p, chunks, chunk_total * sizeof(vm_chunk), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->b_grids.p, grids, grid_total * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->b_views.p, ctx->bh_views.data(), n_views * sizeof(ViewDesc), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(ctx->b_views1.p, single.data(), n_views * sizeof(ViewDesc), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->b_n_views = n_views;
   ctx->b_pixels = pix;
   ctx->b_n_chunks = (uint32_t)chunk_total;
   ctx->b_grid_total = grid_total;
-  ctx->b_hiz_total = hiz_total;
+  ctx->b_total_tiles = (uint32_t)tiles;
+  ctx->b_list_cap = cap;
   ctx->b_underwater = uw;
-  ctx->b_layout_variant = -1;
   drop_graph(ctx);
-  return batch_layout(ctx);
+  return VM_OK;
 }
 
-static FusedArgs batch_args(vm_ctx* ctx) {
-  FusedArgs a = base_args(ctx);
+static vmk::PipeArgs batch_args(vm_ctx* ctx) {
+  vmk::PipeArgs a = base_args(ctx);
   a.frames = (const vm_frame*)ctx->b_frames.p;
   a.views = (const ViewDesc*)ctx->b_views.p;
   a.n_views = ctx->b_n_views;
   a.total_tiles = ctx->b_total_tiles;
   a.chunks = (const vm_chunk*)ctx->b_chunks.p;
   a.grids = (const uint32_t*)ctx->b_grids.p;
-  a.dkmax = (const uint32_t*)ctx->b_dkmax.p;
-  a.sufmax = (const uint32_t*)ctx->b_sufmax.p;
+  a.dkmax = (uint32_t*)ctx->b_dkmax.p;
+  a.sufmax = (uint32_t*)ctx->b_sufmax.p;
+  a.tile_list = (uint16_t*)ctx->b_tile_list.p;
+  a.tile_count = (uint32_t*)ctx->b_tile_count.p;
+  a.list_cap = ctx->b_list_cap;
   a.vis = (unsigned long long*)ctx->b_vis.p;
   a.shadow = (float*)ctx->b_shadow.p;
   a.sec_key = (unsigned long long*)ctx->b_seck.p;
   a.sec_t = (float*)ctx->b_sect.p;
   a.hiz = (uint32_t*)ctx->b_hiz.p;
-  a.traffic = (vmk::Traffic64*)ctx->traffic.p;
-  a.do_shadow = 1;
-  a.do_secondary = 0;
+  a.shadow_q = (vmk::ShadowItem*)ctx->b_shadow_q.p;
+  a.sec_q = (vmk::SecItem*)ctx->b_sec_q.p;
+  a.do_secondary = 0;   // batched views: primary + shadow
   return a;
-}
-
-static int enqueue_batch_persistent(vm_ctx* ctx) {
-  FusedArgs a = batch_args(ctx);
-  vm_frame dummy_f{};
-  ViewDesc dummy_v{};
-  CK(vmk::launch_chunk_bounds(a.frames, a.views, a.n_views, dummy_f, dummy_v, a.chunks, (uint32_t*)a.dkmax,
-                              (uint32_t*)a.sufmax, ctx->stream));
-  CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(uint32_t), ctx->stream));
-  CK(vmk::launch_fused(a, ctx->variant, ctx->b_underwater, false,
-                       fused_grid(ctx, ctx->variant, ctx->b_underwater, false, a.total_tiles), ctx->stream));
-  return VM_OK;
 }
 
 int vm_batch_run(vm_ctx* ctx, int mode) {
   if (!ctx) return VM_E_INVALID;
   if (ctx->b_n_views == 0) return fail(ctx, VM_E_NOT_READY, "no batch set");
   CK(cudaSetDevice(ctx->device));
-  int rc = batch_layout(ctx);
-  if (rc) return rc;
   if (mode == 0) {
+    // every view in one pipeline: one launch per stage, replayed from a graph
     if (!ctx->graph_exec) {
       CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-      rc = enqueue_batch_persistent(ctx);
+      const vmk::PipeArgs a = batch_args(ctx);
+      const cudaError_t le = vmk::launch_pipeline(a, ctx->tuning, ctx->b_underwater, false, ctx->sms, ctx->stream);
       cudaGraph_t g = nullptr;
-      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      if (le != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(ctx, le, "launch_pipeline"); }
       if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
       ctx->graph = g;
       CK(cudaGraphInstantiate(&ctx->graph_exec, g, 0));
@@ -661,22 +652,17 @@ int vm_batch_run(vm_ctx* ctx, int mode) {
     return VM_OK;
   }
   if (mode == 1) {
-    // one launch sequence per view: bounds + counter reset + fused kernel
-    FusedArgs base = batch_args(ctx);
+    // the baseline: one launch sequence per view (same kernels)
+    const vmk::PipeArgs base = batch_args(ctx);
     for (uint32_t v = 0; v < ctx->b_n_views; ++v) {
-      FusedArgs a = base;
+      vmk::PipeArgs a = base;
       const ViewDesc& d = ctx->bh_views[v];
       a.frames = (const vm_frame*)ctx->b_frames.p + v;
       a.views = (const ViewDesc*)ctx->b_views1.p + v;
       a.n_views = 1;
       a.total_tiles = d.tiles_x * d.tiles_y;
-      vm_frame dummy_f{};
-      ViewDesc dummy_v{};
-      CK(vmk::launch_chunk_bounds(a.frames, a.views, 1, dummy_f, dummy_v, a.chunks, (uint32_t*)a.dkmax,
-                                  (uint32_t*)a.sufmax, ctx->stream));
-      CK(cudaMemsetAsync(ctx->work.p, 0, sizeof(uint32_t), ctx->stream));
-      CK(vmk::launch_fused(a, ctx->variant, ctx->b_underwater, false,
-                           fused_grid(ctx, ctx->variant, ctx->b_underwater, false, a.total_tiles), ctx->stream));
+      a.hiz = (uint32_t*)ctx->b_hiz.p + d.tile_begin;
+      CK(vmk::launch_pipeline(a, ctx->tuning, ctx->b_underwater, false, ctx->sms, ctx->stream));
     }
     return VM_OK;
   }

@@ -17,104 +17,11 @@
 //    key is below the pixel's current key, so the result equals the pair
 //    sequence's atomicMax fold bit for bit.
 #include "kernels.cuh"
-#include <cub/block/block_scan.cuh>
+#include "ray_stages.cuh"
 #include <algorithm>
 
 namespace vmk {
 using namespace vmd;
-
-#define FULLMASK 0xFFFFFFFFu
-
-__device__ __forceinline__ uint32_t lanemask_lt() {
-  uint32_t m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-__device__ __forceinline__ bool shadow_active(const vm_frame& f) {   // shadow.wgsl:31-33
-  return (f.flags & VM_FLAG_SHADOWS) != 0u && (f.flags & VM_FLAG_HEATMAP) == 0u && f.daylight > 0.01f;
-}
-
-struct KeyParts { uint32_t ci, vx, vy, vz, mx, my, mz, nid; };
-__device__ __forceinline__ KeyParts split_key(unsigned long long key) {
-  KeyParts k;
-  const uint32_t low = (uint32_t)(key & 0xFFFFFFull);
-  k.ci = (uint32_t)(key >> 24) & 0x1FFFu;
-  k.vx = (low >> 16) & 63u; k.vy = (low >> 8) & 63u; k.vz = low & 63u;
-  k.mx = (low >> 22) & 3u; k.my = (low >> 14) & 3u; k.mz = (low >> 6) & 3u;
-  k.nid = (uint32_t)(key >> 37) & 7u;
-  return k;
-}
-
-// shadow_guide (shadow.wgsl:8-30): the sun ray's origin for a visible pixel,
-// or false when the pixel casts no shadow ray.
-__device__ __forceinline__ bool shadow_setup(const DevWorld& w, const vm_frame& f, unsigned long long key,
-                                             uint32_t px, uint32_t py, F3* origin) {
-  if (key == 0ull) return false;
-  const KeyParts k = split_key(key);
-  const Chunk c = ld_chunk(w, k.ci);
-  const uint32_t id = block_at(w, c, k.vx, k.vy, k.vz);
-  if (id == VM_WATER || id == VM_GLASS) return false;
-  const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
-  F3 n = normal_of(k.nid);
-  if (k.nid >= VM_NORMAL_CROSS_A && dot(n, rd) > 0.0f) n = neg(n);
-  if (dot(n, ld3(f.sun_dir)) <= 0.0f) return false;
-  const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
-  if (!(t >= 0.0f)) return false;
-  const F3 hit = ld3(f.cam_pos) + rd * t;
-  *origin = hit + n * (0.02f * c.vs);
-  return true;
-}
-
-__device__ __forceinline__ float blocker_distance(float blocker) {   // shadow.wgsl:44
-  return blocker >= 0.0f ? fminf(fmaxf(blocker, 0.001f), 65504.0f) : 0.0f;
-}
-
-// The one secondary ray of a water or glass hit:
-//   water: water_refract_leg (resolve.wgsl:1029-1042), gated by
-//          FLAG_WATER_REFRACT and refract_detail > 0 (resolve.wgsl:1098,1524);
-//   glass: shade_glass's straight transmission (resolve.wgsl:1276-1280).
-struct SecRay { F3 o, d; float max_dist; bool water; };
-__device__ __forceinline__ bool secondary_setup(const DevWorld& w, const vm_frame& f, unsigned long long key,
-                                                uint32_t px, uint32_t py, SecRay* s) {
-  if (key == 0ull) return false;
-  const KeyParts k = split_key(key);
-  const Chunk c = ld_chunk(w, k.ci);
-  const uint32_t id = block_at(w, c, k.vx, k.vy, k.vz);
-  const bool water = id == VM_WATER, glass = id == VM_GLASS;
-  if (!water && !glass) return false;
-  const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
-  const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
-  const F3 hit = ld3(f.cam_pos) + rd * t;
-  if (water) {
-    const float detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, t);
-    if (!((f.flags & VM_FLAG_WATER_REFRACT) != 0u && detail > 0.0f)) return false;
-    const F3 rdir = refract(rd, normal_of(k.nid), 1.0f / VM_WATER_IOR);
-    s->o = hit + rdir * VM_SURFACE_EPS;
-    s->d = rdir;
-    s->max_dist = VM_WATER_REFRACT_DIST;
-    s->water = true;
-  } else {
-    s->o = hit + rd * VM_SURFACE_EPS;
-    s->d = rd;
-    s->max_dist = fmaxf(VM_GLASS_TRANSMIT_DIST, f.far_);
-    s->water = false;
-  }
-  return true;
-}
-
-template <bool COUNT>
-__device__ __forceinline__ void secondary_trace(const DevWorld& w, const vm_frame& f, const SecRay& s,
-                                                unsigned long long* out_key, float* out_t, Traffic* tr) {
-  const WorldHit h = s.water ? trace_world<true, COUNT>(w, f, s.o, s.d, s.max_dist, tr)
-                             : trace_world<false, COUNT>(w, f, s.o, s.d, s.max_dist, tr);
-  unsigned long long k = (1ull << 63) | (s.water ? 0ull : (1ull << 61));
-  if (h.hit)
-    k |= (1ull << 62) | ((unsigned long long)h.normal << 37) | ((unsigned long long)h.ci << 24) |
-         (unsigned long long)((h.vx << 16) | (h.vy << 8) | h.vz);
-  *out_key = k;
-  *out_t = h.t;
-}
 
 // ---------------------------------------------------------------------------
 // The engine's pass sequence
@@ -295,289 +202,6 @@ __global__ void __launch_bounds__(256) k_expand(const vm_frame f, const DevWorld
   }
 }
 
-// Per view: the largest depth key any hit in chunk ci can produce (from a
-// lower bound on its hit distance) and its suffix maximum over the view's
-// front-to-back chunk list.  The lower bound allows 1e-5 relative and 0.05
-// voxel absolute rounding slack between the box distance and a march's t.
-struct MaxOp {
-  __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
-};
-
-__global__ void __launch_bounds__(1024) k_chunk_bounds(const vm_frame* __restrict__ frames, const ViewDesc* __restrict__ views,
-                                                       const vm_frame f0, const ViewDesc v0,
-                                                       const vm_chunk* __restrict__ chunks, uint32_t* __restrict__ dkmax,
-                                                       uint32_t* __restrict__ sufmax) {
-  typedef cub::BlockScan<uint32_t, 1024> Scan;
-  __shared__ typename Scan::TempStorage tmp;
-  const uint32_t v = blockIdx.x;
-  const vm_frame& f = frames ? frames[v] : f0;
-  const ViewDesc vd = frames ? views[v] : v0;
-  const uint32_t n = min(f.chunk_count, vd.n_chunks);
-  const F3 cam = ld3(f.cam_pos);
-  const uint32_t per = (n + 1023u) / 1024u;
-  // thread t owns [t*per, t*per+per) in reverse order so that a forward
-  // inclusive max-scan over threads gives the suffix maximum
-  const uint32_t t = 1023u - threadIdx.x;
-  uint32_t local = 0u;
-  for (uint32_t k = 0; k < per; ++k) {
-    const uint32_t ci = t * per + k;
-    if (ci < n) {
-      const vm_chunk& c = chunks[vd.chunk_off + ci];
-      const float dmin = box_distance(cam, ld3(c.aabb_min), ld3(c.aabb_max));
-      const float lb = fmaxf(dmin * (1.0f - 1e-5f) - 0.05f * c.voxel_size, 0.0f);
-      const uint32_t dk = depth_key(f, lb);
-      dkmax[vd.chunk_off + ci] = dk;
-      local = max(local, dk);
-    }
-  }
-  uint32_t excl;
-  Scan(tmp).ExclusiveScan(local, excl, 0u, MaxOp());
-  uint32_t run = excl;   // max over all chunks after this thread's range
-  for (int k = (int)per - 1; k >= 0; --k) {
-    const uint32_t ci = t * per + (uint32_t)k;
-    if (ci < n) {
-      run = max(run, dkmax[vd.chunk_off + ci]);
-      sufmax[vd.chunk_off + ci] = run;
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Fused persistent kernel
-// ---------------------------------------------------------------------------
-constexpr uint32_t LIST_CAP = 1024;
-
-template <int TW, int TH, bool UNDERWATER, bool COUNT>
-__global__ void __launch_bounds__(TW* TH) k_fused(const FusedArgs a) {
-  constexpr uint32_t NT = TW * TH;
-  constexpr uint32_t NSUB = NT / 64;
-  constexpr uint32_t SUBX = TW / 8;
-  constexpr uint32_t NWARP = NT / 32;
-  __shared__ __align__(16) vm_frame s_f;
-  __shared__ ViewDesc s_v;
-  __shared__ uint32_t s_item, s_view, s_subvalid;
-  __shared__ float s_pl[NSUB][13];
-  __shared__ uint32_t s_ci[LIST_CAP], s_dk[LIST_CAP], s_suf[LIST_CAP];
-  __shared__ uint32_t s_wc[NWARP];
-  __shared__ uint32_t s_q[NT];
-  __shared__ float s_qo[NT][3];
-  __shared__ uint32_t s_hz[NWARP];
-
-  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
-  const uint32_t sub = tid >> 6;
-  Traffic tr = {0, 0, 0, 0, 0, 0, 0};
-  uint32_t n_pri = 0, n_sh = 0, n_sec = 0;
-  uint32_t cur_view = 0xFFFFFFFFu;
-
-  for (;;) {
-    if (tid == 0) {
-      const uint32_t item = atomicAdd(a.work, 1u);
-      s_item = item;
-      if (item < a.total_tiles && a.frames == nullptr) {
-        s_view = 0;
-      } else if (item < a.total_tiles) {
-        uint32_t lo = 0, hi = a.n_views - 1;
-        while (lo < hi) {
-          const uint32_t mid = (lo + hi + 1) >> 1;
-          if (a.views[mid].tile_begin <= item) lo = mid; else hi = mid - 1;
-        }
-        s_view = lo;
-      }
-    }
-    __syncthreads();
-    const uint32_t item = s_item;
-    if (item >= a.total_tiles) break;
-    if (s_view != cur_view) {
-      cur_view = s_view;
-      const uint32_t* src = a.frames ? reinterpret_cast<const uint32_t*>(a.frames + cur_view)
-                                     : reinterpret_cast<const uint32_t*>(&a.frame0);
-      for (uint32_t i = tid; i < sizeof(vm_frame) / 4; i += NT) reinterpret_cast<uint32_t*>(&s_f)[i] = src[i];
-      const uint32_t* vsrc = a.frames ? reinterpret_cast<const uint32_t*>(a.views + cur_view)
-                                      : reinterpret_cast<const uint32_t*>(&a.view0);
-      if (tid < sizeof(ViewDesc) / 4) reinterpret_cast<uint32_t*>(&s_v)[tid] = vsrc[tid];
-      __syncthreads();
-    }
-    const vm_frame& f = s_f;
-    const DevWorld w = {a.chunks + s_v.chunk_off, s_v.n_chunks, a.inners, a.n_inners, a.leaves, a.n_leaves,
-                        a.bricks, a.n_bricks, a.grids + s_v.grid_off, s_v.grid_len, a.err};
-    const uint32_t local = item - s_v.tile_begin;
-    const uint32_t x0 = (local % s_v.tiles_x) * TW, y0 = (local / s_v.tiles_x) * TH;
-    const uint32_t px = x0 + (sub % SUBX) * 8u + (tid & 7u), py = y0 + (sub / SUBX) * 8u + ((tid >> 3) & 7u);
-    const bool valid = px < f.res[0] && py < f.res[1];
-
-    if (tid < NSUB) {
-      const uint32_t sx0 = x0 + (tid % SUBX) * 8u, sy0 = y0 + (tid / SUBX) * 8u;
-      const bool sv = sx0 < f.res[0] && sy0 < f.res[1];
-      const TilePlanes tp = tile_planes(f, sx0, sy0);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) { s_pl[tid][3 * i] = tp.n[i].x; s_pl[tid][3 * i + 1] = tp.n[i].y; s_pl[tid][3 * i + 2] = tp.n[i].z; }
-      s_pl[tid][12] = tp.reach;
-      const uint32_t bits = __ballot_sync(NSUB >= 32 ? FULLMASK : ((1u << NSUB) - 1u), sv);
-      if (tid == 0) s_subvalid = bits;
-    }
-    __syncthreads();
-
-    const F3 cam = ld3(f.cam_pos), fwd = ld3(f.cam_fwd);
-    const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
-    const Ray ray = make_ray(cam, rd);
-    const uint32_t n_vis = min(f.chunk_count, s_v.n_chunks);
-    const uint32_t my_bit = 1u << sub;
-    unsigned long long best = 0ull;
-    uint32_t scan = 0;
-    for (;;) {
-      uint32_t list_n = 0;
-      while (scan < n_vis && list_n + NT <= LIST_CAP) {
-        const uint32_t ci = scan + tid;
-        uint32_t mask = 0u;
-        if (ci < n_vis) {
-          if (ci == f.camera_chunk) {
-            mask = s_subvalid;
-          } else {
-            const float* cp = reinterpret_cast<const float*>(w.chunks + ci);
-            const F3 bmin = {__ldg(cp + 0), __ldg(cp + 1), __ldg(cp + 2)};
-            const F3 bmax = {__ldg(cp + 4), __ldg(cp + 5), __ldg(cp + 6)};
-            if (!box_outside(bmin, bmax, fwd, cam)) {
-              const float dmin = box_distance(cam, bmin, bmax);
-#pragma unroll
-              for (uint32_t s = 0; s < NSUB; ++s) {
-                if (!((s_subvalid >> s) & 1u)) continue;
-                const float* pl = s_pl[s];
-                const bool out = box_outside(bmin, bmax, f3(pl[0], pl[1], pl[2]), cam) ||
-                                 box_outside(bmin, bmax, f3(pl[3], pl[4], pl[5]), cam) ||
-                                 box_outside(bmin, bmax, f3(pl[6], pl[7], pl[8]), cam) ||
-                                 box_outside(bmin, bmax, f3(pl[9], pl[10], pl[11]), cam);
-                if (!out && dmin < pl[12]) mask |= 1u << s;
-              }
-            }
-          }
-        }
-        const uint32_t bal = __ballot_sync(FULLMASK, mask != 0u);
-        if (lane == 0) s_wc[warp] = __popc(bal);
-        __syncthreads();
-        uint32_t off = list_n, total = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < NWARP; ++k) {
-          const uint32_t c = s_wc[k];
-          off += k < warp ? c : 0u;
-          total += c;
-        }
-        if (mask) {
-          const uint32_t pos = off + __popc(bal & lanemask_lt());
-          s_ci[pos] = ci | (mask << 16);
-          s_dk[pos] = a.dkmax[s_v.chunk_off + ci];
-          s_suf[pos] = a.sufmax[s_v.chunk_off + ci];
-        }
-        list_n += total;
-        scan += NT;
-        __syncthreads();
-      }
-      if (valid) {
-        for (uint32_t i = 0; i < list_n; ++i) {
-          const uint32_t e = s_ci[i];
-          if (!((e >> 16) & my_bit)) continue;
-          const uint32_t bestd = (uint32_t)(best >> 40);
-          if (s_suf[i] < bestd) break;
-          if (s_dk[i] < bestd) continue;
-          const uint32_t ci = e & 0xFFFFu;
-          const Chunk c = ld_chunk(w, ci);
-          if (ray_skips(f, c.fade, px, py)) continue;
-          const Hit h = march_chunk<UNDERWATER, false, false, COUNT>(w, f, c, ray, f.far_, &tr);
-          if (h.hit) {
-            const unsigned long long k = make_key(f, h, ci);
-            best = k > best ? k : best;
-          }
-        }
-      }
-      if (scan >= n_vis) break;
-      const uint32_t rem = a.sufmax[s_v.chunk_off + scan];
-      if (__syncthreads_and(!valid || rem < (uint32_t)(best >> 40))) break;
-    }
-    if (COUNT && valid) ++n_pri;
-    const uint64_t pix = s_v.pix_off + (uint64_t)py * f.res[0] + px;
-    if (valid) a.vis[pix] = best;
-
-    // Hi-Z of the final visibility per 8x8 tile (build_hiz's reduction)
-    {
-      uint32_t d = valid ? (uint32_t)(best >> 40) : 0u;
-      d = __reduce_min_sync(FULLMASK, d);
-      if (lane == 0) s_hz[warp] = d;
-    }
-
-    // shadow rays from a compacted queue
-    F3 so = {0.0f, 0.0f, 0.0f};
-    const bool want_sh = a.do_shadow && valid && shadow_active(f) && shadow_setup(w, f, best, px, py, &so);
-    {
-      const uint32_t bal = __ballot_sync(FULLMASK, want_sh);
-      if (lane == 0) s_wc[warp] = __popc(bal);
-      __syncthreads();
-      if (tid < NSUB && ((s_subvalid >> tid) & 1u)) {
-        const uint32_t sx0 = x0 + (tid % SUBX) * 8u, sy0 = y0 + (tid / SUBX) * 8u;
-        a.hiz[s_v.hiz_off + (sy0 / 8u) * f.tiles[0] + sx0 / 8u] = min(s_hz[2 * tid], s_hz[2 * tid + 1]);
-      }
-      uint32_t off = 0, total = 0;
-#pragma unroll
-      for (uint32_t k = 0; k < NWARP; ++k) { const uint32_t c = s_wc[k]; off += k < warp ? c : 0u; total += c; }
-      if (want_sh) {
-        const uint32_t pos = off + __popc(bal & lanemask_lt());
-        s_q[pos] = tid;
-        s_qo[pos][0] = so.x; s_qo[pos][1] = so.y; s_qo[pos][2] = so.z;
-      }
-      if (a.do_shadow && valid && !want_sh) a.shadow[pix] = 0.0f;
-      __syncthreads();
-      for (uint32_t k = tid; k < total; k += NT) {
-        const uint32_t lt = s_q[k];
-        const uint32_t qsub = lt >> 6;
-        const uint32_t qx = x0 + (qsub % SUBX) * 8u + (lt & 7u), qy = y0 + (qsub / SUBX) * 8u + ((lt >> 3) & 7u);
-        const float b = shadow_ray_t<COUNT>(w, f, f3(s_qo[k][0], s_qo[k][1], s_qo[k][2]), ld3(f.sun_dir), f.shadow_dist, &tr);
-        a.shadow[s_v.pix_off + (uint64_t)qy * f.res[0] + qx] = blocker_distance(b);
-        if (COUNT) ++n_sh;
-      }
-      __syncthreads();
-    }
-
-    // water / glass secondary rays from a compacted queue
-    if (a.do_secondary) {
-      SecRay sr;
-      const bool want = valid && secondary_setup(w, f, best, px, py, &sr);
-      const uint32_t bal = __ballot_sync(FULLMASK, want);
-      if (lane == 0) s_wc[warp] = __popc(bal);
-      __syncthreads();
-      uint32_t off = 0, total = 0;
-#pragma unroll
-      for (uint32_t k = 0; k < NWARP; ++k) { const uint32_t c = s_wc[k]; off += k < warp ? c : 0u; total += c; }
-      if (want) s_q[off + __popc(bal & lanemask_lt())] = tid;
-      if (valid && !want) { a.sec_key[pix] = 0ull; a.sec_t[pix] = 0.0f; }
-      __syncthreads();
-      for (uint32_t k = tid; k < total; k += NT) {
-        const uint32_t lt = s_q[k];
-        const uint32_t qsub = lt >> 6;
-        const uint32_t qx = x0 + (qsub % SUBX) * 8u + (lt & 7u), qy = y0 + (qsub / SUBX) * 8u + ((lt >> 3) & 7u);
-        const uint64_t qpix = s_v.pix_off + (uint64_t)qy * f.res[0] + qx;
-        SecRay q;
-        secondary_setup(w, f, a.vis[qpix], qx, qy, &q);
-        unsigned long long sk; float st;
-        secondary_trace<COUNT>(w, f, q, &sk, &st, &tr);
-        a.sec_key[qpix] = sk;
-        a.sec_t[qpix] = st;
-        if (COUNT) ++n_sec;
-      }
-      __syncthreads();
-    }
-  }
-  if (COUNT) {
-    atomicAdd(&a.traffic->chunk, (unsigned long long)tr.chunk);
-    atomicAdd(&a.traffic->l1, (unsigned long long)tr.l1);
-    atomicAdd(&a.traffic->leaf, (unsigned long long)tr.leaf);
-    atomicAdd(&a.traffic->attr, (unsigned long long)tr.attr);
-    atomicAdd(&a.traffic->pal, (unsigned long long)tr.pal);
-    atomicAdd(&a.traffic->grid, (unsigned long long)tr.grid);
-    atomicAdd(&a.traffic->iters, (unsigned long long)tr.iters);
-    atomicAdd(&a.traffic->rays_primary, (unsigned long long)n_pri);
-    atomicAdd(&a.traffic->rays_shadow, (unsigned long long)n_sh);
-    atomicAdd(&a.traffic->rays_secondary, (unsigned long long)n_sec);
-  }
-}
-
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -639,60 +263,6 @@ cudaError_t launch_expand(const vm_frame& f, const DevWorld& w, const unsigned l
   const uint32_t grid = (uint32_t)std::min<uint64_t>((npix + 255) / 256, 148ull * 16);
   k_expand<<<grid, 256, 0, s>>>(f, w, vis, wx, wy, wz, dx, dy, dz, voxel, face, t);
   return cudaGetLastError();
-}
-
-cudaError_t launch_chunk_bounds(const vm_frame* frames, const ViewDesc* views, uint32_t n_views, const vm_frame& f0,
-                                const ViewDesc& v0, const vm_chunk* chunks, uint32_t* dkmax, uint32_t* sufmax,
-                                cudaStream_t s) {
-  if (n_views == 0) return cudaSuccess;
-  k_chunk_bounds<<<n_views, 1024, 0, s>>>(frames, views, f0, v0, chunks, dkmax, sufmax);
-  return cudaGetLastError();
-}
-
-template <int TW, int TH>
-static cudaError_t launch_fused_t(const FusedArgs& a, bool underwater, bool count, uint32_t grid, cudaStream_t s) {
-  if (underwater) {
-    if (count) k_fused<TW, TH, true, true><<<grid, TW * TH, 0, s>>>(a);
-    else k_fused<TW, TH, true, false><<<grid, TW * TH, 0, s>>>(a);
-  } else {
-    if (count) k_fused<TW, TH, false, true><<<grid, TW * TH, 0, s>>>(a);
-    else k_fused<TW, TH, false, false><<<grid, TW * TH, 0, s>>>(a);
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t launch_fused(const FusedArgs& a, int variant, bool underwater, bool count, uint32_t grid, cudaStream_t s) {
-  if (a.total_tiles == 0 || grid == 0) return cudaSuccess;
-  switch (variant) {
-    case FUSED_8x8: return launch_fused_t<8, 8>(a, underwater, count, grid, s);
-    case FUSED_16x8: return launch_fused_t<16, 8>(a, underwater, count, grid, s);
-    case FUSED_16x16: return launch_fused_t<16, 16>(a, underwater, count, grid, s);
-    case FUSED_32x16: return launch_fused_t<32, 16>(a, underwater, count, grid, s);
-  }
-  return cudaErrorInvalidValue;
-}
-
-template <int TW, int TH>
-static int occ_t(bool underwater, bool count) {
-  int n = 0;
-  if (underwater) {
-    if (count) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused<TW, TH, true, true>, TW * TH, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused<TW, TH, true, false>, TW * TH, 0);
-  } else {
-    if (count) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused<TW, TH, false, true>, TW * TH, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused<TW, TH, false, false>, TW * TH, 0);
-  }
-  return n;
-}
-
-int fused_max_ctas_per_sm(int variant, bool underwater, bool count) {
-  switch (variant) {
-    case FUSED_8x8: return occ_t<8, 8>(underwater, count);
-    case FUSED_16x8: return occ_t<16, 8>(underwater, count);
-    case FUSED_16x16: return occ_t<16, 16>(underwater, count);
-    case FUSED_32x16: return occ_t<32, 16>(underwater, count);
-  }
-  return 0;
 }
 
 }  // namespace vmk

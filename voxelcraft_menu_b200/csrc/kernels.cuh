@@ -7,57 +7,63 @@
 
 namespace vmk {
 
-// One view of a (possibly batched) fused launch.
+// One view of a (possibly batched) frame pipeline.  Views own consecutive
+// ranges of chunks, grid cells, 8x8 tiles and pixels in the batch buffers.
 struct ViewDesc {
   uint32_t chunk_off;     // first chunk of this view in the concatenated chunk list
   uint32_t n_chunks;      // chunks of this view (visible + shadow-only)
   uint64_t grid_off;      // first grid cell of this view
   uint32_t grid_len;
-  uint32_t tile_begin;    // first work item (fused tile) of this view
-  uint32_t tiles_x, tiles_y;   // fused tiles of this view
+  uint32_t tile_begin;    // first 8x8 tile of this view (also its hiz offset)
+  uint32_t tiles_x, tiles_y;   // 8x8 tiles of this view (the engine's tile grid)
   uint64_t pix_off;       // first pixel of this view in the output buffers
-  uint32_t hiz_off;       // first 8x8 tile of this view in the hiz buffer
-  uint32_t pad;
+  uint32_t pad[2];
 };
+static_assert(sizeof(ViewDesc) == 48, "ViewDesc layout");
 
 struct Traffic64 {
-  unsigned long long chunk, l1, leaf, attr, pal, grid, iters, rays_primary, rays_shadow, rays_secondary;
+  unsigned long long chunk, l1, leaf, attr, pal, grid, iters, rays_primary, rays_shadow, rays_secondary, entries;
 };
 
-struct FusedArgs {
-  const vm_frame* frames;      // one per view
+// Queued secondary work, written by the primary kernel and consumed densely.
+struct ShadowItem { uint32_t view, pix; float o[3]; uint32_t pad; };                 // 24 B
+struct SecItem { uint32_t view, pix; float o[3], d[3]; float max_dist; uint32_t water; };  // 40 B
+
+// Pipeline counters (zeroed before each frame)
+enum : int { W_PRIMARY = 0, W_SHADOW_N = 1, W_SEC_N = 2, W_WORDS = 4 };
+
+struct PipeArgs {
+  const vm_frame* frames;      // one per view; nullptr: single view in frame0 / view0
   const ViewDesc* views;
   uint32_t n_views;
-  uint32_t total_tiles;
+  uint32_t total_tiles;        // 8x8 tiles over all views
   const vm_chunk* chunks;      // concatenated per-view chunk lists
   const uint32_t* grids;       // concatenated per-view grids
   const uint4* inners; uint64_t n_inners;
   const uint2* leaves; uint64_t n_leaves;
   const uint32_t* bricks; uint64_t n_bricks;
-  const uint32_t* dkmax;       // per chunk (concatenated like chunks)
-  const uint32_t* sufmax;
+  uint32_t* dkmax;             // per chunk: best depth key a hit in it can have
+  uint32_t* sufmax;            // suffix maximum of dkmax over the view's list
+  uint16_t* tile_list;         // per 8x8 tile: culled chunk indices, ascending
+  uint32_t* tile_count;        // per 8x8 tile: list length (may exceed list_cap)
+  uint32_t list_cap;
   unsigned long long* vis;
   float* shadow;
   unsigned long long* sec_key;
   float* sec_t;
-  uint32_t* hiz;
-  uint32_t* work;              // work[0] = next tile counter (zeroed before launch)
+  uint32_t* hiz;               // per 8x8 tile: min depth key of the final visibility
+  ShadowItem* shadow_q;
+  SecItem* sec_q;
+  uint32_t* work;              // W_* counters
   uint32_t* err;
-  Traffic64* traffic;          // only with counting kernels
+  Traffic64* traffic;          // counting kernels only
   uint32_t do_shadow, do_secondary;
-  // single-view launches carry their frame and view in the parameter space
-  // (frames == nullptr), so no host->device copy is needed per frame
+  uint32_t px_per_lane;        // primary work item: 1 -> 8x4 pixels, 2 -> 8x8 pixels per warp
   vm_frame frame0;
   ViewDesc view0;
 };
 
-enum FusedVariant : int { FUSED_8x8 = 0, FUSED_16x8 = 1, FUSED_16x16 = 2, FUSED_32x16 = 3, FUSED_VARIANTS = 4 };
-inline void fused_dims(int v, uint32_t* tw, uint32_t* th) {
-  static const uint32_t W[] = {8, 16, 16, 32}, H[] = {8, 8, 16, 16};
-  *tw = W[v]; *th = H[v];
-}
-
-// launchers (return cudaError_t of the launch)
+// launchers of the engine's pass sequence (return cudaError_t of the launch)
 cudaError_t launch_tile_select(const vm_frame& f, const vmd::DevWorld& w, const uint32_t* hiz, uint32_t* pairs,
                                uint32_t* counters, cudaStream_t s);
 cudaError_t launch_finalize(const vm_frame& f, uint32_t* counters, bool recover, cudaStream_t s);
@@ -74,14 +80,16 @@ cudaError_t launch_secondary(const vm_frame& f, const vmd::DevWorld& w, const un
 cudaError_t launch_expand(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                           int32_t wx, int32_t wy, int32_t wz, uint32_t dx, uint32_t dy, uint32_t dz,
                           uint32_t* voxel, uint8_t* face, float* t, cudaStream_t s);
-// frames == nullptr: one view given by value (f0, v0)
-cudaError_t launch_chunk_bounds(const vm_frame* frames, const ViewDesc* views, uint32_t n_views,
-                                const vm_frame& f0, const ViewDesc& v0, const vm_chunk* chunks, uint32_t* dkmax,
-                                uint32_t* sufmax, cudaStream_t s);
-// underwater: the frame's FLAG_UNDERWATER (uniform over a launch; every view of
-// a batched launch must agree).  count: traffic-counting instantiation.
-cudaError_t launch_fused(const FusedArgs& a, int variant, bool underwater, bool count, uint32_t grid_ctas,
-                         cudaStream_t s);
-int fused_max_ctas_per_sm(int variant, bool underwater, bool count);
+
+// The wavefront frame pipeline (pipeline.cu): chunk bounds -> per-tile cull
+// -> primary march (+ queue shadow / secondary rays) -> shadow -> secondary.
+struct PipeTuning {
+  int primary_warps;     // warps per block of the primary kernel (4, 8)
+  int reg_level;         // register budget: 0 unconstrained, 1 ~80, 2 64 registers per thread
+  int ctas_per_sm;       // resident blocks per SM of the persistent primary kernel; 0 = occupancy max
+};
+cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwater, bool count, int sms,
+                            cudaStream_t s);
+int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count);
 
 }  // namespace vmk

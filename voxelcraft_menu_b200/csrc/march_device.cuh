@@ -86,6 +86,25 @@ __device__ __forceinline__ int32_t ffloor_i(float x) { return __float2int_rd(x);
 __device__ __forceinline__ int32_t fceil_i(float x) { return __float2int_ru(x); }
 __device__ __forceinline__ uint32_t popc(uint32_t x) { return __popc(x); }
 
+// x / d for the scales the march divides by.  Voxel sizes (1 << lod) and the
+// 64-voxel chunk edge are powers of two; for those, IEEE division and
+// multiplication by the exact reciprocal round the same real number x * 2^-k
+// and give identical results (subnormals included, as -ftz=false keeps them),
+// so the multiply replaces a multi-instruction correctly rounded divide.
+// Other divisors keep the division.
+struct Scale { float d, inv; bool pow2; };
+__device__ __forceinline__ Scale make_scale(float d) {
+  const uint32_t b = __float_as_uint(d);
+  const uint32_t e = (b >> 23) & 0xFFu;
+  Scale s;
+  s.d = d;
+  s.pow2 = (b & 0x807FFFFFu) == 0u && e >= 27u && e <= 227u;
+  s.inv = s.pow2 ? __uint_as_float((254u - e) << 23) : 0.0f;
+  return s;
+}
+__device__ __forceinline__ float sdiv(float x, const Scale& s) { return s.pow2 ? x * s.inv : x / s.d; }
+constexpr float INV64 = 1.0f / 64.0f;   // exact: dividing by 64 == multiplying by 2^-6
+
 __device__ __forceinline__ uint32_t cell_bit(uint32_t x, uint32_t y, uint32_t z) { return x | (y << 2) | (z << 4); }
 __device__ __forceinline__ bool mask_has(uint32_t lo, uint32_t hi, uint32_t bit) {
   return bit < 32u ? ((lo >> bit) & 1u) != 0u : ((hi >> (bit - 32u)) & 1u) != 0u;
@@ -207,13 +226,14 @@ __device__ __forceinline__ bool grid_rel(const vm_frame& f, int32_t cx, int32_t 
 // world_block_at: common.wgsl:266-277
 static __device__ __noinline__ uint32_t world_block_at(const DevWorld& w, const vm_frame& f, F3 p) {
   uint64_t gi;
-  if (!grid_rel(f, ffloor_i(p.x / 64.0f), ffloor_i(p.y / 64.0f), ffloor_i(p.z / 64.0f), &gi)) return 0u;
+  if (!grid_rel(f, ffloor_i(p.x * INV64), ffloor_i(p.y * INV64), ffloor_i(p.z * INV64), &gi)) return 0u;
   uint32_t ci = ld_grid(w, gi);
   if (ci == VM_NO_CHUNK) return 0u;
   Chunk c = ld_chunk(w, ci);
-  int32_t vx = ffloor_i((p.x - c.origin[0]) / c.vs);
-  int32_t vy = ffloor_i((p.y - c.origin[1]) / c.vs);
-  int32_t vz = ffloor_i((p.z - c.origin[2]) / c.vs);
+  const Scale s = make_scale(c.vs);
+  int32_t vx = ffloor_i(sdiv(p.x - c.origin[0], s));
+  int32_t vy = ffloor_i(sdiv(p.y - c.origin[1], s));
+  int32_t vz = ffloor_i(sdiv(p.z - c.origin[2], s));
   if (vx < 0 || vy < 0 || vz < 0 || vx >= 64 || vy >= 64 || vz >= 64) return 0u;
   if (!voxel_occupied(w, c, vx, vy, vz)) return 0u;
   return block_at(w, c, vx, vy, vz);
@@ -224,6 +244,7 @@ struct Hit {
   uint32_t vx, vy, vz;
   uint32_t mx, my, mz;
   uint32_t iters;
+  uint32_t id;    // block id of the hit voxel (march_chunk<..., WANT_ID = true> only)
 };
 
 __device__ __forceinline__ bool is_tuft(uint32_t b) { return b == VM_TALL_GRASS || b == VM_GRASS_TALL || b == VM_REEDS; }
@@ -244,9 +265,9 @@ __device__ __forceinline__ void micro_entry(uint32_t ux, uint32_t uy, uint32_t u
 
 // cutout_march: common.wgsl:537-577
 static __device__ __noinline__ bool cutout_march(int32_t wx, int32_t wy, int32_t wz, uint32_t ux, uint32_t uy, uint32_t uz,
-                                          F3 ro, F3 rd, float t_in, uint32_t axis_in, bool pdx, bool pdy, bool pdz,
-                                          bool snap, float* t_out, uint32_t* n_out, uint32_t* m_out) {
-  F3 inv = {1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
+                                          F3 ro, F3 rd, F3 inv, float t_in, uint32_t axis_in, bool pdx, bool pdy,
+                                          bool pdz, bool snap, float* t_out, uint32_t* n_out, uint32_t* m_out) {
+  // inv is the ray's 1 / rd, the value the WGSL recomputes here
   const float ms = 1.0f / 4.0f;
   uint32_t me[3];
   micro_entry(ux, uy, uz, ro, rd, t_in, axis_in, pdx, pdy, pdz, snap, me);
@@ -289,28 +310,34 @@ __device__ __forceinline__ Ray make_ray(F3 o, F3 d) {
 //   (skip_foliage only gates the tuft cross-quad trace, which this build does
 //   not have: tufts are transparent, as in the oracle).
 //   COUNT enables the per-ray traffic counters used by the roofline.
-struct Traffic { uint32_t chunk, l1, leaf, attr, pal, grid, iters; };
+struct Traffic { uint32_t chunk, l1, leaf, attr, pal, grid, iters, entries; };
 
-template <bool SKIP_WATER, bool SKIP_GLASS, bool SUN_RAY, bool COUNT>
+//   WANT_ID also returns the hit voxel's block id (block_at, common.wgsl:350),
+//   decoded from the L1 node and leaf slot the march already holds.
+template <bool SKIP_WATER, bool SKIP_GLASS, bool SUN_RAY, bool COUNT, bool WANT_ID = false>
 __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f, const Chunk& c, const Ray& r,
                                            float t_limit, Traffic* tr) {
   Hit h;
   h.hit = false; h.t = 0.0f; h.normal = 0u; h.vx = h.vy = h.vz = 0u; h.mx = h.my = h.mz = 0u; h.iters = 0u;
+  h.id = 0u;
   if (COUNT) tr->chunk++;
   const float vs = c.vs;
+  const Scale sv = make_scale(vs);
   const F3 origin = ld3(c.origin);
-  const F3 ro = (r.o - origin) / vs;
+  const F3 ro = {sdiv(r.o.x - origin.x, sv), sdiv(r.o.y - origin.y, sv), sdiv(r.o.z - origin.z, sv)};
   const F3 rd = r.d;
   const F3 inv = r.inv;
-  const F3 bmin = (ld3(c.aabb_min) - origin) / vs;
-  const F3 bmax = (ld3(c.aabb_max) - origin) / vs;
+  const F3 bmin = {sdiv(c.aabb_min[0] - origin.x, sv), sdiv(c.aabb_min[1] - origin.y, sv),
+                   sdiv(c.aabb_min[2] - origin.z, sv)};
+  const F3 bmax = {sdiv(c.aabb_max[0] - origin.x, sv), sdiv(c.aabb_max[1] - origin.y, sv),
+                   sdiv(c.aabb_max[2] - origin.z, sv)};
   const F3 t0 = (bmin - ro) * inv;
   const F3 t1 = (bmax - ro) * inv;
   const F3 tmin3 = {fminf(t0.x, t1.x), fminf(t0.y, t1.y), fminf(t0.z, t1.z)};
   const F3 tmax3 = {fmaxf(t0.x, t1.x), fmaxf(t0.y, t1.y), fmaxf(t0.z, t1.z)};
   const float t_enter = fmaxf(fmaxf(tmin3.x, tmin3.y), tmin3.z);
   const float t_exit = fminf(fminf(tmax3.x, tmax3.y), tmax3.z);
-  const float t_end = fminf(t_exit, t_limit / vs);
+  const float t_end = fminf(t_exit, sdiv(t_limit, sv));
   float t = fmaxf(t_enter, 0.0f);
   if (t >= t_end) return h;
   uint32_t axis;
@@ -423,14 +450,16 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
     } else {
       skip = block2_empty(trav_lo, trav_hi, l1b & 42u) ? 32 : 16;
     }
+    // block id of a solid voxel: the chunk's id when uniform, else decoded once
+    uint32_t id = c.attr_base;
+    bool id_known = attr_uniform;
     if (solid && any_filter) {
-      // block id of this voxel, decoded once for all filters below
-      uint32_t id = c.attr_base;
       const bool need_id = !attr_uniform && (noncaster_aware || water_interface || water_aware || glass_aware ||
                                              foliage_aware || cutout_aware);
       if (need_id) {
         if (COUNT && (attr & VM_UNIFORM_BIT) == 0u) tr->pal++;
         id = leaf_block(w, attr, ux, uy, uz);
+        id_known = true;
       }
       if (noncaster_aware && id == VM_GLOWSTONE) { solid = false; skip = 1; }
       if (solid && water_interface && id == VM_WATER) {
@@ -448,10 +477,11 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
         const int32_t wy = __float2int_rz(c.origin[1]) + (int32_t)uy;
         const int32_t wz = __float2int_rz(c.origin[2]) + (int32_t)uz;
         float qt; uint32_t qn; uint32_t qm[3];
-        if (cutout_march(wx, wy, wz, ux, uy, uz, ro, rd, t, axis, pdx, pdy, pdz, t > 0.0f, &qt, &qn, qm)) {
+        if (cutout_march(wx, wy, wz, ux, uy, uz, ro, rd, inv, t, axis, pdx, pdy, pdz, t > 0.0f, &qt, &qn, qm)) {
           h.hit = true; h.t = qt * vs; h.normal = qn;
           h.vx = ux; h.vy = uy; h.vz = uz;
           h.mx = qm[0]; h.my = qm[1]; h.mz = qm[2];
+          h.id = id;
           return h;
         }
         solid = false;
@@ -467,6 +497,16 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
       uint32_t m[3];
       micro_entry(ux, uy, uz, ro, rd, t, axis, pdx, pdy, pdz, t > 0.0f, m);
       h.mx = m[0]; h.my = m[1]; h.mz = m[2];
+      if (WANT_ID) {
+        if (!id_known) {
+          // leaf_attr (common.wgsl:336-348) from the L1 node in hand
+          const uint32_t lfb = cell_bit((ux >> 2) & 3u, (uy >> 2) & 3u, (uz >> 2) & 3u);
+          const uint32_t slot = (l1.z & VM_FULL_BIT) != 0u ? lfb : mask_below(l1.x, l1.y, lfb);
+          const uint32_t e = attr_needed ? attr : ld_brick(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + slot);
+          id = leaf_block(w, e, ux, uy, uz);
+        }
+        h.id = id;
+      }
       return h;
     }
     const int32_t bx0 = cx - (cx & (skip - 1)), by0 = cy - (cy & (skip - 1)), bz0 = cz - (cz & (skip - 1));
@@ -491,7 +531,7 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
 template <bool COUNT>
 __device__ __noinline__ float shadow_ray_t(const DevWorld& w, const vm_frame& f, F3 ro, F3 rd, float max_dist, Traffic* tr) {
   const Ray r = make_ray(ro, rd);
-  int32_t cx = ffloor_i(ro.x / 64.0f), cy = ffloor_i(ro.y / 64.0f), cz = ffloor_i(ro.z / 64.0f);
+  int32_t cx = ffloor_i(ro.x * INV64), cy = ffloor_i(ro.y * INV64), cz = ffloor_i(ro.z * INV64);
   uint32_t last = VM_NO_CHUNK;
   for (uint32_t i = 0; i < 24u; ++i) {
     uint64_t gi;
@@ -532,7 +572,7 @@ __device__ __noinline__ WorldHit trace_world(const DevWorld& w, const vm_frame& 
   const F3 inv = {1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z};
   const bool pdx = dir.x > 0.0f, pdy = dir.y > 0.0f, pdz = dir.z > 0.0f;
   const Ray r = make_ray(ro, rd);
-  int32_t cx = ffloor_i(ro.x / 64.0f), cy = ffloor_i(ro.y / 64.0f), cz = ffloor_i(ro.z / 64.0f);
+  int32_t cx = ffloor_i(ro.x * INV64), cy = ffloor_i(ro.y * INV64), cz = ffloor_i(ro.z * INV64);
   for (uint32_t i = 0; i < 16u; ++i) {
     uint64_t gi;
     if (!grid_rel(f, cx, cy, cz, &gi)) return out;
@@ -573,7 +613,7 @@ __device__ __forceinline__ float hit_t(const vm_frame& f, const Chunk& c, uint32
     return ((box_min.x + box_min.z + c.vs) - (f.cam_pos[0] + f.cam_pos[2])) / (rd.x + rd.z);
   }
   const uint32_t axis = nid >> 1u;
-  const float ms = c.vs / 4.0f;
+  const float ms = c.vs * 0.25f;   // == c.vs / 4 exactly
   const uint32_t mi = axis == 0 ? mx : (axis == 1 ? my : mz);
   const float plane = comp(box_min, axis) + (float)(mi + ((nid & 1u) == 1u ? 1u : 0u)) * ms;
   return (plane - f.cam_pos[axis]) / comp(rd, axis);

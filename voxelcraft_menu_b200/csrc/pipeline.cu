@@ -1,0 +1,432 @@
+// The frame as a wavefront pipeline of warp-independent kernels, sm_100a.
+//
+//   k_bounds   per view: for every visible chunk, the largest depth key a hit
+//              in it can have (from a lower bound on its distance) and the
+//              suffix maximum of that bound along the view's front-to-back
+//              chunk list;
+//   k_cull     one warp per 8x8 tile: tile_select's exact test
+//              (tile_select.wgsl:11-92) over every visible chunk, written as
+//              the tile's ascending chunk list;
+//   k_primary  persistent warps steal 8x4-pixel items; each lane marches its
+//              pixel through the tile's list front to back and stops as soon
+//              as no remaining chunk can produce a key above the pixel's
+//              current one, so the key equals the engine's atomicMax over all
+//              of the tile's pairs; the lane then queues its shadow ray and
+//              its water / glass ray with one atomic per warp;
+//   k_shadow,  one thread per queued ray, dense (the queue holds only rays
+//   k_secondary that exist), so whole warps trace together.
+//
+// No kernel synchronises a block: warps never wait on other warps.
+#include "kernels.cuh"
+#include "ray_stages.cuh"
+#include <cub/block/block_scan.cuh>
+#include <algorithm>
+
+namespace vmk {
+
+__device__ __forceinline__ uint32_t find_view(const PipeArgs& a, uint32_t tile) {
+  if (a.frames == nullptr) return 0;
+  uint32_t lo = 0, hi = a.n_views - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (a.views[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ const vm_frame& frame_of(const PipeArgs& a, uint32_t v) {
+  return a.frames ? a.frames[v] : a.frame0;
+}
+__device__ __forceinline__ ViewDesc view_of(const PipeArgs& a, uint32_t v) { return a.frames ? a.views[v] : a.view0; }
+__device__ __forceinline__ DevWorld world_of(const PipeArgs& a, const ViewDesc& vd) {
+  return {a.chunks + vd.chunk_off, vd.n_chunks, a.inners, a.n_inners, a.leaves, a.n_leaves,
+          a.bricks, a.n_bricks, a.grids + vd.grid_off, vd.grid_len, a.err};
+}
+
+struct MaxOp {
+  __device__ __forceinline__ uint32_t operator()(uint32_t x, uint32_t y) const { return x > y ? x : y; }
+};
+
+// A hit in chunk c has t >= dmin * (1 - 1e-5) - 0.05 * vs: the box distance
+// and the march's slab / DDA arithmetic differ by float rounding only, far
+// below that slack.  dkmax = depth_key of that bound (depth keys fall with t).
+constexpr int BOUNDS_THREADS = 256;
+__global__ void __launch_bounds__(BOUNDS_THREADS) k_bounds(const __grid_constant__ PipeArgs a) {
+  typedef cub::BlockScan<uint32_t, BOUNDS_THREADS> Scan;
+  __shared__ typename Scan::TempStorage tmp;
+  const uint32_t v = blockIdx.x;
+  const vm_frame& f = frame_of(a, v);
+  const ViewDesc vd = view_of(a, v);
+  const uint32_t n = min(f.chunk_count, vd.n_chunks);
+  const F3 cam = ld3(f.cam_pos);
+  const uint32_t per = (n + BOUNDS_THREADS - 1) / BOUNDS_THREADS;
+  // thread t owns [t*per, t*per+per); threads are taken in reverse so that an
+  // exclusive max-scan gives every thread the maximum over later chunks
+  const uint32_t t = BOUNDS_THREADS - 1 - threadIdx.x;
+  uint32_t* dk = a.dkmax + vd.chunk_off;
+  uint32_t* suf = a.sufmax + vd.chunk_off;
+  uint32_t local = 0u;
+  for (uint32_t k = 0; k < per; ++k) {
+    const uint32_t ci = t * per + k;
+    if (ci < n) {
+      const vm_chunk& c = a.chunks[vd.chunk_off + ci];
+      const float dmin = box_distance(cam, ld3(c.aabb_min), ld3(c.aabb_max));
+      const float lb = fmaxf(dmin * (1.0f - 1e-5f) - 0.05f * c.voxel_size, 0.0f);
+      const uint32_t d = depth_key(f, lb);
+      dk[ci] = d;
+      local = max(local, d);
+    }
+  }
+  uint32_t run;
+  Scan(tmp).ExclusiveScan(local, run, 0u, MaxOp());
+  for (int k = (int)per - 1; k >= 0; --k) {
+    const uint32_t ci = t * per + (uint32_t)k;
+    if (ci < n) {
+      run = max(run, dk[ci]);
+      suf[ci] = run;
+    }
+  }
+}
+
+// tile_select's per-chunk test (tile_select.wgsl:59-80 without the Hi-Z
+// deferral): the camera chunk always, else inside the near plane and the
+// tile's four side planes and closer than the reach.
+__device__ __forceinline__ bool cull_keep(const vm_frame& f, const TilePlanes& tp, F3 cam, F3 fwd,
+                                          const vm_chunk* ch, uint32_t ci) {
+  if (ci == f.camera_chunk) return true;
+  const float* cp = reinterpret_cast<const float*>(ch + ci);
+  const F3 bmin = {__ldg(cp + 0), __ldg(cp + 1), __ldg(cp + 2)};
+  const F3 bmax = {__ldg(cp + 4), __ldg(cp + 5), __ldg(cp + 6)};
+  if (box_outside(bmin, bmax, fwd, cam) || box_outside(bmin, bmax, tp.n[0], cam) ||
+      box_outside(bmin, bmax, tp.n[1], cam) || box_outside(bmin, bmax, tp.n[2], cam) ||
+      box_outside(bmin, bmax, tp.n[3], cam))
+    return false;
+  return box_distance(cam, bmin, bmax) < tp.reach;
+}
+
+__global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t n_warps = gridDim.x * 8u;
+  for (uint32_t t = blockIdx.x * 8u + (threadIdx.x >> 5); t < a.total_tiles; t += n_warps) {
+    const uint32_t v = find_view(a, t);
+    const vm_frame& f = frame_of(a, v);
+    const ViewDesc vd = view_of(a, v);
+    const uint32_t local = t - vd.tile_begin;
+    const uint32_t tx = local % vd.tiles_x, ty = local / vd.tiles_x;
+    const TilePlanes tp = tile_planes(f, tx * 8u, ty * 8u);
+    const F3 cam = ld3(f.cam_pos), fwd = ld3(f.cam_fwd);
+    const uint32_t n_vis = min(f.chunk_count, vd.n_chunks);
+    const vm_chunk* ch = a.chunks + vd.chunk_off;
+    uint16_t* out = a.tile_list + (uint64_t)t * a.list_cap;
+    uint32_t n = 0;
+    for (uint32_t base = 0; base < n_vis; base += 32u) {
+      const uint32_t ci = base + lane;
+      const bool keep = ci < n_vis && cull_keep(f, tp, cam, fwd, ch, ci);
+      const uint32_t bal = __ballot_sync(FULLMASK, keep);
+      if (keep) {
+        const uint32_t pos = n + __popc(bal & lanemask_lt());
+        if (pos < a.list_cap) out[pos] = (uint16_t)ci;
+      }
+      n += __popc(bal);
+    }
+    if (lane == 0) a.tile_count[t] = n;
+  }
+}
+
+// stage: 0 primary, 1 shadow, 2 secondary (a.traffic holds one record per stage)
+template <bool COUNT>
+__device__ __forceinline__ void flush_traffic(const PipeArgs& a, int stage, const Traffic& tr, uint32_t np,
+                                              uint32_t ns, uint32_t nx) {
+  if (!COUNT) return;
+  unsigned long long v[11] = {tr.chunk, tr.l1, tr.leaf, tr.attr, tr.pal, tr.grid, tr.iters, np, ns, nx, tr.entries};
+  unsigned long long* dst = reinterpret_cast<unsigned long long*>(a.traffic + stage);
+#pragma unroll
+  for (int i = 0; i < 11; ++i) {
+    unsigned long long x = v[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(FULLMASK, x, o);
+    if ((threadIdx.x & 31u) == 0 && x) atomicAdd(dst + i, x);
+  }
+}
+
+// One lane, one pixel, one chunk: march it and fold the key into the pixel's
+// best (the engine's atomicMax), keeping the best hit's block id.
+template <bool UNDERWATER, bool COUNT>
+__device__ __forceinline__ void march_entry(const DevWorld& w, const vm_frame& f, const Ray& ray, uint32_t ci,
+                                            uint32_t px, uint32_t py, unsigned long long& best, uint32_t& best_id,
+                                            Traffic* tr) {
+  if (COUNT) tr->entries++;
+  const Chunk c = ld_chunk(w, ci);
+  if (ray_skips(f, c.fade, px, py)) return;
+  const Hit h = march_chunk<UNDERWATER, false, false, COUNT, true>(w, f, c, ray, f.far_, tr);
+  if (h.hit) {
+    const unsigned long long k = make_key(f, h, ci);
+    if (k > best) { best = k; best_id = h.id; }
+  }
+}
+
+// The rest of tile_select's scan when a tile's list overflowed its capacity:
+// 32 chunks culled per step across the warp, each survivor marched in order.
+// Cold code, kept out of the primary loop's instruction stream.
+template <bool UNDERWATER, bool COUNT>
+__device__ __noinline__ void march_overflow(const DevWorld w, const vm_frame& f, const Ray ray, uint32_t start,
+                                            uint32_t tx, uint32_t ty, uint32_t px, uint32_t py,
+                                            const uint32_t* dk, const uint32_t* suf, bool active,
+                                            unsigned long long* best, uint32_t* best_id, Traffic* tr) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const TilePlanes tp = tile_planes(f, tx * 8u, ty * 8u);
+  const F3 fwd = ld3(f.cam_fwd);
+  const uint32_t n_vis = min(f.chunk_count, w.n_chunks);
+  unsigned long long b = *best;
+  uint32_t id = *best_id;
+  for (uint32_t base = start; base < n_vis; base += 32u) {
+    const uint32_t ci = base + lane;
+    uint32_t bal = __ballot_sync(FULLMASK, ci < n_vis && cull_keep(f, tp, ray.o, fwd, w.chunks, ci));
+    while (bal) {
+      const uint32_t cj = base + (uint32_t)(__ffs(bal) - 1);
+      bal &= bal - 1u;
+      if (!active) continue;
+      const uint32_t bestd = (uint32_t)(b >> 40);
+      if (suf[cj] < bestd) { active = false; continue; }
+      if (dk[cj] < bestd) continue;
+      march_entry<UNDERWATER, COUNT>(w, f, ray, cj, px, py, b, id, tr);
+    }
+  }
+  *best = b;
+  *best_id = id;
+}
+
+// MINB: blocks per SM the register allocation must allow (1: unconstrained),
+// the autotuner's occupancy knob.
+template <int NW, int MINB, bool UNDERWATER, bool COUNT>
+__global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant__ PipeArgs a) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t total = a.total_tiles * 2u;
+  Traffic tr = {};
+  uint32_t np = 0, ns = 0, nx = 0;
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&a.work[W_PRIMARY], 1u);
+    item = __shfl_sync(FULLMASK, item, 0);
+    if (item >= total) break;
+    const uint32_t t = item >> 1, half = item & 1u;
+    const uint32_t v = find_view(a, t);
+    const vm_frame& f = frame_of(a, v);
+    const ViewDesc vd = view_of(a, v);
+    const DevWorld w = world_of(a, vd);
+    const uint32_t local = t - vd.tile_begin;
+    const uint32_t tx = local % vd.tiles_x, ty = local / vd.tiles_x;
+    const uint32_t px = tx * 8u + (lane & 7u), py = ty * 8u + half * 4u + (lane >> 3);
+    const bool valid = px < f.res[0] && py < f.res[1];
+    const uint32_t n = a.tile_count[t];
+    const uint32_t m = min(n, a.list_cap);
+    const uint16_t* list = a.tile_list + (uint64_t)t * a.list_cap;
+    const uint32_t* dk = a.dkmax + vd.chunk_off;
+    const uint32_t* suf = a.sufmax + vd.chunk_off;
+    const F3 cam = ld3(f.cam_pos);
+    const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+    const Ray ray = make_ray(cam, rd);
+    unsigned long long best = 0ull;
+    uint32_t best_id = 0u;
+    bool active = valid;
+    for (uint32_t i = 0; i < m && active; ++i) {
+      const uint32_t ci = list[i];
+      const uint32_t bestd = (uint32_t)(best >> 40);
+      if (suf[ci] < bestd) { active = false; break; }
+      if (dk[ci] < bestd) continue;
+      march_entry<UNDERWATER, COUNT>(w, f, ray, ci, px, py, best, best_id, &tr);
+    }
+    if (n > a.list_cap)
+      march_overflow<UNDERWATER, COUNT>(w, f, ray, (uint32_t)list[a.list_cap - 1] + 1u, tx, ty, px, py, dk, suf,
+                                        active, &best, &best_id, &tr);
+    const uint64_t pix = (uint64_t)py * f.res[0] + px;
+    if (valid) a.vis[vd.pix_off + pix] = best;
+    if (COUNT && valid) ++np;
+    {
+      // build_hiz (march.wgsl:57-76) on the final visibility: pixels outside
+      // the frame count as misses
+      const uint32_t d = __reduce_min_sync(FULLMASK, valid ? (uint32_t)(best >> 40) : 0u);
+      if (lane == 0) atomicMin(&a.hiz[vd.tile_begin + local], d);
+    }
+    // The hit shared by shadow_guide (shadow.wgsl:8-30) and the water / glass
+    // legs (resolve.wgsl:1029-1042,1261-1280): hit_t of the key and its point.
+    bool want_sh = false, want_sec = false;
+    F3 so = {0.0f, 0.0f, 0.0f};
+    SecRay sr;
+    if (valid && best != 0ull) {
+      const KeyParts k = split_key(best);
+      const Chunk c = ld_chunk(w, k.ci);
+      const float th = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+      const F3 hit = cam + rd * th;
+      const bool water = best_id == VM_WATER, glass = best_id == VM_GLASS;
+      if (a.do_shadow && shadow_active(f) && !water && !glass) {
+        F3 nrm = normal_of(k.nid);
+        if (k.nid >= VM_NORMAL_CROSS_A && dot(nrm, rd) > 0.0f) nrm = neg(nrm);
+        if (!(dot(nrm, ld3(f.sun_dir)) <= 0.0f) && th >= 0.0f) {
+          so = hit + nrm * (0.02f * c.vs);
+          want_sh = true;
+        }
+      }
+      if (a.do_secondary && water) {
+        const float detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, th);
+        if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && detail > 0.0f) {
+          const F3 rdir = refract(rd, normal_of(k.nid), 1.0f / VM_WATER_IOR);
+          sr.o = hit + rdir * VM_SURFACE_EPS;
+          sr.d = rdir;
+          sr.max_dist = VM_WATER_REFRACT_DIST;
+          sr.water = true;
+          want_sec = true;
+        }
+      } else if (a.do_secondary && glass) {
+        sr.o = hit + rd * VM_SURFACE_EPS;
+        sr.d = rd;
+        sr.max_dist = fmaxf(VM_GLASS_TRANSMIT_DIST, f.far_);
+        sr.water = false;
+        want_sec = true;
+      }
+    }
+    if (a.do_shadow) {
+      if (valid && !want_sh) a.shadow[vd.pix_off + pix] = 0.0f;
+      const uint32_t bal = __ballot_sync(FULLMASK, want_sh);
+      if (bal) {
+        uint32_t b0 = 0;
+        if (lane == 0) b0 = atomicAdd(&a.work[W_SHADOW_N], __popc(bal));
+        b0 = __shfl_sync(FULLMASK, b0, 0);
+        if (want_sh) {
+          ShadowItem& q = a.shadow_q[b0 + __popc(bal & lanemask_lt())];
+          q.view = v; q.pix = (uint32_t)pix; q.o[0] = so.x; q.o[1] = so.y; q.o[2] = so.z;
+        }
+      }
+    }
+    if (a.do_secondary) {
+      if (valid && !want_sec) { a.sec_key[vd.pix_off + pix] = 0ull; a.sec_t[vd.pix_off + pix] = 0.0f; }
+      const uint32_t bal = __ballot_sync(FULLMASK, want_sec);
+      if (bal) {
+        uint32_t b0 = 0;
+        if (lane == 0) b0 = atomicAdd(&a.work[W_SEC_N], __popc(bal));
+        b0 = __shfl_sync(FULLMASK, b0, 0);
+        if (want_sec) {
+          SecItem& q = a.sec_q[b0 + __popc(bal & lanemask_lt())];
+          q.view = v; q.pix = (uint32_t)pix;
+          q.o[0] = sr.o.x; q.o[1] = sr.o.y; q.o[2] = sr.o.z;
+          q.d[0] = sr.d.x; q.d[1] = sr.d.y; q.d[2] = sr.d.z;
+          q.max_dist = sr.max_dist; q.water = sr.water ? 1u : 0u;
+        }
+      }
+    }
+  }
+  flush_traffic<COUNT>(a, 0, tr, np, ns, nx);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ PipeArgs a) {
+  const uint32_t n = a.work[W_SHADOW_N];
+  Traffic tr = {};
+  uint32_t ns = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const ShadowItem q = a.shadow_q[i];
+    const vm_frame& f = frame_of(a, q.view);
+    const ViewDesc vd = view_of(a, q.view);
+    const DevWorld w = world_of(a, vd);
+    const float b = shadow_ray_t<COUNT>(w, f, f3(q.o[0], q.o[1], q.o[2]), ld3(f.sun_dir), f.shadow_dist, &tr);
+    a.shadow[vd.pix_off + q.pix] = blocker_distance(b);
+    if (COUNT) ++ns;
+  }
+  flush_traffic<COUNT>(a, 1, tr, 0, ns, 0);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_secondary_q(const __grid_constant__ PipeArgs a) {
+  const uint32_t n = a.work[W_SEC_N];
+  Traffic tr = {};
+  uint32_t nx = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const SecItem q = a.sec_q[i];
+    const vm_frame& f = frame_of(a, q.view);
+    const ViewDesc vd = view_of(a, q.view);
+    const DevWorld w = world_of(a, vd);
+    SecRay s;
+    s.o = f3(q.o[0], q.o[1], q.o[2]);
+    s.d = f3(q.d[0], q.d[1], q.d[2]);
+    s.max_dist = q.max_dist;
+    s.water = q.water != 0u;
+    unsigned long long k;
+    float t;
+    secondary_trace<COUNT>(w, f, s, &k, &t, &tr);
+    a.sec_key[vd.pix_off + q.pix] = k;
+    a.sec_t[vd.pix_off + q.pix] = t;
+    if (COUNT) ++nx;
+  }
+  flush_traffic<COUNT>(a, 2, tr, 0, 0, nx);
+}
+
+// ---------------------------------------------------------------------------
+// Register levels: 0 unconstrained, 1 ~80 registers, 2 64 registers per thread.
+template <int NW, int LEVEL>
+struct MinBlocks { static constexpr int value = LEVEL == 0 ? 1 : (LEVEL == 1 ? 24 / NW : 32 / NW); };
+
+template <int NW, int LEVEL, bool UW>
+static void* primary_fn(bool cnt) {
+  if (cnt) return (void*)k_primary<NW, MinBlocks<NW, LEVEL>::value, UW, true>;
+  return (void*)k_primary<NW, MinBlocks<NW, LEVEL>::value, UW, false>;
+}
+
+template <int NW>
+static void* primary_nw(int level, bool uw, bool cnt) {
+  switch (level) {
+    case 0: return uw ? primary_fn<NW, 0, true>(cnt) : primary_fn<NW, 0, false>(cnt);
+    case 1: return uw ? primary_fn<NW, 1, true>(cnt) : primary_fn<NW, 1, false>(cnt);
+    case 2: return uw ? primary_fn<NW, 2, true>(cnt) : primary_fn<NW, 2, false>(cnt);
+  }
+  return nullptr;
+}
+
+static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt) {
+  if (cnt) return primary_nw<4>(0, uw, true);   // the counting run is never timed
+  switch (t.primary_warps) {
+    case 4: return primary_nw<4>(t.reg_level, uw, false);
+    case 8: return primary_nw<8>(t.reg_level, uw, false);
+  }
+  return nullptr;
+}
+
+static int block_warps(const PipeTuning& t, bool cnt) { return cnt ? 4 : t.primary_warps; }
+
+int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count) {
+  void* fn = primary_kernel(t, underwater, count);
+  if (!fn) return 0;
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block_warps(t, count) * 32, 0);
+  return n;
+}
+
+cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwater, bool count, int sms,
+                            cudaStream_t s) {
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(a.work, 0, W_WORDS * sizeof(uint32_t), s)) != cudaSuccess) return e;
+  if (a.total_tiles == 0) return cudaSuccess;
+  if ((e = cudaMemsetAsync(a.hiz, 0xFF, (size_t)a.total_tiles * 4, s)) != cudaSuccess) return e;
+  k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
+  const uint32_t cull_blocks = std::min<uint32_t>((a.total_tiles + 7) / 8, (uint32_t)sms * 16u);
+  k_cull<<<cull_blocks, 256, 0, s>>>(a);
+  void* fn = primary_kernel(t, underwater, count);
+  if (!fn) return cudaErrorInvalidValue;
+  const int nw = block_warps(t, count);
+  int per = t.ctas_per_sm > 0 && !count ? t.ctas_per_sm : primary_max_ctas_per_sm(t, underwater, count);
+  if (per <= 0) per = 1;
+  const uint32_t items_blocks = (a.total_tiles * 2u + nw - 1) / nw;
+  const uint32_t grid = std::min<uint32_t>((uint32_t)sms * (uint32_t)per, items_blocks);
+  void* args[] = {(void*)&a};
+  if ((e = cudaLaunchKernel(fn, dim3(grid), dim3(nw * 32), args, 0, s)) != cudaSuccess) return e;
+  const uint32_t q_blocks = (uint32_t)sms * 8u;
+  if (a.do_shadow) {
+    if (count) k_shadow<true><<<q_blocks, 256, 0, s>>>(a);
+    else k_shadow<false><<<q_blocks, 256, 0, s>>>(a);
+  }
+  if (a.do_secondary) {
+    if (count) k_secondary_q<true><<<q_blocks, 256, 0, s>>>(a);
+    else k_secondary_q<false><<<q_blocks, 256, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace vmk

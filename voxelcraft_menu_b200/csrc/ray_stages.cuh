@@ -1,0 +1,102 @@
+// Per-ray stages shared by the march kernels: key decoding, the shadow ray
+// set-up of shadow_guide and the one water / glass secondary ray per hit.
+#pragma once
+#include "march_device.cuh"
+
+namespace vmk {
+using namespace vmd;
+
+#define FULLMASK 0xFFFFFFFFu
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ bool shadow_active(const vm_frame& f) {   // shadow.wgsl:31-33
+  return (f.flags & VM_FLAG_SHADOWS) != 0u && (f.flags & VM_FLAG_HEATMAP) == 0u && f.daylight > 0.01f;
+}
+
+struct KeyParts { uint32_t ci, vx, vy, vz, mx, my, mz, nid; };
+__device__ __forceinline__ KeyParts split_key(unsigned long long key) {
+  KeyParts k;
+  const uint32_t low = (uint32_t)(key & 0xFFFFFFull);
+  k.ci = (uint32_t)(key >> 24) & 0x1FFFu;
+  k.vx = (low >> 16) & 63u; k.vy = (low >> 8) & 63u; k.vz = low & 63u;
+  k.mx = (low >> 22) & 3u; k.my = (low >> 14) & 3u; k.mz = (low >> 6) & 3u;
+  k.nid = (uint32_t)(key >> 37) & 7u;
+  return k;
+}
+
+// shadow_guide (shadow.wgsl:8-30): the sun ray's origin for a visible pixel,
+// or false when the pixel casts no shadow ray.
+__device__ __forceinline__ bool shadow_setup(const DevWorld& w, const vm_frame& f, unsigned long long key,
+                                             uint32_t px, uint32_t py, F3* origin) {
+  if (key == 0ull) return false;
+  const KeyParts k = split_key(key);
+  const Chunk c = ld_chunk(w, k.ci);
+  const uint32_t id = block_at(w, c, k.vx, k.vy, k.vz);
+  if (id == VM_WATER || id == VM_GLASS) return false;
+  const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+  F3 n = normal_of(k.nid);
+  if (k.nid >= VM_NORMAL_CROSS_A && dot(n, rd) > 0.0f) n = neg(n);
+  if (dot(n, ld3(f.sun_dir)) <= 0.0f) return false;
+  const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+  if (!(t >= 0.0f)) return false;
+  const F3 hit = ld3(f.cam_pos) + rd * t;
+  *origin = hit + n * (0.02f * c.vs);
+  return true;
+}
+
+__device__ __forceinline__ float blocker_distance(float blocker) {   // shadow.wgsl:44
+  return blocker >= 0.0f ? fminf(fmaxf(blocker, 0.001f), 65504.0f) : 0.0f;
+}
+
+// The one secondary ray of a water or glass hit:
+//   water: water_refract_leg (resolve.wgsl:1029-1042), gated by
+//          FLAG_WATER_REFRACT and refract_detail > 0 (resolve.wgsl:1098,1524);
+//   glass: shade_glass's straight transmission (resolve.wgsl:1276-1280).
+struct SecRay { F3 o, d; float max_dist; bool water; };
+__device__ __forceinline__ bool secondary_setup(const DevWorld& w, const vm_frame& f, unsigned long long key,
+                                                uint32_t px, uint32_t py, SecRay* s) {
+  if (key == 0ull) return false;
+  const KeyParts k = split_key(key);
+  const Chunk c = ld_chunk(w, k.ci);
+  const uint32_t id = block_at(w, c, k.vx, k.vy, k.vz);
+  const bool water = id == VM_WATER, glass = id == VM_GLASS;
+  if (!water && !glass) return false;
+  const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+  const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+  const F3 hit = ld3(f.cam_pos) + rd * t;
+  if (water) {
+    const float detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, t);
+    if (!((f.flags & VM_FLAG_WATER_REFRACT) != 0u && detail > 0.0f)) return false;
+    const F3 rdir = refract(rd, normal_of(k.nid), 1.0f / VM_WATER_IOR);
+    s->o = hit + rdir * VM_SURFACE_EPS;
+    s->d = rdir;
+    s->max_dist = VM_WATER_REFRACT_DIST;
+    s->water = true;
+  } else {
+    s->o = hit + rd * VM_SURFACE_EPS;
+    s->d = rd;
+    s->max_dist = fmaxf(VM_GLASS_TRANSMIT_DIST, f.far_);
+    s->water = false;
+  }
+  return true;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ void secondary_trace(const DevWorld& w, const vm_frame& f, const SecRay& s,
+                                                unsigned long long* out_key, float* out_t, Traffic* tr) {
+  const WorldHit h = s.water ? trace_world<true, COUNT>(w, f, s.o, s.d, s.max_dist, tr)
+                             : trace_world<false, COUNT>(w, f, s.o, s.d, s.max_dist, tr);
+  unsigned long long k = (1ull << 63) | (s.water ? 0ull : (1ull << 61));
+  if (h.hit)
+    k |= (1ull << 62) | ((unsigned long long)h.normal << 37) | ((unsigned long long)h.ci << 24) |
+         (unsigned long long)((h.vx << 16) | (h.vy << 8) | h.vz);
+  *out_key = k;
+  *out_t = h.t;
+}
+
+}  // namespace vmk

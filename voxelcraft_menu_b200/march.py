@@ -21,9 +21,9 @@ VM_OK = 0
 STATUS = {0: "VM_OK", 1: "VM_E_INVALID", 2: "VM_E_CAPACITY", 3: "VM_E_TILE_OVERFLOW", 4: "VM_E_ITER_CAP",
           5: "VM_E_TIMEOUT", 6: "VM_E_CUDA", 7: "VM_E_NOT_READY"}
 
-# fused tile variants (vm_set_tuning)
-TILE_8x8, TILE_16x8, TILE_16x16, TILE_32x16 = 0, 1, 2, 3
-TILE_SHAPES = {0: (8, 8), 1: (16, 8), 2: (16, 16), 3: (32, 16)}
+# warps per block and register levels of the persistent primary-ray kernel (vm_set_tuning)
+PRIMARY_WARPS = (4, 8)
+REG_LEVELS = (0, 1, 2)
 
 
 class MarchError(RuntimeError):
@@ -95,8 +95,11 @@ class Marcher:
     def set_frame(self, frame: VmFrame):
         self._ck(self._L.vm_set_frame(self._h, C.byref(frame)))
 
-    def set_tuning(self, tile_variant: int = TILE_16x16, ctas_per_sm: int = 0):
-        self._ck(self._L.vm_set_tuning(self._h, tile_variant, ctas_per_sm))
+    def set_tuning(self, warps: int = 4, reg_level: int = 0, ctas_per_sm: int = 0):
+        """Warps per block (4, 8), register budget (0 unconstrained, 1 ~80,
+        2 64 per thread) and resident blocks per SM (0 = occupancy maximum)
+        of the persistent primary-ray kernel."""
+        self._ck(self._L.vm_set_tuning(self._h, warps, reg_level, ctas_per_sm))
 
     # -- the engine's passes ------------------------------------------------------
     def select(self):
@@ -119,13 +122,17 @@ class Marcher:
         self.secondary()
 
     def render(self):
-        """The fused persistent kernel: same outputs as render_passes()."""
+        """The wavefront pipeline (cull, primary, shadow, secondary kernels):
+        same outputs as render_passes()."""
         self._ck(self._L.vm_render(self._h))
 
     def render_counted(self) -> dict:
         t = VmTraffic()
         self._ck(self._L.vm_render_counted(self._h, C.byref(t)))
-        return {n: int(getattr(t, n)) for n, _ in VmTraffic._fields_}
+        out = {n: int(getattr(t, n)) for n, _ in VmTraffic._fields_[:11]}
+        out["stage_iters"] = [int(x) for x in t.stage_iters]
+        out["stage_chunks"] = [int(x) for x in t.stage_chunks]
+        return out
 
     def sync(self):
         self._ck(self._L.vm_sync(self._h))

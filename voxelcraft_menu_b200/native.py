@@ -111,7 +111,8 @@ class VmStats(C.Structure):
 class VmTraffic(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("chunk_records", "l1_fetches", "leaf_fetches", "attr_fetches",
                                           "palette_decodes", "grid_lookups", "iters", "rays_primary",
-                                          "rays_shadow", "rays_secondary")]
+                                          "rays_shadow", "rays_secondary", "list_entries")] + \
+               [("stage_iters", C.c_uint64 * 3), ("stage_chunks", C.c_uint64 * 3)]
 
 
 class VmDevicePtrs(C.Structure):
@@ -138,7 +139,7 @@ _SIGNATURES = [
     ("vm_primary_shadow", C.c_int, [vp]),
     ("vm_secondary", C.c_int, [vp]),
     ("vm_render", C.c_int, [vp]),
-    ("vm_set_tuning", C.c_int, [vp, C.c_int, C.c_int]),
+    ("vm_set_tuning", C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
     ("vm_read_vis", C.c_int, [vp, vp]),
     ("vm_read_hiz", C.c_int, [vp, vp]),
     ("vm_write_hiz", C.c_int, [vp, vp]),

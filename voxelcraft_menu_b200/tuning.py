@@ -1,17 +1,17 @@
-"""Autotuner of the fused march: tile shape (8x8, 16x8, 16x16, 32x16 pixels
-per CTA, i.e. 2 to 16 warps per block) and resident CTAs per SM of the
-persistent launch.  Every candidate's output is checked against the first
-candidate's before its time counts, so tuning can never change results."""
+"""Autotuner of the frame pipeline's persistent primary-ray kernel: warps per
+block (2, 4, 8) and resident blocks per SM.  Every candidate's output is
+compared with the first candidate's before its time counts, so tuning can
+never change results."""
 from __future__ import annotations
 
 import hashlib
 
 import numpy as np
 
-from .march import TILE_SHAPES, Marcher
+from .march import PRIMARY_WARPS, REG_LEVELS, Marcher
 
 
-def _time(m: Marcher, run, reps: int = 5) -> float:
+def _time(run, reps: int = 5) -> float:
     import torch
     stream = torch.cuda.current_stream()
     run()
@@ -33,45 +33,36 @@ def _digest(*arrays) -> str:
 
 
 def candidates():
-    for v in sorted(TILE_SHAPES):
-        for per in (0, 1, 2, 4):
-            yield v, per
+    for warps in PRIMARY_WARPS:
+        for level in REG_LEVELS:
+            yield warps, level, 0
+
+
+def _tune(m: Marcher, run, read) -> dict:
+    ref = None
+    best = None
+    for warps, level, per in candidates():
+        m.set_tuning(warps, level, per)
+        ms = _time(run)
+        d = _digest(*read())
+        if ref is None:
+            ref = d
+        if d != ref:
+            raise RuntimeError(f"{warps} warps / register level {level} changed the output")
+        if best is None or ms < best["ms"]:
+            best = {"warps": warps, "reg_level": level, "ctas_per_sm": per, "ms": ms}
+    return best
 
 
 def autotune_single(m: Marcher, view, warm=None) -> dict:
-    """Fastest (variant, ctas_per_sm) for vm_render on `view`."""
+    """Fastest (warps, ctas_per_sm) for vm_render on `view`."""
     if warm is not None:
         m.upload_view(warm)
         m.render()
     m.upload_view(view)
-    ref = None
-    best = None
-    for v, per in candidates():
-        m.set_tuning(v, per)
-        ms = _time(m, m.render)
-        d = _digest(m.read_vis(), m.read_shadow())
-        if ref is None:
-            ref = d
-        if d != ref:
-            raise RuntimeError(f"tile variant {v} / {per} CTAs per SM changed the output")
-        if best is None or ms < best["ms"]:
-            best = {"variant": v, "ctas_per_sm": per, "ms": ms}
-    return best
+    return _tune(m, m.render, lambda: (m.read_vis(), m.read_shadow()))
 
 
 def autotune_batch(m: Marcher) -> dict:
-    """Fastest (variant, ctas_per_sm) for the persistent batched launch."""
-    ref = None
-    best = None
-    for v, per in candidates():
-        m.set_tuning(v, per)
-        ms = _time(m, m.batch_run, reps=3)
-        vis, sh = m.batch_read()
-        d = _digest(vis, sh)
-        if ref is None:
-            ref = d
-        if d != ref:
-            raise RuntimeError(f"tile variant {v} / {per} CTAs per SM changed the batch output")
-        if best is None or ms < best["ms"]:
-            best = {"variant": v, "ctas_per_sm": per, "ms": ms}
-    return best
+    """Fastest (warps, ctas_per_sm) for the batched launch."""
+    return _tune(m, m.batch_run, m.batch_read)
