@@ -151,6 +151,24 @@ int vm_device_buffers(vm_ctx* ctx, vm_device_ptrs* out);
 /* Synchronise the context's stream. */
 int vm_sync(vm_ctx* ctx);
 
+/* Frame march that allocates nothing (this entry point has no counterpart in
+ * the reference).  For callers that cannot call cudaMalloc: code inside a
+ * stream capture it does not own, engines that hand out all device memory
+ * from their own arenas, allocation-free real-time paths.  The caller passes
+ * every input and output as device pointers (pools, chunk list, grid, vis,
+ * shadow, a zeroed u32 error word) on the current device and stream; the
+ * pipeline's scratch is one static device array of about 7.5 MB per GPU.
+ * Primary and shadow rays only; at most 262144 pixels and 8192 8x8 tiles per
+ * frame (larger frames return VM_E_CAPACITY).  The first call on a device
+ * looks the array up and must come before any stream capture.  Every call
+ * shares the array: calls that overlap on the GPU race.
+ * vm_static_last_error() describes the last failure of this thread. */
+int vm_render_static(const vm_frame* frame, const vm_chunk* d_chunks, uint32_t n_chunks, const uint32_t* d_grid,
+                     uint64_t grid_len, const uint32_t* d_inners, uint64_t n_inners, const uint32_t* d_leaves,
+                     uint64_t n_leaves, const uint32_t* d_bricks, uint64_t n_bricks, uint64_t* d_vis,
+                     float* d_shadow, uint32_t* d_error, void* cuda_stream);
+const char* vm_static_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

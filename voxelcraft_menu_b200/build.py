@@ -27,7 +27,7 @@ NVCC_FLAGS = ARCH + [
 ]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", f"-I{ROOT}", f"-I{CSRC}"]
 
-CU_SOURCES = ["kernels.cu", "pipeline.cu", "capi.cu"]
+CU_SOURCES = ["kernels.cu", "pipeline.cu", "capi.cu", "static_scratch.cu"]
 CPP_SOURCES = ["world.cpp"]
 HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "ray_stages.cuh", "world.h"]
 

@@ -155,6 +155,9 @@ _SIGNATURES = [
     ("vm_batch_pixels", C.c_uint64, [vp]),
     ("vm_device_buffers", C.c_int, [vp, P(VmDevicePtrs)]),
     ("vm_sync", C.c_int, [vp]),
+    ("vm_render_static", C.c_int, [P(VmFrame), vp, C.c_uint32, vp, C.c_uint64, vp, C.c_uint64, vp, C.c_uint64,
+                                   vp, C.c_uint64, vp, vp, vp, vp]),
+    ("vm_static_last_error", C.c_char_p, []),
     # host world store (include/voxmarch_world.h)
     ("vmw_create", vp, []),
     ("vmw_destroy", None, [vp]),
