@@ -130,14 +130,61 @@ typedef struct vm_traffic {
 int vm_render_counted(vm_ctx* ctx, vm_traffic* out);
 
 /* Batched views: many frames (each with its own chunk list and grid) marched
- * by one persistent work-stealing launch (vm_batch_run mode 0, replayed from
- * a CUDA graph) or by one launch per view (mode 1, the baseline).  Views are
- * packed in order; their outputs are concatenated in the batch buffers. */
+ * by one persistent work-stealing launch (VM_BATCH_PERSISTENT, replayed from
+ * a CUDA graph) or by one launch sequence per view (VM_BATCH_PER_VIEW, the
+ * baseline), optionally | VM_BATCH_SECONDARY to also trace the water / glass
+ * rays (needed by vm_shade_gbuffer).  Views are packed in order; their
+ * outputs are concatenated in the batch buffers.  The engine renders one
+ * view per Renderer::render (src/render/mod.rs:1593); its probe and lookbook
+ * views are separate dispatches, which VM_BATCH_PER_VIEW reproduces. */
+#define VM_BATCH_PERSISTENT 0
+#define VM_BATCH_PER_VIEW 1
+#define VM_BATCH_SECONDARY 2
 int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm_chunk* chunks,
                  const uint32_t* chunk_counts, const uint32_t* grids, const uint32_t* grid_lens);
 int vm_batch_run(vm_ctx* ctx, int mode);
 int vm_batch_read(vm_ctx* ctx, uint64_t* vis, float* shadow);
+/* the secondary rays' keys and distances of the last VM_BATCH_SECONDARY run */
+int vm_batch_read_secondary(vm_ctx* ctx, uint64_t* key, float* t);
 uint64_t vm_batch_pixels(const vm_ctx* ctx);
+
+/* Differentiable shading over a fixed visibility buffer.  The engine has no
+ * such stage: its shading lives in resolve.wgsl:1379-1466.  This pair restates
+ * the terms sun N.L with the shadow verdict, sky ambient, height fog
+ * (common.wgsl:1332-1341) and Beer-Lambert water absorption
+ * (common.wgsl:1262-1265) as a smooth function of VM_SHADE_NPARAMS floats:
+ * [0,768) albedo table 256 x 3, [768,771) sun direction (normalised inside),
+ * [771,774) sky ambient RGB, 774 fog density, [775,778) water absorption RGB.
+ *
+ * vm_shade_gbuffer writes one vm_shade_gbuf per pixel of the last batch
+ * (vm_batch_run with VM_BATCH_SECONDARY).  The fog's optical length per unit
+ * density (e * path of transmittance_from) depends on the geometry and the
+ * fog falloff / height only, so it is computed there once.  vm_shade_forward
+ * writes RGB per pixel (and/or adds the L2 loss against d_target into
+ * *d_loss); vm_shade_backward adds dL/dparams into d_grad_params (FP64) for
+ * dL/dcolour = d_grad_color, or for the L2 loss against d_target when
+ * d_grad_color is NULL, in which case it also adds that loss into *d_loss when
+ * d_loss is not NULL (forward and backward fused).  All pointers are device
+ * pointers on the current device; work is enqueued on cuda_stream. */
+#define VM_SHADE_NPARAMS 778
+#define VM_SHADE_GBUF_BYTES 16
+typedef struct vm_shade_consts {
+  float sun_rgb[3];        /* sun colour times the engine's 0.78 gain */
+  float fog_falloff, fog_height;
+} vm_shade_consts;
+typedef struct vm_shade_gbuf {
+  uint32_t code;           /* id | face << 8 | HIT 1<<11 | LIT 1<<12 | TRACED 1<<13 | HIT2 1<<14 | FLIP 1<<15
+                              | id2 << 16 | face2 << 24 (id2 / face2: the refracted ray's hit) */
+  float t;                 /* primary hit distance (0 for sky) */
+  float d;                 /* water refraction leg length */
+  float fog;               /* fog optical length per unit density (0 for sky) */
+} vm_shade_gbuf;
+int vm_shade_gbuffer(vm_ctx* ctx, const vm_shade_consts* consts, void* d_gbuf);
+int vm_shade_forward(const void* d_gbuf, uint64_t n_pixels, const float* d_params, const vm_shade_consts* consts,
+                     float* d_color, const float* d_target, double* d_loss, void* cuda_stream);
+int vm_shade_backward(const void* d_gbuf, uint64_t n_pixels, const float* d_params, const vm_shade_consts* consts,
+                      const float* d_grad_color, const float* d_target, double* d_grad_params, double* d_loss,
+                      void* cuda_stream);
 
 /* Device pointers of the context's buffers (valid until the next upload that
  * grows them), for zero-copy callers such as a torch binding. */

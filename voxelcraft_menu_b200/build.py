@@ -27,9 +27,12 @@ NVCC_FLAGS = ARCH + [
 ]
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", f"-I{ROOT}", f"-I{CSRC}"]
 
-CU_SOURCES = ["kernels.cu", "pipeline.cu", "capi.cu", "static_scratch.cu"]
+CU_SOURCES = ["kernels.cu", "pipeline.cu", "capi.cu", "gbuffer.cu", "shade.cu", "static_scratch.cu"]
+# The shading model is held to tolerances against FP64, not to bit equality
+# with the oracle, so it may contract a * b + c into fused multiply-adds.
+CU_EXTRA = {"shade.cu": ["--fmad=true"]}
 CPP_SOURCES = ["world.cpp"]
-HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "ray_stages.cuh", "world.h"]
+HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "ray_stages.cuh", "shade.cuh", "world.h"]
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:
@@ -52,7 +55,9 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> Path:
         obj = BUILD / (src + ".o")
         if force or verbose_ptxas or _newer(obj, [CSRC / src] + headers):
             extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-            _run([NVCC, *NVCC_FLAGS, *extra, "-c", str(CSRC / src), "-o", str(obj)])
+            own = CU_EXTRA.get(src, [])
+            flags = [f for f in NVCC_FLAGS if not any(f.split("=")[0] == o.split("=")[0] for o in own)]
+            _run([NVCC, *flags, *own, *extra, "-c", str(CSRC / src), "-o", str(obj)])
         objs.append(obj)
     for src in CPP_SOURCES:
         obj = BUILD / (src + ".o")

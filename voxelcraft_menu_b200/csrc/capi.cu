@@ -50,6 +50,7 @@ struct vm_ctx {
   bool b_underwater = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
+  bool graph_secondary = false;   // the cached graph also traces the secondary rays
   // tuning of the primary kernel
   vmk::PipeTuning tuning{4, 0, 0};
   std::string err_text;
@@ -607,7 +608,7 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
   return VM_OK;
 }
 
-static vmk::PipeArgs batch_args(vm_ctx* ctx) {
+static vmk::PipeArgs batch_args(vm_ctx* ctx, bool secondary) {
   vmk::PipeArgs a = base_args(ctx);
   a.frames = (const vm_frame*)ctx->b_frames.p;
   a.views = (const ViewDesc*)ctx->b_views.p;
@@ -627,7 +628,7 @@ static vmk::PipeArgs batch_args(vm_ctx* ctx) {
   a.hiz = (uint32_t*)ctx->b_hiz.p;
   a.shadow_q = (vmk::ShadowItem*)ctx->b_shadow_q.p;
   a.sec_q = (vmk::SecItem*)ctx->b_sec_q.p;
-  a.do_secondary = 0;   // batched views: primary + shadow
+  a.do_secondary = secondary ? 1 : 0;   // batched views: primary + shadow, optionally the water / glass rays
   return a;
 }
 
@@ -635,25 +636,29 @@ int vm_batch_run(vm_ctx* ctx, int mode) {
   if (!ctx) return VM_E_INVALID;
   if (ctx->b_n_views == 0) return fail(ctx, VM_E_NOT_READY, "no batch set");
   CK(cudaSetDevice(ctx->device));
-  if (mode == 0) {
+  if (mode & ~(VM_BATCH_PER_VIEW | VM_BATCH_SECONDARY)) return fail(ctx, VM_E_INVALID, "unknown batch mode %d", mode);
+  const bool secondary = (mode & VM_BATCH_SECONDARY) != 0;
+  if ((mode & VM_BATCH_PER_VIEW) == 0) {
     // every view in one pipeline: one launch per stage, replayed from a graph
+    if (ctx->graph_exec && ctx->graph_secondary != secondary) drop_graph(ctx);
     if (!ctx->graph_exec) {
       CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-      const vmk::PipeArgs a = batch_args(ctx);
+      const vmk::PipeArgs a = batch_args(ctx, secondary);
       const cudaError_t le = vmk::launch_pipeline(a, ctx->tuning, ctx->b_underwater, false, ctx->sms, ctx->stream);
       cudaGraph_t g = nullptr;
       const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
       if (le != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(ctx, le, "launch_pipeline"); }
       if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
       ctx->graph = g;
+      ctx->graph_secondary = secondary;
       CK(cudaGraphInstantiate(&ctx->graph_exec, g, 0));
     }
     CK(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
     return VM_OK;
   }
-  if (mode == 1) {
+  {
     // the baseline: one launch sequence per view (same kernels)
-    const vmk::PipeArgs base = batch_args(ctx);
+    const vmk::PipeArgs base = batch_args(ctx, secondary);
     for (uint32_t v = 0; v < ctx->b_n_views; ++v) {
       vmk::PipeArgs a = base;
       const ViewDesc& d = ctx->bh_views[v];
@@ -666,7 +671,6 @@ int vm_batch_run(vm_ctx* ctx, int mode) {
     }
     return VM_OK;
   }
-  return fail(ctx, VM_E_INVALID, "unknown batch mode %d", mode);
 }
 
 int vm_batch_read(vm_ctx* ctx, uint64_t* vis, float* shadow) {
@@ -679,6 +683,15 @@ int vm_batch_read(vm_ctx* ctx, uint64_t* vis, float* shadow) {
 }
 
 uint64_t vm_batch_pixels(const vm_ctx* ctx) { return ctx ? ctx->b_pixels : 0; }
+
+int vm_batch_read_secondary(vm_ctx* ctx, uint64_t* key, float* t) {
+  if (!ctx || ctx->b_n_views == 0) return VM_E_NOT_READY;
+  int rc = VM_OK;
+  if (key) rc = read_dev(ctx, key, ctx->b_seck.p, ctx->b_pixels * 8);
+  if (rc) return rc;
+  if (t) rc = read_dev(ctx, t, ctx->b_sect.p, ctx->b_pixels * 4);
+  return rc;
+}
 
 int vm_device_buffers(vm_ctx* ctx, vm_device_ptrs* out) {
   if (!ctx || !out) return VM_E_INVALID;
@@ -696,3 +709,15 @@ int vm_sync(vm_ctx* ctx) {
 }
 
 }  // extern "C"
+
+// The batch's pipeline arguments (with the secondary-ray outputs) and stream,
+// for the shading G-buffer pass (gbuffer.cu).
+int vm_internal_batch_args(vm_ctx* ctx, vmk::PipeArgs* out, uint64_t* pixels, void** stream) {
+  if (!ctx || !out || !pixels || !stream) return VM_E_INVALID;
+  if (ctx->b_n_views == 0) return fail(ctx, VM_E_NOT_READY, "no batch set");
+  CK(cudaSetDevice(ctx->device));
+  *out = batch_args(ctx, true);
+  *pixels = ctx->b_pixels;
+  *stream = (void*)ctx->stream;
+  return VM_OK;
+}

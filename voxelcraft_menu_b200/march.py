@@ -208,8 +208,10 @@ class Marcher:
                                       ptr(grids), ptr(glens)))
         self.batch_views = views
 
-    def batch_run(self, per_view: bool = False):
-        self._ck(self._L.vm_batch_run(self._h, 1 if per_view else 0))
+    def batch_run(self, per_view: bool = False, secondary: bool = False):
+        """All views in one graph-replayed pipeline, or (per_view) one launch
+        sequence per view; secondary also traces the water / glass rays."""
+        self._ck(self._L.vm_batch_run(self._h, (1 if per_view else 0) | (2 if secondary else 0)))
 
     def batch_pixels(self) -> int:
         return int(self._L.vm_batch_pixels(self._h))
@@ -220,6 +222,13 @@ class Marcher:
         sh = np.empty(n, np.float32)
         self._ck(self._L.vm_batch_read(self._h, ptr(vis), ptr(sh)))
         return vis, sh
+
+    def batch_read_secondary(self):
+        n = self.batch_pixels()
+        k = np.empty(n, np.uint64)
+        t = np.empty(n, np.float32)
+        self._ck(self._L.vm_batch_read_secondary(self._h, ptr(k), ptr(t)))
+        return k, t
 
 
 class Renderer:

@@ -153,6 +153,10 @@ _SIGNATURES = [
     ("vm_batch_run", C.c_int, [vp, C.c_int]),
     ("vm_batch_read", C.c_int, [vp, vp, vp]),
     ("vm_batch_pixels", C.c_uint64, [vp]),
+    ("vm_batch_read_secondary", C.c_int, [vp, vp, vp]),
+    ("vm_shade_gbuffer", C.c_int, [vp, vp, vp]),
+    ("vm_shade_forward", C.c_int, [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]),
+    ("vm_shade_backward", C.c_int, [vp, C.c_uint64, vp, vp, vp, vp, vp, vp, vp]),
     ("vm_device_buffers", C.c_int, [vp, P(VmDevicePtrs)]),
     ("vm_sync", C.c_int, [vp]),
     ("vm_render_static", C.c_int, [P(VmFrame), vp, C.c_uint32, vp, C.c_uint64, vp, C.c_uint64, vp, C.c_uint64,
