@@ -172,6 +172,137 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+STAGES = ("cull", "primary", "shadow", "secondary")
+
+
+def stage_bytes(traffic, npix):
+    """Algorithmic bytes per launch of each timed stage: the traversal's
+    fetches (the layout's element sizes), plus what the stage reads and
+    writes per ray: tile-list entries (2 B) and the visibility key (8 B) and
+    queue items (24 B shadow, 40 B secondary) for the primary kernel; the
+    queue item read and the 4 B result for the shadow and secondary kernels."""
+    sb = traffic["stage_bytes"]
+    rs, rsec = traffic["rays_shadow"], traffic["rays_secondary"]
+    return {
+        "primary": sb[0] + 2 * traffic["list_entries"] + 8 * npix + 24 * rs + 40 * rsec,
+        "shadow": sb[1] + (24 + 4) * rs,
+        "secondary": sb[2] + (40 + 12) * rsec,
+    }
+
+
+def bench_batched(local, steps, warmup):
+    """Probe cube captures and player views over the 256x128x256 world: one
+    persistent graph-replayed launch against one launch sequence per view."""
+    import torch
+    from voxelcraft_menu_b200 import tuning
+    from voxelcraft_menu_b200 import views as V
+    from voxelcraft_menu_b200 import world as W
+    from voxelcraft_menu_b200.march import Marcher
+    w = W.World.generate(W.recipe_small_terrain())
+    views = V.probe_views(w) + V.player_views(w)
+    px = sum(v.n_pixels for v in views)
+    m = Marcher(1920, 1080, device=local, max_views=len(views), max_batch_pixels=px)
+    stream = torch.cuda.current_stream()
+    m._ck(m._L.vm_set_stream(m._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
+    m.upload_world(*w.pools())
+    m.batch_set(views)
+    best = tuning.autotune_batch(m)
+    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"])
+    traffic = m.batch_counted()
+    rays = traffic["rays_primary"] + traffic["rays_shadow"]
+
+    def timed(per_view):
+        for _ in range(warmup):
+            m.batch_run(per_view=per_view)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            m.batch_run(per_view=per_view)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_batch = timed(False)
+    out_batch = m.batch_read()
+    ms_views = timed(True)
+    out_views = m.batch_read()
+    identical = all(np.array_equal(a, b) for a, b in zip(out_batch, out_views))
+    m.close()
+    return {"workload": f"{len(views)} views ({len(views) - 4} probe cube faces of 32^2..256^2 + 4 x 1920x1080 "
+                        f"players) over the 256x128x256 world, primary + shadow rays",
+            "pixels": px, "rays_per_step": rays, "value": rays / (ms_batch * 1e-3) / 1e9, "unit": UNIT,
+            "ms_per_step": ms_batch, "per_view": {"value": rays / (ms_views * 1e-3) / 1e9, "ms_per_step": ms_views},
+            "ratio": ms_views / ms_batch, "identical_output": identical, "tuning": best,
+            "steps": steps, "warmup": warmup,
+            "l2": "not flushed: each step writes 12 B x %d pixels (> 126 MB L2)" % px}
+
+
+def bench_shading(local, steps, warmup):
+    """Forward, adjoint and fused loss + gradient of the shading stage over 8
+    views at 960x540 of the 256x128x256 world (one G-buffer, 4.15 Mpx)."""
+    import torch
+    from voxelcraft_menu_b200 import shading as S
+    from voxelcraft_menu_b200 import world as W
+    from voxelcraft_menu_b200.march import Marcher
+    w = W.World.generate(W.recipe_small_terrain())
+    views = S.shade_views(w)
+    m = Marcher(1920, 1080, device=local, max_views=len(views), max_batch_pixels=sum(v.n_pixels for v in views))
+    stream = torch.cuda.current_stream()
+    m._ck(m._L.vm_set_stream(m._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
+    m.upload_world(*w.pools())
+    m.batch_set(views)
+    m.batch_run(secondary=True)
+    k = S.consts()
+    gb = S.gbuffer(m, k, torch)
+    p0 = S.default_params()
+    p = torch.from_numpy(p0).cuda()
+    target, _ = S.forward(gb, torch.from_numpy(S.perturbed(p0)).cuda(), k, torch)
+    gcol = torch.randn_like(target)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.mean(ms))
+
+    n = len(views)
+    fwd = timed(lambda: S.forward(gb, p, k, torch))
+    fwd_loss = timed(lambda: S.forward(gb, p, k, torch, target=target))
+    bwd = timed(lambda: S.backward(gb, p, k, torch, grad_color=gcol))
+    fused = timed(lambda: S.backward(gb, p, k, torch, target=target, with_loss=True))
+    npx = gb.numel() // S.GBUF_BYTES
+    m.close()
+    return {"workload": "8 views x 960x540 over the 256x128x256 world (4.15 Mpx), 778 parameters",
+            "fwd_ms_per_view": fwd / n, "bwd_ms_per_view": bwd / n,
+            "fwd_bwd_ms_per_view": (fwd + bwd) / n, "fwd_bwd_over_fwd": (fwd + bwd) / fwd,
+            "loss_fwd_ms_per_view": fwd_loss / n, "fused_loss_grad_ms_per_view": fused / n,
+            "fused_over_loss_fwd": fused / fwd_loss,
+            "fwd_gbs": npx * (16 + 12) / (fwd * 1e-3) / 1e9, "fused_gbs": npx * (16 + 12) / (fused * 1e-3) / 1e9,
+            "grad_check": "FP64 oracle gradient and central differences: tests/test_shading.py (rel err <= 1e-4)",
+            "l2": "flushed between timed steps (256 MB write)"}
+
+
+def profile_traffic(kernel):
+    """dram bytes per launch of kernel from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / f"{kernel}_1080p.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -181,6 +312,8 @@ def main():
     ap.add_argument("--warps", type=int, default=0, help="primary kernel warps per block (0: autotune)")
     ap.add_argument("--reg-level", type=int, default=0, help="primary kernel register level with --warps")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched probe views")
+    ap.add_argument("--no-shade", action="store_true", help="skip the shading forward / adjoint")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -207,7 +340,7 @@ def main():
     m._ck(m._L.vm_set_stream(m._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
     m.upload_world(*pools)
 
-    # tile shape / CTAs per SM: autotuned on this frame unless fixed
+    # warps per block / register budget of the primary kernel: autotuned on this frame unless fixed
     if args.warps > 0:
         best = {"warps": args.warps, "reg_level": args.reg_level, "ctas_per_sm": 0}
     else:
@@ -224,21 +357,25 @@ def main():
     for _ in range(args.warmup):
         m.render()
     torch.cuda.synchronize(dev)
+    # five events per step, recorded by the library between its stages
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
+    for row in evs:
+        for e in row:
+            e.record(stream)   # creates the underlying CUDA event
+    torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     torch.cuda.synchronize(dev)
     for i in range(args.steps):
         flush.zero_()
-        starts[i].record(stream)
-        m.render()
-        ends[i].record(stream)
+        m.render_events([e.cuda_event for e in evs[i]])
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
-    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = [row[0].elapsed_time(row[4]) for row in evs]
+    stage_ms = {name: float(np.mean([row[j].elapsed_time(row[j + 1]) for row in evs]))
+                for j, name in enumerate(STAGES)}
     ms_step = float(np.mean(ms))
     if world > 1:
         t = torch.tensor([ms_step], device=dev)
@@ -288,10 +425,19 @@ def main():
     h2d = vb.chunks.nbytes + vb.grid.nbytes + 352
     d2h = npix * 12
 
-    algo_bytes = sum(traffic[k] * b for k, b in BYTES.items()) + npix * OUT_BYTES_PER_PIXEL
+    # roofline of the dominant kernel: its algorithmic bytes per launch over
+    # its own event-timed duration
+    sbytes = stage_bytes(traffic, npix)
+    top = max(sbytes, key=lambda k: stage_ms[k])
     peak, peak_kind = peaks()
-    achieved = algo_bytes / (ms_step * 1e-3) / 1e9
+    achieved = sbytes[top] / (stage_ms[top] * 1e-3) / 1e9
     stats = m.stats()
+    m.close()
+    extra = {}
+    if rank == 0 and not args.no_batch:
+        extra["batched"] = bench_batched(local, max(3, min(args.steps, 5)), 3)
+    if rank == 0 and not args.no_shade:
+        extra["shading"] = bench_shading(local, max(5, min(args.steps, 20)), 5)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -300,23 +446,26 @@ def main():
             "config": {"workload": WORKLOAD, "resolution": [1920, 1080], "chunks": int(len(vb.chunks)),
                        "tuning": best, "l2": "flushed between timed steps (256 MB write)",
                        "parallelism": f"replicas x{world}"},
+            "stage_ms": stage_ms,
             "work_per_step": traffic,
             "rays_per_step": {"primary": traffic["rays_primary"], "shadow": traffic["rays_shadow"],
                               "secondary_uncounted": traffic["rays_secondary"]},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": algo_bytes, "dda_steps_per_launch": traffic["iters"],
-                         "bytes_per_dda_step": algo_bytes / max(traffic["iters"], 1)},
+            "roofline": {"bound": "hbm", "kernel": f"k_{top}" if top != "primary" else "k_primary",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic(top), "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": sbytes[top], "launch_ms": stage_ms[top],
+                         "dda_steps_per_launch": traffic["stage_iters"][STAGES.index(top) - 1],
+                         "bytes_per_dda_step": sbytes[top] / max(traffic["stage_iters"][STAGES.index(top) - 1], 1)},
             "e2e": {"value": world * rays / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
             "gpu_launches": 5 * args.steps,   # bounds, cull, primary, shadow, secondary per frame
             "clocks": clocks,
             "device_error": int(stats.device_error),
         }
+        line.update(extra)
         if not args.no_cpu:
             line["cpu_baseline"] = cpu_sample(vb, pools)
         print(json.dumps(line), flush=True)
-    m.close()
     if world > 1:
         dist.destroy_process_group()
 

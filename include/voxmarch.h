@@ -126,8 +126,18 @@ typedef struct vm_traffic {
   uint64_t list_entries;    /* tile-list entries the primary rays examined */
   uint64_t stage_iters[3];  /* DDA steps of the primary, shadow and secondary rays */
   uint64_t stage_chunks[3]; /* chunk marches of the primary, shadow and secondary rays */
+  uint64_t stage_bytes[3];  /* algorithmic bytes of each stage's traversal: 96 per chunk record, 16 per L1
+                               node, 8 per leaf mask, 4 per attribute word, 12 per palette decode, 4 per
+                               grid lookup */
 } vm_traffic;
 int vm_render_counted(vm_ctx* ctx, vm_traffic* out);
+
+/* vm_render that also records five caller-created CUDA events (cudaEvent_t
+ * as void*) on the context's stream: at the start, after the tile cull, and
+ * after the primary, shadow and secondary kernels, so a caller can time each
+ * stage.  No counterpart in the engine, which times whole passes with
+ * timestamp queries (src/render/mod.rs:1593-1919). */
+int vm_render_events(vm_ctx* ctx, void* const* events);
 
 /* Batched views: many frames (each with its own chunk list and grid) marched
  * by one persistent work-stealing launch (VM_BATCH_PERSISTENT, replayed from
@@ -144,6 +154,9 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
                  const uint32_t* chunk_counts, const uint32_t* grids, const uint32_t* grid_lens);
 int vm_batch_run(vm_ctx* ctx, int mode);
 int vm_batch_read(vm_ctx* ctx, uint64_t* vis, float* shadow);
+/* One instrumented run of the whole batch (as VM_BATCH_PERSISTENT, with the
+ * secondary rays when secondary != 0): same outputs, plus its traffic. */
+int vm_batch_counted(vm_ctx* ctx, int secondary, vm_traffic* out);
 /* the secondary rays' keys and distances of the last VM_BATCH_SECONDARY run */
 int vm_batch_read_secondary(vm_ctx* ctx, uint64_t* key, float* t);
 uint64_t vm_batch_pixels(const vm_ctx* ctx);

@@ -174,7 +174,7 @@ vmk::PipeArgs base_args(vm_ctx* ctx) {
 }
 
 // The single-view pipeline (frame and view descriptor by value).
-int enqueue_render(vm_ctx* ctx, bool count) {
+int enqueue_render(vm_ctx* ctx, bool count, const cudaEvent_t* ev = nullptr) {
   const vm_frame& f = ctx->frame;
   ViewDesc v;
   memset(&v, 0, sizeof v);
@@ -204,7 +204,7 @@ int enqueue_render(vm_ctx* ctx, bool count) {
   a.frame0 = f;
   a.view0 = v;
   const bool uw = (f.flags & VM_FLAG_UNDERWATER) != 0u;
-  CK(vmk::launch_pipeline(a, ctx->tuning, uw, count, ctx->sms, ctx->stream));
+  CK(vmk::launch_pipeline(a, ctx->tuning, uw, count, ctx->sms, ctx->stream, ev));
   return VM_OK;
 }
 
@@ -426,6 +426,18 @@ int vm_render(vm_ctx* ctx) {
   return enqueue_render(ctx, false);
 }
 
+static int read_traffic(vm_ctx* ctx, vm_traffic* out);
+
+int vm_render_events(vm_ctx* ctx, void* const* events) {
+  if (!ctx || !events) return VM_E_INVALID;
+  for (int i = 0; i < 5; ++i)
+    if (!events[i]) return fail(ctx, VM_E_INVALID, "event %d is null", i);
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  return enqueue_render(ctx, false, (const cudaEvent_t*)events);
+}
+
 int vm_render_counted(vm_ctx* ctx, vm_traffic* out) {
   if (!ctx || !out) return VM_E_INVALID;
   int rc = check_ready(ctx);
@@ -433,6 +445,10 @@ int vm_render_counted(vm_ctx* ctx, vm_traffic* out) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaMemsetAsync(ctx->traffic.p, 0, 3 * sizeof(vmk::Traffic64), ctx->stream));
   if ((rc = enqueue_render(ctx, true))) return rc;
+  return read_traffic(ctx, out);
+}
+
+static int read_traffic(vm_ctx* ctx, vm_traffic* out) {
   vmk::Traffic64 st[3];
   CK(cudaMemcpyAsync(st, ctx->traffic.p, sizeof st, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -446,6 +462,9 @@ int vm_render_counted(vm_ctx* ctx, vm_traffic* out) {
   for (int s = 0; s < 3; ++s) {
     out->stage_iters[s] = st[s].iters;
     out->stage_chunks[s] = st[s].chunk;
+    // algorithmic bytes: the layout's element sizes times the fetches counted
+    out->stage_bytes[s] = 96ull * st[s].chunk + 16ull * st[s].l1 + 8ull * st[s].leaf + 4ull * st[s].attr +
+                          12ull * st[s].pal + 4ull * st[s].grid;
   }
   return VM_OK;
 }
@@ -671,6 +690,16 @@ int vm_batch_run(vm_ctx* ctx, int mode) {
     }
     return VM_OK;
   }
+}
+
+int vm_batch_counted(vm_ctx* ctx, int secondary, vm_traffic* out) {
+  if (!ctx || !out) return VM_E_INVALID;
+  if (ctx->b_n_views == 0) return fail(ctx, VM_E_NOT_READY, "no batch set");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemsetAsync(ctx->traffic.p, 0, 3 * sizeof(vmk::Traffic64), ctx->stream));
+  const vmk::PipeArgs a = batch_args(ctx, secondary != 0);
+  CK(vmk::launch_pipeline(a, ctx->tuning, ctx->b_underwater, true, ctx->sms, ctx->stream));
+  return read_traffic(ctx, out);
 }
 
 int vm_batch_read(vm_ctx* ctx, uint64_t* vis, float* shadow) {

@@ -88,8 +88,10 @@ struct PipeTuning {
   int reg_level;         // register budget: 0 unconstrained, 1 ~80, 2 64 registers per thread
   int ctas_per_sm;       // resident blocks per SM of the persistent primary kernel; 0 = occupancy max
 };
+// ev (optional): five events recorded at the start, after the cull, after the
+// primary, shadow and secondary kernels.
 cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwater, bool count, int sms,
-                            cudaStream_t s);
+                            cudaStream_t s, const cudaEvent_t* ev = nullptr);
 int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count);
 
 }  // namespace vmk

@@ -400,14 +400,21 @@ int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count) {
 }
 
 cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwater, bool count, int sms,
-                            cudaStream_t s) {
+                            cudaStream_t s, const cudaEvent_t* ev) {
   cudaError_t e;
+  const auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s) : cudaSuccess; };
+  if ((e = mark(0)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(a.work, 0, W_WORDS * sizeof(uint32_t), s)) != cudaSuccess) return e;
-  if (a.total_tiles == 0) return cudaSuccess;
+  if (a.total_tiles == 0) {
+    for (int i = 1; i < 5; ++i)
+      if ((e = mark(i)) != cudaSuccess) return e;
+    return cudaSuccess;
+  }
   if ((e = cudaMemsetAsync(a.hiz, 0xFF, (size_t)a.total_tiles * 4, s)) != cudaSuccess) return e;
   k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
   const uint32_t cull_blocks = std::min<uint32_t>((a.total_tiles + 7) / 8, (uint32_t)sms * 16u);
   k_cull<<<cull_blocks, 256, 0, s>>>(a);
+  if ((e = mark(1)) != cudaSuccess) return e;
   void* fn = primary_kernel(t, underwater, count);
   if (!fn) return cudaErrorInvalidValue;
   const int nw = block_warps(t, count);
@@ -417,15 +424,18 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   const uint32_t grid = std::min<uint32_t>((uint32_t)sms * (uint32_t)per, items_blocks);
   void* args[] = {(void*)&a};
   if ((e = cudaLaunchKernel(fn, dim3(grid), dim3(nw * 32), args, 0, s)) != cudaSuccess) return e;
+  if ((e = mark(2)) != cudaSuccess) return e;
   const uint32_t q_blocks = (uint32_t)sms * 8u;
   if (a.do_shadow) {
     if (count) k_shadow<true><<<q_blocks, 256, 0, s>>>(a);
     else k_shadow<false><<<q_blocks, 256, 0, s>>>(a);
   }
+  if ((e = mark(3)) != cudaSuccess) return e;
   if (a.do_secondary) {
     if (count) k_secondary_q<true><<<q_blocks, 256, 0, s>>>(a);
     else k_secondary_q<false><<<q_blocks, 256, 0, s>>>(a);
   }
+  if ((e = mark(4)) != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(256) k_shade_fwd(const GBuf* __restrict__ gb, 
   __syncthreads();
   float inv_len;
   const F3 sn = sun_unit(sP, &inv_len);
-  double acc = 0.0;
+  float acc = 0.0f;           // a few dozen terms per thread; the block sum is FP64
   const uint64_t step = (uint64_t)gridDim.x * blockDim.x * FPF;
   for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x * FPF + threadIdx.x; i0 < n; i0 += step) {
     GBuf gv[FPF];
@@ -210,13 +210,14 @@ __global__ void __launch_bounds__(256) k_shade_fwd(const GBuf* __restrict__ gb, 
       shade_px<false>(gv[u], sP, k, sn, c, nullptr, false, nullptr);
       if (color) { color[3 * i] = c[0]; color[3 * i + 1] = c[1]; color[3 * i + 2] = c[2]; }
       if (target) {
-        for (int ch = 0; ch < 3; ++ch) { const double e = (double)c[ch] - (double)target[3 * i + ch]; acc += e * e; }
+        for (int ch = 0; ch < 3; ++ch) { const float e = c[ch] - target[3 * i + ch]; acc += e * e; }
       }
     }
   }
   if (loss) {
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xFFFFFFFFu, acc, o);
-    if ((threadIdx.x & 31u) == 0) sLoss[threadIdx.x >> 5] = acc;
+    double a = acc;
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xFFFFFFFFu, a, o);
+    if ((threadIdx.x & 31u) == 0) sLoss[threadIdx.x >> 5] = a;
     __syncthreads();
     if (threadIdx.x == 0) {
       double s = 0.0;

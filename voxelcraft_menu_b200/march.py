@@ -129,10 +129,28 @@ class Marcher:
     def render_counted(self) -> dict:
         t = VmTraffic()
         self._ck(self._L.vm_render_counted(self._h, C.byref(t)))
+        return self._traffic(t)
+
+    def batch_counted(self, secondary: bool = False) -> dict:
+        t = VmTraffic()
+        self._ck(self._L.vm_batch_counted(self._h, 1 if secondary else 0, C.byref(t)))
+        return self._traffic(t)
+
+    @staticmethod
+    def _traffic(t) -> dict:
         out = {n: int(getattr(t, n)) for n, _ in VmTraffic._fields_[:11]}
         out["stage_iters"] = [int(x) for x in t.stage_iters]
         out["stage_chunks"] = [int(x) for x in t.stage_chunks]
+        out["stage_bytes"] = [int(x) for x in t.stage_bytes]
         return out
+
+    def render_events(self, events):
+        """render() recording five CUDA events (start, after the cull, after
+        the primary, shadow and secondary kernels); events are raw
+        cudaEvent_t handles (e.g. torch.cuda.Event().cuda_event after a
+        first record)."""
+        arr = (C.c_void_p * 5)(*events)
+        self._ck(self._L.vm_render_events(self._h, arr))
 
     def sync(self):
         self._ck(self._L.vm_sync(self._h))

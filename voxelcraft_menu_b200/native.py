@@ -112,7 +112,7 @@ class VmTraffic(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("chunk_records", "l1_fetches", "leaf_fetches", "attr_fetches",
                                           "palette_decodes", "grid_lookups", "iters", "rays_primary",
                                           "rays_shadow", "rays_secondary", "list_entries")] + \
-               [("stage_iters", C.c_uint64 * 3), ("stage_chunks", C.c_uint64 * 3)]
+               [("stage_iters", C.c_uint64 * 3), ("stage_chunks", C.c_uint64 * 3), ("stage_bytes", C.c_uint64 * 3)]
 
 
 class VmDevicePtrs(C.Structure):
@@ -149,11 +149,13 @@ _SIGNATURES = [
     ("vm_read_expanded", C.c_int, [vp, vp, vp, vp, vp, vp]),
     ("vm_stats_read", C.c_int, [vp, P(VmStats)]),
     ("vm_render_counted", C.c_int, [vp, P(VmTraffic)]),
+    ("vm_render_events", C.c_int, [vp, P(vp)]),
     ("vm_batch_set", C.c_int, [vp, C.c_uint32, vp, vp, vp, vp, vp]),
     ("vm_batch_run", C.c_int, [vp, C.c_int]),
     ("vm_batch_read", C.c_int, [vp, vp, vp]),
     ("vm_batch_pixels", C.c_uint64, [vp]),
     ("vm_batch_read_secondary", C.c_int, [vp, vp, vp]),
+    ("vm_batch_counted", C.c_int, [vp, C.c_int, P(VmTraffic)]),
     ("vm_shade_gbuffer", C.c_int, [vp, vp, vp]),
     ("vm_shade_forward", C.c_int, [vp, C.c_uint64, vp, vp, vp, vp, vp, vp]),
     ("vm_shade_backward", C.c_int, [vp, C.c_uint64, vp, vp, vp, vp, vp, vp, vp]),
