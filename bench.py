@@ -132,13 +132,15 @@ def cpu_sample(view, pools, budget_s=12.0):
     o = Oracle(view, *pools)
     ty = int(view.frame.tiles[1])
     t_total, rays, px, rows, row0 = 0.0, 0, 0, 2, ty // 2 - 8
-    while t_total < budget_s and row0 < ty:
+    while t_total < budget_s:
+        if row0 >= ty:
+            row0 = 0          # the whole frame again until the budget is spent
         dt, r, p = oracle_rows(o, view, row0, rows)
         t_total += dt
         rays += r
         px += p
         row0 += rows
-        rows *= 2
+        rows = min(rows * 2, 32)
     return {"value": rays / t_total / 1e9, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
             "sample": f"oracle (engine pass sequence restated in C++, OpenMP) over the middle tile rows of the "
                       f"same frame: {px} pixels, {rays} primary+shadow rays in {t_total:.1f}s"}

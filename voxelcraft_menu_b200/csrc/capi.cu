@@ -39,10 +39,10 @@ struct vm_ctx {
   bool have_frame = false;
   // per-frame outputs and scratch
   DevBuf vis, shadow, sec_key, sec_t, hiz, dbg, pairs, counters, err, work, dkmax, sufmax, traffic, expand;
-  DevBuf tile_list, tile_count, shadow_q, sec_q;
+  DevBuf tile_list, tile_count, shadow_q, sec_q, item_cost, tile_order;
   // batch
   DevBuf b_frames, b_views, b_views1, b_chunks, b_grids, b_vis, b_shadow, b_seck, b_sect, b_hiz, b_dkmax, b_sufmax;
-  DevBuf b_tile_list, b_tile_count, b_shadow_q, b_sec_q;
+  DevBuf b_tile_list, b_tile_count, b_shadow_q, b_sec_q, b_item_cost, b_tile_order;
   std::vector<vm_frame> bh_frames;
   std::vector<ViewDesc> bh_views;
   uint32_t b_n_views = 0, b_total_tiles = 0, b_n_chunks = 0, b_list_cap = 1;
@@ -166,6 +166,8 @@ vmk::PipeArgs base_args(vm_ctx* ctx) {
   a.bricks = (const uint32_t*)ctx->bricks.p; a.n_bricks = ctx->n_bricks;
   a.err = (uint32_t*)ctx->err.p;
   a.work = (uint32_t*)ctx->work.p;
+  a.item_cost = (uint32_t*)ctx->item_cost.p;
+  a.tile_order = (uint32_t*)ctx->tile_order.p;
   a.traffic = (vmk::Traffic64*)ctx->traffic.p;
   a.do_shadow = 1;
   a.do_secondary = 1;
@@ -238,7 +240,9 @@ int vm_create(int device_ordinal, const vm_caps* caps, vm_ctx** out) {
   rc |= ensure(ctx, ctx->hiz, tiles * 4);
   rc |= ensure(ctx, ctx->counters, 64);
   rc |= ensure(ctx, ctx->err, 64);
-  rc |= ensure(ctx, ctx->work, 64);
+  rc |= ensure(ctx, ctx->work, vmk::W_WORDS * sizeof(uint32_t));
+  rc |= ensure(ctx, ctx->item_cost, tiles * 8);
+  rc |= ensure(ctx, ctx->tile_order, tiles * 4);
   rc |= ensure(ctx, ctx->traffic, 3 * sizeof(vmk::Traffic64));
   rc |= ensure(ctx, ctx->dkmax, (size_t)ctx->caps.max_chunks * 4);
   rc |= ensure(ctx, ctx->sufmax, (size_t)ctx->caps.max_chunks * 4);
@@ -248,6 +252,7 @@ int vm_create(int device_ordinal, const vm_caps* caps, vm_ctx** out) {
   rc |= ensure(ctx, ctx->sec_q, npix * sizeof(vmk::SecItem));
   if (rc != VM_OK) { vm_destroy(ctx); return VM_E_CUDA; }
   cudaMemsetAsync(ctx->hiz.p, 0, tiles * 4, ctx->stream);
+  cudaMemsetAsync(ctx->item_cost.p, 0, tiles * 8, ctx->stream);
   cudaMemsetAsync(ctx->err.p, 0, 64, ctx->stream);
   cudaMemsetAsync(ctx->counters.p, 0, 64, ctx->stream);
   cudaStreamSynchronize(ctx->stream);
@@ -266,7 +271,8 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->b_views, &ctx->b_views1, &ctx->b_chunks, &ctx->b_grids, &ctx->b_vis, &ctx->b_shadow,
                    &ctx->b_seck, &ctx->b_sect, &ctx->b_hiz, &ctx->b_dkmax, &ctx->b_sufmax, &ctx->tile_list,
                    &ctx->tile_count, &ctx->shadow_q, &ctx->sec_q, &ctx->b_tile_list, &ctx->b_tile_count,
-                   &ctx->b_shadow_q, &ctx->b_sec_q};
+                   &ctx->b_shadow_q, &ctx->b_sec_q, &ctx->item_cost, &ctx->tile_order, &ctx->b_item_cost,
+                   &ctx->b_tile_order};
   for (DevBuf* b : all) release(*b);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
@@ -608,7 +614,10 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
   rc |= ensure(ctx, ctx->b_tile_count, tiles * 4);
   rc |= ensure(ctx, ctx->b_shadow_q, pix * sizeof(vmk::ShadowItem));
   rc |= ensure(ctx, ctx->b_sec_q, pix * sizeof(vmk::SecItem));
+  rc |= ensure(ctx, ctx->b_item_cost, tiles * 8);
+  rc |= ensure(ctx, ctx->b_tile_order, tiles * 4);
   if (rc) return VM_E_CUDA;
+  CK(cudaMemsetAsync(ctx->b_item_cost.p, 0, tiles * 8, ctx->stream));   // a new batch: no costs yet
   CK(cudaMemcpyAsync(ctx->b_frames.p, frames, n_views * sizeof(vm_frame), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->b_chunks.p, chunks, chunk_total * sizeof(vm_chunk), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->b_grids.p, grids, grid_total * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -647,6 +656,8 @@ static vmk::PipeArgs batch_args(vm_ctx* ctx, bool secondary) {
   a.hiz = (uint32_t*)ctx->b_hiz.p;
   a.shadow_q = (vmk::ShadowItem*)ctx->b_shadow_q.p;
   a.sec_q = (vmk::SecItem*)ctx->b_sec_q.p;
+  a.item_cost = (uint32_t*)ctx->b_item_cost.p;
+  a.tile_order = (uint32_t*)ctx->b_tile_order.p;
   a.do_secondary = secondary ? 1 : 0;   // batched views: primary + shadow, optionally the water / glass rays
   return a;
 }
@@ -686,6 +697,8 @@ int vm_batch_run(vm_ctx* ctx, int mode) {
       a.n_views = 1;
       a.total_tiles = d.tiles_x * d.tiles_y;
       a.hiz = (uint32_t*)ctx->b_hiz.p + d.tile_begin;
+      a.item_cost = (uint32_t*)ctx->b_item_cost.p + 2ull * d.tile_begin;
+      a.tile_order = (uint32_t*)ctx->b_tile_order.p + d.tile_begin;
       CK(vmk::launch_pipeline(a, ctx->tuning, ctx->b_underwater, false, ctx->sms, ctx->stream));
     }
     return VM_OK;

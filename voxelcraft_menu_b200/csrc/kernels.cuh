@@ -30,7 +30,22 @@ struct ShadowItem { uint32_t view, pix; float o[3]; uint32_t pad; };            
 struct SecItem { uint32_t view, pix; float o[3], d[3]; float max_dist; uint32_t water; };  // 40 B
 
 // Pipeline counters (zeroed before each frame)
-enum : int { W_PRIMARY = 0, W_SHADOW_N = 1, W_SEC_N = 2, W_WORDS = 4 };
+// Cost order of the primary kernel's work.  Consecutive launches over the
+// same tiles (the next frame, a replayed batch) see nearly the same rays, so
+// the primary kernel records each item's duration (SM cycles) and the next
+// launch takes the tiles in decreasing order of that cost: the few items
+// whose rays run long (up to the 512-step cap in a chunk, or through tree
+// canopies) start first instead of last, where they would hold the frame's
+// tail.  The order only decides when an item starts, never what it computes.
+constexpr uint32_t N_COST_BUCKETS = 16;
+__device__ __forceinline__ uint32_t cost_bucket(uint32_t cycles) {
+  // log2 buckets, 0 the most expensive (>= 2^20 cycles, about 0.5 ms)
+  const uint32_t lg = cycles ? 31u - (uint32_t)__clz(cycles) : 0u;
+  return lg >= 20u ? 0u : (lg <= 5u ? N_COST_BUCKETS - 1u : 20u - lg);
+}
+
+enum : int { W_PRIMARY = 0, W_SHADOW_N = 1, W_SEC_N = 2, W_HIST = 4, W_FILL = W_HIST + (int)N_COST_BUCKETS,
+             W_WORDS = W_FILL + (int)N_COST_BUCKETS };
 
 struct PipeArgs {
   const vm_frame* frames;      // one per view; nullptr: single view in frame0 / view0
@@ -55,6 +70,8 @@ struct PipeArgs {
   ShadowItem* shadow_q;
   SecItem* sec_q;
   uint32_t* work;              // W_* counters
+  uint32_t* item_cost;         // per primary item (2 per tile): SM cycles it took in the last launch
+  uint32_t* tile_order;        // per tile: tiles in decreasing order of that cost
   uint32_t* err;
   Traffic64* traffic;          // counting kernels only
   uint32_t do_shadow, do_secondary;

@@ -128,7 +128,26 @@ __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a
       }
       n += __popc(bal);
     }
-    if (lane == 0) a.tile_count[t] = n;
+    if (lane == 0) {
+      a.tile_count[t] = n;
+      const uint32_t c = max(a.item_cost[2u * t], a.item_cost[2u * t + 1u]);
+      atomicAdd(&a.work[W_HIST + cost_bucket(c)], 1u);
+    }
+  }
+}
+
+// The tiles in decreasing order of the last launch's cost (a counting sort
+// over the cost buckets; ties in any order).
+__global__ void __launch_bounds__(256) k_order(const __grid_constant__ PipeArgs a) {
+  __shared__ uint32_t start[N_COST_BUCKETS];
+  if (threadIdx.x == 0) {
+    uint32_t s = 0;
+    for (uint32_t b = 0; b < N_COST_BUCKETS; ++b) { start[b] = s; s += a.work[W_HIST + b]; }
+  }
+  __syncthreads();
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < a.total_tiles; t += gridDim.x * blockDim.x) {
+    const uint32_t b = cost_bucket(max(a.item_cost[2u * t], a.item_cost[2u * t + 1u]));
+    a.tile_order[start[b] + atomicAdd(&a.work[W_FILL + b], 1u)] = t;
   }
 }
 
@@ -208,7 +227,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
     if (lane == 0) item = atomicAdd(&a.work[W_PRIMARY], 1u);
     item = __shfl_sync(FULLMASK, item, 0);
     if (item >= total) break;
-    const uint32_t t = item >> 1, half = item & 1u;
+    const long long clk0 = clock64();
+    const uint32_t t = a.tile_order[item >> 1], half = item & 1u;
     const uint32_t v = find_view(a, t);
     const vm_frame& f = frame_of(a, v);
     const ViewDesc vd = view_of(a, v);
@@ -313,6 +333,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
         }
       }
     }
+    if (lane == 0) a.item_cost[2u * t + half] = (uint32_t)min(clock64() - clk0, 0xFFFFFFFFll);
   }
   flush_traffic<COUNT>(a, 0, tr, np, ns, nx);
 }
@@ -414,6 +435,7 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
   const uint32_t cull_blocks = std::min<uint32_t>((a.total_tiles + 7) / 8, (uint32_t)sms * 16u);
   k_cull<<<cull_blocks, 256, 0, s>>>(a);
+  k_order<<<std::min<uint32_t>((a.total_tiles + 255) / 256, (uint32_t)sms * 4u), 256, 0, s>>>(a);
   if ((e = mark(1)) != cudaSuccess) return e;
   void* fn = primary_kernel(t, underwater, count);
   if (!fn) return cudaErrorInvalidValue;

@@ -36,6 +36,8 @@ struct StaticScratch {
   uint32_t dkmax[VM_MAX_CHUNKS + 1];
   uint32_t sufmax[VM_MAX_CHUNKS + 1];
   uint32_t tile_count[STATIC_MAX_TILES];
+  uint32_t item_cost[2 * STATIC_MAX_TILES];
+  uint32_t tile_order[STATIC_MAX_TILES];
   uint32_t hiz[STATIC_MAX_TILES];
   uint16_t tile_list[STATIC_MAX_TILES * STATIC_LIST_CAP];
   vmk::ShadowItem shadow_q[STATIC_MAX_PIXELS];
@@ -119,6 +121,8 @@ extern "C" int vm_render_static(const vm_frame* frame, const vm_chunk* d_chunks,
   a.sufmax = s->sufmax;
   a.tile_list = s->tile_list;
   a.tile_count = s->tile_count;
+  a.item_cost = s->item_cost;
+  a.tile_order = s->tile_order;
   a.list_cap = STATIC_LIST_CAP;
   a.vis = reinterpret_cast<unsigned long long*>(d_vis);
   a.shadow = d_shadow;
