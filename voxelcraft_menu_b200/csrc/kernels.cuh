@@ -44,7 +44,7 @@ __device__ __forceinline__ uint32_t cost_bucket(uint32_t cycles) {
   return lg >= 20u ? 0u : (lg <= 5u ? N_COST_BUCKETS - 1u : 20u - lg);
 }
 
-enum : int { W_PRIMARY = 0, W_SHADOW_N = 1, W_SEC_N = 2, W_HIST = 4, W_FILL = W_HIST + (int)N_COST_BUCKETS,
+enum : int { W_PRIMARY = 0, W_SHADOW_N = 1, W_SEC_N = 2, W_SHADOW_TAKE = 3, W_HIST = 4, W_FILL = W_HIST + (int)N_COST_BUCKETS,
              W_WORDS = W_FILL + (int)N_COST_BUCKETS };
 
 struct PipeArgs {

@@ -561,6 +561,57 @@ __device__ __noinline__ float shadow_ray_t(const DevWorld& w, const vm_frame& f,
   return -1.0f;
 }
 
+// shadow_ray_t one chunk-grid cell at a time, for kernels whose lanes take a
+// new ray as soon as theirs ends: the state between cells is the cell, the
+// last chunk marched and the step count, and each step is the loop body of
+// shadow_ray_t above, so the result is the same float.  Returns true when the
+// ray is over, with its blocker distance (-1: none) in *out.
+struct ShadowWalk {
+  Ray r;
+  int32_t cx, cy, cz;
+  uint32_t last, step;
+};
+__device__ __forceinline__ ShadowWalk shadow_walk_begin(F3 ro, F3 rd) {
+  ShadowWalk s;
+  s.r = make_ray(ro, rd);
+  s.cx = ffloor_i(ro.x * INV64); s.cy = ffloor_i(ro.y * INV64); s.cz = ffloor_i(ro.z * INV64);
+  s.last = VM_NO_CHUNK;
+  s.step = 0u;
+  return s;
+}
+template <bool COUNT>
+__device__ __forceinline__ bool shadow_walk_step(const DevWorld& w, const vm_frame& f, ShadowWalk& s, float max_dist,
+                                                 float* out, Traffic* tr) {
+  *out = -1.0f;
+  if (s.step >= 24u) return true;
+  uint64_t gi;
+  if (!grid_rel(f, s.cx, s.cy, s.cz, &gi)) return true;
+  if (COUNT) tr->grid++;
+  const uint32_t ci = ld_grid(w, gi);
+  if (ci != VM_NO_CHUNK && ci != s.last) {
+    s.last = ci;
+    const Chunk c = ld_chunk(w, ci);
+    const Hit m = march_chunk<true, true, true, COUNT>(w, f, c, s.r, max_dist, tr);
+    if (m.hit) { *out = m.t; return true; }
+  }
+  const Ray& r = s.r;
+  const float bx = (float)(r.pdx ? s.cx + 1 : s.cx) * 64.0f;
+  const float by = (float)(r.pdy ? s.cy + 1 : s.cy) * 64.0f;
+  const float bz = (float)(r.pdz ? s.cz + 1 : s.cz) * 64.0f;
+  const float tnx = (bx - r.o.x) * r.inv.x, tny = (by - r.o.y) * r.inv.y, tnz = (bz - r.o.z) * r.inv.z;
+  float t;
+  uint32_t axis = 0u;
+  if (tnx <= tny && tnx <= tnz) t = tnx;
+  else if (tny <= tnz) { t = tny; axis = 1u; }
+  else { t = tnz; axis = 2u; }
+  if (t >= max_dist) return true;
+  if (axis == 0) s.cx += r.pdx ? 1 : -1;
+  else if (axis == 1) s.cy += r.pdy ? 1 : -1;
+  else s.cz += r.pdz ? 1 : -1;
+  ++s.step;
+  return false;
+}
+
 struct WorldHit { bool hit; float t; uint32_t normal; uint32_t vx, vy, vz; uint32_t ci; };
 
 // trace_world: common.wgsl:1205-1253

@@ -137,18 +137,36 @@ __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a
 }
 
 // The tiles in decreasing order of the last launch's cost (a counting sort
-// over the cost buckets; ties in any order).
+// over the cost buckets; ties in any order).  Each block ranks its own
+// contiguous range of tiles in shared memory and reserves one range per
+// bucket with a single global atomic.
+constexpr uint32_t ORDER_TILES = 2048;   // tiles per block
 __global__ void __launch_bounds__(256) k_order(const __grid_constant__ PipeArgs a) {
-  __shared__ uint32_t start[N_COST_BUCKETS];
+  __shared__ uint32_t start[N_COST_BUCKETS], count[N_COST_BUCKETS], base[N_COST_BUCKETS];
+  const uint32_t t0 = blockIdx.x * ORDER_TILES, t1 = min(t0 + ORDER_TILES, a.total_tiles);
+  if (threadIdx.x < N_COST_BUCKETS) count[threadIdx.x] = 0u;
   if (threadIdx.x == 0) {
     uint32_t s = 0;
     for (uint32_t b = 0; b < N_COST_BUCKETS; ++b) { start[b] = s; s += a.work[W_HIST + b]; }
   }
   __syncthreads();
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < a.total_tiles; t += gridDim.x * blockDim.x) {
-    const uint32_t b = cost_bucket(max(a.item_cost[2u * t], a.item_cost[2u * t + 1u]));
-    a.tile_order[start[b] + atomicAdd(&a.work[W_FILL + b], 1u)] = t;
+  uint32_t bk[ORDER_TILES / 256], rank[ORDER_TILES / 256];
+#pragma unroll
+  for (uint32_t k = 0; k < ORDER_TILES / 256; ++k) {
+    const uint32_t t = t0 + k * 256u + threadIdx.x;
+    bk[k] = N_COST_BUCKETS;
+    if (t < t1) {
+      bk[k] = cost_bucket(max(a.item_cost[2u * t], a.item_cost[2u * t + 1u]));
+      rank[k] = atomicAdd(&count[bk[k]], 1u);
+    }
   }
+  __syncthreads();
+  if (threadIdx.x < N_COST_BUCKETS)
+    base[threadIdx.x] = count[threadIdx.x] ? atomicAdd(&a.work[W_FILL + threadIdx.x], count[threadIdx.x]) : 0u;
+  __syncthreads();
+#pragma unroll
+  for (uint32_t k = 0; k < ORDER_TILES / 256; ++k)
+    if (bk[k] < N_COST_BUCKETS) a.tile_order[start[bk[k]] + base[bk[k]] + rank[k]] = t0 + k * 256u + threadIdx.x;
 }
 
 // stage: 0 primary, 1 shadow, 2 secondary (a.traffic holds one record per stage)
@@ -338,19 +356,49 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
   flush_traffic<COUNT>(a, 0, tr, np, ns, nx);
 }
 
+// The sun shadow rays (shadow_ray_t, common.wgsl:1156-1195) of the queue.
+// Persistent lanes: each holds one ray and steps it one chunk-grid cell at a
+// time; a lane whose ray is over takes the next ray of the queue at once
+// (warp-aggregated), so a warp never idles behind its longest ray.
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ PipeArgs a) {
+__global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeArgs a) {
   const uint32_t n = a.work[W_SHADOW_N];
+  const uint32_t lane = threadIdx.x & 31u;
   Traffic tr = {};
   uint32_t ns = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const ShadowItem q = a.shadow_q[i];
-    const vm_frame& f = frame_of(a, q.view);
-    const ViewDesc vd = view_of(a, q.view);
-    const DevWorld w = world_of(a, vd);
-    const float b = shadow_ray_t<COUNT>(w, f, f3(q.o[0], q.o[1], q.o[2]), ld3(f.sun_dir), f.shadow_dist, &tr);
-    a.shadow[vd.pix_off + q.pix] = blocker_distance(b);
-    if (COUNT) ++ns;
+  bool has = false, drained = false;
+  uint32_t view = 0u, pix = 0u;
+  ShadowWalk s;
+  for (;;) {
+    const uint32_t need = __ballot_sync(FULLMASK, !has);
+    if (need && !drained) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&a.work[W_SHADOW_TAKE], __popc(need));
+      base = __shfl_sync(FULLMASK, base, 0);
+      drained = base + __popc(need) >= n;
+      if (!has) {
+        const uint32_t i = base + __popc(need & lanemask_lt());
+        if (i < n) {
+          const ShadowItem q = a.shadow_q[i];
+          view = q.view;
+          pix = q.pix;
+          s = shadow_walk_begin(f3(q.o[0], q.o[1], q.o[2]), ld3(frame_of(a, view).sun_dir));
+          has = true;
+          if (COUNT) ++ns;
+        }
+      }
+    }
+    if (__ballot_sync(FULLMASK, has) == 0u) break;
+    if (has) {
+      const vm_frame& f = frame_of(a, view);
+      const ViewDesc vd = view_of(a, view);
+      const DevWorld w = world_of(a, vd);
+      float b;
+      if (shadow_walk_step<COUNT>(w, f, s, f.shadow_dist, &b, &tr)) {
+        a.shadow[vd.pix_off + pix] = blocker_distance(b);
+        has = false;
+      }
+    }
   }
   flush_traffic<COUNT>(a, 1, tr, 0, ns, 0);
 }
@@ -435,7 +483,7 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
   const uint32_t cull_blocks = std::min<uint32_t>((a.total_tiles + 7) / 8, (uint32_t)sms * 16u);
   k_cull<<<cull_blocks, 256, 0, s>>>(a);
-  k_order<<<std::min<uint32_t>((a.total_tiles + 255) / 256, (uint32_t)sms * 4u), 256, 0, s>>>(a);
+  k_order<<<(a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256, 0, s>>>(a);
   if ((e = mark(1)) != cudaSuccess) return e;
   void* fn = primary_kernel(t, underwater, count);
   if (!fn) return cudaErrorInvalidValue;
