@@ -11,9 +11,18 @@ and one water-refraction / glass-transmission ray per water / glass hit.
 Metric: Grays/s of primary + shadow rays (secondary rays are traced but not
 counted).  `value` is measured on device-resident inputs; `e2e` goes through
 the C ABI with host buffers (frame + chunk list + grid uploaded, visibility
-and shadow buffers read back every step).
+and shadow buffers read back every step).  The library records CUDA events
+between its stages during the timed steps (`stage_ms`); `roofline` is the
+dominant kernel's algorithmic bytes per launch over its own event time.
+
+Two more measurements share the JSON line: `batched` (3072 probe cube faces
+of 32^2..256^2 plus four 1920x1080 player views over the 256x128x256 world,
+one graph-replayed persistent launch against one launch sequence per view,
+primary + shadow) and `shading` (forward, adjoint and fused loss + gradient
+of the differentiable shading stage over 8 views at 960x540).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                       [--no-batch] [--no-shade] [--no-cpu]
 Under torchrun every rank renders its own copy (replicas: the march does not
 shard a frame across GPUs); value is the total over ranks / max rank time.
 """
@@ -21,7 +30,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -37,11 +45,6 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Grays/s at 1080p (primary + shadow rays)"
 UNIT = "Grays/s"
 WORKLOAD = "1920x1080 frame over the 1024x256x1024 terrain (1024 chunks), Hi-Z frame moved 0.5 voxel"
-
-# algorithmic bytes per counted event (the layout's element sizes)
-BYTES = {"chunk_records": 96, "l1_fetches": 16, "leaf_fetches": 8, "attr_fetches": 4, "palette_decodes": 12,
-         "grid_lookups": 4}
-OUT_BYTES_PER_PIXEL = 8 + 4 + 8 + 4      # vis, shadow, secondary key, secondary t
 
 
 def dist_env():
@@ -296,7 +299,7 @@ def bench_shading(local, steps, warmup):
 
 def profile_traffic(kernel):
     """dram bytes per launch of kernel from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / f"{kernel}_1080p.md"
+    f = ROOT / "profiles" / f"k_{kernel}_1080p.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
