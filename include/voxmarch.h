@@ -217,7 +217,7 @@ int vm_sync(vm_ctx* ctx);
  * from their own arenas, allocation-free real-time paths.  The caller passes
  * every input and output as device pointers (pools, chunk list, grid, vis,
  * shadow, a zeroed u32 error word) on the current device and stream; the
- * pipeline's scratch is one static device array of about 7.5 MB per GPU.
+ * pipeline's scratch is one static device array of about 7.6 MB per GPU.
  * Primary and shadow rays only; at most 262144 pixels and 8192 8x8 tiles per
  * frame (larger frames return VM_E_CAPACITY).  The first call on a device
  * looks the array up and must come before any stream capture.  Every call

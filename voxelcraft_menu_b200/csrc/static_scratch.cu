@@ -9,7 +9,7 @@
 //
 // Limits and sharing rules:
 //  * at most STATIC_MAX_PIXELS pixels and STATIC_MAX_TILES 8x8 tiles per frame
-//    (larger frames are rejected with VM_E_CAPACITY); ~7.5 MB of device memory
+//    (larger frames are rejected with VM_E_CAPACITY); ~7.6 MB of device memory
 //    that every GPU loading this library keeps until the process exits;
 //  * primary and shadow rays only (no secondary rays, no Hi-Z output);
 //  * the scratch is shared by every call on a device and keeps the last call's
