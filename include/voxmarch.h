@@ -187,7 +187,8 @@ typedef struct vm_shade_consts {
 } vm_shade_consts;
 typedef struct vm_shade_gbuf {
   uint32_t code;           /* id | face << 8 | HIT 1<<11 | LIT 1<<12 | TRACED 1<<13 | HIT2 1<<14 | FLIP 1<<15
-                              | id2 << 16 | face2 << 24 (id2 / face2: the refracted ray's hit) */
+                              | id2 << 16 | face2 << 24 (id2 / face2: the refracted ray's hit)
+                              | blocked soft-shadow rays << 27 | SOFT 1<<30 (VM_FLAG_SOFT_SHADOWS) */
   float t;                 /* primary hit distance (0 for sky) */
   float d;                 /* water refraction leg length */
   float fog;               /* fog optical length per unit density (0 for sky) */

@@ -48,6 +48,7 @@ def lib():
             "or_last_error": (C.c_int, [C.c_char_p, C.c_int]),
             "or_clear_error": (None, []),
             "or_ray_dir": (None, [vp, C.c_float, C.c_float, vp]),
+            "or_soft_sun_dir": (None, [vp, C.c_uint32, C.c_uint32, C.c_uint32, vp]),
             "or_march_chunk": (C.c_int, [vp, C.c_uint32, vp, vp, C.c_float, C.c_uint32, C.c_uint32, C.c_uint32,
                                          C.c_uint32, C.POINTER(OrHit)]),
             "or_shadow_ray_t": (C.c_float, [vp, vp, vp, C.c_float]),
@@ -192,6 +193,11 @@ class Oracle:
     def ray_dir(self, px, py):
         out = np.zeros(3, np.float32)
         self.L.or_ray_dir(C.byref(self.frame), px, py, _p(out))
+        return out
+
+    def soft_sun_dir(self, px, py, s):
+        out = np.zeros(3, np.float32)
+        self.L.or_soft_sun_dir(C.byref(self.frame), px, py, s, _p(out))
         return out
 
     def depth_key(self, t):

@@ -18,6 +18,9 @@ NP = 778
 P_SUN, P_SKY, P_FOG, P_ABS = 768, 771, 774, 775
 WATER = 13
 G_HIT, G_LIT, G_TRACED, G_HIT2, G_FLIP = 1 << 11, 1 << 12, 1 << 13, 1 << 14, 1 << 15
+G_SOFT, G_SOFT_SHIFT = 1 << 30, 27        # soft shadows: blocked rays of SOFT_SAMPLES in bits 27-29
+SOFT_SAMPLES = 4
+FLAG_SOFT_SHADOWS = 0x40000000
 
 NORMALS = np.array([[-1, 0, 0], [1, 0, 0], [0, -1, 0], [0, 1, 0], [0, 0, -1], [0, 0, 1],
                     [0.70710678, 0, -0.70710678], [0.70710678, 0, 0.70710678]], np.float64)
@@ -55,6 +58,8 @@ def gbuffer_from_oracle(oracle, vis, shadow, sec_key, sec_t, fog_falloff, fog_he
         nid = (key >> 37) & 7
         bid = oracle.block_at(ci, v)
         c = (bid & 0xFF) | (nid << 8) | G_HIT | (G_LIT if shadow[i] == 0.0 else 0)
+        if int(f.flags) & FLAG_SOFT_SHADOWS:
+            c |= G_SOFT | (int(float(shadow[i]) * SOFT_SAMPLES + 0.5) << G_SOFT_SHIFT)
         nf = NORMALS[nid].astype(np.float32)
         if nid >= 6 and (nf[0] * rd[0] + nf[1] * rd[1]) + nf[2] * rd[2] > np.float32(0.0):
             c |= G_FLIP
@@ -84,7 +89,9 @@ class Model:
         self.hit = (code & G_HIT) != 0
         self.id = code & 0xFF
         self.nid = (code >> 8) & 7
-        self.lit = ((code & G_LIT) != 0).astype(np.float64)
+        soft = (code & G_SOFT) != 0
+        self.lit = np.where(soft, 1.0 - ((code >> G_SOFT_SHIFT) & 7) / SOFT_SAMPLES,
+                            ((code & G_LIT) != 0).astype(np.float64))
         self.traced = (code & G_TRACED) != 0
         self.hit2 = (code & G_HIT2) != 0
         self.id2 = (code >> 16) & 0xFF

@@ -292,6 +292,25 @@ inline uint32_t hash_u32(uint32_t x) {
   return h;
 }
 
+// Soft shadows (VM_FLAG_SOFT_SHADOWS, an extension of the engine): the s-th
+// jittered sun direction of pixel (px, py): the sun's tangent basis from a
+// fixed up vector, one rotation of the shared disk pattern picked by hash_u32
+// of pixel and frame, the offset added in the tangent plane, normalised.
+static const float SOFT_DISK[VM_SOFT_ROTATIONS][VM_SOFT_SAMPLES][2] = VM_SOFT_DISK_INIT;
+V3 soft_sun_dir(const vm_frame& f, uint32_t px, uint32_t py, uint32_t s) {
+  const V3 sun = ld3(f.sun_dir);
+  const V3 up = fabsf(sun.y) < 0.99f ? V3{0.0f, 1.0f, 0.0f} : V3{1.0f, 0.0f, 0.0f};
+  const V3 c = cross(sun, up);
+  const float lc = sqrtf(dot(c, c));
+  const V3 tg = {c.x / lc, c.y / lc, c.z / lc};
+  const V3 bt = cross(tg, sun);
+  const uint32_t r = hash_u32((px * 73856093u) ^ (py * 19349663u) ^ (f.frame_index * 83492791u)) &
+                     (VM_SOFT_ROTATIONS - 1u);
+  const V3 v = add(add(sun, muls(tg, SOFT_DISK[r][s][0])), muls(bt, SOFT_DISK[r][s][1]));
+  const float l = sqrtf(dot(v, v));
+  return {v.x / l, v.y / l, v.z / l};
+}
+
 // leaf_solid: common.wgsl:514-518
 bool leaf_solid(I3 wv, U3 m) {
   int32_t qx = (int32_t)((uint32_t)wv.x * 4u + m.x);
@@ -792,6 +811,11 @@ void or_ray_dir(const vm_frame* f, float px, float py, float* out) {
   out[0] = d.x; out[1] = d.y; out[2] = d.z;
 }
 
+void or_soft_sun_dir(const vm_frame* f, uint32_t px, uint32_t py, uint32_t s, float* out) {
+  V3 d = soft_sun_dir(*f, px, py, s);
+  out[0] = d.x; out[1] = d.y; out[2] = d.z;
+}
+
 int or_march_chunk(const or_world* o, uint32_t ci, const float* ro, const float* rd, float t_limit,
                    uint32_t skip_water, uint32_t skip_foliage, uint32_t skip_glass, uint32_t sun_ray,
                    or_hit* out) {
@@ -1040,8 +1064,18 @@ int or_primary_shadow(const or_world* o, const uint64_t* vis, float* out, uint64
               V3 hit = add(cam, muls(rd, t));
               float scale = chunk_at(w, ci).voxel_size;
               if (t >= 0.0f) {
-                cnt_add(&Counters::rays); float blocker = shadow_ray_t(w, add(hit, muls(n, 0.02f * scale)), sun, f.shadow_dist);
-                if (blocker >= 0.0f) distance = fminf(fmaxf(blocker, 0.001f), 65504.0f);
+                const V3 origin = add(hit, muls(n, 0.02f * scale));
+                if ((f.flags & VM_FLAG_SOFT_SHADOWS) != 0u) {
+                  uint32_t blocked = 0;
+                  for (uint32_t s = 0; s < VM_SOFT_SAMPLES; ++s) {
+                    cnt_add(&Counters::rays);
+                    blocked += shadow_ray_t(w, origin, soft_sun_dir(f, px, py, s), f.shadow_dist) >= 0.0f ? 1u : 0u;
+                  }
+                  distance = (float)blocked * (1.0f / (float)VM_SOFT_SAMPLES);
+                } else {
+                  cnt_add(&Counters::rays); float blocker = shadow_ray_t(w, origin, sun, f.shadow_dist);
+                  if (blocker >= 0.0f) distance = fminf(fmaxf(blocker, 0.001f), 65504.0f);
+                }
               }
             }
           }

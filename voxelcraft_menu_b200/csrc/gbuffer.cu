@@ -51,7 +51,10 @@ __global__ void __launch_bounds__(256) k_gbuffer(const __grid_constant__ PipeArg
       const uint32_t id = block_at(w, c, k.vx, k.vy, k.vz);
       g.t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
       g.fog = fog_length(f.cam_pos[1], g.t, rd.y, sk);
-      g.code = (id & 0xFFu) | (k.nid << 8) | G_HIT | (a.shadow[gp] == 0.0f ? G_LIT : 0u);
+      const float sh = a.shadow[gp];
+      g.code = (id & 0xFFu) | (k.nid << 8) | G_HIT | (sh == 0.0f ? G_LIT : 0u);
+      if ((f.flags & VM_FLAG_SOFT_SHADOWS) != 0u)   // the blocked fraction of VM_SOFT_SAMPLES rays
+        g.code |= G_SOFT | ((uint32_t)(sh * (float)VM_SOFT_SAMPLES + 0.5f) << G_SOFT_SHIFT);
       // cross-quad normals face the ray (shadow.wgsl:23)
       if (k.nid >= VM_NORMAL_CROSS_A && dot(normal_of(k.nid), rd) > 0.0f) g.code |= G_FLIP;
       const unsigned long long s2 = a.sec_key[gp];

@@ -162,8 +162,17 @@ __global__ void __launch_bounds__(128) k_primary_shadow(const vm_frame f, const 
   const uint64_t pix = (uint64_t)py * f.res[0] + px;
   float distance = 0.0f;
   F3 o;
-  if (shadow_active(f) && shadow_setup(w, f, vis[pix], px, py, &o))
-    distance = blocker_distance(shadow_ray_t<false>(w, f, o, ld3(f.sun_dir), f.shadow_dist, nullptr));
+  if (shadow_active(f) && shadow_setup(w, f, vis[pix], px, py, &o)) {
+    if (soft_shadows(f)) {
+      // the blocked fraction of the jittered rays
+      uint32_t blocked = 0;
+      for (uint32_t s = 0; s < VM_SOFT_SAMPLES; ++s)
+        blocked += shadow_ray_t<false>(w, f, o, soft_sun_dir(f, px, py, s), f.shadow_dist, nullptr) >= 0.0f ? 1u : 0u;
+      distance = (float)blocked * (1.0f / (float)VM_SOFT_SAMPLES);
+    } else {
+      distance = blocker_distance(shadow_ray_t<false>(w, f, o, ld3(f.sun_dir), f.shadow_dist, nullptr));
+    }
+  }
   out[pix] = distance;
 }
 

@@ -359,7 +359,9 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
 // The sun shadow rays (shadow_ray_t, common.wgsl:1156-1195) of the queue.
 // Persistent lanes: each holds one ray and steps it one chunk-grid cell at a
 // time; a lane whose ray is over takes the next ray of the queue at once
-// (warp-aggregated), so a warp never idles behind its longest ray.
+// (warp-aggregated), so a warp never idles behind its longest ray.  With soft
+// shadows a queue item is VM_SOFT_SAMPLES jittered rays from the same origin,
+// walked one after the other by the lane; the pixel gets the blocked fraction.
 template <bool COUNT>
 __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeArgs a) {
   const uint32_t n = a.work[W_SHADOW_N];
@@ -367,7 +369,8 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
   Traffic tr = {};
   uint32_t ns = 0;
   bool has = false, drained = false;
-  uint32_t view = 0u, pix = 0u;
+  uint32_t view = 0u, pix = 0u, sample = 0u, blocked = 0u;
+  F3 origin = {0.0f, 0.0f, 0.0f};
   ShadowWalk s;
   for (;;) {
     const uint32_t need = __ballot_sync(FULLMASK, !has);
@@ -382,7 +385,12 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
           const ShadowItem q = a.shadow_q[i];
           view = q.view;
           pix = q.pix;
-          s = shadow_walk_begin(f3(q.o[0], q.o[1], q.o[2]), ld3(frame_of(a, view).sun_dir));
+          origin = f3(q.o[0], q.o[1], q.o[2]);
+          sample = 0u;
+          blocked = 0u;
+          const vm_frame& f = frame_of(a, view);
+          s = shadow_walk_begin(origin, soft_shadows(f) ? soft_sun_dir(f, pix % f.res[0], pix / f.res[0], 0u)
+                                                        : ld3(f.sun_dir));
           has = true;
           if (COUNT) ++ns;
         }
@@ -395,8 +403,19 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
       const DevWorld w = world_of(a, vd);
       float b;
       if (shadow_walk_step<COUNT>(w, f, s, f.shadow_dist, &b, &tr)) {
-        a.shadow[vd.pix_off + pix] = blocker_distance(b);
-        has = false;
+        if (!soft_shadows(f)) {
+          a.shadow[vd.pix_off + pix] = blocker_distance(b);
+          has = false;
+        } else {
+          blocked += b >= 0.0f ? 1u : 0u;
+          if (++sample < VM_SOFT_SAMPLES) {
+            s = shadow_walk_begin(origin, soft_sun_dir(f, pix % f.res[0], pix / f.res[0], sample));
+            if (COUNT) ++ns;
+          } else {
+            a.shadow[vd.pix_off + pix] = (float)blocked * (1.0f / (float)VM_SOFT_SAMPLES);
+            has = false;
+          }
+        }
       }
     }
   }

@@ -49,6 +49,27 @@ __device__ __forceinline__ bool shadow_setup(const DevWorld& w, const vm_frame& 
   return true;
 }
 
+// Soft shadows (VM_FLAG_SOFT_SHADOWS): the s-th jittered sun direction of
+// pixel (px, py) at the frame's frame_index.  Tangent basis of the sun
+// direction from a fixed up vector, one of VM_SOFT_ROTATIONS rotations of the
+// disk pattern per pixel (the engine's hash_u32 of pixel and frame), offset
+// added in the tangent plane, normalised (v / sqrt(dot)).
+__device__ static const float g_soft_disk[VM_SOFT_ROTATIONS][VM_SOFT_SAMPLES][2] = VM_SOFT_DISK_INIT;
+__device__ __forceinline__ bool soft_shadows(const vm_frame& f) { return (f.flags & VM_FLAG_SOFT_SHADOWS) != 0u; }
+__device__ __forceinline__ F3 soft_sun_dir(const vm_frame& f, uint32_t px, uint32_t py, uint32_t s) {
+  const F3 sun = ld3(f.sun_dir);
+  const F3 up = fabsf(sun.y) < 0.99f ? f3(0.0f, 1.0f, 0.0f) : f3(1.0f, 0.0f, 0.0f);
+  const F3 c = cross(sun, up);
+  const float lc = sqrtf(dot(c, c));
+  const F3 tg = {c.x / lc, c.y / lc, c.z / lc};
+  const F3 bt = cross(tg, sun);
+  const uint32_t r = hash_u32((px * 73856093u) ^ (py * 19349663u) ^ (f.frame_index * 83492791u)) &
+                     (VM_SOFT_ROTATIONS - 1u);
+  const F3 v = (sun + tg * g_soft_disk[r][s][0]) + bt * g_soft_disk[r][s][1];
+  const float l = sqrtf(dot(v, v));
+  return {v.x / l, v.y / l, v.z / l};
+}
+
 __device__ __forceinline__ float blocker_distance(float blocker) {   // shadow.wgsl:44
   return blocker >= 0.0f ? fminf(fmaxf(blocker, 0.001f), 65504.0f) : 0.0f;
 }

@@ -92,7 +92,8 @@ __device__ __forceinline__ void shade_px(const GBuf& g, const float* __restrict_
   const float* Aw = P + 3 * VM_WATER;
   if (!water) {
     n = nrm_of(g.code);
-    lit = (g.code & G_LIT) ? 1.0f : 0.0f;
+    lit = (g.code & G_SOFT) ? 1.0f - (float)((g.code >> G_SOFT_SHIFT) & 7u) * (1.0f / (float)VM_SOFT_SAMPLES)
+                            : ((g.code & G_LIT) ? 1.0f : 0.0f);
     ndl = fmaxf(dot(n, sn), 0.0f);
     const float* A = P + 3 * id;
     for (int ch = 0; ch < 3; ++ch) c[ch] = A[ch] * (k.sun_rgb[ch] * lit * ndl + K[ch] * 0.5f);

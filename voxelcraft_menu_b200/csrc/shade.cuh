@@ -14,6 +14,8 @@ using namespace vmd;
 constexpr int NP = VM_SHADE_NPARAMS;   // 256*3 albedo + sun 3 + sky 3 + fog 1 + absorb 3
 constexpr int P_SUN = 768, P_SKY = 771, P_FOG = 774, P_ABS = 775;
 constexpr uint32_t G_HIT = 1u << 11, G_LIT = 1u << 12, G_TRACED = 1u << 13, G_HIT2 = 1u << 14, G_FLIP = 1u << 15;
+// soft shadows: G_SOFT set and the number of blocked jittered rays in bits 27-29
+constexpr uint32_t G_SOFT = 1u << 30, G_SOFT_SHIFT = 27;
 
 struct __align__(16) GBuf {   // vm_shade_gbuf: one 128-bit load per pixel
   uint32_t code;

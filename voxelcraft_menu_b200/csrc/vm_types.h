@@ -140,6 +140,34 @@ static_assert(offsetof(vm_chunk, dry_mask) == 80, "dry_mask offset");
 #define VM_FLAG_UNDERWATER 64u
 #define VM_FLAG_WATER_FAR 2097152u
 #define VM_FLAG_WATER_DARK 4194304u
+/* Soft sun shadows (an extension; the engine filters one blocker distance
+ * instead, shadow.wgsl:49-116): VM_SOFT_SAMPLES rays per lit-facing hit, the
+ * sun direction offset inside a 0.02 rad disk, and the shadow buffer holds the
+ * blocked fraction.  A bit the engine's flag set leaves free. */
+#define VM_FLAG_SOFT_SHADOWS 0x40000000u
+#define VM_SOFT_SAMPLES 4u
+#define VM_SOFT_ROTATIONS 16u
+/* Offsets in the sun's tangent plane (radians, radius 0.02): 16 rotations of
+ * a 4-point pattern (radii 0.02 sqrt((s + 1/2) / 4), golden-angle spacing),
+ * one rotation per pixel and frame.  Float literals, so the CUDA kernels and
+ * the CPU restatement use the same values. */
+#define VM_SOFT_DISK_INIT {\
+  {{0.007071067579090595f, 0.0f}, {-0.009030887857079506f, 0.008273032493889332f}, {0.0013823220506310463f, -0.01575084775686264f}, {0.01138284895569086f, 0.01484691072255373f}},\
+  {{0.00653281481936574f, 0.002705980557948351f}, {-0.011509404517710209f, 0.00418731477111578f}, {0.0073046875186264515f, -0.014022893272340298f}, {0.004834714345633984f, 0.018072783946990967f}},\
+  {{0.004999999888241291f, 0.004999999888241291f}, {-0.012235719710588455f, -0.0005358842317946255f}, {0.01211498025804758f, -0.010160081088542938f}, {-0.002449461491778493f, 0.018547240644693375f}},\
+  {{0.002705980557948351f, 0.00653281481936574f}, {-0.011099256575107574f, -0.0051774997264146805f}, {0.015080876648426056f, -0.004750489257276058f}, {-0.009360728785395622f, 0.01619804836809635f}},\
+  {{4.329780239674731e-19f, 0.007071067579090595f}, {-0.008273032493889332f, -0.009030887857079506f}, {0.01575084775686264f, 0.0013823220506310463f}, {-0.01484691072255373f, 0.01138284895569086f}},\
+  {{-0.002705980557948351f, 0.00653281481936574f}, {-0.00418731477111578f, -0.011509404517710209f}, {0.014022893272340298f, 0.0073046875186264515f}, {-0.018072783946990967f, 0.004834714345633984f}},\
+  {{-0.004999999888241291f, 0.004999999888241291f}, {0.0005358842317946255f, -0.012235719710588455f}, {0.010160081088542938f, 0.01211498025804758f}, {-0.018547240644693375f, -0.002449461491778493f}},\
+  {{-0.00653281481936574f, 0.002705980557948351f}, {0.0051774997264146805f, -0.011099256575107574f}, {0.004750489257276058f, 0.015080876648426056f}, {-0.01619804836809635f, -0.009360728785395622f}},\
+  {{-0.007071067579090595f, 8.659560479349462e-19f}, {0.009030887857079506f, -0.008273032493889332f}, {-0.0013823220506310463f, 0.01575084775686264f}, {-0.01138284895569086f, -0.01484691072255373f}},\
+  {{-0.00653281481936574f, -0.002705980557948351f}, {0.011509404517710209f, -0.00418731477111578f}, {-0.0073046875186264515f, 0.014022893272340298f}, {-0.004834714345633984f, -0.018072783946990967f}},\
+  {{-0.004999999888241291f, -0.004999999888241291f}, {0.012235719710588455f, 0.0005358842317946255f}, {-0.01211498025804758f, 0.010160081088542938f}, {0.002449461491778493f, -0.018547240644693375f}},\
+  {{-0.002705980557948351f, -0.00653281481936574f}, {0.011099256575107574f, 0.0051774997264146805f}, {-0.015080876648426056f, 0.004750489257276058f}, {0.009360728785395622f, -0.01619804836809635f}},\
+  {{-1.2989341236012077e-18f, -0.007071067579090595f}, {0.008273032493889332f, 0.009030887857079506f}, {-0.01575084775686264f, -0.0013823220506310463f}, {0.01484691072255373f, -0.01138284895569086f}},\
+  {{0.002705980557948351f, -0.00653281481936574f}, {0.00418731477111578f, 0.011509404517710209f}, {-0.014022893272340298f, -0.0073046875186264515f}, {0.018072783946990967f, -0.004834714345633984f}},\
+  {{0.004999999888241291f, -0.004999999888241291f}, {-0.0005358842317946255f, 0.012235719710588455f}, {-0.010160081088542938f, -0.01211498025804758f}, {0.018547240644693375f, 0.002449461491778493f}},\
+  {{0.00653281481936574f, -0.002705980557948351f}, {-0.0051774997264146805f, 0.011099256575107574f}, {-0.004750489257276058f, -0.015080876648426056f}, {0.01619804836809635f, 0.009360728785395622f}}}
 
 #define VM_ATTR_UNIFORM 1u
 #define VM_ATTR_HAS_WATER 2u
