@@ -18,11 +18,13 @@ dominant kernel's algorithmic bytes per launch over its own event time.
 Two more measurements share the JSON line: `batched` (3072 probe cube faces
 of 32^2..256^2 plus four 1920x1080 player views over the 256x128x256 world,
 one graph-replayed persistent launch against one launch sequence per view,
-primary + shadow) and `shading` (forward, adjoint and fused loss + gradient
-of the differentiable shading stage over 8 views at 960x540).
+primary + shadow), `shading` (forward, adjoint and fused loss + gradient
+of the differentiable shading stage over 8 views at 960x540) and `sparse`
+(64 ragged views over the 4096x256x4096 world with soft shadows and 8
+Halton-jittered frames, then a 50-step Adam fit of the albedo table).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                       [--no-batch] [--no-shade] [--no-cpu]
+                       [--no-batch] [--no-shade] [--no-sparse] [--no-cpu]
 Under torchrun every rank renders its own copy (replicas: the march does not
 shard a frame across GPUs); value is the total over ranks / max rank time.
 """
@@ -297,6 +299,89 @@ def bench_shading(local, steps, warmup):
             "l2": "flushed between timed steps (256 MB write)"}
 
 
+def bench_sparse(local, fit_steps=50):
+    """The 4096x256x4096 sparse world (16384 chunk keys, more than one view's
+    13-bit chunk field: every view carries its own chunk list and grid
+    window): 64 ragged views of 256^2..1024^2 with soft shadows (4 jittered
+    sun rays per hit), 8 frames of the Halton(2,3) jitter, then an inverse
+    albedo fit of 50 FP32 Adam steps on the shading stage."""
+    import torch
+    from voxelcraft_menu_b200 import shading as S
+    from voxelcraft_menu_b200 import tuning
+    from voxelcraft_menu_b200 import views as V
+    from voxelcraft_menu_b200 import world as W
+    from voxelcraft_menu_b200.march import Marcher
+    rec = W.recipe_sparse_world()
+    w = W.World.generate(rec)
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_SOFT_SHADOWS
+    frames = [V.ragged_views(w, flags=flags, jitter=W.halton_jitter(k), frame_index=k) for k in range(8)]
+    n_views = len(frames[0])
+    px = sum(v.n_pixels for v in frames[0])
+    m = Marcher(1024, 1024, device=local, max_views=n_views, max_batch_pixels=px)
+    stream = torch.cuda.current_stream()
+    m._ck(m._L.vm_set_stream(m._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
+    m.upload_world(*w.pools())
+    m.batch_set(frames[0])
+    best = tuning.autotune_batch(m)
+    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"])
+    total_ms, rays, prim, shad = 0.0, 0, 0, 0
+    for views in frames:
+        m.batch_set(views)
+        tr = m.batch_counted()
+        prim += tr["rays_primary"]
+        shad += tr["rays_shadow"]
+        for _ in range(2):
+            m.batch_run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            m.batch_run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1) / 3
+    rays = prim + shad
+    # the inverse albedo fit on frame 0 (water legs traced for the G-buffer)
+    m.batch_set(frames[0])
+    m.batch_run(secondary=True)
+    k = S.consts()
+    gb = S.gbuffer(m, k, torch)
+    p0 = S.default_params()
+    target, _ = S.forward(gb, torch.from_numpy(p0).cuda(), k, torch)
+    p = torch.from_numpy(S.perturbed(p0)).cuda().requires_grad_(True)
+    opt = torch.optim.Adam([p], lr=2e-3)
+    losses, ms_bwd, ms_step = [], [], []
+    for _ in range(fit_steps):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        g, loss = S.backward(gb, p.detach(), k, torch, target=target, with_loss=True)
+        e1.record(stream)
+        p.grad = g.float()
+        opt.step()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        losses.append(loss.item())
+        ms_bwd.append(e0.elapsed_time(e1))
+        ms_step.append(e0.elapsed_time(e2))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(10):
+        S.forward(gb, p.detach(), k, torch)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd = e0.elapsed_time(e1) / 10
+    m.close()
+    return {"workload": f"{n_views} views of 256^2..1024^2 ({px} pixels per frame) over the 4096x256x4096 sparse "
+                        f"world ({int(w.pool_stats().n_chunks)} chunks), soft shadows (4 rays per hit), "
+                        f"8 Halton-jittered frames", "unit": UNIT,
+            "value": rays / (total_ms * 1e-3) / 1e9, "ms_per_frame": total_ms / 8,
+            "rays_per_frame": {"primary": prim // 8, "soft_shadow": shad // 8}, "tuning": best,
+            "fit": {"steps": fit_steps, "loss_first": losses[0], "loss_last": losses[-1],
+                    "fused_loss_grad_ms_per_view": float(np.mean(ms_bwd[5:])) / n_views,
+                    "adam_step_ms": float(np.mean(ms_step[5:])), "fwd_ms_per_view": fwd / n_views,
+                    "grad_check": "FP64 oracle gradient on sparse-world views: tests/test_sparse_soft.py"}}
+
+
 def profile_traffic(kernel):
     """dram bytes per launch of kernel from the committed ncu summary, if any."""
     f = ROOT / "profiles" / f"k_{kernel}_1080p.md"
@@ -319,6 +404,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched probe views")
     ap.add_argument("--no-shade", action="store_true", help="skip the shading forward / adjoint")
+    ap.add_argument("--no-sparse", action="store_true", help="skip the sparse-world views and the fit")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -443,6 +529,8 @@ def main():
         extra["batched"] = bench_batched(local, max(3, min(args.steps, 5)), 3)
     if rank == 0 and not args.no_shade:
         extra["shading"] = bench_shading(local, max(5, min(args.steps, 20)), 5)
+    if rank == 0 and not args.no_sparse:
+        extra["sparse"] = bench_sparse(local)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -137,3 +137,42 @@ def test_sparse_world_views_match_the_oracle(sparse):
         assert np.array_equal(bt[off:off + n].view(np.uint32), st.view(np.uint32))
         off += n
     assert np.count_nonzero(bv) > 0
+
+
+@pytest.mark.gpu
+def test_sparse_soft_gbuffer_and_gradient_match_fp64(sparse):
+    """The fit's inputs on the sparse world: soft-shadow G-buffer equal to the
+    oracle's, gradient within 1e-4 of the FP64 gradient."""
+    torch = pytest.importorskip("torch")
+    from oracle import shade_oracle as SO
+    from voxelcraft_menu_b200 import shading as S
+    from voxelcraft_menu_b200 import views as V
+    from voxelcraft_menu_b200.march import Marcher
+    rec, w, pools = sparse
+    views = V.ragged_views(w, n=3, sizes=(96, 128), flags=SOFT, jitter=W.halton_jitter(3), frame_index=3)
+    m = Marcher(1024, 1024)
+    m.upload_world(*pools)
+    m.batch_set(views)
+    m.batch_run(secondary=True)
+    k = S.consts()
+    gb = S.gbuffer(m, k, torch)
+    got = gb.cpu().numpy().view(S.GBUF_DTYPE)
+    want = []
+    for v in views:
+        o = Oracle(v, *pools)
+        ovis, _, _ = o.frame_vis()
+        sk, st = o.secondary(ovis)
+        want.append(SO.gbuffer_from_oracle(o, ovis, o.shadow(ovis), sk, st, k.fog_falloff, k.fog_height))
+    want = np.concatenate(want)
+    assert np.array_equal(got["code"], want["code"])
+    assert np.array_equal(got["t"].view(np.uint32), want["t"].view(np.uint32))
+    soft = got["code"] & SO.G_SOFT
+    assert np.count_nonzero(soft) > 0
+    model = SO.Model(got, S.SUN_RGB)
+    assert np.count_nonzero((model.lit > 0) & (model.lit < 1)) > 0     # penumbrae reach the shading
+    p = S.default_params()
+    target = model.forward(S.perturbed(p)).astype(np.float32)
+    grad = S.backward(gb, torch.from_numpy(p).cuda(), k, torch, target=torch.from_numpy(target).cuda())
+    g64 = model.grad(p.astype(np.float64), target)
+    g = grad.cpu().numpy()
+    assert np.linalg.norm(g - g64) <= 1e-4 * np.linalg.norm(g64)

@@ -58,3 +58,22 @@ def player_views(world: World, pos=(128.0, 110.0, 20.0), n: int = 4, seed: int =
     rng = np.random.default_rng(seed + 1000)
     return [world.view(Camera(pos=pos, yaw=float(rng.uniform(0.0, 2.0 * math.pi)), pitch=math.radians(pitch_deg),
                               width=width, height=height, **cam)) for _ in range(n)]
+
+
+def ragged_views(world: World, n: int = 64, seed: int = 21, sizes=tuple(range(256, 1025, 64)), height_above=40.0,
+                 pitch_deg: float = -10.0, **cam):
+    """n square views of sides drawn uniformly from sizes (seed), at uniform
+    positions over the world (height_above its surface, or the sea level),
+    random yaw, fixed pitch."""
+    from .world import surface_height
+    rng = np.random.default_rng(seed)
+    sx, _, sz = world.recipe.size
+    views = []
+    for _ in range(n):
+        x, z = rng.uniform(0.07 * sx, 0.93 * sx), rng.uniform(0.07 * sz, 0.93 * sz)
+        h = max(surface_height(world.recipe, int(x), int(z)), world.recipe.water_level)
+        side = int(rng.choice(sizes))
+        views.append(world.view(Camera(pos=(float(x), float(h) + height_above, float(z)),
+                                       yaw=float(rng.uniform(0.0, 2.0 * math.pi)), pitch=math.radians(pitch_deg),
+                                       width=side, height=side, **cam)))
+    return views
