@@ -194,7 +194,17 @@ __device__ __forceinline__ void march_entry(const DevWorld& w, const vm_frame& f
   if (COUNT) tr->entries++;
   const Chunk c = ld_chunk(w, ci);
   if (ray_skips(f, c.fade, px, py)) return;
-  const Hit h = march_chunk<UNDERWATER, false, false, COUNT, true>(w, f, c, ray, f.far_, tr);
+  // The march may stop at a distance T whose depth key is already below the
+  // pixel's best: depth_key falls monotonically with t and the march reports
+  // no hit at or beyond its limit, so every hit it skips has a smaller key.
+  // T is checked here, not assumed; without a best key the limit is far.
+  float t_lim = f.far_;
+  const uint32_t bestd = (uint32_t)(best >> 40);
+  if (bestd >= 3u) {
+    const float t_cut = f.far_ * (1.0f - (float)(bestd - 3u) * (1.0f / 16777215.0f));
+    if (t_cut < f.far_ && depth_key(f, t_cut) < bestd) t_lim = t_cut;
+  }
+  const Hit h = march_chunk<UNDERWATER, false, false, COUNT, true>(w, f, c, ray, t_lim, tr);
   if (h.hit) {
     const unsigned long long k = make_key(f, h, ci);
     if (k > best) { best = k; best_id = h.id; }

@@ -79,6 +79,7 @@ def gbuffer(marcher, k: ShadeConsts, torch):
     n = marcher.batch_pixels()
     g = torch.empty(n * GBUF_BYTES, dtype=torch.uint8, device="cuda")
     marcher._ck(lib().vm_shade_gbuffer(marcher._h, C.byref(k), C.c_void_p(g.data_ptr())))
+    marcher.sync()   # the pass runs on the context's stream; torch's stream reads g next
     return g
 
 
