@@ -39,13 +39,13 @@ struct vm_ctx {
   bool have_frame = false;
   // per-frame outputs and scratch
   DevBuf vis, shadow, sec_key, sec_t, hiz, dbg, pairs, counters, err, work, dkmax, sufmax, traffic, expand;
-  DevBuf tile_list, tile_count, shadow_q, sec_q, item_cost, tile_order;
+  DevBuf tile_list, tile_count, shadow_q, sec_q, item_cost, tile_order, super_list, super_count;
   // batch
   DevBuf b_frames, b_views, b_views1, b_chunks, b_grids, b_vis, b_shadow, b_seck, b_sect, b_hiz, b_dkmax, b_sufmax;
-  DevBuf b_tile_list, b_tile_count, b_shadow_q, b_sec_q, b_item_cost, b_tile_order;
+  DevBuf b_tile_list, b_tile_count, b_shadow_q, b_sec_q, b_item_cost, b_tile_order, b_super_list, b_super_count;
   std::vector<vm_frame> bh_frames;
   std::vector<ViewDesc> bh_views;
-  uint32_t b_n_views = 0, b_total_tiles = 0, b_n_chunks = 0, b_list_cap = 1;
+  uint32_t b_n_views = 0, b_total_tiles = 0, b_n_chunks = 0, b_list_cap = 1, b_total_supers = 0;
   uint64_t b_pixels = 0, b_grid_total = 0;
   bool b_underwater = false;
   cudaGraph_t graph = nullptr;
@@ -195,6 +195,9 @@ int enqueue_render(vm_ctx* ctx, bool count, const cudaEvent_t* ev = nullptr) {
   a.sufmax = (uint32_t*)ctx->sufmax.p;
   a.tile_list = (uint16_t*)ctx->tile_list.p;
   a.tile_count = (uint32_t*)ctx->tile_count.p;
+  a.super_list = (uint16_t*)ctx->super_list.p;
+  a.super_count = (uint32_t*)ctx->super_count.p;
+  a.total_supers = ((v.tiles_x + 3) / 4) * ((v.tiles_y + 3) / 4);
   a.list_cap = std::max(1u, std::min(f.chunk_count, LIST_CAP_MAX));
   a.vis = (unsigned long long*)ctx->vis.p;
   a.shadow = (float*)ctx->shadow.p;
@@ -248,6 +251,9 @@ int vm_create(int device_ordinal, const vm_caps* caps, vm_ctx** out) {
   rc |= ensure(ctx, ctx->sufmax, (size_t)ctx->caps.max_chunks * 4);
   rc |= ensure(ctx, ctx->tile_list, tiles * LIST_CAP_MAX * 2);
   rc |= ensure(ctx, ctx->tile_count, tiles * 4);
+  const uint64_t supers = (uint64_t)((caps->max_width + 31) / 32) * ((caps->max_height + 31) / 32);
+  rc |= ensure(ctx, ctx->super_list, supers * LIST_CAP_MAX * 2);
+  rc |= ensure(ctx, ctx->super_count, supers * 4);
   rc |= ensure(ctx, ctx->shadow_q, npix * sizeof(vmk::ShadowItem));
   rc |= ensure(ctx, ctx->sec_q, npix * sizeof(vmk::SecItem));
   if (rc != VM_OK) { vm_destroy(ctx); return VM_E_CUDA; }
@@ -272,7 +278,8 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->b_seck, &ctx->b_sect, &ctx->b_hiz, &ctx->b_dkmax, &ctx->b_sufmax, &ctx->tile_list,
                    &ctx->tile_count, &ctx->shadow_q, &ctx->sec_q, &ctx->b_tile_list, &ctx->b_tile_count,
                    &ctx->b_shadow_q, &ctx->b_sec_q, &ctx->item_cost, &ctx->tile_order, &ctx->b_item_cost,
-                   &ctx->b_tile_order};
+                   &ctx->b_tile_order, &ctx->super_list, &ctx->super_count, &ctx->b_super_list,
+                   &ctx->b_super_count};
   for (DevBuf* b : all) release(*b);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
@@ -567,7 +574,7 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
   ctx->bh_frames.assign(frames, frames + n_views);
   ctx->bh_views.assign(n_views, ViewDesc{});
   std::vector<ViewDesc> single(n_views);
-  uint64_t chunk_total = 0, grid_total = 0, pix = 0, tiles = 0;
+  uint64_t chunk_total = 0, grid_total = 0, pix = 0, tiles = 0, supers = 0;
   uint32_t max_vis = 1;
   const bool uw = (frames[0].flags & VM_FLAG_UNDERWATER) != 0u;
   for (uint32_t v = 0; v < n_views; ++v) {
@@ -583,14 +590,17 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
     d.grid_len = grid_lens[v];
     d.pix_off = pix;
     d.tile_begin = (uint32_t)tiles;
+    d.super_begin = (uint32_t)supers;
     d.tiles_x = f.tiles[0];
     d.tiles_y = f.tiles[1];
     single[v] = d;
     single[v].tile_begin = 0;   // per-view launches index their own tile scratch from 0
+    single[v].super_begin = 0;
     chunk_total += chunk_counts[v];
     grid_total += grid_lens[v];
     pix += (uint64_t)f.res[0] * f.res[1];
     tiles += (uint64_t)f.tiles[0] * f.tiles[1];
+    supers += (uint64_t)((f.tiles[0] + 3) / 4) * ((f.tiles[1] + 3) / 4);
     max_vis = std::max(max_vis, std::min(f.chunk_count, chunk_counts[v]));
   }
   if (ctx->caps.max_batch_pixels && pix > ctx->caps.max_batch_pixels)
@@ -612,6 +622,8 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
   rc |= ensure(ctx, ctx->b_sufmax, std::max<uint64_t>(chunk_total, 1) * 4);
   rc |= ensure(ctx, ctx->b_tile_list, tiles * cap * 2);
   rc |= ensure(ctx, ctx->b_tile_count, tiles * 4);
+  rc |= ensure(ctx, ctx->b_super_list, std::max<uint64_t>(supers, 1) * cap * 2);
+  rc |= ensure(ctx, ctx->b_super_count, std::max<uint64_t>(supers, 1) * 4);
   rc |= ensure(ctx, ctx->b_shadow_q, pix * sizeof(vmk::ShadowItem));
   rc |= ensure(ctx, ctx->b_sec_q, pix * sizeof(vmk::SecItem));
   rc |= ensure(ctx, ctx->b_item_cost, tiles * 8);
@@ -630,6 +642,7 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
   ctx->b_n_chunks = (uint32_t)chunk_total;
   ctx->b_grid_total = grid_total;
   ctx->b_total_tiles = (uint32_t)tiles;
+  ctx->b_total_supers = (uint32_t)supers;
   ctx->b_list_cap = cap;
   ctx->b_underwater = uw;
   drop_graph(ctx);
@@ -648,6 +661,9 @@ static vmk::PipeArgs batch_args(vm_ctx* ctx, bool secondary) {
   a.sufmax = (uint32_t*)ctx->b_sufmax.p;
   a.tile_list = (uint16_t*)ctx->b_tile_list.p;
   a.tile_count = (uint32_t*)ctx->b_tile_count.p;
+  a.super_list = (uint16_t*)ctx->b_super_list.p;
+  a.super_count = (uint32_t*)ctx->b_super_count.p;
+  a.total_supers = ctx->b_total_supers;
   a.list_cap = ctx->b_list_cap;
   a.vis = (unsigned long long*)ctx->b_vis.p;
   a.shadow = (float*)ctx->b_shadow.p;
@@ -699,6 +715,9 @@ int vm_batch_run(vm_ctx* ctx, int mode) {
       a.hiz = (uint32_t*)ctx->b_hiz.p + d.tile_begin;
       a.item_cost = (uint32_t*)ctx->b_item_cost.p + 2ull * d.tile_begin;
       a.tile_order = (uint32_t*)ctx->b_tile_order.p + d.tile_begin;
+      a.super_list = (uint16_t*)ctx->b_super_list.p + (uint64_t)d.super_begin * ctx->b_list_cap;
+      a.super_count = (uint32_t*)ctx->b_super_count.p + d.super_begin;
+      a.total_supers = ((d.tiles_x + 3) / 4) * ((d.tiles_y + 3) / 4);
       CK(vmk::launch_pipeline(a, ctx->tuning, ctx->b_underwater, false, ctx->sms, ctx->stream));
     }
     return VM_OK;

@@ -17,7 +17,8 @@ struct ViewDesc {
   uint32_t tile_begin;    // first 8x8 tile of this view (also its hiz offset)
   uint32_t tiles_x, tiles_y;   // 8x8 tiles of this view (the engine's tile grid)
   uint64_t pix_off;       // first pixel of this view in the output buffers
-  uint32_t pad[2];
+  uint32_t super_begin;   // first 32x32-pixel super-tile of this view (4x4 tiles)
+  uint32_t pad;
 };
 static_assert(sizeof(ViewDesc) == 48, "ViewDesc layout");
 
@@ -61,6 +62,9 @@ struct PipeArgs {
   uint32_t* sufmax;            // suffix maximum of dkmax over the view's list
   uint16_t* tile_list;         // per 8x8 tile: culled chunk indices, ascending
   uint32_t* tile_count;        // per 8x8 tile: list length (may exceed list_cap)
+  uint16_t* super_list;        // per 32x32 super-tile: chunks its frustum cannot rule out (cap list_cap)
+  uint32_t* super_count;       // per super-tile: their number (above list_cap: no list, test all)
+  uint32_t total_supers;
   uint32_t list_cap;
   unsigned long long* vis;
   float* shadow;

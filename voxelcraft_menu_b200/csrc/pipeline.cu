@@ -103,6 +103,73 @@ __device__ __forceinline__ bool cull_keep(const vm_frame& f, const TilePlanes& t
   return box_distance(cam, bmin, bmax) < tp.reach;
 }
 
+__device__ __forceinline__ uint32_t find_view_super(const PipeArgs& a, uint32_t s) {
+  if (a.frames == nullptr) return 0;
+  uint32_t lo = 0, hi = a.n_views - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (a.views[mid].super_begin <= s) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Coarse cull of a 32x32-pixel super-tile (4x4 of the engine's tiles): a
+// chunk is dropped only when it is outside the super-tile's near plane (the
+// tiles' own test), beyond far (no tile reaches further), or outside one of
+// its four side planes by a margin of 1e-4 of |n| |p - cam| (far above the
+// planes' rounding).  Every pixel ray of the super-tile lies inside those
+// planes, so a dropped chunk can produce no hit for any of its pixels; the
+// tiles then run tile_select's exact test on the survivors only.
+__device__ __forceinline__ bool super_keep(const vm_frame& f, const F3* n, F3 cam, F3 fwd, const vm_chunk* ch,
+                                           uint32_t ci) {
+  if (ci == f.camera_chunk) return true;
+  const float* cp = reinterpret_cast<const float*>(ch + ci);
+  const F3 bmin = {__ldg(cp + 0), __ldg(cp + 1), __ldg(cp + 2)};
+  const F3 bmax = {__ldg(cp + 4), __ldg(cp + 5), __ldg(cp + 6)};
+  if (box_outside(bmin, bmax, fwd, cam)) return false;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const F3 p = {n[i].x > 0.0f ? bmax.x : bmin.x, n[i].y > 0.0f ? bmax.y : bmin.y, n[i].z > 0.0f ? bmax.z : bmin.z};
+    const F3 q = p - cam;
+    if (dot(n[i], q) < -1e-4f * sqrtf(dot(n[i], n[i]) * dot(q, q))) return false;
+  }
+  return box_distance(cam, bmin, bmax) < f.far_;
+}
+
+__global__ void __launch_bounds__(256) k_cull_super(const __grid_constant__ PipeArgs a) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t n_warps = gridDim.x * 8u;
+  for (uint32_t s = blockIdx.x * 8u + (threadIdx.x >> 5); s < a.total_supers; s += n_warps) {
+    const uint32_t v = find_view_super(a, s);
+    const vm_frame& f = frame_of(a, v);
+    const ViewDesc vd = view_of(a, v);
+    const uint32_t local = s - vd.super_begin, sxv = (vd.tiles_x + 3u) >> 2;
+    const float x0 = (float)((local % sxv) * 32u), y0 = (float)((local / sxv) * 32u);
+    const float x1 = x0 + 32.0f, y1 = y0 + 32.0f;
+    const F3 d00 = ray_dir(f, x0, y0), d10 = ray_dir(f, x1, y0), d11 = ray_dir(f, x1, y1), d01 = ray_dir(f, x0, y1);
+    const F3 center = ray_dir(f, (x0 + x1) * 0.5f, (y0 + y1) * 0.5f);
+    F3 n[4] = {cross(d00, d10), cross(d10, d11), cross(d11, d01), cross(d01, d00)};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) if (!(dot(n[i], center) >= 0.0f)) n[i] = neg(n[i]);
+    const F3 cam = ld3(f.cam_pos), fwd = ld3(f.cam_fwd);
+    const uint32_t n_vis = min(f.chunk_count, vd.n_chunks);
+    const vm_chunk* ch = a.chunks + vd.chunk_off;
+    uint16_t* out = a.super_list + (uint64_t)s * a.list_cap;
+    uint32_t cnt = 0;
+    for (uint32_t base = 0; base < n_vis; base += 32u) {
+      const uint32_t ci = base + lane;
+      const bool keep = ci < n_vis && super_keep(f, n, cam, fwd, ch, ci);
+      const uint32_t bal = __ballot_sync(FULLMASK, keep);
+      if (keep) {
+        const uint32_t pos = cnt + __popc(bal & lanemask_lt());
+        if (pos < a.list_cap) out[pos] = (uint16_t)ci;
+      }
+      cnt += __popc(bal);
+    }
+    if (lane == 0) a.super_count[s] = cnt;
+  }
+}
+
 __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t n_warps = gridDim.x * 8u;
@@ -118,9 +185,16 @@ __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a
     const vm_chunk* ch = a.chunks + vd.chunk_off;
     uint16_t* out = a.tile_list + (uint64_t)t * a.list_cap;
     uint32_t n = 0;
-    for (uint32_t base = 0; base < n_vis; base += 32u) {
-      const uint32_t ci = base + lane;
-      const bool keep = ci < n_vis && cull_keep(f, tp, cam, fwd, ch, ci);
+    // the super-tile's survivors (ascending), or every chunk when it has no list
+    const uint32_t s = vd.super_begin + (ty >> 2) * ((vd.tiles_x + 3u) >> 2) + (tx >> 2);
+    const uint32_t ns = a.super_count[s];
+    const bool listed = ns <= a.list_cap;
+    const uint16_t* cand = a.super_list + (uint64_t)s * a.list_cap;
+    const uint32_t n_test = listed ? ns : n_vis;
+    for (uint32_t base = 0; base < n_test; base += 32u) {
+      const uint32_t j = base + lane;
+      const uint32_t ci = j < n_test ? (listed ? (uint32_t)cand[j] : j) : 0u;
+      const bool keep = j < n_test && cull_keep(f, tp, cam, fwd, ch, ci);
       const uint32_t bal = __ballot_sync(FULLMASK, keep);
       if (keep) {
         const uint32_t pos = n + __popc(bal & lanemask_lt());
@@ -511,6 +585,7 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   if ((e = cudaMemsetAsync(a.hiz, 0xFF, (size_t)a.total_tiles * 4, s)) != cudaSuccess) return e;
   k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
   const uint32_t cull_blocks = std::min<uint32_t>((a.total_tiles + 7) / 8, (uint32_t)sms * 16u);
+  k_cull_super<<<std::min<uint32_t>((a.total_supers + 7) / 8, (uint32_t)sms * 16u), 256, 0, s>>>(a);
   k_cull<<<cull_blocks, 256, 0, s>>>(a);
   k_order<<<(a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256, 0, s>>>(a);
   if ((e = mark(1)) != cudaSuccess) return e;

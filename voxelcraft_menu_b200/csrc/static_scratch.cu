@@ -40,6 +40,8 @@ struct StaticScratch {
   uint32_t tile_order[STATIC_MAX_TILES];
   uint32_t hiz[STATIC_MAX_TILES];
   uint16_t tile_list[STATIC_MAX_TILES * STATIC_LIST_CAP];
+  uint16_t super_list[STATIC_MAX_TILES * STATIC_LIST_CAP];   // super-tiles never outnumber tiles
+  uint32_t super_count[STATIC_MAX_TILES];
   vmk::ShadowItem shadow_q[STATIC_MAX_PIXELS];
 };
 
@@ -121,6 +123,9 @@ extern "C" int vm_render_static(const vm_frame* frame, const vm_chunk* d_chunks,
   a.sufmax = s->sufmax;
   a.tile_list = s->tile_list;
   a.tile_count = s->tile_count;
+  a.super_list = s->super_list;
+  a.super_count = s->super_count;
+  a.total_supers = ((f.tiles[0] + 3) / 4) * ((f.tiles[1] + 3) / 4);
   a.item_cost = s->item_cost;
   a.tile_order = s->tile_order;
   a.list_cap = STATIC_LIST_CAP;
