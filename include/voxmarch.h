@@ -86,8 +86,10 @@ int vm_secondary(vm_ctx* ctx);
 int vm_render(vm_ctx* ctx);
 
 /* Tuning of vm_render and vm_batch_run's primary-ray kernel: warps per block
- * (4 or 8), register budget (0 unconstrained, 1 about 80, 2 64 registers per
- * thread) and resident blocks per SM (0 = occupancy maximum). */
+ * (4 or 8), register budget as the resident warps per SM it must allow
+ * (0 unconstrained, 1 24 warps ~80 registers, 2 32 warps 64 registers,
+ * 3 20 warps ~100 registers, 4 16 warps 128 registers) and resident blocks
+ * per SM (0 = occupancy maximum). */
 int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_sm);
 
 /* Read-backs (synchronise the context's stream). */

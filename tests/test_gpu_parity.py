@@ -70,7 +70,7 @@ def test_engine_passes_match_the_oracle(small):
     assert (vis != 0).mean() > 0.3 and (sh > 0).any() and ((sk >> 63) & 1).any()
 
 
-@pytest.mark.parametrize("warps,level,per_sm", [(4, 0, 0), (4, 1, 0), (4, 2, 1), (8, 0, 0), (8, 2, 0)])
+@pytest.mark.parametrize("warps,level,per_sm", [(4, 0, 0), (4, 1, 0), (4, 2, 1), (4, 3, 0), (8, 4, 0), (8, 0, 0), (8, 2, 0)])
 def test_pipeline_matches_the_oracle(small, warps, level, per_sm):
     w, pools, m = small
     v = w.view(W.small_terrain_camera())

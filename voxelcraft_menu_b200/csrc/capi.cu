@@ -358,8 +358,8 @@ int vm_set_frame(vm_ctx* ctx, const vm_frame* frame) {
 
 int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_sm) {
   if (!ctx) return VM_E_INVALID;
-  if (!(warps_per_block == 4 || warps_per_block == 8) || reg_level < 0 || reg_level > 2 || ctas_per_sm < 0)
-    return fail(ctx, VM_E_INVALID, "warps per block must be 4 or 8, register level 0..2, CTAs per SM >= 0");
+  if (!(warps_per_block == 4 || warps_per_block == 8) || reg_level < 0 || reg_level > 4 || ctas_per_sm < 0)
+    return fail(ctx, VM_E_INVALID, "warps per block must be 4 or 8, register level 0..4, CTAs per SM >= 0");
   if (warps_per_block != ctx->tuning.primary_warps || reg_level != ctx->tuning.reg_level ||
       ctas_per_sm != ctx->tuning.ctas_per_sm)
     drop_graph(ctx);

@@ -106,7 +106,7 @@ cudaError_t launch_expand(const vm_frame& f, const vmd::DevWorld& w, const unsig
 // -> primary march (+ queue shadow / secondary rays) -> shadow -> secondary.
 struct PipeTuning {
   int primary_warps;     // warps per block of the primary kernel (4, 8)
-  int reg_level;         // register budget: 0 unconstrained, 1 ~80, 2 64 registers per thread
+  int reg_level;         // register budget (resident warps per SM): 0 unconstrained, 1 24, 2 32, 3 20, 4 16
   int ctas_per_sm;       // resident blocks per SM of the persistent primary kernel; 0 = occupancy max
 };
 // ev (optional): five events recorded at the start, after the cull, after the

@@ -532,9 +532,14 @@ __global__ void __launch_bounds__(256) k_secondary_q(const __grid_constant__ Pip
 }
 
 // ---------------------------------------------------------------------------
-// Register levels: 0 unconstrained, 1 ~80 registers, 2 64 registers per thread.
+// Register levels: the resident warps per SM the allocation must allow.
+// 0 unconstrained, 1 24 warps (~80 registers), 2 32 warps (64 registers),
+// 3 20 warps (~100 registers), 4 16 warps (128 registers).
 template <int NW, int LEVEL>
-struct MinBlocks { static constexpr int value = LEVEL == 0 ? 1 : (LEVEL == 1 ? 24 / NW : 32 / NW); };
+struct MinBlocks {
+  static constexpr int warps = LEVEL == 1 ? 24 : (LEVEL == 2 ? 32 : (LEVEL == 3 ? 20 : 16));
+  static constexpr int value = LEVEL == 0 ? 1 : warps / NW;
+};
 
 template <int NW, int LEVEL, bool UW>
 static void* primary_fn(bool cnt) {
@@ -548,6 +553,8 @@ static void* primary_nw(int level, bool uw, bool cnt) {
     case 0: return uw ? primary_fn<NW, 0, true>(cnt) : primary_fn<NW, 0, false>(cnt);
     case 1: return uw ? primary_fn<NW, 1, true>(cnt) : primary_fn<NW, 1, false>(cnt);
     case 2: return uw ? primary_fn<NW, 2, true>(cnt) : primary_fn<NW, 2, false>(cnt);
+    case 3: return uw ? primary_fn<NW, 3, true>(cnt) : primary_fn<NW, 3, false>(cnt);
+    case 4: return uw ? primary_fn<NW, 4, true>(cnt) : primary_fn<NW, 4, false>(cnt);
   }
   return nullptr;
 }
