@@ -4,19 +4,25 @@
 //              in it can have (from a lower bound on its distance) and the
 //              suffix maximum of that bound along the view's front-to-back
 //              chunk list;
+//   k_cull_super one warp per 32x32 super-tile: the chunks its frustum
+//              cannot rule out;
 //   k_cull     one warp per 8x8 tile: tile_select's exact test
-//              (tile_select.wgsl:11-92) over every visible chunk, written as
-//              the tile's ascending chunk list;
-//   k_primary  persistent warps steal 8x4-pixel items; each lane marches its
-//              pixel through the tile's list front to back and stops as soon
-//              as no remaining chunk can produce a key above the pixel's
-//              current one, so the key equals the engine's atomicMax over all
-//              of the tile's pairs; the lane then queues its shadow ray and
-//              its water / glass ray with one atomic per warp;
-//   k_shadow,  one thread per queued ray, dense (the queue holds only rays
-//   k_secondary that exist), so whole warps trace together.
+//              (tile_select.wgsl:11-92) over its super-tile's survivors,
+//              written as the tile's ascending chunk list;
+//   k_order    the tiles in decreasing order of the last launch's item cost;
+//   k_primary  persistent warps steal 8x4-pixel items in that order; each
+//              lane marches its pixel through the tile's list front to back
+//              and stops as soon as no remaining chunk can produce a key
+//              above the pixel's current one (and a march stops at the
+//              distance past which it cannot), so the key equals the engine's
+//              atomicMax over all of the tile's pairs; the lane then queues
+//              its shadow ray and its water / glass ray, one atomic per warp;
+//   k_shadow   persistent lanes step their queued sun ray one chunk-grid cell
+//              at a time and take the next ray as soon as theirs ends;
+//   k_secondary_q one thread per queued water / glass ray.
 //
-// No kernel synchronises a block: warps never wait on other warps.
+// Only k_bounds (a block scan) and k_order (a block's ranking) synchronise a
+// block; everywhere else warps never wait on other warps.
 #include "kernels.cuh"
 #include "ray_stages.cuh"
 #include <cub/block/block_scan.cuh>
