@@ -314,3 +314,35 @@ def test_invalid_frames_are_rejected(small):
     assert e.value.code == 3, "tile index overflows the pair word"
     big.close()
     m.set_frame(f)
+
+
+def test_cost_order_and_stage_events_leave_the_output_unchanged(small):
+    """Every frame is scheduled by the previous one's measured item costs; the
+    order may change from frame to frame, the output may not.  The stage
+    events bracket the cull, primary, shadow and secondary kernels."""
+    torch = pytest.importorskip("torch")
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera(width=480, height=270))
+    m.upload_view(v)
+    m.render()
+    vis0, sh0, (k0, t0) = m.read_vis(), m.read_shadow(), m.read_secondary()
+    stream = torch.cuda.Stream()
+    m._ck(m._L.vm_set_stream(m._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
+    try:
+        for _ in range(3):
+            evs = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            for e in evs:
+                e.record(stream)
+            torch.cuda.synchronize()
+            m.render_events([e.cuda_event for e in evs])
+            torch.cuda.synchronize()
+            stages = [evs[i].elapsed_time(evs[i + 1]) for i in range(4)]
+            assert all(s >= 0.0 for s in stages) and stages[1] > 0.0
+            assert abs(sum(stages) - evs[0].elapsed_time(evs[4])) < 1e-3
+            assert_same(m.read_vis(), vis0, "vis after reordering")
+            assert_same(m.read_shadow(), sh0, "shadow after reordering")
+            k, t = m.read_secondary()
+            assert_same(k, k0, "secondary keys after reordering")
+            assert_same(t, t0, "secondary t after reordering")
+    finally:
+        m._ck(m._L.vm_set_stream(m._h, None))
