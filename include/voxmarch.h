@@ -103,6 +103,12 @@ int vm_read_heatmap(vm_ctx* ctx, uint32_t* out);             /* FLAG_HEATMAP ite
  * (common.wgsl:1300).  Misses: voxel 0xFFFFFFFF, face 0xFF, t 0. */
 int vm_read_expanded(vm_ctx* ctx, const int32_t origin[3], const uint32_t dims[3], uint32_t* voxel, uint8_t* face,
                      float* t);
+/* The visibility and shadow buffers copied to host memory without waiting:
+ * the copies are enqueued on the context's stream, and the host buffers hold
+ * the frame once that stream is synchronised (vm_sync or an event).  With
+ * page-locked host buffers the copy overlaps other work, e.g. the next frame
+ * of a second context.  Either pointer may be NULL. */
+int vm_read_async(vm_ctx* ctx, uint64_t* vis, float* shadow);
 /* Hi-Z input of the next FLAG_HIZ frame (the engine keeps last frame's buffer). */
 int vm_write_hiz(vm_ctx* ctx, const uint32_t* hiz);
 

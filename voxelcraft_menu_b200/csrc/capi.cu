@@ -490,6 +490,15 @@ static int read_dev(vm_ctx* ctx, void* dst, const void* src, size_t bytes) {
   return VM_OK;
 }
 
+int vm_read_async(vm_ctx* ctx, uint64_t* vis, float* shadow) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  CK(cudaSetDevice(ctx->device));
+  const size_t npix = (size_t)ctx->frame.res[0] * ctx->frame.res[1];
+  if (vis) CK(cudaMemcpyAsync(vis, ctx->vis.p, npix * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (shadow) CK(cudaMemcpyAsync(shadow, ctx->shadow.p, npix * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  return VM_OK;
+}
+
 int vm_read_vis(vm_ctx* ctx, uint64_t* out) {
   if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
   return read_dev(ctx, out, ctx->vis.p, (size_t)ctx->frame.res[0] * ctx->frame.res[1] * 8);

@@ -150,6 +150,7 @@ _SIGNATURES = [
     ("vm_stats_read", C.c_int, [vp, P(VmStats)]),
     ("vm_render_counted", C.c_int, [vp, P(VmTraffic)]),
     ("vm_render_events", C.c_int, [vp, P(vp)]),
+    ("vm_read_async", C.c_int, [vp, vp, vp]),
     ("vm_batch_set", C.c_int, [vp, C.c_uint32, vp, vp, vp, vp, vp]),
     ("vm_batch_run", C.c_int, [vp, C.c_int]),
     ("vm_batch_read", C.c_int, [vp, vp, vp]),
