@@ -22,6 +22,7 @@
 // this file is compiled with floating-point contraction: the model is held to
 // tolerances against FP64, not to bit equality.
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 
 #include "shade.cuh"
@@ -368,12 +369,16 @@ extern "C" int vm_shade_backward(const void* d_gbuf, uint64_t n_pixels, const fl
                                  double* d_grad_params, double* d_loss, void* stream) {
   if (!d_gbuf || !d_params || !d_grad_params || (!d_grad_color && !d_target)) return VM_E_INVALID;
   if (n_pixels == 0) return VM_OK;
-  static bool attr_set = false;   // per process: the attribute is per function, not per device
-  if (!attr_set) {
+  // the kernel's dynamic shared memory limit, raised once per device
+  static std::atomic<uint64_t> attr_set{0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return VM_E_CUDA;
+  const uint64_t bit = 1ull << (dev & 63);
+  if ((attr_set.load() & bit) == 0) {
     if (cudaFuncSetAttribute(vmk::k_shade_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vmk::BWD_SMEM) !=
         cudaSuccess)
       return VM_E_CUDA;
-    attr_set = true;
+    attr_set.fetch_or(bit);
   }
   // BWD_WARPS warps per block, each walking runs of 32 x SEG pixels
   const uint32_t grid = vmk::resident_grid(vmk::k_shade_bwd, (n_pixels + 256 * vmk::SEG - 1) / (256 * vmk::SEG),
