@@ -346,3 +346,21 @@ def test_cost_order_and_stage_events_leave_the_output_unchanged(small):
             assert_same(t, t0, "secondary t after reordering")
     finally:
         m._ck(m._L.vm_set_stream(m._h, None))
+
+
+def test_async_read_back_equals_the_synchronous_one(small):
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera(width=333, height=77))
+    m.upload_view(v)
+    m.render()
+    n = v.n_pixels
+    vis_h = torch.zeros(n, dtype=torch.int64).pin_memory()
+    sh_h = torch.zeros(n, dtype=torch.float32).pin_memory()
+    m._ck(m._L.vm_read_async(m._h, C.c_void_p(vis_h.data_ptr()), C.c_void_p(sh_h.data_ptr())))
+    m.sync()
+    assert_same(vis_h.numpy().view(np.uint64), m.read_vis(), "async vis")
+    assert_same(sh_h.numpy(), m.read_shadow(), "async shadow")
+    m._ck(m._L.vm_read_async(m._h, None, C.c_void_p(sh_h.data_ptr())))   # either pointer may be NULL
+    m.sync()
