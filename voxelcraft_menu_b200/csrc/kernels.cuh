@@ -46,7 +46,7 @@ __device__ __forceinline__ uint32_t cost_bucket(uint32_t cycles) {
 }
 
 enum : int { W_PRIMARY = 0, W_SHADOW_N = 1, W_SEC_N = 2, W_SHADOW_TAKE = 3, W_HIST = 4, W_FILL = W_HIST + (int)N_COST_BUCKETS,
-             W_WORDS = W_FILL + (int)N_COST_BUCKETS };
+             W_SEC_TAKE = W_FILL + (int)N_COST_BUCKETS, W_WORDS = W_SEC_TAKE + 1 };
 
 struct PipeArgs {
   const vm_frame* frames;      // one per view; nullptr: single view in frame0 / view0

@@ -654,6 +654,62 @@ __device__ __noinline__ WorldHit trace_world(const DevWorld& w, const vm_frame& 
   return out;
 }
 
+// trace_world one chunk-grid cell at a time, for kernels whose lanes take a
+// new ray as soon as theirs ends: the loop body of trace_world above, so the
+// hit and its t are the same.  Returns true when the ray is over, with the
+// result in *out.
+struct WorldWalk {
+  Ray r;                 // the march's ray (make_ray of the unmodified direction)
+  F3 inv;                // grid stepping: reciprocal of the tiny-fixed direction
+  bool pdx, pdy, pdz;
+  int32_t cx, cy, cz;
+  uint32_t step;
+};
+__device__ __forceinline__ WorldWalk world_walk_begin(F3 ro, F3 rd) {
+  WorldWalk s;
+  const F3 dir = {tiny_fix(rd.x), tiny_fix(rd.y), tiny_fix(rd.z)};
+  s.inv = {1.0f / dir.x, 1.0f / dir.y, 1.0f / dir.z};
+  s.pdx = dir.x > 0.0f; s.pdy = dir.y > 0.0f; s.pdz = dir.z > 0.0f;
+  s.r = make_ray(ro, rd);
+  s.cx = ffloor_i(ro.x * INV64); s.cy = ffloor_i(ro.y * INV64); s.cz = ffloor_i(ro.z * INV64);
+  s.step = 0u;
+  return s;
+}
+template <bool SKIP_WATER, bool COUNT>
+__device__ __forceinline__ bool world_walk_step(const DevWorld& w, const vm_frame& f, WorldWalk& s, float max_dist,
+                                                WorldHit* out, Traffic* tr) {
+  out->hit = false; out->t = max_dist; out->normal = 0u; out->vx = out->vy = out->vz = 0u; out->ci = VM_NO_CHUNK;
+  if (s.step >= 16u) return true;
+  uint64_t gi;
+  if (!grid_rel(f, s.cx, s.cy, s.cz, &gi)) return true;
+  if (COUNT) tr->grid++;
+  const uint32_t ci = ld_grid(w, gi);
+  const float bx = (float)(s.pdx ? s.cx + 1 : s.cx) * 64.0f;
+  const float by = (float)(s.pdy ? s.cy + 1 : s.cy) * 64.0f;
+  const float bz = (float)(s.pdz ? s.cz + 1 : s.cz) * 64.0f;
+  const F3 ro = s.r.o;
+  const float tnx = (bx - ro.x) * s.inv.x, tny = (by - ro.y) * s.inv.y, tnz = (bz - ro.z) * s.inv.z;
+  float t_exit = tnx;
+  uint32_t axis = 0u;
+  if (tny < t_exit) { t_exit = tny; axis = 1u; }
+  if (tnz < t_exit) { t_exit = tnz; axis = 2u; }
+  if (ci != VM_NO_CHUNK) {
+    const Chunk c = ld_chunk(w, ci);
+    const Hit h = march_chunk<SKIP_WATER, true, false, COUNT>(w, f, c, s.r, fminf(t_exit, max_dist), tr);
+    if (h.hit) {
+      out->hit = true; out->t = h.t; out->normal = h.normal;
+      out->vx = h.vx; out->vy = h.vy; out->vz = h.vz; out->ci = ci;
+      return true;
+    }
+  }
+  if (t_exit >= max_dist) return true;
+  if (axis == 0) s.cx += s.pdx ? 1 : -1;
+  else if (axis == 1) s.cy += s.pdy ? 1 : -1;
+  else s.cz += s.pdz ? 1 : -1;
+  ++s.step;
+  return false;
+}
+
 // hit_t: common.wgsl:1300-1318
 __device__ __forceinline__ float hit_t(const vm_frame& f, const Chunk& c, uint32_t vx, uint32_t vy, uint32_t vz,
                                        uint32_t mx, uint32_t my, uint32_t mz, uint32_t nid, F3 rd) {

@@ -19,7 +19,7 @@
 //              its shadow ray and its water / glass ray, one atomic per warp;
 //   k_shadow   persistent lanes step their queued sun ray one chunk-grid cell
 //              at a time and take the next ray as soon as theirs ends;
-//   k_secondary_q one thread per queued water / glass ray.
+//   k_secondary_q the same for the queued water / glass rays (trace_world).
 //
 // Only k_bounds (a block scan) and k_order (a block's ranking) synchronise a
 // block; everywhere else warps never wait on other warps.
@@ -512,27 +512,59 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
   flush_traffic<COUNT>(a, 1, tr, 0, ns, 0);
 }
 
+// The water / glass rays (trace_world, common.wgsl:1205-1253) of the queue,
+// on persistent lanes like k_shadow: one chunk-grid cell per step, the next
+// ray taken as soon as a lane's ray ends.
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_secondary_q(const __grid_constant__ PipeArgs a) {
+__global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ PipeArgs a) {
   const uint32_t n = a.work[W_SEC_N];
+  const uint32_t lane = threadIdx.x & 31u;
   Traffic tr = {};
   uint32_t nx = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const SecItem q = a.sec_q[i];
-    const vm_frame& f = frame_of(a, q.view);
-    const ViewDesc vd = view_of(a, q.view);
-    const DevWorld w = world_of(a, vd);
-    SecRay s;
-    s.o = f3(q.o[0], q.o[1], q.o[2]);
-    s.d = f3(q.d[0], q.d[1], q.d[2]);
-    s.max_dist = q.max_dist;
-    s.water = q.water != 0u;
-    unsigned long long k;
-    float t;
-    secondary_trace<COUNT>(w, f, s, &k, &t, &tr);
-    a.sec_key[vd.pix_off + q.pix] = k;
-    a.sec_t[vd.pix_off + q.pix] = t;
-    if (COUNT) ++nx;
+  bool has = false, drained = false, water = false;
+  uint32_t view = 0u, pix = 0u;
+  float max_dist = 0.0f;
+  WorldWalk s;
+  for (;;) {
+    const uint32_t need = __ballot_sync(FULLMASK, !has);
+    if (need && !drained) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(&a.work[W_SEC_TAKE], __popc(need));
+      base = __shfl_sync(FULLMASK, base, 0);
+      drained = base + __popc(need) >= n;
+      if (!has) {
+        const uint32_t i = base + __popc(need & lanemask_lt());
+        if (i < n) {
+          const SecItem q = a.sec_q[i];
+          view = q.view;
+          pix = q.pix;
+          max_dist = q.max_dist;
+          water = q.water != 0u;
+          s = world_walk_begin(f3(q.o[0], q.o[1], q.o[2]), f3(q.d[0], q.d[1], q.d[2]));
+          has = true;
+          if (COUNT) ++nx;
+        }
+      }
+    }
+    if (__ballot_sync(FULLMASK, has) == 0u) break;
+    if (has) {
+      const vm_frame& f = frame_of(a, view);
+      const ViewDesc vd = view_of(a, view);
+      const DevWorld w = world_of(a, vd);
+      WorldHit h;
+      const bool over = water ? world_walk_step<true, COUNT>(w, f, s, max_dist, &h, &tr)
+                              : world_walk_step<false, COUNT>(w, f, s, max_dist, &h, &tr);
+      if (over) {
+        // the key of secondary_trace: traced, glass, hit and the hit's fields
+        unsigned long long k = (1ull << 63) | (water ? 0ull : (1ull << 61));
+        if (h.hit)
+          k |= (1ull << 62) | ((unsigned long long)h.normal << 37) | ((unsigned long long)h.ci << 24) |
+               (unsigned long long)((h.vx << 16) | (h.vy << 8) | h.vz);
+        a.sec_key[vd.pix_off + pix] = k;
+        a.sec_t[vd.pix_off + pix] = h.t;
+        has = false;
+      }
+    }
   }
   flush_traffic<COUNT>(a, 2, tr, 0, 0, nx);
 }
