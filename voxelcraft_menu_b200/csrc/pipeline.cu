@@ -60,6 +60,8 @@ __global__ void __launch_bounds__(BOUNDS_THREADS) k_bounds(const __grid_constant
   typedef cub::BlockScan<uint32_t, BOUNDS_THREADS> Scan;
   __shared__ typename Scan::TempStorage tmp;
   const uint32_t v = blockIdx.x;
+  // the launch's counters start at zero (k_bounds is its first kernel)
+  if (v == 0 && threadIdx.x < (uint32_t)W_WORDS) a.work[threadIdx.x] = 0u;
   const vm_frame& f = frame_of(a, v);
   const ViewDesc vd = view_of(a, v);
   const uint32_t n = min(f.chunk_count, vd.n_chunks);
@@ -210,6 +212,7 @@ __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a
     }
     if (lane == 0) {
       a.tile_count[t] = n;
+      a.hiz[t] = 0xFFFFFFFFu;   // the primary kernel folds its pixels' minimum in
       const uint32_t c = max(a.item_cost[2u * t], a.item_cost[2u * t + 1u]);
       atomicAdd(&a.work[W_HIST + cost_bucket(c)], 1u);
     }
@@ -220,7 +223,7 @@ __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a
 // over the cost buckets; ties in any order).  Each block ranks its own
 // contiguous range of tiles in shared memory and reserves one range per
 // bucket with a single global atomic.
-constexpr uint32_t ORDER_TILES = 2048;   // tiles per block
+constexpr uint32_t ORDER_TILES = 512;    // tiles per block
 __global__ void __launch_bounds__(256) k_order(const __grid_constant__ PipeArgs a) {
   __shared__ uint32_t start[N_COST_BUCKETS], count[N_COST_BUCKETS], base[N_COST_BUCKETS];
   const uint32_t t0 = blockIdx.x * ORDER_TILES, t1 = min(t0 + ORDER_TILES, a.total_tiles);
@@ -621,13 +624,12 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   cudaError_t e;
   const auto mark = [&](int i) { return ev ? cudaEventRecord(ev[i], s) : cudaSuccess; };
   if ((e = mark(0)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(a.work, 0, W_WORDS * sizeof(uint32_t), s)) != cudaSuccess) return e;
   if (a.total_tiles == 0) {
+    if ((e = cudaMemsetAsync(a.work, 0, W_WORDS * sizeof(uint32_t), s)) != cudaSuccess) return e;
     for (int i = 1; i < 5; ++i)
       if ((e = mark(i)) != cudaSuccess) return e;
     return cudaSuccess;
   }
-  if ((e = cudaMemsetAsync(a.hiz, 0xFF, (size_t)a.total_tiles * 4, s)) != cudaSuccess) return e;
   k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
   const uint32_t cull_blocks = std::min<uint32_t>((a.total_tiles + 7) / 8, (uint32_t)sms * 16u);
   k_cull_super<<<std::min<uint32_t>((a.total_supers + 7) / 8, (uint32_t)sms * 16u), 256, 0, s>>>(a);
