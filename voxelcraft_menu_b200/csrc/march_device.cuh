@@ -752,23 +752,49 @@ __device__ __forceinline__ float box_distance(F3 p, F3 bmin, F3 bmax) {
 
 struct TilePlanes { F3 n[4]; float reach; };
 
-// tile_select.wgsl:17-57 for the 8x8 tile whose top-left pixel is (x0i, y0i)
-__device__ __forceinline__ TilePlanes tile_planes(const vm_frame& f, uint32_t x0i, uint32_t y0i) {
+// The four corner rays (d00, d10, d11, d01) and the centre ray of the
+// size x size pixel square whose top-left pixel is (x0i, y0i), in that order.
+__device__ __forceinline__ void square_dirs(const vm_frame& f, uint32_t x0i, uint32_t y0i, float size, F3 d[5]) {
   const float x0 = (float)x0i, y0 = (float)y0i;
-  const float x1 = x0 + 8.0f, y1 = y0 + 8.0f;
-  const F3 d00 = ray_dir(f, x0, y0), d10 = ray_dir(f, x1, y0), d11 = ray_dir(f, x1, y1), d01 = ray_dir(f, x0, y1);
-  const F3 center = ray_dir(f, (x0 + x1) * 0.5f, (y0 + y1) * 0.5f);
-  TilePlanes tp;
-  tp.n[0] = cross(d00, d10);
-  tp.n[1] = cross(d10, d11);
-  tp.n[2] = cross(d11, d01);
-  tp.n[3] = cross(d01, d00);
+  const float x1 = x0 + size, y1 = y0 + size;
+  d[0] = ray_dir(f, x0, y0); d[1] = ray_dir(f, x1, y0); d[2] = ray_dir(f, x1, y1); d[3] = ray_dir(f, x0, y1);
+  d[4] = ray_dir(f, (x0 + x1) * 0.5f, (y0 + y1) * 0.5f);
+}
+// square_dirs for a whole warp (all 32 lanes, same square): lane k < 5 traces
+// ray k and the others read it by shuffle, so the warp issues one ray_dir
+// instead of five.  The floats are those of square_dirs.
+__device__ __forceinline__ void square_dirs_warp(const vm_frame& f, uint32_t x0i, uint32_t y0i, float size,
+                                                 uint32_t lane, F3 d[5]) {
+  const float x0 = (float)x0i, y0 = (float)y0i;
+  const float x1 = x0 + size, y1 = y0 + size;
+  const uint32_t k = lane < 5u ? lane : 4u;
+  const float px = k == 4u ? (x0 + x1) * 0.5f : ((k == 1u || k == 2u) ? x1 : x0);
+  const float py = k == 4u ? (y0 + y1) * 0.5f : (k >= 2u ? y1 : y0);
+  const F3 mine = ray_dir(f, px, py);
 #pragma unroll
-  for (int i = 0; i < 4; ++i) if (!(dot(tp.n[i], center) >= 0.0f)) tp.n[i] = neg(tp.n[i]);
+  for (int i = 0; i < 5; ++i)
+    d[i] = {__shfl_sync(0xFFFFFFFFu, mine.x, i), __shfl_sync(0xFFFFFFFFu, mine.y, i),
+            __shfl_sync(0xFFFFFFFFu, mine.z, i)};
+}
+
+// The side planes through consecutive corner rays, oriented towards the centre.
+__device__ __forceinline__ void side_planes(const F3 d[5], F3 n[4]) {
+  n[0] = cross(d[0], d[1]);
+  n[1] = cross(d[1], d[2]);
+  n[2] = cross(d[2], d[3]);
+  n[3] = cross(d[3], d[0]);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) if (!(dot(n[i], d[4]) >= 0.0f)) n[i] = neg(n[i]);
+}
+
+// tile_select.wgsl:17-57 for an 8x8 tile, from its square_dirs
+__device__ __forceinline__ TilePlanes planes_of(const vm_frame& f, const F3 d[5]) {
+  TilePlanes tp;
+  side_planes(d, tp.n);
   float reach = f.far_;
   const uint32_t both = VM_FLAG_UNDERWATER | VM_FLAG_WATER_FAR;
   if ((f.flags & both) == both) {
-    const float up = fmaxf(fmaxf(d00.y, d10.y), fmaxf(d11.y, d01.y));
+    const float up = fmaxf(fmaxf(d[0].y, d[1].y), fmaxf(d[2].y, d[3].y));
     const float submerged = fmaxf(f.sea_level - f.cam_pos[1], 0.0f);
     float escape = 1e30f;
     if (up > 0.0f) escape = submerged / up;
@@ -781,6 +807,19 @@ __device__ __forceinline__ TilePlanes tile_planes(const vm_frame& f, uint32_t x0
   }
   tp.reach = reach;
   return tp;
+}
+
+// tile_select.wgsl:17-57 for the 8x8 tile whose top-left pixel is (x0i, y0i)
+__device__ __forceinline__ TilePlanes tile_planes(const vm_frame& f, uint32_t x0i, uint32_t y0i) {
+  F3 d[5];
+  square_dirs(f, x0i, y0i, 8.0f, d);
+  return planes_of(f, d);
+}
+// tile_planes for a whole warp (square_dirs_warp)
+__device__ __forceinline__ TilePlanes tile_planes_warp(const vm_frame& f, uint32_t x0i, uint32_t y0i, uint32_t lane) {
+  F3 d[5];
+  square_dirs_warp(f, x0i, y0i, 8.0f, lane, d);
+  return planes_of(f, d);
 }
 
 // refract per the WGSL builtin definition

@@ -152,13 +152,9 @@ __global__ void __launch_bounds__(256) k_cull_super(const __grid_constant__ Pipe
     const vm_frame& f = frame_of(a, v);
     const ViewDesc vd = view_of(a, v);
     const uint32_t local = s - vd.super_begin, sxv = (vd.tiles_x + 3u) >> 2;
-    const float x0 = (float)((local % sxv) * 32u), y0 = (float)((local / sxv) * 32u);
-    const float x1 = x0 + 32.0f, y1 = y0 + 32.0f;
-    const F3 d00 = ray_dir(f, x0, y0), d10 = ray_dir(f, x1, y0), d11 = ray_dir(f, x1, y1), d01 = ray_dir(f, x0, y1);
-    const F3 center = ray_dir(f, (x0 + x1) * 0.5f, (y0 + y1) * 0.5f);
-    F3 n[4] = {cross(d00, d10), cross(d10, d11), cross(d11, d01), cross(d01, d00)};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) if (!(dot(n[i], center) >= 0.0f)) n[i] = neg(n[i]);
+    F3 d[5], n[4];
+    square_dirs_warp(f, (local % sxv) * 32u, (local / sxv) * 32u, 32.0f, lane, d);
+    side_planes(d, n);
     const F3 cam = ld3(f.cam_pos), fwd = ld3(f.cam_fwd);
     const uint32_t n_vis = min(f.chunk_count, vd.n_chunks);
     const vm_chunk* ch = a.chunks + vd.chunk_off;
@@ -187,7 +183,7 @@ __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a
     const ViewDesc vd = view_of(a, v);
     const uint32_t local = t - vd.tile_begin;
     const uint32_t tx = local % vd.tiles_x, ty = local / vd.tiles_x;
-    const TilePlanes tp = tile_planes(f, tx * 8u, ty * 8u);
+    const TilePlanes tp = tile_planes_warp(f, tx * 8u, ty * 8u, lane);
     const F3 cam = ld3(f.cam_pos), fwd = ld3(f.cam_fwd);
     const uint32_t n_vis = min(f.chunk_count, vd.n_chunks);
     const vm_chunk* ch = a.chunks + vd.chunk_off;
