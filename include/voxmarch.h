@@ -78,6 +78,22 @@ int vm_march(vm_ctx* ctx);
 int vm_primary_shadow(vm_ctx* ctx);
 int vm_secondary(vm_ctx* ctx);
 
+/* shadow_horizontal + shadow_vertical (src/render/shaders/shadow.wgsl:62-116,
+ * stages 1 and 2 of src/render/mod.rs:1827-1840) with SPEC_SOFT_SHADOWS on: the
+ * bilateral reconstruction of the sun shadow from the frame's blocker
+ * distances (the vis and shadow buffers of vm_render or vm_march +
+ * vm_primary_shadow), guided by shadow_guide (shadow.wgsl:7-31).
+ * radius_limit = SHADOW_RADIUS_LIMIT (1..8; the engine uses 4, or 8 with
+ * FLAG_HI_SOFT_HQ, src/render/mod.rs:2660), penumbra = SOFT_PENUMBRA (1.0,
+ * 1.5 or 3.0, src/render/mod.rs:2664).  The distances are read as the engine's
+ * r16float target stores them and the horizontal pass is rounded as its
+ * rg16float target stores it.  Output (vm_read_shadow_mask): per pixel the
+ * shadow mask clamp(1 - occlusion, 0, 1) as a float, the value the engine
+ * quantises into its r8unorm target; 1 = lit.  Frames with
+ * VM_FLAG_SOFT_SHADOWS (jittered rays, whose shadow buffer holds blocked
+ * fractions) are rejected with VM_E_INVALID. */
+int vm_soften_shadows(vm_ctx* ctx, uint32_t radius_limit, float penumbra);
+
 /* The same frame as vm_select + vm_march + vm_primary_shadow + vm_secondary
  * as a warp-independent wavefront pipeline (per-tile cull, front-to-back
  * primary march with an exact early out, queued shadow and secondary rays);
@@ -98,6 +114,7 @@ int vm_read_hiz(vm_ctx* ctx, uint32_t* out);                 /* tiles.x*tiles.y 
 int vm_read_shadow(vm_ctx* ctx, float* out);                 /* blocker distance, 0 = lit */
 int vm_read_secondary(vm_ctx* ctx, uint64_t* key, float* t); /* see below */
 int vm_read_heatmap(vm_ctx* ctx, uint32_t* out);             /* FLAG_HEATMAP iteration sums (march.wgsl:51-53) */
+int vm_read_shadow_mask(vm_ctx* ctx, float* out);            /* vm_soften_shadows output (shadow.wgsl:115) */
 /* Expanded visibility: voxel index X*(Z*y + z) + x over the world box
  * [origin, origin + dims), face = normal id (common.wgsl:387), t = hit_t
  * (common.wgsl:1300).  Misses: voxel 0xFFFFFFFF, face 0xFF, t 0. */

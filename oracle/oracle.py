@@ -65,6 +65,8 @@ def lib():
             "or_expand": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, C.c_int]),
             "or_grid_block": (C.c_uint32, [vp, C.c_int32, C.c_int32, C.c_int32]),
             "or_pick": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, vp]),
+            "or_soften_shadows": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, C.c_int]),
+            "or_f16_round": (None, [vp, vp, C.c_uint64]),
         }
         for n, (r, a) in sig.items():
             f = getattr(L, n)
@@ -137,6 +139,18 @@ class Oracle:
         if traffic:
             return out, {n: int(getattr(tc, n)) for n, _ in OrCounters._fields_}
         return out
+
+    def soften(self, vis, dist, limit: int = 4, penumbra: float = 1.5):
+        """shadow_horizontal + shadow_vertical over the frame's blocker
+        distances: returns (h, mask), h the horizontal pass (npix, 2) as stored
+        in rg16float, mask clamp(1 - occlusion, 0, 1) before r8unorm."""
+        h = np.zeros((self.npix, 2), np.float32)
+        mask = np.zeros(self.npix, np.float32)
+        v = np.ascontiguousarray(vis, np.uint64)
+        d = np.ascontiguousarray(dist, np.float32)
+        self._check(self.L.or_soften_shadows(C.byref(self.w), _p(v), _p(d), limit, penumbra, _p(h), _p(mask),
+                                             self.threads))
+        return h, mask
 
     def secondary(self, vis, pix=None):
         k = np.zeros(self.npix, np.uint64)
@@ -235,3 +249,12 @@ def leaf_solid(wv, m):
     wv = np.asarray(wv, np.int32)
     m = np.asarray(m, np.uint32)
     return bool(lib().or_leaf_solid(_p(wv), _p(m)))
+
+
+def f16_round(x):
+    """The oracle's binary16 storage rounding of float32 values."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    lib().or_f16_round(_p(x), _p(out), x.size)
+    return out
+

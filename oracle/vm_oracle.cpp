@@ -764,6 +764,75 @@ inline U3 key_micro(uint64_t key) {
 inline uint32_t key_ci(uint64_t key) { return (uint32_t)(key >> 24) & 0x1FFFu; }
 inline uint32_t key_nid(uint64_t key) { return (uint32_t)(key >> 37) & 7u; }
 
+// ---- bilateral shadow reconstruction (shadow.wgsl:7-31, 49-116) -------------
+
+// Storage through the engine's r16float / rg16float targets: IEEE binary16,
+// round to nearest even, read back as f32.  Overflow (|x| >= 65520) gives
+// infinity; subnormal halves are kept.
+float f16_round(float x) {
+  uint32_t b;
+  memcpy(&b, &x, 4);
+  const uint32_t sign = b & 0x80000000u;
+  uint32_t a = b & 0x7FFFFFFFu;
+  if (a >= 0x7F800000u) return x;                       // inf, nan
+  if (a >= 0x477FF000u) a = 0x7F800000u;                // rounds past 65504
+  else if (a < 0x38800000u) {                           // below 2^-14: multiples of 2^-24
+    float m;
+    memcpy(&m, &a, 4);
+    m = nearbyintf(m * 16777216.0f) * (1.0f / 16777216.0f);   // exact scalings, RNE rounding mode
+    memcpy(&a, &m, 4);
+  } else {                                              // 10 mantissa bits kept
+    const uint32_t rem = a & 0x1FFFu;
+    a &= ~0x1FFFu;
+    if (rem > 0x1000u || (rem == 0x1000u && (a & 0x2000u) != 0u)) a += 0x2000u;
+  }
+  a |= sign;
+  float r;
+  memcpy(&r, &a, 4);
+  return r;
+}
+
+// ShadowGuide / shadow_guide: shadow.wgsl:7-31
+struct Guide { V3 hit, n; float t, scale; bool valid; };
+Guide shadow_guide(const World& w, const uint64_t* vis, int32_t px, int32_t py) {
+  const vm_frame& f = *w.f;
+  Guide g{};
+  g.valid = false;
+  if (px < 0 || py < 0 || px >= (int32_t)f.res[0] || py >= (int32_t)f.res[1]) return g;
+  const uint64_t key = vis[(uint64_t)py * f.res[0] + (uint64_t)px];
+  if (key == 0ull) return g;
+  const uint32_t ci = key_ci(key);
+  const U3 v = key_voxel(key);
+  const uint32_t id = block_at(w, ci, v);
+  if (id == VM_WATER || id == VM_GLASS) return g;
+  const uint32_t nid = key_nid(key);
+  const U3 micro = key_micro(key);
+  const V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+  g.n = normal_of(nid);
+  if (nid >= VM_NORMAL_CROSS_A && dot(g.n, rd) > 0.0f) g.n = neg(g.n);
+  if (dot(g.n, ld3(f.sun_dir)) <= 0.0f) return g;
+  g.t = hit_t(w, ci, v, micro, nid, rd);
+  g.hit = add(ld3(f.cam_pos), muls(rd, g.t));
+  g.scale = chunk_at(w, ci).voxel_size;
+  g.valid = g.t >= 0.0f;
+  return g;
+}
+
+// shadow_radius: shadow.wgsl:49-54 (SUN_ANGLE common.wgsl:1535)
+inline float shadow_radius(const vm_frame& f, float distance, float depth, float penumbra, uint32_t limit) {
+  const float proj = (float)f.res[1] / (2.0f * fmaxf(f.tan_half_fov, 0.001f));
+  const float r = distance * 0.0093f * penumbra * proj / fmaxf(depth, 0.01f);
+  return r >= 0.5f ? fminf(r, (float)limit) : 0.0f;
+}
+
+// shadow_compatible: shadow.wgsl:55-60
+inline bool shadow_compatible(const Guide& a, const Guide& b) {
+  if (!b.valid || dot(a.n, b.n) < 0.95f) return false;
+  const float tolerance = fmaxf(0.01f, 0.01f * fminf(a.scale, b.scale));
+  const V3 d = sub(b.hit, a.hit);
+  return fabsf(dot(d, a.n)) <= tolerance && fabsf(dot(d, b.n)) <= tolerance;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -1254,4 +1323,94 @@ int or_pick(const or_world* o, const float* orig, const float* dir, uint32_t max
   return 0;
 }
 
+// shadow_horizontal + shadow_vertical (shadow.wgsl:62-116) with
+// SPEC_SOFT_SHADOWS on: dist is primary_shadow's blocker distance per pixel
+// (stored as r16float), h receives the horizontal pass (occlusion, support),
+// stored as rg16float (2 floats per pixel; may be NULL), and mask the r8unorm
+// target's value before quantisation, clamp(1 - occlusion, 0, 1).  limit =
+// SHADOW_RADIUS_LIMIT, penumbra = SOFT_PENUMBRA.  shadow_guide is a pure
+// function of the pixel, so it is evaluated once per pixel and looked up per
+// tap.
+int or_soften_shadows(const or_world* o, const uint64_t* vis, const float* dist, uint32_t limit, float penumbra,
+                      float* h_out, float* mask, int threads) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  const int32_t W = (int32_t)f.res[0], H = (int32_t)f.res[1];
+  const uint64_t npix = (uint64_t)W * (uint64_t)H;
+  const bool active = (f.flags & VM_FLAG_SHADOWS) != 0u && (f.flags & VM_FLAG_HEATMAP) == 0u && f.daylight > 0.01f;
+  const int32_t L = (int32_t)limit;
+  std::vector<Guide> g(npix);
+  std::vector<float> d(npix), hx(npix), hy(npix);
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < (int64_t)npix; ++i) {
+    g[i] = shadow_guide(w, vis, (int32_t)(i % W), (int32_t)(i / W));
+    d[i] = f16_round(dist[i]);
+  }
+  auto guide = [&](int32_t x, int32_t y) -> Guide {
+    if (x < 0 || y < 0 || x >= W || y >= H) { Guide z{}; z.valid = false; return z; }
+    return g[(uint64_t)y * W + x];
+  };
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t y = 0; y < H; ++y) {
+    for (int32_t x = 0; x < W; ++x) {
+      const uint64_t i = (uint64_t)y * W + x;
+      const float occ = d[i] > 0.0f ? 1.0f : 0.0f;
+      float rx = occ, ry = 0.0f;
+      if (active && g[i].valid) {
+        const Guide& c = g[i];
+        const float rc = shadow_radius(f, d[i], c.t, penumbra, limit);
+        float sum = occ, weight = 1.0f, support = rc;
+        for (int32_t k = -L; k <= L; ++k) {
+          if (k == 0) continue;
+          const Guide q = guide(x + k, (int32_t)y);
+          if (!shadow_compatible(c, q)) continue;
+          const float nd = d[i + k];
+          const float r = fmaxf(rc, shadow_radius(f, nd, q.t, penumbra, limit));
+          if (r < fabsf((float)k)) continue;
+          const float wk = expf(-2.0f * (float)(k * k) / fmaxf(r * r, 0.25f));
+          sum += (nd > 0.0f ? 1.0f : 0.0f) * wk;
+          weight += wk;
+          support = fmaxf(support, r);
+        }
+        rx = sum / weight;
+        ry = support;
+      }
+      hx[i] = f16_round(rx);
+      hy[i] = f16_round(ry);
+    }
+  }
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t y = 0; y < H; ++y) {
+    for (int32_t x = 0; x < W; ++x) {
+      const uint64_t i = (uint64_t)y * W + x;
+      float occ = hx[i];
+      if (active && g[i].valid) {
+        const Guide& c = g[i];
+        float sum = hx[i], weight = 1.0f;
+        for (int32_t k = -L; k <= L; ++k) {
+          if (k == 0) continue;
+          const Guide q = guide(x, (int32_t)y + k);
+          if (!shadow_compatible(c, q)) continue;
+          const uint64_t j = (uint64_t)((int32_t)y + k) * W + x;
+          const float r = fmaxf(hy[i], hy[j]);
+          if (r < fabsf((float)k)) continue;
+          const float wk = expf(-2.0f * (float)(k * k) / fmaxf(r * r, 0.25f));
+          sum += hx[j] * wk;
+          weight += wk;
+        }
+        occ = sum / weight;
+      }
+      mask[i] = fminf(fmaxf(1.0f - occ, 0.0f), 1.0f);
+      if (h_out) { h_out[2 * i] = hx[i]; h_out[2 * i + 1] = hy[i]; }
+    }
+  }
+  return g_err.load();
+}
+
+void or_f16_round(const float* x, float* out, uint64_t n) {
+  for (uint64_t i = 0; i < n; ++i) out[i] = f16_round(x[i]);
+}
+
 }  // extern "C"
+

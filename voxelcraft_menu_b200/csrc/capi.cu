@@ -39,6 +39,7 @@ struct vm_ctx {
   bool have_frame = false;
   // per-frame outputs and scratch
   DevBuf vis, shadow, sec_key, sec_t, hiz, dbg, pairs, counters, err, work, dkmax, sufmax, traffic, expand;
+  DevBuf shadow_mask;   // vm_soften_shadows output, sized on first use
   DevBuf tile_list, tile_count, shadow_q, sec_q, item_cost, tile_order, super_list, super_count;
   // batch
   DevBuf b_frames, b_views, b_views1, b_chunks, b_grids, b_vis, b_shadow, b_seck, b_sect, b_hiz, b_dkmax, b_sufmax;
@@ -421,6 +422,25 @@ int vm_primary_shadow(vm_ctx* ctx) {
   return VM_OK;
 }
 
+int vm_soften_shadows(vm_ctx* ctx, uint32_t radius_limit, float penumbra) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (radius_limit < 1u || radius_limit > vmk::SOFTEN_MAX_LIMIT)
+    return fail(ctx, VM_E_INVALID, "radius limit %u outside 1..%u", radius_limit, vmk::SOFTEN_MAX_LIMIT);
+  if (!(penumbra > 0.0f) || !(penumbra < 1e30f))
+    return fail(ctx, VM_E_INVALID, "penumbra must be positive and finite");
+  if (ctx->frame.flags & VM_FLAG_SOFT_SHADOWS)
+    return fail(ctx, VM_E_INVALID, "the filter reads blocker distances; this frame's shadow buffer holds the "
+                                   "blocked fractions of jittered rays");
+  CK(cudaSetDevice(ctx->device));
+  const vm_frame& f = ctx->frame;
+  if ((rc = ensure(ctx, ctx->shadow_mask, (size_t)f.res[0] * f.res[1] * 4))) return rc;
+  CK(vmk::launch_soften(f, dev_world(ctx), (const unsigned long long*)ctx->vis.p, (const float*)ctx->shadow.p,
+                        (float*)ctx->shadow_mask.p, radius_limit, penumbra, ctx->stream));
+  return VM_OK;
+}
+
 int vm_secondary(vm_ctx* ctx) {
   if (!ctx) return VM_E_INVALID;
   int rc = check_ready(ctx);
@@ -518,6 +538,13 @@ int vm_write_hiz(vm_ctx* ctx, const uint32_t* hiz) {
 int vm_read_shadow(vm_ctx* ctx, float* out) {
   if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
   return read_dev(ctx, out, ctx->shadow.p, (size_t)ctx->frame.res[0] * ctx->frame.res[1] * 4);
+}
+int vm_read_shadow_mask(vm_ctx* ctx, float* out) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  const size_t bytes = (size_t)ctx->frame.res[0] * ctx->frame.res[1] * 4;
+  if (!ctx->shadow_mask.p || ctx->shadow_mask.bytes < bytes)
+    return fail(ctx, VM_E_NOT_READY, "no shadow mask: call vm_soften_shadows first");
+  return read_dev(ctx, out, ctx->shadow_mask.p, bytes);
 }
 int vm_read_secondary(vm_ctx* ctx, uint64_t* key, float* t) {
   if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;

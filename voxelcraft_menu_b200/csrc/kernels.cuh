@@ -98,6 +98,12 @@ cudaError_t launch_primary_shadow(const vm_frame& f, const vmd::DevWorld& w, con
                                   float* out, cudaStream_t s);
 cudaError_t launch_secondary(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                              unsigned long long* sec_key, float* sec_t, cudaStream_t s);
+// shadow_horizontal + shadow_vertical (shadow.wgsl:62-116), fused: the shadow
+// mask (clamp(1 - occlusion, 0, 1)) of the frame's blocker distances.
+// limit = SHADOW_RADIUS_LIMIT (1..SOFTEN_MAX_LIMIT), penumbra = SOFT_PENUMBRA.
+constexpr uint32_t SOFTEN_MAX_LIMIT = 8;
+cudaError_t launch_soften(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis, const float* dist,
+                          float* mask, uint32_t limit, float penumbra, cudaStream_t s);
 cudaError_t launch_expand(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                           int32_t wx, int32_t wy, int32_t wz, uint32_t dx, uint32_t dy, uint32_t dz,
                           uint32_t* voxel, uint8_t* face, float* t, cudaStream_t s);

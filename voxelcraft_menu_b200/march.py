@@ -115,6 +115,12 @@ class Marcher:
     def secondary(self):
         self._ck(self._L.vm_secondary(self._h))
 
+    def soften_shadows(self, radius_limit: int = 4, penumbra: float = 1.5):
+        """shadow_horizontal + shadow_vertical (shadow.wgsl:62-116) over the
+        frame's blocker distances: the bilateral soft-shadow reconstruction
+        (read it with read_shadow_mask)."""
+        self._ck(self._L.vm_soften_shadows(self._h, radius_limit, penumbra))
+
     def render_passes(self):
         """tile_select .. march (+Hi-Z / recover) .. primary_shadow .. secondary"""
         self.select()
@@ -169,6 +175,12 @@ class Marcher:
     def read_shadow(self, out: np.ndarray | None = None) -> np.ndarray:
         out = np.empty(self._npix(), np.float32) if out is None else out
         self._ck(self._L.vm_read_shadow(self._h, ptr(out)))
+        return out
+
+    def read_shadow_mask(self, out: np.ndarray | None = None) -> np.ndarray:
+        """clamp(1 - occlusion, 0, 1) per pixel after soften_shadows; 1 = lit."""
+        out = np.empty(self._npix(), np.float32) if out is None else out
+        self._ck(self._L.vm_read_shadow_mask(self._h, ptr(out)))
         return out
 
     def read_secondary(self):

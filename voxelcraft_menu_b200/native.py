@@ -138,6 +138,7 @@ _SIGNATURES = [
     ("vm_march", C.c_int, [vp]),
     ("vm_primary_shadow", C.c_int, [vp]),
     ("vm_secondary", C.c_int, [vp]),
+    ("vm_soften_shadows", C.c_int, [vp, C.c_uint32, C.c_float]),
     ("vm_render", C.c_int, [vp]),
     ("vm_set_tuning", C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
     ("vm_read_vis", C.c_int, [vp, vp]),
@@ -146,6 +147,7 @@ _SIGNATURES = [
     ("vm_read_shadow", C.c_int, [vp, vp]),
     ("vm_read_secondary", C.c_int, [vp, vp, vp]),
     ("vm_read_heatmap", C.c_int, [vp, vp]),
+    ("vm_read_shadow_mask", C.c_int, [vp, vp]),
     ("vm_read_expanded", C.c_int, [vp, vp, vp, vp, vp, vp]),
     ("vm_stats_read", C.c_int, [vp, P(VmStats)]),
     ("vm_render_counted", C.c_int, [vp, P(VmTraffic)]),

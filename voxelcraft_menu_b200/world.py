@@ -274,6 +274,14 @@ def small_terrain_camera(width=640, height=360, **kw) -> Camera:
     return Camera(pos=(128.0, 110.0, 20.0), width=width, height=height, **kw)
 
 
+def penumbra_camera(width=640, height=360, **kw) -> Camera:
+    """A low camera over the 256x128x256 world, (60.5, 79.5, 60.5), looking +z,
+    pitched -45 deg: close enough to the ground that tree and hill shadows
+    have penumbrae wider than a pixel for the bilateral shadow filter."""
+    kw.setdefault("pitch", math.radians(-45.0))
+    return Camera(pos=(60.5, 79.5, 60.5), width=width, height=height, **kw)
+
+
 def large_terrain_camera(recipe: Recipe, width=1920, height=1080, dx=0.0, **kw) -> Camera:
     """The 1024x256x1024 world's camera: centre column, 30 above the surface,
     looking +z, pitched -15 deg; dx shifts it along x (0.5 for the Hi-Z frame)."""
