@@ -15,7 +15,8 @@ and shadow buffers read back every step).  The library records CUDA events
 between its stages during the timed steps (`stage_ms`); `roofline` is the
 dominant kernel's algorithmic bytes per launch over its own event time.
 
-Two more measurements share the JSON line: `batched` (3072 probe cube faces
+More measurements share the JSON line: `shadow_filter` (the bilateral
+soft-shadow reconstruction over the timed frame), `batched` (3072 probe cube faces
 of 32^2..256^2 plus four 1920x1080 player views over the 256x128x256 world,
 one graph-replayed persistent launch against one launch sequence per view,
 primary + shadow), `shading` (forward, adjoint and fused loss + gradient
@@ -24,7 +25,7 @@ of the differentiable shading stage over 8 views at 960x540) and `sparse`
 Halton-jittered frames, then a 50-step Adam fit of the albedo table).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                       [--no-batch] [--no-shade] [--no-sparse] [--no-cpu]
+                       [--no-batch] [--no-shade] [--no-sparse] [--no-filter] [--no-cpu]
 Under torchrun every rank renders its own copy (replicas: the march does not
 shard a frame across GPUs); value is the total over ranks / max rank time.
 """
@@ -382,6 +383,48 @@ def bench_sparse(local, fit_steps=50):
                     "grad_check": "FP64 oracle gradient on sparse-world views: tests/test_sparse_soft.py"}}
 
 
+def bench_filter(m, vb, pools, stream, flush, steps, warmup, cpu=True):
+    """The bilateral soft-shadow reconstruction (vm_soften_shadows) over the
+    timed 1080p frame's visibility and blocker distances, at the engine's two
+    radius limits (4 with SOFT_PENUMBRA 1.5, 8 with 3.0).  Algorithmic bytes
+    per launch: 16 per pixel (8 key + 4 distance read, 4 mask written)."""
+    import torch
+    peak, peak_kind = peaks()
+    npix = int(vb.frame.res[0]) * int(vb.frame.res[1])
+    out = {"workload": "1920x1080 timed frame of the 1024x256x1024 terrain: its keys and blocker distances",
+           "l2": "flushed between timed steps (256 MB write)"}
+    for limit, pen in ((4, 1.5), (8, 3.0)):
+        for _ in range(warmup):
+            m.soften_shadows(limit, pen)
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            m.soften_shadows(limit, pen)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        t = float(np.mean(ms))
+        mask = m.read_shadow_mask()
+        gbs = 16 * npix / (t * 1e-3) / 1e9
+        rec = {"us": t * 1e3, "mpx_per_s": npix / (t * 1e-3) / 1e6, "soft_pixels": int(((mask > 0) & (mask < 1)).sum()),
+               "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                            "peak_kind": peak_kind, "algorithmic_bytes_per_launch": 16 * npix,
+                            "traffic": profile_traffic("soften") if limit == 4 else None}}
+        if cpu:
+            from oracle.oracle import Oracle
+            vis, dist = m.read_vis(), m.read_shadow()
+            o = Oracle(vb, *pools)
+            t0 = time.perf_counter()
+            _, ref = o.soften(vis, dist, limit, pen)
+            rec["cpu_oracle_ms"] = (time.perf_counter() - t0) * 1e3
+            rec["cpu_cores"] = os.cpu_count()
+            rec["max_abs_diff_vs_oracle"] = float(np.abs(ref - mask).max())
+        out[f"limit{limit}_penumbra{pen}"] = rec
+    return out
+
+
 def profile_traffic(kernel):
     """dram bytes per launch of kernel from the committed ncu summary, if any."""
     f = ROOT / "profiles" / f"k_{kernel}_1080p.md"
@@ -405,6 +448,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched probe views")
     ap.add_argument("--no-shade", action="store_true", help="skip the shading forward / adjoint")
     ap.add_argument("--no-sparse", action="store_true", help="skip the sparse-world views and the fit")
+    ap.add_argument("--no-filter", action="store_true", help="skip the bilateral shadow filter")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -473,6 +517,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_step = float(t.item())
         dist.barrier()
+
+    filt = bench_filter(m, vb, pools, stream, flush, max(5, min(args.steps, 20)), 3,
+                        cpu=not args.no_cpu and rank == 0) if not args.no_filter else None
 
     npix = 1920 * 1080
     rays = traffic["rays_primary"] + traffic["rays_shadow"]
@@ -598,10 +645,13 @@ def main():
             "e2e_serial": {"value": world * rays / (e2e_serial_ms * 1e-3) / 1e9, "unit": UNIT,
                            "ms_per_step": e2e_serial_ms,
                            "method": "one context, synchronous read-back, L2 flushed before each step"},
-            "gpu_launches": 5 * args.steps,   # bounds, cull, primary, shadow, secondary per frame
+            # per frame: k_bounds, k_cull_super, k_cull, k_order, k_primary, k_shadow, k_secondary_q
+            "gpu_launches": 7 * args.steps,
             "clocks": clocks,
             "device_error": int(stats.device_error),
         }
+        if filt is not None:
+            line["shadow_filter"] = filt
         line.update(extra)
         if not args.no_cpu:
             line["cpu_baseline"] = cpu_sample(vb, pools)

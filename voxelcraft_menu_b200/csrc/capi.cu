@@ -280,7 +280,7 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->tile_count, &ctx->shadow_q, &ctx->sec_q, &ctx->b_tile_list, &ctx->b_tile_count,
                    &ctx->b_shadow_q, &ctx->b_sec_q, &ctx->item_cost, &ctx->tile_order, &ctx->b_item_cost,
                    &ctx->b_tile_order, &ctx->super_list, &ctx->super_count, &ctx->b_super_list,
-                   &ctx->b_super_count};
+                   &ctx->b_super_count, &ctx->shadow_mask};
   for (DevBuf* b : all) release(*b);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;

@@ -79,16 +79,23 @@ __device__ __forceinline__ F3 guide_normal(uint8_t code) {
   return (code & G_FLIP) ? neg(n) : n;
 }
 
-// shadow_compatible: shadow.wgsl:55-60, on two guides in shared memory
-__device__ __forceinline__ bool soft_compatible(const SoftSmem& s, int a, int b) {
+// The centre guide of a tap loop, read once
+struct Centre { F3 n, hit; float scale; };
+__device__ __forceinline__ Centre centre_of(const SoftSmem& s, int a) {
+  const float4 h = s.hit_t[a];
+  return {guide_normal(s.code[a]), f3(h.x, h.y, h.z), s.scale[a]};
+}
+
+// shadow_compatible: shadow.wgsl:55-60, centre a against the guide of pixel b
+__device__ __forceinline__ bool soft_compatible(const SoftSmem& s, const Centre& a, int b) {
   const uint8_t cb = s.code[b];
   if (!(cb & G_VALID)) return false;
-  const F3 na = guide_normal(s.code[a]), nb = guide_normal(cb);
-  if (dot(na, nb) < 0.95f) return false;
-  const float tolerance = fmaxf(0.01f, 0.01f * fminf(s.scale[a], s.scale[b]));
-  const float4 ah = s.hit_t[a], bh = s.hit_t[b];
-  const F3 d = f3(bh.x, bh.y, bh.z) - f3(ah.x, ah.y, ah.z);
-  return fabsf(dot(d, na)) <= tolerance && fabsf(dot(d, nb)) <= tolerance;
+  const F3 nb = guide_normal(cb);
+  if (dot(a.n, nb) < 0.95f) return false;
+  const float tolerance = fmaxf(0.01f, 0.01f * fminf(a.scale, s.scale[b]));
+  const float4 bh = s.hit_t[b];
+  const F3 d = f3(bh.x, bh.y, bh.z) - a.hit;
+  return fabsf(dot(d, a.n)) <= tolerance && fabsf(dot(d, nb)) <= tolerance;
 }
 
 __device__ __forceinline__ unsigned long long shifted(unsigned long long m, int j) {
@@ -218,13 +225,14 @@ __global__ void __launch_bounds__(SOFT_THREADS) k_soften(const __grid_constant__
       float hx = s.dist[p] > 0.0f ? 1.0f : 0.0f, hy = 0.0f;
       if (((s.near[r] >> c) & 1ull) && (s.code[p] & G_VALID)) {
         const float rc = s.rad[p];
+        const Centre cp = centre_of(s, p);
         float sum = hx, weight = 1.0f, support = rc;
         for (int k = -L; k <= L; ++k) {
           if (k == 0) continue;
           const int q = p + k;
           const float rr = fmaxf(rc, s.rad[q]);
           if (rr < fabsf((float)k)) continue;
-          if (!soft_compatible(s, p, q)) continue;
+          if (!soft_compatible(s, cp, q)) continue;
           const float wk = expf(-2.0f * (float)(k * k) / fmaxf(rr * rr, 0.25f));
           sum += (s.dist[q] > 0.0f ? 1.0f : 0.0f) * wk;
           weight += wk;
@@ -251,6 +259,7 @@ __global__ void __launch_bounds__(SOFT_THREADS) k_soften(const __grid_constant__
       const float2 hp = s.h[r * SOFT_TILE + tc];
       occ = hp.x;
       if (((s.need[r] >> c) & 1ull) && (s.code[p] & G_VALID)) {
+        const Centre cp = centre_of(s, p);
         float sum = hp.x, weight = 1.0f;
         for (int k = -L; k <= L; ++k) {
           if (k == 0) continue;
@@ -258,7 +267,7 @@ __global__ void __launch_bounds__(SOFT_THREADS) k_soften(const __grid_constant__
           const float2 hq = s.h[(r + k) * SOFT_TILE + tc];
           const float rr = fmaxf(hp.y, hq.y);
           if (rr < fabsf((float)k)) continue;
-          if (!soft_compatible(s, p, q)) continue;
+          if (!soft_compatible(s, cp, q)) continue;
           const float wk = expf(-2.0f * (float)(k * k) / fmaxf(rr * rr, 0.25f));
           sum += hq.x * wk;
           weight += wk;
