@@ -115,6 +115,15 @@ int vm_read_shadow(vm_ctx* ctx, float* out);                 /* blocker distance
 int vm_read_secondary(vm_ctx* ctx, uint64_t* key, float* t); /* see below */
 int vm_read_heatmap(vm_ctx* ctx, uint32_t* out);             /* FLAG_HEATMAP iteration sums (march.wgsl:51-53) */
 int vm_read_shadow_mask(vm_ctx* ctx, float* out);            /* vm_soften_shadows output (shadow.wgsl:115) */
+/* The reflect leg of every water hit (water_reflect_leg, resolve.wgsl:1044-1058,
+ * traced per hit as the refract leg is) of the last vm_render / vm_secondary
+ * frame with FLAG_WATER_REFLECT: key as vm_read_secondary's (bit 61 clear) and
+ * t; key 0 where the pixel has none (no water, reflect_detail 0 beyond 1024
+ * voxels, or a waved surface: FLAG_WAVES on a +Y face, whose wave normal
+ * resolve.wgsl:1107-1150 is not restated).  The first such frame grows the
+ * context's buffers (12 bytes per pixel, and a secondary queue of 2 items per
+ * pixel); VM_E_NOT_READY after a frame without the flag. */
+int vm_read_reflection(vm_ctx* ctx, uint64_t* key, float* t);
 /* Expanded visibility: voxel index X*(Z*y + z) + x over the world box
  * [origin, origin + dims), face = normal id (common.wgsl:387), t = hit_t
  * (common.wgsl:1300).  Misses: voxel 0xFFFFFFFF, face 0xFF, t 0. */

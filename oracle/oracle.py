@@ -66,6 +66,7 @@ def lib():
             "or_grid_block": (C.c_uint32, [vp, C.c_int32, C.c_int32, C.c_int32]),
             "or_pick": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, vp]),
             "or_soften_shadows": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, C.c_int]),
+            "or_reflect": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
             "or_f16_round": (None, [vp, vp, C.c_uint64]),
         }
         for n, (r, a) in sig.items():
@@ -139,6 +140,15 @@ class Oracle:
         if traffic:
             return out, {n: int(getattr(tc, n)) for n, _ in OrCounters._fields_}
         return out
+
+    def reflection(self, vis, pix=None):
+        """The reflect leg of every water hit: (key, t) per pixel, key 0 where none."""
+        k = np.zeros(self.npix, np.uint64)
+        t = np.zeros(self.npix, np.float32)
+        p0, p1 = (0, self.npix) if pix is None else pix
+        v = np.ascontiguousarray(vis, np.uint64)
+        self._check(self.L.or_reflect(C.byref(self.w), _p(v), _p(k), _p(t), p0, p1, self.threads))
+        return k, t
 
     def soften(self, vis, dist, limit: int = 4, penumbra: float = 1.5):
         """shadow_horizontal + shadow_vertical over the frame's blocker

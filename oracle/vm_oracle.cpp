@@ -748,6 +748,12 @@ V3 refract(V3 e1, V3 e2, float e3) {
   return sub(muls(e1, e3), muls(e2, e3 * d + sqrtf(k)));
 }
 
+// reflect per the WGSL builtin definition: e1 - 2 dot(e2, e1) e2
+V3 reflect(V3 e1, V3 e2) {
+  float d = 2.0f * dot(e2, e1);
+  return sub(e1, muls(e2, d));
+}
+
 inline float smoothstep(float e0, float e1, float x) {
   float t = fminf(fmaxf((x - e0) / (e1 - e0), 0.0f), 1.0f);
   return t * t * (3.0f - 2.0f * t);
@@ -1180,6 +1186,56 @@ int or_primary_shadow(const or_world* o, const uint64_t* vis, float* out, uint64
 // sec_key: 0 = no secondary ray; else bit 63 = traced, bit 62 = hit, bit 61 =
 // glass (else water), bits 37-39 normal, 24-36 chunk, 0-23 voxel (x<<16|y<<8|z).
 // sec_t: hit distance along the secondary ray, or its max distance on a miss.
+// The reflect leg of every water hit (water_sec resolve.wgsl:1526-1528,
+// water_reflect_leg 1044-1058): FLAG_WATER_REFLECT, reflect_detail =
+// 1 - smoothstep(512, 1024, t) > 0 (1099), from hit + n * SURFACE_EPS along
+// reflect(rd, nt), trace_world(..., 768, skip_water) (880).  nt = n, the face
+// normal, unless the surface is waved (FLAG_WAVES on a +Y face, 1107); waved
+// pixels get no reflect ray here.  Key as or_secondary's (bit 61 clear).
+int or_reflect(const or_world* o, const uint64_t* vis, uint64_t* refl_key, float* refl_t, uint64_t pix_begin,
+               uint64_t pix_end, int threads) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  uint64_t npix = (uint64_t)f.res[0] * f.res[1];
+  if (pix_end > npix) pix_end = npix;
+  V3 cam = ld3(f.cam_pos);
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t pi = (int64_t)pix_begin; pi < (int64_t)pix_end; ++pi) {
+    uint64_t pix = (uint64_t)pi;
+    uint64_t out_key = 0ull;
+    float out_t = 0.0f;
+    uint64_t key = vis[pix];
+    if (key != 0ull && (f.flags & VM_FLAG_WATER_REFLECT) != 0u) {
+      uint32_t ci = key_ci(key);
+      U3 v = key_voxel(key);
+      uint32_t nid = key_nid(key);
+      bool waved = (f.flags & VM_FLAG_WAVES) != 0u && nid == VM_NORMAL_PY;
+      if (block_at(w, ci, v) == VM_WATER && !waved) {
+        U3 micro = key_micro(key);
+        uint32_t px = (uint32_t)(pix % f.res[0]), py = (uint32_t)(pix / f.res[0]);
+        V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+        float t = hit_t(w, ci, v, micro, nid, rd);
+        float detail = 1.0f - smoothstep(VM_WATER_REFLECT_NEAR, VM_WATER_REFLECT_FAR, t);
+        if (detail > 0.0f) {
+          V3 hit = add(cam, muls(rd, t));
+          V3 n = normal_of(nid);
+          V3 ro3 = add(hit, muls(n, VM_SURFACE_EPS));
+          WorldHit h3 = trace_world(w, ro3, reflect(rd, n), VM_WATER_REFLECT_DIST, true);
+          out_key = 1ull << 63;
+          if (h3.hit)
+            out_key |= (1ull << 62) | ((uint64_t)h3.normal << 37) | ((uint64_t)h3.ci << 24) |
+                       (uint64_t)((h3.voxel.x << 16u) | (h3.voxel.y << 8u) | h3.voxel.z);
+          out_t = h3.t;
+        }
+      }
+    }
+    refl_key[pix] = out_key;
+    refl_t[pix] = out_t;
+  }
+  return g_err.load();
+}
+
 int or_secondary(const or_world* o, const uint64_t* vis, uint64_t* sec_key, float* sec_t,
                  uint64_t pix_begin, uint64_t pix_end, int threads) {
   World w = mk(o);

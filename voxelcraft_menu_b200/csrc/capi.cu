@@ -40,6 +40,8 @@ struct vm_ctx {
   // per-frame outputs and scratch
   DevBuf vis, shadow, sec_key, sec_t, hiz, dbg, pairs, counters, err, work, dkmax, sufmax, traffic, expand;
   DevBuf shadow_mask;   // vm_soften_shadows output, sized on first use
+  DevBuf refl_key, refl_t;   // reflect legs of water hits, sized by the first FLAG_WATER_REFLECT frame
+  bool refl_frame = false;   // the last frame traced them
   DevBuf tile_list, tile_count, shadow_q, sec_q, item_cost, tile_order, super_list, super_count;
   // batch
   DevBuf b_frames, b_views, b_views1, b_chunks, b_grids, b_vis, b_shadow, b_seck, b_sect, b_hiz, b_dkmax, b_sufmax;
@@ -176,9 +178,27 @@ vmk::PipeArgs base_args(vm_ctx* ctx) {
   return a;
 }
 
+// Buffers of the reflect legs when the frame asks for them
+// (FLAG_WATER_REFLECT): one key + t per pixel, and a secondary queue of two
+// items per pixel (a water hit queues its refract and its reflect leg).
+// Allocated by the first such frame and kept.
+int prepare_reflect(vm_ctx* ctx) {
+  const vm_frame& f = ctx->frame;
+  ctx->refl_frame = (f.flags & VM_FLAG_WATER_REFLECT) != 0u;
+  if (!ctx->refl_frame) return VM_OK;
+  const size_t npix = (size_t)f.res[0] * f.res[1];
+  int rc;
+  if ((rc = ensure(ctx, ctx->refl_key, npix * 8))) return rc;
+  if ((rc = ensure(ctx, ctx->refl_t, npix * 4))) return rc;
+  return ensure(ctx, ctx->sec_q, 2 * npix * sizeof(vmk::SecItem));
+}
+
 // The single-view pipeline (frame and view descriptor by value).
 int enqueue_render(vm_ctx* ctx, bool count, const cudaEvent_t* ev = nullptr) {
   const vm_frame& f = ctx->frame;
+  // buffers are grown before any of their pointers is taken below
+  int rc;
+  if ((rc = prepare_reflect(ctx))) return rc;
   ViewDesc v;
   memset(&v, 0, sizeof v);
   v.n_chunks = ctx->n_chunks;
@@ -209,6 +229,11 @@ int enqueue_render(vm_ctx* ctx, bool count, const cudaEvent_t* ev = nullptr) {
   a.sec_q = (vmk::SecItem*)ctx->sec_q.p;
   a.frame0 = f;
   a.view0 = v;
+  if (ctx->refl_frame) {
+    a.refl_key = (unsigned long long*)ctx->refl_key.p;
+    a.refl_t = (float*)ctx->refl_t.p;
+    a.do_reflect = 1;
+  }
   const bool uw = (f.flags & VM_FLAG_UNDERWATER) != 0u;
   CK(vmk::launch_pipeline(a, ctx->tuning, uw, count, ctx->sms, ctx->stream, ev));
   return VM_OK;
@@ -280,7 +305,7 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->tile_count, &ctx->shadow_q, &ctx->sec_q, &ctx->b_tile_list, &ctx->b_tile_count,
                    &ctx->b_shadow_q, &ctx->b_sec_q, &ctx->item_cost, &ctx->tile_order, &ctx->b_item_cost,
                    &ctx->b_tile_order, &ctx->super_list, &ctx->super_count, &ctx->b_super_list,
-                   &ctx->b_super_count, &ctx->shadow_mask};
+                   &ctx->b_super_count, &ctx->shadow_mask, &ctx->refl_key, &ctx->refl_t};
   for (DevBuf* b : all) release(*b);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
@@ -446,8 +471,11 @@ int vm_secondary(vm_ctx* ctx) {
   int rc = check_ready(ctx);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
+  if ((rc = prepare_reflect(ctx))) return rc;
   CK(vmk::launch_secondary(ctx->frame, dev_world(ctx), (const unsigned long long*)ctx->vis.p,
-                           (unsigned long long*)ctx->sec_key.p, (float*)ctx->sec_t.p, ctx->stream));
+                           (unsigned long long*)ctx->sec_key.p, (float*)ctx->sec_t.p,
+                           ctx->refl_frame ? (unsigned long long*)ctx->refl_key.p : nullptr,
+                           ctx->refl_frame ? (float*)ctx->refl_t.p : nullptr, ctx->stream));
   return VM_OK;
 }
 
@@ -552,6 +580,14 @@ int vm_read_secondary(vm_ctx* ctx, uint64_t* key, float* t) {
   int rc = read_dev(ctx, key, ctx->sec_key.p, n * 8);
   if (rc) return rc;
   return read_dev(ctx, t, ctx->sec_t.p, n * 4);
+}
+int vm_read_reflection(vm_ctx* ctx, uint64_t* key, float* t) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  if (!ctx->refl_frame) return fail(ctx, VM_E_NOT_READY, "the last frame had no FLAG_WATER_REFLECT");
+  const size_t n = (size_t)ctx->frame.res[0] * ctx->frame.res[1];
+  int rc = read_dev(ctx, key, ctx->refl_key.p, n * 8);
+  if (rc) return rc;
+  return read_dev(ctx, t, ctx->refl_t.p, n * 4);
 }
 int vm_read_heatmap(vm_ctx* ctx, uint32_t* out) {
   if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;

@@ -177,7 +177,9 @@ __global__ void __launch_bounds__(128) k_primary_shadow(const vm_frame f, const 
 }
 
 __global__ void __launch_bounds__(128) k_secondary(const vm_frame f, const DevWorld w, const unsigned long long* __restrict__ vis,
-                                                   unsigned long long* __restrict__ sec_key, float* __restrict__ sec_t) {
+                                                   unsigned long long* __restrict__ sec_key, float* __restrict__ sec_t,
+                                                   unsigned long long* __restrict__ refl_key,
+                                                   float* __restrict__ refl_t) {
   const uint32_t px = blockIdx.x * 16u + threadIdx.x, py = blockIdx.y * 8u + threadIdx.y;
   if (px >= f.res[0] || py >= f.res[1]) return;
   const uint64_t pix = (uint64_t)py * f.res[0] + px;
@@ -187,6 +189,13 @@ __global__ void __launch_bounds__(128) k_secondary(const vm_frame f, const DevWo
   if (secondary_setup(w, f, vis[pix], px, py, &s)) secondary_trace<false>(w, f, s, &k, &t, nullptr);
   sec_key[pix] = k;
   sec_t[pix] = t;
+  if (refl_key) {
+    k = 0ull;
+    t = 0.0f;
+    if (reflect_setup(w, f, vis[pix], px, py, &s)) secondary_trace<false>(w, f, s, &k, &t, nullptr);
+    refl_key[pix] = k;
+    refl_t[pix] = t;
+  }
 }
 
 // Expanded visibility: voxel index over a world box, face id, hit_t.
@@ -257,10 +266,11 @@ cudaError_t launch_primary_shadow(const vm_frame& f, const DevWorld& w, const un
 }
 
 cudaError_t launch_secondary(const vm_frame& f, const DevWorld& w, const unsigned long long* vis,
-                             unsigned long long* sec_key, float* sec_t, cudaStream_t s) {
+                             unsigned long long* sec_key, float* sec_t, unsigned long long* refl_key, float* refl_t,
+                             cudaStream_t s) {
   if (f.res[0] == 0 || f.res[1] == 0) return cudaSuccess;
   dim3 g((f.res[0] + 15) / 16, (f.res[1] + 7) / 8);
-  k_secondary<<<g, dim3(16, 8), 0, s>>>(f, w, vis, sec_key, sec_t);
+  k_secondary<<<g, dim3(16, 8), 0, s>>>(f, w, vis, sec_key, sec_t, refl_key, refl_t);
   return cudaGetLastError();
 }
 

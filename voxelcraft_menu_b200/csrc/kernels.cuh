@@ -28,7 +28,9 @@ struct Traffic64 {
 
 // Queued secondary work, written by the primary kernel and consumed densely.
 struct ShadowItem { uint32_t view, pix; float o[3]; uint32_t pad; };                 // 24 B
-struct SecItem { uint32_t view, pix; float o[3], d[3]; float max_dist; uint32_t water; };  // 40 B
+// kind: SEC_GLASS, SEC_REFRACT (water refract leg) or SEC_REFLECT (water reflect leg)
+enum : uint32_t { SEC_GLASS = 0u, SEC_REFRACT = 1u, SEC_REFLECT = 2u };
+struct SecItem { uint32_t view, pix; float o[3], d[3]; float max_dist; uint32_t kind; };  // 40 B
 
 // Pipeline counters (zeroed before each frame)
 // Cost order of the primary kernel's work.  Consecutive launches over the
@@ -70,6 +72,8 @@ struct PipeArgs {
   float* shadow;
   unsigned long long* sec_key;
   float* sec_t;
+  unsigned long long* refl_key;  // reflect legs of water hits (do_reflect)
+  float* refl_t;
   uint32_t* hiz;               // per 8x8 tile: min depth key of the final visibility
   ShadowItem* shadow_q;
   SecItem* sec_q;
@@ -79,6 +83,8 @@ struct PipeArgs {
   uint32_t* err;
   Traffic64* traffic;          // counting kernels only
   uint32_t do_shadow, do_secondary;
+  uint32_t do_reflect;         // with do_secondary: also queue the reflect leg of water hits
+                               // (sec_q then holds up to 2 items per pixel)
   uint32_t px_per_lane;        // primary work item: 1 -> 8x4 pixels, 2 -> 8x8 pixels per warp
   vm_frame frame0;
   ViewDesc view0;
@@ -96,8 +102,10 @@ cudaError_t launch_recover(const vm_frame& f, const vmd::DevWorld& w, uint32_t* 
                            const uint32_t* hiz, int sms, cudaStream_t s);
 cudaError_t launch_primary_shadow(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                                   float* out, cudaStream_t s);
+// refl_key / refl_t (may be null): the reflect leg of water hits as well
 cudaError_t launch_secondary(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
-                             unsigned long long* sec_key, float* sec_t, cudaStream_t s);
+                             unsigned long long* sec_key, float* sec_t, unsigned long long* refl_key, float* refl_t,
+                             cudaStream_t s);
 // shadow_horizontal + shadow_vertical (shadow.wgsl:62-116), fused: the shadow
 // mask (clamp(1 - occlusion, 0, 1)) of the frame's blocker distances.
 // limit = SHADOW_RADIUS_LIMIT (1..SOFTEN_MAX_LIMIT), penumbra = SOFT_PENUMBRA.

@@ -829,6 +829,11 @@ __device__ __forceinline__ F3 refract(F3 e1, F3 e2, float e3) {
   if (k < 0.0f) return f3(0.0f, 0.0f, 0.0f);
   return e1 * e3 - e2 * (e3 * d + sqrtf(k));
 }
+// reflect per the WGSL builtin definition: e1 - 2 dot(e2, e1) e2
+__device__ __forceinline__ F3 reflect(F3 e1, F3 e2) {
+  const float d = 2.0f * dot(e2, e1);
+  return e1 - e2 * d;
+}
 __device__ __forceinline__ float smoothstep(float e0, float e1, float x) {
   const float t = fminf(fmaxf((x - e0) / (e1 - e0), 0.0f), 1.0f);
   return t * t * (3.0f - 2.0f * t);

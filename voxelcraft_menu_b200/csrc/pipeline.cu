@@ -376,9 +376,9 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
     }
     // The hit shared by shadow_guide (shadow.wgsl:8-30) and the water / glass
     // legs (resolve.wgsl:1029-1042,1261-1280): hit_t of the key and its point.
-    bool want_sh = false, want_sec = false;
+    bool want_sh = false, want_sec = false, want_refl = false;
     F3 so = {0.0f, 0.0f, 0.0f};
-    SecRay sr;
+    SecRay sr, rr;
     if (valid && best != 0ull) {
       const KeyParts k = split_key(best);
       const Chunk c = ld_chunk(w, k.ci);
@@ -402,6 +402,10 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
           sr.max_dist = VM_WATER_REFRACT_DIST;
           sr.water = true;
           want_sec = true;
+        }
+        if (a.do_reflect && water_reflects(f, k.nid, th)) {
+          rr = reflect_ray(hit, rd, k.nid);
+          want_refl = true;
         }
       } else if (a.do_secondary && glass) {
         sr.o = hit + rd * VM_SURFACE_EPS;
@@ -436,7 +440,23 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
           q.view = v; q.pix = (uint32_t)pix;
           q.o[0] = sr.o.x; q.o[1] = sr.o.y; q.o[2] = sr.o.z;
           q.d[0] = sr.d.x; q.d[1] = sr.d.y; q.d[2] = sr.d.z;
-          q.max_dist = sr.max_dist; q.water = sr.water ? 1u : 0u;
+          q.max_dist = sr.max_dist; q.kind = sr.water ? SEC_REFRACT : SEC_GLASS;
+        }
+      }
+    }
+    if (a.do_reflect) {
+      if (valid && !want_refl) { a.refl_key[vd.pix_off + pix] = 0ull; a.refl_t[vd.pix_off + pix] = 0.0f; }
+      const uint32_t bal = __ballot_sync(FULLMASK, want_refl);
+      if (bal) {
+        uint32_t b0 = 0;
+        if (lane == 0) b0 = atomicAdd(&a.work[W_SEC_N], __popc(bal));
+        b0 = __shfl_sync(FULLMASK, b0, 0);
+        if (want_refl) {
+          SecItem& q = a.sec_q[b0 + __popc(bal & lanemask_lt())];
+          q.view = v; q.pix = (uint32_t)pix;
+          q.o[0] = rr.o.x; q.o[1] = rr.o.y; q.o[2] = rr.o.z;
+          q.d[0] = rr.d.x; q.d[1] = rr.d.y; q.d[2] = rr.d.z;
+          q.max_dist = rr.max_dist; q.kind = SEC_REFLECT;
         }
       }
     }
@@ -511,9 +531,10 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
   flush_traffic<COUNT>(a, 1, tr, 0, ns, 0);
 }
 
-// The water / glass rays (trace_world, common.wgsl:1205-1253) of the queue,
-// on persistent lanes like k_shadow: one chunk-grid cell per step, the next
-// ray taken as soon as a lane's ray ends.
+// The water / glass rays (trace_world, common.wgsl:1205-1253) of the queue —
+// refract and reflect legs of water hits, transmission through glass — on
+// persistent lanes like k_shadow: one chunk-grid cell per step, the next ray
+// taken as soon as a lane's ray ends.
 template <bool COUNT>
 __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ PipeArgs a) {
   const uint32_t n = a.work[W_SEC_N];
@@ -521,7 +542,7 @@ __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ 
   Traffic tr = {};
   uint32_t nx = 0;
   bool has = false, drained = false, water = false;
-  uint32_t view = 0u, pix = 0u;
+  uint32_t view = 0u, pix = 0u, kind = SEC_GLASS;
   float max_dist = 0.0f;
   WorldWalk s;
   for (;;) {
@@ -538,7 +559,8 @@ __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ 
           view = q.view;
           pix = q.pix;
           max_dist = q.max_dist;
-          water = q.water != 0u;
+          kind = q.kind;
+          water = kind != SEC_GLASS;
           s = world_walk_begin(f3(q.o[0], q.o[1], q.o[2]), f3(q.d[0], q.d[1], q.d[2]));
           has = true;
           if (COUNT) ++nx;
@@ -559,8 +581,13 @@ __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ 
         if (h.hit)
           k |= (1ull << 62) | ((unsigned long long)h.normal << 37) | ((unsigned long long)h.ci << 24) |
                (unsigned long long)((h.vx << 16) | (h.vy << 8) | h.vz);
-        a.sec_key[vd.pix_off + pix] = k;
-        a.sec_t[vd.pix_off + pix] = h.t;
+        if (kind == SEC_REFLECT) {
+          a.refl_key[vd.pix_off + pix] = k;
+          a.refl_t[vd.pix_off + pix] = h.t;
+        } else {
+          a.sec_key[vd.pix_off + pix] = k;
+          a.sec_t[vd.pix_off + pix] = h.t;
+        }
         has = false;
       }
     }

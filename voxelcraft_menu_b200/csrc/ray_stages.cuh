@@ -107,6 +107,40 @@ __device__ __forceinline__ bool secondary_setup(const DevWorld& w, const vm_fram
   return true;
 }
 
+// The reflect leg of a water hit (water_reflect_leg, resolve.wgsl:1044-1058,
+// scheduled by water_sec resolve.wgsl:1526-1528): gated by FLAG_WATER_REFLECT
+// and reflect_detail > 0 (resolve.wgsl:1099); from hit + n * SURFACE_EPS
+// along reflect(rd, n), 768 voxels, water transparent.  n is the face normal:
+// water_ctx's nt equals it unless the surface is waved (FLAG_WAVES on a +Y
+// face, resolve.wgsl:1107), whose wave normal is not restated here; such
+// pixels get no reflect ray.
+__device__ __forceinline__ bool water_reflects(const vm_frame& f, uint32_t nid, float t) {
+  if ((f.flags & VM_FLAG_WATER_REFLECT) == 0u) return false;
+  if ((f.flags & VM_FLAG_WAVES) != 0u && nid == VM_NORMAL_PY) return false;
+  return 1.0f - smoothstep(VM_WATER_REFLECT_NEAR, VM_WATER_REFLECT_FAR, t) > 0.0f;
+}
+__device__ __forceinline__ SecRay reflect_ray(F3 hit, F3 rd, uint32_t nid) {
+  const F3 n = normal_of(nid);
+  SecRay s;
+  s.o = hit + n * VM_SURFACE_EPS;
+  s.d = reflect(rd, n);
+  s.max_dist = VM_WATER_REFLECT_DIST;
+  s.water = true;
+  return s;
+}
+__device__ __forceinline__ bool reflect_setup(const DevWorld& w, const vm_frame& f, unsigned long long key,
+                                              uint32_t px, uint32_t py, SecRay* s) {
+  if (key == 0ull) return false;
+  const KeyParts k = split_key(key);
+  const Chunk c = ld_chunk(w, k.ci);
+  if (block_at(w, c, k.vx, k.vy, k.vz) != VM_WATER) return false;
+  const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+  const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+  if (!water_reflects(f, k.nid, t)) return false;
+  *s = reflect_ray(ld3(f.cam_pos) + rd * t, rd, k.nid);
+  return true;
+}
+
 template <bool COUNT>
 __device__ __forceinline__ void secondary_trace(const DevWorld& w, const vm_frame& f, const SecRay& s,
                                                 unsigned long long* out_key, float* out_t, Traffic* tr) {

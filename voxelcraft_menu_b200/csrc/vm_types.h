@@ -138,6 +138,7 @@ static_assert(offsetof(vm_chunk, dry_mask) == 80, "dry_mask offset");
 #define VM_FLAG_WATER_REFLECT 16u
 #define VM_FLAG_WATER_REFRACT 32u
 #define VM_FLAG_UNDERWATER 64u
+#define VM_FLAG_WAVES 512u
 #define VM_FLAG_WATER_FAR 2097152u
 #define VM_FLAG_WATER_DARK 4194304u
 /* Soft sun shadows (an extension; the engine filters one blocker distance
@@ -207,6 +208,9 @@ static_assert(offsetof(vm_chunk, dry_mask) == 80, "dry_mask offset");
 #define VM_WATER_REFRACT_NEAR 96.0f   /* resolve.wgsl:873 */
 #define VM_WATER_REFRACT_FAR 192.0f   /* resolve.wgsl:874 */
 #define VM_GLASS_TRANSMIT_DIST 192.0f /* resolve.wgsl:886 */
+#define VM_WATER_REFLECT_NEAR 512.0f  /* resolve.wgsl:876 */
+#define VM_WATER_REFLECT_FAR 1024.0f  /* resolve.wgsl:877 */
+#define VM_WATER_REFLECT_DIST 768.0f  /* resolve.wgsl:880 */
 #define VM_WATER_FAR_DIST 128.0f      /* common.wgsl:165 */
 #define VM_WATER_DARK_DEPTH 15.0f     /* common.wgsl:167 */
 #define VM_WATER_DARK_DIST 64.0f      /* common.wgsl:172 */

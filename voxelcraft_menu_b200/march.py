@@ -177,6 +177,13 @@ class Marcher:
         self._ck(self._L.vm_read_shadow(self._h, ptr(out)))
         return out
 
+    def read_reflection(self):
+        """Reflect legs of the water hits of the last FLAG_WATER_REFLECT frame: (key, t)."""
+        k = np.empty(self._npix(), np.uint64)
+        t = np.empty(self._npix(), np.float32)
+        self._ck(self._L.vm_read_reflection(self._h, ptr(k), ptr(t)))
+        return k, t
+
     def read_shadow_mask(self, out: np.ndarray | None = None) -> np.ndarray:
         """clamp(1 - occlusion, 0, 1) per pixel after soften_shadows; 1 = lit."""
         out = np.empty(self._npix(), np.float32) if out is None else out

@@ -148,6 +148,7 @@ _SIGNATURES = [
     ("vm_read_secondary", C.c_int, [vp, vp, vp]),
     ("vm_read_heatmap", C.c_int, [vp, vp]),
     ("vm_read_shadow_mask", C.c_int, [vp, vp]),
+    ("vm_read_reflection", C.c_int, [vp, vp, vp]),
     ("vm_read_expanded", C.c_int, [vp, vp, vp, vp, vp, vp]),
     ("vm_stats_read", C.c_int, [vp, P(VmStats)]),
     ("vm_render_counted", C.c_int, [vp, P(VmTraffic)]),

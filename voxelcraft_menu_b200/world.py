@@ -23,6 +23,7 @@ FLAG_SHADOWS = 4
 FLAG_WATER_REFLECT = 16
 FLAG_WATER_REFRACT = 32
 FLAG_UNDERWATER = 64
+FLAG_WAVES = 512
 FLAG_WATER_FAR = 2097152
 FLAG_WATER_DARK = 4194304
 FLAG_SOFT_SHADOWS = 0x40000000      # extension: 4 jittered sun rays per hit, blocked fraction
