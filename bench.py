@@ -16,7 +16,8 @@ between its stages during the timed steps (`stage_ms`); `roofline` is the
 dominant kernel's algorithmic bytes per launch over its own event time.
 
 More measurements share the JSON line: `shadow_filter` (the bilateral
-soft-shadow reconstruction over the timed frame), `batched` (3072 probe cube faces
+soft-shadow reconstruction over the timed frame), `reflect` (the timed frame
+with a reflect leg per water hit), `batched` (3072 probe cube faces
 of 32^2..256^2 plus four 1920x1080 player views over the 256x128x256 world,
 one graph-replayed persistent launch against one launch sequence per view,
 primary + shadow), `shading` (forward, adjoint and fused loss + gradient
@@ -425,6 +426,35 @@ def bench_filter(m, vb, pools, stream, flush, steps, warmup, cpu=True):
     return out
 
 
+def bench_reflect(m, w, stream, flush, steps, warmup):
+    """The timed 1080p frame with FLAG_WATER_REFLECT: every water hit also
+    traces its reflect leg (reflect(rd, n), 768 voxels) on the secondary
+    lanes.  Frame time (CUDA events around vm_render) and reflect rays."""
+    import torch
+    from voxelcraft_menu_b200 import world as W
+    rec = W.recipe_large_terrain()
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_HIZ | W.FLAG_WATER_REFLECT
+    m.upload_view(w.view(W.large_terrain_camera(rec, flags=flags, dx=0.5)))
+    for _ in range(warmup):
+        m.render()
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.render()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    k, _ = m.read_reflection()
+    sk, _ = m.read_secondary()
+    return {"workload": "the timed 1920x1080 frame with FLAG_WATER_REFLECT (reflect leg per water hit)",
+            "ms_per_frame": float(np.mean(ms)),
+            "reflect_rays": int(((k >> np.uint64(63)) & np.uint64(1)).sum()),
+            "refract_and_glass_rays": int(((sk >> np.uint64(63)) & np.uint64(1)).sum()),
+            "l2": "flushed between timed steps (256 MB write)"}
+
+
 def profile_traffic(kernel):
     """dram bytes per launch of kernel from the committed ncu summary, if any."""
     f = ROOT / "profiles" / f"k_{kernel}_1080p.md"
@@ -448,7 +478,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched probe views")
     ap.add_argument("--no-shade", action="store_true", help="skip the shading forward / adjoint")
     ap.add_argument("--no-sparse", action="store_true", help="skip the sparse-world views and the fit")
-    ap.add_argument("--no-filter", action="store_true", help="skip the bilateral shadow filter")
+    ap.add_argument("--no-filter", action="store_true", help="skip the shadow filter and the reflect frame")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -520,6 +550,7 @@ def main():
 
     filt = bench_filter(m, vb, pools, stream, flush, max(5, min(args.steps, 20)), 3,
                         cpu=not args.no_cpu and rank == 0) if not args.no_filter else None
+    refl = bench_reflect(m, w, stream, flush, max(5, min(args.steps, 20)), 3) if not args.no_filter else None
 
     npix = 1920 * 1080
     rays = traffic["rays_primary"] + traffic["rays_shadow"]
@@ -652,6 +683,8 @@ def main():
         }
         if filt is not None:
             line["shadow_filter"] = filt
+        if refl is not None:
+            line["reflect"] = refl
         line.update(extra)
         if not args.no_cpu:
             line["cpu_baseline"] = cpu_sample(vb, pools)

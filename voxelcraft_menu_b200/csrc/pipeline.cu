@@ -321,9 +321,47 @@ __device__ __noinline__ void march_overflow(const DevWorld w, const vm_frame& f,
   *best_id = id;
 }
 
+// The reflect leg of a water hit (key: the pixel's key if it hit water, else
+// 0) queued for k_secondary_q, and the zero key of the pixels without one.
+// The ray direction, hit_t and hit point are recomputed here by the same
+// float operations as in k_primary (same values), and the code is out of
+// line, so the primary kernel's register allocation stays that of frames
+// without reflect legs.  Called by the whole warp.
+__device__ __noinline__ void enqueue_reflect(const PipeArgs& a, uint32_t v, uint32_t px, uint32_t py, uint64_t pix,
+                                             bool valid, unsigned long long key) {
+  const vm_frame& f = frame_of(a, v);
+  bool want = false;
+  SecRay rr;
+  if (key != 0ull) {
+    const KeyParts k = split_key(key);
+    const Chunk c = ld_chunk(world_of(a, view_of(a, v)), k.ci);
+    const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+    const float th = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+    if (water_reflects(f, k.nid, th)) {
+      rr = reflect_ray(ld3(f.cam_pos) + rd * th, rd, k.nid);
+      want = true;
+    }
+  }
+  if (valid && !want) { a.refl_key[pix] = 0ull; a.refl_t[pix] = 0.0f; }
+  const uint32_t bal = __ballot_sync(FULLMASK, want);
+  if (!bal) return;
+  uint32_t b0 = 0;
+  if ((threadIdx.x & 31u) == 0) b0 = atomicAdd(&a.work[W_SEC_N], __popc(bal));
+  b0 = __shfl_sync(FULLMASK, b0, 0);
+  if (want) {
+    SecItem& q = a.sec_q[b0 + __popc(bal & lanemask_lt())];
+    q.view = v; q.pix = py * f.res[0] + px;
+    q.o[0] = rr.o.x; q.o[1] = rr.o.y; q.o[2] = rr.o.z;
+    q.d[0] = rr.d.x; q.d[1] = rr.d.y; q.d[2] = rr.d.z;
+    q.max_dist = rr.max_dist; q.kind = SEC_REFLECT;
+  }
+}
+
 // MINB: blocks per SM the register allocation must allow (1: unconstrained),
 // the autotuner's occupancy knob.
-template <int NW, int MINB, bool UNDERWATER, bool COUNT>
+// REFL: the frame may trace reflect legs (a.do_reflect); without it the
+// kernel carries none of that code.
+template <int NW, int MINB, bool UNDERWATER, bool COUNT, bool REFL>
 __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant__ PipeArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t total = a.total_tiles * 2u;
@@ -376,9 +414,10 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
     }
     // The hit shared by shadow_guide (shadow.wgsl:8-30) and the water / glass
     // legs (resolve.wgsl:1029-1042,1261-1280): hit_t of the key and its point.
-    bool want_sh = false, want_sec = false, want_refl = false;
+    bool want_sh = false, want_sec = false;
     F3 so = {0.0f, 0.0f, 0.0f};
-    SecRay sr, rr;
+    SecRay sr;
+
     if (valid && best != 0ull) {
       const KeyParts k = split_key(best);
       const Chunk c = ld_chunk(w, k.ci);
@@ -402,10 +441,6 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
           sr.max_dist = VM_WATER_REFRACT_DIST;
           sr.water = true;
           want_sec = true;
-        }
-        if (a.do_reflect && water_reflects(f, k.nid, th)) {
-          rr = reflect_ray(hit, rd, k.nid);
-          want_refl = true;
         }
       } else if (a.do_secondary && glass) {
         sr.o = hit + rd * VM_SURFACE_EPS;
@@ -444,22 +479,8 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
         }
       }
     }
-    if (a.do_reflect) {
-      if (valid && !want_refl) { a.refl_key[vd.pix_off + pix] = 0ull; a.refl_t[vd.pix_off + pix] = 0.0f; }
-      const uint32_t bal = __ballot_sync(FULLMASK, want_refl);
-      if (bal) {
-        uint32_t b0 = 0;
-        if (lane == 0) b0 = atomicAdd(&a.work[W_SEC_N], __popc(bal));
-        b0 = __shfl_sync(FULLMASK, b0, 0);
-        if (want_refl) {
-          SecItem& q = a.sec_q[b0 + __popc(bal & lanemask_lt())];
-          q.view = v; q.pix = (uint32_t)pix;
-          q.o[0] = rr.o.x; q.o[1] = rr.o.y; q.o[2] = rr.o.z;
-          q.d[0] = rr.d.x; q.d[1] = rr.d.y; q.d[2] = rr.d.z;
-          q.max_dist = rr.max_dist; q.kind = SEC_REFLECT;
-        }
-      }
-    }
+    if (REFL && a.do_reflect)
+      enqueue_reflect(a, v, px, py, vd.pix_off + pix, valid, valid && best_id == VM_WATER ? best : 0ull);
     if (lane == 0) a.item_cost[2u * t + half] = (uint32_t)min(clock64() - clk0, 0xFFFFFFFFll);
   }
   flush_traffic<COUNT>(a, 0, tr, np, ns, nx);
@@ -606,36 +627,37 @@ struct MinBlocks {
 };
 
 template <int NW, int LEVEL, bool UW>
-static void* primary_fn(bool cnt) {
-  if (cnt) return (void*)k_primary<NW, MinBlocks<NW, LEVEL>::value, UW, true>;
-  return (void*)k_primary<NW, MinBlocks<NW, LEVEL>::value, UW, false>;
+static void* primary_fn(bool cnt, bool refl) {
+  constexpr int MB = MinBlocks<NW, LEVEL>::value;
+  if (cnt) return (void*)k_primary<NW, MB, UW, true, true>;   // counting kernels keep the runtime gate
+  return refl ? (void*)k_primary<NW, MB, UW, false, true> : (void*)k_primary<NW, MB, UW, false, false>;
 }
 
 template <int NW>
-static void* primary_nw(int level, bool uw, bool cnt) {
+static void* primary_nw(int level, bool uw, bool cnt, bool refl) {
   switch (level) {
-    case 0: return uw ? primary_fn<NW, 0, true>(cnt) : primary_fn<NW, 0, false>(cnt);
-    case 1: return uw ? primary_fn<NW, 1, true>(cnt) : primary_fn<NW, 1, false>(cnt);
-    case 2: return uw ? primary_fn<NW, 2, true>(cnt) : primary_fn<NW, 2, false>(cnt);
-    case 3: return uw ? primary_fn<NW, 3, true>(cnt) : primary_fn<NW, 3, false>(cnt);
-    case 4: return uw ? primary_fn<NW, 4, true>(cnt) : primary_fn<NW, 4, false>(cnt);
+    case 0: return uw ? primary_fn<NW, 0, true>(cnt, refl) : primary_fn<NW, 0, false>(cnt, refl);
+    case 1: return uw ? primary_fn<NW, 1, true>(cnt, refl) : primary_fn<NW, 1, false>(cnt, refl);
+    case 2: return uw ? primary_fn<NW, 2, true>(cnt, refl) : primary_fn<NW, 2, false>(cnt, refl);
+    case 3: return uw ? primary_fn<NW, 3, true>(cnt, refl) : primary_fn<NW, 3, false>(cnt, refl);
+    case 4: return uw ? primary_fn<NW, 4, true>(cnt, refl) : primary_fn<NW, 4, false>(cnt, refl);
   }
   return nullptr;
 }
 
-static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt) {
-  if (cnt) return primary_nw<4>(0, uw, true);   // the counting run is never timed
+static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt, bool refl) {
+  if (cnt) return primary_nw<4>(0, uw, true, true);   // the counting run is never timed
   switch (t.primary_warps) {
-    case 4: return primary_nw<4>(t.reg_level, uw, false);
-    case 8: return primary_nw<8>(t.reg_level, uw, false);
+    case 4: return primary_nw<4>(t.reg_level, uw, false, refl);
+    case 8: return primary_nw<8>(t.reg_level, uw, false, refl);
   }
   return nullptr;
 }
 
 static int block_warps(const PipeTuning& t, bool cnt) { return cnt ? 4 : t.primary_warps; }
 
-int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count) {
-  void* fn = primary_kernel(t, underwater, count);
+int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bool reflect) {
+  void* fn = primary_kernel(t, underwater, count, reflect);
   if (!fn) return 0;
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block_warps(t, count) * 32, 0);
@@ -659,10 +681,11 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   k_cull<<<cull_blocks, 256, 0, s>>>(a);
   k_order<<<(a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256, 0, s>>>(a);
   if ((e = mark(1)) != cudaSuccess) return e;
-  void* fn = primary_kernel(t, underwater, count);
+  const bool refl = a.do_reflect != 0u;
+  void* fn = primary_kernel(t, underwater, count, refl);
   if (!fn) return cudaErrorInvalidValue;
   const int nw = block_warps(t, count);
-  int per = t.ctas_per_sm > 0 && !count ? t.ctas_per_sm : primary_max_ctas_per_sm(t, underwater, count);
+  int per = t.ctas_per_sm > 0 && !count ? t.ctas_per_sm : primary_max_ctas_per_sm(t, underwater, count, refl);
   if (per <= 0) per = 1;
   const uint32_t items_blocks = (a.total_tiles * 2u + nw - 1) / nw;
   const uint32_t grid = std::min<uint32_t>((uint32_t)sms * (uint32_t)per, items_blocks);
