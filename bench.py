@@ -17,7 +17,8 @@ dominant kernel's algorithmic bytes per launch over its own event time.
 
 More measurements share the JSON line: `shadow_filter` (the bilateral
 soft-shadow reconstruction over the timed frame), `reflect` (the timed frame
-with a reflect leg per water hit), `batched` (3072 probe cube faces
+with a reflect leg per water hit), `encoder` (the dense -> 64-tree encoder
+over the terrain's 1024 chunks), `batched` (3072 probe cube faces
 of 32^2..256^2 plus four 1920x1080 player views over the 256x128x256 world,
 one graph-replayed persistent launch against one launch sequence per view,
 primary + shadow), `shading` (forward, adjoint and fused loss + gradient
@@ -455,6 +456,52 @@ def bench_reflect(m, w, stream, flush, steps, warmup):
             "l2": "flushed between timed steps (256 MB write)"}
 
 
+def bench_encoder(local, steps, warmup, cpu=True):
+    """The dense -> 64-tree encoder (vm_encode_trees) over every chunk of the
+    1024x256x1024 terrain (1024 dense 64^3 chunks, 512 MB of block ids
+    resident on the device); the engine's own measurement of its CPU encoder
+    is 1325.9 us per chunk (its --bench-terrain "tree build")."""
+    import torch
+    from voxelcraft_menu_b200 import encode as E
+    from voxelcraft_menu_b200 import world as W
+    dense = W.recipe_dense_chunks(W.recipe_large_terrain())
+    n = len(dense)
+    d = torch.from_numpy(dense.view(np.int16)).to(f"cuda:{local}")
+    cap = 16384
+    out = E.DeviceTrees(n, cap, torch, d.device)
+    stream = torch.cuda.current_stream(d.device)
+    for _ in range(warmup):
+        E.gpu_encode(d, n, cap, torch, out)
+    ms = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        E.gpu_encode(d, n, cap, torch, out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = float(np.mean(ms))
+    host = out.to_host()
+    out_bytes = int(n * (64 + 8 + 4) + 24 * host.info["n_l1"].sum() + 8 * host.info["n_leaves"].sum() +
+                    4 * host.info["n_attrs"].sum() + 4 * host.info["n_palette"].sum())
+    algo = n * 64 ** 3 * 2 + out_bytes
+    peak, peak_kind = peaks()
+    rec = {"workload": "1024 dense 64^3 chunks of the 1024x256x1024 terrain (512 MB of u16 block ids on the device)",
+           "ms": t, "us_per_chunk": t * 1e3 / n, "chunks_per_s": n / (t * 1e-3),
+           "roofline": {"bound": "hbm", "achieved": algo / (t * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                        "frac": algo / (t * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
+                        "algorithmic_bytes_per_launch": algo},
+           "reference_cpu_us_per_chunk": 1325.9,
+           "l2": "not flushed: the 512 MB input is larger than L2"}
+    if cpu:
+        sample = dense[::16]
+        t0 = time.perf_counter()
+        E.cpu_build(sample, cap)
+        rec["cpu_restatement_us_per_chunk"] = (time.perf_counter() - t0) * 1e6 / len(sample)
+        rec["cpu_sample"] = f"{len(sample)} of the chunks, one host thread (vmw_build_tree)"
+    return rec
+
+
 def profile_traffic(kernel):
     """dram bytes per launch of kernel from the committed ncu summary, if any."""
     f = ROOT / "profiles" / f"k_{kernel}_1080p.md"
@@ -478,7 +525,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched probe views")
     ap.add_argument("--no-shade", action="store_true", help="skip the shading forward / adjoint")
     ap.add_argument("--no-sparse", action="store_true", help="skip the sparse-world views and the fit")
-    ap.add_argument("--no-filter", action="store_true", help="skip the shadow filter and the reflect frame")
+    ap.add_argument("--no-filter", action="store_true", help="skip the shadow filter, reflect frame and encoder")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -651,6 +698,8 @@ def main():
         extra["shading"] = bench_shading(local, max(5, min(args.steps, 20)), 5)
     if rank == 0 and not args.no_sparse:
         extra["sparse"] = bench_sparse(local)
+    if rank == 0 and not args.no_filter:
+        extra["encoder"] = bench_encoder(local, max(5, min(args.steps, 20)), 3, cpu=not args.no_cpu)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

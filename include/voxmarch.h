@@ -234,6 +234,20 @@ int vm_shade_backward(const void* d_gbuf, uint64_t n_pixels, const float* d_para
                       const float* d_grad_color, const float* d_target, double* d_grad_params, double* d_loss,
                       void* cuda_stream);
 
+/* The engine's dense -> 64-tree encoder (build_local, src/voxel/tree.rs:89-204,
+ * with encode_leaf src/voxel/attributes.rs:90-139) for n_chunks dense chunks
+ * at once, on the GPU; the engine runs it per chunk on the CPU (its
+ * --bench-terrain "tree build").  Device pointers, enqueued on cuda_stream:
+ * d_dense n_chunks x 64^3 block ids (index x | z<<6 | y<<12 within a chunk);
+ * per chunk c: d_info[c], d_l1[64 c ..], d_leaves[4096 c ..],
+ * d_attrs[4096 c ..], d_palette[palette_cap c ..] in the layout of
+ * vm_tree_info (vm_types.h).  A chunk whose palette needs more than
+ * palette_cap words has VM_TREE_PALETTE_OVERFLOW set, n_palette = the words
+ * needed and its first palette_cap words written.  The output equals vmw_build_tree's (the CPU restatement) and
+ * vmw_insert_tree puts it into a world.  No context, no allocation. */
+int vm_encode_trees(const uint16_t* d_dense, uint32_t n_chunks, uint32_t palette_cap, vm_tree_info* d_info,
+                    vm_tree_l1* d_l1, uint64_t* d_leaves, uint32_t* d_attrs, uint32_t* d_palette, void* cuda_stream);
+
 /* Device pointers of the context's buffers (valid until the next upload that
  * grows them), for zero-copy callers such as a torch binding. */
 typedef struct vm_device_ptrs {

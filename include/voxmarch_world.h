@@ -81,6 +81,18 @@ vmw_world* vmw_create(void);
 void vmw_destroy(vmw_world* w);
 /* World::insert_local(key, build_local(dense)); dense index x | z<<6 | y<<12 */
 int vmw_insert_dense(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z, const uint16_t* dense);
+/* build_local (src/voxel/tree.rs:89-204) of one dense chunk (64^3 block ids,
+ * index x | z<<6 | y<<12) into the flat layout that vm_encode_trees writes:
+ * info, up to 64 L1 nodes, up to 4096 leaf masks and attribute entries, and
+ * up to palette_cap palette words (more sets VM_TREE_PALETTE_OVERFLOW).  The
+ * CPU restatement of the engine's encoder: the GPU encoder's parity anchor. */
+int vmw_build_tree(const uint16_t* dense, uint32_t palette_cap, vm_tree_info* info, vm_tree_l1* l1,
+                   uint64_t* leaves, uint32_t* attrs, uint32_t* palette);
+/* World::insert_local (src/voxel/world.rs:63-175) of a chunk in that flat
+ * layout, e.g. from vm_encode_trees: the run / word pools dedup it exactly as
+ * vmw_insert_dense does.  Rejects an overflowed or inconsistent tree (1). */
+int vmw_insert_tree(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z, const vm_tree_info* info,
+                    const vm_tree_l1* l1, const uint64_t* leaves, const uint32_t* attrs, const uint32_t* palette);
 int vmw_remove(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z);
 /* World::get_block (src/voxel/world.rs:258-277) */
 uint32_t vmw_get_block(const vmw_world* w, int32_t x, int32_t y, int32_t z);
@@ -93,6 +105,9 @@ const uint32_t* vmw_leaves(const vmw_world* w);   /* n_leaves x vec2<u32> */
 const uint32_t* vmw_bricks(const vmw_world* w);   /* n_bricks x u32 */
 int vmw_generate(vmw_world* w, const vmw_recipe* r);
 int vmw_recipe_dense(const vmw_recipe* r, int32_t cx, int32_t cy, int32_t cz, uint16_t* dense);
+/* Every chunk of the recipe's world, chunk i = cx + nx (cy + ny cz) at
+ * dense + i * 64^3 (the order vmw_generate inserts them in). */
+int vmw_recipe_dense_all(const vmw_recipe* r, uint16_t* dense);
 int32_t vmw_recipe_height(const vmw_recipe* r, int32_t x, int32_t z);
 void vmw_camera_basis(float yaw, float pitch, float* fwd, float* right, float* up);
 uint32_t vmw_pairs_for(uint32_t tiles_x, uint32_t tiles_y);

@@ -129,6 +129,37 @@ static_assert(offsetof(vm_chunk, dry_mask) == 80, "dry_mask offset");
 #define VM_FULL_BIT 0x80000000u
 #define VM_PTR_MASK 0x7FFFFFFFu
 #define VM_UNIFORM_BIT 0x80000000u
+
+/* One chunk encoded into the 64-tree (build_local, src/voxel/tree.rs:89-204),
+ * flat: the LocalTree fields, its L1 nodes and its variable-length arrays
+ * (leaf masks, attribute entries, palette words) in the encoder's order. */
+#define VM_TREE_LEAVES 4096u          /* leaf masks / attribute entries per chunk at most */
+#define VM_TREE_L1 64u
+#define VM_TREE_WATER 1u
+#define VM_TREE_FOLIAGE 2u
+#define VM_TREE_CUTOUT 4u
+#define VM_TREE_GLASS 8u
+#define VM_TREE_EMITTER 16u
+#define VM_TREE_PALETTE_OVERFLOW 0x80000000u   /* n_palette words needed > palette_cap; palette truncated */
+typedef struct vm_tree_info {
+  uint64_t root_mask, dry_mask;
+  int32_t uniform;               /* the block id when every solid voxel has it, else -1 */
+  uint32_t flags;                /* VM_TREE_* */
+  uint32_t emitters, solid_count, leaf_count;
+  uint32_t n_l1, n_leaves, n_attrs, n_palette;
+  uint8_t aabb_min[3], aabb_max[3];
+  uint8_t pad[6];
+} vm_tree_info;
+typedef struct vm_tree_l1 {     /* LocalL1, src/voxel/tree.rs:37-46 */
+  uint64_t mask;
+  uint32_t leaf_start, leaf_prefix;
+  uint8_t full, water_line;
+  uint8_t pad[6];
+} vm_tree_l1;
+#ifdef __cplusplus
+static_assert(sizeof(vm_tree_info) == 64, "vm_tree_info layout");
+static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
+#endif
 #define VM_PREFIX_MASK 0x0FFFFFFFu
 #define VM_MAX_ITERS 512u             /* common.wgsl:163 */
 

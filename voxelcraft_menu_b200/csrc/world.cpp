@@ -531,6 +531,80 @@ int vmw_insert_dense(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z,
   return 0;
 }
 
+int vmw_build_tree(const uint16_t* dense, uint32_t palette_cap, vm_tree_info* info, vm_tree_l1* l1,
+                   uint64_t* leaves, uint32_t* attrs, uint32_t* palette) {
+  if (!dense || !info || !l1 || !leaves || !attrs || (palette_cap && !palette)) return 1;
+  const LocalTree t = build_local(dense);
+  memset(info, 0, sizeof *info);
+  info->root_mask = t.root_mask;
+  info->dry_mask = t.dry_mask;
+  info->uniform = t.uniform;
+  info->flags = (t.has_water ? VM_TREE_WATER : 0u) | (t.has_foliage ? VM_TREE_FOLIAGE : 0u) |
+                (t.has_cutout ? VM_TREE_CUTOUT : 0u) | (t.has_glass ? VM_TREE_GLASS : 0u) |
+                (t.has_emitter ? VM_TREE_EMITTER : 0u);
+  info->emitters = t.emitters;
+  info->solid_count = t.solid_count;
+  info->leaf_count = t.leaf_count;
+  info->n_l1 = (uint32_t)t.l1.size();
+  info->n_leaves = (uint32_t)t.leaves.size();
+  info->n_attrs = (uint32_t)t.attrs.size();
+  info->n_palette = (uint32_t)t.palette.size();
+  memcpy(info->aabb_min, t.aabb_min, 3);
+  memcpy(info->aabb_max, t.aabb_max, 3);
+  for (size_t i = 0; i < t.l1.size(); ++i) {
+    memset(&l1[i], 0, sizeof l1[i]);
+    l1[i].mask = t.l1[i].mask;
+    l1[i].leaf_start = t.l1[i].leaf_start;
+    l1[i].leaf_prefix = t.l1[i].leaf_prefix;
+    l1[i].full = t.l1[i].full ? 1 : 0;
+    l1[i].water_line = t.l1[i].water_line;
+  }
+  if (!t.leaves.empty()) memcpy(leaves, t.leaves.data(), t.leaves.size() * 8);
+  if (!t.attrs.empty()) memcpy(attrs, t.attrs.data(), t.attrs.size() * 4);
+  if (t.palette.size() > palette_cap) info->flags |= VM_TREE_PALETTE_OVERFLOW;
+  const size_t np = std::min<size_t>(t.palette.size(), palette_cap);
+  if (np) memcpy(palette, t.palette.data(), np * 4);
+  return 0;
+}
+
+int vmw_insert_tree(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z, const vm_tree_info* info,
+                    const vm_tree_l1* l1, const uint64_t* leaves, const uint32_t* attrs, const uint32_t* palette) {
+  if (!w || !info || (info->flags & VM_TREE_PALETTE_OVERFLOW) || info->n_l1 > VM_TREE_L1 ||
+      info->n_leaves > VM_TREE_LEAVES || info->n_attrs > VM_TREE_LEAVES)
+    return 1;
+  LocalTree t;
+  t.root_mask = info->root_mask;
+  t.dry_mask = info->dry_mask;
+  t.uniform = info->uniform;
+  t.has_water = (info->flags & VM_TREE_WATER) != 0u;
+  t.has_foliage = (info->flags & VM_TREE_FOLIAGE) != 0u;
+  t.has_cutout = (info->flags & VM_TREE_CUTOUT) != 0u;
+  t.has_glass = (info->flags & VM_TREE_GLASS) != 0u;
+  t.has_emitter = (info->flags & VM_TREE_EMITTER) != 0u;
+  t.emitters = info->emitters;
+  t.solid_count = info->solid_count;
+  t.leaf_count = info->leaf_count;
+  memcpy(t.aabb_min, info->aabb_min, 3);
+  memcpy(t.aabb_max, info->aabb_max, 3);
+  for (uint32_t i = 0; i < info->n_l1; ++i) {
+    LocalL1 n;
+    n.mask = l1[i].mask;
+    n.leaf_start = l1[i].leaf_start;
+    n.leaf_prefix = l1[i].leaf_prefix;
+    n.full = l1[i].full != 0;
+    n.water_line = l1[i].water_line;
+    if (!n.full && (uint64_t)n.leaf_start + (uint32_t)__builtin_popcountll(n.mask) > info->n_leaves) return 1;
+    t.l1.push_back(n);
+  }
+  t.leaves.assign(leaves, leaves + info->n_leaves);
+  t.attrs.assign(attrs, attrs + info->n_attrs);
+  t.palette.assign(palette, palette + info->n_palette);
+  ChunkKey k; k.lod = lod; k.x = x; k.y = y; k.z = z;
+  std::lock_guard<std::mutex> g(w->mu);
+  w->w.insert_local(k, t);
+  return 0;
+}
+
 int vmw_remove(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z) {
   ChunkKey k; k.lod = lod; k.x = x; k.y = y; k.z = z;
   return w->w.remove_chunk(k) ? 0 : 1;
@@ -602,6 +676,20 @@ int vmw_generate(vmw_world* w, const vmw_recipe* r) {
   for (int64_t i = 0; i < total; ++i) {
     ChunkKey k; k.lod = 0; k.x = (int32_t)(i % nx); k.y = (int32_t)((i / nx) % ny); k.z = (int32_t)(i / ((int64_t)nx * ny));
     w->w.insert_local(k, trees[i]);
+  }
+  return 0;
+}
+
+int vmw_recipe_dense_all(const vmw_recipe* r, uint16_t* dense) {
+  if (!r || !dense) return 1;
+  for (int i = 0; i < 3; ++i) if (r->size[i] == 0 || r->size[i] % 64 != 0) return 2;
+  Heights hs = make_heights(*r);
+  int32_t nx = r->size[0] / 64, ny = r->size[1] / 64, nz = r->size[2] / 64;
+  int64_t total = (int64_t)nx * ny * nz;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t i = 0; i < total; ++i) {
+    int32_t cx = (int32_t)(i % nx), cy = (int32_t)((i / nx) % ny), cz = (int32_t)(i / ((int64_t)nx * ny));
+    fill_chunk(*r, hs, cx, cy, cz, dense + (size_t)i * 64 * 64 * 64);
   }
   return 0;
 }

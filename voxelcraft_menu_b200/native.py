@@ -172,6 +172,9 @@ _SIGNATURES = [
     ("vmw_create", vp, []),
     ("vmw_destroy", None, [vp]),
     ("vmw_insert_dense", C.c_int, [vp, C.c_uint8, C.c_int32, C.c_int32, C.c_int32, vp]),
+    ("vmw_build_tree", C.c_int, [vp, C.c_uint32, vp, vp, vp, vp, vp]),
+    ("vmw_insert_tree", C.c_int, [vp, C.c_uint8, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp]),
+    ("vm_encode_trees", C.c_int, [vp, C.c_uint32, C.c_uint32, vp, vp, vp, vp, vp, vp]),
     ("vmw_remove", C.c_int, [vp, C.c_uint8, C.c_int32, C.c_int32, C.c_int32]),
     ("vmw_get_block", C.c_uint32, [vp, C.c_int32, C.c_int32, C.c_int32]),
     ("vmw_get_chunk_info", C.c_int, [vp, C.c_uint8, C.c_int32, C.c_int32, C.c_int32, P(VmwChunkInfo)]),
@@ -182,6 +185,7 @@ _SIGNATURES = [
     ("vmw_bricks", vp, [vp]),
     ("vmw_generate", C.c_int, [vp, P(VmwRecipe)]),
     ("vmw_recipe_dense", C.c_int, [P(VmwRecipe), C.c_int32, C.c_int32, C.c_int32, vp]),
+    ("vmw_recipe_dense_all", C.c_int, [P(VmwRecipe), vp]),
     ("vmw_recipe_height", C.c_int32, [P(VmwRecipe), C.c_int32, C.c_int32]),
     ("vmw_camera_basis", None, [C.c_float, C.c_float, vp, vp, vp]),
     ("vmw_pairs_for", C.c_uint32, [C.c_uint32, C.c_uint32]),

@@ -265,6 +265,16 @@ def halton_jitter(index: int):
     return float(out[0]), float(out[1])
 
 
+def recipe_dense_chunks(recipe: Recipe) -> np.ndarray:
+    """Every dense chunk of the recipe's world (n x 64^3 u16), chunk i at
+    (i % nx, i // nx % ny, i // (nx ny)), the order World.generate inserts."""
+    n = (recipe.size[0] // 64) * (recipe.size[1] // 64) * (recipe.size[2] // 64)
+    out = np.empty((n, 64 ** 3), np.uint16)
+    if lib().vmw_recipe_dense_all(C.byref(recipe.c()), ptr(out)):
+        raise RuntimeError("vmw_recipe_dense_all failed")
+    return out
+
+
 def surface_height(recipe: Recipe, x: int, z: int) -> int:
     return int(lib().vmw_recipe_height(C.byref(recipe.c()), x, z))
 
