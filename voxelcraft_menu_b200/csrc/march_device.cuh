@@ -583,33 +583,38 @@ template <bool COUNT>
 __device__ __forceinline__ bool shadow_walk_step(const DevWorld& w, const vm_frame& f, ShadowWalk& s, float max_dist,
                                                  float* out, Traffic* tr) {
   *out = -1.0f;
-  if (s.step >= 24u) return true;
-  uint64_t gi;
-  if (!grid_rel(f, s.cx, s.cy, s.cz, &gi)) return true;
-  if (COUNT) tr->grid++;
-  const uint32_t ci = ld_grid(w, gi);
-  if (ci != VM_NO_CHUNK && ci != s.last) {
-    s.last = ci;
-    const Chunk c = ld_chunk(w, ci);
-    const Hit m = march_chunk<true, true, true, COUNT>(w, f, c, s.r, max_dist, tr);
-    if (m.hit) { *out = m.t; return true; }
+  // cells that march nothing (no chunk, or the chunk just marched) are
+  // crossed in the same call, so that the lanes of a warp march together
+  for (;;) {
+    if (s.step >= 24u) return true;
+    uint64_t gi;
+    if (!grid_rel(f, s.cx, s.cy, s.cz, &gi)) return true;
+    if (COUNT) tr->grid++;
+    const uint32_t ci = ld_grid(w, gi);
+    const bool marched = ci != VM_NO_CHUNK && ci != s.last;
+    if (marched) {
+      s.last = ci;
+      const Chunk c = ld_chunk(w, ci);
+      const Hit m = march_chunk<true, true, true, COUNT>(w, f, c, s.r, max_dist, tr);
+      if (m.hit) { *out = m.t; return true; }
+    }
+    const Ray& r = s.r;
+    const float bx = (float)(r.pdx ? s.cx + 1 : s.cx) * 64.0f;
+    const float by = (float)(r.pdy ? s.cy + 1 : s.cy) * 64.0f;
+    const float bz = (float)(r.pdz ? s.cz + 1 : s.cz) * 64.0f;
+    const float tnx = (bx - r.o.x) * r.inv.x, tny = (by - r.o.y) * r.inv.y, tnz = (bz - r.o.z) * r.inv.z;
+    float t;
+    uint32_t axis = 0u;
+    if (tnx <= tny && tnx <= tnz) t = tnx;
+    else if (tny <= tnz) { t = tny; axis = 1u; }
+    else { t = tnz; axis = 2u; }
+    if (t >= max_dist) return true;
+    if (axis == 0) s.cx += r.pdx ? 1 : -1;
+    else if (axis == 1) s.cy += r.pdy ? 1 : -1;
+    else s.cz += r.pdz ? 1 : -1;
+    ++s.step;
+    if (marched) return false;
   }
-  const Ray& r = s.r;
-  const float bx = (float)(r.pdx ? s.cx + 1 : s.cx) * 64.0f;
-  const float by = (float)(r.pdy ? s.cy + 1 : s.cy) * 64.0f;
-  const float bz = (float)(r.pdz ? s.cz + 1 : s.cz) * 64.0f;
-  const float tnx = (bx - r.o.x) * r.inv.x, tny = (by - r.o.y) * r.inv.y, tnz = (bz - r.o.z) * r.inv.z;
-  float t;
-  uint32_t axis = 0u;
-  if (tnx <= tny && tnx <= tnz) t = tnx;
-  else if (tny <= tnz) { t = tny; axis = 1u; }
-  else { t = tnz; axis = 2u; }
-  if (t >= max_dist) return true;
-  if (axis == 0) s.cx += r.pdx ? 1 : -1;
-  else if (axis == 1) s.cy += r.pdy ? 1 : -1;
-  else s.cz += r.pdz ? 1 : -1;
-  ++s.step;
-  return false;
 }
 
 struct WorldHit { bool hit; float t; uint32_t normal; uint32_t vx, vy, vz; uint32_t ci; };
@@ -679,35 +684,39 @@ template <bool SKIP_WATER, bool COUNT>
 __device__ __forceinline__ bool world_walk_step(const DevWorld& w, const vm_frame& f, WorldWalk& s, float max_dist,
                                                 WorldHit* out, Traffic* tr) {
   out->hit = false; out->t = max_dist; out->normal = 0u; out->vx = out->vy = out->vz = 0u; out->ci = VM_NO_CHUNK;
-  if (s.step >= 16u) return true;
-  uint64_t gi;
-  if (!grid_rel(f, s.cx, s.cy, s.cz, &gi)) return true;
-  if (COUNT) tr->grid++;
-  const uint32_t ci = ld_grid(w, gi);
-  const float bx = (float)(s.pdx ? s.cx + 1 : s.cx) * 64.0f;
-  const float by = (float)(s.pdy ? s.cy + 1 : s.cy) * 64.0f;
-  const float bz = (float)(s.pdz ? s.cz + 1 : s.cz) * 64.0f;
-  const F3 ro = s.r.o;
-  const float tnx = (bx - ro.x) * s.inv.x, tny = (by - ro.y) * s.inv.y, tnz = (bz - ro.z) * s.inv.z;
-  float t_exit = tnx;
-  uint32_t axis = 0u;
-  if (tny < t_exit) { t_exit = tny; axis = 1u; }
-  if (tnz < t_exit) { t_exit = tnz; axis = 2u; }
-  if (ci != VM_NO_CHUNK) {
-    const Chunk c = ld_chunk(w, ci);
-    const Hit h = march_chunk<SKIP_WATER, true, false, COUNT>(w, f, c, s.r, fminf(t_exit, max_dist), tr);
-    if (h.hit) {
-      out->hit = true; out->t = h.t; out->normal = h.normal;
-      out->vx = h.vx; out->vy = h.vy; out->vz = h.vz; out->ci = ci;
-      return true;
+  // cells without a chunk are crossed in the same call (see shadow_walk_step)
+  for (;;) {
+    if (s.step >= 16u) return true;
+    uint64_t gi;
+    if (!grid_rel(f, s.cx, s.cy, s.cz, &gi)) return true;
+    if (COUNT) tr->grid++;
+    const uint32_t ci = ld_grid(w, gi);
+    const float bx = (float)(s.pdx ? s.cx + 1 : s.cx) * 64.0f;
+    const float by = (float)(s.pdy ? s.cy + 1 : s.cy) * 64.0f;
+    const float bz = (float)(s.pdz ? s.cz + 1 : s.cz) * 64.0f;
+    const F3 ro = s.r.o;
+    const float tnx = (bx - ro.x) * s.inv.x, tny = (by - ro.y) * s.inv.y, tnz = (bz - ro.z) * s.inv.z;
+    float t_exit = tnx;
+    uint32_t axis = 0u;
+    if (tny < t_exit) { t_exit = tny; axis = 1u; }
+    if (tnz < t_exit) { t_exit = tnz; axis = 2u; }
+    const bool marched = ci != VM_NO_CHUNK;
+    if (marched) {
+      const Chunk c = ld_chunk(w, ci);
+      const Hit h = march_chunk<SKIP_WATER, true, false, COUNT>(w, f, c, s.r, fminf(t_exit, max_dist), tr);
+      if (h.hit) {
+        out->hit = true; out->t = h.t; out->normal = h.normal;
+        out->vx = h.vx; out->vy = h.vy; out->vz = h.vz; out->ci = ci;
+        return true;
+      }
     }
+    if (t_exit >= max_dist) return true;
+    if (axis == 0) s.cx += s.pdx ? 1 : -1;
+    else if (axis == 1) s.cy += s.pdy ? 1 : -1;
+    else s.cz += s.pdz ? 1 : -1;
+    ++s.step;
+    if (marched) return false;
   }
-  if (t_exit >= max_dist) return true;
-  if (axis == 0) s.cx += s.pdx ? 1 : -1;
-  else if (axis == 1) s.cy += s.pdy ? 1 : -1;
-  else s.cz += s.pdz ? 1 : -1;
-  ++s.step;
-  return false;
 }
 
 // hit_t: common.wgsl:1300-1318
