@@ -583,20 +583,22 @@ template <bool COUNT>
 __device__ __forceinline__ bool shadow_walk_step(const DevWorld& w, const vm_frame& f, ShadowWalk& s, float max_dist,
                                                  float* out, Traffic* tr) {
   *out = -1.0f;
-  // cells that march nothing (no chunk, or the chunk just marched) are
-  // crossed in the same call, so that the lanes of a warp march together
+  // cells that march nothing (no chunk, the chunk just marched, or a march
+  // that returns before its first DDA step) are crossed in the same call, so
+  // that the lanes of a warp march together
   for (;;) {
     if (s.step >= 24u) return true;
     uint64_t gi;
     if (!grid_rel(f, s.cx, s.cy, s.cz, &gi)) return true;
     if (COUNT) tr->grid++;
     const uint32_t ci = ld_grid(w, gi);
-    const bool marched = ci != VM_NO_CHUNK && ci != s.last;
-    if (marched) {
+    bool marched = false;   // a chunk march that took DDA steps
+    if (ci != VM_NO_CHUNK && ci != s.last) {
       s.last = ci;
       const Chunk c = ld_chunk(w, ci);
       const Hit m = march_chunk<true, true, true, COUNT>(w, f, c, s.r, max_dist, tr);
       if (m.hit) { *out = m.t; return true; }
+      marched = m.iters > 0u;
     }
     const Ray& r = s.r;
     const float bx = (float)(r.pdx ? s.cx + 1 : s.cx) * 64.0f;
@@ -684,7 +686,8 @@ template <bool SKIP_WATER, bool COUNT>
 __device__ __forceinline__ bool world_walk_step(const DevWorld& w, const vm_frame& f, WorldWalk& s, float max_dist,
                                                 WorldHit* out, Traffic* tr) {
   out->hit = false; out->t = max_dist; out->normal = 0u; out->vx = out->vy = out->vz = 0u; out->ci = VM_NO_CHUNK;
-  // cells without a chunk are crossed in the same call (see shadow_walk_step)
+  // cells without a chunk, or whose march takes no DDA step, are crossed in
+  // the same call (see shadow_walk_step)
   for (;;) {
     if (s.step >= 16u) return true;
     uint64_t gi;
@@ -700,8 +703,8 @@ __device__ __forceinline__ bool world_walk_step(const DevWorld& w, const vm_fram
     uint32_t axis = 0u;
     if (tny < t_exit) { t_exit = tny; axis = 1u; }
     if (tnz < t_exit) { t_exit = tnz; axis = 2u; }
-    const bool marched = ci != VM_NO_CHUNK;
-    if (marched) {
+    bool marched = false;   // a chunk march that took DDA steps
+    if (ci != VM_NO_CHUNK) {
       const Chunk c = ld_chunk(w, ci);
       const Hit h = march_chunk<SKIP_WATER, true, false, COUNT>(w, f, c, s.r, fminf(t_exit, max_dist), tr);
       if (h.hit) {
@@ -709,6 +712,7 @@ __device__ __forceinline__ bool world_walk_step(const DevWorld& w, const vm_fram
         out->vx = h.vx; out->vy = h.vy; out->vz = h.vz; out->ci = ci;
         return true;
       }
+      marched = h.iters > 0u;
     }
     if (t_exit >= max_dist) return true;
     if (axis == 0) s.cx += s.pdx ? 1 : -1;
