@@ -393,12 +393,24 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
     unsigned long long best = 0ull;
     uint32_t best_id = 0u;
     bool active = valid;
-    for (uint32_t i = 0; i < m && active; ++i) {
-      const uint32_t ci = list[i];
-      const uint32_t bestd = (uint32_t)(best >> 40);
-      if (suf[ci] < bestd) { active = false; break; }
-      if (dk[ci] < bestd) continue;
-      march_entry<UNDERWATER, COUNT>(w, f, ray, ci, px, py, best, best_id, &tr);
+    // Each lane walks its list in order with the same tests as ever; the
+    // entries a lane skips (a closer key already found) are passed in an
+    // inner loop, so that every round of the warp is one chunk march for
+    // each lane that still has one.
+    for (uint32_t i = 0;;) {
+      uint32_t ci = 0;
+      bool go = false;
+      while (active && i < m) {
+        ci = list[i];
+        const uint32_t bestd = (uint32_t)(best >> 40);
+        if (suf[ci] < bestd) { active = false; break; }
+        ++i;
+        if (dk[ci] < bestd) continue;
+        go = true;
+        break;
+      }
+      if (!__any_sync(FULLMASK, go)) break;
+      if (go) march_entry<UNDERWATER, COUNT>(w, f, ray, ci, px, py, best, best_id, &tr);
     }
     if (n > a.list_cap)
       march_overflow<UNDERWATER, COUNT>(w, f, ray, (uint32_t)list[a.list_cap - 1] + 1u, tx, ty, px, py, dk, suf,
