@@ -490,7 +490,8 @@ def bench_encoder(local, steps, warmup, cpu=True):
            "ms": t, "us_per_chunk": t * 1e3 / n, "chunks_per_s": n / (t * 1e-3),
            "roofline": {"bound": "hbm", "achieved": algo / (t * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                         "frac": algo / (t * 1e-3) / 1e9 / peak, "peak_kind": peak_kind,
-                        "algorithmic_bytes_per_launch": algo},
+                        "algorithmic_bytes_per_launch": algo,
+                        "traffic": profile_traffic("encode", "1024_chunks")},
            "reference_cpu_us_per_chunk": 1325.9,
            "l2": "not flushed: the 512 MB input is larger than L2"}
     if cpu:
@@ -502,9 +503,9 @@ def bench_encoder(local, steps, warmup, cpu=True):
     return rec
 
 
-def profile_traffic(kernel):
+def profile_traffic(kernel, workload="1080p"):
     """dram bytes per launch of kernel from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / f"k_{kernel}_1080p.md"
+    f = ROOT / "profiles" / f"k_{kernel}_{workload}.md"
     if not f.exists():
         return None
     for line in f.read_text().splitlines():
