@@ -127,6 +127,7 @@ struct PipeTuning {
 // primary, shadow and secondary kernels.
 cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwater, bool count, int sms,
                             cudaStream_t s, const cudaEvent_t* ev = nullptr);
-int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bool reflect = false);
+int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bool reflect = false,
+                            bool single = true);
 
 }  // namespace vmk

@@ -48,6 +48,16 @@ __device__ __forceinline__ DevWorld world_of(const PipeArgs& a, const ViewDesc& 
           a.bricks, a.n_bricks, a.grids + vd.grid_off, vd.grid_len, a.err};
 }
 
+// The same, resolved at compile time when the launch is known to carry one
+// view (frames == nullptr): the frame, view and world then come from the
+// kernel's parameter space instead of registers.
+template <bool SINGLE>
+__device__ __forceinline__ uint32_t find_view_t(const PipeArgs& a, uint32_t tile) { return SINGLE ? 0u : find_view(a, tile); }
+template <bool SINGLE>
+__device__ __forceinline__ const vm_frame& frame_t(const PipeArgs& a, uint32_t v) { return SINGLE ? a.frame0 : a.frames[v]; }
+template <bool SINGLE>
+__device__ __forceinline__ ViewDesc view_t(const PipeArgs& a, uint32_t v) { return SINGLE ? a.view0 : a.views[v]; }
+
 struct MaxOp {
   __device__ __forceinline__ uint32_t operator()(uint32_t x, uint32_t y) const { return x > y ? x : y; }
 };
@@ -360,8 +370,8 @@ __device__ __noinline__ void enqueue_reflect(const PipeArgs& a, uint32_t v, uint
 // MINB: blocks per SM the register allocation must allow (1: unconstrained),
 // the autotuner's occupancy knob.
 // REFL: the frame may trace reflect legs (a.do_reflect); without it the
-// kernel carries none of that code.
-template <int NW, int MINB, bool UNDERWATER, bool COUNT, bool REFL>
+// kernel carries none of that code.  SINGLE: the launch has one view.
+template <int NW, int MINB, bool UNDERWATER, bool COUNT, bool REFL, bool SINGLE>
 __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant__ PipeArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t total = a.total_tiles * 2u;
@@ -374,9 +384,9 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
     if (item >= total) break;
     const long long clk0 = clock64();
     const uint32_t t = a.tile_order[item >> 1], half = item & 1u;
-    const uint32_t v = find_view(a, t);
-    const vm_frame& f = frame_of(a, v);
-    const ViewDesc vd = view_of(a, v);
+    const uint32_t v = find_view_t<SINGLE>(a, t);
+    const vm_frame& f = frame_t<SINGLE>(a, v);
+    const ViewDesc vd = view_t<SINGLE>(a, v);
     const DevWorld w = world_of(a, vd);
     const uint32_t local = t - vd.tile_begin;
     const uint32_t tx = local % vd.tiles_x, ty = local / vd.tiles_x;
@@ -639,37 +649,44 @@ struct MinBlocks {
 };
 
 template <int NW, int LEVEL, bool UW>
-static void* primary_fn(bool cnt, bool refl) {
+static void* primary_fn(bool refl, bool single) {
   constexpr int MB = MinBlocks<NW, LEVEL>::value;
-  if (cnt) return (void*)k_primary<NW, MB, UW, true, true>;   // counting kernels keep the runtime gate
-  return refl ? (void*)k_primary<NW, MB, UW, false, true> : (void*)k_primary<NW, MB, UW, false, false>;
+  if (!single) return (void*)k_primary<NW, MB, UW, false, false, false>;   // batches trace no reflect legs
+  return refl ? (void*)k_primary<NW, MB, UW, false, true, true> : (void*)k_primary<NW, MB, UW, false, false, true>;
 }
 
 template <int NW>
-static void* primary_nw(int level, bool uw, bool cnt, bool refl) {
+static void* primary_nw(int level, bool uw, bool refl, bool single) {
   switch (level) {
-    case 0: return uw ? primary_fn<NW, 0, true>(cnt, refl) : primary_fn<NW, 0, false>(cnt, refl);
-    case 1: return uw ? primary_fn<NW, 1, true>(cnt, refl) : primary_fn<NW, 1, false>(cnt, refl);
-    case 2: return uw ? primary_fn<NW, 2, true>(cnt, refl) : primary_fn<NW, 2, false>(cnt, refl);
-    case 3: return uw ? primary_fn<NW, 3, true>(cnt, refl) : primary_fn<NW, 3, false>(cnt, refl);
-    case 4: return uw ? primary_fn<NW, 4, true>(cnt, refl) : primary_fn<NW, 4, false>(cnt, refl);
+    case 0: return uw ? primary_fn<NW, 0, true>(refl, single) : primary_fn<NW, 0, false>(refl, single);
+    case 1: return uw ? primary_fn<NW, 1, true>(refl, single) : primary_fn<NW, 1, false>(refl, single);
+    case 2: return uw ? primary_fn<NW, 2, true>(refl, single) : primary_fn<NW, 2, false>(refl, single);
+    case 3: return uw ? primary_fn<NW, 3, true>(refl, single) : primary_fn<NW, 3, false>(refl, single);
+    case 4: return uw ? primary_fn<NW, 4, true>(refl, single) : primary_fn<NW, 4, false>(refl, single);
   }
   return nullptr;
 }
 
-static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt, bool refl) {
-  if (cnt) return primary_nw<4>(0, uw, true, true);   // the counting run is never timed
+// the counting run is never timed: 4 warps, unconstrained registers, the
+// reflect code behind its runtime flag
+static void* primary_count(bool uw, bool single) {
+  if (single) return uw ? (void*)k_primary<4, 1, true, true, true, true> : (void*)k_primary<4, 1, false, true, true, true>;
+  return uw ? (void*)k_primary<4, 1, true, true, false, false> : (void*)k_primary<4, 1, false, true, false, false>;
+}
+
+static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt, bool refl, bool single) {
+  if (cnt) return primary_count(uw, single);
   switch (t.primary_warps) {
-    case 4: return primary_nw<4>(t.reg_level, uw, false, refl);
-    case 8: return primary_nw<8>(t.reg_level, uw, false, refl);
+    case 4: return primary_nw<4>(t.reg_level, uw, refl, single);
+    case 8: return primary_nw<8>(t.reg_level, uw, refl, single);
   }
   return nullptr;
 }
 
 static int block_warps(const PipeTuning& t, bool cnt) { return cnt ? 4 : t.primary_warps; }
 
-int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bool reflect) {
-  void* fn = primary_kernel(t, underwater, count, reflect);
+int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bool reflect, bool single) {
+  void* fn = primary_kernel(t, underwater, count, reflect, single);
   if (!fn) return 0;
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block_warps(t, count) * 32, 0);
@@ -693,11 +710,12 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   k_cull<<<cull_blocks, 256, 0, s>>>(a);
   k_order<<<(a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256, 0, s>>>(a);
   if ((e = mark(1)) != cudaSuccess) return e;
-  const bool refl = a.do_reflect != 0u;
-  void* fn = primary_kernel(t, underwater, count, refl);
+  const bool refl = a.do_reflect != 0u, single = a.frames == nullptr;
+  void* fn = primary_kernel(t, underwater, count, refl, single);
   if (!fn) return cudaErrorInvalidValue;
   const int nw = block_warps(t, count);
-  int per = t.ctas_per_sm > 0 && !count ? t.ctas_per_sm : primary_max_ctas_per_sm(t, underwater, count, refl);
+  int per = t.ctas_per_sm > 0 && !count ? t.ctas_per_sm
+                                        : primary_max_ctas_per_sm(t, underwater, count, refl, single);
   if (per <= 0) per = 1;
   const uint32_t items_blocks = (a.total_tiles * 2u + nw - 1) / nw;
   const uint32_t grid = std::min<uint32_t>((uint32_t)sms * (uint32_t)per, items_blocks);
