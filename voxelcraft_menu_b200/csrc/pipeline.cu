@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
 // (warp-aggregated), so a warp never idles behind its longest ray.  With soft
 // shadows a queue item is VM_SOFT_SAMPLES jittered rays from the same origin,
 // walked one after the other by the lane; the pixel gets the blocked fraction.
-template <bool COUNT>
+template <bool COUNT, bool SINGLE>
 __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeArgs a) {
   const uint32_t n = a.work[W_SHADOW_N];
   const uint32_t lane = threadIdx.x & 31u;
@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
           origin = f3(q.o[0], q.o[1], q.o[2]);
           sample = 0u;
           blocked = 0u;
-          const vm_frame& f = frame_of(a, view);
+          const vm_frame& f = frame_t<SINGLE>(a, view);
           s = shadow_walk_begin(origin, soft_shadows(f) ? soft_sun_dir(f, pix % f.res[0], pix / f.res[0], 0u)
                                                         : ld3(f.sun_dir));
           has = true;
@@ -550,8 +550,8 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
     }
     if (__ballot_sync(FULLMASK, has) == 0u) break;
     if (has) {
-      const vm_frame& f = frame_of(a, view);
-      const ViewDesc vd = view_of(a, view);
+      const vm_frame& f = frame_t<SINGLE>(a, view);
+      const ViewDesc vd = view_t<SINGLE>(a, view);
       const DevWorld w = world_of(a, vd);
       float b;
       if (shadow_walk_step<COUNT>(w, f, s, f.shadow_dist, &b, &tr)) {
@@ -578,7 +578,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
 // refract and reflect legs of water hits, transmission through glass — on
 // persistent lanes like k_shadow: one chunk-grid cell per step, the next ray
 // taken as soon as a lane's ray ends.
-template <bool COUNT>
+template <bool COUNT, bool SINGLE>
 __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ PipeArgs a) {
   const uint32_t n = a.work[W_SEC_N];
   const uint32_t lane = threadIdx.x & 31u;
@@ -612,8 +612,8 @@ __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ 
     }
     if (__ballot_sync(FULLMASK, has) == 0u) break;
     if (has) {
-      const vm_frame& f = frame_of(a, view);
-      const ViewDesc vd = view_of(a, view);
+      const vm_frame& f = frame_t<SINGLE>(a, view);
+      const ViewDesc vd = view_t<SINGLE>(a, view);
       const DevWorld w = world_of(a, vd);
       WorldHit h;
       const bool over = water ? world_walk_step<true, COUNT>(w, f, s, max_dist, &h, &tr)
@@ -724,13 +724,17 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   if ((e = mark(2)) != cudaSuccess) return e;
   const uint32_t q_blocks = (uint32_t)sms * 8u;
   if (a.do_shadow) {
-    if (count) k_shadow<true><<<q_blocks, 256, 0, s>>>(a);
-    else k_shadow<false><<<q_blocks, 256, 0, s>>>(a);
+    if (count && single) k_shadow<true, true><<<q_blocks, 256, 0, s>>>(a);
+    else if (count) k_shadow<true, false><<<q_blocks, 256, 0, s>>>(a);
+    else if (single) k_shadow<false, true><<<q_blocks, 256, 0, s>>>(a);
+    else k_shadow<false, false><<<q_blocks, 256, 0, s>>>(a);
   }
   if ((e = mark(3)) != cudaSuccess) return e;
   if (a.do_secondary) {
-    if (count) k_secondary_q<true><<<q_blocks, 256, 0, s>>>(a);
-    else k_secondary_q<false><<<q_blocks, 256, 0, s>>>(a);
+    if (count && single) k_secondary_q<true, true><<<q_blocks, 256, 0, s>>>(a);
+    else if (count) k_secondary_q<true, false><<<q_blocks, 256, 0, s>>>(a);
+    else if (single) k_secondary_q<false, true><<<q_blocks, 256, 0, s>>>(a);
+    else k_secondary_q<false, false><<<q_blocks, 256, 0, s>>>(a);
   }
   if ((e = mark(4)) != cudaSuccess) return e;
   return cudaGetLastError();
