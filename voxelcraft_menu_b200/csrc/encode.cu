@@ -127,18 +127,35 @@ __global__ void __launch_bounds__(ENC_THREADS) k_encode(const uint16_t* __restri
         continue;
       }
       if (m != ~0ull) all_full = false;
-      uint32_t p0, p1, first = 0u;
-      const uint32_t n = enc_palette(id0, id1, in0, in1, &p0, &p1, &first, nullptr);
+      // the first present voxel's id; a leaf of that id alone (the common
+      // case) needs no palette rounds and its statistics are the id's
+      const uint32_t fv = (uint32_t)__ffsll((long long)m) - 1u;
+      uint32_t first = __shfl_sync(ENC_FULL, fv >= 32u ? id1 : id0, (int)(fv & 31u));
+      const bool one = __all_sync(ENC_FULL, (!in0 || id0 == first) && (!in1 || id1 == first));
+      uint32_t n = 1u;
+      if (!one) {
+        uint32_t p0, p1;
+        n = enc_palette(id0, id1, in0, in1, &p0, &p1, &first, nullptr);
+      }
       if (lane == 0) { s.mask[g] = m; s.words[g] = (uint8_t)enc_words(n); s.pal0[g] = (uint16_t)first; }
-      // the lane's statistics
-      const bool w0 = in0 && id0 == VM_WATER, w1 = in1 && id1 == VM_WATER;
-      const bool d0 = in0 && !w0, d1 = in1 && !w1;
-      if (w0 || w1) flags |= VM_TREE_WATER;
-      if (d0 || d1) { dry = true; top = max(top, ly * 4u + vy + 1u); }
-      if ((in0 && enc_foliage(id0)) || (in1 && enc_foliage(id1))) flags |= VM_TREE_FOLIAGE;
-      if ((in0 && enc_cutout(id0)) || (in1 && enc_cutout(id1))) flags |= VM_TREE_CUTOUT;
-      if ((in0 && id0 == VM_GLASS) || (in1 && id1 == VM_GLASS)) flags |= VM_TREE_GLASS;
-      emitters += (in0 && enc_emitter(id0) ? 1u : 0u) + (in1 && enc_emitter(id1) ? 1u : 0u);
+      if (one) {
+        if (first == VM_WATER) flags |= VM_TREE_WATER;
+        else if (in0 || in1) { dry = true; top = max(top, ly * 4u + vy + 1u); }
+        if (enc_foliage(first)) flags |= VM_TREE_FOLIAGE;
+        if (enc_cutout(first)) flags |= VM_TREE_CUTOUT;
+        if (first == VM_GLASS) flags |= VM_TREE_GLASS;
+        if (enc_emitter(first) && lane == 0) emitters += (uint32_t)__popcll(m);
+      } else {
+        // the lane's statistics
+        const bool w0 = in0 && id0 == VM_WATER, w1 = in1 && id1 == VM_WATER;
+        const bool d0 = in0 && !w0, d1 = in1 && !w1;
+        if (w0 || w1) flags |= VM_TREE_WATER;
+        if (d0 || d1) { dry = true; top = max(top, ly * 4u + vy + 1u); }
+        if ((in0 && enc_foliage(id0)) || (in1 && enc_foliage(id1))) flags |= VM_TREE_FOLIAGE;
+        if ((in0 && enc_cutout(id0)) || (in1 && enc_cutout(id1))) flags |= VM_TREE_CUTOUT;
+        if ((in0 && id0 == VM_GLASS) || (in1 && id1 == VM_GLASS)) flags |= VM_TREE_GLASS;
+        emitters += (in0 && enc_emitter(id0) ? 1u : 0u) + (in1 && enc_emitter(id1) ? 1u : 0u);
+      }
       if (in0 || in1) {
         const uint32_t x = bx + vx, y = by + vy;
         mn[0] = min(mn[0], x); mx[0] = max(mx[0], x + 1u);

@@ -154,13 +154,14 @@ __device__ __forceinline__ bool super_keep(const vm_frame& f, const F3* n, F3 ca
   return box_distance(cam, bmin, bmax) < f.far_;
 }
 
+template <bool SINGLE>
 __global__ void __launch_bounds__(256) k_cull_super(const __grid_constant__ PipeArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t n_warps = gridDim.x * 8u;
   for (uint32_t s = blockIdx.x * 8u + (threadIdx.x >> 5); s < a.total_supers; s += n_warps) {
-    const uint32_t v = find_view_super(a, s);
-    const vm_frame& f = frame_of(a, v);
-    const ViewDesc vd = view_of(a, v);
+    const uint32_t v = SINGLE ? 0u : find_view_super(a, s);
+    const vm_frame& f = frame_t<SINGLE>(a, v);
+    const ViewDesc vd = view_t<SINGLE>(a, v);
     const uint32_t local = s - vd.super_begin, sxv = (vd.tiles_x + 3u) >> 2;
     F3 d[5], n[4];
     square_dirs_warp(f, (local % sxv) * 32u, (local / sxv) * 32u, 32.0f, lane, d);
@@ -184,13 +185,14 @@ __global__ void __launch_bounds__(256) k_cull_super(const __grid_constant__ Pipe
   }
 }
 
+template <bool SINGLE>
 __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t n_warps = gridDim.x * 8u;
   for (uint32_t t = blockIdx.x * 8u + (threadIdx.x >> 5); t < a.total_tiles; t += n_warps) {
-    const uint32_t v = find_view(a, t);
-    const vm_frame& f = frame_of(a, v);
-    const ViewDesc vd = view_of(a, v);
+    const uint32_t v = find_view_t<SINGLE>(a, t);
+    const vm_frame& f = frame_t<SINGLE>(a, v);
+    const ViewDesc vd = view_t<SINGLE>(a, v);
     const uint32_t local = t - vd.tile_begin;
     const uint32_t tx = local % vd.tiles_x, ty = local / vd.tiles_x;
     const TilePlanes tp = tile_planes_warp(f, tx * 8u, ty * 8u, lane);
@@ -706,8 +708,14 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   }
   k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
   const uint32_t cull_blocks = std::min<uint32_t>((a.total_tiles + 7) / 8, (uint32_t)sms * 16u);
-  k_cull_super<<<std::min<uint32_t>((a.total_supers + 7) / 8, (uint32_t)sms * 16u), 256, 0, s>>>(a);
-  k_cull<<<cull_blocks, 256, 0, s>>>(a);
+  const uint32_t super_blocks = std::min<uint32_t>((a.total_supers + 7) / 8, (uint32_t)sms * 16u);
+  if (a.frames == nullptr) {
+    k_cull_super<true><<<super_blocks, 256, 0, s>>>(a);
+    k_cull<true><<<cull_blocks, 256, 0, s>>>(a);
+  } else {
+    k_cull_super<false><<<super_blocks, 256, 0, s>>>(a);
+    k_cull<false><<<cull_blocks, 256, 0, s>>>(a);
+  }
   k_order<<<(a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256, 0, s>>>(a);
   if ((e = mark(1)) != cudaSuccess) return e;
   const bool refl = a.do_reflect != 0u, single = a.frames == nullptr;
