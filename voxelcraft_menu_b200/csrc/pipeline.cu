@@ -185,32 +185,86 @@ __global__ void __launch_bounds__(256) k_cull_super(const __grid_constant__ Pipe
   }
 }
 
+// tile_select's per-chunk test (cull_keep) on a box staged in shared memory
+__device__ __forceinline__ bool cull_keep_box(const vm_frame& f, const TilePlanes& tp, F3 cam, F3 fwd, F3 bmin,
+                                              F3 bmax, uint32_t ci) {
+  if (ci == f.camera_chunk) return true;
+  if (box_outside(bmin, bmax, fwd, cam) || box_outside(bmin, bmax, tp.n[0], cam) ||
+      box_outside(bmin, bmax, tp.n[1], cam) || box_outside(bmin, bmax, tp.n[2], cam) ||
+      box_outside(bmin, bmax, tp.n[3], cam))
+    return false;
+  return box_distance(cam, bmin, bmax) < tp.reach;
+}
+
+// cull_keep_box for a survivor of the super-tile cull (super_keep): it has
+// passed the same near-plane test (box_outside with the camera's forward
+// axis) and box_distance < far, so only the tile's four side planes remain,
+// and the reach when the tile's is shorter than far.
+__device__ __forceinline__ bool cull_keep_survivor(const vm_frame& f, const TilePlanes& tp, F3 cam, F3 bmin,
+                                                   F3 bmax, uint32_t ci, bool far_reach) {
+  if (ci == f.camera_chunk) return true;
+  if (box_outside(bmin, bmax, tp.n[0], cam) || box_outside(bmin, bmax, tp.n[1], cam) ||
+      box_outside(bmin, bmax, tp.n[2], cam) || box_outside(bmin, bmax, tp.n[3], cam))
+    return false;
+  return far_reach || box_distance(cam, bmin, bmax) < tp.reach;
+}
+
+// One block per 32x32 super-tile, one warp per 8x8 tile of it: the block
+// stages its candidates' boxes (the super-tile's survivors, or every chunk
+// when it has no list) in shared memory, CULL_BATCH at a time with coalesced
+// loads, and each warp runs tile_select's exact test on them in ascending
+// chunk order, so every tile gets the same list as from a warp that read
+// the boxes from global memory itself.
+constexpr uint32_t CULL_THREADS = 512, CULL_BATCH = 256;
 template <bool SINGLE>
-__global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a) {
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t n_warps = gridDim.x * 8u;
-  for (uint32_t t = blockIdx.x * 8u + (threadIdx.x >> 5); t < a.total_tiles; t += n_warps) {
-    const uint32_t v = find_view_t<SINGLE>(a, t);
-    const vm_frame& f = frame_t<SINGLE>(a, v);
-    const ViewDesc vd = view_t<SINGLE>(a, v);
-    const uint32_t local = t - vd.tile_begin;
-    const uint32_t tx = local % vd.tiles_x, ty = local / vd.tiles_x;
-    const TilePlanes tp = tile_planes_warp(f, tx * 8u, ty * 8u, lane);
-    const F3 cam = ld3(f.cam_pos), fwd = ld3(f.cam_fwd);
-    const uint32_t n_vis = min(f.chunk_count, vd.n_chunks);
-    const vm_chunk* ch = a.chunks + vd.chunk_off;
-    uint16_t* out = a.tile_list + (uint64_t)t * a.list_cap;
-    uint32_t n = 0;
-    // the super-tile's survivors (ascending), or every chunk when it has no list
-    const uint32_t s = vd.super_begin + (ty >> 2) * ((vd.tiles_x + 3u) >> 2) + (tx >> 2);
-    const uint32_t ns = a.super_count[s];
-    const bool listed = ns <= a.list_cap;
-    const uint16_t* cand = a.super_list + (uint64_t)s * a.list_cap;
-    const uint32_t n_test = listed ? ns : n_vis;
-    for (uint32_t base = 0; base < n_test; base += 32u) {
+__global__ void __launch_bounds__(CULL_THREADS) k_cull(const __grid_constant__ PipeArgs a) {
+  __shared__ float s_box[6][CULL_BATCH];
+  __shared__ uint16_t s_ci[CULL_BATCH];
+  __shared__ uint32_t s_hist[N_COST_BUCKETS];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t s = blockIdx.x;
+  if (threadIdx.x < N_COST_BUCKETS) s_hist[threadIdx.x] = 0u;
+  const uint32_t v = SINGLE ? 0u : find_view_super(a, s);
+  const vm_frame& f = frame_t<SINGLE>(a, v);
+  const ViewDesc vd = view_t<SINGLE>(a, v);
+  const uint32_t local_s = s - vd.super_begin, sxv = (vd.tiles_x + 3u) >> 2;
+  const uint32_t tx = (local_s % sxv) * 4u + (warp & 3u), ty = (local_s / sxv) * 4u + (warp >> 2);
+  const bool has_tile = tx < vd.tiles_x && ty < vd.tiles_y;
+  const uint32_t t = vd.tile_begin + ty * vd.tiles_x + tx;
+  TilePlanes tp;
+  if (has_tile) tp = tile_planes_warp(f, tx * 8u, ty * 8u, lane);
+  const F3 cam = ld3(f.cam_pos), fwd = ld3(f.cam_fwd);
+  const uint32_t n_vis = min(f.chunk_count, vd.n_chunks);
+  const vm_chunk* ch = a.chunks + vd.chunk_off;
+  const uint32_t ns = a.super_count[s];
+  const bool listed = ns <= a.list_cap;
+  const uint16_t* cand = a.super_list + (uint64_t)s * a.list_cap;
+  const uint32_t n_test = listed ? ns : n_vis;
+  uint16_t* out = a.tile_list + (uint64_t)(has_tile ? t : 0u) * a.list_cap;
+  const bool far_reach = has_tile && tp.reach == f.far_;
+  uint32_t n = 0;
+  for (uint32_t b0 = 0; b0 < n_test; b0 += CULL_BATCH) {
+    const uint32_t nb = min(CULL_BATCH, n_test - b0);
+    __syncthreads();   // the previous batch is consumed
+    for (uint32_t j = threadIdx.x; j < nb; j += CULL_THREADS) {
+      const uint32_t ci = listed ? (uint32_t)cand[b0 + j] : b0 + j;
+      const float* cp = reinterpret_cast<const float*>(ch + ci);
+      s_box[0][j] = __ldg(cp + 0); s_box[1][j] = __ldg(cp + 1); s_box[2][j] = __ldg(cp + 2);
+      s_box[3][j] = __ldg(cp + 4); s_box[4][j] = __ldg(cp + 5); s_box[5][j] = __ldg(cp + 6);
+      s_ci[j] = (uint16_t)ci;
+    }
+    __syncthreads();
+    if (!has_tile) continue;
+    for (uint32_t base = 0; base < nb; base += 32u) {
       const uint32_t j = base + lane;
-      const uint32_t ci = j < n_test ? (listed ? (uint32_t)cand[j] : j) : 0u;
-      const bool keep = j < n_test && cull_keep(f, tp, cam, fwd, ch, ci);
+      uint32_t ci = 0u;
+      bool keep = false;
+      if (j < nb) {
+        ci = s_ci[j];
+        const F3 bmin = f3(s_box[0][j], s_box[1][j], s_box[2][j]), bmax = f3(s_box[3][j], s_box[4][j], s_box[5][j]);
+        keep = listed ? cull_keep_survivor(f, tp, cam, bmin, bmax, ci, far_reach)
+                      : cull_keep_box(f, tp, cam, fwd, bmin, bmax, ci);
+      }
       const uint32_t bal = __ballot_sync(FULLMASK, keep);
       if (keep) {
         const uint32_t pos = n + __popc(bal & lanemask_lt());
@@ -218,13 +272,18 @@ __global__ void __launch_bounds__(256) k_cull(const __grid_constant__ PipeArgs a
       }
       n += __popc(bal);
     }
-    if (lane == 0) {
-      a.tile_count[t] = n;
-      a.hiz[t] = 0xFFFFFFFFu;   // the primary kernel folds its pixels' minimum in
-      const uint32_t c = max(a.item_cost[2u * t], a.item_cost[2u * t + 1u]);
-      atomicAdd(&a.work[W_HIST + cost_bucket(c)], 1u);
-    }
   }
+  __syncthreads();
+  if (has_tile && lane == 0) {
+    a.tile_count[t] = n;
+    a.hiz[t] = 0xFFFFFFFFu;   // the primary kernel folds its pixels' minimum in
+    const uint32_t c = max(a.item_cost[2u * t], a.item_cost[2u * t + 1u]);
+    atomicAdd(&s_hist[cost_bucket(c)], 1u);
+  }
+  __syncthreads();
+  // the block's tiles in the cost histogram: one global atomic per bucket used
+  if (threadIdx.x < N_COST_BUCKETS && s_hist[threadIdx.x])
+    atomicAdd(&a.work[W_HIST + threadIdx.x], s_hist[threadIdx.x]);
 }
 
 // The tiles in decreasing order of the last launch's cost (a counting sort
@@ -707,14 +766,13 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
     return cudaSuccess;
   }
   k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
-  const uint32_t cull_blocks = std::min<uint32_t>((a.total_tiles + 7) / 8, (uint32_t)sms * 16u);
   const uint32_t super_blocks = std::min<uint32_t>((a.total_supers + 7) / 8, (uint32_t)sms * 16u);
   if (a.frames == nullptr) {
     k_cull_super<true><<<super_blocks, 256, 0, s>>>(a);
-    k_cull<true><<<cull_blocks, 256, 0, s>>>(a);
+    k_cull<true><<<a.total_supers, CULL_THREADS, 0, s>>>(a);
   } else {
     k_cull_super<false><<<super_blocks, 256, 0, s>>>(a);
-    k_cull<false><<<cull_blocks, 256, 0, s>>>(a);
+    k_cull<false><<<a.total_supers, CULL_THREADS, 0, s>>>(a);
   }
   k_order<<<(a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256, 0, s>>>(a);
   if ((e = mark(1)) != cudaSuccess) return e;
