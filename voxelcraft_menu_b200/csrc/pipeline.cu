@@ -66,10 +66,9 @@ struct MaxOp {
 // and the march's slab / DDA arithmetic differ by float rounding only, far
 // below that slack.  dkmax = depth_key of that bound (depth keys fall with t).
 constexpr int BOUNDS_THREADS = 256;
-__global__ void __launch_bounds__(BOUNDS_THREADS) k_bounds(const __grid_constant__ PipeArgs a) {
+__device__ __forceinline__ void bounds_block(const PipeArgs& a, uint32_t v) {
   typedef cub::BlockScan<uint32_t, BOUNDS_THREADS> Scan;
   __shared__ typename Scan::TempStorage tmp;
-  const uint32_t v = blockIdx.x;
   // the launch's counters start at zero (k_bounds is its first kernel)
   if (v == 0 && threadIdx.x < (uint32_t)W_WORDS) a.work[threadIdx.x] = 0u;
   const vm_frame& f = frame_of(a, v);
@@ -155,10 +154,10 @@ __device__ __forceinline__ bool super_keep(const vm_frame& f, const F3* n, F3 ca
 }
 
 template <bool SINGLE>
-__global__ void __launch_bounds__(256) k_cull_super(const __grid_constant__ PipeArgs a) {
+__device__ __forceinline__ void cull_super_blocks(const PipeArgs& a, uint32_t block, uint32_t n_blocks) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t n_warps = gridDim.x * 8u;
-  for (uint32_t s = blockIdx.x * 8u + (threadIdx.x >> 5); s < a.total_supers; s += n_warps) {
+  const uint32_t n_warps = n_blocks * 8u;
+  for (uint32_t s = block * 8u + (threadIdx.x >> 5); s < a.total_supers; s += n_warps) {
     const uint32_t v = SINGLE ? 0u : find_view_super(a, s);
     const vm_frame& f = frame_t<SINGLE>(a, v);
     const ViewDesc vd = view_t<SINGLE>(a, v);
@@ -183,6 +182,15 @@ __global__ void __launch_bounds__(256) k_cull_super(const __grid_constant__ Pipe
     }
     if (lane == 0) a.super_count[s] = cnt;
   }
+}
+
+// The launch's first kernel: blocks [0, n_views) compute their view's chunk
+// depth bounds (and block 0 zeroes the counters), the others run the
+// super-tile cull; the two are independent, one launch serves both.
+template <bool SINGLE>
+__global__ void __launch_bounds__(BOUNDS_THREADS) k_prepass(const __grid_constant__ PipeArgs a) {
+  if (blockIdx.x < a.n_views) bounds_block(a, blockIdx.x);
+  else cull_super_blocks<SINGLE>(a, blockIdx.x - a.n_views, gridDim.x - a.n_views);
 }
 
 // tile_select's per-chunk test (cull_keep) on a box staged in shared memory
@@ -765,13 +773,13 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
       if ((e = mark(i)) != cudaSuccess) return e;
     return cudaSuccess;
   }
-  k_bounds<<<a.n_views, BOUNDS_THREADS, 0, s>>>(a);
+
   const uint32_t super_blocks = std::min<uint32_t>((a.total_supers + 7) / 8, (uint32_t)sms * 16u);
   if (a.frames == nullptr) {
-    k_cull_super<true><<<super_blocks, 256, 0, s>>>(a);
+    k_prepass<true><<<a.n_views + super_blocks, BOUNDS_THREADS, 0, s>>>(a);
     k_cull<true><<<a.total_supers, CULL_THREADS, 0, s>>>(a);
   } else {
-    k_cull_super<false><<<super_blocks, 256, 0, s>>>(a);
+    k_prepass<false><<<a.n_views + super_blocks, BOUNDS_THREADS, 0, s>>>(a);
     k_cull<false><<<a.total_supers, CULL_THREADS, 0, s>>>(a);
   }
   k_order<<<(a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256, 0, s>>>(a);
