@@ -149,9 +149,18 @@ def cpu_sample(view, pools, budget_s=12.0):
         px += p
         row0 += rows
         rows = min(rows * 2, 32)
+    # footnote baseline: the engine's own CPU ray walk (Player::pick, a
+    # unit-voxel DDA over block lookups) per pixel of a few pixel rows
+    height = int(view.frame.res[1])
+    t0 = time.perf_counter()
+    n_pick, hits = o.pick_rows(height // 2 - 8, 16)
+    t_pick = time.perf_counter() - t0
     return {"value": rays / t_total / 1e9, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
             "sample": f"oracle (engine pass sequence restated in C++, OpenMP) over the middle tile rows of the "
-                      f"same frame: {px} pixels, {rays} primary+shadow rays in {t_total:.1f}s"}
+                      f"same frame: {px} pixels, {rays} primary+shadow rays in {t_total:.1f}s",
+            "unit_voxel_walk": {"value": n_pick / t_pick / 1e9, "unit": "Grays/s (primary rays only)",
+                                "sample": f"Player::pick (src/player.rs:334-393) restated, per pixel of 16 pixel rows "
+                                          f"({n_pick} rays, {hits} hits) in {t_pick:.1f}s on every host core"}}
 
 
 def reference_arm(args):
@@ -504,6 +513,18 @@ def bench_encoder(local, steps, warmup, cpu=True):
     return rec
 
 
+def profile_row(kernel, row, workload="1080p"):
+    """A value of the committed ncu summary's table (e.g. "issue active"), if any."""
+    f = ROOT / "profiles" / f"k_{kernel}_{workload}.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) == 2 and cells[0] == row:
+            return cells[1]
+    return None
+
+
 def profile_traffic(kernel, workload="1080p"):
     """dram bytes per launch of kernel from the committed ncu summary, if any."""
     f = ROOT / "profiles" / f"k_{kernel}_{workload}.md"
@@ -717,6 +738,10 @@ def main():
             "roofline": {"bound": "hbm", "kernel": f"k_{top}" if top != "primary" else "k_primary",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profile_traffic(top), "peak_kind": peak_kind,
+                         "note": "the tree pools are L2-resident: the kernel is bound by instruction issue, "
+                                 "not HBM (ncu issue active and threads per instruction below)",
+                         "issue_active_ncu": profile_row(top, "issue active"),
+                         "threads_per_instruction_ncu": profile_row(top, "threads per executed instruction (of 32)"),
                          "algorithmic_bytes_per_launch": sbytes[top], "launch_ms": stage_ms[top],
                          "dda_steps_per_launch": traffic["stage_iters"][STAGES.index(top) - 1],
                          "bytes_per_dda_step": sbytes[top] / max(traffic["stage_iters"][STAGES.index(top) - 1], 1)},

@@ -67,6 +67,7 @@ def lib():
             "or_pick": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, vp]),
             "or_soften_shadows": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, C.c_int]),
             "or_reflect": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
+            "or_pick_rows": (C.c_uint64, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp]),
             "or_f16_round": (None, [vp, vp, C.c_uint64]),
         }
         for n, (r, a) in sig.items():
@@ -242,6 +243,12 @@ class Oracle:
 
     def grid_block(self, x, y, z):
         return int(self.L.or_grid_block(C.byref(self.w), x, y, z))
+
+    def pick_rows(self, row0, rows, max_steps=4096):
+        """Player::pick per pixel of pixel rows [row0, row0 + rows): (pixels, hits)."""
+        hits = C.c_uint64()
+        n = self.L.or_pick_rows(C.byref(self.w), row0, rows, max_steps, self.threads, C.byref(hits))
+        return int(n), int(hits.value)
 
     def pick(self, origin, direction, max_steps=64, reach=1e9):
         o = np.asarray(origin, np.float32)

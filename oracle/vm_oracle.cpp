@@ -1379,6 +1379,32 @@ int or_pick(const or_world* o, const float* orig, const float* dir, uint32_t max
   return 0;
 }
 
+// The engine's own CPU ray walk, Player::pick, as a frame tracer: one
+// unit-voxel walk per pixel of rows [row0, row0 + rows) from the camera
+// along ray_dir, up to max_steps voxels or the frame's far distance.
+// Returns the pixels traced; *hits receives how many hit a block.
+uint64_t or_pick_rows(const or_world* o, uint32_t row0, uint32_t rows, uint32_t max_steps, int threads,
+                      uint64_t* hits) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  const uint32_t W = f.res[0], H = f.res[1];
+  const uint32_t y1 = std::min(H, row0 + rows);
+  if (row0 >= y1) { *hits = 0; return 0; }
+  uint64_t h = 0;
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : h)
+  for (int64_t i = 0; i < (int64_t)(y1 - row0) * W; ++i) {
+    const uint32_t px = (uint32_t)(i % W), py = row0 + (uint32_t)(i / W);
+    const V3 d = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+    const float dd[3] = {d.x, d.y, d.z};
+    int32_t blk[3], nrm[3];
+    float dist;
+    h += (uint64_t)or_pick(o, f.cam_pos, dd, max_steps, f.far_, blk, nrm, &dist);
+  }
+  *hits = h;
+  return (uint64_t)(y1 - row0) * W;
+}
+
 // shadow_horizontal + shadow_vertical (shadow.wgsl:62-116) with
 // SPEC_SOFT_SHADOWS on: dist is primary_shadow's blocker distance per pixel
 // (stored as r16float), h receives the horizontal pass (occlusion, support),
