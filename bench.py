@@ -153,14 +153,14 @@ def cpu_sample(view, pools, budget_s=12.0):
     # unit-voxel DDA over block lookups) per pixel of a few pixel rows
     height = int(view.frame.res[1])
     t0 = time.perf_counter()
-    n_pick, hits = o.pick_rows(height // 2 - 8, 16)
+    n_pick, hits = o.pick_rows(height // 2 - 64, 128)
     t_pick = time.perf_counter() - t0
     return {"value": rays / t_total / 1e9, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
             "sample": f"oracle (engine pass sequence restated in C++, OpenMP) over the middle tile rows of the "
                       f"same frame: {px} pixels, {rays} primary+shadow rays in {t_total:.1f}s",
             "unit_voxel_walk": {"value": n_pick / t_pick / 1e9, "unit": "Grays/s (primary rays only)",
-                                "sample": f"Player::pick (src/player.rs:334-393) restated, per pixel of 16 pixel rows "
-                                          f"({n_pick} rays, {hits} hits) in {t_pick:.1f}s on every host core"}}
+                                "sample": f"Player::pick (src/player.rs:334-393) restated, per pixel of 128 pixel rows "
+                                          f"({n_pick} rays, {hits} hits) in {t_pick:.2f}s on every host core"}}
 
 
 def reference_arm(args):
