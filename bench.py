@@ -752,8 +752,8 @@ def main():
             "e2e_serial": {"value": world * rays / (e2e_serial_ms * 1e-3) / 1e9, "unit": UNIT,
                            "ms_per_step": e2e_serial_ms,
                            "method": "one context, synchronous read-back, L2 flushed before each step"},
-            # per frame: k_bounds, k_cull_super, k_cull, k_order, k_primary, k_shadow, k_secondary_q
-            "gpu_launches": 7 * args.steps,
+            # per frame: k_prepass, k_cull, k_order, k_primary, k_shadow, k_secondary_q
+            "gpu_launches": 6 * args.steps,
             "clocks": clocks,
             "device_error": int(stats.device_error),
         }

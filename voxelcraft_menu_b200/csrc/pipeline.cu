@@ -1,14 +1,14 @@
 // The frame as a wavefront pipeline of warp-independent kernels, sm_100a.
 //
-//   k_bounds   per view: for every visible chunk, the largest depth key a hit
-//              in it can have (from a lower bound on its distance) and the
-//              suffix maximum of that bound along the view's front-to-back
-//              chunk list;
-//   k_cull_super one warp per 32x32 super-tile: the chunks its frustum
-//              cannot rule out;
-//   k_cull     one warp per 8x8 tile: tile_select's exact test
-//              (tile_select.wgsl:11-92) over its super-tile's survivors,
-//              written as the tile's ascending chunk list;
+//   k_prepass  blocks [0, views): for every visible chunk, the largest depth
+//              key a hit in it can have (from a lower bound on its distance)
+//              and the suffix maximum of that bound along the view's
+//              front-to-back chunk list; the other blocks: one warp per
+//              32x32 super-tile, the chunks its frustum cannot rule out;
+//   k_cull     one block per super-tile, one warp per 8x8 tile:
+//              tile_select's exact test (tile_select.wgsl:11-92) over the
+//              super-tile's survivors, written as the tile's ascending chunk
+//              list;
 //   k_order    the tiles in decreasing order of the last launch's item cost;
 //   k_primary  persistent warps steal 8x4-pixel items in that order; each
 //              lane marches its pixel through the tile's list front to back
@@ -17,12 +17,13 @@
 //              distance past which it cannot), so the key equals the engine's
 //              atomicMax over all of the tile's pairs; the lane then queues
 //              its shadow ray and its water / glass ray, one atomic per warp;
-//   k_shadow   persistent lanes step their queued sun ray one chunk-grid cell
-//              at a time and take the next ray as soon as theirs ends;
+//   k_shadow   persistent lanes step their queued sun ray one chunk march at
+//              a time and take the next ray as soon as theirs ends;
 //   k_secondary_q the same for the queued water / glass rays (trace_world).
 //
-// Only k_bounds (a block scan) and k_order (a block's ranking) synchronise a
-// block; everywhere else warps never wait on other warps.
+// Only the prepass's depth bounds (a block scan), k_cull (its staged boxes)
+// and k_order (a block's ranking) synchronise a block; everywhere else warps
+// never wait on other warps.
 #include "kernels.cuh"
 #include "ray_stages.cuh"
 #include <cub/block/block_scan.cuh>
@@ -69,7 +70,7 @@ constexpr int BOUNDS_THREADS = 256;
 __device__ __forceinline__ void bounds_block(const PipeArgs& a, uint32_t v) {
   typedef cub::BlockScan<uint32_t, BOUNDS_THREADS> Scan;
   __shared__ typename Scan::TempStorage tmp;
-  // the launch's counters start at zero (k_bounds is its first kernel)
+  // the launch's counters start at zero (the prepass is its first kernel)
   if (v == 0 && threadIdx.x < (uint32_t)W_WORDS) a.work[threadIdx.x] = 0u;
   const vm_frame& f = frame_of(a, v);
   const ViewDesc vd = view_of(a, v);
