@@ -642,6 +642,12 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
     }
   }
   flush_traffic<COUNT>(a, 1, tr, 0, ns, 0);
+  // When launched behind k_secondary_q with programmatic serialization, the
+  // kernel ends only once that grid has completed and its writes are
+  // visible, so whatever follows in the stream sees both kernels' outputs.
+  // That grid waits on nothing and all its blocks were running before this
+  // kernel could start; in an ordinary launch this returns at once.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 // The water / glass rays (trace_world, common.wgsl:1205-1253) of the queue —
@@ -650,6 +656,10 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
 // taken as soon as a lane's ray ends.
 template <bool COUNT, bool SINGLE>
 __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ PipeArgs a) {
+  // a shadow kernel launched after this one with programmatic serialization
+  // may take the SMs this kernel's blocks leave (it reads nothing this kernel
+  // writes); without one this has no effect
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const uint32_t n = a.work[W_SEC_N];
   const uint32_t lane = threadIdx.x & 31u;
   Traffic tr = {};
@@ -798,6 +808,28 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   if ((e = cudaLaunchKernel(fn, dim3(grid), dim3(nw * 32), args, 0, s)) != cudaSuccess) return e;
   if ((e = mark(2)) != cudaSuccess) return e;
   const uint32_t q_blocks = (uint32_t)sms * 8u;
+  if (!count && single && a.do_shadow && a.do_secondary) {
+    // The water / glass rays first, on exactly the blocks that fit at once
+    // (4 per SM), then the shadow rays with programmatic stream serialization:
+    // the shadow kernel needs only the primary kernel's queue, complete
+    // before either starts, so its blocks take the SMs the few long water /
+    // glass walks leave instead of waiting for the last of them.  Events 3
+    // and 4 both follow the two kernels.
+    k_secondary_q<false, true><<<(uint32_t)sms * 4u, 256, 0, s>>>(a);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(q_blocks);
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if ((e = cudaLaunchKernelEx(&cfg, k_shadow<false, true>, a)) != cudaSuccess) return e;
+    if ((e = mark(3)) != cudaSuccess) return e;
+    if ((e = mark(4)) != cudaSuccess) return e;
+    return cudaGetLastError();
+  }
   if (a.do_shadow) {
     if (count && single) k_shadow<true, true><<<q_blocks, 256, 0, s>>>(a);
     else if (count) k_shadow<true, false><<<q_blocks, 256, 0, s>>>(a);
