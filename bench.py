@@ -192,7 +192,14 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
-STAGES = ("cull", "primary", "shadow", "secondary")
+# The library records five events per frame: before the prepass, after
+# k_order, after k_primary, and two after the ray kernels.  The water / glass
+# kernel and the shadow kernel run concurrently (the shadow kernel is a
+# programmatic dependent launch behind it), so they form one timed stage,
+# events 2 -> 4.
+STAGES = {"cull": (0, 1), "primary": (1, 2), "shadow+secondary": (2, 4)}
+STAGE_KERNELS = {"cull": "k_prepass + k_cull + k_order", "primary": "k_primary",
+                 "shadow+secondary": "k_secondary_q + k_shadow (concurrent)"}
 
 
 def stage_bytes(traffic, npix):
@@ -200,14 +207,20 @@ def stage_bytes(traffic, npix):
     fetches (the layout's element sizes), plus what the stage reads and
     writes per ray: tile-list entries (2 B) and the visibility key (8 B) and
     queue items (24 B shadow, 40 B secondary) for the primary kernel; the
-    queue item read and the 4 B result for the shadow and secondary kernels."""
+    queue item read and the 4 B result (12 B for a water / glass ray) for the
+    two ray kernels."""
     sb = traffic["stage_bytes"]
     rs, rsec = traffic["rays_shadow"], traffic["rays_secondary"]
     return {
         "primary": sb[0] + 2 * traffic["list_entries"] + 8 * npix + 24 * rs + 40 * rsec,
-        "shadow": sb[1] + (24 + 4) * rs,
-        "secondary": sb[2] + (40 + 12) * rsec,
+        "shadow+secondary": sb[1] + (24 + 4) * rs + sb[2] + (40 + 12) * rsec,
     }
+
+
+def stage_iters(traffic, stage):
+    """DDA steps of a timed stage (the primary kernel, or both ray kernels)."""
+    it = traffic["stage_iters"]
+    return it[0] if stage == "primary" else it[1] + it[2]
 
 
 def bench_batched(local, steps, warmup):
@@ -592,7 +605,7 @@ def main():
     for _ in range(args.warmup):
         m.render()
     torch.cuda.synchronize(dev)
-    # five events per step, recorded by the library between its stages
+    # five events per step, recorded by the library between its stages (STAGES)
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
     for row in evs:
         for e in row:
@@ -609,8 +622,8 @@ def main():
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
     ms = [row[0].elapsed_time(row[4]) for row in evs]
-    stage_ms = {name: float(np.mean([row[j].elapsed_time(row[j + 1]) for row in evs]))
-                for j, name in enumerate(STAGES)}
+    stage_ms = {name: float(np.mean([row[i].elapsed_time(row[j]) for row in evs]))
+                for name, (i, j) in STAGES.items()}
     ms_step = float(np.mean(ms))
     if world > 1:
         t = torch.tensor([ms_step], device=dev)
@@ -735,7 +748,7 @@ def main():
             "work_per_step": traffic,
             "rays_per_step": {"primary": traffic["rays_primary"], "shadow": traffic["rays_shadow"],
                               "secondary_uncounted": traffic["rays_secondary"]},
-            "roofline": {"bound": "hbm", "kernel": f"k_{top}" if top != "primary" else "k_primary",
+            "roofline": {"bound": "hbm", "kernel": STAGE_KERNELS[top],
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profile_traffic(top), "peak_kind": peak_kind,
                          "note": "the tree pools are L2-resident: the kernel is bound by instruction issue, "
@@ -743,8 +756,8 @@ def main():
                          "issue_active_ncu": profile_row(top, "issue active"),
                          "threads_per_instruction_ncu": profile_row(top, "threads per executed instruction (of 32)"),
                          "algorithmic_bytes_per_launch": sbytes[top], "launch_ms": stage_ms[top],
-                         "dda_steps_per_launch": traffic["stage_iters"][STAGES.index(top) - 1],
-                         "bytes_per_dda_step": sbytes[top] / max(traffic["stage_iters"][STAGES.index(top) - 1], 1)},
+                         "dda_steps_per_launch": stage_iters(traffic, top),
+                         "bytes_per_dda_step": sbytes[top] / max(stage_iters(traffic, top), 1)},
             "e2e": {"value": world * rays / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                     "method": "two contexts alternate; every step uploads its inputs from pinned host memory and "
