@@ -190,6 +190,9 @@ __device__ __forceinline__ void cull_super_blocks(const PipeArgs& a, uint32_t bl
 // super-tile cull; the two are independent, one launch serves both.
 template <bool SINGLE>
 __global__ void __launch_bounds__(BOUNDS_THREADS) k_prepass(const __grid_constant__ PipeArgs a) {
+  // k_cull, launched behind this kernel with programmatic serialization,
+  // traces its tile rays while this kernel runs
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (blockIdx.x < a.n_views) bounds_block(a, blockIdx.x);
   else cull_super_blocks<SINGLE>(a, blockIdx.x - a.n_views, gridDim.x - a.n_views);
 }
@@ -223,10 +226,12 @@ __device__ __forceinline__ bool cull_keep_survivor(const vm_frame& f, const Tile
 // when it has no list) in shared memory, CULL_BATCH at a time with coalesced
 // loads, and each warp runs tile_select's exact test on them in ascending
 // chunk order, so every tile gets the same list as from a warp that read
-// the boxes from global memory itself.
+// the boxes from global memory itself.  Three blocks per SM (40 registers).
+// Launched behind k_prepass with programmatic serialization: a block traces
+// its tiles' rays (frame parameters only) before it waits for the prepass.
 constexpr uint32_t CULL_THREADS = 512, CULL_BATCH = 256;
 template <bool SINGLE>
-__global__ void __launch_bounds__(CULL_THREADS) k_cull(const __grid_constant__ PipeArgs a) {
+__global__ void __launch_bounds__(CULL_THREADS, 3) k_cull(const __grid_constant__ PipeArgs a) {
   __shared__ float s_box[6][CULL_BATCH];
   __shared__ uint16_t s_ci[CULL_BATCH];
   __shared__ uint32_t s_hist[N_COST_BUCKETS];
@@ -242,6 +247,8 @@ __global__ void __launch_bounds__(CULL_THREADS) k_cull(const __grid_constant__ P
   const uint32_t t = vd.tile_begin + ty * vd.tiles_x + tx;
   TilePlanes tp;
   if (has_tile) tp = tile_planes_warp(f, tx * 8u, ty * 8u, lane);
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");   // the prepass's lists, bounds and zeroed counters
   const F3 cam = ld3(f.cam_pos), fwd = ld3(f.cam_fwd);
   const uint32_t n_vis = min(f.chunk_count, vd.n_chunks);
   const vm_chunk* ch = a.chunks + vd.chunk_off;
@@ -304,6 +311,7 @@ __global__ void __launch_bounds__(256) k_order(const __grid_constant__ PipeArgs 
   __shared__ uint32_t start[N_COST_BUCKETS], count[N_COST_BUCKETS], base[N_COST_BUCKETS];
   const uint32_t t0 = blockIdx.x * ORDER_TILES, t1 = min(t0 + ORDER_TILES, a.total_tiles);
   if (threadIdx.x < N_COST_BUCKETS) count[threadIdx.x] = 0u;
+  asm volatile("griddepcontrol.wait;" ::: "memory");   // k_cull's histogram
   if (threadIdx.x == 0) {
     uint32_t s = 0;
     for (uint32_t b = 0; b < N_COST_BUCKETS; ++b) { start[b] = s; s += a.work[W_HIST + b]; }
@@ -773,6 +781,28 @@ int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bo
   return n;
 }
 
+namespace {
+
+// A launch with programmatic stream serialization: the kernel may start once
+// every block of the kernel before it in the stream has started (or run
+// griddepcontrol.launch_dependents); it waits for that kernel's results with
+// griddepcontrol.wait.
+template <typename K>
+cudaError_t launch_after(K kernel, uint32_t blocks, uint32_t threads, cudaStream_t s, const PipeArgs& a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(threads);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
+}  // namespace
+
 cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwater, bool count, int sms,
                             cudaStream_t s, const cudaEvent_t* ev) {
   cudaError_t e;
@@ -786,14 +816,20 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   }
 
   const uint32_t super_blocks = std::min<uint32_t>((a.total_supers + 7) / 8, (uint32_t)sms * 16u);
+  // k_cull and k_order with programmatic serialization: each starts once the
+  // kernel before it has started all its blocks and waits for its results
+  // (griddepcontrol.wait), so the launches' latency and k_cull's ray setup
+  // overlap the kernel before
   if (a.frames == nullptr) {
     k_prepass<true><<<a.n_views + super_blocks, BOUNDS_THREADS, 0, s>>>(a);
-    k_cull<true><<<a.total_supers, CULL_THREADS, 0, s>>>(a);
+    e = launch_after(k_cull<true>, a.total_supers, CULL_THREADS, s, a);
   } else {
     k_prepass<false><<<a.n_views + super_blocks, BOUNDS_THREADS, 0, s>>>(a);
-    k_cull<false><<<a.total_supers, CULL_THREADS, 0, s>>>(a);
+    e = launch_after(k_cull<false>, a.total_supers, CULL_THREADS, s, a);
   }
-  k_order<<<(a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256, 0, s>>>(a);
+  if (e != cudaSuccess) return e;
+  if ((e = launch_after(k_order, (a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256u, s, a)) != cudaSuccess)
+    return e;
   if ((e = mark(1)) != cudaSuccess) return e;
   const bool refl = a.do_reflect != 0u, single = a.frames == nullptr;
   void* fn = primary_kernel(t, underwater, count, refl, single);
@@ -816,16 +852,7 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
     // glass walks leave instead of waiting for the last of them.  Events 3
     // and 4 both follow the two kernels.
     k_secondary_q<false, true><<<(uint32_t)sms * 4u, 256, 0, s>>>(a);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(q_blocks);
-    cfg.blockDim = dim3(256);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if ((e = cudaLaunchKernelEx(&cfg, k_shadow<false, true>, a)) != cudaSuccess) return e;
+    if ((e = launch_after(k_shadow<false, true>, q_blocks, 256u, s, a)) != cudaSuccess) return e;
     if ((e = mark(3)) != cudaSuccess) return e;
     if ((e = mark(4)) != cudaSuccess) return e;
     return cudaGetLastError();
