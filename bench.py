@@ -11,7 +11,8 @@ and one water-refraction / glass-transmission ray per water / glass hit.
 Metric: Grays/s of primary + shadow rays (secondary rays are traced but not
 counted).  `value` is measured on device-resident inputs; `e2e` goes through
 the C ABI with host buffers (frame + chunk list + grid uploaded, visibility
-and shadow buffers read back every step).  The library records CUDA events
+keys and the shadow buffer in the engine's r16float target format read back
+every step; `e2e_f32` reads the shadow back as float).  The library records CUDA events
 between its stages during the timed steps (`stage_ms`); `roofline` is the
 dominant kernel's algorithmic bytes per launch over its own event time.
 
@@ -671,53 +672,81 @@ def main():
         e_ms.append(ev0.elapsed_time(ev1))
     e2e_serial_ms = float(np.mean(e_ms))
 
-    # e2e as a renderer runs consecutive frames: two contexts alternate, each
-    # step uploads its frame's chunk list, grid and frame, renders, and
-    # enqueues its visibility + shadow read-back into page-locked host memory
-    # (vm_read_async); a step's read-back overlaps the next step's kernels.
-    # Device time from an event before the first step to the later of the
-    # two streams' ends, over the steps.
+    # e2e as a renderer runs consecutive frames: two contexts alternate; each
+    # step renders its frame after the other context's last render
+    # (vm_wait_render), uploads the next frame's chunk list, grid and frame
+    # from page-locked host memory to the other context, and enqueues its own
+    # visibility + shadow read-back into page-locked host memory
+    # (vm_read_async_r16f: the shadow in the engine's R16F target format; and
+    # vm_read_async: as float); a step's read-back overlaps the next step's
+    # kernels.  Device time from an event before the first step to the later
+    # of the two streams' ends, over the steps.
     m2 = Marcher(1920, 1080, device=local)
     m2.upload_world(*pools)
     m2.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"])
     m2.upload_view(va)
     m2.render()
     ctxs = (m, m2)
-    host = [(torch.empty(npix, dtype=torch.int64).pin_memory(), torch.empty(npix, dtype=torch.float32).pin_memory())
-            for _ in ctxs]
     m._ck(L.vm_set_stream(m._h, None))   # both contexts on their own streams
     streams = [torch.cuda.ExternalStream(c.device_buffers().stream, device=dev) for c in ctxs]
 
-    def e2e_async(i):
-        c = ctxs[i % 2]
-        vh, shh = host[i % 2]
-        c._ck(L.vm_upload_chunks(c._h, C.c_void_p(ch_h.data_ptr()), len(vb.chunks), C.c_void_p(gr_h.data_ptr()),
-                                 vb.grid.size))
-        c._ck(L.vm_set_frame(c._h, C.byref(vb.frame)))
-        c._ck(L.vm_render(c._h))
-        c._ck(L.vm_read_async(c._h, C.c_void_p(vh.data_ptr()), C.c_void_p(shh.data_ptr())))
+    def e2e_two_contexts(r16f):
+        """ms per step; r16f: the shadow read back in the engine's R16F
+        target format (vm_read_async_r16f), else as float (vm_read_async)."""
+        sh_dtype = torch.int16 if r16f else torch.float32
+        host = [(torch.empty(npix, dtype=torch.int64).pin_memory(), torch.empty(npix, dtype=sh_dtype).pin_memory())
+                for _ in ctxs]
+        read = L.vm_read_async_r16f if r16f else L.vm_read_async
 
-    for i in range(4):
-        e2e_async(i)
-    torch.cuda.synchronize(dev)
-    start = torch.cuda.Event(enable_timing=True)
-    start.record(streams[0])
-    streams[1].wait_event(start)
-    for i in range(args.steps):
-        e2e_async(i)
-    ends = [torch.cuda.Event(enable_timing=True) for _ in ctxs]
-    for e, st in zip(ends, streams):
-        e.record(st)
-    torch.cuda.synchronize(dev)
-    e2e_ms = max(start.elapsed_time(e) for e in ends) / args.steps
-    assert np.array_equal(host[0][0].numpy().view(np.uint64), host[1][0].numpy().view(np.uint64))
+        def upload(c):
+            c._ck(L.vm_upload_chunks(c._h, C.c_void_p(ch_h.data_ptr()), len(vb.chunks), C.c_void_p(gr_h.data_ptr()),
+                                     vb.grid.size))
+            c._ck(L.vm_set_frame(c._h, C.byref(vb.frame)))
+
+        def step(i):
+            # frame i on context i % 2, its inputs uploaded by the step before
+            c, other = ctxs[i % 2], ctxs[(i + 1) % 2]
+            vh, shh = host[i % 2]
+            # this frame's kernels start once the previous frame's are done
+            # (not its read-back): each frame has the whole GPU while the
+            # previous one's result crosses the host link
+            c._ck(L.vm_wait_render(c._h, other._h))
+            c._ck(L.vm_render(c._h))
+            # the next frame's inputs, enqueued ahead of this frame's
+            # read-back so that the small upload does not queue behind it
+            upload(other)
+            c._ck(read(c._h, C.c_void_p(vh.data_ptr()), C.c_void_p(shh.data_ptr())))
+
+        upload(ctxs[0])
+        for i in range(4):
+            step(i)
+        torch.cuda.synchronize(dev)
+        start = torch.cuda.Event(enable_timing=True)
+        start.record(streams[0])
+        streams[1].wait_event(start)
+        for i in range(4, 4 + args.steps):
+            step(i)
+        ends = [torch.cuda.Event(enable_timing=True) for _ in ctxs]
+        for e, st in zip(ends, streams):
+            e.record(st)
+        torch.cuda.synchronize(dev)
+        ms_ = max(start.elapsed_time(e) for e in ends) / args.steps
+        for vh, shh in host:
+            assert np.array_equal(vh.numpy().view(np.uint64), vis_h.numpy().view(np.uint64))
+            want = sh_h.numpy().astype(np.float16).view(np.int16) if r16f else sh_h.numpy()
+            assert np.array_equal(shh.numpy(), want)
+        if world > 1:
+            t = torch.tensor([ms_], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_ = float(t.item())
+        return ms_
+
+    e2e_ms = e2e_two_contexts(True)
+    e2e_f32_ms = e2e_two_contexts(False)
     m2.close()
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
     h2d = vb.chunks.nbytes + vb.grid.nbytes + 352
-    d2h = npix * 12
+    d2h = npix * (8 + 2)       # vis keys + binary16 blocker distances
+    d2h_f32 = npix * (8 + 4)
 
     # roofline of the dominant kernel: its algorithmic bytes per launch over
     # its own event-timed duration
@@ -760,8 +789,14 @@ def main():
                          "bytes_per_dda_step": sbytes[top] / max(stage_iters(traffic, top), 1)},
             "e2e": {"value": world * rays / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                    "method": "two contexts alternate; every step uploads its inputs from pinned host memory and "
-                              "reads vis + shadow back (vm_read_async), overlapping the next step's kernels"},
+                    "method": "two contexts alternate; every step renders once the other context's last render is "
+                              "done (vm_wait_render), uploads the next step's inputs from pinned host memory ahead "
+                              "of its own read-back, and reads vis (u64 keys) + shadow back in the engine's own "
+                              "formats (the shadow target is r16float, shadow.wgsl:1; vm_read_async_r16f), "
+                              "overlapping the next step's kernels"},
+            "e2e_f32": {"value": world * rays / (e2e_f32_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h_f32, "ms_per_step": e2e_f32_ms,
+                        "method": "as e2e, the shadow read back as float (vm_read_async)"},
             "e2e_serial": {"value": world * rays / (e2e_serial_ms * 1e-3) / 1e9, "unit": UNIT,
                            "ms_per_step": e2e_serial_ms,
                            "method": "one context, synchronous read-back, L2 flushed before each step"},

@@ -135,6 +135,20 @@ int vm_read_expanded(vm_ctx* ctx, const int32_t origin[3], const uint32_t dims[3
  * page-locked host buffers the copy overlaps other work, e.g. the next frame
  * of a second context.  Either pointer may be NULL. */
 int vm_read_async(vm_ctx* ctx, uint64_t* vis, float* shadow);
+/* vm_read_async with the blocker distances in the engine's own shadow target
+ * format: shadow_dist_tex is texture_storage_2d<r16float> (shadow.wgsl:1),
+ * so shadow receives res.x*res.y binary16 values (IEEE half, rounded to
+ * nearest even from the float blocker distances): 10 bytes per pixel cross
+ * the host link instead of 12.  Either pointer may be NULL. */
+int vm_read_async_r16f(vm_ctx* ctx, uint64_t* vis, uint16_t* shadow);
+/* Frames in flight over several contexts on one device: work enqueued on ctx
+ * after this call waits until other's last vm_render has finished its
+ * kernels, but not for other's read-back.  A caller that alternates two
+ * contexts and calls this before each vm_render runs the frames' kernels
+ * one after another, each on the whole GPU, while the previous frame's
+ * read-back crosses the host link.  No counterpart in the engine, which keeps
+ * its frames in flight inside wgpu's queue.  No-op if other has not rendered. */
+int vm_wait_render(vm_ctx* ctx, vm_ctx* other);
 /* Hi-Z input of the next FLAG_HIZ frame (the engine keeps last frame's buffer). */
 int vm_write_hiz(vm_ctx* ctx, const uint32_t* hiz);
 

@@ -364,3 +364,58 @@ def test_async_read_back_equals_the_synchronous_one(small):
     assert_same(sh_h.numpy(), m.read_shadow(), "async shadow")
     m._ck(m._L.vm_read_async(m._h, None, C.c_void_p(sh_h.data_ptr())))   # either pointer may be NULL
     m.sync()
+
+
+@pytest.mark.parametrize("res", [(333, 77), (1920, 1080)])
+def test_r16f_read_back_is_the_oracle_shadow_in_binary16(small, res):
+    """vm_read_async_r16f: the engine's R16F shadow target (shadow.wgsl:1),
+    i.e. the oracle's blocker distances rounded to binary16 (nearest even);
+    333x77 leaves a ragged tail of the 4-pixel conversion."""
+    from oracle.oracle import f16_round
+    w, pools, m = small
+    v = w.view(W.small_terrain_camera(width=res[0], height=res[1]))
+    m.upload_view(v)
+    m.render()
+    r16 = m.read_shadow_r16f()
+    _, _, _, _, sh, _, _ = oracle_all(v, pools)
+    assert_same(r16, sh.astype(np.float16).view(np.uint16), "r16f shadow vs numpy binary16 of the oracle")
+    assert_same(r16.view(np.float16).astype(np.float32), f16_round(sh), "r16f shadow vs the oracle's f16 rounding")
+    assert_same(m.read_shadow(), sh, "float shadow unchanged")
+
+
+def test_contexts_in_flight_give_each_frame_its_own_output(small):
+    """Two contexts alternating with vm_wait_render and asynchronous
+    read-backs (the bench's end-to-end loop) return every frame's own
+    visibility and R16F shadow."""
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    w, pools, m = small
+    views = [w.view(W.small_terrain_camera(width=320, height=200, yaw=math.radians(yaw)))
+             for yaw in (60.0, 90.0, 120.0, 150.0)]
+    want = []
+    for v in views:
+        m.upload_view(v)
+        m.render()
+        want.append((m.read_vis(), m.read_shadow().astype(np.float16).view(np.uint16)))
+    ctxs = [Marcher(320, 200) for _ in range(2)]
+    try:
+        n = 320 * 200
+        host = [(torch.zeros(n, dtype=torch.int64).pin_memory(), torch.zeros(n, dtype=torch.int16).pin_memory())
+                for _ in views]
+        for c in ctxs:
+            c.upload_world(*pools)
+        for i, v in enumerate(views):
+            c, prev = ctxs[i % 2], ctxs[(i + 1) % 2]
+            c.upload_view(v)
+            c.wait_render(prev)
+            c._ck(c._L.vm_render(c._h))
+            vh, sh = host[i]
+            c._ck(c._L.vm_read_async_r16f(c._h, C.c_void_p(vh.data_ptr()), C.c_void_p(sh.data_ptr())))
+        for c in ctxs:
+            c.sync()
+        for i, (vh, sh) in enumerate(host):
+            assert_same(vh.numpy().view(np.uint64), want[i][0], f"frame {i} vis")
+            assert_same(sh.numpy().view(np.uint16), want[i][1], f"frame {i} r16f shadow")
+    finally:
+        for c in ctxs:
+            c.close()

@@ -25,6 +25,8 @@ struct vm_ctx {
   int device = 0;
   int sms = 148;
   cudaStream_t own = nullptr, stream = nullptr;
+  cudaEvent_t rendered = nullptr;   // recorded after each vm_render's kernels (vm_wait_render)
+  bool have_rendered = false;
   vm_caps caps{};
   // world pools
   DevBuf inners, leaves, bricks;
@@ -40,6 +42,7 @@ struct vm_ctx {
   // per-frame outputs and scratch
   DevBuf vis, shadow, sec_key, sec_t, hiz, dbg, pairs, counters, err, work, dkmax, sufmax, traffic, expand;
   DevBuf shadow_mask;   // vm_soften_shadows output, sized on first use
+  DevBuf shadow16;      // vm_read_async_r16f staging, sized on first use
   DevBuf refl_key, refl_t;   // reflect legs of water hits, sized by the first FLAG_WATER_REFLECT frame
   bool refl_frame = false;   // the last frame traced them
   DevBuf tile_list, tile_count, shadow_q, sec_q, item_cost, tile_order, super_list, super_count;
@@ -305,8 +308,10 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->tile_count, &ctx->shadow_q, &ctx->sec_q, &ctx->b_tile_list, &ctx->b_tile_count,
                    &ctx->b_shadow_q, &ctx->b_sec_q, &ctx->item_cost, &ctx->tile_order, &ctx->b_item_cost,
                    &ctx->b_tile_order, &ctx->super_list, &ctx->super_count, &ctx->b_super_list,
-                   &ctx->b_super_count, &ctx->shadow_mask, &ctx->refl_key, &ctx->refl_t};
+                   &ctx->b_super_count, &ctx->shadow_mask, &ctx->refl_key, &ctx->refl_t,
+                   &ctx->shadow16};
   for (DevBuf* b : all) release(*b);
+  if (ctx->rendered) cudaEventDestroy(ctx->rendered);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
 }
@@ -484,7 +489,19 @@ int vm_render(vm_ctx* ctx) {
   int rc = check_ready(ctx);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
-  return enqueue_render(ctx, false);
+  if ((rc = enqueue_render(ctx, false))) return rc;
+  if (!ctx->rendered) CK(cudaEventCreateWithFlags(&ctx->rendered, cudaEventDisableTiming));
+  CK(cudaEventRecord(ctx->rendered, ctx->stream));
+  ctx->have_rendered = true;
+  return VM_OK;
+}
+
+int vm_wait_render(vm_ctx* ctx, vm_ctx* other) {
+  if (!ctx || !other) return VM_E_INVALID;
+  if (!other->have_rendered) return VM_OK;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamWaitEvent(ctx->stream, other->rendered, 0));
+  return VM_OK;
 }
 
 static int read_traffic(vm_ctx* ctx, vm_traffic* out);
@@ -544,6 +561,20 @@ int vm_read_async(vm_ctx* ctx, uint64_t* vis, float* shadow) {
   const size_t npix = (size_t)ctx->frame.res[0] * ctx->frame.res[1];
   if (vis) CK(cudaMemcpyAsync(vis, ctx->vis.p, npix * 8, cudaMemcpyDeviceToHost, ctx->stream));
   if (shadow) CK(cudaMemcpyAsync(shadow, ctx->shadow.p, npix * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  return VM_OK;
+}
+
+int vm_read_async_r16f(vm_ctx* ctx, uint64_t* vis, uint16_t* shadow) {
+  if (!ctx || !ctx->have_frame) return VM_E_NOT_READY;
+  CK(cudaSetDevice(ctx->device));
+  const size_t npix = (size_t)ctx->frame.res[0] * ctx->frame.res[1];
+  if (vis) CK(cudaMemcpyAsync(vis, ctx->vis.p, npix * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (shadow) {
+    int rc;
+    if ((rc = ensure(ctx, ctx->shadow16, npix * 2))) return rc;
+    CK(vmk::launch_to_r16f((const float*)ctx->shadow.p, (uint16_t*)ctx->shadow16.p, npix, ctx->sms, ctx->stream));
+    CK(cudaMemcpyAsync(shadow, ctx->shadow16.p, npix * 2, cudaMemcpyDeviceToHost, ctx->stream));
+  }
   return VM_OK;
 }
 

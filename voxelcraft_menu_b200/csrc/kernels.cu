@@ -19,6 +19,7 @@
 #include "kernels.cuh"
 #include "ray_stages.cuh"
 #include <algorithm>
+#include <cuda_fp16.h>
 
 namespace vmk {
 using namespace vmd;
@@ -271,6 +272,33 @@ cudaError_t launch_secondary(const vm_frame& f, const DevWorld& w, const unsigne
   if (f.res[0] == 0 || f.res[1] == 0) return cudaSuccess;
   dim3 g((f.res[0] + 15) / 16, (f.res[1] + 7) / 8);
   k_secondary<<<g, dim3(16, 8), 0, s>>>(f, w, vis, sec_key, sec_t, refl_key, refl_t);
+  return cudaGetLastError();
+}
+
+// The blocker distances in the engine's shadow target format
+// (shadow_dist_tex, texture_storage_2d<r16float>, shadow.wgsl:1): binary16,
+// rounded to nearest even.  Four pixels per thread (16 B in, 8 B out).
+__global__ void __launch_bounds__(256) k_to_r16f(const float* __restrict__ in, uint16_t* __restrict__ out,
+                                                 uint64_t n) {
+  const uint64_t n4 = n / 4u, stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t i = i0; i < n4; i += stride) {
+    const float4 v = reinterpret_cast<const float4*>(in)[i];
+    ushort4 h;
+    h.x = __half_as_ushort(__float2half_rn(v.x));
+    h.y = __half_as_ushort(__float2half_rn(v.y));
+    h.z = __half_as_ushort(__float2half_rn(v.z));
+    h.w = __half_as_ushort(__float2half_rn(v.w));
+    reinterpret_cast<ushort4*>(out)[i] = h;
+  }
+  for (uint64_t i = 4u * n4 + i0; i < n; i += stride) out[i] = __half_as_ushort(__float2half_rn(in[i]));
+}
+
+cudaError_t launch_to_r16f(const float* in, uint16_t* out, uint64_t n, int sms, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const uint64_t want = (n / 4u + 255u) / 256u;
+  const uint32_t blocks = (uint32_t)std::max<uint64_t>(1u, std::min<uint64_t>(want, (uint64_t)sms * 8u));
+  k_to_r16f<<<blocks, 256, 0, s>>>(in, out, n);
   return cudaGetLastError();
 }
 

@@ -106,6 +106,9 @@ cudaError_t launch_primary_shadow(const vm_frame& f, const vmd::DevWorld& w, con
 cudaError_t launch_secondary(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                              unsigned long long* sec_key, float* sec_t, unsigned long long* refl_key, float* refl_t,
                              cudaStream_t s);
+// n blocker distances as binary16 (the engine's R16F shadow target), rounded
+// to nearest even; in and out 16-byte / 8-byte aligned
+cudaError_t launch_to_r16f(const float* in, uint16_t* out, uint64_t n, int sms, cudaStream_t s);
 // shadow_horizontal + shadow_vertical (shadow.wgsl:62-116), fused: the shadow
 // mask (clamp(1 - occlusion, 0, 1)) of the frame's blocker distances.
 // limit = SHADOW_RADIUS_LIMIT (1..SOFTEN_MAX_LIMIT), penumbra = SOFT_PENUMBRA.

@@ -177,6 +177,19 @@ class Marcher:
         self._ck(self._L.vm_read_shadow(self._h, ptr(out)))
         return out
 
+    def wait_render(self, other: "Marcher"):
+        """vm_wait_render: later work of this context waits for other's last
+        render (its kernels, not its read-back)."""
+        self._ck(self._L.vm_wait_render(self._h, other._h))
+
+    def read_shadow_r16f(self) -> np.ndarray:
+        """The blocker distances as the engine's R16F shadow target
+        (vm_read_async_r16f): binary16 bit patterns, rounded to nearest even."""
+        out = np.empty(self._npix(), np.uint16)
+        self._ck(self._L.vm_read_async_r16f(self._h, None, ptr(out)))
+        self.sync()
+        return out
+
     def read_reflection(self):
         """Reflect legs of the water hits of the last FLAG_WATER_REFLECT frame: (key, t)."""
         k = np.empty(self._npix(), np.uint64)

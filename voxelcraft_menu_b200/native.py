@@ -154,6 +154,8 @@ _SIGNATURES = [
     ("vm_render_counted", C.c_int, [vp, P(VmTraffic)]),
     ("vm_render_events", C.c_int, [vp, P(vp)]),
     ("vm_read_async", C.c_int, [vp, vp, vp]),
+    ("vm_read_async_r16f", C.c_int, [vp, vp, vp]),
+    ("vm_wait_render", C.c_int, [vp, vp]),
     ("vm_batch_set", C.c_int, [vp, C.c_uint32, vp, vp, vp, vp, vp]),
     ("vm_batch_run", C.c_int, [vp, C.c_int]),
     ("vm_batch_read", C.c_int, [vp, vp, vp]),
