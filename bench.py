@@ -61,43 +61,73 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    reads every millisecond or so (read-only queries), else nvidia-smi every
+    200 ms."""
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []      # (sm_mhz, max_mhz, set of reason names)
+        self.source = None
         self._stop = threading.Event()
         self._t = None
 
+    def _nvml(self):
+        import pynvml as N
+        N.nvmlInit()
+        h = N.nvmlDeviceGetHandleByIndex(self.index)
+        bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
+                N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
+        mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        self.source = "nvml"
+        try:
+            while not self._stop.is_set():
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), {n for n, b in zip(self.NAMES, bits) if r & b}))
+                self._stop.wait(0.001)
+        finally:
+            N.nvmlShutdown()
+
+    def _smi(self):
+        self.source = "nvidia-smi"
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                f = [x.strip() for x in out.split(",")]
+                if len(f) >= 6 and f[0].replace(".", "").isdigit():
+                    self.samples.append((float(f[0]), float(f[1]),
+                                         {n for n, v in zip(self.NAMES, f[2:6]) if "Active" in v and "Not" not in v}))
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
     def start(self):
         def run():
-            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_power_cap")
-            while not self._stop.is_set():
-                try:
-                    out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.samples.append([s.strip() for s in out.split(",")])
-                except Exception:
-                    pass
-                self._stop.wait(0.2)
+            try:
+                self._nvml()
+            except Exception:
+                if not self._stop.is_set():
+                    self._smi()
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
+        time.sleep(0.005)   # first sample before the timed region
 
     def stop(self):
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]
-                          and "Not" not in s[3 + i]})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        sm = [x[0] for x in self.samples]
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(x[1] for x in self.samples) if self.samples else None,
+                "reasons": sorted(set().union(*[x[2] for x in self.samples])) if self.samples else [],
+                "samples": len(self.samples), "source": self.source}
 
 
 def peaks():
