@@ -252,3 +252,74 @@ def test_hiz_does_not_change_the_visibility():
     assert np.array_equal(vis0, visA) and np.array_equal(vis0, visB)
     assert cB[1] > 0, "the second frame defers pairs"
     assert cB[5] <= cB[1]
+
+
+# ---- the underwater reach: tests/submerged.rs --------------------------------
+# The engine pins tile_select's reach (tile_select.wgsl:116-133) by reading its
+# shader source; here the same properties are checked on the oracle's per-tile
+# chunk lists (or_tile_pairs): the reach applies only when both
+# FLAG_UNDERWATER and FLAG_WATER_FAR are set, it is decided by where the
+# tile's most upward corner ray leaves the water (frame.sea_level), and the
+# cull compares each chunk's box distance with it.
+
+def _tile_lists(flags, pos=(128.5, 62.0, 2.5), pitch=0.0):
+    w = World.generate(W.recipe_small_terrain())
+    v = w.view(Camera(pos=pos, pitch=math.radians(pitch), width=320, height=200, flags=flags))
+    v.frame.flags = flags          # exactly these flags, whatever the camera's medium
+    o = Oracle(v, *w.pools())
+    f = v.frame
+    return v, o, {t: o.tile_pairs(t)[0] for t in range(int(f.tiles[0]) * int(f.tiles[1]))}
+
+
+def _box_distance(p, c):
+    lo, hi = np.asarray(c["aabb_min"], np.float64), np.asarray(c["aabb_max"], np.float64)
+    d = np.maximum(np.maximum(lo - p, 0.0), p - hi)
+    return float(np.sqrt((d * d).sum()))
+
+
+def test_reach_needs_both_flags():
+    """submerged.rs: FLAG_WATER_FAR alone would clamp a dry camera; the
+    reach tests both flags in one expression."""
+    base = W.FLAG_SHADOWS
+    _, _, ref = _tile_lists(base)
+    for extra in (W.FLAG_WATER_FAR, W.FLAG_UNDERWATER):
+        _, _, got = _tile_lists(base | extra)
+        assert all(np.array_equal(got[t], ref[t]) for t in ref), f"flag {extra} alone changed the tile lists"
+
+
+def test_reach_culls_by_box_distance_below_the_water_only():
+    """submerged.rs: the cull reads the per-tile reach (dmin >= reach), and
+    the reach follows the water path: tiles whose corner rays all point down
+    never leave the water and lose every chunk at WATER_FAR_DIST or beyond;
+    tiles whose most upward corner ray reaches sea_level within that
+    distance keep the full view distance."""
+    base = W.FLAG_SHADOWS
+    v, o, ref = _tile_lists(base)
+    _, _, got = _tile_lists(base | W.FLAG_UNDERWATER | W.FLAG_WATER_FAR)
+    cam = np.asarray(v.frame.cam_pos, np.float64)
+    tx, ty = int(v.frame.tiles[0]), int(v.frame.tiles[1])
+    dropped_any = False
+    for t in ref:
+        kept = set(got[t].tolist())
+        assert kept <= set(ref[t].tolist())
+        row = t // tx
+        for ci in set(ref[t].tolist()) - kept:
+            dropped_any = True
+            assert row > ty // 2, f"tile {t} (an upward row) lost chunk {ci}"
+            assert _box_distance(cam, v.chunks[ci]) >= 128.0 - 1e-3
+        if row > ty // 2 + 1:                 # corner rays all below the horizon: reach 128
+            for ci in kept:
+                assert _box_distance(cam, v.chunks[ci]) < 128.0 + 1e-3 or ci == v.frame.camera_chunk
+        if row < ty // 2 - 1:                 # upward rows: sea level within 2 / up < 128
+            assert np.array_equal(got[t], ref[t])
+    assert dropped_any, "the camera sees chunks beyond the reach"
+
+
+def test_water_far_dist_is_shorter_than_the_view_distance():
+    """submerged.rs: 128 <= WATER_FAR_DIST < the default view distance
+    (2600, src/lod.rs:44)."""
+    from pathlib import Path
+    import re
+    src = (Path(__file__).resolve().parents[1] / "voxelcraft_menu_b200" / "csrc" / "vm_types.h").read_text()
+    reach = float(re.search(r"#define VM_WATER_FAR_DIST ([0-9.]+)f", src).group(1))
+    assert 128.0 <= reach < 2600.0
