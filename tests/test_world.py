@@ -1,11 +1,14 @@
 """Layout producers: the C++ restatement of the engine's encoder and pools,
 checked with the reference's own fixtures and assertions (tests/tree.rs,
-tests/full_march.rs, tests/emitter_gate.rs, tests/pairs.rs, tests/camera.rs)."""
+tests/full_march.rs, tests/emitter_gate.rs, tests/pairs.rs, tests/camera.rs,
+tests/shadow_grid.rs)."""
+import math
+
 import numpy as np
 import pytest
 
 from voxelcraft_menu_b200 import world as W
-from voxelcraft_menu_b200.world import World, dense_index
+from voxelcraft_menu_b200.world import Camera, World, dense_index
 
 X, Y, Z = np.meshgrid(np.arange(64, dtype=np.uint32), np.arange(64, dtype=np.uint32),
                       np.arange(64, dtype=np.uint32), indexing="ij")
@@ -290,3 +293,80 @@ def test_view_chunk_list_is_sorted_and_grid_indexes_it():
     assert used.size == len(ch) and np.array_equal(np.sort(used), np.arange(len(ch)))
     assert f.tiles[0] == 80 and f.tiles[1] == 45
     assert f.max_pairs == 1 << 20
+
+
+# ---- the shadow casters' grid: tests/shadow_grid.rs --------------------------
+# build_chunk_list + partition_for_grid (src/render/mod.rs:88-138,1447-1564):
+# the frame's list is the frustum-visible chunks (frame.chunk_count of them)
+# followed by the off-screen chunks that cover a cell of the grid lattice,
+# which only shadow and secondary rays reach.
+
+def _partition(w, yaw_deg, offscreen=True, grid_dim=None, pos=(128.5, 110.0, 128.5)):
+    cam = Camera(pos=pos, yaw=math.radians(yaw_deg), pitch=math.radians(-14.0), width=1280, height=720,
+                 offscreen_shadows=offscreen, grid_dim=grid_dim)
+    v = w.view(cam)
+    keys = [(int(c["origin"][0]) // 64, int(c["origin"][1]) // 64, int(c["origin"][2]) // 64, int(c["lod"]))
+            for c in v.chunks]
+    n_vis = int(v.frame.chunk_count)
+    gd = grid_dim or (W.GRID_X, W.GRID_Y, W.GRID_Z)
+    gmin = (math.floor(pos[0] / 64.0) - gd[0] // 2, 0, math.floor(pos[2] / 64.0) - gd[2] // 2)
+    return keys[:n_vis], keys[n_vis:], gmin, gd
+
+
+def _grid_span(key, gmin, gd):
+    """mod.rs:93-107 for a chunk key (x, y, z, lod)"""
+    span = 1 << key[3]
+    lo = [max(key[i] * span - gmin[i], 0) for i in range(3)]
+    hi = [min(key[i] * span - gmin[i] + span, gd[i]) for i in range(3)]
+    return (lo, hi) if all(l < h for l, h in zip(lo, hi)) else None
+
+
+@pytest.fixture(scope="module")
+def small_world():
+    return World.generate(W.recipe_small_terrain())
+
+
+def test_the_grid_set_is_the_same_at_every_yaw(small_world):
+    """shadow_grid.rs:78-103"""
+    ref = None
+    for gd in (None, (4, 2, 2)):
+        ref = None
+        for yaw in (0.0, 45.0, 90.0, 135.0, 180.0, 225.0, 265.0, 315.0):
+            vis, off, gmin, g = _partition(small_world, yaw, grid_dim=gd)
+            got = sorted(k for k in vis + off if _grid_span(k, gmin, g))
+            if ref is None:
+                ref = got
+            assert got == ref, f"grid {g}: the grid-eligible set changed at yaw {yaw}"
+        assert ref
+
+
+def test_the_drawn_set_still_depends_on_the_yaw(small_world):
+    """shadow_grid.rs:105-131"""
+    seen = []
+    for yaw in (0.0, 90.0, 180.0, 265.0):
+        vis, off, _, _ = _partition(small_world, yaw)
+        assert vis, f"nothing drawn at yaw {yaw}"
+        assert off, f"nothing shadow-only at yaw {yaw}"
+        seen.append(sorted(vis))
+    assert any(a != b for a, b in zip(seen, seen[1:])), "the frustum cull is not running"
+
+
+def test_the_control_leaves_exactly_the_frustum_culled_set(small_world):
+    """shadow_grid.rs:133-149"""
+    on_vis, on_off, _, _ = _partition(small_world, 265.0)
+    off_vis, off_off, _, _ = _partition(small_world, 265.0, offscreen=False)
+    assert not off_off, "the control left a shadow-only tail"
+    assert on_off, "the feature added no shadow-only tail"
+    assert on_vis == off_vis, "the control changed the drawn list"
+
+
+def test_every_shadow_only_chunk_reaches_the_lattice(small_world):
+    """shadow_grid.rs:151-165, on the full lattice and on one smaller than
+    the world"""
+    for gd in (None, (4, 2, 2)):
+        _, off, gmin, g = _partition(small_world, 265.0, grid_dim=gd)
+        for k in off:
+            span = _grid_span(k, gmin, g)
+            assert span is not None, f"{k} is in the tail and covers no grid cell"
+            lo, hi = span
+            assert all(0 <= l < h <= n for l, h, n in zip(lo, hi, g))
