@@ -60,6 +60,25 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(ms, world, device):
+    """The largest of the ranks' times: each replica times its own device,
+    and the job's step ends when the slowest rank's does.  Every rank calls
+    this at the same point (one all-reduce)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, rays_per_rank, ms):
+    """Whole-job Grays/s: every replica traces the same frame, so the job
+    traces world x rays_per_rank rays per step of ms milliseconds."""
+    return world * rays_per_rank / (ms * 1e-3) / 1e9
+
+
 class ClockSampler:
     """SM clocks and throttle reasons sampled during the timed region: NVML
     reads every millisecond or so (read-only queries), else nvidia-smi every
@@ -655,11 +674,8 @@ def main():
     ms = [row[0].elapsed_time(row[4]) for row in evs]
     stage_ms = {name: float(np.mean([row[i].elapsed_time(row[j]) for row in evs]))
                 for name, (i, j) in STAGES.items()}
-    ms_step = float(np.mean(ms))
+    ms_step = max_over_ranks(float(np.mean(ms)), world, dev)
     if world > 1:
-        t = torch.tensor([ms_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
         dist.barrier()
 
     filt = bench_filter(m, vb, pools, stream, flush, max(5, min(args.steps, 20)), 3,
@@ -668,7 +684,7 @@ def main():
 
     npix = 1920 * 1080
     rays = traffic["rays_primary"] + traffic["rays_shadow"]
-    value = world * rays / (ms_step * 1e-3) / 1e9
+    value = job_value(world, rays, ms_step)
 
     # e2e through the C ABI with host buffers (pinned), per step: frame + chunk
     # list + grid up, render, vis + shadow down
@@ -700,7 +716,7 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize(dev)
         e_ms.append(ev0.elapsed_time(ev1))
-    e2e_serial_ms = float(np.mean(e_ms))
+    e2e_serial_ms = max_over_ranks(float(np.mean(e_ms)), world, dev)
 
     # e2e as a renderer runs consecutive frames: two contexts alternate; each
     # step renders its frame after the other context's last render
@@ -765,11 +781,7 @@ def main():
             assert np.array_equal(vh.numpy().view(np.uint64), vis_h.numpy().view(np.uint64))
             want = sh_h.numpy().astype(np.float16).view(np.int16) if r16f else sh_h.numpy()
             assert np.array_equal(shh.numpy(), want)
-        if world > 1:
-            t = torch.tensor([ms_], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms_ = float(t.item())
-        return ms_
+        return max_over_ranks(ms_, world, dev)
 
     e2e_ms = e2e_two_contexts(True)
     e2e_f32_ms = e2e_two_contexts(False)
@@ -817,17 +829,17 @@ def main():
                          "algorithmic_bytes_per_launch": sbytes[top], "launch_ms": stage_ms[top],
                          "dda_steps_per_launch": stage_iters(traffic, top),
                          "bytes_per_dda_step": sbytes[top] / max(stage_iters(traffic, top), 1)},
-            "e2e": {"value": world * rays / (e2e_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "e2e": {"value": job_value(world, rays, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                     "method": "two contexts alternate; every step renders once the other context's last render is "
                               "done (vm_wait_render), uploads the next step's inputs from pinned host memory ahead "
                               "of its own read-back, and reads vis (u64 keys) + shadow back in the engine's own "
                               "formats (the shadow target is r16float, shadow.wgsl:1; vm_read_async_r16f), "
                               "overlapping the next step's kernels"},
-            "e2e_f32": {"value": world * rays / (e2e_f32_ms * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "e2e_f32": {"value": job_value(world, rays, e2e_f32_ms), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h_f32, "ms_per_step": e2e_f32_ms,
                         "method": "as e2e, the shadow read back as float (vm_read_async)"},
-            "e2e_serial": {"value": world * rays / (e2e_serial_ms * 1e-3) / 1e9, "unit": UNIT,
+            "e2e_serial": {"value": job_value(world, rays, e2e_serial_ms), "unit": UNIT,
                            "ms_per_step": e2e_serial_ms,
                            "method": "one context, synchronous read-back, L2 flushed before each step"},
             # per frame: k_prepass, k_cull, k_order, k_primary, k_shadow, k_secondary_q
