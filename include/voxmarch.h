@@ -33,7 +33,8 @@ typedef enum vm_status {
   VM_E_ITER_CAP = 4,       /* informational: some march hit MAX_ITERS (common.wgsl:698-701); counted, not fatal */
   VM_E_TIMEOUT = 5,        /* a bounded device wait gave up */
   VM_E_CUDA = 6,           /* CUDA runtime error */
-  VM_E_NOT_READY = 7       /* call order: e.g. march before world / frame */
+  VM_E_NOT_READY = 7,      /* call order: e.g. march before world / frame */
+  VM_E_TOO_LARGE = 8       /* the frame exceeds a fixed limit of vm_render_static (nothing was run) */
 } vm_status;
 
 typedef struct vm_ctx vm_ctx;
@@ -63,7 +64,12 @@ int vm_update_pool(vm_ctx* ctx, int pool, uint64_t offset, const uint32_t* data,
 /* build_chunk_list's uploads (src/render/mod.rs:1555-1562): the chunk list
  * (visible chunks first, then shadow-only ones) and the chunk grid. */
 int vm_upload_chunks(vm_ctx* ctx, const vm_chunk* chunks, uint32_t n_chunks, const uint32_t* grid, uint64_t grid_len);
-/* queue.write_buffer of GpuFrame (src/render/mod.rs:1707). */
+/* queue.write_buffer of GpuFrame (src/render/mod.rs:1707).  A sun_dir with a
+ * zero component is accepted (the engine's sun(t), src/scene.rs:10-14, has
+ * dir.y == 0 at t = 0.25 with shadows on): as in shadow_ray_t
+ * (common.wgsl:1157) the reciprocal is then an IEEE infinity and the shadow
+ * DDA runs on IEEE arithmetic (NaN comparisons false, NaN -> 0 conversions,
+ * wrapping i32 subtraction), the same operations as the oracle's. */
 int vm_set_frame(vm_ctx* ctx, const vm_frame* frame);
 
 /* The engine's passes, one call per group of dispatches (src/render/mod.rs:1716-1851):
@@ -280,9 +286,9 @@ int vm_sync(vm_ctx* ctx);
  * from their own arenas, allocation-free real-time paths.  The caller passes
  * every input and output as device pointers (pools, chunk list, grid, vis,
  * shadow, a zeroed u32 error word) on the current device and stream; the
- * pipeline's scratch is one static device array of about 7.6 MB per GPU.
- * Primary and shadow rays only; at most 262144 pixels and 8192 8x8 tiles per
- * frame (larger frames return VM_E_CAPACITY).  The first call on a device
+ * pipeline's scratch is one static device array of 8,650,900 bytes (8.25 MiB)
+ * per GPU.  Primary and shadow rays only; at most 262144 pixels and 8192 8x8
+ * tiles per frame (larger frames return VM_E_TOO_LARGE and run nothing).  The first call on a device
  * looks the array up and must come before any stream capture.  Every call
  * shares the array: calls that overlap on the GPU race.
  * vm_static_last_error() describes the last failure of this thread. */

@@ -221,6 +221,12 @@ inline uint64_t grid_index(const World& w, I3 rel) {
   return (uint64_t)(uint32_t)rel.x + (uint64_t)(uint32_t)rel.y * gd[0] +
          (uint64_t)(uint32_t)rel.z * gd[0] * gd[1];
 }
+// i32 subtraction with WGSL's wrapping semantics (a cell from the floor of an
+// infinite coordinate saturates to INT32_MAX / INT32_MIN and may overflow)
+inline int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
+inline I3 grid_rel(const World& w, I3 cell) {
+  return {wsub(cell.x, w.f->grid_min[0]), wsub(cell.y, w.f->grid_min[1]), wsub(cell.z, w.f->grid_min[2])};
+}
 inline bool grid_outside(const World& w, I3 rel) {
   const uint32_t* gd = w.f->grid_dim;
   return rel.x < 0 || rel.y < 0 || rel.z < 0 || rel.x >= (int32_t)gd[0] ||
@@ -230,7 +236,7 @@ inline bool grid_outside(const World& w, I3 rel) {
 // world_block_at: common.wgsl:266-277
 uint32_t world_block_at(const World& w, V3 p) {
   I3 cell = floor_i(divs(p, 64.0f));
-  cell = {cell.x - w.f->grid_min[0], cell.y - w.f->grid_min[1], cell.z - w.f->grid_min[2]};
+  cell = grid_rel(w, cell);
   if (grid_outside(w, cell)) return 0u;
   cnt_add(&Counters::grid_lookups);
   uint32_t ci = grid_at(w, grid_index(w, cell));
@@ -606,7 +612,7 @@ float shadow_ray_t(const World& w, V3 ro, V3 rd, float max_dist) {
   float t = 0.0f;
   uint32_t last = VM_NO_CHUNK;
   for (uint32_t i = 0; i < 24u; ++i) {
-    I3 rel{cell.x - w.f->grid_min[0], cell.y - w.f->grid_min[1], cell.z - w.f->grid_min[2]};
+    I3 rel = grid_rel(w, cell);
     if (grid_outside(w, rel)) return -1.0f;
     cnt_add(&Counters::grid_lookups);
     uint32_t ci = grid_at(w, grid_index(w, rel));
@@ -641,7 +647,7 @@ WorldHit trace_world(const World& w, V3 ro, V3 rd, float max_dist, bool skip_wat
   bool pos_dir[3] = {dir.x > 0.0f, dir.y > 0.0f, dir.z > 0.0f};
   I3 cell = floor_i(divs(ro, 64.0f));
   for (uint32_t i = 0; i < 16u; ++i) {
-    I3 rel{cell.x - w.f->grid_min[0], cell.y - w.f->grid_min[1], cell.z - w.f->grid_min[2]};
+    I3 rel = grid_rel(w, cell);
     if (grid_outside(w, rel)) return out;
     cnt_add(&Counters::grid_lookups);
     uint32_t ci = grid_at(w, grid_index(w, rel));
@@ -1329,7 +1335,7 @@ int or_expand(const or_world* o, const uint64_t* vis, const int32_t* wmin, const
 // Block lookup through the chunk grid (lod-0 chunks), for the unit DDA below.
 static uint32_t grid_block(const World& w, int32_t x, int32_t y, int32_t z) {
   I3 cell{x >> 6, y >> 6, z >> 6};
-  I3 rel{cell.x - w.f->grid_min[0], cell.y - w.f->grid_min[1], cell.z - w.f->grid_min[2]};
+  I3 rel = grid_rel(w, cell);
   if (grid_outside(w, rel)) return 0u;
   uint32_t ci = grid_at(w, grid_index(w, rel));
   if (ci == VM_NO_CHUNK) return 0u;

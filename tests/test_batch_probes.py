@@ -72,3 +72,31 @@ def test_probe_batch_matches_per_view_and_oracle(world):
         assert np.array_equal(bs[off:off + n], sh)
         off += n
     assert traffic["rays_shadow"] == shadow_rays
+
+
+@pytest.mark.gpu
+def test_256_probe_faces_and_a_full_hd_player_view_match_the_oracle(world):
+    """The largest members of the batched workload: 256x256 cube faces and a
+    1920x1080 player view, in one persistent batch, equal the oracle bit for
+    bit (visibility and shadow distances)."""
+    from oracle.oracle import Oracle
+    from voxelcraft_menu_b200.march import Marcher
+    pools = world.pools()
+    views = V.probe_views(world, n_probes=2, res=(256,)) + V.player_views(world, n=1)
+    assert views[-1].res == (1920, 1080)
+    m = Marcher(1920, 1080)
+    m.upload_world(*pools)
+    m.batch_set(views)
+    m.batch_run()
+    bv, bs = m.batch_read()
+    off = 0
+    for v in views:
+        n = v.n_pixels
+        o = Oracle(v, *pools)
+        vis, _, _ = o.frame_vis()
+        sh = o.shadow(vis)
+        assert np.array_equal(bv[off:off + n], vis), f"view {v.res}: visibility differs"
+        assert np.array_equal(bs[off:off + n], sh), f"view {v.res}: shadow differs"
+        off += n
+    assert (bv != 0).mean() > 0.3
+    m.close()

@@ -46,6 +46,16 @@ def oracle_all(view, pools, hiz_in=None, tiles=None):
     return o, vis, hiz, ctr, sh, sk, st
 
 
+def tile_min_depth(vis, view):
+    """build_hiz (march.wgsl:57-76) over a visibility buffer: per 8x8 tile the
+    minimum depth key, 0 when a pixel of the tile (or outside the frame) missed."""
+    w, h = view.res
+    tx, ty = int(view.frame.tiles[0]), int(view.frame.tiles[1])
+    d = np.zeros((ty * 8, tx * 8), np.uint32)
+    d[:h, :w] = (vis >> np.uint64(40)).astype(np.uint32).reshape(h, w)
+    return d.reshape(ty, 8, tx, 8).min(axis=(1, 3)).reshape(-1)
+
+
 def assert_same(got, want, what):
     if not np.array_equal(got, want):
         bad = np.flatnonzero(got != want)
@@ -256,6 +266,91 @@ def test_large_world_full_hd(large):
     assert_same(fv[sl], vis[sl], "vis band")
     sh = o.shadow(vis, pix=(sl.start, sl.stop))
     assert_same(fs[sl], sh[sl], "shadow band")
+
+
+def test_large_world_full_frame_a_and_b_match_the_oracle(large):
+    """The benchmarked frame pair over every pixel: frame A with FLAG_HIZ and a
+    cleared Hi-Z, then frame B with the camera moved half a voxel and A's Hi-Z
+    carried over.  Visibility, shadow distances, water / glass keys and
+    distances and the Hi-Z equal the oracle's through both the engine pass
+    sequence and vm_render; the engine passes also report the oracle's
+    deferred / recovered pair counts."""
+    rec, w, pools, m = large
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_HIZ
+    cam_a = W.large_terrain_camera(rec, flags=flags)
+    va = w.view(cam_a)
+    cam_b = W.large_terrain_camera(rec, flags=flags)
+    cam_b.pos = (cam_b.pos[0] + 0.5, cam_b.pos[1], cam_b.pos[2])
+    vb = w.view(cam_b)
+    ntiles = int(va.frame.tiles[0]) * int(va.frame.tiles[1])
+    oa = Oracle(va, *pools)
+    vis_a, hiz_a, ctr_a = oa.frame_vis(hiz_in=np.zeros(ntiles, np.uint32))
+    sh_a = oa.shadow(vis_a)
+    sk_a, st_a = oa.secondary(vis_a)
+    ob = Oracle(vb, *pools)
+    vis_b, hiz_b, ctr_b = ob.frame_vis(hiz_in=hiz_a)
+    sh_b = ob.shadow(vis_b)
+    sk_b, st_b = ob.secondary(vis_b)
+    assert ctr_b[1] > 0, "frame B defers pairs against A's Hi-Z"
+    assert (sh_b > 0).any() and (sk_b >> 62 & 1).any()
+
+    def check(tag, vis, sh, sk, st, hiz):
+        assert_same(m.read_vis(), vis, f"{tag} vis")
+        assert_same(m.read_shadow(), sh, f"{tag} shadow")
+        gk, gt = m.read_secondary()
+        assert_same(gk, sk, f"{tag} secondary key")
+        assert_same(gt, st, f"{tag} secondary t")
+        assert_same(m.read_hiz(), hiz, f"{tag} hiz")
+        assert m.stats().device_error == 0
+
+    # engine pass sequence
+    m.upload_view(va)
+    m.write_hiz(np.zeros(ntiles, np.uint32))
+    m.render_passes()
+    check("passes A", vis_a, sh_a, sk_a, st_a, hiz_a)
+    m.upload_view(vb)
+    m.render_passes()
+    check("passes B", vis_b, sh_b, sk_b, st_b, hiz_b)
+    s = m.stats()
+    assert s.pairs_deferred == ctr_b[1] and s.pairs_recovered == ctr_b[5] and s.pairs_selected == ctr_b[4]
+    # the wavefront pipeline, frame A then B; its Hi-Z output is build_hiz
+    # (march.wgsl:57-76) of the final visibility
+    m.upload_view(va)
+    m.render()
+    check("pipeline A", vis_a, sh_a, sk_a, st_a, tile_min_depth(vis_a, va))
+    m.upload_view(vb)
+    m.render()
+    check("pipeline B", vis_b, sh_b, sk_b, st_b, tile_min_depth(vis_b, vb))
+
+
+def _sun(t):
+    """The engine's sun(t) direction (src/scene.rs:10-14) in float32, with
+    glam's normalize (v * (1 / length))."""
+    a = np.float32((t - 0.25) * np.float32(2.0 * np.pi))
+    v = np.array([np.cos(a) * np.float32(0.55), np.sin(a), np.float32(0.42)], np.float32)
+    r = np.float32(1.0) / np.sqrt(np.float32((v * v).sum()))
+    return tuple((v * r).astype(np.float32).tolist())
+
+
+@pytest.mark.parametrize("sun", ["t=0.25", (0.0, 0.8, 0.6), (0.6, 0.8, 0.0), (0.0, 1.0, 0.0)])
+def test_sun_with_zero_components_matches_the_oracle(small, sun):
+    """The engine's sun at t = 0.25 has dir.y == 0 exactly, with daylight 0.375
+    and shadows on; axis-aligned suns give infinite reciprocals in x or z.
+    Both sides follow IEEE arithmetic from 1 / 0 = inf on."""
+    w, pools, m = small
+    d = _sun(0.25) if sun == "t=0.25" else sun
+    if sun == "t=0.25":
+        assert d[1] == 0.0
+    v = w.view(W.small_terrain_camera(sun_dir=d, daylight=0.375))
+    m.upload_view(v)
+    o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
+    m.render()
+    assert_same(m.read_vis(), vis, "vis")
+    assert_same(m.read_shadow(), sh, "shadow")
+    gk, gt = m.read_secondary()
+    assert_same(gk, sk, "secondary key")
+    m.render_passes()
+    assert_same(m.read_shadow(), sh, "passes shadow")
 
 
 def test_batch_matches_single_views(small):

@@ -145,8 +145,6 @@ int check_frame(vm_ctx* ctx, const vm_frame& f, uint32_t n_chunks, uint64_t grid
   if ((uint64_t)f.grid_dim[0] * f.grid_dim[1] * f.grid_dim[2] > grid_len)
     return fail(ctx, VM_E_INVALID, "grid_dim product exceeds the uploaded grid");
   if (!(f.far_ > 0.0f)) return fail(ctx, VM_E_INVALID, "far must be positive");
-  if (f.sun_dir[0] == 0.0f || f.sun_dir[1] == 0.0f || f.sun_dir[2] == 0.0f)
-    return fail(ctx, VM_E_INVALID, "sun_dir components must be nonzero (the shadow DDA divides by them)");
   if (f.max_pairs == 0 || f.max_pairs > 0x7FFFFFFFu) return fail(ctx, VM_E_INVALID, "max_pairs out of range");
   return VM_OK;
 }

@@ -213,8 +213,12 @@ __device__ __forceinline__ bool voxel_occupied(const DevWorld& w, const Chunk& c
   return mask_has(leaf.x, leaf.y, cell_bit(ux & 3u, uy & 3u, uz & 3u));
 }
 
+// i32 subtraction with WGSL's wrapping semantics (a cell from the floor of an
+// infinite coordinate saturates to INT32_MAX / INT32_MIN and may overflow)
+__device__ __forceinline__ int32_t wsub(int32_t a, int32_t b) { return (int32_t)((uint32_t)a - (uint32_t)b); }
+
 __device__ __forceinline__ bool grid_rel(const vm_frame& f, int32_t cx, int32_t cy, int32_t cz, uint64_t* idx) {
-  int32_t rx = cx - f.grid_min[0], ry = cy - f.grid_min[1], rz = cz - f.grid_min[2];
+  int32_t rx = wsub(cx, f.grid_min[0]), ry = wsub(cy, f.grid_min[1]), rz = wsub(cz, f.grid_min[2]);
   if (rx < 0 || ry < 0 || rz < 0 || rx >= (int32_t)f.grid_dim[0] || ry >= (int32_t)f.grid_dim[1] ||
       rz >= (int32_t)f.grid_dim[2])
     return false;
@@ -292,7 +296,10 @@ static __device__ __noinline__ bool cutout_march(int32_t wx, int32_t wy, int32_t
   return false;
 }
 
-// Ray state shared by a sequence of march_chunk calls on one ray.
+// Ray state shared by a sequence of march_chunk calls on one ray.  A zero
+// direction component (a sun exactly on the horizon) gives an infinite
+// reciprocal, as the WGSL's 1.0 / rd does; every later step is IEEE
+// arithmetic, which the oracle repeats operation for operation.
 struct Ray {
   F3 o, d, inv;
   bool pdx, pdy, pdz;

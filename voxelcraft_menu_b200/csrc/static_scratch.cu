@@ -9,8 +9,9 @@
 //
 // Limits and sharing rules:
 //  * at most STATIC_MAX_PIXELS pixels and STATIC_MAX_TILES 8x8 tiles per frame
-//    (larger frames are rejected with VM_E_CAPACITY); ~7.6 MB of device memory
-//    that every GPU loading this library keeps until the process exits;
+//    (larger frames are rejected with VM_E_TOO_LARGE); 8,650,900 bytes (8.25 MiB)
+//    of device memory that every GPU loading this library keeps until the
+//    process exits (checked by a static_assert below);
 //  * primary and shadow rays only (no secondary rays, no Hi-Z output);
 //  * the scratch is shared by every call on a device and keeps the last call's
 //    contents; calls whose work overlaps on the GPU (different streams, or
@@ -44,6 +45,7 @@ struct StaticScratch {
   uint32_t super_count[STATIC_MAX_TILES];
   vmk::ShadowItem shadow_q[STATIC_MAX_PIXELS];
 };
+static_assert(sizeof(StaticScratch) == 8650900, "the documented size of the static scratch");
 
 __device__ __align__(256) StaticScratch g_static_scratch;
 
@@ -75,15 +77,14 @@ extern "C" int vm_render_static(const vm_frame* frame, const vm_chunk* d_chunks,
   if (f.tiles[0] != (f.res[0] + 7) / 8 || f.tiles[1] != (f.res[1] + 7) / 8)
     return fail(VM_E_INVALID, "tiles do not match the resolution in 8x8 tiles");
   if (npix > STATIC_MAX_PIXELS || tiles > STATIC_MAX_TILES)
-    return fail(VM_E_CAPACITY, "frame exceeds the static scratch: at most 262144 pixels and 8192 8x8 tiles");
+    return fail(VM_E_TOO_LARGE, "frame exceeds the static scratch: at most 262144 pixels and 8192 8x8 tiles");
   if (n_chunks > VM_MAX_CHUNKS || f.chunk_count > n_chunks)
     return fail(VM_E_INVALID, "chunk_count must not exceed the chunk list, which must not exceed 8191");
   if (f.camera_chunk != VM_NO_CHUNK && f.camera_chunk >= f.chunk_count)
     return fail(VM_E_INVALID, "camera_chunk outside the visible list");
   if ((uint64_t)f.grid_dim[0] * f.grid_dim[1] * f.grid_dim[2] > grid_len)
     return fail(VM_E_INVALID, "grid_dim product exceeds the grid");
-  if (!(f.far_ > 0.0f) || f.sun_dir[0] == 0.0f || f.sun_dir[1] == 0.0f || f.sun_dir[2] == 0.0f)
-    return fail(VM_E_INVALID, "far must be positive and sun_dir components nonzero");
+  if (!(f.far_ > 0.0f)) return fail(VM_E_INVALID, "far must be positive");
 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail(VM_E_CUDA, "no current CUDA device");

@@ -19,7 +19,7 @@ from .world import FLAG_HIZ, View, World
 
 VM_OK = 0
 STATUS = {0: "VM_OK", 1: "VM_E_INVALID", 2: "VM_E_CAPACITY", 3: "VM_E_TILE_OVERFLOW", 4: "VM_E_ITER_CAP",
-          5: "VM_E_TIMEOUT", 6: "VM_E_CUDA", 7: "VM_E_NOT_READY"}
+          5: "VM_E_TIMEOUT", 6: "VM_E_CUDA", 7: "VM_E_NOT_READY", 8: "VM_E_TOO_LARGE"}
 
 # warps per block and register levels of the persistent primary-ray kernel (vm_set_tuning)
 PRIMARY_WARPS = (4, 8)
