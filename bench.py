@@ -168,75 +168,93 @@ def build_workload():
     return w, pools, view_a, view_b
 
 
-def oracle_rows(o, view, row0, rows):
-    """Time the oracle's frame (engine pass sequence) + shadow pass over tile
-    rows [row0, row0 + rows); returns (seconds, primary + shadow rays)."""
-    tx, ty = int(view.frame.tiles[0]), int(view.frame.tiles[1])
-    rows = min(rows, ty - row0)
-    width, height = int(view.frame.res[0]), int(view.frame.res[1])
-    tiles = (row0 * tx, (row0 + rows) * tx)
-    p0, p1 = row0 * 8 * width, min((row0 + rows) * 8, height) * width
-    t0 = time.perf_counter()
-    vis, _, _, tr = o.frame_vis(tiles=tiles, traffic=True)
-    _, tr2 = o.shadow(vis, pix=(p0, p1), traffic=True)
-    dt = time.perf_counter() - t0
-    return dt, tr["rays"] + tr2["rays"], p1 - p0
+def oracle_workload():
+    """The benchmark's frame pair built by the oracle's own producer (the
+    engine's encoder, pools and chunk list restated in oracle/producer.cpp):
+    the CPU legs never load the product library."""
+    from oracle import producer as OP
+    from voxelcraft_menu_b200 import world as W
+    rec = W.recipe_large_terrain()
+    ow = OP.OracleWorld.generate(rec)
+    h = OP.surface_height(rec, 512, 512)
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_HIZ
+    va, vb = (ow.view(W.Camera(pos=(512.0 + dx, float(h + 30), 512.0), width=1920, height=1080, flags=flags))
+              for dx in (0.0, 0.5))
+    return ow, ow.pools(), va, vb
 
 
-def cpu_sample(view, pools, budget_s=12.0):
-    """The oracle (the engine's pass sequence restated on the CPU) over a
-    bounded band of tile rows of the same frame, on every host core."""
-    from oracle.oracle import Oracle
-    o = Oracle(view, *pools)
-    ty = int(view.frame.tiles[1])
-    t_total, rays, px, rows, row0 = 0.0, 0, 0, 2, ty // 2 - 8
-    while t_total < budget_s:
-        if row0 >= ty:
-            row0 = 0          # the whole frame again until the budget is spent
-        dt, r, p = oracle_rows(o, view, row0, rows)
+class OracleFrames:
+    """The oracle over the whole timed frame: frame B's visibility by the
+    engine's pass sequence with frame A's Hi-Z, its shadow rays and its water
+    / glass rays -- the work one GPU step does."""
+
+    def __init__(self, pools, va, vb):
+        from oracle.oracle import Oracle
+        oa = Oracle(va, *pools)
+        self.hiz_a = oa.frame_vis(hiz_in=np.zeros(oa.ntiles, np.uint32))[1]
+        self.o = Oracle(vb, *pools)
+        self.npix = self.o.npix
+
+    def step(self):
+        """One frame; returns (seconds, primary + shadow rays)."""
+        t0 = time.perf_counter()
+        vis, _, _, tr = self.o.frame_vis(hiz_in=self.hiz_a, traffic=True)
+        _, tr2 = self.o.shadow(vis, traffic=True)
+        self.o.secondary(vis)
+        return time.perf_counter() - t0, tr["rays"] + tr2["rays"]
+
+
+def cpu_sample(pools, va, vb, budget_s=10.0):
+    """The oracle (the engine's pass sequence restated on the CPU) over whole
+    frames of the timed workload, on every host core, until the budget is
+    spent (at least one frame)."""
+    fr = OracleFrames(pools, va, vb)
+    t_total, rays, frames = 0.0, 0, 0
+    while frames == 0 or t_total < budget_s:
+        dt, r = fr.step()
         t_total += dt
         rays += r
-        px += p
-        row0 += rows
-        rows = min(rows * 2, 32)
+        frames += 1
     # footnote baseline: the engine's own CPU ray walk (Player::pick, a
     # unit-voxel DDA over block lookups) per pixel of a few pixel rows
-    height = int(view.frame.res[1])
+    height = int(vb.frame.res[1])
     t0 = time.perf_counter()
-    n_pick, hits = o.pick_rows(height // 2 - 64, 128)
+    n_pick, hits = fr.o.pick_rows(height // 2 - 64, 128)
     t_pick = time.perf_counter() - t0
     return {"value": rays / t_total / 1e9, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"oracle (engine pass sequence restated in C++, OpenMP) over the middle tile rows of the "
-                      f"same frame: {px} pixels, {rays} primary+shadow rays in {t_total:.1f}s",
+            "sample": f"oracle (engine pass sequence restated in C++, OpenMP) over {frames} whole frames of the "
+                      f"timed workload (frame B with frame A's Hi-Z, shadow and water / glass rays): "
+                      f"{rays} primary+shadow rays in {t_total:.1f}s",
             "unit_voxel_walk": {"value": n_pick / t_pick / 1e9, "unit": "Grays/s (primary rays only)",
                                 "sample": f"Player::pick (src/player.rs:334-393) restated, per pixel of 128 pixel rows "
                                           f"({n_pick} rays, {hits} hits) in {t_pick:.2f}s on every host core"}}
 
 
 def reference_arm(args):
+    """The engine's path on the CPU: the oracle restatement of its march over
+    the same frame, with its world built by the oracle's producer; the whole
+    frame every step (the GPU arm's pixel set), on every host core."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    w, pools, va, vb = build_workload()
-    from oracle.oracle import Oracle
-    o = Oracle(vb, *pools)
-    ty = int(vb.frame.tiles[1])
-    rows = 8
-    row0 = ty // 2 - rows // 2
-    times, rays, px = [], 0, 0
+    _, pools, va, vb = oracle_workload()
+    fr = OracleFrames(pools, va, vb)
+    times, rays = [], 0
     for i in range(args.warmup + args.steps):
-        dt, r, p = oracle_rows(o, vb, row0, rows)
+        dt, r = fr.step()
         if i >= args.warmup:
             times.append(dt)
-            rays, px = r, p
+            rays = r
     mean = float(np.mean(times))
     value = rays / mean / 1e9
-    sample = f"oracle over {rows} middle tile rows per step ({px} pixels, {rays} primary+shadow rays)"
+    sample = (f"oracle over the whole frame every step ({fr.npix} pixels, {rays} primary+shadow rays, plus the "
+              f"water / glass rays), world and chunk list from the oracle's producer")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "resolution": [1920, 1080], "chunks": int(len(vb.chunks)),
-                       "sample": sample, "parallelism": f"{os.cpu_count()} host threads"},
+                       "l2": "host caches (the CPU arm flushes nothing)", "parallelism": "replicas x1"},
+            "host_threads": os.cpu_count(),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -813,8 +831,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "resolution": [1920, 1080], "chunks": int(len(vb.chunks)),
-                       "tuning": best, "l2": "flushed between timed steps (256 MB write)",
-                       "parallelism": f"replicas x{world}"},
+                       "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{world}"},
+            "tuning": best,
             "stage_ms": stage_ms,
             "work_per_step": traffic,
             "rays_per_step": {"primary": traffic["rays_primary"], "shadow": traffic["rays_shadow"],
@@ -853,7 +871,8 @@ def main():
             line["reflect"] = refl
         line.update(extra)
         if not args.no_cpu:
-            line["cpu_baseline"] = cpu_sample(vb, pools)
+            _, o_pools, o_va, o_vb = oracle_workload()
+            line["cpu_baseline"] = cpu_sample(o_pools, o_va, o_vb)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

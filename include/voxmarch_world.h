@@ -5,9 +5,14 @@
  * src/voxel/world.rs:63-175, src/voxel/geometry.rs:64-219,
  * src/voxel/attributes.rs:6-139) and, per frame, the chunk list and chunk grid
  * (src/render/mod.rs:88-138,1447-1564).  An engine that keeps its own Rust
- * world only needs include/voxmarch.h; this header is the same host work in
- * C++ for callers without it (the tests, the benchmarks and the smoke check),
- * producing byte-identical buffers.
+ * world only needs include/voxmarch.h.  This header is a world store for
+ * callers without one (the tests, the benchmarks and the smoke check): the
+ * same encoded chunk format and pool node formats, the same chunk list and
+ * grid, and march outputs identical to those over the engine's pools.  The
+ * pools' offsets are its own: chunks are kept encoded and the pools are
+ * packed from them, in insertion order with identical leaf-mask and
+ * inner-node runs shared, whenever a view or a pool is asked for after an
+ * edit (no reference counts, no free lists).
  */
 #ifndef VOXMARCH_WORLD_H
 #define VOXMARCH_WORLD_H
@@ -79,32 +84,47 @@ typedef struct vmw_pool_stats_t {
 
 vmw_world* vmw_create(void);
 void vmw_destroy(vmw_world* w);
-/* World::insert_local(key, build_local(dense)); dense index x | z<<6 | y<<12 */
+/* Insert (or replace) the chunk of level lod at chunk cell (x, y, z), encoded
+ * from dense 64^3 block ids, index x | z<<6 | y<<12 (World::insert_local of
+ * build_local, src/voxel/world.rs:63, src/voxel/tree.rs:89).  The chunk
+ * becomes the last of the render set, with fade 1. */
 int vmw_insert_dense(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z, const uint16_t* dense);
-/* build_local (src/voxel/tree.rs:89-204) of one dense chunk (64^3 block ids,
- * index x | z<<6 | y<<12) into the flat layout that vm_encode_trees writes:
- * info, up to 64 L1 nodes, up to 4096 leaf masks and attribute entries, and
- * up to palette_cap palette words (more sets VM_TREE_PALETTE_OVERFLOW).  The
- * CPU restatement of the engine's encoder: the GPU encoder's parity anchor. */
+/* The encoder on the host (build_local, src/voxel/tree.rs:89-204, with
+ * encode_leaf src/voxel/attributes.rs:90-139) for one dense chunk, in the flat
+ * layout that vm_encode_trees writes, by the same passes: info, up to 64 L1
+ * nodes, up to 4096 leaf masks and attribute entries, and up to palette_cap
+ * palette words (more sets VM_TREE_PALETTE_OVERFLOW). */
 int vmw_build_tree(const uint16_t* dense, uint32_t palette_cap, vm_tree_info* info, vm_tree_l1* l1,
                    uint64_t* leaves, uint32_t* attrs, uint32_t* palette);
-/* World::insert_local (src/voxel/world.rs:63-175) of a chunk in that flat
- * layout, e.g. from vm_encode_trees: the run / word pools dedup it exactly as
- * vmw_insert_dense does.  Rejects an overflowed or inconsistent tree (1). */
+/* Insert a chunk given in that flat layout, e.g. from vm_encode_trees, as
+ * vmw_insert_dense does.  Rejects an overflowed or inconsistent tree (1): a
+ * leaf run, attribute range or palette offset outside its arrays. */
 int vmw_insert_tree(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z, const vm_tree_info* info,
                     const vm_tree_l1* l1, const uint64_t* leaves, const uint32_t* attrs, const uint32_t* palette);
 int vmw_remove(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z);
-/* World::get_block (src/voxel/world.rs:258-277) */
+/* The chunk's LOD cross-fade as the engine's render item carries it
+ * (RenderItem::fade, src/lod.rs:56-80): 1 solid, f in (0, 1) a fading-in
+ * finer chunk, -f its fading-out coarser parent.  It goes into GpuChunk.fade
+ * (the march's dither, common.wgsl:370-385) and orders the grid fill by share
+ * (src/render/mod.rs:1536-1552).  1 no such chunk, 2 fade outside [-1, 1] or 0. */
+int vmw_set_fade(vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z, float fade);
+/* World::get_block (src/voxel/world.rs:258-277): the block of lod-0 chunks */
 uint32_t vmw_get_block(const vmw_world* w, int32_t x, int32_t y, int32_t z);
 int vmw_get_chunk_info(const vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z, vmw_chunk_info* out);
-/* World::l1_node (src/voxel/world.rs:225-234): 1 found, 0 absent, -1 no chunk */
-int vmw_l1_node(const vmw_world* w, uint8_t lod, int32_t x, int32_t y, int32_t z, uint32_t l1b, uint32_t* out4);
+/* Pool sizes after packing; live_* equal n_* (packed pools hold no free
+ * space) and referenced_* count the elements all chunks refer to, so
+ * referenced - live is what run sharing saved. */
 void vmw_pool_stats(const vmw_world* w, vmw_pool_stats_t* s);
 const uint32_t* vmw_inners(const vmw_world* w);   /* n_inners x vec4<u32> */
 const uint32_t* vmw_leaves(const vmw_world* w);   /* n_leaves x vec2<u32> */
 const uint32_t* vmw_bricks(const vmw_world* w);   /* n_bricks x u32 */
 int vmw_generate(vmw_world* w, const vmw_recipe* r);
 int vmw_recipe_dense(const vmw_recipe* r, int32_t cx, int32_t cy, int32_t cz, uint16_t* dense);
+/* A chunk of level lod (voxels of 1 << lod blocks, lod <= 4) at chunk cell
+ * (cx, cy, cz) of that level, sampled from the recipe's heightfield: each
+ * voxel column takes the height at its first block, each voxel the layer
+ * block of its top block inside the terrain (no trees, no glass). */
+int vmw_recipe_dense_lod(const vmw_recipe* r, uint32_t lod, int32_t cx, int32_t cy, int32_t cz, uint16_t* dense);
 /* Every chunk of the recipe's world, chunk i = cx + nx (cy + ny cz) at
  * dense + i * 64^3 (the order vmw_generate inserts them in). */
 int vmw_recipe_dense_all(const vmw_recipe* r, uint16_t* dense);

@@ -1,4 +1,5 @@
-"""Builds the oracle (CPU restatement of the engine's march) as oracle/liboracle.so.
+"""Builds the oracle (CPU restatement of the engine's march and of its world
+producers) as oracle/liboracle.so.
 
 Test infrastructure: only tests/, __graft_entry__.smoke() and bench.py's CPU
 baseline leg load the result.  Compiled without FMA contraction
@@ -14,14 +15,15 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 LIB = HERE / "liboracle.so"
-SRC = HERE / "vm_oracle.cpp"
-DEPS = [SRC, ROOT / "voxelcraft_menu_b200" / "csrc" / "vm_types.h"]
+SRCS = [HERE / "vm_oracle.cpp", HERE / "producer.cpp"]
+DEPS = SRCS + [ROOT / "voxelcraft_menu_b200" / "csrc" / h for h in ("vm_types.h", "recipe.h")] + \
+    [ROOT / "include" / "voxmarch_world.h"]
 
 
 def build(force: bool = False) -> Path:
     if force or not LIB.exists() or any(d.stat().st_mtime > LIB.stat().st_mtime for d in DEPS):
         cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
-               "-mno-fma", f"-I{ROOT}", str(SRC), "-o", str(LIB)]
+               "-mno-fma", f"-I{ROOT}", *map(str, SRCS), "-o", str(LIB)]
         print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
     return LIB

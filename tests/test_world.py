@@ -1,14 +1,39 @@
-"""Layout producers: the C++ restatement of the engine's encoder and pools,
-checked with the reference's own fixtures and assertions (tests/tree.rs,
-tests/full_march.rs, tests/emitter_gate.rs, tests/pairs.rs, tests/camera.rs,
-tests/shadow_grid.rs)."""
+"""Layout producers, checked with the reference's own fixtures and assertions
+(tests/tree.rs, tests/full_march.rs, tests/emitter_gate.rs, tests/pairs.rs,
+tests/camera.rs, tests/shadow_grid.rs): the oracle's restatement of the
+engine's encoder, pools and chunk list (oracle/producer.cpp) and the
+product's world store (csrc/store.cpp) each pass them, and the two agree on
+every block, chunk record and grid cell."""
 import math
 
 import numpy as np
 import pytest
 
+from oracle.producer import OracleWorld
+from oracle import producer as OP
 from voxelcraft_menu_b200 import world as W
 from voxelcraft_menu_b200.world import Camera, World, dense_index
+
+PRODUCERS = {"product": World, "oracle": OracleWorld}
+
+
+@pytest.fixture(params=sorted(PRODUCERS))
+def producer(request):
+    return PRODUCERS[request.param]
+
+
+def l1_node(w, key, l1b):
+    """World::l1_node (src/voxel/world.rs:225-234) read through the packed
+    pools: (mask, run_ptr, leaf_prefix), or None when the cell is empty."""
+    rec = w.chunk_info(key)
+    root = rec.root[0] | (rec.root[1] << 32)
+    if not (root >> l1b) & 1:
+        return None
+    if rec.root[2] & 0x80000000:
+        return ((1 << 64) - 1, 0x80000000, l1b * 64)
+    inners, _, _ = w.pools()
+    n = inners[rec.root[2] + bin(root & ((1 << l1b) - 1)).count("1")]
+    return (int(n[0]) | (int(n[1]) << 32), int(n[2]), int(n[3]))
 
 X, Y, Z = np.meshgrid(np.arange(64, dtype=np.uint32), np.arange(64, dtype=np.uint32),
                       np.arange(64, dtype=np.uint32), indexing="ij")
@@ -67,19 +92,19 @@ def assert_pools_empty(w):
     assert s.used_words == 0
 
 
-def test_local_roundtrip():
+def test_local_roundtrip(producer):
     """tests/tree.rs:77-92"""
     d = dense_from(terrain(1))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
     assert w.chunk_info((0, 0, 0)).solid_count > 0
     assert world_matches(w, (0, 0, 0), d)
 
 
-def test_world_roundtrip_and_aabb():
+def test_world_roundtrip_and_aabb(producer):
     """tests/tree.rs:94-109"""
     d = dense_from(terrain(2))
-    w = World()
+    w = producer()
     w.insert_dense((3, 1, -2), d)
     assert world_matches(w, (3, 1, -2), d)
     rec = w.chunk_info((3, 1, -2))
@@ -92,10 +117,10 @@ def test_world_roundtrip_and_aabb():
     assert_pools_empty(w)
 
 
-def test_identical_chunks_share_runs():
+def test_identical_chunks_share_runs(producer):
     """tests/tree.rs:111-135"""
     d = dense_from(terrain(3))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
     s0 = w.pool_stats()
     assert s0.live_leaves > 0 and s0.live_inners > 0
@@ -112,10 +137,10 @@ def test_identical_chunks_share_runs():
     assert_pools_empty(w)
 
 
-def test_uniform_chunk_costs_nothing():
+def test_uniform_chunk_costs_nothing(producer):
     """tests/tree.rs:137-152"""
     d = dense_from(lambda x, y, z: np.full(x.shape, W.STONE))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
     rec = w.chunk_info((0, 0, 0))
     assert rec.root[2] & 0x80000000, "root must be full"
@@ -125,34 +150,34 @@ def test_uniform_chunk_costs_nothing():
     assert w.get_block(17, 33, 60) == W.STONE
 
 
-def test_empty_chunk():
+def test_empty_chunk(producer):
     """tests/tree.rs:154-157 (the insertion half; edits are not on the march path)"""
     d = dense_from(lambda x, y, z: np.zeros(x.shape))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
     rec = w.chunk_info((0, 0, 0))
     assert rec.root[0] == 0 and rec.root[1] == 0
     assert w.get_block(1, 2, 3) == W.AIR
 
 
-def test_many_block_types_attribute_recovery():
+def test_many_block_types_attribute_recovery(producer):
     """tests/tree.rs:231-246 (every palette width: up to 25 ids per leaf)"""
     d = dense_from(lambda x, y, z: np.where(y > 40, 0, 1 + (x * 7 + y * 3 + z * 5) % 25))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
     assert world_matches(w, (0, 0, 0), d)
     w.remove((0, 0, 0))
     assert_pools_empty(w)
 
 
-def test_water_line_packing_and_stratification():
+def test_water_line_packing_and_stratification(producer):
     """tests/tree.rs:281-314"""
     d = dense_from(lambda x, y, z: np.where(y <= 9, W.DIRT, np.where(y <= 12, W.WATER, W.AIR)))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
     rec = w.chunk_info((0, 0, 0))
     for l1b in range(64):
-        n = w.l1_node((0, 0, 0), l1b)
+        n = l1_node(w, (0, 0, 0), l1b)
         if n is None:
             continue
         _mask, run_ptr, prefix = n
@@ -166,12 +191,12 @@ def test_water_line_packing_and_stratification():
     assert rec.dry_mask != 0
 
 
-def test_water_only_cells_report_fifteen_and_leave_the_dry_mask():
+def test_water_only_cells_report_fifteen_and_leave_the_dry_mask(producer):
     """tests/tree.rs:316-345"""
     d = dense_from(lambda x, y, z: np.where(y <= 4, W.STONE, np.where(y <= 30, W.WATER, W.AIR)))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
-    nodes = [w.l1_node((0, 0, 0), b) for b in range(64)]
+    nodes = [l1_node(w, (0, 0, 0), b) for b in range(64)]
     nodes = [n for n in nodes if n is not None]
     water_only = sum(1 for m, rp, pre in nodes if pre >> 28 == 15 and not rp & 0x80000000)
     assert water_only == 16
@@ -185,11 +210,11 @@ def test_water_only_cells_report_fifteen_and_leave_the_dry_mask():
     assert bin(root_mask).count("1") == 32
 
 
-def test_full_mixed_root():
+def test_full_mixed_root(producer):
     """tests/full_march.rs:7-40: water above stone collapses to a full root whose
     dry mask holds exactly the bottom 32 cells."""
     d = dense_from(lambda x, y, z: np.where(y < 32, W.STONE, W.WATER))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
     rec = w.chunk_info((0, 0, 0))
     assert rec.root[2] & 0x80000000
@@ -198,16 +223,16 @@ def test_full_mixed_root():
     assert bin(rec.dry_mask).count("1") == 32
 
 
-def test_seabed_sets_its_line_and_open_sea_carries_fifteen():
+def test_seabed_sets_its_line_and_open_sea_carries_fifteen(producer):
     """tests/emitter_gate.rs:108-140"""
     d = dense_from(lambda x, y, z: np.where(y <= 8, W.STONE, np.where(y <= 40, W.WATER, W.AIR)))
-    w = World()
+    w = producer()
     w.insert_dense((0, 0, 0), d)
     rec = w.chunk_info((0, 0, 0))
     assert not rec.root[2] & 0x80000000
     for l1b in range(64):
         yn = (l1b >> 2) & 3
-        n = w.l1_node((0, 0, 0), l1b)
+        n = l1_node(w, (0, 0, 0), l1b)
         if yn == 0:
             assert n[2] >> 28 == 8
         elif yn == 3:

@@ -32,8 +32,8 @@ CU_SOURCES = ["kernels.cu", "pipeline.cu", "capi.cu", "gbuffer.cu", "shade.cu", 
 # The shading model is held to tolerances against FP64, not to bit equality
 # with the oracle, so it may contract a * b + c into fused multiply-adds.
 CU_EXTRA = {"shade.cu": ["--fmad=true"]}
-CPP_SOURCES = ["world.cpp"]
-HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "ray_stages.cuh", "shade.cuh", "world.h"]
+CPP_SOURCES = ["store.cpp"]
+HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "ray_stages.cuh", "shade.cuh", "store.h", "recipe.h"]
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:

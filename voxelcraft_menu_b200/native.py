@@ -180,7 +180,7 @@ _SIGNATURES = [
     ("vmw_remove", C.c_int, [vp, C.c_uint8, C.c_int32, C.c_int32, C.c_int32]),
     ("vmw_get_block", C.c_uint32, [vp, C.c_int32, C.c_int32, C.c_int32]),
     ("vmw_get_chunk_info", C.c_int, [vp, C.c_uint8, C.c_int32, C.c_int32, C.c_int32, P(VmwChunkInfo)]),
-    ("vmw_l1_node", C.c_int, [vp, C.c_uint8, C.c_int32, C.c_int32, C.c_int32, C.c_uint32, vp]),
+    ("vmw_set_fade", C.c_int, [vp, C.c_uint8, C.c_int32, C.c_int32, C.c_int32, C.c_float]),
     ("vmw_pool_stats", None, [vp, P(VmwPoolStats)]),
     ("vmw_inners", vp, [vp]),
     ("vmw_leaves", vp, [vp]),
@@ -188,6 +188,7 @@ _SIGNATURES = [
     ("vmw_generate", C.c_int, [vp, P(VmwRecipe)]),
     ("vmw_recipe_dense", C.c_int, [P(VmwRecipe), C.c_int32, C.c_int32, C.c_int32, vp]),
     ("vmw_recipe_dense_all", C.c_int, [P(VmwRecipe), vp]),
+    ("vmw_recipe_dense_lod", C.c_int, [P(VmwRecipe), C.c_uint32, C.c_int32, C.c_int32, C.c_int32, vp]),
     ("vmw_recipe_height", C.c_int32, [P(VmwRecipe), C.c_int32, C.c_int32]),
     ("vmw_camera_basis", None, [C.c_float, C.c_float, vp, vp, vp]),
     ("vmw_pairs_for", C.c_uint32, [C.c_uint32, C.c_uint32]),

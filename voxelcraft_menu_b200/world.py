@@ -1,8 +1,9 @@
 """Host-side world store and the synthetic workloads.
 
-`World` wraps the C++ restatement of the engine's encoder and pools
-(src/voxel/tree.rs, world.rs, geometry.rs, attributes.rs); `World.view()` is
-the engine's per-frame `build_chunk_list` plus the GpuFrame fill
+`World` wraps the library's world store (include/voxmarch_world.h): chunks
+encoded in the engine's tree format (build_local, src/voxel/tree.rs:89-204)
+and packed into the three pools the march reads; `World.view()` is the
+engine's per-frame `build_chunk_list` plus the GpuFrame fill
 (src/render/mod.rs:1447-1564, 1640-1707).
 """
 from __future__ import annotations
@@ -202,15 +203,11 @@ class World:
             return None
         return info
 
-    def l1_node(self, key: tuple, l1b: int, lod: int = 0):
-        """Inner node (mask u64, run_ptr, leaf_prefix) or None (src/voxel/world.rs:225)."""
-        out = np.zeros(4, np.uint32)
-        rc = self._L.vmw_l1_node(self._h, lod, key[0], key[1], key[2], l1b, ptr(out))
-        if rc < 0:
-            raise KeyError(key)
-        if rc == 0:
-            return None
-        return (int(out[0]) | (int(out[1]) << 32), int(out[2]), int(out[3]))
+    def set_fade(self, key: tuple, fade: float, lod: int = 0):
+        """The chunk's LOD cross-fade (RenderItem::fade, src/lod.rs:56-80)."""
+        rc = self._L.vmw_set_fade(self._h, lod, key[0], key[1], key[2], fade)
+        if rc:
+            raise KeyError(key) if rc == 1 else ValueError(fade)
 
     def pool_stats(self) -> VmwPoolStats:
         s = VmwPoolStats()
@@ -272,6 +269,63 @@ def recipe_dense_chunks(recipe: Recipe) -> np.ndarray:
     out = np.empty((n, 64 ** 3), np.uint16)
     if lib().vmw_recipe_dense_all(C.byref(recipe.c()), ptr(out)):
         raise RuntimeError("vmw_recipe_dense_all failed")
+    return out
+
+
+def recipe_mixed_lod() -> Recipe:
+    """512x128x512 terrain (the small world's noise, water and trees) for the
+    mixed level-of-detail layout."""
+    return Recipe(size=(512, 128, 512))
+
+
+def mixed_lod_layout():
+    """(lod, chunk cell, fade) of a world mixing the engine's LOD levels: lod-0
+    chunks over x, z in [0, 256), of which the 2x2x2 block over [128, 256)^2
+    fades in (0.6) over its fading-out lod-1 parent (-0.6); lod-1 chunks
+    (voxels of 2) over x in [256, 512), z in [0, 256); lod-2 chunks (voxels of
+    4) over z in [256, 512).  Chunk cells are in units of the level's chunk
+    size (64 << lod)."""
+    items = []
+    for cz in range(4):
+        for cy in range(2):
+            for cx in range(4):
+                fading = cx >= 2 and cz >= 2
+                items.append((0, (cx, cy, cz), 0.6 if fading else 1.0))
+    items.append((1, (1, 0, 1), -0.6))
+    for cz in range(2):
+        for cx in range(2, 4):
+            items.append((1, (cx, 0, cz), 1.0))
+    for cx in range(2):
+        items.append((2, (cx, 0, 1), 1.0))
+    return items
+
+
+def layout_dense(recipe: Recipe, lod: int, key: tuple) -> np.ndarray:
+    """Dense blocks of one chunk of a layout: the recipe's full-resolution
+    chunk for lod 0, its sampled coarse chunk otherwise."""
+    if lod == 0:
+        out = np.empty(64 ** 3, np.uint16)
+        if lib().vmw_recipe_dense(C.byref(recipe.c()), key[0], key[1], key[2], ptr(out)):
+            raise ValueError("vmw_recipe_dense failed")
+        return out
+    return recipe_dense_lod(recipe, lod, key)
+
+
+def build_layout(world, recipe: Recipe, layout) -> None:
+    """Insert every chunk of layout [(lod, key, fade)] into world and set its fade."""
+    for lod, key, fade in layout:
+        world.insert_dense(key, layout_dense(recipe, lod, key), lod=lod)
+    for lod, key, fade in layout:
+        if fade != 1.0:
+            world.set_fade(key, fade, lod=lod)
+    world.recipe = recipe
+
+
+def recipe_dense_lod(recipe: Recipe, lod: int, key: tuple) -> np.ndarray:
+    """The recipe's chunk of level lod at chunk cell key of that level (u16[64^3])."""
+    out = np.empty(64 ** 3, np.uint16)
+    if lib().vmw_recipe_dense_lod(C.byref(recipe.c()), lod, key[0], key[1], key[2], ptr(out)):
+        raise ValueError("vmw_recipe_dense_lod failed")
     return out
 
 
