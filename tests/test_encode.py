@@ -1,18 +1,33 @@
 """The dense -> 64-tree chunk encoder (build_local, src/voxel/tree.rs:89-204).
 
-CPU: the flat export of the CPU encoder (vmw_build_tree) inserted chunk by
-chunk (vmw_insert_tree) gives the same pools as World.generate; hand-made
-chunks cover the encoder's cases (empty, one id everywhere, full L1 nodes of
-mixed ids, water-only nodes and water lines, 64 distinct ids in a leaf,
-emitters, foliage, glass, palette overflow).  GPU: vm_encode_trees equals the
-CPU encoder field for field on those chunks and on every chunk of the
-256x128x256 and 1024x256x1024 terrains, and a world built from its output
-has the CPU world's pools."""
+The checker is the oracle's restatement of build_local (oracle/producer.cpp,
+orw_build_tree).  CPU: the product's host encoder (vmw_build_tree) equals it
+on hand-made chunks covering the encoder's cases (empty, one id everywhere,
+full L1 nodes of mixed ids, water-only nodes and water lines, 64 distinct ids
+in a leaf, emitters, foliage, glass, palette overflow), and its flat export
+inserted chunk by chunk (vmw_insert_tree) gives the same pools as
+World.generate.  GPU: vm_encode_trees equals the oracle field for field on
+those chunks and on every chunk of the 256x128x256 and 1024x256x1024
+terrains, and a world built from its output has World.generate's pools."""
 import numpy as np
 import pytest
 
+from oracle import producer as OP
 from voxelcraft_menu_b200 import encode as E
 from voxelcraft_menu_b200 import world as W
+
+
+def oracle_trees(dense, palette_cap):
+    """orw_build_tree of every chunk, in the Trees layout."""
+    out = E.empty(len(dense), palette_cap)
+    for i, d in enumerate(dense):
+        info, l1, leaves, attrs, pal = OP.build_tree(d, max(palette_cap, 1))
+        out.info[i] = info[0]
+        out.l1[i, :len(l1)] = l1
+        out.leaves[i, :len(leaves)] = leaves
+        out.attrs[i, :len(attrs)] = attrs
+        out.palette[i, :len(pal)] = pal
+    return out
 
 
 def dense_index(x, y, z):
@@ -75,6 +90,9 @@ def test_cpu_special_chunks():
     # the comparison used by the GPU tests: equal to itself, not to a neighbour
     assert all(E.same_chunk(t, i, t, i) for i in range(len(t)))
     assert not E.same_chunk(t, 2, t, 6)
+    # and the host encoder is the oracle's build_local
+    for cap in (1 << 18, 100):
+        assert_same_trees(E.cpu_build(d, cap), oracle_trees(d, cap))
 
 
 def gpu_trees(dense, palette_cap):
@@ -94,14 +112,21 @@ def assert_same_trees(g, c):
 def test_gpu_special_chunks():
     d = special_chunks()
     for cap in (1 << 18, 100):
-        assert_same_trees(gpu_trees(d, cap), E.cpu_build(d, cap))
+        assert_same_trees(gpu_trees(d, cap), oracle_trees(d, cap))
+
+
+@pytest.mark.gpu
+def test_gpu_lod_chunks():
+    rec = W.recipe_mixed_lod()
+    d = np.stack([W.recipe_dense_lod(rec, lod, key) for lod, key, _ in W.mixed_lod_layout() if lod > 0])
+    assert_same_trees(gpu_trees(d, 16384), oracle_trees(d, 16384))
 
 
 @pytest.mark.gpu
 def test_gpu_terrains_and_world(small_dense):
     rec = W.recipe_small_terrain()
     g = gpu_trees(small_dense, 16384)
-    assert_same_trees(g, E.cpu_build(small_dense, 16384))
+    assert_same_trees(g, oracle_trees(small_dense, 16384))
     w = W.World()
     nx, ny = rec.size[0] // 64, rec.size[1] // 64
     for i in range(len(g)):
@@ -109,4 +134,4 @@ def test_gpu_terrains_and_world(small_dense):
     for a, b in zip(w.pools(), W.World.generate(rec).pools()):
         assert np.array_equal(a, b)
     large = W.recipe_dense_chunks(W.recipe_large_terrain())
-    assert_same_trees(gpu_trees(large, 16384), E.cpu_build(large, 16384))
+    assert_same_trees(gpu_trees(large, 16384), oracle_trees(large, 16384))
