@@ -50,7 +50,8 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Grays/s at 1080p (primary + shadow rays)"
 UNIT = "Grays/s"
-WORKLOAD = "1920x1080 frame over the 1024x256x1024 terrain (1024 chunks), Hi-Z frame moved 0.5 voxel"
+WORKLOAD = ("1920x1080 frames over the 1024x256x1024 terrain (1024 chunks), camera moving 0.5 voxel per frame "
+            "(Hi-Z from the frame before)")
 
 
 def dist_env():
@@ -157,15 +158,28 @@ def peaks():
     return 6650.0, "fallback"
 
 
+FLAGS = 4 | 32 | 1     # FLAG_SHADOWS | FLAG_WATER_REFRACT | FLAG_HIZ
+
+
 def build_workload():
     from voxelcraft_menu_b200 import world as W
     rec = W.recipe_large_terrain()
     w = W.World.generate(rec)
     pools = w.pools()
-    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_HIZ
-    view_a = w.view(W.large_terrain_camera(rec, flags=flags))
-    view_b = w.view(W.large_terrain_camera(rec, flags=flags, dx=0.5))
+    view_a = w.view(W.large_terrain_camera(rec, flags=FLAGS))
+    view_b = w.view(W.large_terrain_camera(rec, flags=FLAGS, dx=0.5))
     return w, pools, view_a, view_b
+
+
+def mean_traffic(records):
+    """Field-wise mean of vm_render_counted records (lists element-wise)."""
+    out = {}
+    for k, v in records[0].items():
+        if isinstance(v, (list, tuple)):
+            out[k] = [float(np.mean([r[k][i] for r in records])) for i in range(len(v))]
+        else:
+            out[k] = float(np.mean([r[k] for r in records]))
+    return out
 
 
 def oracle_workload():
@@ -308,7 +322,7 @@ def bench_batched(local, steps, warmup):
     m.upload_world(*w.pools())
     m.batch_set(views)
     best = tuning.autotune_batch(m)
-    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"])
+    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"], best["packet"])
     traffic = m.batch_counted()
     rays = traffic["rays_primary"] + traffic["rays_shadow"]
 
@@ -417,7 +431,7 @@ def bench_sparse(local, fit_steps=50):
     m.upload_world(*w.pools())
     m.batch_set(frames[0])
     best = tuning.autotune_batch(m)
-    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"])
+    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"], best["packet"])
     total_ms, rays, prim, shad = 0.0, 0, 0, 0
     for views in frames:
         m.batch_set(views)
@@ -625,6 +639,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--warps", type=int, default=0, help="primary kernel warps per block (0: autotune)")
     ap.add_argument("--reg-level", type=int, default=0, help="primary kernel register level with --warps")
+    ap.add_argument("--packet", type=int, default=1, help="primary kernel pixels per lane with --warps")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched probe views")
     ap.add_argument("--no-shade", action="store_true", help="skip the shading forward / adjoint")
@@ -646,7 +661,9 @@ def main():
 
     from voxelcraft_menu_b200.march import Marcher
     from voxelcraft_menu_b200 import tuning
+    from voxelcraft_menu_b200 import world as W
 
+    rec = W.recipe_large_terrain()
     w, pools, va, vb = build_workload()
     m = Marcher(1920, 1080, device=local)
     # the library enqueues on torch's (non-default) current stream, so torch's
@@ -658,19 +675,43 @@ def main():
 
     # warps per block / register budget of the primary kernel: autotuned on this frame unless fixed
     if args.warps > 0:
-        best = {"warps": args.warps, "reg_level": args.reg_level, "ctas_per_sm": 0}
+        best = {"warps": args.warps, "reg_level": args.reg_level, "ctas_per_sm": 0, "packet": args.packet}
     else:
         best = tuning.autotune_single(m, vb, warm=va)
-    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"])
+    m.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"], best["packet"])
 
-    # frame A then the timed frame B (Hi-Z of A carried over)
+    # A moving camera: frame A at the centre, then one view per step, each 0.5
+    # voxel further along x (the first is frame B), so every timed frame's
+    # Hi-Z and primary cost order come from the frame before it, as in a
+    # renderer.  Each view's chunk list, grid and frame are uploaded from
+    # page-locked memory on the stream before the step's first event.
+    import ctypes as C
+    L = m._L
+    path = [vb] + [w.view(W.large_terrain_camera(rec, flags=FLAGS, dx=0.5 * (k + 2)))
+                   for k in range(args.warmup + args.steps - 1)]
+    pinned = [(torch.from_numpy(v.chunks.view(np.uint8).copy()).pin_memory(),
+               torch.from_numpy(v.grid.view(np.int32).copy()).pin_memory()) for v in path]
+
+    def put(c, k):
+        v, (ch, gr) = path[k], pinned[k]
+        c._ck(L.vm_upload_chunks(c._h, C.c_void_p(ch.data_ptr()), len(v.chunks), C.c_void_p(gr.data_ptr()),
+                                 v.grid.size))
+        c._ck(L.vm_set_frame(c._h, C.byref(v.frame)))
+
+    timed_views = range(args.warmup, args.warmup + args.steps)
+    counted = []
+    for k in timed_views:
+        put(m, k - 1)
+        m.render()
+        put(m, k)
+        counted.append(m.render_counted())
+    traffic = mean_traffic(counted)
     m.upload_view(va)
     m.render()
-    m.upload_view(vb)
-    traffic = m.render_counted()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)   # > 126 MB L2
 
-    for _ in range(args.warmup):
+    for k in range(args.warmup):
+        put(m, k)
         m.render()
     torch.cuda.synchronize(dev)
     # five events per step, recorded by the library between its stages (STAGES)
@@ -686,9 +727,11 @@ def main():
     torch.cuda.synchronize(dev)
     for i in range(args.steps):
         flush.zero_()
+        put(m, args.warmup + i)
         m.render_events([e.cuda_event for e in evs[i]])
     torch.cuda.synchronize(dev)
     clocks = sampler.stop()
+    m.upload_view(vb)
     ms = [row[0].elapsed_time(row[4]) for row in evs]
     stage_ms = {name: float(np.mean([row[i].elapsed_time(row[j]) for row in evs]))
                 for name, (i, j) in STAGES.items()}
@@ -710,8 +753,6 @@ def main():
     sh_h = torch.empty(npix, dtype=torch.float32).pin_memory()
     ch_h = torch.from_numpy(vb.chunks.view(np.uint8).copy()).pin_memory()
     gr_h = torch.from_numpy(vb.grid.view(np.int32).copy()).pin_memory()
-    import ctypes as C
-    L = m._L
 
     def e2e_step():
         m._ck(L.vm_upload_chunks(m._h, C.c_void_p(ch_h.data_ptr()), len(vb.chunks), C.c_void_p(gr_h.data_ptr()),
@@ -747,7 +788,7 @@ def main():
     # of the two streams' ends, over the steps.
     m2 = Marcher(1920, 1080, device=local)
     m2.upload_world(*pools)
-    m2.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"])
+    m2.set_tuning(best["warps"], best["reg_level"], best["ctas_per_sm"], best["packet"])
     m2.upload_view(va)
     m2.render()
     ctxs = (m, m2)
@@ -762,13 +803,9 @@ def main():
                 for _ in ctxs]
         read = L.vm_read_async_r16f if r16f else L.vm_read_async
 
-        def upload(c):
-            c._ck(L.vm_upload_chunks(c._h, C.c_void_p(ch_h.data_ptr()), len(vb.chunks), C.c_void_p(gr_h.data_ptr()),
-                                     vb.grid.size))
-            c._ck(L.vm_set_frame(c._h, C.byref(vb.frame)))
-
         def step(i):
-            # frame i on context i % 2, its inputs uploaded by the step before
+            # frame i (view i of the camera path) on context i % 2, its inputs
+            # uploaded by the step before
             c, other = ctxs[i % 2], ctxs[(i + 1) % 2]
             vh, shh = host[i % 2]
             # this frame's kernels start once the previous frame's are done
@@ -778,10 +815,10 @@ def main():
             c._ck(L.vm_render(c._h))
             # the next frame's inputs, enqueued ahead of this frame's
             # read-back so that the small upload does not queue behind it
-            upload(other)
+            put(other, (i + 1) % len(path))
             c._ck(read(c._h, C.c_void_p(vh.data_ptr()), C.c_void_p(shh.data_ptr())))
 
-        upload(ctxs[0])
+        put(ctxs[0], 0)
         for i in range(4):
             step(i)
         torch.cuda.synchronize(dev)
@@ -795,16 +832,22 @@ def main():
             e.record(st)
         torch.cuda.synchronize(dev)
         ms_ = max(start.elapsed_time(e) for e in ends) / args.steps
-        for vh, shh in host:
-            assert np.array_equal(vh.numpy().view(np.uint64), vis_h.numpy().view(np.uint64))
-            want = sh_h.numpy().astype(np.float16).view(np.int16) if r16f else sh_h.numpy()
+        # the last two frames read back equal those views rendered alone
+        last = 4 + args.steps - 1
+        for i in (last - 1, last):
+            m2.upload_view(path[i % len(path)])
+            m2.render()
+            vh, shh = host[i % 2]
+            assert np.array_equal(vh.numpy().view(np.uint64), m2.read_vis())
+            want = m2.read_shadow()
+            want = want.astype(np.float16).view(np.int16) if r16f else want
             assert np.array_equal(shh.numpy(), want)
         return max_over_ranks(ms_, world, dev)
 
     e2e_ms = e2e_two_contexts(True)
     e2e_f32_ms = e2e_two_contexts(False)
     m2.close()
-    h2d = vb.chunks.nbytes + vb.grid.nbytes + 352
+    h2d = int(np.mean([v.chunks.nbytes + v.grid.nbytes for v in path])) + 352
     d2h = npix * (8 + 2)       # vis keys + binary16 blocker distances
     d2h_f32 = npix * (8 + 4)
 

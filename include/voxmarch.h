@@ -113,6 +113,12 @@ int vm_render(vm_ctx* ctx);
  * 3 20 warps ~100 registers, 4 16 warps 128 registers) and resident blocks
  * per SM (0 = occupancy maximum). */
 int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_sm);
+/* Packet size of the same kernel: pixels each lane marches (1: a warp takes
+ * 8x4-pixel items, half an 8x8 tile; 2: whole 8x8 tiles, a lane starting its
+ * second pixel as soon as its first is done).  Output is identical; no
+ * counterpart in the engine, which runs one 64-thread group per (tile, chunk)
+ * pair (march.wgsl:1-55). */
+int vm_set_packet(vm_ctx* ctx, int pixels_per_lane);
 
 /* Read-backs (synchronise the context's stream). */
 int vm_read_vis(vm_ctx* ctx, uint64_t* out);                 /* res.x*res.y keys (common.wgsl:1324) */

@@ -80,12 +80,14 @@ def test_engine_passes_match_the_oracle(small):
     assert (vis != 0).mean() > 0.3 and (sh > 0).any() and ((sk >> 63) & 1).any()
 
 
-@pytest.mark.parametrize("warps,level,per_sm", [(4, 0, 0), (4, 1, 0), (4, 2, 1), (4, 3, 0), (8, 4, 0), (8, 0, 0), (8, 2, 0)])
-def test_pipeline_matches_the_oracle(small, warps, level, per_sm):
+@pytest.mark.parametrize("warps,level,per_sm,packet", [(4, 0, 0, 1), (4, 1, 0, 1), (4, 2, 1, 1), (4, 3, 0, 1),
+                                                        (8, 4, 0, 1), (8, 0, 0, 1), (8, 2, 0, 1), (4, 1, 0, 2),
+                                                        (4, 3, 4, 2), (8, 0, 0, 2)])
+def test_pipeline_matches_the_oracle(small, warps, level, per_sm, packet):
     w, pools, m = small
     v = w.view(W.small_terrain_camera())
     m.upload_view(v)
-    m.set_tuning(warps, level, per_sm)
+    m.set_tuning(warps, level, per_sm, packet)
     m.render()
     o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
     assert_same(m.read_vis(), vis, "vis")
@@ -165,10 +167,11 @@ def test_ragged_resolutions(small, res):
     m.upload_view(v)
     o, vis, hiz, ctr, sh, sk, st = oracle_all(v, pools)
     for warps in PRIMARY_WARPS:
-        m.set_tuning(warps)
-        m.render()
-        assert_same(m.read_vis(), vis, f"pipeline {warps} warps vis")
-        assert_same(m.read_shadow(), sh, f"pipeline {warps} warps shadow")
+        for packet in (1, 2):
+            m.set_tuning(warps, packet=packet)
+            m.render()
+            assert_same(m.read_vis(), vis, f"pipeline {warps} warps, packet {packet}: vis")
+            assert_same(m.read_shadow(), sh, f"pipeline {warps} warps, packet {packet}: shadow")
     m.set_tuning()
     m.render_passes()
     assert_same(m.read_vis(), vis, "passes vis")
@@ -370,6 +373,12 @@ def test_batch_matches_single_views(small):
     pv, ps = m.batch_read()
     assert_same(pv, bv, "per-view vs persistent vis")
     assert_same(ps, bs, "per-view vs persistent shadow")
+    m.set_tuning(8, 3, 0, 2)
+    m.batch_run()
+    qv, qs = m.batch_read()
+    m.set_tuning()
+    assert_same(qv, bv, "8x8-pixel items vs 8x4 vis")
+    assert_same(qs, bs, "8x8-pixel items vs 8x4 shadow")
     off = 0
     for v in views:
         n = v.n_pixels

@@ -58,7 +58,7 @@ struct vm_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   bool graph_secondary = false;   // the cached graph also traces the secondary rays
   // tuning of the primary kernel
-  vmk::PipeTuning tuning{4, 0, 0};
+  vmk::PipeTuning tuning{4, 0, 0, 1};
   std::string err_text;
 };
 
@@ -175,7 +175,6 @@ vmk::PipeArgs base_args(vm_ctx* ctx) {
   a.traffic = (vmk::Traffic64*)ctx->traffic.p;
   a.do_shadow = 1;
   a.do_secondary = 1;
-  a.px_per_lane = 1;
   return a;
 }
 
@@ -395,6 +394,15 @@ int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_
   ctx->tuning.primary_warps = warps_per_block;
   ctx->tuning.reg_level = reg_level;
   ctx->tuning.ctas_per_sm = ctas_per_sm;
+  return VM_OK;
+}
+
+int vm_set_packet(vm_ctx* ctx, int pixels_per_lane) {
+  if (!ctx) return VM_E_INVALID;
+  if (pixels_per_lane != 1 && pixels_per_lane != 2)
+    return fail(ctx, VM_E_INVALID, "pixels per lane must be 1 (8x4-pixel items) or 2 (8x8-pixel items)");
+  if (pixels_per_lane != ctx->tuning.px_per_lane) drop_graph(ctx);
+  ctx->tuning.px_per_lane = pixels_per_lane;
   return VM_OK;
 }
 

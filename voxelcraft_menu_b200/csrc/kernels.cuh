@@ -85,7 +85,6 @@ struct PipeArgs {
   uint32_t do_shadow, do_secondary;
   uint32_t do_reflect;         // with do_secondary: also queue the reflect leg of water hits
                                // (sec_q then holds up to 2 items per pixel)
-  uint32_t px_per_lane;        // primary work item: 1 -> 8x4 pixels, 2 -> 8x8 pixels per warp
   vm_frame frame0;
   ViewDesc view0;
 };
@@ -125,6 +124,7 @@ struct PipeTuning {
   int primary_warps;     // warps per block of the primary kernel (4, 8)
   int reg_level;         // register budget (resident warps per SM): 0 unconstrained, 1 24, 2 32, 3 20, 4 16
   int ctas_per_sm;       // resident blocks per SM of the persistent primary kernel; 0 = occupancy max
+  int px_per_lane;       // pixels per lane (1: 8x4-pixel items, 2: 8x8-pixel items)
 };
 // ev (optional): five events recorded at the start, after the cull, after the
 // primary, shadow and secondary kernels.

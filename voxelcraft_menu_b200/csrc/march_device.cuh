@@ -227,8 +227,11 @@ __device__ __forceinline__ bool grid_rel(const vm_frame& f, int32_t cx, int32_t 
   return true;
 }
 
-// world_block_at: common.wgsl:266-277
-static __device__ __noinline__ uint32_t world_block_at(const DevWorld& w, const vm_frame& f, F3 p) {
+// world_block_at: common.wgsl:266-277.  Inlined (as is cutout_march): an
+// out-of-line call made the march kernels save and restore their live
+// registers around it (a stack frame and spills), which cost more than the
+// larger body.
+static __device__ __forceinline__ uint32_t world_block_at(const DevWorld& w, const vm_frame& f, F3 p) {
   uint64_t gi;
   if (!grid_rel(f, ffloor_i(p.x * INV64), ffloor_i(p.y * INV64), ffloor_i(p.z * INV64), &gi)) return 0u;
   uint32_t ci = ld_grid(w, gi);
@@ -268,7 +271,7 @@ __device__ __forceinline__ void micro_entry(uint32_t ux, uint32_t uy, uint32_t u
 }
 
 // cutout_march: common.wgsl:537-577
-static __device__ __noinline__ bool cutout_march(int32_t wx, int32_t wy, int32_t wz, uint32_t ux, uint32_t uy, uint32_t uz,
+static __device__ __forceinline__ bool cutout_march(int32_t wx, int32_t wy, int32_t wz, uint32_t ux, uint32_t uy, uint32_t uz,
                                           F3 ro, F3 rd, F3 inv, float t_in, uint32_t axis_in, bool pdx, bool pdy,
                                           bool pdz, bool snap, float* t_out, uint32_t* n_out, uint32_t* m_out) {
   // inv is the ray's 1 / rd, the value the WGSL recomputes here
@@ -395,6 +398,22 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
   uint32_t leaf_cached = 0xFFFFFFFFu;
   uint2 leaf = make_uint2(0u, 0u);
   uint32_t attr = 0u;
+  // The leaf's attribute word is read the first time a solid voxel of the
+  // leaf needs its block id, not when the leaf is entered: most leaves a ray
+  // crosses yield no hit, and the read was a dependent load on every new
+  // leaf's critical path.  A pure read, so the results are unchanged.
+  uint32_t attr_slot = 0xFFFFFFFFu;   // attribute index of the leaf in hand
+  bool attr_have = false;
+  // A cell a march has already left without a hit, reached again: the step
+  // out of a cell that yields no hit depends on the cell alone (its masks
+  // decide the skip, its box the next t and axis; the water-repair and
+  // cutout tests either hit or skip 1), so the walk is then a cycle through
+  // the same cells with the same entry t and axis, no hit and no exit, until
+  // the 512-step cap ends it with no hit.  Marches that run past 64 steps
+  // (float rounding sends grazing rays back into a cell they left) keep a
+  // cell at steps 64, 128, 256 and stop with the cap's result when they come
+  // back to it: h.iters = MAX_ITERS + 1, hit false, as the cap gives.
+  int32_t kx = -1, ky = -1, kz = -1;
   for (;;) {
     h.iters += 1u;
     if (COUNT) tr->iters++;
@@ -434,8 +453,8 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
         solid = true;
         if (attr_needed && lfb != leaf_cached) {
           leaf_cached = lfb;
-          if (COUNT) tr->attr++;
-          attr = ld_brick(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + lfb);
+          attr_slot = (l1.w & 0x0FFFFFFFu) + lfb;
+          attr_have = false;
         }
       } else if (mask_has(l1.x, l1.y, lfb)) {
         if (lfb != leaf_cached) {
@@ -443,10 +462,8 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
           const uint32_t li = mask_below(l1.x, l1.y, lfb);
           if (COUNT) tr->leaf++;
           leaf = ld_leaf(w, (uint64_t)(l1.z & VM_PTR_MASK) + li);
-          if (attr_needed) {
-            if (COUNT) tr->attr++;
-            attr = ld_brick(w, (uint64_t)c.attr_base + (l1.w & 0x0FFFFFFFu) + li);
-          }
+          attr_slot = (l1.w & 0x0FFFFFFFu) + li;
+          attr_have = false;
         }
         const uint32_t vb = cell_bit(ux & 3u, uy & 3u, uz & 3u);
         if (mask_has(leaf.x, leaf.y, vb)) solid = true;
@@ -463,6 +480,11 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
     if (solid && any_filter) {
       const bool need_id = !attr_uniform && (noncaster_aware || water_interface || water_aware || glass_aware ||
                                              foliage_aware || cutout_aware);
+      if (attr_needed && !attr_have) {
+        if (COUNT) tr->attr++;
+        attr = ld_brick(w, (uint64_t)c.attr_base + attr_slot);
+        attr_have = true;
+      }
       if (need_id) {
         if (COUNT && (attr & VM_UNIFORM_BIT) == 0u) tr->pal++;
         id = leaf_block(w, attr, ux, uy, uz);
@@ -515,6 +537,10 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
         h.id = id;
       }
       return h;
+    }
+    if (h.iters >= 64u) {
+      if (cx == kx && cy == ky && cz == kz) { h.iters = VM_MAX_ITERS + 1u; break; }
+      if ((h.iters & (h.iters - 1u)) == 0u) { kx = cx; ky = cy; kz = cz; }
     }
     const int32_t bx0 = cx - (cx & (skip - 1)), by0 = cy - (cy & (skip - 1)), bz0 = cz - (cz & (skip - 1));
     const float bndx = (float)(pdx ? bx0 + skip : bx0);

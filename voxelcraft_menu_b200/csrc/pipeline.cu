@@ -449,10 +449,24 @@ __device__ __noinline__ void enqueue_reflect(const PipeArgs& a, uint32_t v, uint
 // the autotuner's occupancy knob.
 // REFL: the frame may trace reflect legs (a.do_reflect); without it the
 // kernel carries none of that code.  SINGLE: the launch has one view.
-template <int NW, int MINB, bool UNDERWATER, bool COUNT, bool REFL, bool SINGLE>
+// PX: pixels per lane (the packet).  A warp's item is 8 x 4 PX pixels of one
+// 8x8 tile: PX = 1 half a tile, PX = 2 the whole tile.  A lane walks its PX
+// pixels one after the other and starts its next pixel as soon as one is
+// done, so lanes whose rays end early do not idle until the warp's slowest
+// ray ends; the pixels' results are then finished together.
+template <int NW, int MINB, bool UNDERWATER, bool COUNT, bool REFL, bool SINGLE, int PX>
 __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant__ PipeArgs a) {
+  static_assert(PX == 1 || PX == 2, "one or two pixels per lane");
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t total = a.total_tiles * 2u;
+  const uint32_t total = a.total_tiles * (2u / PX);
+  // Every lane walks the same tile list: the warp stages the item's first 32
+  // entries and their depth bounds in shared memory with one load per lane,
+  // so a lane's walk reads them there instead of chaining a list load, a
+  // bounds load and only then the chunk record through global memory.
+  __shared__ uint32_t s_ci[NW][32], s_dk[NW][32], s_suf[NW][32];
+  uint32_t* my_ci = s_ci[threadIdx.x >> 5];
+  uint32_t* my_dk = s_dk[threadIdx.x >> 5];
+  uint32_t* my_suf = s_suf[threadIdx.x >> 5];
   Traffic tr = {};
   uint32_t np = 0, ns = 0, nx = 0;
   for (;;) {
@@ -461,55 +475,91 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
     item = __shfl_sync(FULLMASK, item, 0);
     if (item >= total) break;
     const long long clk0 = clock64();
-    const uint32_t t = a.tile_order[item >> 1], half = item & 1u;
+    const uint32_t t = PX == 1 ? a.tile_order[item >> 1] : a.tile_order[item];
+    const uint32_t half0 = PX == 1 ? (item & 1u) : 0u;
     const uint32_t v = find_view_t<SINGLE>(a, t);
     const vm_frame& f = frame_t<SINGLE>(a, v);
     const ViewDesc vd = view_t<SINGLE>(a, v);
     const DevWorld w = world_of(a, vd);
     const uint32_t local = t - vd.tile_begin;
     const uint32_t tx = local % vd.tiles_x, ty = local / vd.tiles_x;
-    const uint32_t px = tx * 8u + (lane & 7u), py = ty * 8u + half * 4u + (lane >> 3);
-    const bool valid = px < f.res[0] && py < f.res[1];
+    const uint32_t px = tx * 8u + (lane & 7u), py0 = ty * 8u + half0 * 4u + (lane >> 3);
     const uint32_t n = a.tile_count[t];
     const uint32_t m = min(n, a.list_cap);
     const uint16_t* list = a.tile_list + (uint64_t)t * a.list_cap;
     const uint32_t* dk = a.dkmax + vd.chunk_off;
     const uint32_t* suf = a.sufmax + vd.chunk_off;
+    __syncwarp();   // the previous item's reads of the staged entries are done
+    if (lane < m) {
+      const uint32_t c0 = list[lane];
+      my_ci[lane] = c0; my_dk[lane] = dk[c0]; my_suf[lane] = suf[c0];
+    }
+    __syncwarp();
     const F3 cam = ld3(f.cam_pos);
-    const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
-    const Ray ray = make_ray(cam, rd);
+    // the lane's current pixel (slot k of its PX) and its walk
+    uint32_t k = 0, py = py0, i = 0;
+    bool valid = px < f.res[0] && py < f.res[1];
+    F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+    Ray ray = make_ray(cam, rd);
     unsigned long long best = 0ull;
     uint32_t best_id = 0u;
     bool active = valid;
+    // slot 0's result once the lane has moved on to slot 1 (PX == 2)
+    unsigned long long best0 = 0ull;
+    uint32_t best_id0 = 0u;
+    bool active0 = false;
     // Each lane walks its list in order with the same tests as ever; the
     // entries a lane skips (a closer key already found) are passed in an
     // inner loop, so that every round of the warp is one chunk march for
     // each lane that still has one.
-    for (uint32_t i = 0;;) {
+    for (;;) {
       uint32_t ci = 0;
       bool go = false;
-      while (active && i < m) {
-        ci = list[i];
-        const uint32_t bestd = (uint32_t)(best >> 40);
-        if (suf[ci] < bestd) { active = false; break; }
-        ++i;
-        if (dk[ci] < bestd) continue;
-        go = true;
-        break;
+      for (;;) {
+        while (active && i < m) {
+          uint32_t sv, dv;
+          if (i < 32u) { ci = my_ci[i]; sv = my_suf[i]; dv = my_dk[i]; }
+          else { ci = list[i]; sv = suf[ci]; dv = dk[ci]; }
+          const uint32_t bestd = (uint32_t)(best >> 40);
+          if (sv < bestd) { active = false; break; }
+          ++i;
+          if (dv < bestd) continue;
+          go = true;
+          break;
+        }
+        if (go || PX == 1 || k + 1u >= (uint32_t)PX) break;
+        // this pixel's walk is over: keep its result, start the next pixel
+        best0 = best; best_id0 = best_id; active0 = active;
+        ++k;
+        py += 4u;
+        valid = px < f.res[0] && py < f.res[1];
+        rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+        ray = make_ray(cam, rd);
+        best = 0ull; best_id = 0u; active = valid; i = 0;
       }
       if (!__any_sync(FULLMASK, go)) break;
       if (go) march_entry<UNDERWATER, COUNT>(w, f, ray, ci, px, py, best, best_id, &tr);
     }
+#pragma unroll
+    for (uint32_t slot = 0; slot < (uint32_t)PX; ++slot) {
+    // finish the lane's pixel of this slot (the last one's walk state is live)
+    const bool last = slot + 1u == (uint32_t)PX;
+    unsigned long long pbest = last ? best : best0;
+    uint32_t pbest_id = last ? best_id : best_id0;
+    const bool pactive = last ? active : active0;
+    const uint32_t ppy = py0 + 4u * slot;
+    const bool pvalid = px < f.res[0] && ppy < f.res[1];
+    const F3 prd = last ? rd : ray_dir(f, (float)px + 0.5f, (float)ppy + 0.5f);
     if (n > a.list_cap)
-      march_overflow<UNDERWATER, COUNT>(w, f, ray, (uint32_t)list[a.list_cap - 1] + 1u, tx, ty, px, py, dk, suf,
-                                        active, &best, &best_id, &tr);
-    const uint64_t pix = (uint64_t)py * f.res[0] + px;
-    if (valid) a.vis[vd.pix_off + pix] = best;
-    if (COUNT && valid) ++np;
+      march_overflow<UNDERWATER, COUNT>(w, f, last ? ray : make_ray(cam, prd), (uint32_t)list[a.list_cap - 1] + 1u,
+                                        tx, ty, px, ppy, dk, suf, pactive, &pbest, &pbest_id, &tr);
+    const uint64_t pix = (uint64_t)ppy * f.res[0] + px;
+    if (pvalid) a.vis[vd.pix_off + pix] = pbest;
+    if (COUNT && pvalid) ++np;
     {
       // build_hiz (march.wgsl:57-76) on the final visibility: pixels outside
       // the frame count as misses
-      const uint32_t d = __reduce_min_sync(FULLMASK, valid ? (uint32_t)(best >> 40) : 0u);
+      const uint32_t d = __reduce_min_sync(FULLMASK, pvalid ? (uint32_t)(pbest >> 40) : 0u);
       if (lane == 0) atomicMin(&a.hiz[vd.tile_begin + local], d);
     }
     // The hit shared by shadow_guide (shadow.wgsl:8-30) and the water / glass
@@ -518,15 +568,15 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
     F3 so = {0.0f, 0.0f, 0.0f};
     SecRay sr;
 
-    if (valid && best != 0ull) {
-      const KeyParts k = split_key(best);
+    if (pvalid && pbest != 0ull) {
+      const KeyParts k = split_key(pbest);
       const Chunk c = ld_chunk(w, k.ci);
-      const float th = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
-      const F3 hit = cam + rd * th;
-      const bool water = best_id == VM_WATER, glass = best_id == VM_GLASS;
+      const float th = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, prd);
+      const F3 hit = cam + prd * th;
+      const bool water = pbest_id == VM_WATER, glass = pbest_id == VM_GLASS;
       if (a.do_shadow && shadow_active(f) && !water && !glass) {
         F3 nrm = normal_of(k.nid);
-        if (k.nid >= VM_NORMAL_CROSS_A && dot(nrm, rd) > 0.0f) nrm = neg(nrm);
+        if (k.nid >= VM_NORMAL_CROSS_A && dot(nrm, prd) > 0.0f) nrm = neg(nrm);
         if (!(dot(nrm, ld3(f.sun_dir)) <= 0.0f) && th >= 0.0f) {
           so = hit + nrm * (0.02f * c.vs);
           want_sh = true;
@@ -535,7 +585,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
       if (a.do_secondary && water) {
         const float detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, th);
         if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && detail > 0.0f) {
-          const F3 rdir = refract(rd, normal_of(k.nid), 1.0f / VM_WATER_IOR);
+          const F3 rdir = refract(prd, normal_of(k.nid), 1.0f / VM_WATER_IOR);
           sr.o = hit + rdir * VM_SURFACE_EPS;
           sr.d = rdir;
           sr.max_dist = VM_WATER_REFRACT_DIST;
@@ -543,15 +593,15 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
           want_sec = true;
         }
       } else if (a.do_secondary && glass) {
-        sr.o = hit + rd * VM_SURFACE_EPS;
-        sr.d = rd;
+        sr.o = hit + prd * VM_SURFACE_EPS;
+        sr.d = prd;
         sr.max_dist = fmaxf(VM_GLASS_TRANSMIT_DIST, f.far_);
         sr.water = false;
         want_sec = true;
       }
     }
     if (a.do_shadow) {
-      if (valid && !want_sh) a.shadow[vd.pix_off + pix] = 0.0f;
+      if (pvalid && !want_sh) a.shadow[vd.pix_off + pix] = 0.0f;
       const uint32_t bal = __ballot_sync(FULLMASK, want_sh);
       if (bal) {
         uint32_t b0 = 0;
@@ -564,7 +614,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
       }
     }
     if (a.do_secondary) {
-      if (valid && !want_sec) { a.sec_key[vd.pix_off + pix] = 0ull; a.sec_t[vd.pix_off + pix] = 0.0f; }
+      if (pvalid && !want_sec) { a.sec_key[vd.pix_off + pix] = 0ull; a.sec_t[vd.pix_off + pix] = 0.0f; }
       const uint32_t bal = __ballot_sync(FULLMASK, want_sec);
       if (bal) {
         uint32_t b0 = 0;
@@ -580,8 +630,13 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
       }
     }
     if (REFL && a.do_reflect)
-      enqueue_reflect(a, v, px, py, vd.pix_off + pix, valid, valid && best_id == VM_WATER ? best : 0ull);
-    if (lane == 0) a.item_cost[2u * t + half] = (uint32_t)min(clock64() - clk0, 0xFFFFFFFFll);
+      enqueue_reflect(a, v, px, ppy, vd.pix_off + pix, pvalid, pvalid && pbest_id == VM_WATER ? pbest : 0ull);
+    }
+    if (lane == 0) {
+      const uint32_t cost = (uint32_t)min(clock64() - clk0, 0xFFFFFFFFll);
+      if (PX == 1) a.item_cost[2u * t + half0] = cost;
+      else a.item_cost[2u * t] = a.item_cost[2u * t + 1u] = cost;
+    }
   }
   flush_traffic<COUNT>(a, 0, tr, np, ns, nx);
 }
@@ -736,40 +791,47 @@ struct MinBlocks {
   static constexpr int value = LEVEL == 0 ? 1 : warps / NW;
 };
 
-template <int NW, int LEVEL, bool UW>
+template <int NW, int LEVEL, bool UW, int PX>
 static void* primary_fn(bool refl, bool single) {
   constexpr int MB = MinBlocks<NW, LEVEL>::value;
-  if (!single) return (void*)k_primary<NW, MB, UW, false, false, false>;   // batches trace no reflect legs
-  return refl ? (void*)k_primary<NW, MB, UW, false, true, true> : (void*)k_primary<NW, MB, UW, false, false, true>;
+  if (!single) return (void*)k_primary<NW, MB, UW, false, false, false, PX>;   // batches trace no reflect legs
+  return refl ? (void*)k_primary<NW, MB, UW, false, true, true, PX> : (void*)k_primary<NW, MB, UW, false, false, true, PX>;
 }
 
-template <int NW>
+template <int NW, int PX>
 static void* primary_nw(int level, bool uw, bool refl, bool single) {
   switch (level) {
-    case 0: return uw ? primary_fn<NW, 0, true>(refl, single) : primary_fn<NW, 0, false>(refl, single);
-    case 1: return uw ? primary_fn<NW, 1, true>(refl, single) : primary_fn<NW, 1, false>(refl, single);
-    case 2: return uw ? primary_fn<NW, 2, true>(refl, single) : primary_fn<NW, 2, false>(refl, single);
-    case 3: return uw ? primary_fn<NW, 3, true>(refl, single) : primary_fn<NW, 3, false>(refl, single);
-    case 4: return uw ? primary_fn<NW, 4, true>(refl, single) : primary_fn<NW, 4, false>(refl, single);
+    case 0: return uw ? primary_fn<NW, 0, true, PX>(refl, single) : primary_fn<NW, 0, false, PX>(refl, single);
+    case 1: return uw ? primary_fn<NW, 1, true, PX>(refl, single) : primary_fn<NW, 1, false, PX>(refl, single);
+    case 2: return uw ? primary_fn<NW, 2, true, PX>(refl, single) : primary_fn<NW, 2, false, PX>(refl, single);
+    case 3: return uw ? primary_fn<NW, 3, true, PX>(refl, single) : primary_fn<NW, 3, false, PX>(refl, single);
+    case 4: return uw ? primary_fn<NW, 4, true, PX>(refl, single) : primary_fn<NW, 4, false, PX>(refl, single);
   }
   return nullptr;
 }
 
-// the counting run is never timed: 4 warps, unconstrained registers, the
-// reflect code behind its runtime flag
+// the counting run is never timed: 4 warps, unconstrained registers, one
+// pixel per lane, the reflect code behind its runtime flag
 static void* primary_count(bool uw, bool single) {
-  if (single) return uw ? (void*)k_primary<4, 1, true, true, true, true> : (void*)k_primary<4, 1, false, true, true, true>;
-  return uw ? (void*)k_primary<4, 1, true, true, false, false> : (void*)k_primary<4, 1, false, true, false, false>;
+  if (single)
+    return uw ? (void*)k_primary<4, 1, true, true, true, true, 1> : (void*)k_primary<4, 1, false, true, true, true, 1>;
+  return uw ? (void*)k_primary<4, 1, true, true, false, false, 1> : (void*)k_primary<4, 1, false, true, false, false, 1>;
 }
 
 static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt, bool refl, bool single) {
   if (cnt) return primary_count(uw, single);
-  switch (t.primary_warps) {
-    case 4: return primary_nw<4>(t.reg_level, uw, refl, single);
-    case 8: return primary_nw<8>(t.reg_level, uw, refl, single);
+  const int px = t.px_per_lane == 2 ? 2 : 1;
+  switch (t.primary_warps * 4 + px) {
+    case 4 * 4 + 1: return primary_nw<4, 1>(t.reg_level, uw, refl, single);
+    case 4 * 4 + 2: return primary_nw<4, 2>(t.reg_level, uw, refl, single);
+    case 8 * 4 + 1: return primary_nw<8, 1>(t.reg_level, uw, refl, single);
+    case 8 * 4 + 2: return primary_nw<8, 2>(t.reg_level, uw, refl, single);
   }
   return nullptr;
 }
+
+// pixels per lane of the primary kernel a launch runs
+static int packet_of(const PipeTuning& t, bool cnt) { return cnt ? 1 : (t.px_per_lane == 2 ? 2 : 1); }
 
 static int block_warps(const PipeTuning& t, bool cnt) { return cnt ? 4 : t.primary_warps; }
 
@@ -838,7 +900,7 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   int per = t.ctas_per_sm > 0 && !count ? t.ctas_per_sm
                                         : primary_max_ctas_per_sm(t, underwater, count, refl, single);
   if (per <= 0) per = 1;
-  const uint32_t items_blocks = (a.total_tiles * 2u + nw - 1) / nw;
+  const uint32_t items_blocks = (a.total_tiles * (2u / (uint32_t)packet_of(t, count)) + nw - 1) / nw;
   const uint32_t grid = std::min<uint32_t>((uint32_t)sms * (uint32_t)per, items_blocks);
   void* args[] = {(void*)&a};
   if ((e = cudaLaunchKernel(fn, dim3(grid), dim3(nw * 32), args, 0, s)) != cudaSuccess) return e;

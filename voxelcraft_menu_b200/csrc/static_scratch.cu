@@ -140,7 +140,7 @@ extern "C" int vm_render_static(const vm_frame* frame, const vm_chunk* d_chunks,
   a.do_secondary = 0;
   a.frame0 = f;
   a.view0 = v;
-  const vmk::PipeTuning t{4, 1, 0};
+  const vmk::PipeTuning t{4, 1, 0, 1};
   const cudaError_t e = vmk::launch_pipeline(a, t, (f.flags & VM_FLAG_UNDERWATER) != 0u, false, sms,
                                              static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return fail(VM_E_CUDA, cudaGetErrorString(e));

@@ -24,6 +24,7 @@ STATUS = {0: "VM_OK", 1: "VM_E_INVALID", 2: "VM_E_CAPACITY", 3: "VM_E_TILE_OVERF
 # warps per block and register levels of the persistent primary-ray kernel (vm_set_tuning)
 PRIMARY_WARPS = (4, 8)
 REG_LEVELS = (0, 1, 2, 3, 4)
+PACKETS = (1, 2)
 
 
 class MarchError(RuntimeError):
@@ -95,12 +96,13 @@ class Marcher:
     def set_frame(self, frame: VmFrame):
         self._ck(self._L.vm_set_frame(self._h, C.byref(frame)))
 
-    def set_tuning(self, warps: int = 4, reg_level: int = 0, ctas_per_sm: int = 0):
+    def set_tuning(self, warps: int = 4, reg_level: int = 0, ctas_per_sm: int = 0, packet: int = 1):
         """Warps per block (4, 8), register budget (resident warps per SM the
-        allocation must allow: 0 unconstrained, 1 24, 2 32, 3 20, 4 16) and
-        resident blocks per SM (0 = occupancy maximum) of the persistent
-        primary-ray kernel."""
+        allocation must allow: 0 unconstrained, 1 24, 2 32, 3 20, 4 16),
+        resident blocks per SM (0 = occupancy maximum) and pixels per lane
+        (1: 8x4-pixel items, 2: 8x8) of the persistent primary-ray kernel."""
         self._ck(self._L.vm_set_tuning(self._h, warps, reg_level, ctas_per_sm))
+        self._ck(self._L.vm_set_packet(self._h, packet))
 
     # -- the engine's passes ------------------------------------------------------
     def select(self):

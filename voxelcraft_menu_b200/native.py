@@ -141,6 +141,7 @@ _SIGNATURES = [
     ("vm_soften_shadows", C.c_int, [vp, C.c_uint32, C.c_float]),
     ("vm_render", C.c_int, [vp]),
     ("vm_set_tuning", C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+    ("vm_set_packet", C.c_int, [vp, C.c_int]),
     ("vm_read_vis", C.c_int, [vp, vp]),
     ("vm_read_hiz", C.c_int, [vp, vp]),
     ("vm_write_hiz", C.c_int, [vp, vp]),
