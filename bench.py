@@ -161,6 +161,28 @@ def peaks():
 FLAGS = 4 | 32 | 1     # FLAG_SHADOWS | FLAG_WATER_REFRACT | FLAG_HIZ
 
 
+def l2_copy_gbs(dev, mb: int = 24, reps: int = 50) -> float:
+    """Measured L2 bandwidth: a device copy between two mb-MB buffers that
+    both stay in the 126 MB L2 (read + write bytes over CUDA-event time, best
+    of five runs of reps copies, after a warm-up)."""
+    import torch
+    a = torch.empty(mb << 20, dtype=torch.uint8, device=dev)
+    b = torch.empty_like(a)
+    for _ in range(10):
+        b.copy_(a)
+    best = 0.0
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            b.copy_(a)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        best = max(best, 2 * a.numel() * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9)
+    return best
+
+
 def build_workload():
     from voxelcraft_menu_b200 import world as W
     rec = W.recipe_large_terrain()
@@ -857,6 +879,7 @@ def main():
     top = max(sbytes, key=lambda k: stage_ms[k])
     peak, peak_kind = peaks()
     achieved = sbytes[top] / (stage_ms[top] * 1e-3) / 1e9
+    l2_peak = l2_copy_gbs(dev)
     stats = m.stats()
     m.close()
     extra = {}
@@ -889,7 +912,10 @@ def main():
                          "threads_per_instruction_ncu": profile_row(top, "threads per executed instruction (of 32)"),
                          "algorithmic_bytes_per_launch": sbytes[top], "launch_ms": stage_ms[top],
                          "dda_steps_per_launch": stage_iters(traffic, top),
-                         "bytes_per_dda_step": sbytes[top] / max(stage_iters(traffic, top), 1)},
+                         "bytes_per_dda_step": sbytes[top] / max(stage_iters(traffic, top), 1),
+                         "l2": {"achieved": achieved, "peak": l2_peak, "unit": "GB/s", "frac": achieved / l2_peak,
+                                "peak_kind": "measured here: device copy between two 24 MB buffers resident in L2",
+                                "note": "the bound the tree pools (L2-resident) would set"}},
             "e2e": {"value": job_value(world, rays, e2e_ms), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                     "method": "two contexts alternate; every step renders once the other context's last render is "

@@ -119,6 +119,14 @@ int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_
  * counterpart in the engine, which runs one 64-thread group per (tile, chunk)
  * pair (march.wgsl:1-55). */
 int vm_set_packet(vm_ctx* ctx, int pixels_per_lane);
+/* The engine's pipeline specialisations of the march (make_spec,
+ * src/render/mod.rs:2355-2689): VM_SPEC_* bits (vm_types.h), VM_SPEC_DEFAULT
+ * on creation.  They select the full-root shortcut (--no-full-march), the
+ * water-interface repair (--legacy-water), leaf cutouts (--no-leaf-cutout),
+ * glass as its own surface, emitters without sun shadow, tufts as foliage, the
+ * Snell bend of underwater primary rays (--snell-bend) and the leaf fill
+ * (--no-leaf-thin).  Unknown bits: VM_E_INVALID. */
+int vm_set_spec(vm_ctx* ctx, uint32_t spec);
 
 /* Read-backs (synchronise the context's stream). */
 int vm_read_vis(vm_ctx* ctx, uint64_t* out);                 /* res.x*res.y keys (common.wgsl:1324) */

@@ -21,7 +21,14 @@ vp = C.c_void_p
 class OrWorld(C.Structure):
     _fields_ = [("frame", vp), ("chunks", vp), ("n_chunks", C.c_uint32), ("inners", vp), ("n_inners", C.c_uint64),
                 ("leaves", vp), ("n_leaves", C.c_uint64), ("bricks", vp), ("n_bricks", C.c_uint64), ("grid", vp),
-                ("n_grid", C.c_uint64)]
+                ("n_grid", C.c_uint64), ("spec", C.c_uint32)]
+
+
+# pipeline specialisations (VM_SPEC_* of vm_types.h; the engine's make_spec, src/render/mod.rs:2355-2689)
+SPEC_FULL_MARCH, SPEC_WATER_REPAIR, SPEC_LEAF_CUTOUT, SPEC_GLASS = 1, 2, 4, 8
+SPEC_EMITTER_GATHER, SPEC_FOLIAGE, SPEC_SNELL_BEND, SPEC_LEAF_THIN = 16, 32, 64, 128
+SPEC_DEFAULT = SPEC_FULL_MARCH | SPEC_WATER_REPAIR | SPEC_LEAF_CUTOUT | SPEC_GLASS | SPEC_EMITTER_GATHER | \
+    SPEC_FOLIAGE | SPEC_LEAF_THIN
 
 
 class OrHit(C.Structure):
@@ -84,7 +91,7 @@ def _p(a):
 class Oracle:
     """The oracle bound to one view (frame + chunk list + grid) and the pools."""
 
-    def __init__(self, view, inners, leaves, bricks, threads: int = 0):
+    def __init__(self, view, inners, leaves, bricks, threads: int = 0, spec: int = SPEC_DEFAULT):
         self.L = lib()
         self.view = view
         self.frame = view.frame
@@ -93,7 +100,7 @@ class Oracle:
                       np.ascontiguousarray(view.grid, np.uint32)]
         ch, i, l, b, g = self._keep
         self.w = OrWorld(C.cast(C.pointer(self.frame), vp), _p(ch), len(ch), _p(i), i.size // 4, _p(l), l.size // 2,
-                         _p(b), b.size, _p(g), g.size)
+                         _p(b), b.size, _p(g), g.size, spec)
         self.threads = threads
         self.L.or_clear_error()
 

@@ -94,6 +94,7 @@ inline V3 ld3(const float* p) { return {p[0], p[1], p[2]}; }
 
 // ----------------------------------------------------------------------------
 struct World {
+  uint32_t spec = VM_SPEC_DEFAULT;   // pipeline specialisations (VM_SPEC_*)
   const vm_frame* f;
   const vm_chunk* chunks; uint32_t n_chunks;
   const uint32_t* inners; uint64_t n_inners;   // count of vec4<u32>
@@ -318,13 +319,13 @@ V3 soft_sun_dir(const vm_frame& f, uint32_t px, uint32_t py, uint32_t s) {
 }
 
 // leaf_solid: common.wgsl:514-518
-bool leaf_solid(I3 wv, U3 m) {
+bool leaf_solid(I3 wv, U3 m, float fill = VM_LEAF_FILL) {
   int32_t qx = (int32_t)((uint32_t)wv.x * 4u + m.x);
   int32_t qy = (int32_t)((uint32_t)wv.y * 4u + m.y);
   int32_t qz = (int32_t)((uint32_t)wv.z * 4u + m.z);
   uint32_t h = hash_u32(((uint32_t)qx * 73856093u) ^ ((uint32_t)qy * 19349663u) ^
                         ((uint32_t)qz * 83492791u));
-  return (float)(h >> 8u) * (1.0f / 16777216.0f) < VM_LEAF_FILL;
+  return (float)(h >> 8u) * (1.0f / 16777216.0f) < fill;
 }
 
 // micro_entry: common.wgsl:520-528
@@ -340,7 +341,7 @@ struct MicroHit { bool hit; float t; uint32_t normal; U3 micro; };
 
 // cutout_march: common.wgsl:537-577
 MicroHit cutout_march(I3 wv, U3 uc, V3 ro, V3 rd, float t_in, uint32_t axis_in,
-                      const bool* pos_dir, bool snap) {
+                      const bool* pos_dir, bool snap, float fill) {
   MicroHit r{false, t_in, 0u, {0u, 0u, 0u}};
   V3 base = v3((float)uc.x, (float)uc.y, (float)uc.z);
   V3 inv = v3(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
@@ -351,7 +352,7 @@ MicroHit cutout_march(I3 wv, U3 uc, V3 ro, V3 rd, float t_in, uint32_t axis_in,
   uint32_t axis = axis_in;
   for (uint32_t i = 0; i < 12u; ++i) {
     if (m.x < 0 || m.y < 0 || m.z < 0 || m.x >= 4 || m.y >= 4 || m.z >= 4) return r;
-    if (leaf_solid(wv, U3{(uint32_t)m.x, (uint32_t)m.y, (uint32_t)m.z})) {
+    if (leaf_solid(wv, U3{(uint32_t)m.x, (uint32_t)m.y, (uint32_t)m.z}, fill)) {
       r.hit = true;
       r.t = t;
       r.normal = axis * 2u + (pos_dir[axis] ? 0u : 1u);
@@ -421,27 +422,36 @@ Hit march_chunk(const World& w, uint32_t ci, V3 ro_w, V3 rd, float t_limit, bool
     water_aware = false;
   }
   bool attr_uniform = (c.attr_flags & VM_ATTR_UNIFORM) != 0u;
-  bool foliage_aware = (c.attr_flags & VM_ATTR_HAS_FOLIAGE) != 0u;
+  // pipeline specialisations (common.wgsl:635-666): SPEC_FOLIAGE,
+  // SPEC_LEAF_CUTOUT, SPEC_GLASS, SPEC_EMITTER_GATHER, SPEC_WATER_REPAIR
+  bool foliage_aware = (w.spec & VM_SPEC_FOLIAGE) != 0u && (c.attr_flags & VM_ATTR_HAS_FOLIAGE) != 0u;
   if (foliage_aware && attr_uniform && !is_tuft(c.attr_base)) foliage_aware = false;
-  bool cutout_aware = (c.attr_flags & VM_ATTR_HAS_CUTOUT) != 0u && vs == 1.0f;
+  bool cutout_aware = (w.spec & VM_SPEC_LEAF_CUTOUT) != 0u && (c.attr_flags & VM_ATTR_HAS_CUTOUT) != 0u && vs == 1.0f;
   if (cutout_aware && attr_uniform && c.attr_base != VM_LEAVES && c.attr_base != VM_PINE_LEAVES)
     cutout_aware = false;
-  bool glass_aware = skip_glass && (c.attr_flags & VM_ATTR_HAS_GLASS) != 0u;
+  bool glass_aware = (w.spec & VM_SPEC_GLASS) != 0u && skip_glass && (c.attr_flags & VM_ATTR_HAS_GLASS) != 0u;
   if (glass_aware && attr_uniform) {
     if (c.attr_base == VM_GLASS) return h;
     glass_aware = false;
   }
-  bool noncaster_aware = sun_ray && (c.attr_flags & VM_ATTR_HAS_EMITTER) != 0u;
+  bool noncaster_aware = (w.spec & VM_SPEC_EMITTER_GATHER) != 0u && sun_ray && (c.attr_flags & VM_ATTR_HAS_EMITTER) != 0u;
   if (noncaster_aware && attr_uniform && !casts_sun_shadow(c.attr_base)) return h;
-  bool water_interface = !skip_water && (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
+  bool water_interface = (w.spec & VM_SPEC_WATER_REPAIR) != 0u && !skip_water && (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
   bool attr_needed = (noncaster_aware && !attr_uniform) || (water_interface && !attr_uniform) ||
                      water_aware || glass_aware || ((foliage_aware || cutout_aware) && !attr_uniform);
 
   U2 trav_mask = root_mask;
   if (water_aware) trav_mask = U2{c.dry_mask[0], c.dry_mask[1]};
   bool root_full = (c.root[2] & VM_FULL_BIT) != 0u;
-  // SPEC_FULL_MARCH is on (its default), so the full-root short cut at
-  // common.wgsl:677-686 never fires.
+  // the full-root short cut without SPEC_FULL_MARCH (common.wgsl:677-686)
+  if (root_full && (w.spec & VM_SPEC_FULL_MARCH) == 0u && !noncaster_aware && !water_interface) {
+    h.hit = true;
+    h.t = t * vs;
+    h.normal = axis * 2u + (pos_dir[axis] ? 0u : 1u);
+    h.voxel = {(uint32_t)cell.x, (uint32_t)cell.y, (uint32_t)cell.z};
+    h.micro = micro_entry(h.voxel, ro, rd, t, axis, pos_dir, t > 0.0f);
+    return h;
+  }
   if (trav_mask.x == 0u && trav_mask.y == 0u) return h;
 
   uint32_t l1_cached = 0xFFFFFFFFu;
@@ -567,7 +577,8 @@ Hit march_chunk(const World& w, uint32_t ci, V3 ro_w, V3 rd, float t_limit, bool
       if (is_cutout_id(bid)) {
         I3 wv{f2i(c.origin[0]) + (int32_t)uc.x, f2i(c.origin[1]) + (int32_t)uc.y,
               f2i(c.origin[2]) + (int32_t)uc.z};
-        MicroHit q = cutout_march(wv, uc, ro, rd, t, axis, pos_dir, t > 0.0f);
+        MicroHit q = cutout_march(wv, uc, ro, rd, t, axis, pos_dir, t > 0.0f,
+                                  (w.spec & VM_SPEC_LEAF_THIN) ? VM_LEAF_FILL : VM_LEAF_FILL_PRE43);
         if (q.hit) {
           h.hit = true;
           h.t = q.t * vs;
@@ -602,6 +613,30 @@ Hit march_chunk(const World& w, uint32_t ci, V3 ro_w, V3 rd, float t_limit, bool
     setc(cell, axis, pos_dir[axis] ? comp(bmax_i, axis) : comp(bmin_i, axis) - 1);
   }
   return h;
+}
+
+V3 refract(V3 e1, V3 e2, float e3);
+
+// glass is its own surface only with SPEC_GLASS (shadow.wgsl:18, resolve.wgsl:1440)
+inline bool glass_leg(const World& w, uint32_t id) { return (w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS; }
+
+// SPEC_SNELL_BEND: march.wgsl:23-44 (the straight march of chunk ci missed)
+void snell_bend(const World& w, uint32_t ci, V3 rd, Hit& h) {
+  const vm_frame& f = *w.f;
+  const float depth = f.sea_level - f.cam_pos[1];
+  if (!(depth > 0.0f)) return;
+  const float t_surf = depth / rd.y;
+  if (!(t_surf < f.far_)) return;
+  const V3 surf = add(ld3(f.cam_pos), muls(rd, t_surf));
+  const V3 rd2 = refract(rd, v3(0.0f, -1.0f, 0.0f), VM_WATER_IOR);
+  if (!(dot(rd2, rd2) > 0.0f)) return;
+  Hit h2 = march_chunk(w, ci, add(surf, muls(rd2, VM_SURFACE_EPS)), rd2, f.far_ - t_surf, true, false, false, false);
+  if (h2.hit) {
+    const uint32_t straight_iters = h.iters;
+    h = h2;
+    h.t = t_surf + h2.t;
+    h.iters = straight_iters + h2.iters;
+  }
 }
 
 // shadow_ray_t: common.wgsl:1156-1195
@@ -816,7 +851,7 @@ Guide shadow_guide(const World& w, const uint64_t* vis, int32_t px, int32_t py) 
   const uint32_t ci = key_ci(key);
   const U3 v = key_voxel(key);
   const uint32_t id = block_at(w, ci, v);
-  if (id == VM_WATER || id == VM_GLASS) return g;
+  if (id == VM_WATER || glass_leg(w, id)) return g;
   const uint32_t nid = key_nid(key);
   const U3 micro = key_micro(key);
   const V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
@@ -859,6 +894,7 @@ typedef struct or_world {
   const uint32_t* leaves; uint64_t n_leaves;
   const uint32_t* bricks; uint64_t n_bricks;
   const uint32_t* grid; uint64_t n_grid;
+  uint32_t spec;     // VM_SPEC_* pipeline specialisations
 } or_world;
 
 typedef struct or_hit {
@@ -877,6 +913,7 @@ static World mk(const or_world* o) {
   w.leaves = o->leaves; w.n_leaves = o->n_leaves;
   w.bricks = o->bricks; w.n_bricks = o->n_bricks;
   w.grid = o->grid; w.n_grid = o->n_grid;
+  w.spec = o->spec;
   return w;
 }
 
@@ -1005,6 +1042,8 @@ int or_frame(const or_world* o, const uint32_t* hiz_in, uint64_t* vis, uint32_t*
               if (ray_skips(f, c.fade, px, py)) continue;
               V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
               Hit h = march_chunk(w, ci, cam, rd, f.far_, underwater, false, false, false);
+              if ((w.spec & VM_SPEC_SNELL_BEND) != 0u && underwater && !h.hit && rd.y > 0.0f)
+                snell_bend(w, ci, rd, h);
               uint64_t pix = (uint64_t)py * f.res[0] + px;
               if (h.hit) {
                 uint64_t k = make_key(f, h.t, h.normal, ci, h.voxel, h.micro);
@@ -1133,7 +1172,7 @@ int or_primary_shadow(const or_world* o, const uint64_t* vis, float* out, uint64
           uint32_t ci = key_ci(key);
           U3 v = key_voxel(key);
           uint32_t id = block_at(w, ci, v);
-          if (!(id == VM_WATER || id == VM_GLASS)) {
+          if (!(id == VM_WATER || glass_leg(w, id))) {
             uint32_t nid = key_nid(key);
             U3 micro = key_micro(key);
             uint32_t px = (uint32_t)(pix % f.res[0]), py = (uint32_t)(pix / f.res[0]);
@@ -1261,7 +1300,7 @@ int or_secondary(const or_world* o, const uint64_t* vis, uint64_t* sec_key, floa
       uint32_t ci = key_ci(key);
       U3 v = key_voxel(key);
       uint32_t id = block_at(w, ci, v);
-      bool water = id == VM_WATER, glass = id == VM_GLASS;
+      bool water = id == VM_WATER, glass = glass_leg(w, id);
       if (water || glass) {
         uint32_t nid = key_nid(key);
         U3 micro = key_micro(key);

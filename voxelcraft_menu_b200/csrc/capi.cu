@@ -59,6 +59,7 @@ struct vm_ctx {
   bool graph_secondary = false;   // the cached graph also traces the secondary rays
   // tuning of the primary kernel
   vmk::PipeTuning tuning{4, 0, 0, 1};
+  uint32_t spec = VM_SPEC_DEFAULT;   // VM_SPEC_* pipeline specialisations
   std::string err_text;
 };
 
@@ -126,6 +127,7 @@ vmd::DevWorld dev_world(vm_ctx* ctx) {
   w.bricks = (const uint32_t*)ctx->bricks.p; w.n_bricks = ctx->n_bricks;
   w.grid = (const uint32_t*)ctx->grid.p; w.n_grid = ctx->grid_len;
   w.err = (uint32_t*)ctx->err.p;
+  w.spec = ctx->spec;
   return w;
 }
 
@@ -174,6 +176,7 @@ vmk::PipeArgs base_args(vm_ctx* ctx) {
   a.tile_order = (uint32_t*)ctx->tile_order.p;
   a.traffic = (vmk::Traffic64*)ctx->traffic.p;
   a.do_shadow = 1;
+  a.spec = ctx->spec;
   a.do_secondary = 1;
   return a;
 }
@@ -394,6 +397,14 @@ int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_
   ctx->tuning.primary_warps = warps_per_block;
   ctx->tuning.reg_level = reg_level;
   ctx->tuning.ctas_per_sm = ctas_per_sm;
+  return VM_OK;
+}
+
+int vm_set_spec(vm_ctx* ctx, uint32_t spec) {
+  if (!ctx) return VM_E_INVALID;
+  if ((spec & ~VM_SPEC_ALL) != 0u) return fail(ctx, VM_E_INVALID, "unknown VM_SPEC bits 0x%x", spec & ~VM_SPEC_ALL);
+  if (spec != ctx->spec) drop_graph(ctx);
+  ctx->spec = spec;
   return VM_OK;
 }
 

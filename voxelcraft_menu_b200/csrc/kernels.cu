@@ -113,7 +113,8 @@ __global__ void __launch_bounds__(256) k_march_pairs(const vm_frame f, const Dev
     const Chunk c = ld_chunk(w, ci);
     if (ray_skips(f, c.fade, px, py)) continue;
     const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
-    const Hit h = march_chunk<UNDERWATER, false, false, false>(w, f, c, make_ray(cam, rd), f.far_, nullptr);
+    Hit h = march_chunk<UNDERWATER, false, false, false>(w, f, c, make_ray(cam, rd), f.far_, nullptr);
+    if (UNDERWATER && (w.spec & VM_SPEC_SNELL_BEND) != 0u && !h.hit) snell_bend<false, false>(w, f, c, rd, &h, nullptr);
     const uint64_t pix = (uint64_t)py * f.res[0] + px;
     if (h.hit) atomicMax(&vis[pix], make_key(f, h, ci));
     if (heat) atomicAdd(&dbg[pix], h.iters);

@@ -83,6 +83,7 @@ struct PipeArgs {
   uint32_t* err;
   Traffic64* traffic;          // counting kernels only
   uint32_t do_shadow, do_secondary;
+  uint32_t spec;               // VM_SPEC_* pipeline specialisations
   uint32_t do_reflect;         // with do_secondary: also queue the reflect leg of water hits
                                // (sec_q then holds up to 2 items per pixel)
   vm_frame frame0;

@@ -22,6 +22,7 @@ struct DevWorld {
   const uint32_t* bricks; uint64_t n_bricks;
   const uint32_t* grid; uint64_t n_grid;
   uint32_t* err;
+  uint32_t spec;     // VM_SPEC_* pipeline specialisations
 };
 
 enum : uint32_t { ERR_CHUNK = 1u, ERR_INNER = 2u, ERR_LEAF = 4u, ERR_BRICK = 8u, ERR_GRID = 16u, ERR_LIST = 32u };
@@ -162,10 +163,14 @@ __device__ __forceinline__ uint32_t hash_u32(uint32_t h) {
   h ^= h >> 16u; h *= 0x7feb352du; h ^= h >> 15u; h *= 0x846ca68bu; h ^= h >> 16u;
   return h;
 }
-__device__ __forceinline__ bool leaf_solid(int32_t wx, int32_t wy, int32_t wz, uint32_t mx, uint32_t my, uint32_t mz) {
+__device__ __forceinline__ float leaf_fill(uint32_t spec) {   // SPEC_LEAF_FILL
+  return (spec & VM_SPEC_LEAF_THIN) ? VM_LEAF_FILL : VM_LEAF_FILL_PRE43;
+}
+__device__ __forceinline__ bool leaf_solid(int32_t wx, int32_t wy, int32_t wz, uint32_t mx, uint32_t my, uint32_t mz,
+                                           float fill = VM_LEAF_FILL) {
   uint32_t qx = (uint32_t)wx * 4u + mx, qy = (uint32_t)wy * 4u + my, qz = (uint32_t)wz * 4u + mz;
   uint32_t h = hash_u32((qx * 73856093u) ^ (qy * 19349663u) ^ (qz * 83492791u));
-  return (float)(h >> 8u) * (1.0f / 16777216.0f) < VM_LEAF_FILL;
+  return (float)(h >> 8u) * (1.0f / 16777216.0f) < fill;
 }
 
 // leaf_block: common.wgsl:320-334
@@ -273,7 +278,8 @@ __device__ __forceinline__ void micro_entry(uint32_t ux, uint32_t uy, uint32_t u
 // cutout_march: common.wgsl:537-577
 static __device__ __forceinline__ bool cutout_march(int32_t wx, int32_t wy, int32_t wz, uint32_t ux, uint32_t uy, uint32_t uz,
                                           F3 ro, F3 rd, F3 inv, float t_in, uint32_t axis_in, bool pdx, bool pdy,
-                                          bool pdz, bool snap, float* t_out, uint32_t* n_out, uint32_t* m_out) {
+                                          bool pdz, bool snap, float fill, float* t_out, uint32_t* n_out,
+                                          uint32_t* m_out) {
   // inv is the ray's 1 / rd, the value the WGSL recomputes here
   const float ms = 1.0f / 4.0f;
   uint32_t me[3];
@@ -283,7 +289,7 @@ static __device__ __forceinline__ bool cutout_march(int32_t wx, int32_t wy, int3
   uint32_t axis = axis_in;
   for (uint32_t i = 0; i < 12u; ++i) {
     if (m0 < 0 || m1 < 0 || m2 < 0 || m0 >= 4 || m1 >= 4 || m2 >= 4) return false;
-    if (leaf_solid(wx, wy, wz, m0, m1, m2)) {
+    if (leaf_solid(wx, wy, wz, m0, m1, m2, fill)) {
       *t_out = t;
       bool pd = axis == 0 ? pdx : (axis == 1 ? pdy : pdz);
       *n_out = axis * 2u + (pd ? 0u : 1u);
@@ -298,6 +304,8 @@ static __device__ __forceinline__ bool cutout_march(int32_t wx, int32_t wy, int3
   }
   return false;
 }
+
+__device__ __forceinline__ F3 refract(F3 e1, F3 e2, float e3);
 
 // Ray state shared by a sequence of march_chunk calls on one ray.  A zero
 // direction component (a sun exactly on the horizon) gives an infinite
@@ -372,18 +380,21 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
     if (c.attr_base == VM_WATER) return h;
     water_aware = false;
   }
-  bool foliage_aware = (c.attr_flags & VM_ATTR_HAS_FOLIAGE) != 0u;
+  const uint32_t spec = w.spec;
+  bool foliage_aware = (spec & VM_SPEC_FOLIAGE) != 0u && (c.attr_flags & VM_ATTR_HAS_FOLIAGE) != 0u;
   if (foliage_aware && attr_uniform && !is_tuft(c.attr_base)) foliage_aware = false;
-  bool cutout_aware = (c.attr_flags & VM_ATTR_HAS_CUTOUT) != 0u && vs == 1.0f;
+  bool cutout_aware = (spec & VM_SPEC_LEAF_CUTOUT) != 0u && (c.attr_flags & VM_ATTR_HAS_CUTOUT) != 0u && vs == 1.0f;
   if (cutout_aware && attr_uniform && c.attr_base != VM_LEAVES && c.attr_base != VM_PINE_LEAVES) cutout_aware = false;
-  bool glass_aware = SKIP_GLASS && (c.attr_flags & VM_ATTR_HAS_GLASS) != 0u;
+  bool glass_aware = SKIP_GLASS && (spec & VM_SPEC_GLASS) != 0u && (c.attr_flags & VM_ATTR_HAS_GLASS) != 0u;
   if (glass_aware && attr_uniform) {
     if (c.attr_base == VM_GLASS) return h;
     glass_aware = false;
   }
-  const bool noncaster_aware = SUN_RAY && (c.attr_flags & VM_ATTR_HAS_EMITTER) != 0u;
+  const bool noncaster_aware = SUN_RAY && (spec & VM_SPEC_EMITTER_GATHER) != 0u &&
+                               (c.attr_flags & VM_ATTR_HAS_EMITTER) != 0u;
   if (noncaster_aware && attr_uniform && c.attr_base == VM_GLOWSTONE) return h;
-  const bool water_interface = !SKIP_WATER && (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
+  const bool water_interface = !SKIP_WATER && (spec & VM_SPEC_WATER_REPAIR) != 0u &&
+                               (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
   const bool attr_needed = (noncaster_aware && !attr_uniform) || (water_interface && !attr_uniform) || water_aware ||
                            glass_aware || ((foliage_aware || cutout_aware) && !attr_uniform);
   const bool any_filter = noncaster_aware || water_interface || water_aware || glass_aware || foliage_aware || cutout_aware;
@@ -391,6 +402,19 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
   uint32_t trav_lo = root_lo, trav_hi = root_hi;
   if (water_aware) { trav_lo = c.dry[0]; trav_hi = c.dry[1]; }
   const bool root_full = (c.root[2] & VM_FULL_BIT) != 0u;
+  if (root_full && (spec & VM_SPEC_FULL_MARCH) == 0u && !noncaster_aware && !water_interface) {
+    // the full-root shortcut (common.wgsl:677-686): the entry cell is the hit
+    h.hit = true;
+    h.t = t * vs;
+    const bool pd = axis == 0 ? pdx : (axis == 1 ? pdy : pdz);
+    h.normal = axis * 2u + (pd ? 0u : 1u);
+    h.vx = cx; h.vy = cy; h.vz = cz;
+    uint32_t m[3];
+    micro_entry(cx, cy, cz, ro, rd, t, axis, pdx, pdy, pdz, t > 0.0f, m);
+    h.mx = m[0]; h.my = m[1]; h.mz = m[2];
+    if (WANT_ID) h.id = attr_uniform ? c.attr_base : block_at(w, c, cx, cy, cz);
+    return h;
+  }
   if (trav_lo == 0u && trav_hi == 0u) return h;
 
   uint32_t l1_cached = 0xFFFFFFFFu;
@@ -506,7 +530,8 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
         const int32_t wy = __float2int_rz(c.origin[1]) + (int32_t)uy;
         const int32_t wz = __float2int_rz(c.origin[2]) + (int32_t)uz;
         float qt; uint32_t qn; uint32_t qm[3];
-        if (cutout_march(wx, wy, wz, ux, uy, uz, ro, rd, inv, t, axis, pdx, pdy, pdz, t > 0.0f, &qt, &qn, qm)) {
+        if (cutout_march(wx, wy, wz, ux, uy, uz, ro, rd, inv, t, axis, pdx, pdy, pdz, t > 0.0f, leaf_fill(spec), &qt,
+                         &qn, qm)) {
           h.hit = true; h.t = qt * vs; h.normal = qn;
           h.vx = ux; h.vy = uy; h.vz = uz;
           h.mx = qm[0]; h.my = qm[1]; h.mz = qm[2];
@@ -558,6 +583,32 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
     else cz = pdz ? bz0 + skip : bz0 - 1;
   }
   return h;
+}
+
+// SPEC_SNELL_BEND (march.wgsl:23-44): from an underwater camera, a primary
+// ray that rises and misses chunk c straight is bent at the flat sea level
+// (refract(rd, -y, WATER_IOR)) and marched again from the surface; a hit
+// there replaces the miss, with t the whole path (surface distance + bent
+// leg) and the iterations of both marches.
+template <bool COUNT, bool WANT_ID>
+__device__ __forceinline__ void snell_bend(const DevWorld& w, const vm_frame& f, const Chunk& c, F3 rd, Hit* h,
+                                           Traffic* tr) {
+  if (!(rd.y > 0.0f)) return;
+  const float depth = f.sea_level - f.cam_pos[1];
+  if (!(depth > 0.0f)) return;
+  const float t_surf = depth / rd.y;
+  if (!(t_surf < f.far_)) return;
+  const F3 surf = ld3(f.cam_pos) + rd * t_surf;
+  const F3 rd2 = refract(rd, f3(0.0f, -1.0f, 0.0f), VM_WATER_IOR);
+  if (!(dot(rd2, rd2) > 0.0f)) return;
+  const Hit h2 = march_chunk<true, false, false, COUNT, WANT_ID>(w, f, c, make_ray(surf + rd2 * VM_SURFACE_EPS, rd2),
+                                                                  f.far_ - t_surf, tr);
+  if (h2.hit) {
+    const uint32_t straight_iters = h->iters;
+    *h = h2;
+    h->t = t_surf + h2.t;
+    h->iters = straight_iters + h2.iters;
+  }
 }
 
 // shadow_ray_t: common.wgsl:1156-1195

@@ -46,7 +46,7 @@ __device__ __forceinline__ const vm_frame& frame_of(const PipeArgs& a, uint32_t 
 __device__ __forceinline__ ViewDesc view_of(const PipeArgs& a, uint32_t v) { return a.frames ? a.views[v] : a.view0; }
 __device__ __forceinline__ DevWorld world_of(const PipeArgs& a, const ViewDesc& vd) {
   return {a.chunks + vd.chunk_off, vd.n_chunks, a.inners, a.n_inners, a.leaves, a.n_leaves,
-          a.bricks, a.n_bricks, a.grids + vd.grid_off, vd.grid_len, a.err};
+          a.bricks, a.n_bricks, a.grids + vd.grid_off, vd.grid_len, a.err, a.spec};
 }
 
 // The same, resolved at compile time when the launch is known to carry one
@@ -371,7 +371,12 @@ __device__ __forceinline__ void march_entry(const DevWorld& w, const vm_frame& f
     const float t_cut = f.far_ * (1.0f - (float)(bestd - 3u) * (1.0f / 16777215.0f));
     if (t_cut < f.far_ && depth_key(f, t_cut) < bestd) t_lim = t_cut;
   }
-  const Hit h = march_chunk<UNDERWATER, false, false, COUNT, true>(w, f, c, ray, t_lim, tr);
+  // With the Snell bend a miss of the straight march (over its full length,
+  // as the engine marches it) is what lets the bent ray count, so the
+  // distance limit is not applied to it.
+  const bool bend = UNDERWATER && (w.spec & VM_SPEC_SNELL_BEND) != 0u;
+  Hit h = march_chunk<UNDERWATER, false, false, COUNT, true>(w, f, c, ray, bend ? f.far_ : t_lim, tr);
+  if (bend && !h.hit) snell_bend<COUNT, true>(w, f, c, ray.d, &h, tr);
   if (h.hit) {
     const unsigned long long k = make_key(f, h, ci);
     if (k > best) { best = k; best_id = h.id; }
@@ -573,7 +578,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
       const Chunk c = ld_chunk(w, k.ci);
       const float th = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, prd);
       const F3 hit = cam + prd * th;
-      const bool water = pbest_id == VM_WATER, glass = pbest_id == VM_GLASS;
+      const bool water = pbest_id == VM_WATER, glass = is_glass_leg(a.spec, pbest_id);
       if (a.do_shadow && shadow_active(f) && !water && !glass) {
         F3 nrm = normal_of(k.nid);
         if (k.nid >= VM_NORMAL_CROSS_A && dot(nrm, prd) > 0.0f) nrm = neg(nrm);

@@ -18,6 +18,13 @@ __device__ __forceinline__ bool shadow_active(const vm_frame& f) {   // shadow.w
   return (f.flags & VM_FLAG_SHADOWS) != 0u && (f.flags & VM_FLAG_HEATMAP) == 0u && f.daylight > 0.01f;
 }
 
+// Glass is its own surface (no sun-shadow ray of its own, a transmission
+// leg) only with SPEC_GLASS (shadow.wgsl:18, resolve.wgsl:1440); without it
+// glass blocks shade as opaque blocks.
+__device__ __forceinline__ bool is_glass_leg(uint32_t spec, uint32_t id) {
+  return (spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS;
+}
+
 struct KeyParts { uint32_t ci, vx, vy, vz, mx, my, mz, nid; };
 __device__ __forceinline__ KeyParts split_key(unsigned long long key) {
   KeyParts k;
@@ -37,7 +44,7 @@ __device__ __forceinline__ bool shadow_setup(const DevWorld& w, const vm_frame& 
   const KeyParts k = split_key(key);
   const Chunk c = ld_chunk(w, k.ci);
   const uint32_t id = block_at(w, c, k.vx, k.vy, k.vz);
-  if (id == VM_WATER || id == VM_GLASS) return false;
+  if (id == VM_WATER || (is_glass_leg(w.spec, id))) return false;
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   F3 n = normal_of(k.nid);
   if (k.nid >= VM_NORMAL_CROSS_A && dot(n, rd) > 0.0f) n = neg(n);
@@ -85,7 +92,7 @@ __device__ __forceinline__ bool secondary_setup(const DevWorld& w, const vm_fram
   const KeyParts k = split_key(key);
   const Chunk c = ld_chunk(w, k.ci);
   const uint32_t id = block_at(w, c, k.vx, k.vy, k.vz);
-  const bool water = id == VM_WATER, glass = id == VM_GLASS;
+  const bool water = id == VM_WATER, glass = is_glass_leg(w.spec, id);
   if (!water && !glass) return false;
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);

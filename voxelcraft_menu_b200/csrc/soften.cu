@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(SOFT_THREADS) k_soften(const __grid_constant__
         const KeyParts k = split_key(key);
         const Chunk ch = ld_chunk(w, k.ci);
         const uint32_t id = block_at(w, ch, k.vx, k.vy, k.vz);
-        if (id != VM_WATER && id != VM_GLASS) {
+        if (id != VM_WATER && !is_glass_leg(w.spec, id)) {
           const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
           F3 n = normal_of(k.nid);
           bool flip = false;

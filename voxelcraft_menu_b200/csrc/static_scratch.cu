@@ -137,6 +137,7 @@ extern "C" int vm_render_static(const vm_frame* frame, const vm_chunk* d_chunks,
   a.work = s->work;
   a.err = d_error;
   a.do_shadow = 1;
+  a.spec = VM_SPEC_DEFAULT;
   a.do_secondary = 0;
   a.frame0 = f;
   a.view0 = v;

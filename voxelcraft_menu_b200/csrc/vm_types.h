@@ -233,6 +233,23 @@ static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
 
 /* WGSL override defaults that reach the march (common.wgsl:180-263) */
 #define VM_LEAF_FILL 0.62f
+#define VM_LEAF_FILL_PRE43 0.72f    /* SPEC_LEAF_FILL without FLAG_LEAF_THIN (src/render/mod.rs:321-323,2500-2506) */
+
+/* Pipeline specialisations of the march (the engine's override constants,
+ * make_spec src/render/mod.rs:2355-2689, common.wgsl:180-262), set per
+ * context with vm_set_spec.  VM_SPEC_DEFAULT is the engine's default
+ * configuration (src/config.rs:305-348). */
+#define VM_SPEC_FULL_MARCH 1u       /* SPEC_FULL_MARCH: march full roots (else the full-root shortcut, common.wgsl:677-686) */
+#define VM_SPEC_WATER_REPAIR 2u     /* SPEC_WATER_REPAIR: the water-interface repair (common.wgsl:666) */
+#define VM_SPEC_LEAF_CUTOUT 4u      /* SPEC_LEAF_CUTOUT: micro-voxel leaves (common.wgsl:643-649) */
+#define VM_SPEC_GLASS 8u            /* SPEC_GLASS: glass transparent to shadow / secondary rays, its own legs */
+#define VM_SPEC_EMITTER_GATHER 16u  /* SPEC_EMITTER_GATHER: emitters cast no sun shadow (common.wgsl:664) */
+#define VM_SPEC_FOLIAGE 32u         /* SPEC_FOLIAGE: tuft blocks are foliage (else plain solid cubes) */
+#define VM_SPEC_SNELL_BEND 64u      /* SPEC_SNELL_BEND: bent primary rays from underwater (march.wgsl:23-44) */
+#define VM_SPEC_LEAF_THIN 128u      /* FLAG_LEAF_THIN: SPEC_LEAF_FILL = 0.62, else 0.72 */
+#define VM_SPEC_DEFAULT (VM_SPEC_FULL_MARCH | VM_SPEC_WATER_REPAIR | VM_SPEC_LEAF_CUTOUT | VM_SPEC_GLASS | \
+                         VM_SPEC_EMITTER_GATHER | VM_SPEC_FOLIAGE | VM_SPEC_LEAF_THIN)
+#define VM_SPEC_ALL 255u
 #define VM_SURFACE_EPS 0.02f          /* common.wgsl:1258 */
 #define VM_WATER_IOR 1.333f           /* common.wgsl:1256 */
 #define VM_WATER_REFRACT_DIST 96.0f   /* resolve.wgsl:879 */

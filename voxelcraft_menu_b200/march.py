@@ -25,6 +25,11 @@ STATUS = {0: "VM_OK", 1: "VM_E_INVALID", 2: "VM_E_CAPACITY", 3: "VM_E_TILE_OVERF
 PRIMARY_WARPS = (4, 8)
 REG_LEVELS = (0, 1, 2, 3, 4)
 PACKETS = (1, 2)
+# pipeline specialisations (VM_SPEC_* of vm_types.h)
+SPEC_FULL_MARCH, SPEC_WATER_REPAIR, SPEC_LEAF_CUTOUT, SPEC_GLASS = 1, 2, 4, 8
+SPEC_EMITTER_GATHER, SPEC_FOLIAGE, SPEC_SNELL_BEND, SPEC_LEAF_THIN = 16, 32, 64, 128
+SPEC_DEFAULT = SPEC_FULL_MARCH | SPEC_WATER_REPAIR | SPEC_LEAF_CUTOUT | SPEC_GLASS | SPEC_EMITTER_GATHER | \
+    SPEC_FOLIAGE | SPEC_LEAF_THIN
 
 
 class MarchError(RuntimeError):
@@ -103,6 +108,11 @@ class Marcher:
         (1: 8x4-pixel items, 2: 8x8) of the persistent primary-ray kernel."""
         self._ck(self._L.vm_set_tuning(self._h, warps, reg_level, ctas_per_sm))
         self._ck(self._L.vm_set_packet(self._h, packet))
+
+    def set_spec(self, spec: int = None):
+        """The pipeline specialisations (VM_SPEC_* bits, the engine's make_spec
+        override constants); None restores the engine's defaults."""
+        self._ck(self._L.vm_set_spec(self._h, SPEC_DEFAULT if spec is None else spec))
 
     # -- the engine's passes ------------------------------------------------------
     def select(self):
