@@ -138,12 +138,26 @@ int vm_read_shadow_mask(vm_ctx* ctx, float* out);            /* vm_soften_shadow
 /* The reflect leg of every water hit (water_reflect_leg, resolve.wgsl:1044-1058,
  * traced per hit as the refract leg is) of the last vm_render / vm_secondary
  * frame with FLAG_WATER_REFLECT: key as vm_read_secondary's (bit 61 clear) and
- * t; key 0 where the pixel has none (no water, reflect_detail 0 beyond 1024
- * voxels, or a waved surface: FLAG_WAVES on a +Y face, whose wave normal
- * resolve.wgsl:1107-1150 is not restated).  The first such frame grows the
+ * t; key 0 where the pixel has none (no water, or reflect_detail 0 beyond
+ * 1024 voxels).  The leg leaves along water_ctx's mirror_t: the face normal's
+ * reflection, on a waved +Y face (FLAG_WAVES) the wave normal's
+ * (resolve.wgsl:1107-1163, with FLAG_WAVE_ANISO / _SHOAL / _FILL, the frame's
+ * time and wave_* fields).  The first such frame grows the
  * context's buffers (12 bytes per pixel, and a secondary queue of 2 items per
  * pixel); VM_E_NOT_READY after a frame without the flag. */
 int vm_read_reflection(vm_ctx* ctx, uint64_t* key, float* t);
+/* The engine's schedule of the water legs (water_sec, resolve.wgsl:1468-1535,
+ * WATER_SEC_SHIFT = 1), over the visibility of the last frame: for every
+ * (1 << shift)^2 pixel block (shift 0..3), its water pixel nearest the camera
+ * (smallest hit_t; the first in x-major order on a tie) traces the refract leg
+ * (FLAG_WATER_REFRACT, water_refract_leg) and the reflect leg
+ * (FLAG_WATER_REFLECT, water_reflect_leg, along water_ctx's mirror_t,
+ * waved surfaces included).  vm_read_water_sec then returns
+ * ceil(res.x / 2^shift) * ceil(res.y / 2^shift) cells, row-major: keys as
+ * vm_read_secondary's (0 = no leg) and the legs' hit distances.  Any pointer
+ * may be NULL.  The cell buffers are allocated by the first call. */
+int vm_water_sec(vm_ctx* ctx, uint32_t shift);
+int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* refl_key, float* refl_t);
 /* Expanded visibility: voxel index X*(Z*y + z) + x over the world box
  * [origin, origin + dims), face = normal id (common.wgsl:387), t = hit_t
  * (common.wgsl:1300).  Misses: voxel 0xFFFFFFFF, face 0xFF, t 0. */

@@ -74,6 +74,7 @@ def lib():
             "or_pick": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, vp]),
             "or_soften_shadows": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, C.c_int]),
             "or_reflect": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
+            "or_water_sec": (C.c_int, [vp, vp, C.c_uint32, vp, vp, vp, vp, C.c_int]),
             "or_pick_rows": (C.c_uint64, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp]),
             "or_f16_round": (None, [vp, vp, C.c_uint64]),
         }
@@ -157,6 +158,18 @@ class Oracle:
         v = np.ascontiguousarray(vis, np.uint64)
         self._check(self.L.or_reflect(C.byref(self.w), _p(v), _p(k), _p(t), p0, p1, self.threads))
         return k, t
+
+    def water_sec(self, vis, shift: int = 1):
+        """water_sec (resolve.wgsl:1468-1535): (refract key, refract t,
+        reflect key, reflect t) per (2^shift)^2 block, shaped (rows, cols)."""
+        w, h = int(self.frame.res[0]), int(self.frame.res[1])
+        sp = 1 << shift
+        shape = ((h + sp - 1) // sp, (w + sp - 1) // sp)
+        out = [np.zeros(shape, np.uint64), np.zeros(shape, np.float32), np.zeros(shape, np.uint64),
+               np.zeros(shape, np.float32)]
+        v = np.ascontiguousarray(vis, np.uint64)
+        self._check(self.L.or_water_sec(C.byref(self.w), _p(v), shift, *(_p(a) for a in out), self.threads))
+        return tuple(out)
 
     def soften(self, vis, dist, limit: int = 4, penumbra: float = 1.5):
         """shadow_horizontal + shadow_vertical over the frame's blocker

@@ -931,6 +931,12 @@ int orw_build_view(const orw_world* wp, const vmw_camera* cam, vm_frame* frame, 
   frame->water_absorb = 1.0f;
   frame->jitter[0] = cam->jitter[0]; frame->jitter[1] = cam->jitter[1];
   frame->taa_feedback = 1.0f;
+  // the wave parameters of the engine's default configuration
+  // (src/config.rs:318-321 through src/render/mod.rs:1690-1694)
+  frame->wave_amp = 0.12f;
+  frame->wave_scale = 32.0f;
+  frame->wave_speed = 0.32f;
+  frame->wave_reflect_slope = 0.0f;
   frame->frame_index = cam->frame_index % 64u;
   return 0;
 }

@@ -1237,6 +1237,102 @@ int or_primary_shadow(const or_world* o, const uint64_t* vis, float* out, uint64
 // reflect(rd, nt), trace_world(..., 768, skip_water) (880).  nt = n, the face
 // normal, unless the surface is waved (FLAG_WAVES on a +Y face, 1107); waved
 // pixels get no reflect ray here.  Key as or_secondary's (bit 61 clear).
+}  // extern "C"
+
+// ---- water_ctx's reflect direction: resolve.wgsl:902-975,1078-1166 ----
+namespace {
+const float WAVE_TAU = 6.28318531f, WAVE_GRAZE_MIN = 1e-3f, SHOAL_DEPTH = 6.0f, WAVE_FILTER_K = 1.0f;
+
+// wave_octave: resolve.wgsl:928-942 (slope vector x, z and the variance)
+V3 wave_octave(float x, float z, float dx, float dz, float lambda, float slope, float phase, float px, float vhx,
+               float vhz, float kk, bool aniso) {
+  float fade;
+  if (aniso) {
+    float d = dx * vhx + dz * vhz;
+    float ext = px * sqrtf(1.0f + kk * d * d);
+    float u = ext / lambda;
+    fade = expf(-WAVE_FILTER_K * u * u);
+  } else {
+    fade = smoothstep(2.0f, 4.0f, lambda / fmaxf(px, 1e-4f));
+  }
+  float g = slope * fade * cosf(WAVE_TAU / lambda * (x * dx + z * dz) + phase);
+  return v3(dx * g, dz * g, 0.5f * slope * slope * (1.0f - fade * fade));
+}
+
+// wave_field: resolve.wgsl:944-965
+V3 wave_field(const vm_frame& f, float x, float z, float px, float vhx, float vhz, float kk, bool aniso, float shoal) {
+  struct Oct { float dx, dz, div, amp, ph; };
+  static const Oct fill[8] = {{-0.438371f, 0.898794f, 1.0f, 0.3086f, 1.0000f},
+                              {-0.927184f, 0.374607f, 1.3934f, 0.2584f, 1.1804f},
+                              {-0.190809f, 0.981627f, 1.9417f, 0.2163f, 1.3934f},
+                              {-0.669131f, 0.743145f, 2.7056f, 0.1810f, 1.6449f},
+                              {0.121869f, 0.992546f, 3.7700f, 0.1515f, 1.9417f},
+                              {0.694658f, 0.719340f, 5.2533f, 0.1269f, 2.2920f},
+                              {0.970296f, 0.241922f, 7.3201f, 0.1062f, 2.7056f},
+                              {0.438371f, 0.898794f, 10.2000f, 0.0889f, 3.1937f}};
+  static const Oct base[4] = {{0.913089f, 0.407760f, 1.0f, 0.42f, 1.0000f},
+                              {-0.388685f, 0.921371f, 2.17f, 0.27f, 1.4731f},
+                              {-0.980382f, -0.197108f, 4.71f, 0.19f, 2.1703f},
+                              {0.477328f, -0.878725f, 10.20f, 0.12f, 3.1937f}};
+  const bool full = (f.flags & VM_FLAG_WAVE_FILL) != 0u;
+  const Oct* o = full ? fill : base;
+  const int n = full ? 8 : 4;
+  const float l0 = f.wave_scale, a = f.wave_amp * shoal, ph = f.time * f.wave_speed * WAVE_TAU;
+  V3 s = v3(0.0f, 0.0f, 0.0f);
+  for (int i = 0; i < n; ++i) {
+    float lambda = i == 0 ? l0 : l0 / o[i].div;
+    s = add(s, wave_octave(x, z, o[i].dx, o[i].dz, lambda, a * o[i].amp, ph * o[i].ph, px, vhx, vhz, kk, aniso));
+  }
+  return s;
+}
+
+// water_ctx's mirror_t (resolve.wgsl:1078-1163; SPEC_WATER_LOOK off)
+V3 water_mirror_t(const World& w, uint32_t nid, V3 hit, V3 rd, float t) {
+  const vm_frame& f = *w.f;
+  const V3 n = normal_of(nid);
+  V3 nt = n;
+  float unresolved = 0.0f;
+  const bool waved = (f.flags & VM_FLAG_WAVES) != 0u && nid == VM_NORMAL_PY;
+  if (waved) {
+    float px_world = fmaxf(t, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1];
+    float kk = 0.0f, vhx = 0.0f, vhz = 0.0f;
+    const bool aniso = (f.flags & VM_FLAG_WAVE_ANISO) != 0u;
+    if (aniso) {
+      float k = 1.0f / fmaxf(fabsf(rd.y), WAVE_GRAZE_MIN);
+      kk = k * k - 1.0f;
+      float r = 1.0f / sqrtf(fmaxf(rd.x * rd.x + rd.z * rd.z, 1e-12f));
+      vhx = rd.x * r; vhz = rd.z * r;
+    }
+    float shoal = 1.0f;
+    if ((f.flags & VM_FLAG_WAVE_SHOAL) != 0u) {
+      V3 dro = v3(floorf(hit.x) + 0.5f, hit.y - VM_SURFACE_EPS, floorf(hit.z) + 0.5f);
+      WorldHit dh = trace_world(w, dro, v3(0.001f, -0.999999f, 0.001f), SHOAL_DEPTH, true);
+      shoal = smoothstep(0.0f, SHOAL_DEPTH, dh.hit ? dh.t : SHOAL_DEPTH);
+    }
+    V3 wf = wave_field(f, hit.x, hit.z, px_world, vhx, vhz, kk, aniso, shoal);
+    unresolved = fmaxf(wf.z, 0.0f);
+    float gl = sqrtf(wf.x * wf.x + wf.y * wf.y);
+    float lim = fminf(1.0f, f.wave_reflect_slope / fmaxf(gl, 1e-6f));
+    nt = normalize(v3(-(wf.x * lim), 1.0f, -(wf.y * lim)));
+  }
+  float rough = fminf(fmaxf(1.0f - expf(-8.0f * unresolved), 0.0f), 1.0f);
+  nt = normalize(add(muls(nt, 1.0f - rough), muls(n, rough)));
+  V3 m = reflect(rd, nt);
+  if (waved) m = normalize(v3(m.x, fmaxf(m.y, 0.0f), m.z));
+  return m;
+}
+
+uint64_t water_leg_key(const WorldHit& h) {
+  uint64_t k = 1ull << 63;
+  if (h.hit)
+    k |= (1ull << 62) | ((uint64_t)h.normal << 37) | ((uint64_t)h.ci << 24) |
+         (uint64_t)((h.voxel.x << 16u) | (h.voxel.y << 8u) | h.voxel.z);
+  return k;
+}
+}  // namespace
+
+extern "C" {
+
 int or_reflect(const or_world* o, const uint64_t* vis, uint64_t* refl_key, float* refl_t, uint64_t pix_begin,
                uint64_t pix_end, int threads) {
   World w = mk(o);
@@ -1255,8 +1351,7 @@ int or_reflect(const or_world* o, const uint64_t* vis, uint64_t* refl_key, float
       uint32_t ci = key_ci(key);
       U3 v = key_voxel(key);
       uint32_t nid = key_nid(key);
-      bool waved = (f.flags & VM_FLAG_WAVES) != 0u && nid == VM_NORMAL_PY;
-      if (block_at(w, ci, v) == VM_WATER && !waved) {
+      if (block_at(w, ci, v) == VM_WATER) {
         U3 micro = key_micro(key);
         uint32_t px = (uint32_t)(pix % f.res[0]), py = (uint32_t)(pix / f.res[0]);
         V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
@@ -1266,17 +1361,70 @@ int or_reflect(const or_world* o, const uint64_t* vis, uint64_t* refl_key, float
           V3 hit = add(cam, muls(rd, t));
           V3 n = normal_of(nid);
           V3 ro3 = add(hit, muls(n, VM_SURFACE_EPS));
-          WorldHit h3 = trace_world(w, ro3, reflect(rd, n), VM_WATER_REFLECT_DIST, true);
-          out_key = 1ull << 63;
-          if (h3.hit)
-            out_key |= (1ull << 62) | ((uint64_t)h3.normal << 37) | ((uint64_t)h3.ci << 24) |
-                       (uint64_t)((h3.voxel.x << 16u) | (h3.voxel.y << 8u) | h3.voxel.z);
+          WorldHit h3 = trace_world(w, ro3, water_mirror_t(w, nid, hit, rd, t), VM_WATER_REFLECT_DIST, true);
+          out_key = water_leg_key(h3);
           out_t = h3.t;
         }
       }
     }
     refl_key[pix] = out_key;
     refl_t[pix] = out_t;
+  }
+  return g_err.load();
+}
+
+// water_sec: resolve.wgsl:1468-1535 (cells row-major, ceil(res / 2^shift))
+int or_water_sec(const or_world* o, const uint64_t* vis, uint32_t shift, uint64_t* refr_key, float* refr_t,
+                 uint64_t* refl_key, float* refl_t, int threads) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  const uint32_t span = 1u << shift;
+  const uint32_t hw = (f.res[0] + span - 1u) >> shift, hh = (f.res[1] + span - 1u) >> shift;
+  const V3 cam = ld3(f.cam_pos);
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t c = 0; c < (int64_t)hw * hh; ++c) {
+    const uint32_t hx = (uint32_t)(c % hw), hy = (uint32_t)(c / hw);
+    float best_t = 3.4e38f;
+    bool has = false;
+    uint32_t bci = 0, bnid = 0, bpx = 0, bpy = 0;
+    for (uint32_t i = 0; i < span; ++i)
+      for (uint32_t j = 0; j < span; ++j) {
+        const uint32_t pxs = span * hx + i, pys = span * hy + j;
+        if (pxs >= f.res[0] || pys >= f.res[1]) continue;
+        const uint64_t key = vis[(uint64_t)pys * f.res[0] + pxs];
+        if (key == 0ull) continue;
+        const uint32_t cis = key_ci(key), nids = key_nid(key);
+        const U3 vs_ = key_voxel(key), micros = key_micro(key);
+        if (block_at(w, cis, vs_) != VM_WATER) continue;
+        const V3 rd0 = ray_dir(f, (float)pxs + 0.5f, (float)pys + 0.5f);
+        const float ts = hit_t(w, cis, vs_, micros, nids, rd0);
+        if (ts < best_t) { best_t = ts; bci = cis; bnid = nids; bpx = pxs; bpy = pys; has = true; }
+      }
+    (void)bci;
+    uint64_t kr = 0ull, km = 0ull;
+    float tr = 0.0f, tm = 0.0f;
+    if (has) {
+      const V3 rd = ray_dir(f, (float)bpx + 0.5f, (float)bpy + 0.5f);
+      const V3 hit = add(cam, muls(rd, best_t));
+      const V3 n = normal_of(bnid);
+      if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u &&
+          1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, best_t) > 0.0f) {
+        const V3 rdir = refract(rd, n, 1.0f / VM_WATER_IOR);
+        const WorldHit h2 = trace_world(w, add(hit, muls(rdir, VM_SURFACE_EPS)), rdir, VM_WATER_REFRACT_DIST, true);
+        kr = water_leg_key(h2);
+        tr = h2.t;
+      }
+      if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u &&
+          1.0f - smoothstep(VM_WATER_REFLECT_NEAR, VM_WATER_REFLECT_FAR, best_t) > 0.0f) {
+        const WorldHit h3 = trace_world(w, add(hit, muls(n, VM_SURFACE_EPS)), water_mirror_t(w, bnid, hit, rd, best_t),
+                                        VM_WATER_REFLECT_DIST, true);
+        km = water_leg_key(h3);
+        tm = h3.t;
+      }
+    }
+    refr_key[c] = kr; refr_t[c] = tr;
+    refl_key[c] = km; refl_t[c] = tm;
   }
   return g_err.load();
 }

@@ -1,12 +1,16 @@
 """The reflect leg of water hits (water_reflect_leg, resolve.wgsl:1044-1058).
 
 CPU: the oracle traces one reflect ray per water hit closer than 1024 voxels
-when FLAG_WATER_REFLECT is set, none for other blocks, none without the flag
-and none on waved (+Y with FLAG_WAVES) surfaces; a ray that leaves a +Y water
-face rises (a hit above the surface, or the 768-voxel distance).
+when FLAG_WATER_REFLECT is set, none for other blocks and none without the
+flag; a ray that leaves a +Y water face rises (a hit above the surface, or
+the 768-voxel distance).  On waved surfaces (FLAG_WAVES on +Y faces) the leg
+follows water_ctx's mirror_t: with the engine's default wave_reflect_slope of
+0 it is the flat surface's, with a positive slope the wave normal's.
 GPU: the reflect keys and distances of the wavefront pipeline and of the
-engine pass sequence equal the oracle's bit for bit; the flag leaves the
-frame's other outputs unchanged."""
+engine pass sequence equal the oracle's bit for bit (flat and default waves;
+with a positive reflect slope, whose wave field runs through cos and exp,
+at most 0.5% of the legs may differ); the flag leaves the frame's other
+outputs unchanged."""
 import numpy as np
 import pytest
 
@@ -14,6 +18,7 @@ from oracle.oracle import Oracle
 from voxelcraft_menu_b200 import world as W
 
 REFL = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_WATER_REFLECT
+WAVE_OPTS = 1024 | 2048 | 4096        # FLAG_WAVE_ANISO | FLAG_WAVE_SHOAL | FLAG_WAVE_FILL
 
 
 @pytest.fixture(scope="module")
@@ -48,20 +53,32 @@ def test_oracle_reflect_rays(small):
     v2 = w.view(W.small_terrain_camera(flags=W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT))
     k2, _ = Oracle(v2, *pools).reflection(vis)
     assert (k2 == 0).all()
-    v3 = w.view(W.small_terrain_camera(flags=REFL | W.FLAG_WAVES))
+    # waves at the default reflect slope 0: the flat legs; a positive slope
+    # moves some +Y legs and no other face's
+    waves = W.FLAG_WAVES | WAVE_OPTS
+    v3 = w.view(W.small_terrain_camera(flags=REFL | waves))
     k3, t3 = Oracle(v3, *pools).reflection(vis)
+    # the waved direction is renormalised (normalize(x, max(y, 0), z)): the
+    # same voxels, distances within float rounding
+    assert np.array_equal(k3, k) and np.allclose(t3, t, rtol=1e-5, atol=0.0)
+    v3.frame.wave_reflect_slope, v3.frame.time = 0.35, 1.7
+    k4, t4 = Oracle(v3, *pools).reflection(vis)
     py = nid == 3
-    assert (k3[py] == 0).all()
-    assert np.array_equal(k3[~py], k[~py]) and np.array_equal(t3[~py], t[~py])
+    assert np.array_equal(k4[~py], k[~py])
+    assert (k4[py] != k[py]).sum() > 100
+    assert ((k4 >> np.uint64(63)) & np.uint64(1) == 1)[py & water].all()
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("waves", [False, True])
+@pytest.mark.parametrize("waves", ["flat", "waves", "waves_all", "slope"])
 def test_gpu_reflect_matches_oracle(small, waves):
     from voxelcraft_menu_b200.march import Marcher
     w, pools = small
-    flags = REFL | (W.FLAG_WAVES if waves else 0)
+    flags = REFL | {"flat": 0, "waves": W.FLAG_WAVES, "waves_all": W.FLAG_WAVES | WAVE_OPTS,
+                    "slope": W.FLAG_WAVES | WAVE_OPTS}[waves]
     v = w.view(W.small_terrain_camera(flags=flags))
+    if waves == "slope":
+        v.frame.wave_reflect_slope, v.frame.time = 0.35, 1.7
     o = Oracle(v, *pools)
     ovis, _, _ = o.frame_vis()
     ok, ot = o.reflection(ovis)
@@ -73,12 +90,18 @@ def test_gpu_reflect_matches_oracle(small, waves):
             run()
             assert np.array_equal(m.read_vis(), ovis)
             k, t = m.read_reflection()
-            assert np.array_equal(k, ok), f"{run.__name__}: {(k != ok).sum()} reflect keys differ"
-            assert np.array_equal(t, ot), f"{run.__name__}: reflect t differs"
+            if waves == "slope":
+                traced = ((ok >> np.uint64(63)) & np.uint64(1)).sum()
+                assert np.array_equal(k != 0, ok != 0), "the same pixels trace a leg"
+                assert (k != ok).sum() <= 0.005 * traced, f"{run.__name__}: {(k != ok).sum()} of {traced} differ"
+            else:
+                assert np.array_equal(k, ok), f"{run.__name__}: {(k != ok).sum()} reflect keys differ"
+                assert np.array_equal(t, ot), f"{run.__name__}: reflect t differs"
             assert m.stats().device_error == 0
         # the flag adds the reflect legs and changes nothing else
         vis, sh, (sk, st) = m.read_vis(), m.read_shadow(), m.read_secondary()
         v0 = w.view(W.small_terrain_camera(flags=flags & ~W.FLAG_WATER_REFLECT))
+        v0.frame.wave_reflect_slope, v0.frame.time = v.frame.wave_reflect_slope, v.frame.time
         m.upload_view(v0)
         m.render()
         assert np.array_equal(m.read_vis(), vis) and np.array_equal(m.read_shadow(), sh)

@@ -44,6 +44,9 @@ struct vm_ctx {
   DevBuf shadow_mask;   // vm_soften_shadows output, sized on first use
   DevBuf shadow16;      // vm_read_async_r16f staging, sized on first use
   DevBuf refl_key, refl_t;   // reflect legs of water hits, sized by the first FLAG_WATER_REFLECT frame
+  DevBuf ws_refr_key, ws_refr_t, ws_refl_key, ws_refl_t;   // vm_water_sec cells, sized by its first call
+  uint32_t ws_shift = 0, ws_cells = 0;
+  bool ws_done = false;
   bool refl_frame = false;   // the last frame traced them
   DevBuf tile_list, tile_count, shadow_q, sec_q, item_cost, tile_order, super_list, super_count;
   // batch
@@ -309,7 +312,7 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->b_shadow_q, &ctx->b_sec_q, &ctx->item_cost, &ctx->tile_order, &ctx->b_item_cost,
                    &ctx->b_tile_order, &ctx->super_list, &ctx->super_count, &ctx->b_super_list,
                    &ctx->b_super_count, &ctx->shadow_mask, &ctx->refl_key, &ctx->refl_t,
-                   &ctx->shadow16};
+                   &ctx->shadow16, &ctx->ws_refr_key, &ctx->ws_refr_t, &ctx->ws_refl_key, &ctx->ws_refl_t};
   for (DevBuf* b : all) release(*b);
   if (ctx->rendered) cudaEventDestroy(ctx->rendered);
   if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -498,6 +501,40 @@ int vm_secondary(vm_ctx* ctx) {
                            (unsigned long long*)ctx->sec_key.p, (float*)ctx->sec_t.p,
                            ctx->refl_frame ? (unsigned long long*)ctx->refl_key.p : nullptr,
                            ctx->refl_frame ? (float*)ctx->refl_t.p : nullptr, ctx->stream));
+  return VM_OK;
+}
+
+int vm_water_sec(vm_ctx* ctx, uint32_t shift) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  if (shift > 3) return fail(ctx, VM_E_INVALID, "water_sec shift %u outside 0..3", shift);
+  CK(cudaSetDevice(ctx->device));
+  const vm_frame& f = ctx->frame;
+  const uint32_t span = 1u << shift;
+  const size_t cells = (size_t)((f.res[0] + span - 1) >> shift) * ((f.res[1] + span - 1) >> shift);
+  if ((rc = ensure(ctx, ctx->ws_refr_key, cells * 8)) || (rc = ensure(ctx, ctx->ws_refr_t, cells * 4)) ||
+      (rc = ensure(ctx, ctx->ws_refl_key, cells * 8)) || (rc = ensure(ctx, ctx->ws_refl_t, cells * 4)))
+    return rc;
+  CK(vmk::launch_water_sec(f, dev_world(ctx), (const unsigned long long*)ctx->vis.p, shift,
+                           (unsigned long long*)ctx->ws_refr_key.p, (float*)ctx->ws_refr_t.p,
+                           (unsigned long long*)ctx->ws_refl_key.p, (float*)ctx->ws_refl_t.p, ctx->stream));
+  ctx->ws_shift = shift;
+  ctx->ws_cells = (uint32_t)cells;
+  ctx->ws_done = true;
+  return VM_OK;
+}
+
+static int read_dev(vm_ctx* ctx, void* dst, const void* src, size_t bytes);
+
+int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* refl_key, float* refl_t) {
+  if (!ctx || !ctx->ws_done) return ctx ? fail(ctx, VM_E_NOT_READY, "no vm_water_sec yet") : VM_E_INVALID;
+  const size_t n = ctx->ws_cells;
+  int rc = VM_OK;
+  if (refr_key && (rc = read_dev(ctx, refr_key, ctx->ws_refr_key.p, n * 8))) return rc;
+  if (refr_t && (rc = read_dev(ctx, refr_t, ctx->ws_refr_t.p, n * 4))) return rc;
+  if (refl_key && (rc = read_dev(ctx, refl_key, ctx->ws_refl_key.p, n * 8))) return rc;
+  if (refl_t && (rc = read_dev(ctx, refl_t, ctx->ws_refl_t.p, n * 4))) return rc;
   return VM_OK;
 }
 

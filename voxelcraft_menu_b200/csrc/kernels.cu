@@ -200,6 +200,64 @@ __global__ void __launch_bounds__(128) k_secondary(const vm_frame f, const DevWo
   }
 }
 
+// water_sec (resolve.wgsl:1468-1535): the engine's schedule of the water
+// legs, one per (1 << shift)^2 pixel block (WATER_SEC_SHIFT = 1: 2x2).  The
+// block's water pixel nearest the camera (smallest hit_t, the first in x-major
+// order on a tie) traces the refract leg (water_refract_leg, along the face
+// normal) and the reflect leg (water_reflect_leg, along water_ctx's
+// mirror_t); blocks without water, or legs their detail gate turns off, get
+// key 0.  Keys as the secondary keys (bit 61 clear: water), t the leg's hit
+// distance.
+__global__ void __launch_bounds__(128) k_water_sec(const vm_frame f, const DevWorld w,
+                                                   const unsigned long long* __restrict__ vis, uint32_t shift,
+                                                   unsigned long long* __restrict__ refr_key, float* __restrict__ refr_t,
+                                                   unsigned long long* __restrict__ refl_key,
+                                                   float* __restrict__ refl_t) {
+  const uint32_t span = 1u << shift;
+  const uint32_t hw = (f.res[0] + span - 1u) >> shift, hh = (f.res[1] + span - 1u) >> shift;
+  const uint32_t hx = blockIdx.x * 16u + threadIdx.x, hy = blockIdx.y * 8u + threadIdx.y;
+  if (hx >= hw || hy >= hh) return;
+  float best_t = 3.4e38f;
+  bool has = false;
+  KeyParts best = {};
+  uint32_t bpx = 0, bpy = 0;
+  for (uint32_t i = 0; i < span; ++i)
+    for (uint32_t j = 0; j < span; ++j) {
+      const uint32_t pxs = span * hx + i, pys = span * hy + j;
+      if (pxs >= f.res[0] || pys >= f.res[1]) continue;
+      const unsigned long long key = vis[(uint64_t)pys * f.res[0] + pxs];
+      if (key == 0ull) continue;
+      const KeyParts k = split_key(key);
+      const Chunk c = ld_chunk(w, k.ci);
+      if (block_at(w, c, k.vx, k.vy, k.vz) != VM_WATER) continue;
+      const F3 rd0 = ray_dir(f, (float)pxs + 0.5f, (float)pys + 0.5f);
+      const float ts = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd0);
+      if (ts < best_t) { best_t = ts; best = k; bpx = pxs; bpy = pys; has = true; }
+    }
+  unsigned long long kr = 0ull, km = 0ull;
+  float tr_ = 0.0f, tm = 0.0f;
+  if (has) {
+    const F3 rd = ray_dir(f, (float)bpx + 0.5f, (float)bpy + 0.5f);
+    const F3 hit = ld3(f.cam_pos) + rd * best_t;
+    SecRay s;
+    if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u &&
+        1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, best_t) > 0.0f) {
+      s.d = refract(rd, normal_of(best.nid), 1.0f / VM_WATER_IOR);
+      s.o = hit + s.d * VM_SURFACE_EPS;
+      s.max_dist = VM_WATER_REFRACT_DIST;
+      s.water = true;
+      secondary_trace<false>(w, f, s, &kr, &tr_, nullptr);
+    }
+    if (water_reflects(f, best_t)) {
+      s = reflect_ray<false>(w, f, hit, rd, best.nid, best_t, nullptr);
+      secondary_trace<false>(w, f, s, &km, &tm, nullptr);
+    }
+  }
+  const uint64_t h = (uint64_t)hy * hw + hx;
+  refr_key[h] = kr; refr_t[h] = tr_;
+  refl_key[h] = km; refl_t[h] = tm;
+}
+
 // Expanded visibility: voxel index over a world box, face id, hit_t.
 __global__ void __launch_bounds__(256) k_expand(const vm_frame f, const DevWorld w, const unsigned long long* __restrict__ vis,
                                                 int32_t wx, int32_t wy, int32_t wz, uint32_t dx, uint32_t dy, uint32_t dz,
@@ -273,6 +331,17 @@ cudaError_t launch_secondary(const vm_frame& f, const DevWorld& w, const unsigne
   if (f.res[0] == 0 || f.res[1] == 0) return cudaSuccess;
   dim3 g((f.res[0] + 15) / 16, (f.res[1] + 7) / 8);
   k_secondary<<<g, dim3(16, 8), 0, s>>>(f, w, vis, sec_key, sec_t, refl_key, refl_t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_water_sec(const vm_frame& f, const DevWorld& w, const unsigned long long* vis, uint32_t shift,
+                             unsigned long long* refr_key, float* refr_t, unsigned long long* refl_key,
+                             float* refl_t, cudaStream_t s) {
+  const uint32_t span = 1u << shift;
+  const uint32_t hw = (f.res[0] + span - 1u) >> shift, hh = (f.res[1] + span - 1u) >> shift;
+  if (hw == 0 || hh == 0) return cudaSuccess;
+  k_water_sec<<<dim3((hw + 15) / 16, (hh + 7) / 8), dim3(16, 8), 0, s>>>(f, w, vis, shift, refr_key, refr_t, refl_key,
+                                                                           refl_t);
   return cudaGetLastError();
 }
 

@@ -106,6 +106,11 @@ cudaError_t launch_primary_shadow(const vm_frame& f, const vmd::DevWorld& w, con
 cudaError_t launch_secondary(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                              unsigned long long* sec_key, float* sec_t, unsigned long long* refl_key, float* refl_t,
                              cudaStream_t s);
+// water_sec (resolve.wgsl:1468-1535): refract and reflect legs of each
+// (1 << shift)^2 block's nearest water pixel, ceil(res / (1 << shift)) cells
+cudaError_t launch_water_sec(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis, uint32_t shift,
+                             unsigned long long* refr_key, float* refr_t, unsigned long long* refl_key,
+                             float* refl_t, cudaStream_t s);
 // n blocker distances as binary16 (the engine's R16F shadow target), rounded
 // to nearest even; in and out 16-byte / 8-byte aligned
 cudaError_t launch_to_r16f(const float* in, uint16_t* out, uint64_t n, int sms, cudaStream_t s);

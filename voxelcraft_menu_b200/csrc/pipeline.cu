@@ -430,8 +430,8 @@ __device__ __noinline__ void enqueue_reflect(const PipeArgs& a, uint32_t v, uint
     const Chunk c = ld_chunk(world_of(a, view_of(a, v)), k.ci);
     const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
     const float th = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
-    if (water_reflects(f, k.nid, th)) {
-      rr = reflect_ray(ld3(f.cam_pos) + rd * th, rd, k.nid);
+    if (water_reflects(f, th)) {
+      rr = reflect_ray<false>(world_of(a, view_of(a, v)), f, ld3(f.cam_pos) + rd * th, rd, k.nid, th, nullptr);
       want = true;
     }
   }

@@ -2,6 +2,7 @@
 // set-up of shadow_guide and the one water / glass secondary ray per hit.
 #pragma once
 #include "march_device.cuh"
+#include "water.cuh"
 
 namespace vmk {
 using namespace vmd;
@@ -116,21 +117,20 @@ __device__ __forceinline__ bool secondary_setup(const DevWorld& w, const vm_fram
 
 // The reflect leg of a water hit (water_reflect_leg, resolve.wgsl:1044-1058,
 // scheduled by water_sec resolve.wgsl:1526-1528): gated by FLAG_WATER_REFLECT
-// and reflect_detail > 0 (resolve.wgsl:1099); from hit + n * SURFACE_EPS
-// along reflect(rd, n), 768 voxels, water transparent.  n is the face normal:
-// water_ctx's nt equals it unless the surface is waved (FLAG_WAVES on a +Y
-// face, resolve.wgsl:1107), whose wave normal is not restated here; such
-// pixels get no reflect ray.
-__device__ __forceinline__ bool water_reflects(const vm_frame& f, uint32_t nid, float t) {
+// and reflect_detail > 0 (resolve.wgsl:1099); from hit + n * SURFACE_EPS (the
+// face normal) along water_ctx's mirror_t (water.cuh: the face normal's
+// reflection, or the wave normal's on a waved +Y face), 768 voxels, water
+// transparent.
+__device__ __forceinline__ bool water_reflects(const vm_frame& f, float t) {
   if ((f.flags & VM_FLAG_WATER_REFLECT) == 0u) return false;
-  if ((f.flags & VM_FLAG_WAVES) != 0u && nid == VM_NORMAL_PY) return false;
   return 1.0f - smoothstep(VM_WATER_REFLECT_NEAR, VM_WATER_REFLECT_FAR, t) > 0.0f;
 }
-__device__ __forceinline__ SecRay reflect_ray(F3 hit, F3 rd, uint32_t nid) {
-  const F3 n = normal_of(nid);
+template <bool COUNT>
+__device__ __forceinline__ SecRay reflect_ray(const DevWorld& w, const vm_frame& f, F3 hit, F3 rd, uint32_t nid,
+                                              float t, Traffic* tr) {
   SecRay s;
-  s.o = hit + n * VM_SURFACE_EPS;
-  s.d = reflect(rd, n);
+  s.o = hit + normal_of(nid) * VM_SURFACE_EPS;
+  s.d = water_mirror_t<COUNT>(w, f, nid, hit, rd, t, tr);
   s.max_dist = VM_WATER_REFLECT_DIST;
   s.water = true;
   return s;
@@ -143,8 +143,8 @@ __device__ __forceinline__ bool reflect_setup(const DevWorld& w, const vm_frame&
   if (block_at(w, c, k.vx, k.vy, k.vz) != VM_WATER) return false;
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
-  if (!water_reflects(f, k.nid, t)) return false;
-  *s = reflect_ray(ld3(f.cam_pos) + rd * t, rd, k.nid);
+  if (!water_reflects(f, t)) return false;
+  *s = reflect_ray<false>(w, f, ld3(f.cam_pos) + rd * t, rd, k.nid, t, nullptr);
   return true;
 }
 

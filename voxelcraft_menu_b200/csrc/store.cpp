@@ -717,6 +717,12 @@ int vmw_build_view(const vmw_world* wc, const vmw_camera* cam, vm_frame* frame, 
   frame->water_absorb = 1.0f;
   memcpy(frame->jitter, cam->jitter, sizeof frame->jitter);
   frame->taa_feedback = 1.0f;
+  // the wave parameters of the engine's default configuration
+  // (src/config.rs:318-321 through src/render/mod.rs:1690-1694)
+  frame->wave_amp = 0.12f;
+  frame->wave_scale = 32.0f;
+  frame->wave_speed = 0.32f;
+  frame->wave_reflect_slope = 0.0f;
   frame->frame_index = cam->frame_index % 64u;
   return 0;
 }

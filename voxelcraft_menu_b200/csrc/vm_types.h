@@ -170,6 +170,9 @@ static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
 #define VM_FLAG_WATER_REFRACT 32u
 #define VM_FLAG_UNDERWATER 64u
 #define VM_FLAG_WAVES 512u
+#define VM_FLAG_WAVE_ANISO 1024u
+#define VM_FLAG_WAVE_SHOAL 2048u
+#define VM_FLAG_WAVE_FILL 4096u
 #define VM_FLAG_WATER_FAR 2097152u
 #define VM_FLAG_WATER_DARK 4194304u
 /* Soft sun shadows (an extension; the engine filters one blocker distance

@@ -1,0 +1,116 @@
+// The water surface of a hit: the reflect direction of water_ctx
+// (resolve.wgsl:1078-1166), which on a waved surface comes from the wave
+// field (wave_octave / wave_field / wave_normal, resolve.wgsl:902-975) with
+// its anisotropic filter, the shoal-depth damping (a short downward
+// trace_world) and the optical roughness that pulls the normal back to the
+// face normal.  Compiled with the march's float contract; cos and exp are
+// CUDA's, the oracle uses the host's, so on a waved surface with a positive
+// reflect slope the direction can differ in its last bits.  With the
+// engine's default slope of 0 the traced normal is the face normal whatever
+// the wave field is, and the direction is exact.
+#pragma once
+#include "march_device.cuh"
+
+namespace vmd {
+
+constexpr float WAVE_TAU = 6.28318531f;
+constexpr float WAVE_GRAZE_MIN = 1e-3f;
+constexpr float SHOAL_DEPTH = 6.0f;
+constexpr float WAVE_FILTER_K = 1.0f;
+
+// one octave: slope vector and the unresolved slope variance it leaves
+__device__ __forceinline__ F3 wave_octave(float px_, float pz_, float dx, float dz, float lambda, float slope,
+                                          float phase, float px, float vhx, float vhz, float kk, bool aniso) {
+  float fade;
+  if (aniso) {
+    const float d = dx * vhx + dz * vhz;
+    const float ext = px * sqrtf(1.0f + kk * d * d);
+    const float u = ext / lambda;
+    fade = expf(-WAVE_FILTER_K * u * u);
+  } else {
+    fade = smoothstep(2.0f, 4.0f, lambda / fmaxf(px, 1e-4f));
+  }
+  const float s = slope * fade * cosf(WAVE_TAU / lambda * (px_ * dx + pz_ * dz) + phase);
+  return {dx * s, dz * s, 0.5f * slope * slope * (1.0f - fade * fade)};
+}
+
+// wave_field: the sum of the octaves (8 with FLAG_WAVE_FILL, else 4)
+__device__ __forceinline__ F3 wave_field(const vm_frame& f, float x, float z, float px, float vhx, float vhz, float kk,
+                                         bool aniso, float shoal) {
+  const float l0 = f.wave_scale;
+  const float a = f.wave_amp * shoal;
+  const float ph = f.time * f.wave_speed * WAVE_TAU;
+  F3 s = {0.0f, 0.0f, 0.0f};
+  if ((f.flags & VM_FLAG_WAVE_FILL) != 0u) {
+    const float dir[8][2] = {{-0.438371f, 0.898794f}, {-0.927184f, 0.374607f}, {-0.190809f, 0.981627f},
+                             {-0.669131f, 0.743145f}, {0.121869f, 0.992546f},  {0.694658f, 0.719340f},
+                             {0.970296f, 0.241922f},  {0.438371f, 0.898794f}};
+    const float div[8] = {1.0f, 1.3934f, 1.9417f, 2.7056f, 3.7700f, 5.2533f, 7.3201f, 10.2000f};
+    const float amp[8] = {0.3086f, 0.2584f, 0.2163f, 0.1810f, 0.1515f, 0.1269f, 0.1062f, 0.0889f};
+    const float phm[8] = {1.0000f, 1.1804f, 1.3934f, 1.6449f, 1.9417f, 2.2920f, 2.7056f, 3.1937f};
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const float lambda = i == 0 ? l0 : l0 / div[i];
+      s = s + wave_octave(x, z, dir[i][0], dir[i][1], lambda, a * amp[i], ph * phm[i], px, vhx, vhz, kk, aniso);
+    }
+    return s;
+  }
+  const float dir[4][2] = {{0.913089f, 0.407760f}, {-0.388685f, 0.921371f}, {-0.980382f, -0.197108f},
+                           {0.477328f, -0.878725f}};
+  const float div[4] = {1.0f, 2.17f, 4.71f, 10.20f};
+  const float amp[4] = {0.42f, 0.27f, 0.19f, 0.12f};
+  const float phm[4] = {1.0000f, 1.4731f, 2.1703f, 3.1937f};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float lambda = i == 0 ? l0 : l0 / div[i];
+    s = s + wave_octave(x, z, dir[i][0], dir[i][1], lambda, a * amp[i], ph * phm[i], px, vhx, vhz, kk, aniso);
+  }
+  return s;
+}
+
+__device__ __forceinline__ F3 unit(F3 v) {   // WGSL normalize: v / sqrt(dot(v, v))
+  const float l = sqrtf(dot(v, v));
+  return {v.x / l, v.y / l, v.z / l};
+}
+
+// The direction water_reflect_leg traces from a water hit (water_ctx's
+// mirror_t): reflect(rd, nt), with nt the wave normal for FLAG_WAVES on a +Y
+// face, limited by wave_reflect_slope and pulled to the face normal by the
+// optical roughness; a waved direction never points below the horizon.
+template <bool COUNT>
+__device__ __forceinline__ F3 water_mirror_t(const DevWorld& w, const vm_frame& f, uint32_t nid, F3 hit, F3 rd,
+                                             float t, Traffic* tr) {
+  const F3 n = normal_of(nid);
+  F3 nt = n;
+  float unresolved = 0.0f;
+  const bool waved = (f.flags & VM_FLAG_WAVES) != 0u && nid == VM_NORMAL_PY;
+  if (waved) {
+    const float px_world = fmaxf(t, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1];
+    float kk = 0.0f, vhx = 0.0f, vhz = 0.0f;
+    const bool aniso = (f.flags & VM_FLAG_WAVE_ANISO) != 0u;
+    if (aniso) {
+      const float k = 1.0f / fmaxf(fabsf(rd.y), WAVE_GRAZE_MIN);
+      kk = k * k - 1.0f;
+      const float r = 1.0f / sqrtf(fmaxf(rd.x * rd.x + rd.z * rd.z, 1e-12f));
+      vhx = rd.x * r; vhz = rd.z * r;
+    }
+    float shoal = 1.0f;
+    if ((f.flags & VM_FLAG_WAVE_SHOAL) != 0u) {
+      const F3 dro = {floorf(hit.x) + 0.5f, hit.y - VM_SURFACE_EPS, floorf(hit.z) + 0.5f};
+      const WorldHit dh = trace_world<true, COUNT>(w, f, dro, f3(0.001f, -0.999999f, 0.001f), SHOAL_DEPTH, tr);
+      shoal = smoothstep(0.0f, SHOAL_DEPTH, dh.hit ? dh.t : SHOAL_DEPTH);
+    }
+    const F3 wf = wave_field(f, hit.x, hit.z, px_world, vhx, vhz, kk, aniso, shoal);
+    unresolved = fmaxf(wf.z, 0.0f);
+    const float gl = sqrtf(wf.x * wf.x + wf.y * wf.y);
+    const float lim = fminf(1.0f, f.wave_reflect_slope / fmaxf(gl, 1e-6f));
+    nt = unit(f3(-(wf.x * lim), 1.0f, -(wf.y * lim)));   // wave_normal
+  }
+  const float rough = fminf(fmaxf(1.0f - expf(-8.0f * unresolved), 0.0f), 1.0f);
+  nt = unit(nt * (1.0f - rough) + n * rough);              // normalize(mix(nt, n, rough))
+  F3 m = reflect(rd, nt);
+  if (waved) m = unit(f3(m.x, fmaxf(m.y, 0.0f), m.z));
+  return m;
+}
+
+}  // namespace vmd

@@ -209,6 +209,23 @@ class Marcher:
         self._ck(self._L.vm_read_reflection(self._h, ptr(k), ptr(t)))
         return k, t
 
+    def water_sec(self, shift: int = 1):
+        """The engine's water-leg schedule (water_sec, resolve.wgsl:1468-1535)
+        over the last frame's visibility, one leg pair per 2^shift square."""
+        self._ck(self._L.vm_water_sec(self._h, shift))
+        self._ws_shift = shift
+
+    def read_water_sec(self):
+        """(refract key, refract t, reflect key, reflect t) per water_sec cell,
+        shaped (ceil(h / 2^shift), ceil(w / 2^shift))."""
+        w, h = int(self.view.frame.res[0]), int(self.view.frame.res[1])
+        sp = 1 << self._ws_shift
+        shape = ((h + sp - 1) // sp, (w + sp - 1) // sp)
+        out = [np.empty(shape, np.uint64), np.empty(shape, np.float32), np.empty(shape, np.uint64),
+               np.empty(shape, np.float32)]
+        self._ck(self._L.vm_read_water_sec(self._h, *(ptr(a) for a in out)))
+        return tuple(out)
+
     def read_shadow_mask(self, out: np.ndarray | None = None) -> np.ndarray:
         """clamp(1 - occlusion, 0, 1) per pixel after soften_shadows; 1 = lit."""
         out = np.empty(self._npix(), np.float32) if out is None else out

@@ -143,6 +143,8 @@ _SIGNATURES = [
     ("vm_set_tuning", C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
     ("vm_set_packet", C.c_int, [vp, C.c_int]),
     ("vm_set_spec", C.c_int, [vp, C.c_uint32]),
+    ("vm_water_sec", C.c_int, [vp, C.c_uint32]),
+    ("vm_read_water_sec", C.c_int, [vp, vp, vp, vp, vp]),
     ("vm_read_vis", C.c_int, [vp, vp]),
     ("vm_read_hiz", C.c_int, [vp, vp]),
     ("vm_write_hiz", C.c_int, [vp, vp]),
