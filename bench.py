@@ -443,11 +443,13 @@ def bench_sparse(local, fit_steps=50):
     from voxelcraft_menu_b200.march import Marcher
     rec = W.recipe_sparse_world()
     w = W.World.generate(rec)
-    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_SOFT_SHADOWS
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT
     frames = [V.ragged_views(w, flags=flags, jitter=W.halton_jitter(k), frame_index=k) for k in range(8)]
     n_views = len(frames[0])
     px = sum(v.n_pixels for v in frames[0])
     m = Marcher(1024, 1024, device=local, max_views=n_views, max_batch_pixels=px)
+    from voxelcraft_menu_b200.march import SPEC_DEFAULT, SPEC_SOFT_RAYS
+    m.set_spec(SPEC_DEFAULT | SPEC_SOFT_RAYS)
     stream = torch.cuda.current_stream()
     m._ck(m._L.vm_set_stream(m._h, __import__("ctypes").c_void_p(stream.cuda_stream)))
     m.upload_world(*w.pools())

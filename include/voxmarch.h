@@ -95,9 +95,9 @@ int vm_secondary(vm_ctx* ctx);
  * r16float target stores them and the horizontal pass is rounded as its
  * rg16float target stores it.  Output (vm_read_shadow_mask): per pixel the
  * shadow mask clamp(1 - occlusion, 0, 1) as a float, the value the engine
- * quantises into its r8unorm target; 1 = lit.  Frames with
- * VM_FLAG_SOFT_SHADOWS (jittered rays, whose shadow buffer holds blocked
- * fractions) are rejected with VM_E_INVALID. */
+ * quantises into its r8unorm target; 1 = lit.  A context with
+ * VM_SPEC_SOFT_RAYS (jittered rays, whose shadow buffer holds blocked
+ * fractions) is rejected with VM_E_INVALID. */
 int vm_soften_shadows(vm_ctx* ctx, uint32_t radius_limit, float penumbra);
 
 /* The same frame as vm_select + vm_march + vm_primary_shadow + vm_secondary
@@ -125,7 +125,9 @@ int vm_set_packet(vm_ctx* ctx, int pixels_per_lane);
  * water-interface repair (--legacy-water), leaf cutouts (--no-leaf-cutout),
  * glass as its own surface, emitters without sun shadow, tufts as foliage, the
  * Snell bend of underwater primary rays (--snell-bend) and the leaf fill
- * (--no-leaf-thin).  Unknown bits: VM_E_INVALID. */
+ * (--no-leaf-thin).  VM_SPEC_SOFT_RAYS (an extension, no engine counterpart)
+ * traces VM_SOFT_SAMPLES jittered sun rays per lit-facing hit and stores the
+ * blocked fraction in the shadow buffer.  Unknown bits: VM_E_INVALID. */
 int vm_set_spec(vm_ctx* ctx, uint32_t spec);
 
 /* Read-backs (synchronise the context's stream). */
@@ -270,7 +272,7 @@ typedef struct vm_shade_consts {
 typedef struct vm_shade_gbuf {
   uint32_t code;           /* id | face << 8 | HIT 1<<11 | LIT 1<<12 | TRACED 1<<13 | HIT2 1<<14 | FLIP 1<<15
                               | id2 << 16 | face2 << 24 (id2 / face2: the refracted ray's hit)
-                              | blocked soft-shadow rays << 27 | SOFT 1<<30 (VM_FLAG_SOFT_SHADOWS) */
+                              | blocked soft-shadow rays << 27 | SOFT 1<<30 (VM_SPEC_SOFT_RAYS) */
   float t;                 /* primary hit distance (0 for sky) */
   float d;                 /* water refraction leg length */
   float fog;               /* fog optical length per unit density (0 for sky) */

@@ -29,6 +29,7 @@ SPEC_FULL_MARCH, SPEC_WATER_REPAIR, SPEC_LEAF_CUTOUT, SPEC_GLASS = 1, 2, 4, 8
 SPEC_EMITTER_GATHER, SPEC_FOLIAGE, SPEC_SNELL_BEND, SPEC_LEAF_THIN = 16, 32, 64, 128
 SPEC_DEFAULT = SPEC_FULL_MARCH | SPEC_WATER_REPAIR | SPEC_LEAF_CUTOUT | SPEC_GLASS | SPEC_EMITTER_GATHER | \
     SPEC_FOLIAGE | SPEC_LEAF_THIN
+SPEC_SOFT_RAYS = 256      # extension: jittered sun rays per hit, the shadow buffer holds the blocked fraction
 
 
 class OrHit(C.Structure):
@@ -102,6 +103,7 @@ class Oracle:
         ch, i, l, b, g = self._keep
         self.w = OrWorld(C.cast(C.pointer(self.frame), vp), _p(ch), len(ch), _p(i), i.size // 4, _p(l), l.size // 2,
                          _p(b), b.size, _p(g), g.size, spec)
+        self.spec = spec
         self.threads = threads
         self.L.or_clear_error()
 

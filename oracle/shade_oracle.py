@@ -20,7 +20,7 @@ WATER = 13
 G_HIT, G_LIT, G_TRACED, G_HIT2, G_FLIP = 1 << 11, 1 << 12, 1 << 13, 1 << 14, 1 << 15
 G_SOFT, G_SOFT_SHIFT = 1 << 30, 27        # soft shadows: blocked rays of SOFT_SAMPLES in bits 27-29
 SOFT_SAMPLES = 4
-FLAG_SOFT_SHADOWS = 0x40000000
+SPEC_SOFT_RAYS = 256                      # VM_SPEC_SOFT_RAYS: jittered rays, blocked fraction
 
 NORMALS = np.array([[-1, 0, 0], [1, 0, 0], [0, -1, 0], [0, 1, 0], [0, 0, -1], [0, 0, 1],
                     [0.70710678, 0, -0.70710678], [0.70710678, 0, 0.70710678]], np.float64)
@@ -58,7 +58,7 @@ def gbuffer_from_oracle(oracle, vis, shadow, sec_key, sec_t, fog_falloff, fog_he
         nid = (key >> 37) & 7
         bid = oracle.block_at(ci, v)
         c = (bid & 0xFF) | (nid << 8) | G_HIT | (G_LIT if shadow[i] == 0.0 else 0)
-        if int(f.flags) & FLAG_SOFT_SHADOWS:
+        if int(oracle.spec) & SPEC_SOFT_RAYS:
             c |= G_SOFT | (int(float(shadow[i]) * SOFT_SAMPLES + 0.5) << G_SOFT_SHIFT)
         nf = NORMALS[nid].astype(np.float32)
         if nid >= 6 and (nf[0] * rd[0] + nf[1] * rd[1]) + nf[2] * rd[2] > np.float32(0.0):

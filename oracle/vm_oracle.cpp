@@ -299,7 +299,7 @@ inline uint32_t hash_u32(uint32_t x) {
   return h;
 }
 
-// Soft shadows (VM_FLAG_SOFT_SHADOWS, an extension of the engine): the s-th
+// Soft shadows (VM_SPEC_SOFT_RAYS, an extension of the engine): the s-th
 // jittered sun direction of pixel (px, py): the sun's tangent basis from a
 // fixed up vector, one rotation of the shared disk pattern picked by hash_u32
 // of pixel and frame, the offset added in the tangent plane, normalised.
@@ -1185,7 +1185,7 @@ int or_primary_shadow(const or_world* o, const uint64_t* vis, float* out, uint64
               float scale = chunk_at(w, ci).voxel_size;
               if (t >= 0.0f) {
                 const V3 origin = add(hit, muls(n, 0.02f * scale));
-                if ((f.flags & VM_FLAG_SOFT_SHADOWS) != 0u) {
+                if ((w.spec & VM_SPEC_SOFT_RAYS) != 0u) {
                   uint32_t blocked = 0;
                   for (uint32_t s = 0; s < VM_SOFT_SAMPLES; ++s) {
                     cnt_add(&Counters::rays);

@@ -16,7 +16,7 @@ import math
 import numpy as np
 import pytest
 
-from oracle.oracle import Oracle, f16_round
+from oracle.oracle import SPEC_DEFAULT, SPEC_SOFT_RAYS, Oracle, f16_round
 from voxelcraft_menu_b200 import world as W
 
 MASK_ATOL = 1e-3            # |GPU - oracle| at every pixel
@@ -170,8 +170,7 @@ def test_gpu_soften_rejects_bad_arguments(small):
         for limit, pen in ((0, 1.5), (9, 1.5), (4, 0.0), (4, math.inf), (4, math.nan)):
             with pytest.raises(RuntimeError):
                 m.soften_shadows(limit, pen)
-        f = W.penumbra_camera(flags=W.FLAG_SHADOWS | W.FLAG_SOFT_SHADOWS)
-        m.upload_view(w.view(f))
+        m.set_spec(SPEC_DEFAULT | SPEC_SOFT_RAYS)
         m.render()
         with pytest.raises(RuntimeError):
             m.soften_shadows(4, 1.5)               # jittered rays: blocked fractions, not distances

@@ -11,10 +11,11 @@ import math
 import numpy as np
 import pytest
 
-from oracle.oracle import Oracle
+from oracle.oracle import SPEC_DEFAULT, SPEC_SOFT_RAYS, Oracle
 from voxelcraft_menu_b200 import world as W
 
-SOFT = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_SOFT_SHADOWS
+SOFT = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT
+SOFT_SPEC = SPEC_DEFAULT | SPEC_SOFT_RAYS
 
 
 @pytest.fixture(scope="module")
@@ -44,7 +45,7 @@ def sparse_views(rec, w, n, size, seed=21):
 def test_soft_directions_stay_in_the_disk(small):
     w, pools = small
     v = w.view(W.small_terrain_camera(width=64, height=36, flags=SOFT))
-    o = Oracle(v, *pools)
+    o = Oracle(v, *pools, spec=SOFT_SPEC)
     sun = np.array(v.frame.sun_dir, np.float64)
     seen = set()
     for py in range(0, 36, 7):
@@ -77,6 +78,7 @@ def test_soft_shadows_match_the_oracle(small):
     from voxelcraft_menu_b200.march import Marcher
     w, pools = small
     m = Marcher(640, 360)
+    m.set_spec(SOFT_SPEC)
     m.upload_world(*pools)
     v = w.view(W.small_terrain_camera(width=320, height=180, flags=SOFT))
     m.upload_view(v)
@@ -84,7 +86,7 @@ def test_soft_shadows_match_the_oracle(small):
     vis, sh = m.read_vis(), m.read_shadow()
     m.render_passes()
     assert np.array_equal(m.read_vis(), vis) and np.array_equal(m.read_shadow(), sh)
-    o = Oracle(v, *pools)
+    o = Oracle(v, *pools, spec=SOFT_SPEC)
     ovis, _, _ = o.frame_vis()
     osh = o.shadow(ovis)
     assert np.array_equal(vis, ovis)
@@ -102,13 +104,14 @@ def test_halton_jittered_frames_match_the_oracle(small):
     from voxelcraft_menu_b200.march import Marcher
     w, pools = small
     m = Marcher(640, 360)
+    m.set_spec(SOFT_SPEC)
     m.upload_world(*pools)
     for k in (1, 6):
         cam = W.small_terrain_camera(width=160, height=90, flags=SOFT, jitter=W.halton_jitter(k), frame_index=k)
         v = w.view(cam)
         m.upload_view(v)
         m.render()
-        o = Oracle(v, *pools)
+        o = Oracle(v, *pools, spec=SOFT_SPEC)
         ovis, _, _ = o.frame_vis()
         assert np.array_equal(m.read_vis(), ovis)
         assert np.array_equal(m.read_shadow().view(np.uint32), o.shadow(ovis).view(np.uint32))
@@ -120,6 +123,7 @@ def test_sparse_world_views_match_the_oracle(sparse):
     rec, w, pools = sparse
     views = sparse_views(rec, w, 3, 96)
     m = Marcher(1024, 1024)
+    m.set_spec(SOFT_SPEC)
     m.upload_world(*pools)
     m.batch_set(views)
     m.batch_run(secondary=True)
@@ -128,7 +132,7 @@ def test_sparse_world_views_match_the_oracle(sparse):
     off = 0
     for v in views:
         n = v.n_pixels
-        o = Oracle(v, *pools)
+        o = Oracle(v, *pools, spec=SOFT_SPEC)
         ovis, _, _ = o.frame_vis()
         assert np.array_equal(bv[off:off + n], ovis)
         assert np.array_equal(bs[off:off + n].view(np.uint32), o.shadow(ovis).view(np.uint32))
@@ -151,6 +155,7 @@ def test_sparse_soft_gbuffer_and_gradient_match_fp64(sparse):
     rec, w, pools = sparse
     views = V.ragged_views(w, n=3, sizes=(96, 128), flags=SOFT, jitter=W.halton_jitter(3), frame_index=3)
     m = Marcher(1024, 1024)
+    m.set_spec(SOFT_SPEC)
     m.upload_world(*pools)
     m.batch_set(views)
     m.batch_run(secondary=True)
@@ -159,7 +164,7 @@ def test_sparse_soft_gbuffer_and_gradient_match_fp64(sparse):
     got = gb.cpu().numpy().view(S.GBUF_DTYPE)
     want = []
     for v in views:
-        o = Oracle(v, *pools)
+        o = Oracle(v, *pools, spec=SOFT_SPEC)
         ovis, _, _ = o.frame_vis()
         sk, st = o.secondary(ovis)
         want.append(SO.gbuffer_from_oracle(o, ovis, o.shadow(ovis), sk, st, k.fog_falloff, k.fog_height))

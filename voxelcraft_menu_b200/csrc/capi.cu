@@ -405,7 +405,8 @@ int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_
 
 int vm_set_spec(vm_ctx* ctx, uint32_t spec) {
   if (!ctx) return VM_E_INVALID;
-  if ((spec & ~VM_SPEC_ALL) != 0u) return fail(ctx, VM_E_INVALID, "unknown VM_SPEC bits 0x%x", spec & ~VM_SPEC_ALL);
+  const uint32_t known = VM_SPEC_ALL | VM_SPEC_SOFT_RAYS;
+  if ((spec & ~known) != 0u) return fail(ctx, VM_E_INVALID, "unknown VM_SPEC bits 0x%x", spec & ~known);
   if (spec != ctx->spec) drop_graph(ctx);
   ctx->spec = spec;
   return VM_OK;
@@ -480,7 +481,7 @@ int vm_soften_shadows(vm_ctx* ctx, uint32_t radius_limit, float penumbra) {
     return fail(ctx, VM_E_INVALID, "radius limit %u outside 1..%u", radius_limit, vmk::SOFTEN_MAX_LIMIT);
   if (!(penumbra > 0.0f) || !(penumbra < 1e30f))
     return fail(ctx, VM_E_INVALID, "penumbra must be positive and finite");
-  if (ctx->frame.flags & VM_FLAG_SOFT_SHADOWS)
+  if (ctx->spec & VM_SPEC_SOFT_RAYS)
     return fail(ctx, VM_E_INVALID, "the filter reads blocker distances; this frame's shadow buffer holds the "
                                    "blocked fractions of jittered rays");
   CK(cudaSetDevice(ctx->device));

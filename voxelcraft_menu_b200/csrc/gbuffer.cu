@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(256) k_gbuffer(const __grid_constant__ PipeArg
       g.fog = fog_length(f.cam_pos[1], g.t, rd.y, sk);
       const float sh = a.shadow[gp];
       g.code = (id & 0xFFu) | (k.nid << 8) | G_HIT | (sh == 0.0f ? G_LIT : 0u);
-      if ((f.flags & VM_FLAG_SOFT_SHADOWS) != 0u)   // the blocked fraction of VM_SOFT_SAMPLES rays
+      if ((a.spec & VM_SPEC_SOFT_RAYS) != 0u)   // the blocked fraction of VM_SOFT_SAMPLES rays
         g.code |= G_SOFT | ((uint32_t)(sh * (float)VM_SOFT_SAMPLES + 0.5f) << G_SOFT_SHIFT);
       // cross-quad normals face the ray (shadow.wgsl:23)
       if (k.nid >= VM_NORMAL_CROSS_A && dot(normal_of(k.nid), rd) > 0.0f) g.code |= G_FLIP;

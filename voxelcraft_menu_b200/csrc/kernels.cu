@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(128) k_primary_shadow(const vm_frame f, const 
   float distance = 0.0f;
   F3 o;
   if (shadow_active(f) && shadow_setup(w, f, vis[pix], px, py, &o)) {
-    if (soft_shadows(f)) {
+    if (soft_shadows(w.spec)) {
       // the blocked fraction of the jittered rays
       uint32_t blocked = 0;
       for (uint32_t s = 0; s < VM_SOFT_SAMPLES; ++s)

@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
           sample = 0u;
           blocked = 0u;
           const vm_frame& f = frame_t<SINGLE>(a, view);
-          s = shadow_walk_begin(origin, soft_shadows(f) ? soft_sun_dir(f, pix % f.res[0], pix / f.res[0], 0u)
+          s = shadow_walk_begin(origin, soft_shadows(a.spec) ? soft_sun_dir(f, pix % f.res[0], pix / f.res[0], 0u)
                                                         : ld3(f.sun_dir));
           has = true;
           if (COUNT) ++ns;
@@ -693,7 +693,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
       const DevWorld w = world_of(a, vd);
       float b;
       if (shadow_walk_step<COUNT>(w, f, s, f.shadow_dist, &b, &tr)) {
-        if (!soft_shadows(f)) {
+        if (!soft_shadows(a.spec)) {
           a.shadow[vd.pix_off + pix] = blocker_distance(b);
           has = false;
         } else {

@@ -57,13 +57,13 @@ __device__ __forceinline__ bool shadow_setup(const DevWorld& w, const vm_frame& 
   return true;
 }
 
-// Soft shadows (VM_FLAG_SOFT_SHADOWS): the s-th jittered sun direction of
+// Soft shadows (VM_SPEC_SOFT_RAYS): the s-th jittered sun direction of
 // pixel (px, py) at the frame's frame_index.  Tangent basis of the sun
 // direction from a fixed up vector, one of VM_SOFT_ROTATIONS rotations of the
 // disk pattern per pixel (the engine's hash_u32 of pixel and frame), offset
 // added in the tangent plane, normalised (v / sqrt(dot)).
 __device__ static const float g_soft_disk[VM_SOFT_ROTATIONS][VM_SOFT_SAMPLES][2] = VM_SOFT_DISK_INIT;
-__device__ __forceinline__ bool soft_shadows(const vm_frame& f) { return (f.flags & VM_FLAG_SOFT_SHADOWS) != 0u; }
+__device__ __forceinline__ bool soft_shadows(uint32_t spec) { return (spec & VM_SPEC_SOFT_RAYS) != 0u; }
 __device__ __forceinline__ F3 soft_sun_dir(const vm_frame& f, uint32_t px, uint32_t py, uint32_t s) {
   const F3 sun = ld3(f.sun_dir);
   const F3 up = fabsf(sun.y) < 0.99f ? f3(0.0f, 1.0f, 0.0f) : f3(1.0f, 0.0f, 0.0f);

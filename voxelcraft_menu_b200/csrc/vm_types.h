@@ -179,7 +179,7 @@ static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
  * instead, shadow.wgsl:49-116): VM_SOFT_SAMPLES rays per lit-facing hit, the
  * sun direction offset inside a 0.02 rad disk, and the shadow buffer holds the
  * blocked fraction.  A bit the engine's flag set leaves free. */
-#define VM_FLAG_SOFT_SHADOWS 0x40000000u
+
 #define VM_SOFT_SAMPLES 4u
 #define VM_SOFT_ROTATIONS 16u
 /* Offsets in the sun's tangent plane (radians, radius 0.02): 16 rotations of
@@ -253,6 +253,11 @@ static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
 #define VM_SPEC_DEFAULT (VM_SPEC_FULL_MARCH | VM_SPEC_WATER_REPAIR | VM_SPEC_LEAF_CUTOUT | VM_SPEC_GLASS | \
                          VM_SPEC_EMITTER_GATHER | VM_SPEC_FOLIAGE | VM_SPEC_LEAF_THIN)
 #define VM_SPEC_ALL 255u
+/* Extension, outside the engine's spec set: soft shadows, VM_SOFT_SAMPLES jittered
+ * sun rays per lit-facing hit whose shadow buffer entry is the blocked fraction.
+ * Every bit of the engine's frame flags word is taken, so the switch is a
+ * specialisation of the context, not a frame flag. */
+#define VM_SPEC_SOFT_RAYS 256u
 #define VM_SURFACE_EPS 0.02f          /* common.wgsl:1258 */
 #define VM_WATER_IOR 1.333f           /* common.wgsl:1256 */
 #define VM_WATER_REFRACT_DIST 96.0f   /* resolve.wgsl:879 */

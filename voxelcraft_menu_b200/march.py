@@ -30,6 +30,7 @@ SPEC_FULL_MARCH, SPEC_WATER_REPAIR, SPEC_LEAF_CUTOUT, SPEC_GLASS = 1, 2, 4, 8
 SPEC_EMITTER_GATHER, SPEC_FOLIAGE, SPEC_SNELL_BEND, SPEC_LEAF_THIN = 16, 32, 64, 128
 SPEC_DEFAULT = SPEC_FULL_MARCH | SPEC_WATER_REPAIR | SPEC_LEAF_CUTOUT | SPEC_GLASS | SPEC_EMITTER_GATHER | \
     SPEC_FOLIAGE | SPEC_LEAF_THIN
+SPEC_SOFT_RAYS = 256      # extension: VM_SOFT_SAMPLES jittered sun rays per hit, blocked fraction
 
 
 class MarchError(RuntimeError):

@@ -27,7 +27,6 @@ FLAG_UNDERWATER = 64
 FLAG_WAVES = 512
 FLAG_WATER_FAR = 2097152
 FLAG_WATER_DARK = 4194304
-FLAG_SOFT_SHADOWS = 0x40000000      # extension: 4 jittered sun rays per hit, blocked fraction
 
 NO_CHUNK = 0xFFFFFFFF
 GRID_X, GRID_Y, GRID_Z = 32, 8, 32
