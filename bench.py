@@ -585,6 +585,64 @@ def bench_reflect(m, w, stream, flush, steps, warmup):
             "l2": "flushed between timed steps (256 MB write)"}
 
 
+def bench_resolve(m, w, pools, stream, flush, steps, warmup, cpu=True):
+    """Lane 0 of the resolve (vm_resolve: sky and opaque surfaces with the
+    engine's default look, probe field and shaft envelope) over the timed
+    1080p frame.  Algorithmic bytes per launch: 28 per pixel (8 key + 4 shadow
+    read, 16 RGBA written); the material gathers (chunk records, light, tree
+    nodes, atlas, probes, shaft) are L2-resident.  The oracle is timed on a
+    bounded sample of rows and compared there."""
+    import torch
+    from oracle.oracle import Oracle
+    from voxelcraft_menu_b200 import look as LK
+    from voxelcraft_menu_b200 import world as W
+    rec = W.recipe_large_terrain()
+    flags = W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_HIZ | LK.LOOK_FLAGS
+    v = w.view(W.large_terrain_camera(rec, flags=flags, dx=0.5))
+    LK.apply_defaults(v.frame, rec.seed)
+    look = (LK.atlas(rec.seed), LK.block_faces(), LK.probe_field(rec.seed),
+            LK.shaft_envelope(rec, v.frame.sun_dir, v.frame.shaft_origin, 4.0))
+    m.upload_view(v)
+    m.upload_look(*look)
+    m.render()
+    for _ in range(warmup):
+        m.resolve(LK.HI_DEFAULT)
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.resolve(LK.HI_DEFAULT)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = float(np.mean(ms))
+    npix = v.n_pixels
+    peak, peak_kind = peaks()
+    gbs = 28 * npix / (t * 1e-3) / 1e9
+    out = {"workload": "the timed 1920x1080 frame of the 1024x256x1024 terrain, the engine's default look "
+                       "(fog, clouds, god rays, biome tint, probes, shaft envelope)",
+           "l2": "flushed between timed steps (256 MB write)", "us": t * 1e3, "gpx_per_s": npix / (t * 1e-3) / 1e9,
+           "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                        "peak_kind": peak_kind, "algorithmic_bytes_per_launch": 28 * npix,
+                        "traffic": profile_traffic("resolve"),
+                        "note": "issue-bound: per pixel the transcendental-heavy look (sky, clouds, shafts, "
+                                "noise) and a 9-sample light gather over L2-resident tables"}}
+    if cpu:
+        color = m.read_color()
+        vis, sh = m.read_vis(), m.read_shadow()
+        o = Oracle(v, *pools)
+        rows = 68                                  # a band of 68 rows through the frame's centre
+        p0, p1 = 506 * 1920, (506 + rows) * 1920
+        t0 = time.perf_counter()
+        ref = o.resolve(vis, LK.sun_visibility(sh), *look, spec_hi=LK.HI_DEFAULT, pix=(p0, p1))
+        dt = time.perf_counter() - t0
+        out["cpu_oracle"] = {"sample": f"{rows} rows ({p1 - p0} pixels) of the frame", "s": dt,
+                             "mpx_per_s": (p1 - p0) / dt / 1e6, "cores": os.cpu_count(),
+                             "max_abs_diff": float(np.abs(ref - color[p0:p1]).max())}
+    return out
+
+
 def bench_encoder(local, steps, warmup, cpu=True):
     """The dense -> 64-tree encoder (vm_encode_trees) over every chunk of the
     1024x256x1024 terrain (1024 dense 64^3 chunks, 512 MB of block ids
@@ -766,6 +824,8 @@ def main():
     filt = bench_filter(m, vb, pools, stream, flush, max(5, min(args.steps, 20)), 3,
                         cpu=not args.no_cpu and rank == 0) if not args.no_filter else None
     refl = bench_reflect(m, w, stream, flush, max(5, min(args.steps, 20)), 3) if not args.no_filter else None
+    resolve = bench_resolve(m, w, pools, stream, flush, max(5, min(args.steps, 20)), 3,
+                            cpu=not args.no_cpu and rank == 0) if not args.no_filter else None
 
     npix = 1920 * 1080
     rays = traffic["rays_primary"] + traffic["rays_shadow"]
@@ -940,6 +1000,8 @@ def main():
             line["shadow_filter"] = filt
         if refl is not None:
             line["reflect"] = refl
+        if resolve is not None:
+            line["resolve"] = resolve
         line.update(extra)
         if not args.no_cpu:
             _, o_pools, o_va, o_vb = oracle_workload()

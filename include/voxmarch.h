@@ -160,6 +160,49 @@ int vm_read_reflection(vm_ctx* ctx, uint64_t* key, float* t);
  * may be NULL.  The cell buffers are allocated by the first call. */
 int vm_water_sec(vm_ctx* ctx, uint32_t shift);
 int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* refl_key, float* refl_t);
+
+/* The resolve of sky and opaque surfaces: lane 0 of the engine's resolve pass
+ * (src/render/shaders/resolve.wgsl:1378-1466, RESOLVE_LANE 0), i.e.
+ * shade_hit_legacy_cached (resolve.wgsl:1537-1788: atlas texel with texture
+ * variation, biome tint, shore wetting, smooth light with AO from the light
+ * bricks, the frame's sun visibility, distant terrain shadow, cloud shadow,
+ * probe field, sky specular) plus the fog blend toward sky_base with the sun
+ * shafts, and sky_color with clouds for sky pixels.  Water and glass pixels
+ * are the engine's other lanes: their colour is left 0 with alpha 0.
+ *
+ * Material inputs, set once (the engine's own buffers):
+ *   vm_upload_atlas        the block atlas as make_atlas uploads it
+ *                          (src/render/mod.rs:2159-2222): Rgba8UnormSrgb,
+ *                          layers x 16 x 16, mips 16, 8, 4, 2 one after the
+ *                          other (each [layer][y][x][rgba]); decoded to
+ *                          linear float here.  Replaces textureSampleLevel on
+ *                          `atlas` (mag nearest, min / mipmap linear, clamp).
+ *   vm_upload_block_faces  block_faces (src/block.rs:265-276 face_table): 8
+ *                          words per block id, layer | perm class << 16.
+ *   vm_upload_probes       the probe field (src/render/mod.rs:2248-2300):
+ *                          RGBA16F, 128 x 768 x 128; NULL: the engine's
+ *                          initial fill of 1.0.
+ *   vm_upload_shaft        the shaft pass's envelope (the SHAFT_RESULT slice
+ *                          of `shaft`, common.wgsl:174-178): 512 x 512 f32;
+ *                          NULL: no terrain shadow (shade 1).
+ * vm_resolve(ctx, spec_hi): after vm_render (and vm_soften_shadows when the
+ * engine's SPEC_SOFT_SHADOWS is on: its mask is then the sun visibility, as
+ * the engine's primary_sun texture), spec_hi = the engine's FLAG_HI_* word
+ * (src/render/mod.rs:196-300; SKY_SPECULAR, SHORE_WET, CAUSTICS,
+ * TINT_BALANCE, SKY_LOOK, SKY_COOL, FOLIAGE_RICH, CANOPY_RELIEF,
+ * LEGACY_LIGHTING are read; COMPACT_SHADE_HIT and the surface debug views
+ * return VM_E_INVALID, as do underwater, heat-map, probe-tap and
+ * probe-ambient frames).  The frame flags give the rest (AO, TINT,
+ * TEX_VARIATION, DISTANT_SHADOWS, TERRAIN_SHAFTS, PROBE_CUBE / BOUNCE / SUN /
+ * SUN_HIGH, LIGHT_RGB, SKY_TINT), as make_spec derives them.
+ * vm_read_color: res.x * res.y RGBA float, the value the engine stores into
+ * its rgba16float target. */
+int vm_upload_atlas(vm_ctx* ctx, const uint8_t* rgba, uint32_t layers, uint32_t size, uint32_t mips);
+int vm_upload_block_faces(vm_ctx* ctx, const uint32_t* words, uint32_t n);
+int vm_upload_probes(vm_ctx* ctx, const uint16_t* rgba16f, uint32_t nx, uint32_t ny, uint32_t nz);
+int vm_upload_shaft(vm_ctx* ctx, const float* envelope, uint32_t dim);
+int vm_resolve(vm_ctx* ctx, uint32_t spec_hi);
+int vm_read_color(vm_ctx* ctx, float* rgba);
 /* Expanded visibility: voxel index X*(Z*y + z) + x over the world box
  * [origin, origin + dims), face = normal id (common.wgsl:387), t = hit_t
  * (common.wgsl:1300).  Misses: voxel 0xFFFFFFFF, face 0xFF, t 0. */

@@ -135,6 +135,27 @@ int vmw_build_view(const vmw_world* w, const vmw_camera* cam, vm_frame* frame, v
                    uint32_t cap, uint32_t* n_chunks_out, uint32_t* grid_out);
 void vmw_halton_jitter(uint64_t index, float* out2);
 
+/* Material inputs of the resolve (vm_upload_atlas, vm_upload_block_faces,
+ * vm_upload_probes, vm_upload_shaft) for callers without the engine's own.
+ * vmw_build_atlas: a procedural atlas of this library's own design in the
+ * engine's format (VM_TEX_COUNT Rgba8UnormSrgb layers of 16x16, mips 16, 8, 4,
+ * 2 in sequence, vmw_atlas_bytes(VM_TEX_COUNT) bytes; mips box-filtered in
+ * linear light; alpha = the tint mask of grass / leaves / meadow faces and the
+ * coverage of tufts).  vmw_block_faces: the engine's face table
+ * (src/block.rs:265-276: 8 words per block id, layer | perm class << 16; n >=
+ * 8 * VM_BLOCK_COUNT).  vmw_probe_field: a 128 x 768 x 128 RGBA16F field of
+ * values in [0.55, 1].  vmw_shaft_envelope: the terrain sun envelope of a
+ * recipe on the 512 x 512 texel window at `origin` (x, z) with `texel`
+ * blocks per texel.  vmw_look_defaults: the engine's default fog, cloud, god
+ * ray, tint (seed = the world seed) and shaft parameters of a frame, the
+ * shaft window centred on the frame's camera. */
+uint64_t vmw_atlas_bytes(uint32_t layers);
+int vmw_build_atlas(uint32_t seed, uint8_t* out);
+int vmw_block_faces(uint32_t* out, uint32_t n);
+int vmw_probe_field(uint32_t seed, uint16_t* out);
+int vmw_shaft_envelope(const vmw_recipe* r, const float* sun_dir, const float* origin, float texel, float* out);
+void vmw_look_defaults(vm_frame* f, int32_t seed);
+
 #ifdef __cplusplus
 }
 #endif

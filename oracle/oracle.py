@@ -32,6 +32,12 @@ SPEC_DEFAULT = SPEC_FULL_MARCH | SPEC_WATER_REPAIR | SPEC_LEAF_CUTOUT | SPEC_GLA
 SPEC_SOFT_RAYS = 256      # extension: jittered sun rays per hit, the shadow buffer holds the blocked fraction
 
 
+class OrLook(C.Structure):
+    """The resolve's material inputs as the engine uploads them."""
+    _fields_ = [("atlas_srgb", vp), ("layers", C.c_uint32), ("faces", vp), ("n_faces", C.c_uint32), ("probes", vp),
+                ("shaft", vp), ("spec_hi", C.c_uint32)]
+
+
 class OrHit(C.Structure):
     _fields_ = [("hit", C.c_uint32), ("t", C.c_float), ("normal", C.c_uint32), ("voxel", C.c_uint32 * 3),
                 ("micro", C.c_uint32 * 3), ("iters", C.c_uint32)]
@@ -76,6 +82,7 @@ def lib():
             "or_soften_shadows": (C.c_int, [vp, vp, vp, C.c_uint32, C.c_float, vp, vp, C.c_int]),
             "or_reflect": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
             "or_water_sec": (C.c_int, [vp, vp, C.c_uint32, vp, vp, vp, vp, C.c_int]),
+            "or_resolve": (C.c_int, [vp, vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
             "or_pick_rows": (C.c_uint64, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp]),
             "or_f16_round": (None, [vp, vp, C.c_uint64]),
         }
@@ -172,6 +179,22 @@ class Oracle:
         v = np.ascontiguousarray(vis, np.uint64)
         self._check(self.L.or_water_sec(C.byref(self.w), _p(v), shift, *(_p(a) for a in out), self.threads))
         return tuple(out)
+
+    def resolve(self, vis, sun_vis, atlas, faces, probes=None, shaft=None, spec_hi: int = 0, pix=None):
+        """Lane 0 of the resolve (resolve.wgsl:1378-1466): RGBA float per pixel
+        of [pix[0], pix[1]) (default: all), alpha 0 for water and glass pixels.
+        sun_vis: the per-pixel sun visibility (the engine's primary_sun)."""
+        b, e = (0, self.npix) if pix is None else pix
+        keep = [np.ascontiguousarray(atlas, np.uint8), np.ascontiguousarray(faces, np.uint32)]
+        pr = None if probes is None else np.ascontiguousarray(probes, np.uint16)
+        sh = None if shaft is None else np.ascontiguousarray(shaft, np.float32)
+        look = OrLook(_p(keep[0]), keep[0].size // (4 * 340), _p(keep[1]), keep[1].size,
+                      None if pr is None else _p(pr), None if sh is None else _p(sh), spec_hi)
+        v = np.ascontiguousarray(vis, np.uint64)
+        sv = np.ascontiguousarray(sun_vis, np.float32)
+        out = np.zeros((e - b, 4), np.float32)
+        self._check(self.L.or_resolve(C.byref(self.w), C.byref(look), _p(v), _p(sv), _p(out), b, e, self.threads))
+        return out
 
     def soften(self, vis, dist, limit: int = 4, penumbra: float = 1.5):
         """shadow_horizontal + shadow_vertical over the frame's blocker

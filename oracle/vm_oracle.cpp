@@ -1689,3 +1689,757 @@ void or_f16_round(const float* x, float* out, uint64_t n) {
 
 }  // extern "C"
 
+
+// ============================================================================
+// The resolve of sky and opaque surfaces: lane 0 of resolve.wgsl:1378-1466,
+// shade_hit_legacy_cached (resolve.wgsl:1537-1788), sky_color and the sun
+// shafts (common.wgsl:1332-1643).  Texture reads are restated from the
+// sampler equations (the engine's atlas sampler: mag nearest, min / mipmap
+// linear, clamp to edge; the probe sampler: linear, repeat in u and w, clamp
+// in v) on the atlas decoded to linear float by the sRGB transfer function.
+// ============================================================================
+namespace {
+
+struct Look {
+  const float* atlas; uint32_t layers;    // linear RGBA floats, mips 16, 8, 4, 2, each [layer][y][x][4]
+  const uint32_t* faces; uint32_t n_faces;
+  const uint16_t* probes;                 // RGBA16F 128 x 768 x 128, or null (1.0)
+  const float* shaft;                     // 512 x 512 envelope, or null
+  uint32_t spec_hi;
+  float grad_cos[32], grad_sin[32];
+};
+
+constexpr uint32_t HI_SKY_SPECULAR = 1u, HI_SHORE_WET = 8u, HI_CAUSTICS = 64u, HI_TINT_BALANCE = 512u,
+                   HI_SKY_LOOK = 1024u, HI_SKY_COOL = 2048u, HI_FOLIAGE_RICH = 8192u, HI_CANOPY_RELIEF = 16384u,
+                   HI_LEGACY_LIGHTING = 1048576u;
+
+inline float mixs(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+inline V3 mixv(V3 a, V3 b, float t) { return {mixs(a.x, b.x, t), mixs(a.y, b.y, t), mixs(a.z, b.z, t)}; }
+inline float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+inline bool cool(const Look& L) { return (L.spec_hi & HI_SKY_COOL) != 0u; }
+inline bool repair(const Look& L) { return (L.spec_hi & HI_LEGACY_LIGHTING) == 0u; }
+const V3 SCATTER_TINT = {1.0000f, 0.4770f, 0.1474f};
+
+// transmittance_from: common.wgsl:1332-1341
+float transmittance_from(const vm_frame& f, float y0, float s, V3 rd) {
+  float lambda = f.fog_falloff;
+  float x = clampf(lambda * s * rd.y, -60.0f, 60.0f);
+  float path = s;
+  if (fabsf(x) > 1e-4f) path = s * (1.0f - expf(-x)) / x;
+  float rho = f.fog_density * expf(-clampf(lambda * (y0 - f.fog_height), -60.0f, 60.0f));
+  return expf(-clampf(rho * path, 0.0f, 60.0f));
+}
+
+// hg_gain / scatter_lobe / sky_base: common.wgsl:1359-1395
+float hg_gain(float cos_t, float g) {
+  float g2 = g * g;
+  float d = 1.0f + g2 - 2.0f * g * cos_t;
+  return (1.0f - g2) / powf(fmaxf(d, 1e-4f), 1.5f);
+}
+V3 scatter_lobe(const vm_frame& f, V3 rd) {
+  float sd = dot(rd, ld3(f.sun_dir));
+  return muls(SCATTER_TINT, hg_gain(sd, f.fog_g) * f.fog_scatter * f.daylight);
+}
+V3 sky_base(const vm_frame& f, const Look& L, V3 rd, float shaft) {
+  float day = f.daylight;
+  float up = clampf(rd.y, 0.0f, 1.0f);
+  V3 horizon = mixv(v3(0.0049f, 0.0060f, 0.0134f), cool(L) ? v3(0.4074f, 0.6057f, 0.9150f) : v3(0.4480f, 0.6210f, 0.8900f), day);
+  V3 zenith = mixv(v3(0.0008f, 0.0015f, 0.0039f), cool(L) ? v3(0.0385f, 0.1892f, 0.8600f) : v3(0.0637f, 0.2140f, 0.8276f), day);
+  V3 c = mixv(horizon, zenith, powf(up, 0.55f));
+  float sd = dot(rd, ld3(f.sun_dir));
+  c = add(c, muls(muls(v3(1.0f, 0.8276f, 0.5225f), smoothstep(0.9975f, 0.9990f, sd)), fmaxf(day, 0.2f)));
+  c = add(c, muls(scatter_lobe(f, rd), shaft));
+  bool look = (L.spec_hi & HI_SKY_LOOK) != 0u;
+  if (look && f.haze_warm > 0.0f) {
+    float band = powf(1.0f - up, 3.0f);
+    float toward = 0.35f + 0.65f * powf(fmaxf(sd, 0.0f), 4.0f);
+    c = add(c, muls(SCATTER_TINT, band * toward * f.haze_warm * day * 0.22f));
+  }
+  if (look && f.zenith_deep > 0.0f) {
+    float z = powf(up, 0.55f);
+    c = mul(c, mixv(v3(1.0f, 1.0f, 1.0f), v3(0.80f, 0.90f, 1.16f), f.zenith_deep * z * day));
+  }
+  return mixv(c, muls(horizon, 0.26f), smoothstep(0.0f, -0.35f, rd.y));
+}
+
+// cloud_lattice / cloud_noise / cloud_fbm: common.wgsl:1432-1468
+float cloud_lattice(int32_t x, int32_t y) {
+  uint32_t h = hash_u32((uint32_t)x ^ (hash_u32((uint32_t)y) * 0x9e3779b9u));
+  return (float)(h >> 8u) * (1.0f / 16777216.0f);
+}
+float cloud_noise(float px, float py) {
+  float ix = floorf(px), iy = floorf(py);
+  float fx = px - ix, fy = py - iy;
+  float wx = fx * fx * fx * (fx * (fx * 6.0f - 15.0f) + 10.0f);
+  float wy = fy * fy * fy * (fy * (fy * 6.0f - 15.0f) + 10.0f);
+  int32_t cx = f2i(ix), cy = f2i(iy);
+  int32_t cx1 = (int32_t)((uint32_t)cx + 1u), cy1 = (int32_t)((uint32_t)cy + 1u);
+  float a = cloud_lattice(cx, cy), b = cloud_lattice(cx1, cy), d = cloud_lattice(cx, cy1), e = cloud_lattice(cx1, cy1);
+  return mixs(mixs(a, b, wx), mixs(d, e, wx), wy);
+}
+float cloud_fbm(float px, float py, float fp) {
+  float freq = 1.0f, amp = 1.0f, sum = 0.0f, norm = 0.0f;
+  for (uint32_t i = 0; i < 4u; ++i) {
+    float wgt = amp * (1.0f - smoothstep(0.25f, 0.5f, fp * freq));
+    if (wgt > 0.0f) {
+      sum += wgt * cloud_noise(px * freq, py * freq);
+      norm += wgt;
+    }
+    freq *= 2.0f;
+    amp *= 0.5f;
+  }
+  if (norm <= 0.0f) return 0.5f;
+  return sum / norm;
+}
+
+// cloud_shade: common.wgsl:1537-1555
+float cloud_shade(const vm_frame& f, V3 p, float fp) {
+  if (f.cloud_shadow <= 0.0f || f.cloud_cover <= 0.0f) return 1.0f;
+  float dy = f.cloud_height - p.y;
+  if (dy * f.sun_dir[1] <= 0.0f) return 1.0f;
+  float t = dy / f.sun_dir[1];
+  if (t > 1.0e5f) return 1.0f;
+  float qx = p.x + f.sun_dir[0] * t, qz = p.z + f.sun_dir[2] * t;
+  float drift = f.time * f.cloud_speed;
+  float dx = 0.94f * drift, dz = 0.34f * drift;
+  float n = cloud_fbm((qx + dx) / f.cloud_scale, (qz + dz) / f.cloud_scale, fmaxf(fp, t * 0.0093f) / f.cloud_scale);
+  float thr = 1.0f - f.cloud_cover;
+  return 1.0f - smoothstep(thr, thr + 0.14f, n) * f.cloud_shadow;
+}
+
+// cloud_radiance / sky_color: common.wgsl:1470-1530
+V3 cloud_radiance(const vm_frame& f, const Look& L, float dens, float depth, V3 rd) {
+  float day = f.daylight;
+  float thick = rd.y < 0.0f ? 0.0f : depth;
+  float warm = 1.0f - smoothstep(0.02f, 0.30f, f.sun_dir[1]);
+  V3 sun_tint = mixv(v3(1.0f, 1.0f, 1.0f), SCATTER_TINT, warm * 0.72f);
+  V3 lit = cool(L) ? v3(1.0f, 1.0f, 1.0f) : v3(1.0000f, 0.9575f, 0.8963f);
+  V3 base = cool(L) ? v3(0.4420f, 0.4880f, 0.6010f) : v3(0.4854f, 0.5312f, 0.6462f);
+  V3 day_c = mixv(mul(lit, sun_tint), base, thick);
+  V3 glow = muls(SCATTER_TINT, hg_gain(dot(rd, ld3(f.sun_dir)), 0.82f) * 0.055f * day * (1.0f - dens));
+  return add(mixv(v3(0.0021f, 0.0026f, 0.0052f), day_c, day), glow);
+}
+V3 sky_color(const vm_frame& f, const Look& L, V3 ro, V3 rd, float travelled, float shaft) {
+  V3 base = sky_base(f, L, rd, shaft);
+  if (f.cloud_cover <= 0.0f) return base;
+  float dy = f.cloud_height - ro.y;
+  if (dy * rd.y <= 0.0f) return base;
+  float t = dy / rd.y;
+  if (t > 1.0e5f) return base;
+  float px = ro.x + rd.x * t, pz = ro.z + rd.z * t;
+  float px_angle = 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
+  float fp = (travelled + t) * px_angle / (fabsf(rd.y) * f.cloud_scale);
+  float drift = f.time * f.cloud_speed;
+  float qx = px + 0.94f * drift, qz = pz + 0.34f * drift;
+  float n = cloud_fbm(qx / f.cloud_scale, qz / f.cloud_scale, fp);
+  float thr = 1.0f - f.cloud_cover;
+  bool look = (L.spec_hi & HI_SKY_LOOK) != 0u;
+  if (look && f.cloud_patch > 0.0f) {
+    float m = cloud_fbm(qx / (f.cloud_scale * 6.0f), qz / (f.cloud_scale * 6.0f), fp / 6.0f);
+    thr = clampf(thr + (m - 0.5f) * f.cloud_patch, 0.0f, 0.99f);
+  }
+  float dens = smoothstep(thr, thr + 0.14f, n);
+  if (dens <= 0.0f) return base;
+  float depth = smoothstep(thr, thr + 0.55f, n);
+  if (look && f.cloud_relief > 0.0f) {
+    float ax = f.sun_dir[0] + 1.0e-3f, az = f.sun_dir[2];
+    float l = sqrtf(ax * ax + az * az);
+    ax = ax / l; az = az / l;
+    float step = (8.0f + f.sun_dir[1] * 48.0f) / f.cloud_scale;
+    float ns = cloud_fbm(qx / f.cloud_scale + ax * step, qz / f.cloud_scale + az * step, fp);
+    depth = clampf(depth + (ns - n) * (2.2f * f.cloud_relief), 0.0f, 1.0f);
+  }
+  float reach = 1.0f - smoothstep(3.0e4f, 1.0e5f, t);
+  float a = dens * reach * transmittance_from(f, ro.y, t, rd);
+  return mixv(base, cloud_radiance(f, L, dens, depth, rd), a);
+}
+
+// shaft_sample / terrain_shade: common.wgsl:1557-1580
+float terrain_shade(const vm_frame& f, const Look& L, V3 p) {
+  if (!L.shaft) return 1.0f;
+  float tx = (p.x - f.shaft_origin[0]) / f.shaft_texel - 0.5f;
+  float tz = (p.z - f.shaft_origin[1]) / f.shaft_texel - 0.5f;
+  float hi = (float)VM_SHAFT_DIM - 1.0f;
+  float cx = clampf(tx, 0.0f, hi), cz = clampf(tz, 0.0f, hi);
+  float f0x = floorf(cx), f0z = floorf(cz);
+  float frx = cx - f0x, frz = cz - f0z;
+  uint32_t i0x = f2u(f0x), i0z = f2u(f0z);
+  uint32_t i1x = std::min(i0x + 1u, VM_SHAFT_DIM - 1u), i1z = std::min(i0z + 1u, VM_SHAFT_DIM - 1u);
+  auto at = [&](uint32_t x, uint32_t z) { return L.shaft[(uint64_t)z * VM_SHAFT_DIM + x]; };
+  float e = mixs(mixs(at(i0x, i0z), at(i1x, i0z), frx), mixs(at(i0x, i1z), at(i1x, i1z), frx), frz);
+  return smoothstep(e - f.shaft_soft, e + f.shaft_soft, p.y);
+}
+
+float dither_px(const vm_frame& f, uint32_t px, uint32_t py) {
+  float p0 = (float)px + 5.588238f * (float)f.frame_index, p1 = (float)py;
+  return fractf(52.9829189f * fractf(p0 * 0.06711056f + p1 * 0.00583715f));
+}
+
+// sun_shaft: common.wgsl:1582-1643
+float sun_shaft(const vm_frame& f, const Look& L, V3 ro, V3 rd, float dist, float alpha, uint32_t px, uint32_t py) {
+  bool terrain = (f.flags & VM_FLAG_TERRAIN_SHAFTS) != 0u;
+  bool deck = f.cloud_shadow > 0.0f && f.cloud_cover > 0.0f;
+  if (f.godray_strength <= 0.0f) return 1.0f;
+  if (!deck && !terrain) return 1.0f;
+  V3 lobe = scatter_lobe(f, rd);
+  float imp = smoothstep(0.0040f, 0.0120f, fmaxf(fmaxf(lobe.x, lobe.y), lobe.z) * alpha);
+  if (imp <= 0.0f) return 1.0f;
+  float d = fminf(dist, f.godray_dist);
+  if (d <= 0.0f) return 1.0f;
+  float opac = 1.0f - transmittance_from(f, ro.y, d, rd);
+  if (opac <= 1e-6f) return 1.0f;
+  float lambda = f.fog_falloff;
+  float rho0 = f.fog_density * expf(-clampf(lambda * (ro.y - f.fog_height), -60.0f, 60.0f));
+  float k = lambda * rd.y;
+  float off = dither_px(f, px, py);
+  float px_angle = 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
+  float sum = 0.0f;
+  for (uint32_t i = 0; i < f.godray_steps; ++i) {
+    float u = ((float)i + off) / (float)f.godray_steps;
+    float path = -logf(1.0f - u * opac) / rho0;
+    float s = path;
+    float kp = k * path;
+    if (fabsf(kp) > 1e-4f) s = -logf(fmaxf(1.0f - kp, 1e-6f)) / k;
+    s = clampf(s, 0.0f, d);
+    V3 p = add(ro, muls(rd, s));
+    float v = cloud_shade(f, p, s * px_angle);
+    if (terrain) v = v * terrain_shade(f, L, p);
+    sum += v;
+  }
+  float vis = sum / (float)f.godray_steps;
+  float covered = 1.0f;
+  if (d < dist) {
+    float full = 1.0f - transmittance_from(f, ro.y, dist, rd);
+    if (full > 1e-6f) covered = fminf(opac / full, 1.0f);
+  }
+  return fmaxf(mixs(1.0f, vis, imp * f.godray_strength * covered), 0.0f);
+}
+
+// light_at / voxel_occludes / world_sample / gather_face: common.wgsl:977-1096
+uint32_t light_at(const World& w, uint32_t ci, I3 v) {
+  const vm_chunk& c = chunk_at(w, ci);
+  if ((c.light_flags & 1u) != 0u) return c.light_base;
+  if (v.x < 0 || v.y < 0 || v.z < 0 || v.x > 63 || v.y > 63 || v.z > 63) return 0xF000u;
+  U3 uv{(uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z};
+  uint32_t cell = (uv.x >> 2u) | ((uv.y >> 2u) << 4u) | ((uv.z >> 2u) << 8u);
+  uint32_t entry = brick_at(w, (uint64_t)c.light_base + cell);
+  if ((entry & VM_UNIFORM_BIT) != 0u) return entry & 0xFFFFu;
+  uint32_t vb = cell_bit(uand(uv, 3u));
+  uint32_t word = brick_at(w, (uint64_t)entry + (vb >> 1u));
+  return (word >> ((vb & 1u) * 16u)) & 0xFFFFu;
+}
+bool voxel_occludes(const World& w, uint32_t ci, I3 v) {
+  bool occupied = voxel_occupied(w, ci, v);
+  const vm_chunk& c = chunk_at(w, ci);
+  if (occupied && (c.attr_flags & (VM_ATTR_HAS_WATER | VM_ATTR_HAS_FOLIAGE)) != 0u) {
+    uint32_t b = block_at(w, ci, U3{(uint32_t)v.x, (uint32_t)v.y, (uint32_t)v.z});
+    return b != VM_WATER && !is_tuft(b);
+  }
+  return occupied;
+}
+U2 world_sample(const World& w, V3 p) {
+  I3 cell = grid_rel(w, floor_i(divs(p, 64.0f)));
+  if (grid_outside(w, cell)) return U2{0xF000u, 0u};
+  uint32_t ci = grid_at(w, grid_index(w, cell));
+  if (ci == VM_NO_CHUNK) return U2{0xF000u, 0u};
+  const vm_chunk& c = chunk_at(w, ci);
+  I3 v = floor_i(divs(sub(p, ld3(c.origin)), c.voxel_size));
+  return U2{light_at(w, ci, v), voxel_occludes(w, ci, v) ? 1u : 0u};
+}
+void gather_face(const World& w, uint32_t ci, I3 base, I3 ta, I3 tb, U2* out) {
+  const vm_chunk& c = chunk_at(w, ci);
+  bool has_water = (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
+  for (uint32_t i = 0; i < 9u; ++i) {
+    int32_t a = (int32_t)(i % 3u) - 1, b = (int32_t)(i / 3u) - 1;
+    I3 uv{base.x + ta.x * a + tb.x * b, base.y + ta.y * a + tb.y * b, base.z + ta.z * a + tb.z * b};
+    bool solid = voxel_occupied(w, ci, uv);
+    if (solid && has_water) solid = block_at(w, ci, U3{(uint32_t)uv.x, (uint32_t)uv.y, (uint32_t)uv.z}) != VM_WATER;
+    out[i] = U2{light_at(w, ci, uv), solid ? 1u : 0u};
+  }
+}
+
+float light_sky(uint32_t p) { return (float)(p >> 12u); }
+V3 light_block_rgb(uint32_t p) { return v3((float)((p >> 8u) & 0xFu), (float)((p >> 4u) & 0xFu), (float)(p & 0xFu)); }
+float light_block_level(uint32_t p) { V3 c = light_block_rgb(p); return fmaxf(c.x, fmaxf(c.y, c.z)); }
+float light_curve(float level) { float l = level / 15.0f; return l * l * (0.6f + 0.4f * l); }
+V3 light_curve3(V3 level) {
+  V3 l = divs(level, 15.0f);
+  return mul(mul(l, l), v3(0.6f + 0.4f * l.x, 0.6f + 0.4f * l.y, 0.6f + 0.4f * l.z));
+}
+V3 block_ambient(V3 blk, float sk, V3 sky) {
+  float bk = fmaxf(blk.x, fmaxf(blk.y, blk.z));
+  V3 tint = divs(blk, fmaxf(bk, 1e-4f));
+  return muls(mixv(sky, tint, bk / fmaxf(sk + bk, 1e-4f)), fmaxf(sk, bk));
+}
+const V3 BLOCK_TINT = {1.0000f, 0.6500f, 0.3200f};
+
+// sky_ambient_tint / surface_sky_fill: resolve.wgsl:1-5, 73-89
+V3 sky_ambient_tint(const vm_frame& f, V3 n) {
+  const V3 sky_tint = {0.6038f, 0.7084f, 1.0000f};
+  if ((f.flags & VM_FLAG_SKY_TINT) == 0u) return sky_tint;
+  float day = f.daylight;
+  V3 horizon = mixv(v3(0.0049f, 0.0060f, 0.0134f), v3(0.4480f, 0.6210f, 0.8900f), day);
+  V3 zenith = mixv(v3(0.0008f, 0.0015f, 0.0039f), v3(0.0637f, 0.2140f, 0.8276f), day);
+  float wgt = n.y < -0.5f ? 0.0f : (n.y > 0.5f ? 0.78431373f : 0.58578900f);
+  V3 c = mixv(horizon, zenith, wgt);
+  c = add(c, muls(SCATTER_TINT, f.fog_scatter * day * 4.0f * fmaxf(dot(n, ld3(f.sun_dir)), 0.0f)));
+  V3 t = mul(sky_tint, v3(powf(c.x / 0.14658824f, 2.5f), powf(c.y / 0.30178431f, 2.5f), powf(c.z / 0.84105882f, 2.5f)));
+  float luma = 0.2126f * t.x + 0.7152f * t.y + 0.0722f * t.z;
+  return muls(t, 0.70721556f / fmaxf(luma, 1e-6f));
+}
+V3 surface_sky_fill(const vm_frame& f, const Look& L, V3 n) {
+  V3 sky = sky_ambient_tint(f, n);
+  if (!repair(L)) return sky;
+  return muls(sky, 0.60f * mixs(0.35f, 1.0f, clampf(n.y * 0.5f + 0.5f, 0.0f, 1.0f)));
+}
+
+// textureSampleLevel on the atlas: bilinear taps with clamp to edge, nearest
+// texel when the level magnifies (level <= 0), linear blend of two mips
+struct F4 { float r, g, b, a; };
+inline F4 mix4(F4 x, F4 y, float t) { return {mixs(x.r, y.r, t), mixs(x.g, y.g, t), mixs(x.b, y.b, t), mixs(x.a, y.a, t)}; }
+F4 atlas_texel(const Look& L, uint32_t mip, uint32_t layer, int32_t x, int32_t y) {
+  uint64_t base = 0;
+  for (uint32_t m = 0; m < mip; ++m) base += (uint64_t)L.layers * (16u >> m) * (16u >> m);
+  int32_t size = (int32_t)(16u >> mip);
+  x = std::min(std::max(x, 0), size - 1);
+  y = std::min(std::max(y, 0), size - 1);
+  const float* p = L.atlas + 4 * (base + ((uint64_t)layer * size + y) * size + x);
+  return {p[0], p[1], p[2], p[3]};
+}
+F4 atlas_bilinear(const Look& L, uint32_t mip, uint32_t layer, float u, float v) {
+  float size = (float)(16u >> mip);
+  float x = u * size - 0.5f, y = v * size - 0.5f;
+  float x0 = floorf(x), y0 = floorf(y);
+  float ax = x - x0, ay = y - y0;
+  int32_t ix = f2i(x0), iy = f2i(y0);
+  int32_t ix1 = (int32_t)((uint32_t)ix + 1u), iy1 = (int32_t)((uint32_t)iy + 1u);
+  return mix4(mix4(atlas_texel(L, mip, layer, ix, iy), atlas_texel(L, mip, layer, ix1, iy), ax),
+              mix4(atlas_texel(L, mip, layer, ix, iy1), atlas_texel(L, mip, layer, ix1, iy1), ax), ay);
+}
+F4 atlas_sample(const Look& L, float u, float v, uint32_t layer, float lod) {
+  if (layer >= L.layers) layer = L.layers - 1u;
+  if (!(lod > 0.0f)) return atlas_texel(L, 0, layer, f2i(floorf(u * 16.0f)), f2i(floorf(v * 16.0f)));
+  float d = fminf(lod, 3.0f);
+  float dl = floorf(d);
+  float delta = d - dl;
+  uint32_t m0 = f2u(dl);
+  F4 a = atlas_bilinear(L, m0, layer, u, v);
+  if (!(delta > 0.0f) || m0 + 1u >= 4u) return a;
+  return mix4(a, atlas_bilinear(L, m0 + 1u, layer, u, v), delta);
+}
+
+float half_to_float(uint16_t h) {
+  uint32_t sign = (uint32_t)(h >> 15) << 31, e = (h >> 10) & 0x1Fu, m = h & 0x3FFu, bits;
+  if (e == 0) {
+    if (m == 0) { bits = sign; }
+    else {   // subnormal: normalise
+      int32_t ex = -1;
+      do { m <<= 1; ++ex; } while ((m & 0x400u) == 0);
+      bits = sign | ((uint32_t)(127 - 15 - ex) << 23) | ((m & 0x3FFu) << 13);
+    }
+  } else if (e == 31) {
+    bits = sign | 0x7F800000u | (m << 13);
+  } else {
+    bits = sign | ((e - 15 + 127) << 23) | (m << 13);
+  }
+  float out;
+  memcpy(&out, &bits, 4);
+  return out;
+}
+F4 probe_texel(const Look& L, int32_t x, int32_t y, int32_t z) {
+  x = ((x % 128) + 128) % 128;
+  z = ((z % 128) + 128) % 128;
+  y = std::min(std::max(y, 0), 767);
+  const uint16_t* p = L.probes + 4 * (((uint64_t)z * 768 + y) * 128 + x);
+  return {half_to_float(p[0]), half_to_float(p[1]), half_to_float(p[2]), half_to_float(p[3])};
+}
+// probe_field: resolve.wgsl:106-118
+F4 probe_field(const Look& L, V3 p, uint32_t nid) {
+  if (!L.probes) return {1.0f, 1.0f, 1.0f, 1.0f};
+  uint32_t slab = nid >= VM_NORMAL_CROSS_A ? 3u : nid;
+  V3 t = muls(p, 1.0f / 4.0f);
+  float y = clampf(t.y, 0.5f, 128.0f - 0.5f);
+  float u = t.x * (1.0f / 128.0f), v = ((float)slab * 128.0f + y) * (1.0f / (128.0f * 6.0f)), wz = t.z * (1.0f / 128.0f);
+  float x = u * 128.0f - 0.5f, yy = v * 768.0f - 0.5f, z = wz * 128.0f - 0.5f;
+  float x0 = floorf(x), y0 = floorf(yy), z0 = floorf(z);
+  float ax = x - x0, ay = yy - y0, az = z - z0;
+  int32_t ix = f2i(x0), iy = f2i(y0), iz = f2i(z0);
+  F4 s[2];
+  for (int dz = 0; dz < 2; ++dz) {
+    F4 a = mix4(probe_texel(L, ix, iy, iz + dz), probe_texel(L, ix + 1, iy, iz + dz), ax);
+    F4 b = mix4(probe_texel(L, ix, iy + 1, iz + dz), probe_texel(L, ix + 1, iy + 1, iz + dz), ax);
+    s[dz] = mix4(a, b, ay);
+  }
+  return mix4(s[0], s[1], az);
+}
+
+// face_uv / perm_key / permute_uv: resolve.wgsl:129-164
+void face_uv(uint32_t nid, V3 local, float& u, float& v) {
+  if (nid >= VM_NORMAL_CROSS_A) { u = local.x; v = 1.0f - local.y; return; }
+  uint32_t axis = nid >> 1u;
+  if (axis == 0u) { u = local.z; v = 1.0f - local.y; }
+  else if (axis == 1u) { u = local.x; v = local.z; }
+  else { u = local.x; v = 1.0f - local.y; }
+  if (nid == 1u || nid == 4u) u = 1.0f - u;
+}
+uint32_t perm_key(V3 box_min, uint32_t nid) {
+  I3 c = floor_i(box_min);
+  return hash_u32(((uint32_t)c.x * 0x9e3779b9u) ^ ((uint32_t)c.y * 0x85ebca6bu) ^ ((uint32_t)c.z * 0xc2b2ae35u) ^
+                  (nid * 0x27d4eb2fu));
+}
+void permute_uv(float& u, float& v, uint32_t pclass, uint32_t h) {
+  bool d4 = pclass == 2u;
+  float px = u, py = v;
+  if (d4 && (h & 1u) != 0u) { px = v; py = u; }
+  if (pclass != 0u && (h & 2u) != 0u) px = 1.0f - px;
+  if (d4 && (h & 4u) != 0u) py = 1.0f - py;
+  u = px; v = py;
+}
+// hash_alpha: common.wgsl:400-406
+float hash_alpha(V3 p) {
+  I3 q = floor_i(muls(p, 64.0f));
+  uint32_t h = ((uint32_t)q.x * 73856093u) ^ ((uint32_t)q.y * 19349663u) ^ ((uint32_t)q.z * 83492791u);
+  h = h ^ (h >> 13u);
+  h = h * 1274126177u;
+  return (float)((h >> 8u) & 0xFFFFFFu) / 16777216.0f;
+}
+
+// simplex_grad / biome_noise / biome_band_weights / biome_tint: resolve.wgsl:180-285
+float simplex_grad(const Look& L, uint32_t seed, uint32_t xp, uint32_t yp, float xd, float yd) {
+  uint32_t h = (seed ^ xp ^ yp) * 0x27d4eb2du;
+  int32_t hs = (int32_t)h;
+  uint32_t idx = (uint32_t)((hs ^ (hs >> 15)) & 254);
+  uint32_t k = idx < 240u ? (idx % 48u) >> 1u : 24u + ((idx - 240u) >> 1u);
+  return xd * L.grad_cos[k] + yd * L.grad_sin[k];
+}
+int32_t biome_fast_floor(float f) { return f >= 0.0f ? f2i(f) : f2i(f) - 1; }
+float biome_noise(const Look& L, int32_t seed_i, float freq, float px, float pz) {
+  uint32_t seed = (uint32_t)seed_i;
+  float sqrt3 = 1.7320508075688772f;
+  float g2 = (3.0f - sqrt3) / 6.0f;
+  float f2 = 0.5f * (sqrt3 - 1.0f);
+  float x = px * freq, y = pz * freq;
+  float s = (x + y) * f2;
+  x = x + s; y = y + s;
+  int32_t i0 = biome_fast_floor(x), j0 = biome_fast_floor(y);
+  float xi = x - (float)i0, yi = y - (float)j0;
+  float t = (xi + yi) * g2;
+  float x0 = xi - t, y0 = yi - t;
+  uint32_t i = (uint32_t)i0 * 501125321u, j = (uint32_t)j0 * 1136930381u;
+  float a = 0.5f - x0 * x0 - y0 * y0;
+  float n0 = 0.0f;
+  if (a > 0.0f) n0 = (a * a) * (a * a) * simplex_grad(L, seed, i, j, x0, y0);
+  float c = (2.0f * (1.0f - 2.0f * g2) * (1.0f / g2 - 2.0f)) * t + ((-2.0f * (1.0f - 2.0f * g2) * (1.0f - 2.0f * g2)) + a);
+  float n2 = 0.0f;
+  if (c > 0.0f) {
+    float x2 = x0 + (2.0f * g2 - 1.0f), y2 = y0 + (2.0f * g2 - 1.0f);
+    n2 = (c * c) * (c * c) * simplex_grad(L, seed, i + 501125321u, j + 1136930381u, x2, y2);
+  }
+  float n1 = 0.0f;
+  if (y0 > x0) {
+    float x1 = x0 + g2, y1 = y0 + (g2 - 1.0f);
+    float b = 0.5f - x1 * x1 - y1 * y1;
+    if (b > 0.0f) n1 = (b * b) * (b * b) * simplex_grad(L, seed, i, j + 1136930381u, x1, y1);
+  } else {
+    float x1 = x0 + (g2 - 1.0f), y1 = y0 + g2;
+    float b = 0.5f - x1 * x1 - y1 * y1;
+    if (b > 0.0f) n1 = (b * b) * (b * b) * simplex_grad(L, seed, i + 501125321u, j, x1, y1);
+  }
+  return (n0 + n1 + n2) * 99.83685446303647f;
+}
+V3 biome_band_weights(float n) {
+  float hot = smoothstep(0.22f - 0.18f, 0.22f + 0.18f, n);
+  float cold = 1.0f - smoothstep(-0.22f - 0.18f, -0.22f + 0.18f, n);
+  return v3(cold, 1.0f - cold - hot, hot);
+}
+V3 biome_tint(const vm_frame& f, const Look& L, float x, float z) {
+  float temperature = biome_noise(L, (int32_t)((uint32_t)f.tint_seed + 7u), f.tint_freq_t, x, z);
+  float humidity = biome_noise(L, (int32_t)((uint32_t)f.tint_seed + 8u), f.tint_freq_h, x, z);
+  V3 wt = biome_band_weights(temperature), wh = biome_band_weights(humidity);
+  V3 plains = (L.spec_hi & HI_TINT_BALANCE) ? v3(0.935f, 1.067f, 0.892f) : v3(1.0f, 1.0f, 1.0f);
+  V3 forest = v3(0.664f, 1.045f, 1.000f), savanna = v3(1.842f, 0.935f, 0.793f), desert = v3(2.096f, 0.957f, 0.699f);
+  V3 taiga = v3(0.832f, 0.935f, 2.096f), tundra = v3(0.755f, 0.893f, 2.812f);
+  V3 dry = add(add(muls(tundra, wt.x), muls(plains, wt.y)), muls(desert, wt.z));
+  V3 mid = add(add(muls(taiga, wt.x), muls(plains, wt.y)), muls(savanna, wt.z));
+  V3 wet = add(add(muls(taiga, wt.x), muls(forest, wt.y)), muls(forest, wt.z));
+  return add(add(muls(dry, wh.x), muls(mid, wh.y)), muls(wet, wh.z));
+}
+
+float schlick_ground(float cos_i) {
+  float m = clampf(1.0f - cos_i, 0.0f, 1.0f);
+  float m2 = m * m;
+  float top = fmaxf(1.0f - 0.9f, 0.04f);
+  return 0.04f + (top - 0.04f) * m2 * m2 * m;
+}
+float face_shade(uint32_t nid) {
+  switch (nid) {
+    case 3u: return 1.00f;
+    case 2u: return 0.50f;
+    case 4u: case 5u: return 0.80f;
+    case 6u: case 7u: return 0.90f;
+    default: return 0.62f;
+  }
+}
+
+// shade_hit_legacy_cached: resolve.wgsl:1537-1788 (smooth_light, do_spec)
+V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint32_t nid, V3 hit, V3 rd, float dist,
+             float lit_frame) {
+  const vm_frame& f = *w.f;
+  const vm_chunk& c = chunk_at(w, ci);
+  float vs = c.voxel_size;
+  bool foliage = nid >= VM_NORMAL_CROSS_A;
+  V3 n = normal_of(nid);
+  if (foliage && dot(n, rd) > 0.0f) n = neg(n);
+  V3 sun = ld3(f.sun_dir);
+  V3 spec_pre = v3(0.0f, 0.0f, 0.0f);
+  if ((L.spec_hi & HI_SKY_SPECULAR) != 0u)
+    spec_pre = muls(sky_base(f, L, reflect(rd, n), 1.0f), schlick_ground(clampf(dot(n, neg(rd)), 0.0f, 1.0f)));
+  uint32_t axis = nid >> 1u;
+  V3 box_min = add(ld3(c.origin), muls(v3((float)v.x, (float)v.y, (float)v.z), vs));
+  V3 lq = divs(sub(hit, box_min), vs);
+  V3 local = v3(clampf(lq.x, 0.0f, 1.0f), clampf(lq.y, 0.0f, 1.0f), clampf(lq.z, 0.0f, 1.0f));
+  uint32_t fi = id * 8u + nid;
+  uint32_t face_word = fi < L.n_faces ? L.faces[fi] : 0u;
+  uint32_t layer = face_word & 0xFFFFu;
+  float u, tv;
+  face_uv(nid, local, u, tv);
+  if ((f.flags & VM_FLAG_TEX_VARIATION) != 0u) permute_uv(u, tv, face_word >> 16u, perm_key(box_min, nid));
+  float fa, fb;
+  I3 ta{0, 0, 0}, tb{0, 0, 0};
+  if (axis == 0u) { fa = local.y; fb = local.z; ta.y = 1; tb.z = 1; }
+  else if (axis == 1u) { fa = local.x; fb = local.z; ta.x = 1; tb.z = 1; }
+  else { fa = local.x; fb = local.y; ta.x = 1; tb.y = 1; }
+  float grazing = fmaxf(fabsf(dot(n, rd)), 0.25f);
+  float footprint = fmaxf(dist, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs / grazing;
+  float lod = clampf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f, 3.0f);
+  F4 texel = atlas_sample(L, u, tv, layer, lod);
+  V3 albedo = v3(texel.r, texel.g, texel.b);
+  float tint_mask = foliage ? 1.0f : texel.a;
+  if ((f.flags & VM_FLAG_TINT) != 0u && tint_mask > 0.0f) {
+    float k = tint_mask * f.tint_strength;
+    albedo = mul(albedo, mixv(v3(1.0f, 1.0f, 1.0f), biome_tint(f, L, hit.x, hit.z), k));
+  }
+  if ((L.spec_hi & HI_SHORE_WET) != 0u && id == VM_SAND) {
+    float wet = 1.0f - smoothstep(f.sea_level, f.sea_level + 1.5f, hit.y);
+    albedo = muls(albedo, mixs(1.0f, 0.62f, wet));
+  }
+  if ((L.spec_hi & HI_FOLIAGE_RICH) != 0u && (foliage || ((id == VM_GRASS || id == VM_MEADOW) && nid == VM_NORMAL_PY))) {
+    float hr = hash_alpha(box_min);
+    float hv = hash_alpha(add(box_min, v3(17.31f, 7.77f, 3.03f)));
+    V3 rich = v3(1.0f, 1.0f, 1.0f);
+    if (hr < 0.16f) rich = v3(1.30f, 1.10f, 0.55f);
+    else if (hr > 0.97f) rich = v3(1.35f, 0.72f, 0.95f);
+    albedo = muls(mul(albedo, rich), mixs(0.88f, 1.10f, hv));
+  }
+  if ((L.spec_hi & HI_CANOPY_RELIEF) != 0u && is_cutout_id(id)) {
+    float clump = cloud_noise(box_min.x * 0.21f + box_min.y * 0.313f, box_min.z * 0.21f + box_min.y * 0.173f);
+    float relief = mixs(0.72f, 1.34f, clump * clump);
+    float micro = mixs(0.92f, 1.08f, hash_alpha(box_min));
+    float toward_sun = clampf(dot(n, sun) * 0.5f + 0.5f, 0.0f, 1.0f);
+    albedo = muls(muls(muls(albedo, relief), micro), mixs(0.84f, 1.0f, toward_sun));
+  }
+  V3 sky_tint = surface_sky_fill(f, L, n);
+  bool light_rgb = (f.flags & VM_FLAG_LIGHT_RGB) != 0u;
+  bool gather = (w.spec & VM_SPEC_EMITTER_GATHER) != 0u;
+  float ao = 1.0f, sky_sm = 0.0f;
+  V3 amb = v3(0.0f, 0.0f, 0.0f);
+  if (foliage) {
+    uint32_t packed = light_at(w, ci, I3{(int32_t)v.x, (int32_t)v.y, (int32_t)v.z});
+    float sk = light_curve(light_sky(packed)) * f.daylight;
+    sky_sm = sk;
+    if (light_rgb) {
+      amb = block_ambient(light_curve3(light_block_rgb(packed)), sk, sky_tint);
+    } else {
+      float bk = light_curve(light_block_level(packed));
+      amb = muls(mixv(sky_tint, BLOCK_TINT, bk / fmaxf(sk + bk, 1e-4f)), fmaxf(sk, bk));
+    }
+  } else {
+    V3 air_c = add(add(box_min, v3(0.5f * vs, 0.5f * vs, 0.5f * vs)), muls(n, vs));
+    V3 step_a = muls(v3((float)ta.x, (float)ta.y, (float)ta.z), vs);
+    V3 step_b = muls(v3((float)tb.x, (float)tb.y, (float)tb.z), vs);
+    I3 air_v{(int32_t)v.x + (int32_t)n.x, (int32_t)v.y + (int32_t)n.y, (int32_t)v.z + (int32_t)n.z};
+    I3 span{ta.x + tb.x, ta.y + tb.y, ta.z + tb.z};
+    bool local_only = air_v.x - span.x >= 0 && air_v.y - span.y >= 0 && air_v.z - span.z >= 0 &&
+                      air_v.x + span.x <= 63 && air_v.y + span.y <= 63 && air_v.z + span.z <= 63;
+    U2 nb[9];
+    if (local_only) {
+      gather_face(w, ci, air_v, ta, tb, nb);
+    } else {
+      for (uint32_t i = 0; i < 9u; ++i)
+        nb[i] = world_sample(w, add(add(air_c, muls(step_a, (float)(i % 3u) - 1.0f)), muls(step_b, (float)(i / 3u) - 1.0f)));
+    }
+    float sky_n[9], blk_n[9], open_n[9];
+    uint32_t any_blk = 0u;
+    for (uint32_t i = 0; i < 9u; ++i) {
+      sky_n[i] = light_curve(light_sky(nb[i].x)) * f.daylight;
+      blk_n[i] = 0.0f;
+      if (light_rgb) {
+        if (gather) any_blk = any_blk | (nb[i].x & 0xFFFu);
+      } else {
+        blk_n[i] = light_curve(light_block_level(nb[i].x));
+      }
+      open_n[i] = 1.0f - (float)nb[i].y;
+    }
+    V3 blk4 = v3(0.0f, 0.0f, 0.0f);
+    if (gather && light_rgb && any_blk != 0u) blk4 = light_curve3(light_block_rgb(nb[4].x));
+    bool ao_on = (f.flags & VM_FLAG_AO) != 0u;
+    V3 amb_c[4];
+    float sky_c[4], ao_c[4];
+    for (uint32_t k = 0; k < 4u; ++k) {
+      uint32_t ia = (uint32_t)(4 + ((int32_t)(k & 1u) * 2 - 1));
+      uint32_t ib = (uint32_t)(4 + ((int32_t)(k >> 1u) * 2 - 1) * 3);
+      uint32_t ic = ia + ib - 4u;
+      float inv = 1.0f / (1.0f + open_n[ia] + open_n[ib] + open_n[ic]);
+      float sk = (sky_n[4] + sky_n[ia] * open_n[ia] + sky_n[ib] * open_n[ib] + sky_n[ic] * open_n[ic]) * inv;
+      sky_c[k] = sk;
+      if (light_rgb) {
+        if (gather && any_blk != 0u) {
+          V3 ba = light_curve3(light_block_rgb(nb[ia].x));
+          V3 bb = light_curve3(light_block_rgb(nb[ib].x));
+          V3 bc = light_curve3(light_block_rgb(nb[ic].x));
+          V3 bkv = muls(add(add(add(blk4, muls(ba, open_n[ia])), muls(bb, open_n[ib])), muls(bc, open_n[ic])), inv);
+          amb_c[k] = block_ambient(bkv, sk, sky_tint);
+        } else {
+          amb_c[k] = muls(sky_tint, sk);
+        }
+      } else {
+        float bk = (blk_n[4] + blk_n[ia] * open_n[ia] + blk_n[ib] * open_n[ib] + blk_n[ic] * open_n[ic]) * inv;
+        amb_c[k] = muls(mixv(sky_tint, BLOCK_TINT, bk / fmaxf(sk + bk, 1e-4f)), fmaxf(sk, bk));
+      }
+      float s1 = 1.0f - open_n[ia];
+      float s2 = 1.0f - open_n[ib];
+      float occ = (s1 > 0.5f && s2 > 0.5f) ? 3.0f : s1 + s2 + 1.0f - open_n[ic];
+      ao_c[k] = ao_on ? 1.0f - occ * 0.25f : 1.0f;
+    }
+    ao = mixs(mixs(ao_c[0], ao_c[1], fa), mixs(ao_c[2], ao_c[3], fa), fb);
+    sky_sm = mixs(mixs(sky_c[0], sky_c[1], fa), mixs(sky_c[2], sky_c[3], fa), fb);
+    amb = mixv(mixv(amb_c[0], amb_c[1], fa), mixv(amb_c[2], amb_c[3], fa), fb);
+  }
+  float direct = 0.0f;
+  float ndl = dot(n, sun);
+  if (ndl > 0.0f && f.daylight > 0.01f) {
+    float lit = 1.0f;
+    if ((f.flags & VM_FLAG_SHADOWS) != 0u) {
+      lit = lit_frame;
+      if ((f.flags & VM_FLAG_DISTANT_SHADOWS) != 0u && lit > 0.0f)
+        lit = lit * terrain_shade(f, L, add(hit, muls(sun, f.shadow_dist)));
+    }
+    if (lit > 0.0f) {
+      float cloud_fp = fmaxf(dist, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
+      lit = lit * cloud_shade(f, hit, cloud_fp);
+    }
+    direct = lit * ndl * sky_sm;
+    if ((L.spec_hi & HI_CAUSTICS) != 0u) {
+      float cdepth = f.sea_level - hit.y;
+      if (cdepth > 0.0f && cdepth < 8.0f && direct > 0.0f) {
+        float k = cdepth / fmaxf(sun.y, 1e-3f);
+        float spx = hit.x - sun.x * k, spz = hit.z - sun.z * k;
+        float a = f.wave_amp, l0 = f.wave_scale, ph = f.time * f.wave_speed * WAVE_TAU;
+        V3 g0 = wave_octave(spx, spz, 0.913089f, 0.407760f, l0, a * 0.42f, ph, 0.35f, 0.0f, 0.0f, 0.0f, false);
+        V3 g1 = wave_octave(spx, spz, -0.388685f, 0.921371f, l0 / 2.17f, a * 0.27f, ph * 1.4731f, 0.35f, 0.0f, 0.0f,
+                            0.0f, false);
+        float r0 = g0.x * g0.x + g0.y * g0.y;
+        float r1 = g1.x * g1.x + g1.y * g1.y;
+        float sheets = r0 * r1 * 4000.0f;
+        direct = direct * (1.0f + sheets * expf(-cdepth * 0.30f));
+      }
+    }
+  }
+  bool probe_cube = (f.flags & VM_FLAG_PROBE_CUBE) != 0u, probe_bounce = (f.flags & VM_FLAG_PROBE_BOUNCE) != 0u;
+  F4 probe = {1.0f, 1.0f, 1.0f, 1.0f};
+  if (probe_cube || probe_bounce) probe = probe_field(L, add(hit, muls(n, 2.0f)), nid);
+  float shade = repair(L) ? 1.0f : face_shade(nid);
+  if (probe_cube) shade = shade * probe.a;
+  V3 ambient_rgb = muls(amb, 0.50f);
+  V3 sun_rgb = muls(v3(1.0000f, 0.8469f, 0.5647f), direct * (repair(L) ? 0.78f : 0.52f));
+  V3 floor_rgb = muls(v3(0.85f, 0.90f, 1.00f), f.ambient);
+  V3 prgb = v3(probe.r, probe.g, probe.b);
+  if (probe_bounce) floor_rgb = mul(floor_rgb, prgb);
+  if ((f.flags & VM_FLAG_PROBE_SUN) != 0u) {
+    float gain = (f.flags & VM_FLAG_PROBE_SUN_HIGH) != 0u ? 0.25f : 0.10f;
+    floor_rgb = add(floor_rgb, muls(mul(v3(0.85f, 0.90f, 1.00f), prgb), gain * sky_sm));
+  }
+  V3 spec_rgb = muls(spec_pre, sky_sm * 0.5f);
+  V3 light = repair(L) ? add(add(muls(muls(ambient_rgb, ao), shade), sun_rgb), floor_rgb)
+                       : muls(add(muls(add(ambient_rgb, sun_rgb), ao), floor_rgb), shade);
+  if (repair(L) && id == VM_GLOWSTONE) return mul(albedo, add(muls(v3(1.0f, 0.7111f, 0.3024f), 1.5f), muls(light, 0.15f)));
+  return add(mul(albedo, light), spec_rgb);
+}
+
+float srgb_to_linear(uint8_t u) {
+  float c = (float)u / 255.0f;
+  return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f);
+}
+
+}  // namespace
+
+extern "C" {
+
+typedef struct or_look {
+  const uint8_t* atlas_srgb; uint32_t layers;   // Rgba8UnormSrgb, 16x16, 4 mips as the engine uploads them
+  const uint32_t* faces; uint32_t n_faces;
+  const uint16_t* probes;                       // RGBA16F 128 x 768 x 128, or null
+  const float* shaft;                           // 512 x 512, or null
+  uint32_t spec_hi;
+} or_look;
+
+// The resolve's colour (RGBA, alpha 1; water and glass pixels 0) of pixels
+// [pix_begin, pix_end) from the frame's keys and the sun visibility of each
+// pixel (the engine's primary_sun: r8unorm of the soft mask, or 1 - blocked).
+int or_resolve(const or_world* o, const or_look* lk, const uint64_t* vis, const float* sun_vis, float* rgba,
+               uint64_t pix_begin, uint64_t pix_end, int threads) {
+  World w = mk(o);
+  const vm_frame& f = *w.f;
+  size_t texels = 0;
+  for (uint32_t m = 0; m < 4; ++m) texels += (size_t)lk->layers * (16u >> m) * (16u >> m);
+  std::vector<float> lin(texels * 4);
+  for (size_t i = 0; i < texels; ++i) {
+    for (int ch = 0; ch < 3; ++ch) lin[i * 4 + ch] = srgb_to_linear(lk->atlas_srgb[i * 4 + ch]);
+    lin[i * 4 + 3] = (float)lk->atlas_srgb[i * 4 + 3] / 255.0f;
+  }
+  Look L;
+  L.atlas = lin.data(); L.layers = lk->layers;
+  L.faces = lk->faces; L.n_faces = lk->n_faces;
+  L.probes = lk->probes; L.shaft = lk->shaft; L.spec_hi = lk->spec_hi;
+  for (uint32_t k = 0; k < 32; ++k) {
+    float a = k < 24 ? 1.4398966328953218f - 0.26179938779914946f * (float)k
+                     : 1.1780972450961724f - 0.7853981633974483f * (float)(k - 24);
+    L.grad_cos[k] = cosf(a);
+    L.grad_sin[k] = sinf(a);
+  }
+  const uint64_t npix = (uint64_t)f.res[0] * f.res[1];
+  if (pix_end > npix) pix_end = npix;
+  if (threads > 0) omp_set_num_threads(threads);
+  V3 cam = ld3(f.cam_pos);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t pi = (int64_t)pix_begin; pi < (int64_t)pix_end; ++pi) {
+    uint64_t pix = (uint64_t)pi;
+    uint32_t px = (uint32_t)(pix % f.res[0]), py = (uint32_t)(pix / f.res[0]);
+    V3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+    uint64_t key = vis[pix];
+    V3 color;
+    float* out = rgba + 4 * (pix - pix_begin);
+    if (key == 0) {
+      float shaft = sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
+      color = sky_color(f, L, cam, rd, 0.0f, shaft);
+    } else {
+      uint32_t nid = key_nid(key), ci = key_ci(key);
+      U3 v = key_voxel(key), micro = key_micro(key);
+      float t = hit_t(w, ci, v, micro, nid, rd);
+      V3 hit = add(cam, muls(rd, t));
+      uint32_t id = block_at(w, ci, v);
+      if (id == VM_WATER || glass_leg(w, id)) {
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+        continue;
+      }
+      color = shade_hit(w, L, ci, v, id, nid, hit, rd, t, sun_vis[pix]);
+      float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
+      float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
+      color = mixv(color, sky_base(f, L, rd, shaft), alpha);
+    }
+    out[0] = color.x; out[1] = color.y; out[2] = color.z; out[3] = 1.0f;
+  }
+  return g_err.load();
+}
+
+}  // extern "C"

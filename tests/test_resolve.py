@@ -1,0 +1,298 @@
+"""The resolve of sky and opaque surfaces (lane 0 of resolve.wgsl:1378-1466:
+shade_hit_legacy_cached, the fog blend with sun shafts, sky_color with
+clouds) against the oracle's restatement.
+
+The kernel and the oracle share the float contract but not the
+transcendental functions (CUDA's expf / powf / log2f / logf / exp2f against
+the host's), so colours are compared within a tolerance: 2e-4 absolute plus
+1e-3 relative at 99.9% of the pixels, and 0.05 absolute at every pixel (a
+last-bit difference can move a texture-level or a smoothstep edge).  Water
+and glass pixels (the engine's other lanes) must be alpha 0 on both sides.
+
+CPU: the material builders (atlas format and mips, the engine's face table),
+the sun-visibility rounding and oracle properties.  GPU: frames of the small
+world with the engine's default look, with probes, the shaft envelope, a
+soft-shadow mask, non-uniform light bricks, every resolve override the
+kernel reads, and the whole 1920x1080 frame of the 1024x256x1024 terrain."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from voxelcraft_menu_b200 import look as LK
+from voxelcraft_menu_b200 import world as W
+
+ABS, REL, FRAC, WORST = 2e-4, 1e-3, 1e-3, 0.05
+
+
+def within(got, want, what):
+    got, want = np.asarray(got, np.float64), np.asarray(want, np.float64)
+    assert np.array_equal(got[:, 3], want[:, 3]), f"{what}: lane masks differ"
+    d = np.abs(got[:, :3] - want[:, :3])
+    tol = ABS + REL * np.abs(want[:, :3])
+    bad = np.any(d > tol, axis=1)
+    assert np.isfinite(got).all(), f"{what}: non-finite colour"
+    assert bad.mean() <= FRAC, f"{what}: {bad.sum()} of {len(bad)} pixels outside tolerance (max {d.max():.3g})"
+    assert d.max() <= WORST, f"{what}: largest difference {d.max():.3g}"
+
+
+@pytest.fixture(scope="module")
+def small():
+    w = W.World.generate(W.recipe_small_terrain())
+    return w, w.pools()
+
+
+def look_camera(width=480, height=270, flags=0, **kw):
+    return W.small_terrain_camera(width=width, height=height,
+                                  flags=W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | LK.LOOK_FLAGS | flags, **kw)
+
+
+def look_view(w, cam, seed=1):
+    v = w.view(cam)
+    LK.apply_defaults(v.frame, seed)
+    v.frame.time = 37.5
+    return v
+
+
+# ---------------------------------------------------------------- CPU -----
+
+def test_atlas_layout_and_mips():
+    a = LK.atlas(3)
+    assert a.size == LK.TEX_COUNT * 340 * 4
+    mip0 = a[: LK.TEX_COUNT * 256 * 4].reshape(LK.TEX_COUNT, 16, 16, 4)
+    mip1 = a[LK.TEX_COUNT * 256 * 4: LK.TEX_COUNT * 320 * 4].reshape(LK.TEX_COUNT, 8, 8, 4)
+    # alpha is the tint mask of grass tops and leaves, 0 for stone and dirt
+    assert (mip0[2, :, :, 3] == 255).all() and (mip0[8, :, :, 3] == 255).all()
+    assert (mip0[0, :, :, 3] == 0).all() and (mip0[1, :, :, 3] == 0).all()
+    # each mip is the 2x2 box average of the one above (alpha linear)
+    want = mip0[:, :, :, 3].reshape(LK.TEX_COUNT, 8, 2, 8, 2).astype(np.float64).mean(axis=(2, 4))
+    assert np.abs(mip1[:, :, :, 3] - want).max() <= 0.5 + 1e-9
+    assert not np.array_equal(LK.atlas(3), LK.atlas(4))
+
+
+def test_block_faces_follow_the_engine_table():
+    f = LK.block_faces().reshape(26, 8)
+    layer, perm = f & 0xFFFF, f >> 16
+    # src/block.rs:136-170: grass = column(GRASS_SIDE 3, DIRT 1, GRASS_TOP 2), log = column(6, 7, 7)
+    assert layer[3].tolist() == [3, 3, 1, 2, 3, 3, 3, 3]
+    assert layer[6].tolist() == [6, 6, 7, 7, 6, 6, 6, 6]
+    assert layer[23].tolist() == [24, 24, 1, 20, 24, 24, 24, 24]       # meadow-side
+    assert (layer[1] == 0).all() and (layer[13] == 14).all() and (layer[25] == 26).all()
+    # perm classes (src/block.rs:74-92): D4 on dirt / grass top / leaves, FLIP_U on grass side
+    assert perm[2].tolist() == [2] * 8 and perm[7].tolist() == [2] * 8
+    assert perm[3].tolist() == [1, 1, 2, 2, 1, 1, 1, 1]
+    assert (perm[1] == 0).all() and (perm[18] == 0).all()
+
+
+def test_sun_visibility_rounds_to_the_8bit_target():
+    sh = np.array([0.0, 3.5, 0.0, 12.0], np.float32)
+    assert LK.sun_visibility(sh).tolist() == [1.0, 0.0, 1.0, 0.0]
+    m = np.array([0.0, 0.5, 0.999, 1.2, -0.1, 0.00196], np.float32)
+    got = LK.sun_visibility(sh[:1].repeat(6), mask=m)
+    assert np.array_equal(got * np.float32(255.0), np.round(np.clip(m, 0, 1) * 255.0).astype(np.float32))
+    frac = np.array([0.25, 1.0], np.float32)
+    assert LK.sun_visibility(frac, soft_rays=True).tolist() == pytest.approx([0.74901962, 0.0])
+
+
+def test_oracle_resolve_properties(small):
+    w, pools = small
+    v = look_view(w, look_camera(160, 90))
+    o = Oracle(v, *pools)
+    vis = o.frame_vis()[0]
+    sh = o.shadow(vis)
+    sv = LK.sun_visibility(sh)
+    atlas, faces = LK.atlas(1), LK.block_faces()
+    c = o.resolve(vis, sv, atlas, faces, spec_hi=LK.HI_DEFAULT)
+    assert np.isfinite(c).all()
+    sky = vis == 0
+    assert sky.any() and (~sky).any()
+    assert (c[sky, 3] == 1.0).all()
+    # water and glass pixels belong to the other lanes
+    ids = np.array([o.block_at(int(k >> 24) & 0x1FFF, [(int(k) >> 16) & 63, (int(k) >> 8) & 63, int(k) & 63])
+                    if k else 0 for k in vis])
+    lane = (~sky) & ((ids == 13) | (ids == 10))
+    assert lane.any()
+    assert (c[lane] == 0.0).all() and (c[~lane, 3] == 1.0).all()
+    # a part of the range equals the same pixels of the whole frame
+    part = o.resolve(vis, sv, atlas, faces, spec_hi=LK.HI_DEFAULT, pix=(3000, 5000))
+    assert np.array_equal(part, c[3000:5000])
+    # shadowed surfaces are darker than the same frame fully lit
+    lit = o.resolve(vis, np.ones_like(sv), atlas, faces, spec_hi=LK.HI_DEFAULT)
+    shadowed = (sv == 0.0) & (~lane) & (~sky)
+    assert shadowed.any()
+    assert (lit[shadowed, :3].sum(1) >= c[shadowed, :3].sum(1)).all()
+    assert (lit[shadowed, :3].sum(1) > c[shadowed, :3].sum(1)).mean() > 0.5
+
+
+def test_oracle_sky_without_clouds_is_sky_base(small):
+    """With no clouds, no god rays and no scatter lobe the sky is sky_base's
+    gradient and sun disk (common.wgsl:1370-1395), restated here in float64."""
+    w, pools = small
+    v = look_view(w, look_camera(64, 36, pitch=math.radians(40.0)))
+    v.frame.cloud_cover = 0.0
+    v.frame.godray_strength = 0.0
+    v.frame.fog_scatter = 0.0
+    o = Oracle(v, *pools)
+    c = o.resolve(np.zeros(o.npix, np.uint64), np.ones(o.npix, np.float32), LK.atlas(1), LK.block_faces())
+    day = float(v.frame.daylight)
+    hor = np.array([0.0049, 0.0060, 0.0134]) * (1 - day) + np.array([0.4480, 0.6210, 0.8900]) * day
+    zen = np.array([0.0008, 0.0015, 0.0039]) * (1 - day) + np.array([0.0637, 0.2140, 0.8276]) * day
+    sun = np.array(v.frame.sun_dir, np.float64)
+
+    def smooth(e0, e1, x):
+        t = min(max((x - e0) / (e1 - e0), 0.0), 1.0)
+        return t * t * (3 - 2 * t)
+
+    for pix in range(0, o.npix, 7):
+        rd = o.ray_dir(pix % 64 + 0.5, pix // 64 + 0.5).astype(np.float64)
+        up = min(max(rd[1], 0.0), 1.0)
+        g = up ** 0.55
+        col = hor * (1 - g) + zen * g
+        col = col + np.array([1.0, 0.8276, 0.5225]) * smooth(0.9975, 0.9990, float(rd @ sun)) * max(day, 0.2)
+        k = smooth(0.0, -0.35, rd[1])
+        col = col * (1 - k) + hor * 0.26 * k
+        assert np.allclose(c[pix, :3], col, rtol=2e-4, atol=2e-6), pix   # float32 rd . sun at the disk edge
+
+
+# ---------------------------------------------------------------- GPU -----
+
+def light_bricks(v, bricks, seed):
+    """Non-uniform light volumes for every chunk of the view, appended to the
+    brick pool in the engine's format (light.rs pack_bricks: 4096 cell words,
+    uniform cells UNIFORM_BIT | packed, others a pointer to 32 words of two
+    16-bit voxels)."""
+    rng = np.random.default_rng(seed)
+    extra = []
+    base = bricks.size
+    chunks = v.chunks.copy()
+    for i in range(len(chunks)):
+        cells = np.empty(4096, np.uint32)
+        words = []
+        for cell in range(4096):
+            if rng.random() < 0.6:
+                sky = int(rng.integers(0, 16))
+                rgb = rng.integers(0, 16, 3) * (rng.random() < 0.2)
+                cells[cell] = 0x80000000 | (sky << 12) | (int(rgb[0]) << 8) | (int(rgb[1]) << 4) | int(rgb[2])
+            else:
+                vox = (rng.integers(0, 16, 64) << 12) | (rng.integers(0, 16, 64) * (rng.random(64) < 0.3))
+                vox = vox.astype(np.uint32)
+                cells[cell] = base + 4096 + sum(len(x) for x in words)
+                words.append((vox[0::2] | (vox[1::2] << 16)).astype(np.uint32))
+        chunks[i]["light_base"] = base
+        chunks[i]["light_flags"] = 0
+        blob = np.concatenate([cells] + words)
+        extra.append(blob)
+        base += blob.size
+    return chunks, np.concatenate([bricks] + extra)
+
+
+def gpu_resolve(v, pools, look, spec_hi, soften=None, spec=None):
+    from voxelcraft_menu_b200.march import Marcher
+    m = Marcher(v.res[0], v.res[1])
+    try:
+        if spec is not None:
+            m.set_spec(spec)
+        m.upload_world(*pools)
+        m.upload_view(v)
+        m.upload_look(*look)
+        m.render()
+        mask = None
+        if soften is not None:
+            m.soften_shadows(*soften)
+            mask = m.read_shadow_mask()
+        m.resolve(spec_hi)
+        return m.read_vis(), m.read_shadow(), mask, m.read_color()
+    finally:
+        m.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["default", "probes_shaft", "plain_flags", "legacy_lighting"])
+def test_resolve_matches_the_oracle(small, case):
+    w, pools = small
+    cam = look_camera()
+    v = look_view(w, cam)
+    probes = shaft = None
+    spec_hi = LK.HI_DEFAULT
+    if case == "probes_shaft":
+        probes = LK.probe_field(5)
+        shaft = LK.shaft_envelope(w.recipe, v.frame.sun_dir, v.frame.shaft_origin, 4.0)
+    elif case == "plain_flags":
+        v.frame.flags &= ~(LK.FLAG_LIGHT_RGB | LK.FLAG_SKY_TINT | LK.FLAG_AO | LK.FLAG_TEX_VARIATION | LK.FLAG_TINT)
+        spec_hi = 0
+    elif case == "legacy_lighting":
+        spec_hi = LK.HI_DEFAULT | LK.HI_LEGACY_LIGHTING
+    look = (LK.atlas(2), LK.block_faces(), probes, shaft)
+    vis, sh, _, got = gpu_resolve(v, pools, look, spec_hi)
+    o = Oracle(v, *pools)
+    want_vis = o.frame_vis()[0]
+    assert np.array_equal(vis, want_vis)
+    want = o.resolve(vis, LK.sun_visibility(sh), *look, spec_hi=spec_hi)
+    within(got, want, case)
+
+
+@pytest.mark.gpu
+def test_resolve_with_light_bricks_soft_mask_and_overrides(small):
+    w, pools = small
+    cam = look_camera(flags=0)
+    v = look_view(w, cam, seed=11)
+    v.frame.haze_warm, v.frame.zenith_deep, v.frame.cloud_patch, v.frame.cloud_relief = 0.6, 0.4, 0.5, 0.7
+    v.frame.daylight = 0.7
+    chunks, bricks = light_bricks(v, pools[2], seed=4)
+    v.chunks = chunks
+    lp = (pools[0], pools[1], bricks)
+    probes = LK.probe_field(9)
+    shaft = LK.shaft_envelope(w.recipe, v.frame.sun_dir, v.frame.shaft_origin, 4.0)
+    look = (LK.atlas(5), LK.block_faces(), probes, shaft)
+    spec_hi = (LK.HI_DEFAULT | LK.HI_SKY_LOOK | LK.HI_SKY_COOL | LK.HI_FOLIAGE_RICH | LK.HI_CANOPY_RELIEF |
+               LK.HI_CAUSTICS | LK.HI_TINT_BALANCE)
+    vis, sh, mask, got = gpu_resolve(v, lp, look, spec_hi, soften=(4, 1.5))
+    o = Oracle(v, *lp)
+    want = o.resolve(vis, LK.sun_visibility(sh, mask=mask), *look, spec_hi=spec_hi)
+    within(got, want, "light bricks + overrides")
+
+
+@pytest.mark.gpu
+def test_resolve_rejects_unbuilt_variants(small):
+    from voxelcraft_menu_b200.march import Marcher
+    w, pools = small
+    v = look_view(w, look_camera(64, 36))
+    m = Marcher(64, 36)
+    try:
+        m.upload_world(*pools)
+        m.upload_view(v)
+        m.render()
+        with pytest.raises(RuntimeError):
+            m.resolve(LK.HI_DEFAULT)                      # no atlas yet
+        m.upload_look(LK.atlas(1), LK.block_faces())
+        with pytest.raises(RuntimeError):
+            m.read_color()                                # no resolve yet
+        with pytest.raises(RuntimeError):
+            m.resolve(LK.HI_COMPACT_SHADE_HIT)
+        m.resolve(LK.HI_DEFAULT)
+        assert m.read_color().shape == (64 * 36, 4)
+        v.frame.flags |= LK.FLAG_PROBE_TAP
+        m.upload_view(v)
+        m.render()
+        with pytest.raises(RuntimeError):
+            m.resolve(LK.HI_DEFAULT)
+    finally:
+        m.close()
+
+
+@pytest.mark.gpu
+def test_full_hd_frame_resolve_matches_the_oracle():
+    rec = W.recipe_large_terrain()
+    w = W.World.generate(rec)
+    pools = w.pools()
+    cam = W.large_terrain_camera(rec, flags=W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | LK.LOOK_FLAGS)
+    v = w.view(cam)
+    LK.apply_defaults(v.frame, rec.seed)
+    probes = LK.probe_field(rec.seed)
+    shaft = LK.shaft_envelope(rec, v.frame.sun_dir, v.frame.shaft_origin, 4.0)
+    look = (LK.atlas(rec.seed), LK.block_faces(), probes, shaft)
+    vis, sh, _, got = gpu_resolve(v, pools, look, LK.HI_DEFAULT)
+    o = Oracle(v, *pools)
+    want = o.resolve(vis, LK.sun_visibility(sh), *look, spec_hi=LK.HI_DEFAULT)
+    within(got, want, "1080p")

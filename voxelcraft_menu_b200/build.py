@@ -28,12 +28,13 @@ NVCC_FLAGS = ARCH + [
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", f"-I{ROOT}", f"-I{CSRC}"]
 
 CU_SOURCES = ["kernels.cu", "pipeline.cu", "capi.cu", "gbuffer.cu", "shade.cu", "static_scratch.cu", "soften.cu",
-              "encode.cu"]
+              "encode.cu", "resolve.cu"]
 # The shading model is held to tolerances against FP64, not to bit equality
 # with the oracle, so it may contract a * b + c into fused multiply-adds.
 CU_EXTRA = {"shade.cu": ["--fmad=true"]}
-CPP_SOURCES = ["store.cpp"]
-HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "ray_stages.cuh", "shade.cuh", "store.h", "recipe.h"]
+CPP_SOURCES = ["store.cpp", "look.cpp"]
+HEADERS = ["vm_types.h", "march_device.cuh", "kernels.cuh", "ray_stages.cuh", "shade.cuh", "store.h", "recipe.h",
+           "water.cuh", "resolve.cuh"]
 
 
 def _newer(target: Path, deps: list[Path]) -> bool:

@@ -9,6 +9,7 @@
 
 #include "../../include/voxmarch.h"
 #include "kernels.cuh"
+#include "resolve.cuh"
 
 using vmk::ViewDesc;
 
@@ -42,6 +43,11 @@ struct vm_ctx {
   // per-frame outputs and scratch
   DevBuf vis, shadow, sec_key, sec_t, hiz, dbg, pairs, counters, err, work, dkmax, sufmax, traffic, expand;
   DevBuf shadow_mask;   // vm_soften_shadows output, sized on first use
+  bool mask_valid = false;   // the mask belongs to the last rendered frame
+  // the resolve's material inputs and output (vm_upload_atlas ... vm_resolve)
+  DevBuf atlas, faces, probes, shaft, grad, color;
+  uint32_t atlas_layers = 0, n_faces = 0;
+  bool have_probes = false, have_shaft = false, color_done = false;
   DevBuf shadow16;      // vm_read_async_r16f staging, sized on first use
   DevBuf refl_key, refl_t;   // reflect legs of water hits, sized by the first FLAG_WATER_REFLECT frame
   DevBuf ws_refr_key, ws_refr_t, ws_refl_key, ws_refl_t;   // vm_water_sec cells, sized by its first call
@@ -201,6 +207,8 @@ int prepare_reflect(vm_ctx* ctx) {
 
 // The single-view pipeline (frame and view descriptor by value).
 int enqueue_render(vm_ctx* ctx, bool count, const cudaEvent_t* ev = nullptr) {
+  ctx->mask_valid = false;
+  ctx->color_done = false;
   const vm_frame& f = ctx->frame;
   // buffers are grown before any of their pointers is taken below
   int rc;
@@ -312,7 +320,8 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->b_shadow_q, &ctx->b_sec_q, &ctx->item_cost, &ctx->tile_order, &ctx->b_item_cost,
                    &ctx->b_tile_order, &ctx->super_list, &ctx->super_count, &ctx->b_super_list,
                    &ctx->b_super_count, &ctx->shadow_mask, &ctx->refl_key, &ctx->refl_t,
-                   &ctx->shadow16, &ctx->ws_refr_key, &ctx->ws_refr_t, &ctx->ws_refl_key, &ctx->ws_refl_t};
+                   &ctx->shadow16, &ctx->ws_refr_key, &ctx->ws_refr_t, &ctx->ws_refl_key, &ctx->ws_refl_t,
+                   &ctx->atlas, &ctx->faces, &ctx->probes, &ctx->shaft, &ctx->grad, &ctx->color};
   for (DevBuf* b : all) release(*b);
   if (ctx->rendered) cudaEventDestroy(ctx->rendered);
   if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -464,6 +473,10 @@ int vm_march(vm_ctx* ctx) {
 }
 
 int vm_primary_shadow(vm_ctx* ctx) {
+  if (ctx) {
+    ctx->mask_valid = false;
+    ctx->color_done = false;
+  }
   if (!ctx) return VM_E_INVALID;
   int rc = check_ready(ctx);
   if (rc) return rc;
@@ -489,6 +502,7 @@ int vm_soften_shadows(vm_ctx* ctx, uint32_t radius_limit, float penumbra) {
   if ((rc = ensure(ctx, ctx->shadow_mask, (size_t)f.res[0] * f.res[1] * 4))) return rc;
   CK(vmk::launch_soften(f, dev_world(ctx), (const unsigned long long*)ctx->vis.p, (const float*)ctx->shadow.p,
                         (float*)ctx->shadow_mask.p, radius_limit, penumbra, ctx->stream));
+  ctx->mask_valid = true;
   return VM_OK;
 }
 
@@ -939,4 +953,131 @@ int vm_internal_batch_args(vm_ctx* ctx, vmk::PipeArgs* out, uint64_t* pixels, vo
   *pixels = ctx->b_pixels;
   *stream = (void*)ctx->stream;
   return VM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The resolve of sky and opaque pixels (lane 0 of resolve.wgsl:1378-1466) and
+// its material inputs.
+
+namespace {
+
+// the sRGB transfer function (IEC 61966-2-1), as the texture unit applies it
+// to an Rgba8UnormSrgb texel before filtering
+float srgb_decode(uint8_t u) {
+  const float c = (float)u / 255.0f;
+  return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f);
+}
+
+constexpr uint32_t HI_UNBUILT = 131072u /* COMPACT_SHADE_HIT */ | 8388608u | 16777216u | 33554432u /* DEBUG */;
+
+}  // namespace
+
+int vm_upload_atlas(vm_ctx* ctx, const uint8_t* rgba, uint32_t layers, uint32_t size, uint32_t mips) {
+  if (!ctx) return VM_E_INVALID;
+  if (!rgba || layers == 0 || layers > 0xFFFFu) return fail(ctx, VM_E_INVALID, "atlas needs 1..65535 layers");
+  if (size != VM_ATLAS_SIZE || mips != VM_ATLAS_MIPS)
+    return fail(ctx, VM_E_INVALID, "atlas must be %ux%u with %u mips (got %ux%u, %u)", VM_ATLAS_SIZE, VM_ATLAS_SIZE,
+                VM_ATLAS_MIPS, size, size, mips);
+  size_t texels = 0;
+  for (uint32_t m = 0; m < mips; ++m) texels += (size_t)layers * (size >> m) * (size >> m);
+  std::vector<float> lin(texels * 4);
+  for (size_t i = 0; i < texels; ++i) {
+    for (int c = 0; c < 3; ++c) lin[i * 4 + c] = srgb_decode(rgba[i * 4 + c]);
+    lin[i * 4 + 3] = (float)rgba[i * 4 + 3] / 255.0f;
+  }
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = ensure(ctx, ctx->atlas, lin.size() * 4))) return rc;
+  CK(cudaMemcpyAsync(ctx->atlas.p, lin.data(), lin.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  // (cos, sin) of the simplex gradient angles (resolve.wgsl:175-192)
+  float grad[64];
+  for (uint32_t k = 0; k < 32; ++k) {
+    const float a = k < 24 ? 1.4398966328953218f - 0.26179938779914946f * (float)k
+                           : 1.1780972450961724f - 0.7853981633974483f * (float)(k - 24);
+    grad[2 * k] = cosf(a);
+    grad[2 * k + 1] = sinf(a);
+  }
+  if ((rc = ensure(ctx, ctx->grad, sizeof grad))) return rc;
+  CK(cudaMemcpyAsync(ctx->grad.p, grad, sizeof grad, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->atlas_layers = layers;
+  return VM_OK;
+}
+
+int vm_upload_block_faces(vm_ctx* ctx, const uint32_t* words, uint32_t n) {
+  if (!ctx) return VM_E_INVALID;
+  if (!words || n == 0 || n % 8u != 0u) return fail(ctx, VM_E_INVALID, "block faces: 8 words per block id");
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = ensure(ctx, ctx->faces, (size_t)n * 4))) return rc;
+  CK(cudaMemcpyAsync(ctx->faces.p, words, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->n_faces = n;
+  return VM_OK;
+}
+
+int vm_upload_probes(vm_ctx* ctx, const uint16_t* rgba16f, uint32_t nx, uint32_t ny, uint32_t nz) {
+  if (!ctx) return VM_E_INVALID;
+  if (!rgba16f) { ctx->have_probes = false; return VM_OK; }
+  if (nx != VM_PROBE_NX || ny != VM_PROBE_NY || nz != VM_PROBE_NZ)
+    return fail(ctx, VM_E_INVALID, "probe field must be %ux%ux%u", VM_PROBE_NX, VM_PROBE_NY, VM_PROBE_NZ);
+  const size_t bytes = (size_t)nx * ny * nz * 8;
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = ensure(ctx, ctx->probes, bytes))) return rc;
+  CK(cudaMemcpyAsync(ctx->probes.p, rgba16f, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->have_probes = true;
+  return VM_OK;
+}
+
+int vm_upload_shaft(vm_ctx* ctx, const float* envelope, uint32_t dim) {
+  if (!ctx) return VM_E_INVALID;
+  if (!envelope) { ctx->have_shaft = false; return VM_OK; }
+  if (dim != VM_SHAFT_DIM) return fail(ctx, VM_E_INVALID, "shaft envelope must be %ux%u", VM_SHAFT_DIM, VM_SHAFT_DIM);
+  const size_t bytes = (size_t)dim * dim * 4;
+  CK(cudaSetDevice(ctx->device));
+  int rc;
+  if ((rc = ensure(ctx, ctx->shaft, bytes))) return rc;
+  CK(cudaMemcpyAsync(ctx->shaft.p, envelope, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->have_shaft = true;
+  return VM_OK;
+}
+
+int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
+  if (!ctx) return VM_E_INVALID;
+  int rc = check_ready(ctx);
+  if (rc) return rc;
+  const vm_frame& f = ctx->frame;
+  const size_t npix = (size_t)f.res[0] * f.res[1];
+  if (!ctx->vis.p || ctx->vis.bytes < npix * 8 || !ctx->shadow.p)
+    return fail(ctx, VM_E_NOT_READY, "no rendered frame to resolve");
+  if (!ctx->atlas_layers || !ctx->n_faces) return fail(ctx, VM_E_NOT_READY, "no atlas / block faces uploaded");
+  if (f.flags & (VM_FLAG_UNDERWATER | VM_FLAG_HEATMAP | VM_FLAG_PROBE_TAP | VM_FLAG_PROBE_AMBIENT))
+    return fail(ctx, VM_E_INVALID, "resolve of underwater, heat-map, probe-tap or probe-ambient frames is not built");
+  if (spec_hi & HI_UNBUILT)
+    return fail(ctx, VM_E_INVALID, "spec_hi 0x%x: compact shade_hit and surface debug views are not built",
+                spec_hi & HI_UNBUILT);
+  CK(cudaSetDevice(ctx->device));
+  if ((rc = ensure(ctx, ctx->color, npix * 16))) return rc;
+  vmd::Look L;
+  L.atlas = (const float4*)ctx->atlas.p; L.atlas_layers = ctx->atlas_layers;
+  L.faces = (const uint32_t*)ctx->faces.p; L.n_faces = ctx->n_faces;
+  L.probes = ctx->have_probes ? (const ushort4*)ctx->probes.p : nullptr;
+  L.shaft = ctx->have_shaft ? (const float*)ctx->shaft.p : nullptr;
+  L.grad = (const float2*)ctx->grad.p;
+  L.spec_hi = spec_hi;
+  const float* mask = ctx->mask_valid ? (const float*)ctx->shadow_mask.p : nullptr;
+  CK(vmk::launch_resolve(f, dev_world(ctx), L, (const unsigned long long*)ctx->vis.p, mask,
+                         (const float*)ctx->shadow.p, (ctx->spec & VM_SPEC_SOFT_RAYS) != 0u, (float4*)ctx->color.p,
+                         ctx->stream));
+  ctx->color_done = true;
+  return VM_OK;
+}
+
+int vm_read_color(vm_ctx* ctx, float* rgba) {
+  if (!ctx) return VM_E_INVALID;
+  if (!ctx->color_done) return fail(ctx, VM_E_NOT_READY, "no vm_resolve for this frame");
+  return read_dev(ctx, rgba, ctx->color.p, (size_t)ctx->frame.res[0] * ctx->frame.res[1] * 16);
 }

@@ -175,10 +175,35 @@ static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
 #define VM_FLAG_WAVE_FILL 4096u
 #define VM_FLAG_WATER_FAR 2097152u
 #define VM_FLAG_WATER_DARK 4194304u
+/* the rest of the engine's frame flags word (src/render/mod.rs:140-262), read
+ * by the resolve */
+#define VM_FLAG_AO 8u
+#define VM_FLAG_TINT 128u
+#define VM_FLAG_FOLIAGE 256u
+#define VM_FLAG_TERRAIN_SHAFTS 8192u
+#define VM_FLAG_TEX_VARIATION 16384u
+#define VM_FLAG_DISTANT_SHADOWS 32768u
+#define VM_FLAG_PROBE_TAP 16777216u
+#define VM_FLAG_PROBE_AMBIENT 33554432u
+#define VM_FLAG_PROBE_CUBE 67108864u
+#define VM_FLAG_PROBE_BOUNCE 134217728u
+#define VM_FLAG_LIGHT_RGB 268435456u
+#define VM_FLAG_PROBE_SUN 536870912u
+#define VM_FLAG_PROBE_SUN_HIGH 1073741824u
+#define VM_FLAG_SKY_TINT 2147483648u
+/* the resolve's material inputs (src/textures.rs:3-4, src/render/mod.rs:2240-2246,
+ * src/shaft.rs:3, common.wgsl:174-178) */
+#define VM_TEX_COUNT 27u              /* atlas layers (src/block.rs:37-65) */
+#define VM_ATLAS_SIZE 16u
+#define VM_ATLAS_MIPS 4u
+#define VM_PROBE_NX 128u
+#define VM_PROBE_NY 768u             /* 6 slabs (one per face normal) of 128 */
+#define VM_PROBE_NZ 128u
+#define VM_SHAFT_DIM 512u
 /* Soft sun shadows (an extension; the engine filters one blocker distance
  * instead, shadow.wgsl:49-116): VM_SOFT_SAMPLES rays per lit-facing hit, the
  * sun direction offset inside a 0.02 rad disk, and the shadow buffer holds the
- * blocked fraction.  A bit the engine's flag set leaves free. */
+ * blocked fraction (VM_SPEC_SOFT_RAYS). */
 
 #define VM_SOFT_SAMPLES 4u
 #define VM_SOFT_ROTATIONS 16u
@@ -227,6 +252,7 @@ static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
 #define VM_WATER 13u
 #define VM_PINE_LEAVES 16u
 #define VM_TALL_GRASS 18u
+#define VM_MEADOW 19u
 #define VM_AMBER_LAMP 20u
 #define VM_AZURE_LAMP 21u
 #define VM_VERDANT_LAMP 22u

@@ -227,6 +227,38 @@ class Marcher:
         self._ck(self._L.vm_read_water_sec(self._h, *(ptr(a) for a in out)))
         return tuple(out)
 
+    def upload_look(self, atlas: np.ndarray, faces: np.ndarray, probes: np.ndarray | None = None,
+                    shaft: np.ndarray | None = None):
+        """The resolve's material inputs (vm_upload_atlas, vm_upload_block_faces,
+        vm_upload_probes, vm_upload_shaft); None for the probe field or the
+        shaft envelope keeps the engine's neutral default."""
+        a = np.ascontiguousarray(atlas, np.uint8)
+        self._ck(self._L.vm_upload_atlas(self._h, ptr(a), a.size // (4 * 340), 16, 4))
+        fc = np.ascontiguousarray(faces, np.uint32)
+        self._ck(self._L.vm_upload_block_faces(self._h, ptr(fc), fc.size))
+        if probes is None:
+            self._ck(self._L.vm_upload_probes(self._h, None, 0, 0, 0))
+        else:
+            pr = np.ascontiguousarray(probes, np.uint16)
+            self._ck(self._L.vm_upload_probes(self._h, ptr(pr), 128, 768, 128))
+        if shaft is None:
+            self._ck(self._L.vm_upload_shaft(self._h, None, 0))
+        else:
+            sh = np.ascontiguousarray(shaft, np.float32)
+            self._ck(self._L.vm_upload_shaft(self._h, ptr(sh), 512))
+        self._look = (a, fc, probes, shaft)
+
+    def resolve(self, spec_hi: int):
+        """Lane 0 of the engine's resolve (sky and opaque surfaces) over the
+        last frame: vm_resolve with the engine's FLAG_HI_* word."""
+        self._ck(self._L.vm_resolve(self._h, spec_hi))
+
+    def read_color(self) -> np.ndarray:
+        """RGBA float per pixel (alpha 0 for the water and glass pixels)."""
+        out = np.empty((self._npix(), 4), np.float32)
+        self._ck(self._L.vm_read_color(self._h, ptr(out)))
+        return out
+
     def read_shadow_mask(self, out: np.ndarray | None = None) -> np.ndarray:
         """clamp(1 - occlusion, 0, 1) per pixel after soften_shadows; 1 = lit."""
         out = np.empty(self._npix(), np.float32) if out is None else out

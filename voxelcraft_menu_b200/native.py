@@ -145,6 +145,12 @@ _SIGNATURES = [
     ("vm_set_spec", C.c_int, [vp, C.c_uint32]),
     ("vm_water_sec", C.c_int, [vp, C.c_uint32]),
     ("vm_read_water_sec", C.c_int, [vp, vp, vp, vp, vp]),
+    ("vm_upload_atlas", C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32]),
+    ("vm_upload_block_faces", C.c_int, [vp, vp, C.c_uint32]),
+    ("vm_upload_probes", C.c_int, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32]),
+    ("vm_upload_shaft", C.c_int, [vp, vp, C.c_uint32]),
+    ("vm_resolve", C.c_int, [vp, C.c_uint32]),
+    ("vm_read_color", C.c_int, [vp, vp]),
     ("vm_read_vis", C.c_int, [vp, vp]),
     ("vm_read_hiz", C.c_int, [vp, vp]),
     ("vm_write_hiz", C.c_int, [vp, vp]),
@@ -198,6 +204,12 @@ _SIGNATURES = [
     ("vmw_pairs_for", C.c_uint32, [C.c_uint32, C.c_uint32]),
     ("vmw_build_view", C.c_int, [vp, P(VmwCamera), P(VmFrame), vp, C.c_uint32, P(C.c_uint32), vp]),
     ("vmw_halton_jitter", None, [C.c_uint64, vp]),
+    ("vmw_atlas_bytes", C.c_uint64, [C.c_uint32]),
+    ("vmw_build_atlas", C.c_int, [C.c_uint32, vp]),
+    ("vmw_block_faces", C.c_int, [vp, C.c_uint32]),
+    ("vmw_probe_field", C.c_int, [C.c_uint32, vp]),
+    ("vmw_shaft_envelope", C.c_int, [vp, vp, vp, C.c_float, vp]),
+    ("vmw_look_defaults", None, [vp, C.c_int32]),
 ]
 
 EXPORTED = [s[0] for s in _SIGNATURES]
