@@ -522,6 +522,8 @@ def bench_filter(m, vb, pools, stream, flush, steps, warmup, cpu=True):
     import torch
     peak, peak_kind = peaks()
     npix = int(vb.frame.res[0]) * int(vb.frame.res[1])
+    m.upload_view(vb)
+    m.render()                       # the filter's input: frame B's keys and blocker distances
     out = {"workload": "1920x1080 timed frame of the 1024x256x1024 terrain: its keys and blocker distances",
            "l2": "flushed between timed steps (256 MB write)"}
     for limit, pen in ((4, 1.5), (8, 3.0)):

@@ -44,6 +44,7 @@ typedef struct vmw_recipe {
   uint32_t tree_permille;
   uint32_t glass_permille;
   uint32_t island_permille;
+  uint32_t tuft_permille;    /* foliage tufts (TALL_GRASS, GRASS_TALL, REEDS) on dry surface columns without a tree */
 } vmw_recipe;
 
 typedef struct vmw_camera {

@@ -21,7 +21,8 @@ vp = C.c_void_p
 class OrWorld(C.Structure):
     _fields_ = [("frame", vp), ("chunks", vp), ("n_chunks", C.c_uint32), ("inners", vp), ("n_inners", C.c_uint64),
                 ("leaves", vp), ("n_leaves", C.c_uint64), ("bricks", vp), ("n_bricks", C.c_uint64), ("grid", vp),
-                ("n_grid", C.c_uint64), ("spec", C.c_uint32)]
+                ("n_grid", C.c_uint64), ("spec", C.c_uint32), ("atlas", vp), ("atlas_layers", C.c_uint32),
+                ("faces", vp), ("n_faces", C.c_uint32)]
 
 
 # pipeline specialisations (VM_SPEC_* of vm_types.h; the engine's make_spec, src/render/mod.rs:2355-2689)
@@ -100,7 +101,10 @@ def _p(a):
 class Oracle:
     """The oracle bound to one view (frame + chunk list + grid) and the pools."""
 
-    def __init__(self, view, inners, leaves, bricks, threads: int = 0, spec: int = SPEC_DEFAULT):
+    def __init__(self, view, inners, leaves, bricks, threads: int = 0, spec: int = SPEC_DEFAULT, atlas=None,
+                 faces=None):
+        """atlas / faces: the engine's atlas bytes and face table, for the
+        tuft cross-quads (without them tufts are transparent)."""
         self.L = lib()
         self.view = view
         self.frame = view.frame
@@ -110,6 +114,11 @@ class Oracle:
         ch, i, l, b, g = self._keep
         self.w = OrWorld(C.cast(C.pointer(self.frame), vp), _p(ch), len(ch), _p(i), i.size // 4, _p(l), l.size // 2,
                          _p(b), b.size, _p(g), g.size, spec)
+        if atlas is not None and faces is not None:
+            a, fc = np.ascontiguousarray(atlas, np.uint8), np.ascontiguousarray(faces, np.uint32)
+            self._keep += [a, fc]
+            self.w.atlas, self.w.atlas_layers = _p(a), a.size // (4 * 340)
+            self.w.faces, self.w.n_faces = _p(fc), fc.size
         self.spec = spec
         self.threads = threads
         self.L.or_clear_error()

@@ -101,6 +101,10 @@ struct World {
   const uint32_t* leaves; uint64_t n_leaves;   // count of vec2<u32>
   const uint32_t* bricks; uint64_t n_bricks;   // count of u32
   const uint32_t* grid; uint64_t n_grid;
+  // the engine's atlas (Rgba8UnormSrgb, 16x16 layers, mips 16, 8, 4, 2) and
+  // face table, for the tuft cross-quads; atlas null: tufts transparent
+  const uint8_t* atlas = nullptr; uint32_t atlas_layers = 0;
+  const uint32_t* faces = nullptr; uint32_t n_faces = 0;
 };
 
 // per-thread counters of the traversal's memory traffic (for the roofline)
@@ -376,12 +380,93 @@ inline bool casts_sun_shadow(uint32_t id) { return id != VM_GLOWSTONE; }  // com
 
 struct Hit { bool hit; float t; uint32_t normal; U3 voxel; U3 micro; uint32_t iters; };
 
-// march_chunk: common.wgsl:579-910.  Foliage tufts (ids 18/24/25) are
-// transparent here: their cross quads need the atlas alpha (cross_quad,
-// common.wgsl:425-487), which has no device-buffer form in this build.
+// textureSampleLevel(atlas, atlas_samp, uv, layer, lod).a with the engine's
+// atlas sampler (mag nearest, min / mipmap linear, clamp to edge), the alpha
+// of the Rgba8UnormSrgb texels being linear (a / 255)
+float atlas_alpha_texel(const World& w, uint32_t mip, uint32_t layer, int32_t x, int32_t y) {
+  uint64_t base = 0;
+  for (uint32_t m = 0; m < mip; ++m) base += (uint64_t)w.atlas_layers * (16u >> m) * (16u >> m);
+  int32_t size = (int32_t)(16u >> mip);
+  x = std::min(std::max(x, 0), size - 1);
+  y = std::min(std::max(y, 0), size - 1);
+  return (float)w.atlas[4 * (base + ((uint64_t)layer * size + y) * size + x) + 3] / 255.0f;
+}
+float atlas_alpha_bilinear(const World& w, uint32_t mip, uint32_t layer, float u, float v) {
+  float size = (float)(16u >> mip);
+  float x = u * size - 0.5f, y = v * size - 0.5f;
+  float x0 = floorf(x), y0 = floorf(y);
+  float ax = x - x0, ay = y - y0;
+  int32_t ix = f2i(x0), iy = f2i(y0);
+  int32_t ix1 = (int32_t)((uint32_t)ix + 1u), iy1 = (int32_t)((uint32_t)iy + 1u);
+  float a0 = atlas_alpha_texel(w, mip, layer, ix, iy) * (1.0f - ax) + atlas_alpha_texel(w, mip, layer, ix1, iy) * ax;
+  float a1 = atlas_alpha_texel(w, mip, layer, ix, iy1) * (1.0f - ax) + atlas_alpha_texel(w, mip, layer, ix1, iy1) * ax;
+  return a0 * (1.0f - ay) + a1 * ay;
+}
+float atlas_alpha(const World& w, uint32_t layer, float u, float v, float lod) {
+  if (layer >= w.atlas_layers) layer = w.atlas_layers - 1u;
+  if (!(lod > 0.0f)) return atlas_alpha_texel(w, 0, layer, f2i(floorf(u * 16.0f)), f2i(floorf(v * 16.0f)));
+  float d = fminf(lod, 3.0f), dl = floorf(d), delta = d - dl;
+  uint32_t m0 = f2u(dl);
+  float a = atlas_alpha_bilinear(w, m0, layer, u, v);
+  if (!(delta > 0.0f) || m0 + 1u >= 4u) return a;
+  return a * (1.0f - delta) + atlas_alpha_bilinear(w, m0 + 1u, layer, u, v) * delta;
+}
+
+// hash_alpha: common.wgsl:400-406
+float hash_alpha_p(V3 p) {
+  I3 q = floor_i(muls(p, 64.0f));
+  uint32_t h = ((uint32_t)q.x * 73856093u) ^ ((uint32_t)q.y * 19349663u) ^ ((uint32_t)q.z * 83492791u);
+  h = h ^ (h >> 13u);
+  h = h * 1274126177u;
+  return (float)((h >> 8u) & 0xFFFFFFu) / 16777216.0f;
+}
+
+struct CrossHit { bool hit; float t; uint32_t normal; };
+
+// cross_quad: common.wgsl:425-487 (shear: wind_shear, SPEC_WIND_SWAY)
+CrossHit cross_quad(const World& w, U3 uc, V3 ro, V3 rd, uint32_t layer, float vs, bool sway, float shx, float shz) {
+  const vm_frame& f = *w.f;
+  CrossHit r{false, 0.0f, VM_NORMAL_CROSS_A};
+  V3 base = v3((float)uc.x, (float)uc.y, (float)uc.z);
+  float ts[2] = {-1.0f, -1.0f};
+  if (sway) {
+    float dy = ro.y - base.y;
+    float ka = shx - shz, kb = shx + shz;
+    float da = rd.x - rd.z - ka * rd.y;
+    if (fabsf(da) > 1e-6f) ts[0] = ((base.x - base.z) + ka * dy - (ro.x - ro.z)) / da;
+    float db = rd.x + rd.z - kb * rd.y;
+    if (fabsf(db) > 1e-6f) ts[1] = ((base.x + base.z + 1.0f) + kb * dy - (ro.x + ro.z)) / db;
+  } else {
+    float da = rd.x - rd.z;
+    if (fabsf(da) > 1e-6f) ts[0] = ((base.x - base.z) - (ro.x - ro.z)) / da;
+    float db = rd.x + rd.z;
+    if (fabsf(db) > 1e-6f) ts[1] = ((base.x + base.z + 1.0f) - (ro.x + ro.z)) / db;
+  }
+  uint32_t order[2] = {VM_NORMAL_CROSS_A, VM_NORMAL_CROSS_B};
+  if (ts[1] < ts[0]) { std::swap(ts[0], ts[1]); std::swap(order[0], order[1]); }
+  for (uint32_t i = 0; i < 2u; ++i) {
+    float tq = ts[i];
+    if (tq < 0.0f) continue;
+    V3 p = add(ro, muls(rd, tq));
+    V3 local = sub(p, base);
+    if (local.x < -1e-4f || local.y < -1e-4f || local.z < -1e-4f || local.x > 1.0f + 1e-4f ||
+        local.y > 1.0f + 1e-4f || local.z > 1.0f + 1e-4f)
+      continue;
+    float footprint = fmaxf(tq * vs, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs;
+    float lod = fminf(fmaxf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f), 3.0f);
+    float a = atlas_alpha(w, layer, local.x, 1.0f - local.y, lod);
+    if (a <= hash_alpha_p(p)) continue;
+    r.hit = true; r.t = tq; r.normal = order[i];
+    return r;
+  }
+  return r;
+}
+
+// march_chunk: common.wgsl:579-910.  Tufts (ids 18/24/25) are traced as
+// cross quads when the world carries the atlas (foliage_trace), else they
+// are transparent.
 Hit march_chunk(const World& w, uint32_t ci, V3 ro_w, V3 rd, float t_limit, bool skip_water,
                 bool skip_foliage, bool skip_glass, bool sun_ray) {
-  (void)skip_foliage;
   Hit h{false, 0.0f, 0u, {0u, 0u, 0u}, {0u, 0u, 0u}, 0u};
   cnt_add(&Counters::march_calls);
   cnt_add(&Counters::chunk_records);
@@ -570,7 +655,32 @@ Hit march_chunk(const World& w, uint32_t ci, V3 ro_w, V3 rd, float t_limit, bool
     }
     if (solid && foliage_aware) {
       uint32_t bid = attr_uniform ? c.attr_base : leaf_block(w, attr, uc);
-      if (is_tuft(bid)) { solid = false; skip = 1; }
+      if (is_tuft(bid)) {
+        solid = false;
+        skip = 1;
+        if (!skip_foliage && w.atlas != nullptr) {
+          bool sway = (w.spec & VM_SPEC_WIND_SWAY) != 0u;
+          float shx = 0.0f, shz = 0.0f;
+          if (sway) {
+            float wx = c.origin[0] + (float)uc.x * vs, wz = c.origin[2] + (float)uc.z * vs;
+            float time = w.f->time * w.f->cloud_speed;
+            float g = 0.65f * sinf(time * 1.9f + wx * 0.11f + wz * 0.07f) +
+                      0.35f * sinf(time * 3.1f + wx * 0.173f + wz * 0.129f + 1.7f);
+            shx = g * 0.8f * 0.09f;
+            shz = g * 0.6f * 0.09f;
+          }
+          uint32_t fi = bid * 8u + VM_NORMAL_CROSS_A;
+          uint32_t layer = fi < w.n_faces ? (w.faces[fi] & 0xFFFFu) : 0u;
+          CrossHit q = cross_quad(w, uc, ro, rd, layer, vs, sway, shx, shz);
+          if (q.hit) {
+            h.hit = true;
+            h.t = q.t * vs;
+            h.normal = q.normal;
+            h.voxel = uc;
+            return h;
+          }
+        }
+      }
     }
     if (solid && cutout_aware) {
       uint32_t bid = attr_uniform ? c.attr_base : leaf_block(w, attr, uc);
@@ -895,6 +1005,8 @@ typedef struct or_world {
   const uint32_t* bricks; uint64_t n_bricks;
   const uint32_t* grid; uint64_t n_grid;
   uint32_t spec;     // VM_SPEC_* pipeline specialisations
+  const uint8_t* atlas; uint32_t atlas_layers;   // for the tuft quads; null: tufts transparent
+  const uint32_t* faces; uint32_t n_faces;
 } or_world;
 
 typedef struct or_hit {
@@ -914,6 +1026,8 @@ static World mk(const or_world* o) {
   w.bricks = o->bricks; w.n_bricks = o->n_bricks;
   w.grid = o->grid; w.n_grid = o->n_grid;
   w.spec = o->spec;
+  w.atlas = o->atlas; w.atlas_layers = o->atlas_layers;
+  w.faces = o->faces; w.n_faces = o->n_faces;
   return w;
 }
 

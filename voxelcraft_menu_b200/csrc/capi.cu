@@ -47,6 +47,10 @@ struct vm_ctx {
   // the resolve's material inputs and output (vm_upload_atlas ... vm_resolve)
   DevBuf atlas, faces, probes, shaft, grad, color;
   uint32_t atlas_layers = 0, n_faces = 0;
+  DevBuf atlas_alpha;          // the atlas's alpha channel for the tuft quads of the march
+  uint32_t tuft_layer[3] = {0, 0, 0};
+  bool chunks_foliage = false;   // a chunk of the uploaded list holds tufts (VM_ATTR_HAS_FOLIAGE)
+  bool batch_foliage = false;    // the same for the batch's chunk lists
   bool have_probes = false, have_shaft = false, color_done = false;
   DevBuf shadow16;      // vm_read_async_r16f staging, sized on first use
   DevBuf refl_key, refl_t;   // reflect legs of water hits, sized by the first FLAG_WATER_REFLECT frame
@@ -137,6 +141,10 @@ vmd::DevWorld dev_world(vm_ctx* ctx) {
   w.grid = (const uint32_t*)ctx->grid.p; w.n_grid = ctx->grid_len;
   w.err = (uint32_t*)ctx->err.p;
   w.spec = ctx->spec;
+  const bool tufts = ctx->atlas_layers && ctx->n_faces;   // the march reads the atlas once both are in
+  w.atlas_alpha = tufts ? (const float*)ctx->atlas_alpha.p : nullptr;
+  w.atlas_layers = ctx->atlas_layers;
+  for (int i = 0; i < 3; ++i) w.tuft_layer[i] = ctx->tuft_layer[i];
   return w;
 }
 
@@ -186,6 +194,12 @@ vmk::PipeArgs base_args(vm_ctx* ctx) {
   a.traffic = (vmk::Traffic64*)ctx->traffic.p;
   a.do_shadow = 1;
   a.spec = ctx->spec;
+  const bool tufts = ctx->atlas_layers && ctx->n_faces;
+  a.atlas_alpha = tufts ? (const float*)ctx->atlas_alpha.p : nullptr;
+  a.atlas_layers = ctx->atlas_layers;
+  for (int i = 0; i < 3; ++i) a.tuft_layer[i] = ctx->tuft_layer[i];
+  // the tuft kernels: the single view's chunks (the batch paths set their own)
+  a.tufts = tufts && (ctx->spec & VM_SPEC_FOLIAGE) != 0u && ctx->chunks_foliage ? 1u : 0u;
   a.do_secondary = 1;
   return a;
 }
@@ -321,7 +335,8 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->b_tile_order, &ctx->super_list, &ctx->super_count, &ctx->b_super_list,
                    &ctx->b_super_count, &ctx->shadow_mask, &ctx->refl_key, &ctx->refl_t,
                    &ctx->shadow16, &ctx->ws_refr_key, &ctx->ws_refr_t, &ctx->ws_refl_key, &ctx->ws_refl_t,
-                   &ctx->atlas, &ctx->faces, &ctx->probes, &ctx->shaft, &ctx->grad, &ctx->color};
+                   &ctx->atlas, &ctx->faces, &ctx->probes, &ctx->shaft, &ctx->grad, &ctx->color,
+                   &ctx->atlas_alpha};
   for (DevBuf* b : all) release(*b);
   if (ctx->rendered) cudaEventDestroy(ctx->rendered);
   if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -389,6 +404,9 @@ int vm_upload_chunks(vm_ctx* ctx, const vm_chunk* chunks, uint32_t n_chunks, con
   ctx->n_chunks = n_chunks;
   ctx->grid_len = grid_len;
   ctx->have_chunks = true;
+  ctx->chunks_foliage = false;
+  for (uint32_t i = 0; i < n_chunks && !ctx->chunks_foliage; ++i)
+    ctx->chunks_foliage = (chunks[i].attr_flags & VM_ATTR_HAS_FOLIAGE) != 0u;
   return VM_OK;
 }
 
@@ -414,7 +432,7 @@ int vm_set_tuning(vm_ctx* ctx, int warps_per_block, int reg_level, int ctas_per_
 
 int vm_set_spec(vm_ctx* ctx, uint32_t spec) {
   if (!ctx) return VM_E_INVALID;
-  const uint32_t known = VM_SPEC_ALL | VM_SPEC_SOFT_RAYS;
+  const uint32_t known = VM_SPEC_ALL | VM_SPEC_SOFT_RAYS | VM_SPEC_WIND_SWAY;
   if ((spec & ~known) != 0u) return fail(ctx, VM_E_INVALID, "unknown VM_SPEC bits 0x%x", spec & ~known);
   if (spec != ctx->spec) drop_graph(ctx);
   ctx->spec = spec;
@@ -804,6 +822,9 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
   CK(cudaMemsetAsync(ctx->b_item_cost.p, 0, tiles * 8, ctx->stream));   // a new batch: no costs yet
   CK(cudaMemcpyAsync(ctx->b_frames.p, frames, n_views * sizeof(vm_frame), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->b_chunks.p, chunks, chunk_total * sizeof(vm_chunk), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->batch_foliage = false;
+  for (uint64_t i = 0; i < chunk_total && !ctx->batch_foliage; ++i)
+    ctx->batch_foliage = (chunks[i].attr_flags & VM_ATTR_HAS_FOLIAGE) != 0u;
   CK(cudaMemcpyAsync(ctx->b_grids.p, grids, grid_total * 4, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemcpyAsync(ctx->b_views.p, ctx->bh_views.data(), n_views * sizeof(ViewDesc), cudaMemcpyHostToDevice,
                      ctx->stream));
@@ -823,6 +844,7 @@ int vm_batch_set(vm_ctx* ctx, uint32_t n_views, const vm_frame* frames, const vm
 
 static vmk::PipeArgs batch_args(vm_ctx* ctx, bool secondary) {
   vmk::PipeArgs a = base_args(ctx);
+  a.tufts = a.atlas_alpha != nullptr && (ctx->spec & VM_SPEC_FOLIAGE) != 0u && ctx->batch_foliage ? 1u : 0u;
   a.frames = (const vm_frame*)ctx->b_frames.p;
   a.views = (const ViewDesc*)ctx->b_views.p;
   a.n_views = ctx->b_n_views;
@@ -989,6 +1011,11 @@ int vm_upload_atlas(vm_ctx* ctx, const uint8_t* rgba, uint32_t layers, uint32_t 
   int rc;
   if ((rc = ensure(ctx, ctx->atlas, lin.size() * 4))) return rc;
   CK(cudaMemcpyAsync(ctx->atlas.p, lin.data(), lin.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<float> alpha(texels);
+  for (size_t i = 0; i < texels; ++i) alpha[i] = lin[i * 4 + 3];
+  if ((rc = ensure(ctx, ctx->atlas_alpha, alpha.size() * 4))) return rc;
+  CK(cudaMemcpyAsync(ctx->atlas_alpha.p, alpha.data(), alpha.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  drop_graph(ctx);   // cached launches carry the atlas pointers
   // (cos, sin) of the simplex gradient angles (resolve.wgsl:175-192)
   float grad[64];
   for (uint32_t k = 0; k < 32; ++k) {
@@ -1013,6 +1040,13 @@ int vm_upload_block_faces(vm_ctx* ctx, const uint32_t* words, uint32_t n) {
   CK(cudaMemcpyAsync(ctx->faces.p, words, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->n_faces = n;
+  // the cross-quad layer of each tuft block (block_faces[id * 8 + NORMAL_CROSS_A])
+  const uint32_t tufts[3] = {VM_TALL_GRASS, VM_GRASS_TALL, VM_REEDS};
+  for (int i = 0; i < 3; ++i) {
+    const uint32_t k = tufts[i] * 8u + VM_NORMAL_CROSS_A;
+    ctx->tuft_layer[i] = k < n ? (words[k] & 0xFFFFu) : 0u;
+  }
+  drop_graph(ctx);
   return VM_OK;
 }
 

@@ -38,7 +38,8 @@ __global__ void __launch_bounds__(256) k_gbuffer(const __grid_constant__ PipeArg
     const vm_frame& f = a.frames[lo];
     const ViewDesc vd = a.views[lo];
     const DevWorld w = {a.chunks + vd.chunk_off, vd.n_chunks, a.inners, a.n_inners, a.leaves, a.n_leaves,
-                        a.bricks, a.n_bricks, a.grids + vd.grid_off, vd.grid_len, a.err, a.spec};
+                        a.bricks, a.n_bricks, a.grids + vd.grid_off, vd.grid_len, a.err, a.spec, a.atlas_alpha,
+                        a.atlas_layers, {a.tuft_layer[0], a.tuft_layer[1], a.tuft_layer[2]}};
     const uint64_t pix = gp - vd.pix_off;
     GBuf g;
     g.code = 0u; g.t = 0.0f; g.d = 0.0f; g.fog = 0.0f;

@@ -113,8 +113,8 @@ __global__ void __launch_bounds__(256) k_march_pairs(const vm_frame f, const Dev
     const Chunk c = ld_chunk(w, ci);
     if (ray_skips(f, c.fade, px, py)) continue;
     const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
-    Hit h = march_chunk<UNDERWATER, false, false, false>(w, f, c, make_ray(cam, rd), f.far_, nullptr);
-    if (UNDERWATER && (w.spec & VM_SPEC_SNELL_BEND) != 0u && !h.hit) snell_bend<false, false>(w, f, c, rd, &h, nullptr);
+    Hit h = march_chunk<UNDERWATER, false, false, false, false, true>(w, f, c, make_ray(cam, rd), f.far_, nullptr);
+    if (UNDERWATER && (w.spec & VM_SPEC_SNELL_BEND) != 0u && !h.hit) snell_bend<false, false, true>(w, f, c, rd, &h, nullptr);
     const uint64_t pix = (uint64_t)py * f.res[0] + px;
     if (h.hit) atomicMax(&vis[pix], make_key(f, h, ci));
     if (heat) atomicAdd(&dbg[pix], h.iters);
@@ -188,13 +188,13 @@ __global__ void __launch_bounds__(128) k_secondary(const vm_frame f, const DevWo
   unsigned long long k = 0ull;
   float t = 0.0f;
   SecRay s;
-  if (secondary_setup(w, f, vis[pix], px, py, &s)) secondary_trace<false>(w, f, s, &k, &t, nullptr);
+  if (secondary_setup(w, f, vis[pix], px, py, &s)) secondary_trace<false, true>(w, f, s, &k, &t, nullptr);
   sec_key[pix] = k;
   sec_t[pix] = t;
   if (refl_key) {
     k = 0ull;
     t = 0.0f;
-    if (reflect_setup(w, f, vis[pix], px, py, &s)) secondary_trace<false>(w, f, s, &k, &t, nullptr);
+    if (reflect_setup<true>(w, f, vis[pix], px, py, &s)) secondary_trace<false, true>(w, f, s, &k, &t, nullptr);
     refl_key[pix] = k;
     refl_t[pix] = t;
   }
@@ -246,11 +246,11 @@ __global__ void __launch_bounds__(128) k_water_sec(const vm_frame f, const DevWo
       s.o = hit + s.d * VM_SURFACE_EPS;
       s.max_dist = VM_WATER_REFRACT_DIST;
       s.water = true;
-      secondary_trace<false>(w, f, s, &kr, &tr_, nullptr);
+      secondary_trace<false, true>(w, f, s, &kr, &tr_, nullptr);
     }
     if (water_reflects(f, best_t)) {
-      s = reflect_ray<false>(w, f, hit, rd, best.nid, best_t, nullptr);
-      secondary_trace<false>(w, f, s, &km, &tm, nullptr);
+      s = reflect_ray<false, true>(w, f, hit, rd, best.nid, best_t, nullptr);
+      secondary_trace<false, true>(w, f, s, &km, &tm, nullptr);
     }
   }
   const uint64_t h = (uint64_t)hy * hw + hx;

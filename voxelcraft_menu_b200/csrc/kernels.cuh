@@ -86,6 +86,10 @@ struct PipeArgs {
   Traffic64* traffic;          // counting kernels only
   uint32_t do_shadow, do_secondary;
   uint32_t spec;               // VM_SPEC_* pipeline specialisations
+  const float* atlas_alpha;    // the tuft quads' atlas alpha (DevWorld), or null
+  uint32_t atlas_layers;
+  uint32_t tuft_layer[3];
+  uint32_t tufts;              // trace tuft cross quads: the chunks hold tufts and atlas_alpha is set
   uint32_t do_reflect;         // with do_secondary: also queue the reflect leg of water hits
                                // (sec_q then holds up to 2 items per pixel)
   vm_frame frame0;
@@ -145,6 +149,6 @@ struct PipeTuning {
 cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwater, bool count, int sms,
                             cudaStream_t s, const cudaEvent_t* ev = nullptr);
 int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bool reflect = false,
-                            bool single = true);
+                            bool single = true, bool tufts = false);
 
 }  // namespace vmk

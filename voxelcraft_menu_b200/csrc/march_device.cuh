@@ -23,6 +23,11 @@ struct DevWorld {
   const uint32_t* grid; uint64_t n_grid;
   uint32_t* err;
   uint32_t spec;     // VM_SPEC_* pipeline specialisations
+  // the atlas alpha the tuft cross-quads test (the engine's atlas, sampled at
+  // an explicit level), [mip][layer][y][x] for mips 16, 8, 4, 2; null: no
+  // atlas uploaded, tufts stay transparent
+  const float* atlas_alpha; uint32_t atlas_layers;
+  uint32_t tuft_layer[3];   // block_faces[id * 8 + NORMAL_CROSS_A] of TALL_GRASS, GRASS_TALL, REEDS
 };
 
 enum : uint32_t { ERR_CHUNK = 1u, ERR_INNER = 2u, ERR_LEAF = 4u, ERR_BRICK = 8u, ERR_GRID = 16u, ERR_LIST = 32u };
@@ -323,16 +328,120 @@ __device__ __forceinline__ Ray make_ray(F3 o, F3 d) {
   return r;
 }
 
+// The atlas alpha at (u, v) of a layer at an explicit level, through the
+// engine's atlas sampler (mag nearest, min / mipmap linear, clamp to edge):
+// level <= 0 magnifies (nearest texel of mip 0), otherwise the two mips
+// around it are sampled bilinearly and blended.
+__device__ __forceinline__ float atlas_alpha_at(const DevWorld& w, uint32_t mip, uint32_t layer, int32_t x, int32_t y) {
+  const uint32_t size = 16u >> mip;
+  uint64_t base = 0;
+  for (uint32_t m = 0; m < mip; ++m) base += (uint64_t)w.atlas_layers * (16u >> m) * (16u >> m);
+  x = min(max(x, 0), (int32_t)size - 1);
+  y = min(max(y, 0), (int32_t)size - 1);
+  return __ldg(w.atlas_alpha + base + ((uint64_t)layer * size + (uint32_t)y) * size + (uint32_t)x);
+}
+__device__ __forceinline__ float atlas_alpha_bilinear(const DevWorld& w, uint32_t mip, uint32_t layer, float u, float v) {
+  const float size = (float)(16u >> mip);
+  const float x = u * size - 0.5f, y = v * size - 0.5f;
+  const float x0 = floorf(x), y0 = floorf(y);
+  const float ax = x - x0, ay = y - y0;
+  const int32_t ix = ffloor_i(x0), iy = ffloor_i(y0);
+  const int32_t ix1 = (int32_t)((uint32_t)ix + 1u), iy1 = (int32_t)((uint32_t)iy + 1u);
+  const float a0 = atlas_alpha_at(w, mip, layer, ix, iy) * (1.0f - ax) + atlas_alpha_at(w, mip, layer, ix1, iy) * ax;
+  const float a1 = atlas_alpha_at(w, mip, layer, ix, iy1) * (1.0f - ax) + atlas_alpha_at(w, mip, layer, ix1, iy1) * ax;
+  return a0 * (1.0f - ay) + a1 * ay;
+}
+__device__ __forceinline__ float atlas_alpha(const DevWorld& w, uint32_t layer, float u, float v, float lod) {
+  layer = min(layer, w.atlas_layers - 1u);
+  if (!(lod > 0.0f)) return atlas_alpha_at(w, 0, layer, ffloor_i(u * 16.0f), ffloor_i(v * 16.0f));
+  const float d = fminf(lod, 3.0f);
+  const float dl = floorf(d);
+  const float delta = d - dl;
+  const uint32_t m0 = __float2uint_rz(dl);
+  const float a = atlas_alpha_bilinear(w, m0, layer, u, v);
+  if (!(delta > 0.0f) || m0 + 1u >= 4u) return a;
+  return a * (1.0f - delta) + atlas_alpha_bilinear(w, m0 + 1u, layer, u, v) * delta;
+}
+
+// hash_alpha: common.wgsl:400-406
+__device__ __forceinline__ float hash_alpha3(float x, float y, float z) {
+  const int32_t qx = ffloor_i(x * 64.0f), qy = ffloor_i(y * 64.0f), qz = ffloor_i(z * 64.0f);
+  uint32_t h = ((uint32_t)qx * 73856093u) ^ ((uint32_t)qy * 19349663u) ^ ((uint32_t)qz * 83492791u);
+  h = h ^ (h >> 13u);
+  h = h * 1274126177u;
+  return (float)((h >> 8u) & 0xFFFFFFu) / 16777216.0f;
+}
+
+// wind_shear: common.wgsl:419-423 (SPEC_WIND_SWAY)
+__device__ __forceinline__ void wind_shear(float wx, float wz, float time, float* sx, float* sz) {
+  const float g = 0.65f * sinf(time * 1.9f + wx * 0.11f + wz * 0.07f) +
+                  0.35f * sinf(time * 3.1f + wx * 0.173f + wz * 0.129f + 1.7f);
+  *sx = g * 0.8f * 0.09f;
+  *sz = g * 0.6f * 0.09f;
+}
+
+// cross_quad: common.wgsl:425-487.  The two diagonal quads of a tuft voxel
+// (x - z = const: NORMAL_CROSS_A, x + z = const: NORMAL_CROSS_B), nearest
+// first; a quad hit counts where the atlas alpha at its texel exceeds the
+// voxel's hash threshold.  ro, rd and t are chunk-local (voxel units).
+// Out of line: only tuft voxels reach it, and inlined it cost the march
+// kernels registers (more spills) on every path.
+static __device__ __noinline__ bool cross_quad(const DevWorld& w, const vm_frame& f, uint32_t ux, uint32_t uy, uint32_t uz,
+                                           F3 ro, F3 rd, uint32_t layer, float vs, float shx, float shz, bool sway,
+                                           float* qt, uint32_t* qn) {
+  const float bx = (float)ux, by = (float)uy, bz = (float)uz;
+  float tsx = -1.0f, tsy = -1.0f;
+  if (sway) {
+    const float dy = ro.y - by;
+    const float ka = shx - shz, kb = shx + shz;
+    const float da = rd.x - rd.z - ka * rd.y;
+    if (fabsf(da) > 1e-6f) tsx = ((bx - bz) + ka * dy - (ro.x - ro.z)) / da;
+    const float db = rd.x + rd.z - kb * rd.y;
+    if (fabsf(db) > 1e-6f) tsy = ((bx + bz + 1.0f) + kb * dy - (ro.x + ro.z)) / db;
+  } else {
+    const float da = rd.x - rd.z;
+    if (fabsf(da) > 1e-6f) tsx = ((bx - bz) - (ro.x - ro.z)) / da;
+    const float db = rd.x + rd.z;
+    if (fabsf(db) > 1e-6f) tsy = ((bx + bz + 1.0f) - (ro.x + ro.z)) / db;
+  }
+  uint32_t o0 = VM_NORMAL_CROSS_A, o1 = VM_NORMAL_CROSS_B;
+  if (tsy < tsx) {
+    const float tt = tsx; tsx = tsy; tsy = tt;
+    o0 = VM_NORMAL_CROSS_B; o1 = VM_NORMAL_CROSS_A;
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const float tq = i == 0 ? tsx : tsy;
+    if (tq < 0.0f) continue;
+    const F3 p = ro + rd * tq;
+    const F3 local = {p.x - bx, p.y - by, p.z - bz};
+    if (local.x < -1e-4f || local.y < -1e-4f || local.z < -1e-4f || local.x > 1.0f + 1e-4f ||
+        local.y > 1.0f + 1e-4f || local.z > 1.0f + 1e-4f)
+      continue;
+    const float footprint = fmaxf(tq * vs, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs;
+    const float lod = fminf(fmaxf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f), 3.0f);
+    const float a = atlas_alpha(w, layer, local.x, 1.0f - local.y, lod);
+    if (a <= hash_alpha3(p.x, p.y, p.z)) continue;
+    *qt = tq;
+    *qn = i == 0 ? o0 : o1;
+    return true;
+  }
+  return false;
+}
+
 // march_chunk: common.wgsl:579-910.
-//   SKIP_WATER / SKIP_GLASS / SUN_RAY are the WGSL arguments of the same name
-//   (skip_foliage only gates the tuft cross-quad trace, which this build does
-//   not have: tufts are transparent, as in the oracle).
+//   SKIP_WATER / SKIP_GLASS / SUN_RAY are the WGSL arguments of the same name;
+//   skip_foliage, which gates the tuft cross-quad trace, equals sun_ray at
+//   every call site of the engine (march.wgsl:21,32; common.wgsl:1125,1172,1237).
 //   COUNT enables the per-ray traffic counters used by the roofline.
 struct Traffic { uint32_t chunk, l1, leaf, attr, pal, grid, iters, entries; };
 
 //   WANT_ID also returns the hit voxel's block id (block_at, common.wgsl:350),
 //   decoded from the L1 node and leaf slot the march already holds.
-template <bool SKIP_WATER, bool SKIP_GLASS, bool SUN_RAY, bool COUNT, bool WANT_ID = false>
+//   TUFTS compiles the tuft cross-quad trace in (the host selects such
+//   kernels only for frames whose chunks hold tufts and whose context has the
+//   atlas): the code costs the march registers on every path.
+template <bool SKIP_WATER, bool SKIP_GLASS, bool SUN_RAY, bool COUNT, bool WANT_ID = false, bool TUFTS = false>
 __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f, const Chunk& c, const Ray& r,
                                            float t_limit, Traffic* tr) {
   Hit h;
@@ -524,7 +633,25 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
       }
       if (solid && water_aware && id == VM_WATER) { solid = false; skip = (attr & VM_UNIFORM_BIT) != 0u ? 4 : 1; }
       if (solid && glass_aware && id == VM_GLASS) { solid = false; skip = (attr & VM_UNIFORM_BIT) != 0u ? 4 : 1; }
-      if (solid && foliage_aware && is_tuft(id)) { solid = false; skip = 1; }
+      if (solid && foliage_aware && is_tuft(id)) {
+        solid = false;
+        skip = 1;
+        if (TUFTS && !SUN_RAY && w.atlas_alpha != nullptr) {
+          float shx = 0.0f, shz = 0.0f;
+          const bool sway = (spec & VM_SPEC_WIND_SWAY) != 0u;
+          if (sway)
+            wind_shear(c.origin[0] + (float)ux * vs, c.origin[2] + (float)uz * vs, f.time * f.cloud_speed, &shx, &shz);
+          const uint32_t layer = w.tuft_layer[id == VM_TALL_GRASS ? 0 : (id == VM_GRASS_TALL ? 1 : 2)];
+          float qt; uint32_t qn;
+          if (cross_quad(w, f, ux, uy, uz, ro, rd, layer, vs, shx, shz, sway, &qt, &qn)) {
+            h.hit = true; h.t = qt * vs; h.normal = qn;
+            h.vx = ux; h.vy = uy; h.vz = uz;
+            h.mx = h.my = h.mz = 0u;
+            h.id = id;
+            return h;
+          }
+        }
+      }
       if (solid && cutout_aware && is_cutout_id(id)) {
         const int32_t wx = __float2int_rz(c.origin[0]) + (int32_t)ux;
         const int32_t wy = __float2int_rz(c.origin[1]) + (int32_t)uy;
@@ -590,7 +717,7 @@ __device__ __forceinline__ Hit march_chunk(const DevWorld& w, const vm_frame& f,
 // (refract(rd, -y, WATER_IOR)) and marched again from the surface; a hit
 // there replaces the miss, with t the whole path (surface distance + bent
 // leg) and the iterations of both marches.
-template <bool COUNT, bool WANT_ID>
+template <bool COUNT, bool WANT_ID, bool TUFTS = false>
 __device__ __forceinline__ void snell_bend(const DevWorld& w, const vm_frame& f, const Chunk& c, F3 rd, Hit* h,
                                            Traffic* tr) {
   if (!(rd.y > 0.0f)) return;
@@ -601,7 +728,7 @@ __device__ __forceinline__ void snell_bend(const DevWorld& w, const vm_frame& f,
   const F3 surf = ld3(f.cam_pos) + rd * t_surf;
   const F3 rd2 = refract(rd, f3(0.0f, -1.0f, 0.0f), VM_WATER_IOR);
   if (!(dot(rd2, rd2) > 0.0f)) return;
-  const Hit h2 = march_chunk<true, false, false, COUNT, WANT_ID>(w, f, c, make_ray(surf + rd2 * VM_SURFACE_EPS, rd2),
+  const Hit h2 = march_chunk<true, false, false, COUNT, WANT_ID, TUFTS>(w, f, c, make_ray(surf + rd2 * VM_SURFACE_EPS, rd2),
                                                                   f.far_ - t_surf, tr);
   if (h2.hit) {
     const uint32_t straight_iters = h->iters;
@@ -706,7 +833,7 @@ __device__ __forceinline__ bool shadow_walk_step(const DevWorld& w, const vm_fra
 struct WorldHit { bool hit; float t; uint32_t normal; uint32_t vx, vy, vz; uint32_t ci; };
 
 // trace_world: common.wgsl:1205-1253
-template <bool SKIP_WATER, bool COUNT>
+template <bool SKIP_WATER, bool COUNT, bool TUFTS = false>
 __device__ __noinline__ WorldHit trace_world(const DevWorld& w, const vm_frame& f, F3 ro, F3 rd, float max_dist, Traffic* tr) {
   WorldHit out;
   out.hit = false; out.t = max_dist; out.normal = 0u; out.vx = out.vy = out.vz = 0u; out.ci = VM_NO_CHUNK;
@@ -730,7 +857,7 @@ __device__ __noinline__ WorldHit trace_world(const DevWorld& w, const vm_frame& 
     if (tnz < t_exit) { t_exit = tnz; axis = 2u; }
     if (ci != VM_NO_CHUNK) {
       const Chunk c = ld_chunk(w, ci);
-      const Hit h = march_chunk<SKIP_WATER, true, false, COUNT>(w, f, c, r, fminf(t_exit, max_dist), tr);
+      const Hit h = march_chunk<SKIP_WATER, true, false, COUNT, false, TUFTS>(w, f, c, r, fminf(t_exit, max_dist), tr);
       if (h.hit) {
         out.hit = true; out.t = h.t; out.normal = h.normal;
         out.vx = h.vx; out.vy = h.vy; out.vz = h.vz; out.ci = ci;
@@ -766,7 +893,7 @@ __device__ __forceinline__ WorldWalk world_walk_begin(F3 ro, F3 rd) {
   s.step = 0u;
   return s;
 }
-template <bool SKIP_WATER, bool COUNT>
+template <bool SKIP_WATER, bool COUNT, bool TUFTS = false>
 __device__ __forceinline__ bool world_walk_step(const DevWorld& w, const vm_frame& f, WorldWalk& s, float max_dist,
                                                 WorldHit* out, Traffic* tr) {
   out->hit = false; out->t = max_dist; out->normal = 0u; out->vx = out->vy = out->vz = 0u; out->ci = VM_NO_CHUNK;
@@ -790,7 +917,7 @@ __device__ __forceinline__ bool world_walk_step(const DevWorld& w, const vm_fram
     bool marched = false;   // a chunk march that took DDA steps
     if (ci != VM_NO_CHUNK) {
       const Chunk c = ld_chunk(w, ci);
-      const Hit h = march_chunk<SKIP_WATER, true, false, COUNT>(w, f, c, s.r, fminf(t_exit, max_dist), tr);
+      const Hit h = march_chunk<SKIP_WATER, true, false, COUNT, false, TUFTS>(w, f, c, s.r, fminf(t_exit, max_dist), tr);
       if (h.hit) {
         out->hit = true; out->t = h.t; out->normal = h.normal;
         out->vx = h.vx; out->vy = h.vy; out->vz = h.vz; out->ci = ci;

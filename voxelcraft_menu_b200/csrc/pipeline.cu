@@ -46,7 +46,8 @@ __device__ __forceinline__ const vm_frame& frame_of(const PipeArgs& a, uint32_t 
 __device__ __forceinline__ ViewDesc view_of(const PipeArgs& a, uint32_t v) { return a.frames ? a.views[v] : a.view0; }
 __device__ __forceinline__ DevWorld world_of(const PipeArgs& a, const ViewDesc& vd) {
   return {a.chunks + vd.chunk_off, vd.n_chunks, a.inners, a.n_inners, a.leaves, a.n_leaves,
-          a.bricks, a.n_bricks, a.grids + vd.grid_off, vd.grid_len, a.err, a.spec};
+          a.bricks, a.n_bricks, a.grids + vd.grid_off, vd.grid_len, a.err, a.spec, a.atlas_alpha, a.atlas_layers,
+          {a.tuft_layer[0], a.tuft_layer[1], a.tuft_layer[2]}};
 }
 
 // The same, resolved at compile time when the launch is known to carry one
@@ -354,7 +355,7 @@ __device__ __forceinline__ void flush_traffic(const PipeArgs& a, int stage, cons
 
 // One lane, one pixel, one chunk: march it and fold the key into the pixel's
 // best (the engine's atomicMax), keeping the best hit's block id.
-template <bool UNDERWATER, bool COUNT>
+template <bool UNDERWATER, bool COUNT, bool TUFTS>
 __device__ __forceinline__ void march_entry(const DevWorld& w, const vm_frame& f, const Ray& ray, uint32_t ci,
                                             uint32_t px, uint32_t py, unsigned long long& best, uint32_t& best_id,
                                             Traffic* tr) {
@@ -375,8 +376,8 @@ __device__ __forceinline__ void march_entry(const DevWorld& w, const vm_frame& f
   // as the engine marches it) is what lets the bent ray count, so the
   // distance limit is not applied to it.
   const bool bend = UNDERWATER && (w.spec & VM_SPEC_SNELL_BEND) != 0u;
-  Hit h = march_chunk<UNDERWATER, false, false, COUNT, true>(w, f, c, ray, bend ? f.far_ : t_lim, tr);
-  if (bend && !h.hit) snell_bend<COUNT, true>(w, f, c, ray.d, &h, tr);
+  Hit h = march_chunk<UNDERWATER, false, false, COUNT, true, TUFTS>(w, f, c, ray, bend ? f.far_ : t_lim, tr);
+  if (bend && !h.hit) snell_bend<COUNT, true, TUFTS>(w, f, c, ray.d, &h, tr);
   if (h.hit) {
     const unsigned long long k = make_key(f, h, ci);
     if (k > best) { best = k; best_id = h.id; }
@@ -386,7 +387,7 @@ __device__ __forceinline__ void march_entry(const DevWorld& w, const vm_frame& f
 // The rest of tile_select's scan when a tile's list overflowed its capacity:
 // 32 chunks culled per step across the warp, each survivor marched in order.
 // Cold code, kept out of the primary loop's instruction stream.
-template <bool UNDERWATER, bool COUNT>
+template <bool UNDERWATER, bool COUNT, bool TUFTS>
 __device__ __noinline__ void march_overflow(const DevWorld w, const vm_frame& f, const Ray ray, uint32_t start,
                                             uint32_t tx, uint32_t ty, uint32_t px, uint32_t py,
                                             const uint32_t* dk, const uint32_t* suf, bool active,
@@ -407,7 +408,7 @@ __device__ __noinline__ void march_overflow(const DevWorld w, const vm_frame& f,
       const uint32_t bestd = (uint32_t)(b >> 40);
       if (suf[cj] < bestd) { active = false; continue; }
       if (dk[cj] < bestd) continue;
-      march_entry<UNDERWATER, COUNT>(w, f, ray, cj, px, py, b, id, tr);
+      march_entry<UNDERWATER, COUNT, TUFTS>(w, f, ray, cj, px, py, b, id, tr);
     }
   }
   *best = b;
@@ -420,6 +421,7 @@ __device__ __noinline__ void march_overflow(const DevWorld w, const vm_frame& f,
 // float operations as in k_primary (same values), and the code is out of
 // line, so the primary kernel's register allocation stays that of frames
 // without reflect legs.  Called by the whole warp.
+template <bool TUFTS>
 __device__ __noinline__ void enqueue_reflect(const PipeArgs& a, uint32_t v, uint32_t px, uint32_t py, uint64_t pix,
                                              bool valid, unsigned long long key) {
   const vm_frame& f = frame_of(a, v);
@@ -431,7 +433,7 @@ __device__ __noinline__ void enqueue_reflect(const PipeArgs& a, uint32_t v, uint
     const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
     const float th = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
     if (water_reflects(f, th)) {
-      rr = reflect_ray<false>(world_of(a, view_of(a, v)), f, ld3(f.cam_pos) + rd * th, rd, k.nid, th, nullptr);
+      rr = reflect_ray<false, TUFTS>(world_of(a, view_of(a, v)), f, ld3(f.cam_pos) + rd * th, rd, k.nid, th, nullptr);
       want = true;
     }
   }
@@ -459,7 +461,9 @@ __device__ __noinline__ void enqueue_reflect(const PipeArgs& a, uint32_t v, uint
 // pixels one after the other and starts its next pixel as soon as one is
 // done, so lanes whose rays end early do not idle until the warp's slowest
 // ray ends; the pixels' results are then finished together.
-template <int NW, int MINB, bool UNDERWATER, bool COUNT, bool REFL, bool SINGLE, int PX>
+// TUFTS: the chunks hold foliage tufts and the context has the atlas: the
+// march traces their cross quads (a generic shape, selected per frame).
+template <int NW, int MINB, bool UNDERWATER, bool COUNT, bool REFL, bool SINGLE, int PX, bool TUFTS = false>
 __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant__ PipeArgs a) {
   static_assert(PX == 1 || PX == 2, "one or two pixels per lane");
   const uint32_t lane = threadIdx.x & 31u;
@@ -543,7 +547,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
         best = 0ull; best_id = 0u; active = valid; i = 0;
       }
       if (!__any_sync(FULLMASK, go)) break;
-      if (go) march_entry<UNDERWATER, COUNT>(w, f, ray, ci, px, py, best, best_id, &tr);
+      if (go) march_entry<UNDERWATER, COUNT, TUFTS>(w, f, ray, ci, px, py, best, best_id, &tr);
     }
 #pragma unroll
     for (uint32_t slot = 0; slot < (uint32_t)PX; ++slot) {
@@ -556,7 +560,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
     const bool pvalid = px < f.res[0] && ppy < f.res[1];
     const F3 prd = last ? rd : ray_dir(f, (float)px + 0.5f, (float)ppy + 0.5f);
     if (n > a.list_cap)
-      march_overflow<UNDERWATER, COUNT>(w, f, last ? ray : make_ray(cam, prd), (uint32_t)list[a.list_cap - 1] + 1u,
+      march_overflow<UNDERWATER, COUNT, TUFTS>(w, f, last ? ray : make_ray(cam, prd), (uint32_t)list[a.list_cap - 1] + 1u,
                                         tx, ty, px, ppy, dk, suf, pactive, &pbest, &pbest_id, &tr);
     const uint64_t pix = (uint64_t)ppy * f.res[0] + px;
     if (pvalid) a.vis[vd.pix_off + pix] = pbest;
@@ -635,7 +639,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_primary(const __grid_constant
       }
     }
     if (REFL && a.do_reflect)
-      enqueue_reflect(a, v, px, ppy, vd.pix_off + pix, pvalid, pvalid && pbest_id == VM_WATER ? pbest : 0ull);
+      enqueue_reflect<TUFTS>(a, v, px, ppy, vd.pix_off + pix, pvalid, pvalid && pbest_id == VM_WATER ? pbest : 0ull);
     }
     if (lane == 0) {
       const uint32_t cost = (uint32_t)min(clock64() - clk0, 0xFFFFFFFFll);
@@ -722,7 +726,7 @@ __global__ void __launch_bounds__(256, 4) k_shadow(const __grid_constant__ PipeA
 // refract and reflect legs of water hits, transmission through glass — on
 // persistent lanes like k_shadow: one chunk-grid cell per step, the next ray
 // taken as soon as a lane's ray ends.
-template <bool COUNT, bool SINGLE>
+template <bool COUNT, bool SINGLE, bool TUFTS = false>
 __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ PipeArgs a) {
   // a shadow kernel launched after this one with programmatic serialization
   // may take the SMs this kernel's blocks leave (it reads nothing this kernel
@@ -764,8 +768,8 @@ __global__ void __launch_bounds__(256, 4) k_secondary_q(const __grid_constant__ 
       const ViewDesc vd = view_t<SINGLE>(a, view);
       const DevWorld w = world_of(a, vd);
       WorldHit h;
-      const bool over = water ? world_walk_step<true, COUNT>(w, f, s, max_dist, &h, &tr)
-                              : world_walk_step<false, COUNT>(w, f, s, max_dist, &h, &tr);
+      const bool over = water ? world_walk_step<true, COUNT, TUFTS>(w, f, s, max_dist, &h, &tr)
+                              : world_walk_step<false, COUNT, TUFTS>(w, f, s, max_dist, &h, &tr);
       if (over) {
         // the key of secondary_trace: traced, glass, hit and the hit's fields
         unsigned long long k = (1ull << 63) | (water ? 0ull : (1ull << 61));
@@ -816,15 +820,31 @@ static void* primary_nw(int level, bool uw, bool refl, bool single) {
 }
 
 // the counting run is never timed: 4 warps, unconstrained registers, one
-// pixel per lane, the reflect code behind its runtime flag
+// pixel per lane, the reflect code behind its runtime flag, tufts traced
 static void* primary_count(bool uw, bool single) {
   if (single)
-    return uw ? (void*)k_primary<4, 1, true, true, true, true, 1> : (void*)k_primary<4, 1, false, true, true, true, 1>;
-  return uw ? (void*)k_primary<4, 1, true, true, false, false, 1> : (void*)k_primary<4, 1, false, true, false, false, 1>;
+    return uw ? (void*)k_primary<4, 1, true, true, true, true, 1, true>
+              : (void*)k_primary<4, 1, false, true, true, true, 1, true>;
+  return uw ? (void*)k_primary<4, 1, true, true, false, false, 1, true>
+            : (void*)k_primary<4, 1, false, true, false, false, 1, true>;
 }
 
-static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt, bool refl, bool single) {
+// frames with tufts: one generic shape (4 warps, unconstrained registers, one
+// pixel per lane), the tuned shapes stay free of the cross-quad code
+static void* primary_tufts(bool uw, bool refl, bool single) {
+  if (!single)
+    return uw ? (void*)k_primary<4, 1, true, false, false, false, 1, true>
+              : (void*)k_primary<4, 1, false, false, false, false, 1, true>;
+  if (refl)
+    return uw ? (void*)k_primary<4, 1, true, false, true, true, 1, true>
+              : (void*)k_primary<4, 1, false, false, true, true, 1, true>;
+  return uw ? (void*)k_primary<4, 1, true, false, false, true, 1, true>
+            : (void*)k_primary<4, 1, false, false, false, true, 1, true>;
+}
+
+static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt, bool refl, bool single, bool tufts) {
   if (cnt) return primary_count(uw, single);
+  if (tufts) return primary_tufts(uw, refl, single);
   const int px = t.px_per_lane == 2 ? 2 : 1;
   switch (t.primary_warps * 4 + px) {
     case 4 * 4 + 1: return primary_nw<4, 1>(t.reg_level, uw, refl, single);
@@ -835,16 +855,17 @@ static void* primary_kernel(const PipeTuning& t, bool uw, bool cnt, bool refl, b
   return nullptr;
 }
 
-// pixels per lane of the primary kernel a launch runs
+// pixels per lane of the primary kernel a launch runs (cnt: the counting or
+// the tuft kernel, whose shape is fixed)
 static int packet_of(const PipeTuning& t, bool cnt) { return cnt ? 1 : (t.px_per_lane == 2 ? 2 : 1); }
 
 static int block_warps(const PipeTuning& t, bool cnt) { return cnt ? 4 : t.primary_warps; }
 
-int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bool reflect, bool single) {
-  void* fn = primary_kernel(t, underwater, count, reflect, single);
+int primary_max_ctas_per_sm(const PipeTuning& t, bool underwater, bool count, bool reflect, bool single, bool tufts) {
+  void* fn = primary_kernel(t, underwater, count, reflect, single, tufts);
   if (!fn) return 0;
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block_warps(t, count) * 32, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block_warps(t, count || tufts) * 32, 0);
   return n;
 }
 
@@ -898,14 +919,15 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   if ((e = launch_after(k_order, (a.total_tiles + ORDER_TILES - 1) / ORDER_TILES, 256u, s, a)) != cudaSuccess)
     return e;
   if ((e = mark(1)) != cudaSuccess) return e;
-  const bool refl = a.do_reflect != 0u, single = a.frames == nullptr;
-  void* fn = primary_kernel(t, underwater, count, refl, single);
+  const bool refl = a.do_reflect != 0u, single = a.frames == nullptr, tufts = a.tufts != 0u;
+  void* fn = primary_kernel(t, underwater, count, refl, single, tufts);
   if (!fn) return cudaErrorInvalidValue;
-  const int nw = block_warps(t, count);
-  int per = t.ctas_per_sm > 0 && !count ? t.ctas_per_sm
-                                        : primary_max_ctas_per_sm(t, underwater, count, refl, single);
+  const bool fixed = count || tufts;   // a shape the tuning does not choose
+  const int nw = block_warps(t, fixed);
+  int per = t.ctas_per_sm > 0 && !fixed ? t.ctas_per_sm
+                                        : primary_max_ctas_per_sm(t, underwater, count, refl, single, tufts);
   if (per <= 0) per = 1;
-  const uint32_t items_blocks = (a.total_tiles * (2u / (uint32_t)packet_of(t, count)) + nw - 1) / nw;
+  const uint32_t items_blocks = (a.total_tiles * (2u / (uint32_t)packet_of(t, fixed)) + nw - 1) / nw;
   const uint32_t grid = std::min<uint32_t>((uint32_t)sms * (uint32_t)per, items_blocks);
   void* args[] = {(void*)&a};
   if ((e = cudaLaunchKernel(fn, dim3(grid), dim3(nw * 32), args, 0, s)) != cudaSuccess) return e;
@@ -918,7 +940,8 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
     // before either starts, so its blocks take the SMs the few long water /
     // glass walks leave instead of waiting for the last of them.  Events 3
     // and 4 both follow the two kernels.
-    k_secondary_q<false, true><<<(uint32_t)sms * 4u, 256, 0, s>>>(a);
+    if (tufts) k_secondary_q<false, true, true><<<(uint32_t)sms * 4u, 256, 0, s>>>(a);
+    else k_secondary_q<false, true><<<(uint32_t)sms * 4u, 256, 0, s>>>(a);
     if ((e = launch_after(k_shadow<false, true>, q_blocks, 256u, s, a)) != cudaSuccess) return e;
     if ((e = mark(3)) != cudaSuccess) return e;
     if ((e = mark(4)) != cudaSuccess) return e;
@@ -932,9 +955,11 @@ cudaError_t launch_pipeline(const PipeArgs& a, const PipeTuning& t, bool underwa
   }
   if ((e = mark(3)) != cudaSuccess) return e;
   if (a.do_secondary) {
-    if (count && single) k_secondary_q<true, true><<<q_blocks, 256, 0, s>>>(a);
-    else if (count) k_secondary_q<true, false><<<q_blocks, 256, 0, s>>>(a);
+    if (count && single) k_secondary_q<true, true, true><<<q_blocks, 256, 0, s>>>(a);
+    else if (count) k_secondary_q<true, false, true><<<q_blocks, 256, 0, s>>>(a);
+    else if (single && tufts) k_secondary_q<false, true, true><<<q_blocks, 256, 0, s>>>(a);
     else if (single) k_secondary_q<false, true><<<q_blocks, 256, 0, s>>>(a);
+    else if (tufts) k_secondary_q<false, false, true><<<q_blocks, 256, 0, s>>>(a);
     else k_secondary_q<false, false><<<q_blocks, 256, 0, s>>>(a);
   }
   if ((e = mark(4)) != cudaSuccess) return e;

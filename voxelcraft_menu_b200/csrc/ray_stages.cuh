@@ -125,16 +125,17 @@ __device__ __forceinline__ bool water_reflects(const vm_frame& f, float t) {
   if ((f.flags & VM_FLAG_WATER_REFLECT) == 0u) return false;
   return 1.0f - smoothstep(VM_WATER_REFLECT_NEAR, VM_WATER_REFLECT_FAR, t) > 0.0f;
 }
-template <bool COUNT>
+template <bool COUNT, bool TUFTS = false>
 __device__ __forceinline__ SecRay reflect_ray(const DevWorld& w, const vm_frame& f, F3 hit, F3 rd, uint32_t nid,
                                               float t, Traffic* tr) {
   SecRay s;
   s.o = hit + normal_of(nid) * VM_SURFACE_EPS;
-  s.d = water_mirror_t<COUNT>(w, f, nid, hit, rd, t, tr);
+  s.d = water_mirror_t<COUNT, TUFTS>(w, f, nid, hit, rd, t, tr);
   s.max_dist = VM_WATER_REFLECT_DIST;
   s.water = true;
   return s;
 }
+template <bool TUFTS>
 __device__ __forceinline__ bool reflect_setup(const DevWorld& w, const vm_frame& f, unsigned long long key,
                                               uint32_t px, uint32_t py, SecRay* s) {
   if (key == 0ull) return false;
@@ -144,15 +145,15 @@ __device__ __forceinline__ bool reflect_setup(const DevWorld& w, const vm_frame&
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
   if (!water_reflects(f, t)) return false;
-  *s = reflect_ray<false>(w, f, ld3(f.cam_pos) + rd * t, rd, k.nid, t, nullptr);
+  *s = reflect_ray<false, TUFTS>(w, f, ld3(f.cam_pos) + rd * t, rd, k.nid, t, nullptr);
   return true;
 }
 
-template <bool COUNT>
+template <bool COUNT, bool TUFTS>
 __device__ __forceinline__ void secondary_trace(const DevWorld& w, const vm_frame& f, const SecRay& s,
                                                 unsigned long long* out_key, float* out_t, Traffic* tr) {
-  const WorldHit h = s.water ? trace_world<true, COUNT>(w, f, s.o, s.d, s.max_dist, tr)
-                             : trace_world<false, COUNT>(w, f, s.o, s.d, s.max_dist, tr);
+  const WorldHit h = s.water ? trace_world<true, COUNT, TUFTS>(w, f, s.o, s.d, s.max_dist, tr)
+                             : trace_world<false, COUNT, TUFTS>(w, f, s.o, s.d, s.max_dist, tr);
   unsigned long long k = (1ull << 63) | (s.water ? 0ull : (1ull << 61));
   if (h.hit)
     k |= (1ull << 62) | ((unsigned long long)h.normal << 37) | ((unsigned long long)h.ci << 24) |

@@ -73,6 +73,17 @@ inline bool column_tree(const vmw_recipe& r, int32_t x, int32_t z, int32_t h) {
   return h > 0 && dry && r.tree_permille > 0 && hash3(x, 7, z, r.seed ^ 0x7777u) % 1000u < r.tree_permille;
 }
 
+// A foliage tuft on the first air block of a dry grass column without a tree:
+// TALL_GRASS, GRASS_TALL or REEDS by the column's hash.
+inline uint16_t column_tuft(const vmw_recipe& r, int32_t x, int32_t z, int32_t h, bool tree) {
+  if (tree || h <= 0 || r.tuft_permille == 0) return VM_AIR;
+  if (r.water_level >= 0 && h - 1 < r.water_level) return VM_AIR;
+  const uint32_t k = hash3(x, 11, z, r.seed ^ 0x3131u);
+  if (k % 1000u >= r.tuft_permille) return VM_AIR;
+  const uint16_t ids[3] = {VM_TALL_GRASS, VM_GRASS_TALL, VM_REEDS};
+  return ids[(k >> 10) % 3u];
+}
+
 struct Heights {
   uint32_t sx = 0, sz = 0;
   std::vector<int32_t> h;
@@ -121,6 +132,8 @@ inline void fill_chunk(const vmw_recipe& r, const Heights& hs, int32_t cx, int32
             id = VM_GLASS;
         } else if (r.water_level >= 0 && y < r.water_level && (r.island_permille == 0 || y >= r.water_level - r.water_depth)) {
           id = VM_WATER;
+        } else if (y == h) {
+          id = column_tuft(r, x, z, h, hs.tree[(size_t)z * hs.sx + x] != 0);
         }
         dense[lx | (lz << 6) | (ly << 12)] = id;
       }

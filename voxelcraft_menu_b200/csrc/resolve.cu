@@ -10,7 +10,7 @@
 
 namespace vmd {
 
-__device__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx, uint32_t vy,
+__device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx, uint32_t vy,
                             uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist, float lit_in) {
   const Chunk c = ld_chunk(w, ci);
   const float vs = c.vs;
@@ -90,15 +90,12 @@ __device__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L,
     const bool local_only = ax - sx >= 0 && ay - sy >= 0 && az - sz >= 0 && ax + sx <= 63 && ay + sy <= 63 &&
                             az + sz <= 63;
     uint2 nb[9];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-      const int32_t da = i % 3 - 1, db = i / 3 - 1;
-      if (local_only) {
-        nb[i] = gather_one(w, c, ax + ta[0] * da + tb[0] * db, ay + ta[1] * da + tb[1] * db,
-                           az + ta[2] * da + tb[2] * db);
-      } else {
+    if (local_only) {
+      gather_face(w, c, ax, ay, az, ta[0], ta[1], ta[2], tb[0], tb[1], tb[2], nb);
+    } else {
+#pragma unroll 1
+      for (int i = 0; i < 9; ++i)
         nb[i] = world_sample(w, f, air_c + step_a * ((float)(i % 3) - 1.0f) + step_b * ((float)(i / 3) - 1.0f));
-      }
     }
     float sky_n[9], blk_n[9], open_n[9];
     uint32_t any_blk = 0u;
@@ -215,7 +212,8 @@ __device__ __forceinline__ float sun_visibility(const float* mask, const float* 
   return floorf(clampf(m, 0.0f, 1.0f) * 255.0f + 0.5f) / 255.0f;
 }
 
-__global__ void __launch_bounds__(128) k_resolve(const vm_frame f, const DevWorld w, const Look L,
+__global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_frame f, const __grid_constant__ DevWorld w,
+                                                 const __grid_constant__ Look L,
                                                  const unsigned long long* __restrict__ vis,
                                                  const float* __restrict__ mask, const float* __restrict__ dist,
                                                  bool soft, float4* __restrict__ out) {

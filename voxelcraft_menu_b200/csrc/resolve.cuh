@@ -14,7 +14,10 @@
 // agree up to the last bits of the transcendental functions.
 //
 // Compiled with the march's float contract (--fmad=false): block lookups
-// and voxel indices must match the march exactly.
+// and voxel indices must match the march exactly.  The larger helpers (sky,
+// cloud octaves, biome noise, light samples, texture filters, shafts) stay
+// out of line: inlined at every call site the kernel's code outgrew the
+// instruction cache and its warps stalled on instruction fetch.
 #pragma once
 #include <cuda_fp16.h>
 #include "march_device.cuh"
@@ -80,7 +83,7 @@ __device__ __forceinline__ F3 sky_zenith(const Look& L, float day) {
   return mix3(f3(0.0008f, 0.0015f, 0.0039f), day_z, day);
 }
 
-__device__ __forceinline__ F3 sky_base(const vm_frame& f, const Look& L, F3 rd, float shaft) {
+static __device__ __noinline__ F3 sky_base(const vm_frame& f, const Look& L, F3 rd, float shaft) {
   const float day = f.daylight;
   const float up = clampf(rd.y, 0.0f, 1.0f);
   const F3 horizon = sky_horizon(L, day);
@@ -125,7 +128,7 @@ __device__ __forceinline__ float cloud_noise(float px, float py) {
   return mixf(mixf(a, b, wx), mixf(d, e, wx), wy);
 }
 
-__device__ __forceinline__ float cloud_fbm(float px, float py, float fp) {
+static __device__ __noinline__ float cloud_fbm(float px, float py, float fp) {
   float freq = 1.0f, amp = 1.0f, sum = 0.0f, norm = 0.0f;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -168,7 +171,7 @@ __device__ __forceinline__ F3 cloud_radiance(const vm_frame& f, const Look& L, f
   return mix3(f3(0.0021f, 0.0026f, 0.0052f), day_c, day) + glow;
 }
 
-__device__ __forceinline__ F3 sky_color(const vm_frame& f, const Look& L, F3 ro, F3 rd, float travelled, float shaft) {
+static __device__ __noinline__ F3 sky_color(const vm_frame& f, const Look& L, F3 ro, F3 rd, float travelled, float shaft) {
   const F3 base = sky_base(f, L, rd, shaft);
   if (f.cloud_cover <= 0.0f) return base;
   const float dy = f.cloud_height - ro.y;
@@ -211,7 +214,7 @@ __device__ __forceinline__ float shaft_at(const Look& L, uint32_t x, uint32_t y)
   return __ldg(L.shaft + (uint64_t)y * VM_SHAFT_DIM + x);
 }
 
-__device__ __forceinline__ float terrain_shade(const vm_frame& f, const Look& L, F3 p) {
+static __device__ __noinline__ float terrain_shade(const vm_frame& f, const Look& L, F3 p) {
   if (L.shaft == nullptr) return 1.0f;
   const float tx = (p.x - f.shaft_origin[0]) / f.shaft_texel - 0.5f;
   const float tz = (p.z - f.shaft_origin[1]) / f.shaft_texel - 0.5f;
@@ -233,7 +236,7 @@ __device__ __forceinline__ float dither(const vm_frame& f, uint32_t px, uint32_t
   return fractf(52.9829189f * fractf(p0 * 0.06711056f + p1 * 0.00583715f));
 }
 
-__device__ __forceinline__ float sun_shaft(const vm_frame& f, const Look& L, F3 ro, F3 rd, float dist, float alpha,
+static __device__ __noinline__ float sun_shaft(const vm_frame& f, const Look& L, F3 ro, F3 rd, float dist, float alpha,
                                            uint32_t px, uint32_t py) {
   const bool terrain = (f.flags & VM_FLAG_TERRAIN_SHAFTS) != 0u;
   const bool deck = f.cloud_shadow > 0.0f && f.cloud_cover > 0.0f;
@@ -301,7 +304,7 @@ __device__ __forceinline__ bool voxel_occludes(const DevWorld& w, const Chunk& c
 }
 
 // world_sample: common.wgsl:1015-1032 (light word, occluding bit)
-__device__ __forceinline__ uint2 world_sample(const DevWorld& w, const vm_frame& f, F3 p) {
+static __device__ __noinline__ uint2 world_sample(const DevWorld& w, const vm_frame& f, F3 p) {
   uint64_t gi;
   if (!grid_rel(f, ffloor_i(p.x * INV64), ffloor_i(p.y * INV64), ffloor_i(p.z * INV64), &gi))
     return make_uint2(LIGHT_OPEN_SKY, 0u);
@@ -315,13 +318,67 @@ __device__ __forceinline__ uint2 world_sample(const DevWorld& w, const vm_frame&
   return make_uint2(light_at(w, c, vx, vy, vz), voxel_occludes(w, c, vx, vy, vz) ? 1u : 0u);
 }
 
-// gather_face: common.wgsl:1034-1096.  Unlike voxel_occludes it keeps tufts
-// solid (only water is cleared).
-__device__ __forceinline__ uint2 gather_one(const DevWorld& w, const Chunk& c, int32_t x, int32_t y, int32_t z) {
-  bool solid = voxel_occupied(w, c, x, y, z);
-  if (solid && (c.attr_flags & VM_ATTR_HAS_WATER) != 0u)
-    solid = block_at(w, c, (uint32_t)x, (uint32_t)y, (uint32_t)z) != VM_WATER;
-  return make_uint2(light_at(w, c, x, y, z), solid ? 1u : 0u);
+// gather_face: common.wgsl:1034-1096.  The nine air voxels of a face's 3x3
+// neighbourhood inside one chunk: occupancy (only water cleared, unlike
+// voxel_occludes, which also clears tufts) and light word.  The samples walk
+// a 3x3 square, so the L1 node, leaf mask and light cell of the previous
+// sample are kept, as the engine's loop keeps them.
+static __device__ __noinline__ void gather_face(const DevWorld& w, const Chunk& c, int32_t bx, int32_t by, int32_t bz,
+                                                int32_t tax, int32_t tay, int32_t taz, int32_t tbx, int32_t tby,
+                                                int32_t tbz, uint2* out) {
+  const uint32_t root_lo = c.root[0], root_hi = c.root[1];
+  const bool root_full = (c.root[2] & VM_FULL_BIT) != 0u;
+  const uint32_t root_ptr = c.root[2] & VM_PTR_MASK;
+  const bool light_uniform = (c.light_flags & 1u) != 0u;
+  const bool has_water = (c.attr_flags & VM_ATTR_HAS_WATER) != 0u;
+  uint32_t l1_key = 0xFFFFFFFFu, leaf_key = 0xFFFFFFFFu, brick_key = 0xFFFFFFFFu;
+  uint4 l1 = make_uint4(0u, 0u, 0u, 0u);
+  uint2 leaf = make_uint2(0u, 0u);
+  uint32_t brick = 0u;
+  for (int i = 0; i < 9; ++i) {
+    const int32_t da = i % 3 - 1, db = i / 3 - 1;
+    const uint32_t ux = (uint32_t)(bx + tax * da + tbx * db), uy = (uint32_t)(by + tay * da + tby * db),
+                   uz = (uint32_t)(bz + taz * da + tbz * db);
+    bool solid = false;
+    const uint32_t l1b = cell_bit(ux >> 4, uy >> 4, uz >> 4);
+    if (mask_has(root_lo, root_hi, l1b)) {
+      if (root_full) {
+        solid = true;
+      } else {
+        if (l1b != l1_key) {
+          l1_key = l1b;
+          l1 = ld_inner(w, (uint64_t)root_ptr + mask_below(root_lo, root_hi, l1b));
+          leaf_key = 0xFFFFFFFFu;
+        }
+        const uint32_t lfb = cell_bit((ux >> 2) & 3u, (uy >> 2) & 3u, (uz >> 2) & 3u);
+        if ((l1.z & VM_FULL_BIT) != 0u) {
+          solid = true;
+        } else if (mask_has(l1.x, l1.y, lfb)) {
+          if (lfb != leaf_key) {
+            leaf_key = lfb;
+            leaf = ld_leaf(w, (uint64_t)(l1.z & VM_PTR_MASK) + mask_below(l1.x, l1.y, lfb));
+          }
+          solid = mask_has(leaf.x, leaf.y, cell_bit(ux & 3u, uy & 3u, uz & 3u));
+        }
+      }
+    }
+    if (solid && has_water) solid = block_at(w, c, ux, uy, uz) != VM_WATER;
+    uint32_t packed = c.light_base;
+    if (!light_uniform) {
+      const uint32_t cell = (ux >> 2) | ((uy >> 2) << 4) | ((uz >> 2) << 8);
+      if (cell != brick_key) {
+        brick_key = cell;
+        brick = ld_brick(w, (uint64_t)c.light_base + cell);
+      }
+      if ((brick & VM_UNIFORM_BIT) != 0u) {
+        packed = brick & 0xFFFFu;
+      } else {
+        const uint32_t vb = cell_bit(ux & 3u, uy & 3u, uz & 3u);
+        packed = (ld_brick(w, (uint64_t)brick + (vb >> 1)) >> ((vb & 1u) * 16u)) & 0xFFFFu;
+      }
+    }
+    out[i] = make_uint2(packed, solid ? 1u : 0u);
+  }
 }
 
 __device__ __forceinline__ float light_sky(uint32_t p) { return (float)(p >> 12u); }
@@ -364,7 +421,7 @@ __device__ __forceinline__ F3 sky_ambient_tint(const vm_frame& f, const Look& L,
   return t * (0.70721556f / fmaxf(luma, 1e-6f));
 }
 __device__ __forceinline__ bool lighting_repair(const Look& L) { return (L.spec_hi & HI_LEGACY_LIGHTING) == 0u; }
-__device__ __forceinline__ F3 surface_sky_fill(const vm_frame& f, const Look& L, F3 n) {
+static __device__ __noinline__ F3 surface_sky_fill(const vm_frame& f, const Look& L, F3 n) {
   const F3 sky = sky_ambient_tint(f, L, n);
   if (!lighting_repair(L)) return sky;
   return sky * (0.60f * mixf(0.35f, 1.0f, clampf(n.y * 0.5f + 0.5f, 0.0f, 1.0f)));
@@ -403,7 +460,7 @@ __device__ __forceinline__ float4 atlas_bilinear(const Look& L, uint32_t mip, ui
   const float4 t01 = atlas_texel(L, base, size, layer, ix, iy1), t11 = atlas_texel(L, base, size, layer, ix1, iy1);
   return mix4(mix4(t00, t10, ax), mix4(t01, t11, ax), ay);
 }
-__device__ __forceinline__ float4 atlas_sample(const Look& L, float u, float v, uint32_t layer, float lod) {
+static __device__ __noinline__ float4 atlas_sample(const Look& L, float u, float v, uint32_t layer, float lod) {
   layer = min(layer, L.atlas_layers - 1u);   // an array index past the last layer reads the last one
   if (!(lod > 0.0f)) {
     const int32_t x = ffloor_i(u * (float)ATLAS_SIZE), y = ffloor_i(v * (float)ATLAS_SIZE);
@@ -428,7 +485,7 @@ __device__ __forceinline__ float4 probe_texel(const Look& L, int32_t x, int32_t 
   return make_float4(__half2float(__ushort_as_half(h.x)), __half2float(__ushort_as_half(h.y)),
                      __half2float(__ushort_as_half(h.z)), __half2float(__ushort_as_half(h.w)));
 }
-__device__ __forceinline__ float4 probe_field(const Look& L, F3 p, uint32_t nid) {
+static __device__ __noinline__ float4 probe_field(const Look& L, F3 p, uint32_t nid) {
   if (L.probes == nullptr) return make_float4(1.0f, 1.0f, 1.0f, 1.0f);
   const uint32_t slab = nid >= VM_NORMAL_CROSS_A ? 3u : nid;
   const F3 t = p * 0.25f;
@@ -499,7 +556,7 @@ __device__ __forceinline__ int32_t biome_fast_floor(float f) {
   const int32_t i = __float2int_rz(f);
   return f >= 0.0f ? i : i - 1;
 }
-__device__ __forceinline__ float biome_noise(const Look& L, int32_t seed_i, float freq, float px, float pz) {
+static __device__ __noinline__ float biome_noise(const Look& L, int32_t seed_i, float freq, float px, float pz) {
   const uint32_t seed = (uint32_t)seed_i;
   const float sqrt3 = 1.7320508075688772f;
   const float g2 = (3.0f - sqrt3) / 6.0f;
@@ -573,7 +630,7 @@ __device__ __forceinline__ float face_shade(uint32_t nid) {
 // ---------------------------------------------------------------------------
 // shade_hit_legacy_cached: resolve.wgsl:1537-1788 (smooth_light and do_spec
 // on, the sun visibility read from the frame's shadow mask)
-__device__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx, uint32_t vy,
+__device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx, uint32_t vy,
                             uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist, float lit_in);
 
 }  // namespace vmd

@@ -284,6 +284,9 @@ static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
  * Every bit of the engine's frame flags word is taken, so the switch is a
  * specialisation of the context, not a frame flag. */
 #define VM_SPEC_SOFT_RAYS 256u
+/* SPEC_WIND_SWAY (FLAG_HI_WIND_SWAY, src/render/mod.rs:232): tuft quads sheared by the wind
+ * (common.wgsl:419-423, 433-447); off in the engine's default configuration. */
+#define VM_SPEC_WIND_SWAY 512u
 #define VM_SURFACE_EPS 0.02f          /* common.wgsl:1258 */
 #define VM_WATER_IOR 1.333f           /* common.wgsl:1256 */
 #define VM_WATER_REFRACT_DIST 96.0f   /* resolve.wgsl:879 */

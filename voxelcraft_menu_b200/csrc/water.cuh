@@ -77,7 +77,7 @@ __device__ __forceinline__ F3 unit(F3 v) {   // WGSL normalize: v / sqrt(dot(v, 
 // mirror_t): reflect(rd, nt), with nt the wave normal for FLAG_WAVES on a +Y
 // face, limited by wave_reflect_slope and pulled to the face normal by the
 // optical roughness; a waved direction never points below the horizon.
-template <bool COUNT>
+template <bool COUNT, bool TUFTS = false>
 __device__ __forceinline__ F3 water_mirror_t(const DevWorld& w, const vm_frame& f, uint32_t nid, F3 hit, F3 rd,
                                              float t, Traffic* tr) {
   const F3 n = normal_of(nid);
@@ -97,7 +97,7 @@ __device__ __forceinline__ F3 water_mirror_t(const DevWorld& w, const vm_frame& 
     float shoal = 1.0f;
     if ((f.flags & VM_FLAG_WAVE_SHOAL) != 0u) {
       const F3 dro = {floorf(hit.x) + 0.5f, hit.y - VM_SURFACE_EPS, floorf(hit.z) + 0.5f};
-      const WorldHit dh = trace_world<true, COUNT>(w, f, dro, f3(0.001f, -0.999999f, 0.001f), SHOAL_DEPTH, tr);
+      const WorldHit dh = trace_world<true, COUNT, TUFTS>(w, f, dro, f3(0.001f, -0.999999f, 0.001f), SHOAL_DEPTH, tr);
       shoal = smoothstep(0.0f, SHOAL_DEPTH, dh.hit ? dh.t : SHOAL_DEPTH);
     }
     const F3 wf = wave_field(f, hit.x, hit.z, px_world, vhx, vhz, kk, aniso, shoal);

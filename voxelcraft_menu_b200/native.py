@@ -69,6 +69,7 @@ class VmwRecipe(C.Structure):
         ("size", c_u3), ("octaves", C.c_uint32), ("seed", C.c_uint32), ("base", C.c_float),
         ("amplitude", C.c_float), ("base_freq", C.c_float), ("water_level", C.c_int32), ("water_depth", C.c_int32),
         ("tree_permille", C.c_uint32), ("glass_permille", C.c_uint32), ("island_permille", C.c_uint32),
+        ("tuft_permille", C.c_uint32),
     ]
 
 

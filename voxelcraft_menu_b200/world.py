@@ -56,6 +56,7 @@ class Recipe:
     tree_permille: int = 10
     glass_permille: int = 0
     island_permille: int = 0
+    tuft_permille: int = 0
 
     def c(self) -> VmwRecipe:
         r = VmwRecipe()
@@ -63,6 +64,7 @@ class Recipe:
         r.octaves, r.seed, r.base, r.amplitude, r.base_freq = self.octaves, self.seed, self.base, self.amplitude, self.base_freq
         r.water_level, r.water_depth = self.water_level, self.water_depth
         r.tree_permille, r.glass_permille, r.island_permille = self.tree_permille, self.glass_permille, self.island_permille
+        r.tuft_permille = self.tuft_permille
         return r
 
 
