@@ -15,7 +15,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
 LIB = HERE / "liboracle.so"
-SRCS = [HERE / "vm_oracle.cpp", HERE / "producer.cpp"]
+SRCS = [HERE / "vm_oracle.cpp", HERE / "producer.cpp", HERE / "atlas.cpp"]
 DEPS = SRCS + [ROOT / "voxelcraft_menu_b200" / "csrc" / h for h in ("vm_types.h", "recipe.h")] + \
     [ROOT / "include" / "voxmarch_world.h"]
 

@@ -84,6 +84,7 @@ def lib():
             "or_reflect": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
             "or_water_sec": (C.c_int, [vp, vp, C.c_uint32, vp, vp, vp, vp, C.c_int]),
             "or_resolve": (C.c_int, [vp, vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
+            "or_build_atlas": (None, [C.c_float, C.c_int, vp]),
             "or_pick_rows": (C.c_uint64, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp]),
             "or_f16_round": (None, [vp, vp, C.c_uint64]),
         }
@@ -96,6 +97,14 @@ def lib():
 
 def _p(a):
     return C.c_void_p(a.ctypes.data)
+
+
+def engine_atlas(water_mottle: float = 0.0, tint_balance: bool = False) -> np.ndarray:
+    """The engine's block atlas (src/textures.rs build_atlas + downsample, as
+    make_atlas uploads it): uint8 sRGB RGBA, 27 layers, mips 16, 8, 4, 2."""
+    out = np.zeros(27 * 340 * 4, np.uint8)
+    lib().or_build_atlas(water_mottle, 1 if tint_balance else 0, _p(out))
+    return out
 
 
 class Oracle:

@@ -19,7 +19,7 @@ import math
 import numpy as np
 import pytest
 
-from oracle.oracle import Oracle
+from oracle.oracle import Oracle, engine_atlas
 from voxelcraft_menu_b200 import look as LK
 from voxelcraft_menu_b200 import world as W
 
@@ -69,6 +69,23 @@ def test_atlas_layout_and_mips():
     want = mip0[:, :, :, 3].reshape(LK.TEX_COUNT, 8, 2, 8, 2).astype(np.float64).mean(axis=(2, 4))
     assert np.abs(mip1[:, :, :, 3] - want).max() <= 0.5 + 1e-9
     assert not np.array_equal(LK.atlas(3), LK.atlas(4))
+
+
+def test_engine_atlas_layout():
+    """The oracle's restatement of the engine's atlas: tint masks on grass tops
+    and leaves, tuft layers fully transparent or opaque, mips in sequence."""
+    a = engine_atlas()
+    assert a.size == LK.TEX_COUNT * 340 * 4
+    mip0 = a[: LK.TEX_COUNT * 256 * 4].reshape(LK.TEX_COUNT, 16, 16, 4)
+    assert (mip0[2, :, :, 3] == 255).all() and (mip0[8, :, :, 3] == 255).all()
+    assert (mip0[0, :, :, 3] == 0).all() and (mip0[14, :, :, 3] == 0).all()
+    for layer in (19, 25, 26):
+        al = mip0[layer, :, :, 3]
+        assert set(np.unique(al)) <= {0, 255} and 0.3 < (al > 0).mean() < 0.8
+        assert (al[-1] > 0).any() and not (al[0] > 0).all()      # blades grow from the bottom row
+    mip3 = a[LK.TEX_COUNT * 336 * 4:].reshape(LK.TEX_COUNT, 2, 2, 4)
+    assert 0 < int(mip3[19, :, :, 3].mean()) < 255
+    assert not np.array_equal(engine_atlas(), engine_atlas(tint_balance=True))
 
 
 def test_block_faces_follow_the_engine_table():
@@ -208,7 +225,7 @@ def gpu_resolve(v, pools, look, spec_hi, soften=None, spec=None):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["default", "probes_shaft", "plain_flags", "legacy_lighting"])
+@pytest.mark.parametrize("case", ["default", "engine_atlas", "probes_shaft", "plain_flags", "legacy_lighting"])
 def test_resolve_matches_the_oracle(small, case):
     w, pools = small
     cam = look_camera()
@@ -223,7 +240,8 @@ def test_resolve_matches_the_oracle(small, case):
         spec_hi = 0
     elif case == "legacy_lighting":
         spec_hi = LK.HI_DEFAULT | LK.HI_LEGACY_LIGHTING
-    look = (LK.atlas(2), LK.block_faces(), probes, shaft)
+    atlas = engine_atlas() if case == "engine_atlas" else LK.atlas(2)
+    look = (atlas, LK.block_faces(), probes, shaft)
     vis, sh, _, got = gpu_resolve(v, pools, look, spec_hi)
     o = Oracle(v, *pools)
     want_vis = o.frame_vis()[0]

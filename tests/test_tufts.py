@@ -14,7 +14,7 @@ import math
 import numpy as np
 import pytest
 
-from oracle.oracle import SPEC_DEFAULT, Oracle
+from oracle.oracle import SPEC_DEFAULT, Oracle, engine_atlas
 from voxelcraft_menu_b200 import look as LK
 from voxelcraft_menu_b200 import world as W
 
@@ -92,11 +92,12 @@ def test_oracle_with_an_atlas_hits_cross_quads(tufted):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("spec", [SPEC_DEFAULT, SPEC_DEFAULT | SPEC_WIND_SWAY])
-def test_tufts_match_the_oracle(tufted, spec):
+@pytest.mark.parametrize("spec,source", [(SPEC_DEFAULT, "library"), (SPEC_DEFAULT, "engine"),
+                                         (SPEC_DEFAULT | SPEC_WIND_SWAY, "engine")])
+def test_tufts_match_the_oracle(tufted, spec, source):
     from voxelcraft_menu_b200.march import Marcher
     rec, w, pools, _, _ = tufted
-    atlas, faces = LK.atlas(1), LK.block_faces()
+    atlas, faces = (engine_atlas() if source == "engine" else LK.atlas(1)), LK.block_faces()
     v = w.view(low_camera(480, 270, flags=W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT))
     v.frame.time, v.frame.cloud_speed = 12.5, 3.0
     o = Oracle(v, *pools, spec=spec, atlas=atlas, faces=faces)

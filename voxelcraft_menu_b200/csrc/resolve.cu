@@ -212,19 +212,25 @@ __device__ __forceinline__ float sun_visibility(const float* mask, const float* 
   return floorf(clampf(m, 0.0f, 1.0f) * 255.0f + 0.5f) / 255.0f;
 }
 
+// SKY: the pass over the sky pixels (sky_color with clouds and the sun
+// shafts), else the pass over the opaque surfaces.  Two launches over the
+// frame instead of one with both paths: each kernel's code is half the size
+// (the single kernel stalled on instruction fetch) and a warp runs one path.
+template <bool SKY>
 __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_frame f, const __grid_constant__ DevWorld w,
-                                                 const __grid_constant__ Look L,
-                                                 const unsigned long long* __restrict__ vis,
-                                                 const float* __restrict__ mask, const float* __restrict__ dist,
-                                                 bool soft, float4* __restrict__ out) {
+                                                    const __grid_constant__ Look L,
+                                                    const unsigned long long* __restrict__ vis,
+                                                    const float* __restrict__ mask, const float* __restrict__ dist,
+                                                    bool soft, float4* __restrict__ out) {
   const uint32_t px = blockIdx.x * 32u + threadIdx.x, py = blockIdx.y * 4u + threadIdx.y;
   if (px >= f.res[0] || py >= f.res[1]) return;
   const uint64_t pix = (uint64_t)py * f.res[0] + px;
+  const unsigned long long key = vis[pix];
+  if ((key == 0ull) != SKY) return;
   const F3 cam = ld3(f.cam_pos);
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
-  const unsigned long long key = vis[pix];
   F3 color;
-  if (key == 0ull) {
+  if (SKY) {
     const float shaft = sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
     color = sky_color(f, L, cam, rd, 0.0f, shaft);
   } else {
@@ -252,7 +258,8 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, float4* out, cudaStream_t s) {
   const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
-  k_resolve<<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, out);
+  k_resolve<false><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, out);
+  k_resolve<true><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, out);
   return cudaGetLastError();
 }
 
