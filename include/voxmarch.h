@@ -161,14 +161,20 @@ int vm_read_reflection(vm_ctx* ctx, uint64_t* key, float* t);
 int vm_water_sec(vm_ctx* ctx, uint32_t shift);
 int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* refl_key, float* refl_t);
 
-/* The resolve of sky and opaque surfaces: lane 0 of the engine's resolve pass
- * (src/render/shaders/resolve.wgsl:1378-1466, RESOLVE_LANE 0), i.e.
- * shade_hit_legacy_cached (resolve.wgsl:1537-1788: atlas texel with texture
- * variation, biome tint, shore wetting, smooth light with AO from the light
- * bricks, the frame's sun visibility, distant terrain shadow, cloud shadow,
- * probe field, sky specular) plus the fog blend toward sky_base with the sun
- * shafts, and sky_color with clouds for sky pixels.  Water and glass pixels
- * are the engine's other lanes: their colour is left 0 with alpha 0.
+/* The resolve: the engine's resolve pass (src/render/shaders/resolve.wgsl:
+ * 1378-1466, its three lanes).  Opaque surfaces: shade_hit_legacy_cached
+ * (resolve.wgsl:1537-1788: atlas texel with texture variation, biome tint,
+ * shore wetting, smooth light with AO from the light bricks, the frame's sun
+ * visibility, distant terrain shadow, cloud shadow, probe field, sky
+ * specular).  Water: water_ctx and water_compose (resolve.wgsl:1078-1221:
+ * body colour, wave normals, foam, glint, the refract leg through the water
+ * medium and the reflect leg, each leg's hit shaded with a traced sun test),
+ * the legs from the half-resolution water_sec pass (FLAG_HI_WATER_SEC: a
+ * 2x2 block's nearest water pixel, through the engine's rgba16float targets;
+ * blocks that are not one flat water plane trace their own legs) or per
+ * pixel.  Glass: shade_glass (resolve.wgsl:1261-1319: transmission, the
+ * reflection, FLAG_HI_GLASS_REFLECT).  Then the fog blend toward sky_base
+ * with the sun shafts; sky pixels get sky_color with clouds.
  *
  * Material inputs, set once (the engine's own buffers):
  *   vm_upload_atlas        the block atlas as make_atlas uploads it
@@ -188,15 +194,17 @@ int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* 
  * vm_resolve(ctx, spec_hi): after vm_render (and vm_soften_shadows when the
  * engine's SPEC_SOFT_SHADOWS is on: its mask is then the sun visibility, as
  * the engine's primary_sun texture), spec_hi = the engine's FLAG_HI_* word
- * (src/render/mod.rs:196-300; SKY_SPECULAR, SHORE_WET, CAUSTICS,
- * TINT_BALANCE, SKY_LOOK, SKY_COOL, FOLIAGE_RICH, CANOPY_RELIEF,
- * LEGACY_LIGHTING are read; COMPACT_SHADE_HIT and the surface debug views
- * return VM_E_INVALID, as do underwater, heat-map, probe-tap and
- * probe-ambient frames).  The frame flags give the rest (AO, TINT,
- * TEX_VARIATION, DISTANT_SHADOWS, TERRAIN_SHAFTS, PROBE_CUBE / BOUNCE / SUN /
- * SUN_HIGH, LIGHT_RGB, SKY_TINT), as make_spec derives them.
- * vm_read_color: res.x * res.y RGBA float, the value the engine stores into
- * its rgba16float target. */
+ * (src/render/mod.rs:196-300; SKY_SPECULAR, SHORE_WET, SHORE_FOAM,
+ * WATER_SEC, CAUSTICS, GLASS_REFLECT, TINT_BALANCE, SKY_LOOK, SKY_COOL,
+ * FOLIAGE_RICH, CANOPY_RELIEF, LEGACY_LIGHTING are read; COMPACT_SHADE_HIT,
+ * WATER_LOOK and the surface debug views return VM_E_INVALID, as do
+ * underwater, heat-map, probe-tap and probe-ambient frames).  The frame
+ * flags give the rest (AO, TINT, TEX_VARIATION, DISTANT_SHADOWS,
+ * TERRAIN_SHAFTS, FLAT_SECONDARY, WAVES..., PROBE_CUBE / BOUNCE / SUN /
+ * SUN_HIGH, LIGHT_RGB, SKY_TINT, WATER_REFRACT / REFLECT), as make_spec
+ * derives them; WATER_SEC_SHIFT is 1 (the engine's water_sec_scale 2).
+ * vm_read_color: res.x * res.y RGBA float (alpha 1), the value the engine
+ * stores into its rgba16float target. */
 int vm_upload_atlas(vm_ctx* ctx, const uint8_t* rgba, uint32_t layers, uint32_t size, uint32_t mips);
 int vm_upload_block_faces(vm_ctx* ctx, const uint32_t* words, uint32_t n);
 int vm_upload_probes(vm_ctx* ctx, const uint16_t* rgba16f, uint32_t nx, uint32_t ny, uint32_t nz);

@@ -2295,9 +2295,48 @@ float face_shade(uint32_t nid) {
   }
 }
 
-// shade_hit_legacy_cached: resolve.wgsl:1537-1788 (smooth_light, do_spec)
+// shadow_ray: common.wgsl:1098-1148 (the boolean sun test of secondary hits)
+bool shadow_ray(const World& w, V3 ro, V3 rd, float max_dist) {
+  const vm_frame& f = *w.f;
+  V3 r_ro = ro;
+  float r_dist = max_dist;
+  if ((w.spec & VM_SPEC_WATER_REPAIR) != 0u && rd.y > 1e-4f && ro.y < f.sea_level) {
+    float t_surf = (f.sea_level - ro.y) / rd.y;
+    if (t_surf >= r_dist) return false;
+    r_ro = add(ro, muls(rd, t_surf));
+    r_dist = r_dist - t_surf;
+  }
+  V3 inv = v3(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
+  bool pos_dir[3] = {rd.x > 0.0f, rd.y > 0.0f, rd.z > 0.0f};
+  I3 cell = floor_i(divs(r_ro, 64.0f));
+  uint32_t last = VM_NO_CHUNK;
+  for (uint32_t i = 0; i < 24u; ++i) {
+    I3 rel = grid_rel(w, cell);
+    if (grid_outside(w, rel)) return false;
+    uint32_t ci = grid_at(w, grid_index(w, rel));
+    if (ci != VM_NO_CHUNK && ci != last) {
+      last = ci;
+      if (march_chunk(w, ci, r_ro, rd, r_dist, true, true, true, true).hit) return true;
+    }
+    V3 bounds = v3((float)(pos_dir[0] ? cell.x + 1 : cell.x) * 64.0f, (float)(pos_dir[1] ? cell.y + 1 : cell.y) * 64.0f,
+                   (float)(pos_dir[2] ? cell.z + 1 : cell.z) * 64.0f);
+    V3 tn = mul(sub(bounds, r_ro), inv);
+    uint32_t axis = 0u;
+    float t;
+    if (tn.x <= tn.y && tn.x <= tn.z) t = tn.x;
+    else if (tn.y <= tn.z) { t = tn.y; axis = 1u; }
+    else { t = tn.z; axis = 2u; }
+    if (t >= r_dist) return false;
+    setc(cell, axis, comp(cell, axis) + (pos_dir[axis] ? 1 : -1));
+  }
+  return false;
+}
+
+// shade_hit_legacy (resolve.wgsl:289-585) and shade_hit_legacy_cached
+// (resolve.wgsl:1537-1788): lit_frame >= 0 is the cached sun visibility,
+// lit_frame < 0 traces shadow_ray over shadow_dist
 V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint32_t nid, V3 hit, V3 rd, float dist,
-             float lit_frame) {
+             float shadow_dist, bool smooth_light, bool do_spec, float lit_frame) {
   const vm_frame& f = *w.f;
   const vm_chunk& c = chunk_at(w, ci);
   float vs = c.voxel_size;
@@ -2306,7 +2345,7 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
   if (foliage && dot(n, rd) > 0.0f) n = neg(n);
   V3 sun = ld3(f.sun_dir);
   V3 spec_pre = v3(0.0f, 0.0f, 0.0f);
-  if ((L.spec_hi & HI_SKY_SPECULAR) != 0u)
+  if ((L.spec_hi & HI_SKY_SPECULAR) != 0u && do_spec)
     spec_pre = muls(sky_base(f, L, reflect(rd, n), 1.0f), schlick_ground(clampf(dot(n, neg(rd)), 0.0f, 1.0f)));
   uint32_t axis = nid >> 1u;
   V3 box_min = add(ld3(c.origin), muls(v3((float)v.x, (float)v.y, (float)v.z), vs));
@@ -2366,6 +2405,21 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
     } else {
       float bk = light_curve(light_block_level(packed));
       amb = muls(mixv(sky_tint, BLOCK_TINT, bk / fmaxf(sk + bk, 1e-4f)), fmaxf(sk, bk));
+    }
+  } else if (!smooth_light) {
+    I3 air_v1{(int32_t)v.x + (int32_t)n.x, (int32_t)v.y + (int32_t)n.y, (int32_t)v.z + (int32_t)n.z};
+    uint32_t packed1;
+    if (air_v1.x >= 0 && air_v1.y >= 0 && air_v1.z >= 0 && air_v1.x <= 63 && air_v1.y <= 63 && air_v1.z <= 63)
+      packed1 = light_at(w, ci, air_v1);
+    else
+      packed1 = world_sample(w, add(add(box_min, v3(0.5f * vs, 0.5f * vs, 0.5f * vs)), muls(n, vs))).x;
+    float sk1 = light_curve(light_sky(packed1)) * f.daylight;
+    sky_sm = sk1;
+    if (light_rgb) {
+      amb = block_ambient(light_curve3(light_block_rgb(packed1)), sk1, sky_tint);
+    } else {
+      float bk1 = light_curve(light_block_level(packed1));
+      amb = muls(mixv(sky_tint, BLOCK_TINT, bk1 / fmaxf(sk1 + bk1, 1e-4f)), fmaxf(sk1, bk1));
     }
   } else {
     V3 air_c = add(add(box_min, v3(0.5f * vs, 0.5f * vs, 0.5f * vs)), muls(n, vs));
@@ -2434,9 +2488,9 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
   if (ndl > 0.0f && f.daylight > 0.01f) {
     float lit = 1.0f;
     if ((f.flags & VM_FLAG_SHADOWS) != 0u) {
-      lit = lit_frame;
+      lit = lit_frame >= 0.0f ? lit_frame : (shadow_ray(w, add(hit, muls(n, 0.02f * vs)), sun, shadow_dist) ? 0.0f : 1.0f);
       if ((f.flags & VM_FLAG_DISTANT_SHADOWS) != 0u && lit > 0.0f)
-        lit = lit * terrain_shade(f, L, add(hit, muls(sun, f.shadow_dist)));
+        lit = lit * terrain_shade(f, L, add(hit, muls(sun, shadow_dist)));
     }
     if (lit > 0.0f) {
       float cloud_fp = fmaxf(dist, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
@@ -2478,6 +2532,280 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
                        : muls(add(muls(add(ambient_rgb, sun_rgb), ao), floor_rgb), shade);
   if (repair(L) && id == VM_GLOWSTONE) return mul(albedo, add(muls(v3(1.0f, 0.7111f, 0.3024f), 1.5f), muls(light, 0.15f)));
   return add(mul(albedo, light), spec_rgb);
+}
+
+// ---- the water and glass lanes: resolve.wgsl:896-1320 ----------------------
+constexpr uint32_t HI_SHORE_FOAM = 16u, HI_WATER_SEC = 32u, HI_GLASS_REFLECT = 128u;
+
+inline bool secondary_smooth(const vm_frame& f) { return (f.flags & VM_FLAG_FLAT_SECONDARY) == 0u; }
+float medium_light(const vm_frame& f, uint32_t packed) {
+  float sky_l = light_curve(light_sky(packed)) * f.daylight;
+  float blk_l = light_curve(light_block_level(packed));
+  return fmaxf(sky_l, blk_l) * 0.50f + f.ambient;
+}
+V3 water_medium(const vm_frame& f, V3 c, float d, V3 body) {   // common.wgsl:1262-1265
+  float dd = fmaxf(d, 0.0f);
+  V3 tr = v3(expf(-0.280f * f.water_absorb * dd), expf(-0.055f * f.water_absorb * dd),
+             expf(-0.020f * f.water_absorb * dd));
+  return add(mul(c, tr), mul(body, v3(1.0f - tr.x, 1.0f - tr.y, 1.0f - tr.z)));
+}
+float schlick_f0(float f0, float cos_i) {   // common.wgsl:1267-1279
+  float m = clampf(1.0f - cos_i, 0.0f, 1.0f);
+  float m2 = m * m;
+  return f0 + (1.0f - f0) * m2 * m2 * m;
+}
+
+struct WaterCtx {
+  V3 body; float ml; V3 n, nw, nt; float gloss; bool waved; float refract_detail, reflect_detail;
+  V3 mirror, mirror_t, hit, rd; float t, roughness;
+};
+
+// water_ctx: resolve.wgsl:1078-1166 (SPEC_WATER_LOOK off)
+WaterCtx water_ctx(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t nid, V3 hit, V3 rd, float t) {
+  const vm_frame& f = *w.f;
+  WaterCtx x;
+  const vm_chunk& c = chunk_at(w, ci);
+  float vs = c.voxel_size;
+  V3 n = normal_of(nid);
+  V3 box_min = add(ld3(c.origin), muls(v3((float)v.x, (float)v.y, (float)v.z), vs));
+  V3 lq = divs(sub(hit, box_min), vs);
+  V3 local = v3(clampf(lq.x, 0.0f, 1.0f), clampf(lq.y, 0.0f, 1.0f), clampf(lq.z, 0.0f, 1.0f));
+  float footprint = fmaxf(t, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs;
+  float lod = clampf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f, 3.0f);
+  uint32_t fi = VM_WATER * 8u + nid;
+  uint32_t layer = (fi < L.n_faces ? L.faces[fi] : 0u) & 0xFFFFu;
+  float u, tv;
+  face_uv(nid, local, u, tv);
+  F4 tint = atlas_sample(L, u, tv, layer, lod);
+  if ((w.spec & VM_SPEC_WATER_REPAIR) != 0u) tint = atlas_sample(L, 0.5f, 0.5f, layer, 3.0f);
+  x.ml = medium_light(f, light_at(w, ci, I3{(int32_t)v.x, (int32_t)v.y, (int32_t)v.z}));
+  x.body = muls(v3(tint.r, tint.g, tint.b), x.ml);
+  x.refract_detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, t);
+  x.reflect_detail = 1.0f - smoothstep(VM_WATER_REFLECT_NEAR, VM_WATER_REFLECT_FAR, t);
+  float px_world = fmaxf(t, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1];
+  V3 nw = n, nt = n;
+  float gloss = 1.0f, unresolved = 0.0f;
+  bool waved = (f.flags & VM_FLAG_WAVES) != 0u && nid == VM_NORMAL_PY;
+  if (waved) {
+    float kk = 0.0f, vhx = 0.0f, vhz = 0.0f;
+    bool aniso = (f.flags & VM_FLAG_WAVE_ANISO) != 0u;
+    if (aniso) {
+      float k = 1.0f / fmaxf(fabsf(rd.y), WAVE_GRAZE_MIN);
+      kk = k * k - 1.0f;
+      float r = 1.0f / sqrtf(fmaxf(rd.x * rd.x + rd.z * rd.z, 1e-12f));
+      vhx = rd.x * r; vhz = rd.z * r;
+    }
+    float shoal = 1.0f;
+    if ((f.flags & VM_FLAG_WAVE_SHOAL) != 0u) {
+      V3 dro = v3(floorf(hit.x) + 0.5f, hit.y - VM_SURFACE_EPS, floorf(hit.z) + 0.5f);
+      WorldHit dh = trace_world(w, dro, v3(0.001f, -0.999999f, 0.001f), SHOAL_DEPTH, true);
+      shoal = smoothstep(0.0f, SHOAL_DEPTH, dh.hit ? dh.t : SHOAL_DEPTH);
+    }
+    V3 wf = wave_field(f, hit.x, hit.z, px_world, vhx, vhz, kk, aniso, shoal);
+    unresolved = fmaxf(wf.z, 0.0f);
+    nw = normalize(v3(-wf.x, 1.0f, -wf.y));
+    float gl = sqrtf(wf.x * wf.x + wf.y * wf.y);
+    float lim = fminf(1.0f, f.wave_reflect_slope / fmaxf(gl, 1e-6f));
+    nt = normalize(v3(-(wf.x * lim), 1.0f, -(wf.y * lim)));
+    gloss = 1.0f / (1.0f + 0.5f * 320.0f * wf.z);
+  }
+  float rough = clampf(1.0f - expf(-8.0f * unresolved), 0.0f, 1.0f);
+  nw = normalize(add(muls(nw, 1.0f - rough), muls(n, rough)));
+  nt = normalize(add(muls(nt, 1.0f - rough), muls(n, rough)));
+  x.n = n; x.nw = nw; x.nt = nt; x.gloss = gloss; x.waved = waved;
+  x.mirror = reflect(rd, nw);
+  V3 mt = reflect(rd, nt);
+  if (waved) mt = normalize(v3(mt.x, fmaxf(mt.y, 0.0f), mt.z));
+  x.mirror_t = mt;
+  x.hit = hit; x.rd = rd; x.t = t; x.roughness = rough;
+  return x;
+}
+
+V3 shade_leg(const World& w, const Look& L, const WorldHit& h, V3 p, V3 d, float dist, float shadow_dist) {
+  uint32_t id = block_at(w, h.ci, h.voxel);
+  return shade_hit(w, L, h.ci, h.voxel, id, h.normal, p, d, dist, shadow_dist, secondary_smooth(*w.f), false, -1.0f);
+}
+F4 water_refract_leg(const World& w, const Look& L, V3 hit, V3 n, V3 rd, float t) {   // resolve.wgsl:1029-1042
+  V3 rdir = refract(rd, n, 1.0f / VM_WATER_IOR);
+  V3 ro2 = add(hit, muls(rdir, VM_SURFACE_EPS));
+  WorldHit h2 = trace_world(w, ro2, rdir, VM_WATER_REFRACT_DIST, true);
+  V3 under = v3(0.0f, 0.0f, 0.0f);
+  float depth = VM_WATER_REFRACT_DIST;
+  if (h2.hit) {
+    under = shade_leg(w, L, h2, add(ro2, muls(rdir, h2.t)), rdir, t + h2.t, 16.0f);
+    depth = h2.t;
+  }
+  return {under.x, under.y, under.z, depth};
+}
+F4 water_reflect_leg(const World& w, const Look& L, V3 hit, V3 n, V3 mirror_t, float t) {   // resolve.wgsl:1044-1058
+  V3 ro3 = add(hit, muls(n, VM_SURFACE_EPS));
+  WorldHit h3 = trace_world(w, ro3, mirror_t, VM_WATER_REFLECT_DIST, true);
+  if (!h3.hit) return {0.0f, 0.0f, 0.0f, 0.0f};
+  V3 lit = shade_leg(w, L, h3, add(ro3, muls(mirror_t, h3.t)), mirror_t, t + h3.t, w.f->shadow_dist);
+  lit = mixv(lit, sky_base(*w.f, L, mirror_t, 1.0f), 1.0f - transmittance_from(*w.f, hit.y, h3.t, mirror_t));
+  return {lit.x, lit.y, lit.z, 1.0f};
+}
+
+// foam_hash / foam_mottle: resolve.wgsl:1011-1027
+float foam_hash(float ix, float iy) {
+  int32_t qx = f2i(ix), qy = f2i(iy);
+  return (float)((hash_u32((uint32_t)qx * 374761393u + (uint32_t)qy * 668265263u) >> 8u) & 0xFFFFFFu) / 16777216.0f;
+}
+float foam_mottle(float x, float z, float time) {
+  const float k = (float)(1.0 / 0.7);   // the abstract-float constant 1.0 / 0.7 as f32
+  float px = x * k, pz = z * k;
+  float ix = floorf(px), iz = floorf(pz);
+  float wx = px - ix, wz = pz - iz;
+  float ux = wx * wx * (3.0f - 2.0f * wx), uz = wz * wz * (3.0f - 2.0f * wz);
+  float m0 = mixs(foam_hash(ix, iz), foam_hash(ix + 1.0f, iz), ux);
+  float m1 = mixs(foam_hash(ix, iz + 1.0f), foam_hash(ix + 1.0f, iz + 1.0f), ux);
+  float m = mixs(m0, m1, uz);
+  float ph = time * 0.55f * 4.0f + foam_hash(ix * 2.23f, iz * 2.71f) * 6.28318f;
+  return m * (0.5f + 0.5f * sinf(ph));
+}
+
+// water_compose: resolve.wgsl:1169-1207
+V3 water_compose(const vm_frame& f, const Look& L, const WaterCtx& x, F4 leg_r, F4 leg_m) {
+  V3 refr = x.body;
+  float column_depth = VM_WATER_REFRACT_DIST;
+  if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && x.refract_detail > 0.0f) {
+    refr = mixv(refr, water_medium(f, v3(leg_r.r, leg_r.g, leg_r.b), leg_r.a, x.body), x.refract_detail);
+    column_depth = leg_r.a;
+  }
+  if ((L.spec_hi & HI_SHORE_FOAM) != 0u && x.refract_detail > 0.0f && column_depth < 2.5f) {
+    float shall = 1.0f - smoothstep(0.0f, 2.5f, column_depth);
+    float m = foam_mottle(x.hit.x, x.hit.z, f.time * f.wave_speed);
+    float foam = shall * smoothstep(0.45f, 0.75f, m) * x.refract_detail;
+    refr = mixv(refr, muls(v3(0.92f, 0.97f, 1.0f), x.ml), clampf(foam, 0.0f, 1.0f) * 0.85f);
+  }
+  V3 refl = add(sky_color(f, L, x.hit, x.mirror, x.t, 1.0f),
+                muls(v3(1.0000f, 0.8469f, 0.5647f),
+                     powf(fmaxf(dot(x.mirror, ld3(f.sun_dir)), 0.0f), 320.0f * x.gloss) * 2.5f * x.gloss * f.daylight));
+  if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f && leg_m.a > 0.0f)
+    refl = mixv(refl, v3(leg_m.r, leg_m.g, leg_m.b), x.reflect_detail);
+  refl = mixv(refl, sky_base(f, L, x.n, 1.0f), x.roughness * 0.65f);
+  return mixv(refr, refl, schlick_f0(0.02f, fmaxf(-dot(x.rd, x.nw), 1e-3f)));
+}
+
+V3 shade_water(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t nid, V3 hit, V3 rd, float t) {
+  const vm_frame& f = *w.f;
+  WaterCtx x = water_ctx(w, L, ci, v, nid, hit, rd, t);
+  F4 leg_r{0.0f, 0.0f, 0.0f, VM_WATER_REFRACT_DIST};
+  if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && x.refract_detail > 0.0f) leg_r = water_refract_leg(w, L, hit, x.n, rd, t);
+  F4 leg_m{0.0f, 0.0f, 0.0f, 0.0f};
+  if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f)
+    leg_m = water_reflect_leg(w, L, hit, x.n, x.mirror_t, t);
+  return water_compose(f, L, x, leg_r, leg_m);
+}
+
+// shade_glass: resolve.wgsl:1261-1319
+V3 shade_glass(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t nid, V3 hit, V3 rd, float t) {
+  const vm_frame& f = *w.f;
+  const vm_chunk& c = chunk_at(w, ci);
+  float vs = c.voxel_size;
+  V3 n = normal_of(nid);
+  if (dot(n, rd) > 0.0f) n = neg(n);
+  V3 box_min = add(ld3(c.origin), muls(v3((float)v.x, (float)v.y, (float)v.z), vs));
+  V3 lq = divs(sub(hit, box_min), vs);
+  V3 local = v3(clampf(lq.x, 0.0f, 1.0f), clampf(lq.y, 0.0f, 1.0f), clampf(lq.z, 0.0f, 1.0f));
+  float footprint = fmaxf(t, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs;
+  float lod = clampf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f, 3.0f);
+  uint32_t fi = VM_GLASS * 8u + nid;
+  uint32_t layer = (fi < L.n_faces ? L.faces[fi] : 0u) & 0xFFFFu;
+  float u, tv;
+  face_uv(nid, local, u, tv);
+  F4 tx = atlas_sample(L, u, tv, layer, lod);
+  V3 tint = v3(tx.r, tx.g, tx.b);
+  V3 ro2 = add(hit, muls(rd, VM_SURFACE_EPS));
+  float reach = fmaxf(VM_GLASS_TRANSMIT_DIST, f.far_);
+  WorldHit h2 = trace_world(w, ro2, rd, reach, false);
+  V3 through = sky_color(f, L, ro2, rd, t, 1.0f);
+  if (h2.hit) {
+    V3 p2 = add(ro2, muls(rd, h2.t));
+    if (block_at(w, h2.ci, h2.voxel) == VM_WATER)
+      through = shade_water(w, L, h2.ci, h2.voxel, h2.normal, p2, rd, t + h2.t);
+    else
+      through = shade_leg(w, L, h2, p2, rd, t + h2.t, 48.0f);
+    through = mixv(through, sky_base(f, L, rd, 1.0f), 1.0f - transmittance_from(f, hit.y, h2.t, rd));
+  }
+  V3 mirror = reflect(rd, n);
+  V3 refl = sky_color(f, L, hit, mirror, t, 1.0f);
+  if ((L.spec_hi & HI_GLASS_REFLECT) != 0u) {
+    V3 origin = add(hit, muls(n, VM_SURFACE_EPS));
+    WorldHit r = trace_world(w, origin, mirror, reach, false);
+    if (r.hit) {
+      V3 point = add(origin, muls(mirror, r.t));
+      if (block_at(w, r.ci, r.voxel) == VM_WATER)
+        refl = shade_water(w, L, r.ci, r.voxel, r.normal, point, mirror, t + r.t);
+      else
+        refl = shade_leg(w, L, r, point, mirror, t + r.t, 48.0f);
+      refl = mixv(refl, sky_base(f, L, mirror, 1.0f), 1.0f - transmittance_from(f, hit.y, r.t, mirror));
+    }
+  }
+  return mixv(mul(through, tint), refl, schlick_f0(0.0426f, fmaxf(-dot(rd, n), 1e-3f)));
+}
+
+// water_share_safe: resolve.wgsl:1223-1245
+bool water_share_safe(const World& w, const uint64_t* vis, uint32_t shift, uint32_t px, uint32_t py, uint32_t nid,
+                      V3 hit, float t) {
+  const vm_frame& f = *w.f;
+  if (nid != VM_NORMAL_PY) return false;
+  uint32_t span = 1u << shift;
+  uint32_t bx = (px >> shift) * span, by = (py >> shift) * span;
+  for (uint32_t y = 0; y < span; ++y)
+    for (uint32_t x = 0; x < span; ++x) {
+      uint32_t qx = bx + x, qy = by + y;
+      if (qx >= f.res[0] || qy >= f.res[1]) continue;
+      uint64_t key = vis[(uint64_t)qy * f.res[0] + qx];
+      if (key == 0) return false;
+      if (key_nid(key) != nid) return false;
+      uint32_t ci = key_ci(key);
+      U3 v = key_voxel(key), micro = key_micro(key);
+      if (block_at(w, ci, v) != VM_WATER) return false;
+      V3 rd = ray_dir(f, (float)qx + 0.5f, (float)qy + 0.5f);
+      float td = hit_t(w, ci, v, micro, nid, rd);
+      V3 hd = add(ld3(f.cam_pos), muls(rd, td));
+      if (fabsf(hd.y - hit.y) > 0.01f || fabsf(td - t) > fmaxf(0.1f, fminf(1.0f, t * 0.02f))) return false;
+    }
+  return true;
+}
+
+// the water_sec pass's colour (resolve.wgsl:1468-1535) of block (hx, hy):
+// the water pixel of least hit distance, its legs, through the rgba16float
+// targets' rounding
+void water_sec_legs(const World& w, const Look& L, const uint64_t* vis, uint32_t shift, uint32_t hx, uint32_t hy,
+                    F4* leg_r_out, F4* leg_m_out) {
+  const vm_frame& f = *w.f;
+  uint32_t span = 1u << shift;
+  F4 leg_r{0.0f, 0.0f, 0.0f, VM_WATER_REFRACT_DIST}, leg_m{0.0f, 0.0f, 0.0f, 0.0f};
+  float best_t = 3.4e38f;
+  bool has = false;
+  uint32_t bci = 0, bnid = 0, bpx = 0, bpy = 0;
+  U3 bv{0, 0, 0};
+  for (uint32_t i = 0; i < span; ++i)
+    for (uint32_t j = 0; j < span; ++j) {
+      uint32_t pxs = span * hx + i, pys = span * hy + j;
+      if (pxs >= f.res[0] || pys >= f.res[1]) continue;
+      uint64_t key = vis[(uint64_t)pys * f.res[0] + pxs];
+      if (key == 0) continue;
+      uint32_t nids = key_nid(key), cis = key_ci(key);
+      U3 vs_ = key_voxel(key), micros = key_micro(key);
+      if (block_at(w, cis, vs_) != VM_WATER) continue;
+      V3 rd0 = ray_dir(f, (float)pxs + 0.5f, (float)pys + 0.5f);
+      float ts = hit_t(w, cis, vs_, micros, nids, rd0);
+      if (ts < best_t) { best_t = ts; bci = cis; bv = vs_; bnid = nids; bpx = pxs; bpy = pys; has = true; }
+    }
+  if (has) {
+    V3 rd_d = ray_dir(f, (float)bpx + 0.5f, (float)bpy + 0.5f);
+    V3 hit_d = add(ld3(f.cam_pos), muls(rd_d, best_t));
+    WaterCtx x = water_ctx(w, L, bci, bv, bnid, hit_d, rd_d, best_t);
+    if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && x.refract_detail > 0.0f)
+      leg_r = water_refract_leg(w, L, hit_d, x.n, rd_d, best_t);
+    if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f)
+      leg_m = water_reflect_leg(w, L, hit_d, x.n, x.mirror_t, best_t);
+  }
+  *leg_r_out = {f16_round(leg_r.r), f16_round(leg_r.g), f16_round(leg_r.b), f16_round(leg_r.a)};
+  *leg_m_out = {f16_round(leg_m.r), f16_round(leg_m.g), f16_round(leg_m.b), f16_round(leg_m.a)};
 }
 
 float srgb_to_linear(uint8_t u) {
@@ -2542,11 +2870,23 @@ int or_resolve(const or_world* o, const or_look* lk, const uint64_t* vis, const 
       float t = hit_t(w, ci, v, micro, nid, rd);
       V3 hit = add(cam, muls(rd, t));
       uint32_t id = block_at(w, ci, v);
-      if (id == VM_WATER || glass_leg(w, id)) {
-        out[0] = out[1] = out[2] = out[3] = 0.0f;
-        continue;
+      if (id == VM_WATER) {
+        // shade_water_sec (resolve.wgsl:1247-1259), or shade_water without SPEC_WATER_SEC
+        bool shared = (lk->spec_hi & HI_WATER_SEC) != 0u &&
+                      !((w.spec & VM_SPEC_WATER_REPAIR) != 0u && !water_share_safe(w, vis, 1u, px, py, nid, hit, t));
+        if (shared) {
+          WaterCtx x = water_ctx(w, L, ci, v, nid, hit, rd, t);
+          F4 leg_r, leg_m;
+          water_sec_legs(w, L, vis, 1u, px >> 1, py >> 1, &leg_r, &leg_m);
+          color = water_compose(f, L, x, leg_r, leg_m);
+        } else {
+          color = shade_water(w, L, ci, v, nid, hit, rd, t);
+        }
+      } else if (glass_leg(w, id)) {
+        color = shade_glass(w, L, ci, v, nid, hit, rd, t);
+      } else {
+        color = shade_hit(w, L, ci, v, id, nid, hit, rd, t, f.shadow_dist, true, true, sun_vis[pix]);
       }
-      color = shade_hit(w, L, ci, v, id, nid, hit, rd, t, sun_vis[pix]);
       float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
       float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
       color = mixv(color, sky_base(f, L, rd, shaft), alpha);

@@ -1,13 +1,15 @@
-"""The resolve of sky and opaque surfaces (lane 0 of resolve.wgsl:1378-1466:
-shade_hit_legacy_cached, the fog blend with sun shafts, sky_color with
+"""The resolve (resolve.wgsl:1378-1466, its three lanes: sky and opaque
+surfaces with shade_hit_legacy_cached, water with water_ctx / water_compose
+and the half-resolution water_sec legs or per-pixel legs, glass with its
+transmission and reflection; the fog blend with sun shafts, sky_color with
 clouds) against the oracle's restatement.
 
 The kernel and the oracle share the float contract but not the
 transcendental functions (CUDA's expf / powf / log2f / logf / exp2f against
 the host's), so colours are compared within a tolerance: 2e-4 absolute plus
 1e-3 relative at 99.9% of the pixels, and 0.05 absolute at every pixel (a
-last-bit difference can move a texture-level or a smoothstep edge).  Water
-and glass pixels (the engine's other lanes) must be alpha 0 on both sides.
+last-bit difference can move a texture-level or a smoothstep edge, or a
+water_sec leg across a binary16 rounding step).
 
 CPU: the material builders (atlas format and mips, the engine's face table),
 the sun-visibility rounding and oracle properties.  GPU: frames of the small
@@ -125,12 +127,17 @@ def test_oracle_resolve_properties(small):
     sky = vis == 0
     assert sky.any() and (~sky).any()
     assert (c[sky, 3] == 1.0).all()
-    # water and glass pixels belong to the other lanes
+    # water and glass pixels: their lanes' colour (water_compose, shade_glass)
     ids = np.array([o.block_at(int(k >> 24) & 0x1FFF, [(int(k) >> 16) & 63, (int(k) >> 8) & 63, int(k) & 63])
                     if k else 0 for k in vis])
     lane = (~sky) & ((ids == 13) | (ids == 10))
-    assert lane.any()
-    assert (c[lane] == 0.0).all() and (c[~lane, 3] == 1.0).all()
+    assert lane.any() and (c[:, 3] == 1.0).all()
+    assert (c[lane, :3] > 0.0).all() and (c[ids == 13, 2] > c[ids == 13, 0]).mean() > 0.9   # water is blue
+    # the half-resolution legs and per-pixel legs agree where a block is flat water
+    own = o.resolve(vis, sv, atlas, faces, spec_hi=LK.HI_DEFAULT & ~LK.HI_WATER_SEC)
+    water = ids == 13
+    assert np.abs(own[water, :3] - c[water, :3]).mean() < 0.02
+    assert np.array_equal(own[~water], c[~water])
     # a part of the range equals the same pixels of the whole frame
     part = o.resolve(vis, sv, atlas, faces, spec_hi=LK.HI_DEFAULT, pix=(3000, 5000))
     assert np.array_equal(part, c[3000:5000])
@@ -225,7 +232,8 @@ def gpu_resolve(v, pools, look, spec_hi, soften=None, spec=None):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["default", "engine_atlas", "probes_shaft", "plain_flags", "legacy_lighting"])
+@pytest.mark.parametrize("case", ["default", "engine_atlas", "probes_shaft", "plain_flags", "legacy_lighting",
+                                  "reflect_legs", "per_pixel_legs"])
 def test_resolve_matches_the_oracle(small, case):
     w, pools = small
     cam = look_camera()
@@ -240,6 +248,13 @@ def test_resolve_matches_the_oracle(small, case):
         spec_hi = 0
     elif case == "legacy_lighting":
         spec_hi = LK.HI_DEFAULT | LK.HI_LEGACY_LIGHTING
+    elif case == "reflect_legs":
+        v.frame.flags |= W.FLAG_WATER_REFLECT | W.FLAG_WAVES
+        spec_hi = LK.HI_DEFAULT | LK.HI_GLASS_REFLECT
+    elif case == "per_pixel_legs":
+        v.frame.flags |= W.FLAG_WATER_REFLECT
+        v.frame.flags &= ~LK.FLAG_FLAT_SECONDARY
+        spec_hi = LK.HI_DEFAULT & ~LK.HI_WATER_SEC
     atlas = engine_atlas() if case == "engine_atlas" else LK.atlas(2)
     look = (atlas, LK.block_faces(), probes, shaft)
     vis, sh, _, got = gpu_resolve(v, pools, look, spec_hi)

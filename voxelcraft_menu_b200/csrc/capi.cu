@@ -45,7 +45,7 @@ struct vm_ctx {
   DevBuf shadow_mask;   // vm_soften_shadows output, sized on first use
   bool mask_valid = false;   // the mask belongs to the last rendered frame
   // the resolve's material inputs and output (vm_upload_atlas ... vm_resolve)
-  DevBuf atlas, faces, probes, shaft, grad, color;
+  DevBuf atlas, faces, probes, shaft, grad, color, leg_refr, leg_refl;
   uint32_t atlas_layers = 0, n_faces = 0;
   DevBuf atlas_alpha;          // the atlas's alpha channel for the tuft quads of the march
   uint32_t tuft_layer[3] = {0, 0, 0};
@@ -336,7 +336,7 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->b_super_count, &ctx->shadow_mask, &ctx->refl_key, &ctx->refl_t,
                    &ctx->shadow16, &ctx->ws_refr_key, &ctx->ws_refr_t, &ctx->ws_refl_key, &ctx->ws_refl_t,
                    &ctx->atlas, &ctx->faces, &ctx->probes, &ctx->shaft, &ctx->grad, &ctx->color,
-                   &ctx->atlas_alpha};
+                   &ctx->atlas_alpha, &ctx->leg_refr, &ctx->leg_refl};
   for (DevBuf* b : all) release(*b);
   if (ctx->rendered) cudaEventDestroy(ctx->rendered);
   if (ctx->own) cudaStreamDestroy(ctx->own);
@@ -990,7 +990,10 @@ float srgb_decode(uint8_t u) {
   return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f);
 }
 
-constexpr uint32_t HI_UNBUILT = 131072u /* COMPACT_SHADE_HIT */ | 8388608u | 16777216u | 33554432u /* DEBUG */;
+constexpr uint32_t HI_UNBUILT = 131072u /* COMPACT_SHADE_HIT */ | 8388608u | 16777216u | 33554432u /* DEBUG */ |
+                               4096u /* WATER_LOOK */;
+constexpr uint32_t HI_WATER_SEC = 32u;
+constexpr uint32_t WATER_SEC_SHIFT = 1u;   // WATER_SEC_SHIFT of the engine's default water_sec_scale 2
 
 }  // namespace
 
@@ -1091,8 +1094,8 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
   if (f.flags & (VM_FLAG_UNDERWATER | VM_FLAG_HEATMAP | VM_FLAG_PROBE_TAP | VM_FLAG_PROBE_AMBIENT))
     return fail(ctx, VM_E_INVALID, "resolve of underwater, heat-map, probe-tap or probe-ambient frames is not built");
   if (spec_hi & HI_UNBUILT)
-    return fail(ctx, VM_E_INVALID, "spec_hi 0x%x: compact shade_hit and surface debug views are not built",
-                spec_hi & HI_UNBUILT);
+    return fail(ctx, VM_E_INVALID, "spec_hi 0x%x: compact shade_hit, the water look and surface debug views "
+                "are not built", spec_hi & HI_UNBUILT);
   CK(cudaSetDevice(ctx->device));
   if ((rc = ensure(ctx, ctx->color, npix * 16))) return rc;
   vmd::Look L;
@@ -1103,9 +1106,17 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
   L.grad = (const float2*)ctx->grad.p;
   L.spec_hi = spec_hi;
   const float* mask = ctx->mask_valid ? (const float*)ctx->shadow_mask.p : nullptr;
+  uint16_t *refr = nullptr, *refl = nullptr;
+  if (spec_hi & HI_WATER_SEC) {
+    const uint32_t span = 1u << WATER_SEC_SHIFT;
+    const size_t cells = (size_t)((f.res[0] + span - 1) >> WATER_SEC_SHIFT) * ((f.res[1] + span - 1) >> WATER_SEC_SHIFT);
+    if ((rc = ensure(ctx, ctx->leg_refr, cells * 8)) || (rc = ensure(ctx, ctx->leg_refl, cells * 8))) return rc;
+    refr = (uint16_t*)ctx->leg_refr.p;
+    refl = (uint16_t*)ctx->leg_refl.p;
+  }
   CK(vmk::launch_resolve(f, dev_world(ctx), L, (const unsigned long long*)ctx->vis.p, mask,
-                         (const float*)ctx->shadow.p, (ctx->spec & VM_SPEC_SOFT_RAYS) != 0u, (float4*)ctx->color.p,
-                         ctx->stream));
+                         (const float*)ctx->shadow.p, (ctx->spec & VM_SPEC_SOFT_RAYS) != 0u, WATER_SEC_SHIFT, refr,
+                         refl, (float4*)ctx->color.p, ctx->stream));
   ctx->color_done = true;
   return VM_OK;
 }

@@ -126,12 +126,14 @@ cudaError_t launch_to_r16f(const float* in, uint16_t* out, uint64_t n, int sms, 
 constexpr uint32_t SOFTEN_MAX_LIMIT = 8;
 cudaError_t launch_soften(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis, const float* dist,
                           float* mask, uint32_t limit, float penumbra, cudaStream_t s);
-// lane 0 of the resolve (resolve.wgsl:1378-1466): RGBA colour of every sky
-// and opaque pixel (alpha 1), 0 for water and glass pixels.  mask: the soft
-// shadow mask of this frame, or null (visibility from the blocker distances,
-// or from the blocked fractions when soft rays traced them).
+// the resolve (resolve.wgsl:1378-1466, all three lanes): RGBA colour of every
+// pixel.  mask: the soft shadow mask of this frame, or null (visibility from
+// the blocker distances, or from the blocked fractions when soft rays traced
+// them).  leg_refr / leg_refl: the water_sec targets (4 halves per
+// (2^shift)^2 block; null: every water pixel traces its own legs).
 cudaError_t launch_resolve(const vm_frame& f, const vmd::DevWorld& w, const vmd::Look& L, const unsigned long long* vis,
-                           const float* mask, const float* dist, bool soft_rays, float4* out, cudaStream_t s);
+                           const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
+                           uint16_t* leg_refr, uint16_t* leg_refl, float4* out, cudaStream_t s);
 cudaError_t launch_expand(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                           int32_t wx, int32_t wy, int32_t wz, uint32_t dx, uint32_t dy, uint32_t dz,
                           uint32_t* voxel, uint8_t* face, float* t, cudaStream_t s);

@@ -772,6 +772,47 @@ __device__ __noinline__ float shadow_ray_t(const DevWorld& w, const vm_frame& f,
   return -1.0f;
 }
 
+// shadow_ray: common.wgsl:1098-1148, the boolean sun test of shade_hit for
+// secondary hits: from below the sea level a rising ray (SPEC_WATER_REPAIR)
+// starts at the flat sea surface, the rest is shadow_ray_t's walk.
+static __device__ __noinline__ bool shadow_ray_hit(const DevWorld& w, const vm_frame& f, F3 ro, F3 rd, float max_dist) {
+  F3 r_ro = ro;
+  float r_dist = max_dist;
+  if ((w.spec & VM_SPEC_WATER_REPAIR) != 0u && rd.y > 1e-4f && ro.y < f.sea_level) {
+    const float t_surf = (f.sea_level - ro.y) / rd.y;
+    if (t_surf >= r_dist) return false;
+    r_ro = ro + rd * t_surf;
+    r_dist = r_dist - t_surf;
+  }
+  const Ray r = make_ray(r_ro, rd);
+  int32_t cx = ffloor_i(r_ro.x * INV64), cy = ffloor_i(r_ro.y * INV64), cz = ffloor_i(r_ro.z * INV64);
+  uint32_t last = VM_NO_CHUNK;
+  for (uint32_t i = 0; i < 24u; ++i) {
+    uint64_t gi;
+    if (!grid_rel(f, cx, cy, cz, &gi)) return false;
+    const uint32_t ci = ld_grid(w, gi);
+    if (ci != VM_NO_CHUNK && ci != last) {
+      last = ci;
+      const Chunk c = ld_chunk(w, ci);
+      if (march_chunk<true, true, true, false>(w, f, c, r, r_dist, nullptr).hit) return true;
+    }
+    const float bx = (float)(r.pdx ? cx + 1 : cx) * 64.0f;
+    const float by = (float)(r.pdy ? cy + 1 : cy) * 64.0f;
+    const float bz = (float)(r.pdz ? cz + 1 : cz) * 64.0f;
+    const float tnx = (bx - r_ro.x) * r.inv.x, tny = (by - r_ro.y) * r.inv.y, tnz = (bz - r_ro.z) * r.inv.z;
+    float t;
+    uint32_t axis = 0u;
+    if (tnx <= tny && tnx <= tnz) t = tnx;
+    else if (tny <= tnz) { t = tny; axis = 1u; }
+    else { t = tnz; axis = 2u; }
+    if (t >= r_dist) return false;
+    if (axis == 0) cx += r.pdx ? 1 : -1;
+    else if (axis == 1) cy += r.pdy ? 1 : -1;
+    else cz += r.pdz ? 1 : -1;
+  }
+  return false;
+}
+
 // shadow_ray_t one chunk-grid cell at a time, for kernels whose lanes take a
 // new ray as soon as theirs ends: the state between cells is the cell, the
 // last chunk marched and the step count, and each step is the loop body of

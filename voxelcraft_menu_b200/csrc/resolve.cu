@@ -7,11 +7,13 @@
 // (transcendentals, the 9-sample light gather, the noise octaves).
 #include "resolve.cuh"
 #include "kernels.cuh"
+#include "ray_stages.cuh"
 
 namespace vmd {
 
-__device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx, uint32_t vy,
-                            uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist, float lit_in) {
+__device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx,
+                                         uint32_t vy, uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist,
+                                         float shadow_dist, bool smooth, bool do_spec, float lit_in) {
   const Chunk c = ld_chunk(w, ci);
   const float vs = c.vs;
   const bool foliage = nid >= VM_NORMAL_CROSS_A;
@@ -19,7 +21,7 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
   if (foliage && dot(n, rd) > 0.0f) n = neg(n);
   const F3 sun = ld3(f.sun_dir);
   F3 spec_pre = {0.0f, 0.0f, 0.0f};
-  if ((L.spec_hi & HI_SKY_SPECULAR) != 0u)
+  if ((L.spec_hi & HI_SKY_SPECULAR) != 0u && do_spec)
     spec_pre = sky_base(f, L, reflect(rd, n), 1.0f) * schlick_ground(clampf(dot(n, neg(rd)), 0.0f, 1.0f));
   const uint32_t axis = nid >> 1u;
   const F3 box_min = ld3(c.origin) + f3((float)vx, (float)vy, (float)vz) * vs;
@@ -80,6 +82,23 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
     } else {
       const float bk = light_curve(light_block_level(packed));
       amb = mix3(sky_tint, block_tint(), bk / fmaxf(sk + bk, 1e-4f)) * fmaxf(sk, bk);
+    }
+  } else if (!smooth) {
+    // one light sample: the voxel in front of the face, in this chunk or
+    // through the grid
+    const int32_t ax = (int32_t)vx + nx, ay = (int32_t)vy + ny, az = (int32_t)vz + nz;
+    uint32_t packed1;
+    if (ax >= 0 && ay >= 0 && az >= 0 && ax <= 63 && ay <= 63 && az <= 63)
+      packed1 = light_at(w, c, ax, ay, az);
+    else
+      packed1 = world_sample(w, f, box_min + f3(0.5f * vs, 0.5f * vs, 0.5f * vs) + n * vs).x;
+    const float sk1 = light_curve(light_sky(packed1)) * f.daylight;
+    sky_sm = sk1;
+    if (light_rgb) {
+      amb = block_ambient(light_curve3(light_block_rgb(packed1)), sk1, sky_tint);
+    } else {
+      const float bk1 = light_curve(light_block_level(packed1));
+      amb = mix3(sky_tint, block_tint(), bk1 / fmaxf(sk1 + bk1, 1e-4f)) * fmaxf(sk1, bk1);
     }
   } else {
     const F3 air_c = box_min + f3(0.5f * vs, 0.5f * vs, 0.5f * vs) + n * vs;
@@ -151,9 +170,9 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
   if (ndl > 0.0f && f.daylight > 0.01f) {
     float lit = 1.0f;
     if ((f.flags & VM_FLAG_SHADOWS) != 0u) {
-      lit = lit_in;
+      lit = lit_in >= 0.0f ? lit_in : (shadow_ray_hit(w, f, hit + n * (0.02f * vs), sun, shadow_dist) ? 0.0f : 1.0f);
       if ((f.flags & VM_FLAG_DISTANT_SHADOWS) != 0u && lit > 0.0f)
-        lit = lit * terrain_shade(f, L, hit + sun * f.shadow_dist);
+        lit = lit * terrain_shade(f, L, hit + sun * shadow_dist);
     }
     if (lit > 0.0f) {
       const float cloud_fp = fmaxf(dist, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
@@ -199,6 +218,248 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
   return albedo * light + spec_rgb;
 }
 
+
+// ---------------------------------------------------------------------------
+// the water and glass lanes: resolve.wgsl:896-1320
+
+constexpr uint32_t HI_SHORE_FOAM = 16u, HI_WATER_SEC = 32u, HI_GLASS_REFLECT = 128u;
+constexpr float WATER_SHADOW_DIST = 16.0f;    // SPEC_WATER_SHADOW_DIST
+constexpr float GLASS_SHADOW_DIST = 48.0f;
+
+__device__ __forceinline__ bool secondary_smooth(const vm_frame& f) { return (f.flags & VM_FLAG_FLAT_SECONDARY) == 0u; }
+
+__device__ __forceinline__ float medium_light(const vm_frame& f, uint32_t packed) {
+  const float sky_l = light_curve(light_sky(packed)) * f.daylight;
+  const float blk_l = light_curve(light_block_level(packed));
+  return fmaxf(sky_l, blk_l) * 0.50f + f.ambient;
+}
+
+// water_medium: common.wgsl:1262-1265 (WATER_EXT per channel)
+__device__ __forceinline__ F3 water_medium(const vm_frame& f, F3 c, float d, F3 body) {
+  const float dd = fmaxf(d, 0.0f);
+  const F3 tr = {expf(-0.280f * f.water_absorb * dd), expf(-0.055f * f.water_absorb * dd),
+                 expf(-0.020f * f.water_absorb * dd)};
+  return c * tr + body * f3(1.0f - tr.x, 1.0f - tr.y, 1.0f - tr.z);
+}
+__device__ __forceinline__ float schlick_f0(float f0, float cos_i) {   // schlick / schlick_glass
+  const float m = clampf(1.0f - cos_i, 0.0f, 1.0f);
+  const float m2 = m * m;
+  return f0 + (1.0f - f0) * m2 * m2 * m;
+}
+
+struct WaterCtx {
+  F3 body; float ml;
+  F3 n, nw, nt;
+  float gloss; bool waved;
+  float refract_detail, reflect_detail;
+  F3 mirror, mirror_t, hit, rd;
+  float t, roughness;
+};
+
+// water_ctx: resolve.wgsl:1078-1166 (SPEC_WATER_LOOK off)
+static __device__ __noinline__ WaterCtx water_ctx(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci,
+                                                  uint32_t vx, uint32_t vy, uint32_t vz, uint32_t nid, F3 hit, F3 rd,
+                                                  float t) {
+  WaterCtx x;
+  const Chunk c = ld_chunk(w, ci);
+  const float vs = c.vs;
+  const F3 n = normal_of(nid);
+  const F3 box_min = ld3(c.origin) + f3((float)vx, (float)vy, (float)vz) * vs;
+  const F3 lq = (hit - box_min) / vs;
+  const F3 local = {clampf(lq.x, 0.0f, 1.0f), clampf(lq.y, 0.0f, 1.0f), clampf(lq.z, 0.0f, 1.0f)};
+  const float footprint = fmaxf(t, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs;
+  const float lod = clampf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f, 3.0f);
+  const uint32_t fi = VM_WATER * 8u + nid;
+  const uint32_t layer = (fi < L.n_faces ? __ldg(L.faces + fi) : 0u) & 0xFFFFu;
+  float u, v;
+  face_uv(nid, local, &u, &v);
+  float4 tint = atlas_sample(L, u, v, layer, lod);
+  if ((w.spec & VM_SPEC_WATER_REPAIR) != 0u) tint = atlas_sample(L, 0.5f, 0.5f, layer, 3.0f);
+  x.ml = medium_light(f, light_at(w, c, (int32_t)vx, (int32_t)vy, (int32_t)vz));
+  x.body = f3(tint.x, tint.y, tint.z) * x.ml;
+  x.refract_detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, t);
+  x.reflect_detail = 1.0f - smoothstep(VM_WATER_REFLECT_NEAR, VM_WATER_REFLECT_FAR, t);
+  const float px_world = fmaxf(t, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1];
+  F3 nw = n, nt = n;
+  float gloss = 1.0f, unresolved = 0.0f;
+  const bool waved = (f.flags & VM_FLAG_WAVES) != 0u && nid == VM_NORMAL_PY;
+  if (waved) {
+    float kk = 0.0f, vhx = 0.0f, vhz = 0.0f;
+    const bool aniso = (f.flags & VM_FLAG_WAVE_ANISO) != 0u;
+    if (aniso) {
+      const float k = 1.0f / fmaxf(fabsf(rd.y), WAVE_GRAZE_MIN);
+      kk = k * k - 1.0f;
+      const float r = 1.0f / sqrtf(fmaxf(rd.x * rd.x + rd.z * rd.z, 1e-12f));
+      vhx = rd.x * r; vhz = rd.z * r;
+    }
+    float shoal = 1.0f;
+    if ((f.flags & VM_FLAG_WAVE_SHOAL) != 0u) {
+      const F3 dro = {floorf(hit.x) + 0.5f, hit.y - VM_SURFACE_EPS, floorf(hit.z) + 0.5f};
+      const WorldHit dh = trace_world<true, false, true>(w, f, dro, f3(0.001f, -0.999999f, 0.001f), SHOAL_DEPTH,
+                                                          nullptr);
+      shoal = smoothstep(0.0f, SHOAL_DEPTH, dh.hit ? dh.t : SHOAL_DEPTH);
+    }
+    const F3 wf = wave_field(f, hit.x, hit.z, px_world, vhx, vhz, kk, aniso, shoal);
+    unresolved = fmaxf(wf.z, 0.0f);
+    nw = unit(f3(-wf.x, 1.0f, -wf.y));
+    const float gl = sqrtf(wf.x * wf.x + wf.y * wf.y);
+    const float lim = fminf(1.0f, f.wave_reflect_slope / fmaxf(gl, 1e-6f));
+    nt = unit(f3(-(wf.x * lim), 1.0f, -(wf.y * lim)));
+    gloss = 1.0f / (1.0f + 0.5f * 320.0f * wf.z);
+  }
+  const float rough = clampf(1.0f - expf(-8.0f * unresolved), 0.0f, 1.0f);
+  nw = unit(nw * (1.0f - rough) + n * rough);
+  nt = unit(nt * (1.0f - rough) + n * rough);
+  x.n = n; x.nw = nw; x.nt = nt; x.gloss = gloss; x.waved = waved;
+  x.mirror = reflect(rd, nw);
+  F3 mt = reflect(rd, nt);
+  if (waved) mt = unit(f3(mt.x, fmaxf(mt.y, 0.0f), mt.z));
+  x.mirror_t = mt;
+  x.hit = hit; x.rd = rd; x.t = t; x.roughness = rough;
+  return x;
+}
+
+// the colour of a leg's hit (shade_hit with a traced sun test)
+static __device__ __noinline__ F3 shade_leg(const DevWorld& w, const vm_frame& f, const Look& L, const WorldHit& h,
+                                            F3 p, F3 d, float dist, float shadow_dist) {
+  const Chunk c = ld_chunk(w, h.ci);
+  const uint32_t id = block_at(w, c, h.vx, h.vy, h.vz);
+  return shade_surface(w, f, L, h.ci, h.vx, h.vy, h.vz, id, h.normal, p, d, dist, shadow_dist, secondary_smooth(f),
+                       false, -1.0f);
+}
+
+// water_refract_leg / water_reflect_leg: resolve.wgsl:1029-1058, as
+// (rgb, depth) and (rgb, 1 when hit)
+static __device__ __noinline__ float4 water_refract_leg(const DevWorld& w, const vm_frame& f, const Look& L, F3 hit,
+                                                        F3 n, F3 rd, float t) {
+  const F3 rdir = refract(rd, n, 1.0f / VM_WATER_IOR);
+  const F3 ro2 = hit + rdir * VM_SURFACE_EPS;
+  const WorldHit h2 = trace_world<true, false, true>(w, f, ro2, rdir, VM_WATER_REFRACT_DIST, nullptr);
+  F3 under = {0.0f, 0.0f, 0.0f};
+  float depth = VM_WATER_REFRACT_DIST;
+  if (h2.hit) {
+    under = shade_leg(w, f, L, h2, ro2 + rdir * h2.t, rdir, t + h2.t, WATER_SHADOW_DIST);
+    depth = h2.t;
+  }
+  return make_float4(under.x, under.y, under.z, depth);
+}
+static __device__ __noinline__ float4 water_reflect_leg(const DevWorld& w, const vm_frame& f, const Look& L, F3 hit,
+                                                        F3 n, F3 mirror_t, float t) {
+  const F3 ro3 = hit + n * VM_SURFACE_EPS;
+  const WorldHit h3 = trace_world<true, false, true>(w, f, ro3, mirror_t, VM_WATER_REFLECT_DIST, nullptr);
+  if (!h3.hit) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  F3 lit = shade_leg(w, f, L, h3, ro3 + mirror_t * h3.t, mirror_t, t + h3.t, f.shadow_dist);
+  lit = mix3(lit, sky_base(f, L, mirror_t, 1.0f), 1.0f - transmittance_from(f, hit.y, h3.t, mirror_t));
+  return make_float4(lit.x, lit.y, lit.z, 1.0f);
+}
+
+// foam_hash / foam_mottle: resolve.wgsl:1011-1027
+__device__ __forceinline__ float foam_hash(float ix, float iy) {
+  const int32_t qx = __float2int_rz(ix), qy = __float2int_rz(iy);
+  return (float)((hash_u32((uint32_t)qx * 374761393u + (uint32_t)qy * 668265263u) >> 8u) & 0xFFFFFFu) / 16777216.0f;
+}
+static __device__ __noinline__ float foam_mottle(float x, float z, float time) {
+  const float k = (float)(1.0 / 0.7);     // the WGSL constant 1.0 / 0.7, folded before the f32 conversion
+  const float px = x * k, pz = z * k;
+  const float ix = floorf(px), iz = floorf(pz);
+  const float wx = px - ix, wz = pz - iz;
+  const float ux = wx * wx * (3.0f - 2.0f * wx), uz = wz * wz * (3.0f - 2.0f * wz);
+  const float m0 = mixf(foam_hash(ix, iz), foam_hash(ix + 1.0f, iz), ux);
+  const float m1 = mixf(foam_hash(ix, iz + 1.0f), foam_hash(ix + 1.0f, iz + 1.0f), ux);
+  const float m = mixf(m0, m1, uz);
+  const float ph = time * 0.55f * 4.0f + foam_hash(ix * 2.23f, iz * 2.71f) * 6.28318f;
+  return m * (0.5f + 0.5f * sinf(ph));
+}
+
+// water_compose: resolve.wgsl:1169-1207 (SPEC_WATER_LOOK off)
+static __device__ __noinline__ F3 water_compose(const vm_frame& f, const Look& L, const WaterCtx& x, float4 leg_r,
+                                                float4 leg_m) {
+  F3 refr = x.body;
+  float column_depth = VM_WATER_REFRACT_DIST;
+  if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && x.refract_detail > 0.0f) {
+    refr = mix3(refr, water_medium(f, f3(leg_r.x, leg_r.y, leg_r.z), leg_r.w, x.body), x.refract_detail);
+    column_depth = leg_r.w;
+  }
+  if ((L.spec_hi & HI_SHORE_FOAM) != 0u && x.refract_detail > 0.0f && column_depth < 2.5f) {
+    const float shall = 1.0f - smoothstep(0.0f, 2.5f, column_depth);
+    const float m = foam_mottle(x.hit.x, x.hit.z, f.time * f.wave_speed);
+    const float foam = shall * smoothstep(0.45f, 0.75f, m) * x.refract_detail;
+    refr = mix3(refr, f3(0.92f, 0.97f, 1.0f) * x.ml, clampf(foam, 0.0f, 1.0f) * 0.85f);
+  }
+  const F3 sun = ld3(f.sun_dir);
+  F3 refl = sky_color(f, L, x.hit, x.mirror, x.t, 1.0f) +
+            f3(1.0000f, 0.8469f, 0.5647f) *
+                (powf(fmaxf(dot(x.mirror, sun), 0.0f), 320.0f * x.gloss) * 2.5f * x.gloss * f.daylight);
+  if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f && leg_m.w > 0.0f)
+    refl = mix3(refl, f3(leg_m.x, leg_m.y, leg_m.z), x.reflect_detail);
+  refl = mix3(refl, sky_base(f, L, x.n, 1.0f), x.roughness * 0.65f);
+  return mix3(refr, refl, schlick_f0(0.02f, fmaxf(-dot(x.rd, x.nw), 1e-3f)));
+}
+
+// shade_water: resolve.wgsl:1209-1221
+static __device__ __noinline__ F3 shade_water(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci,
+                                              uint32_t vx, uint32_t vy, uint32_t vz, uint32_t nid, F3 hit, F3 rd,
+                                              float t) {
+  const WaterCtx x = water_ctx(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
+  float4 leg_r = make_float4(0.0f, 0.0f, 0.0f, VM_WATER_REFRACT_DIST);
+  if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && x.refract_detail > 0.0f)
+    leg_r = water_refract_leg(w, f, L, hit, x.n, rd, t);
+  float4 leg_m = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f)
+    leg_m = water_reflect_leg(w, f, L, hit, x.n, x.mirror_t, t);
+  return water_compose(f, L, x, leg_r, leg_m);
+}
+
+// shade_glass: resolve.wgsl:1261-1319
+static __device__ __noinline__ F3 shade_glass(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci,
+                                              uint32_t vx, uint32_t vy, uint32_t vz, uint32_t nid, F3 hit, F3 rd,
+                                              float t) {
+  const Chunk c = ld_chunk(w, ci);
+  const float vs = c.vs;
+  F3 n = normal_of(nid);
+  if (dot(n, rd) > 0.0f) n = neg(n);
+  const F3 box_min = ld3(c.origin) + f3((float)vx, (float)vy, (float)vz) * vs;
+  const F3 lq = (hit - box_min) / vs;
+  const F3 local = {clampf(lq.x, 0.0f, 1.0f), clampf(lq.y, 0.0f, 1.0f), clampf(lq.z, 0.0f, 1.0f)};
+  const float footprint = fmaxf(t, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs;
+  const float lod = clampf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f, 3.0f);
+  const uint32_t fi = VM_GLASS * 8u + nid;
+  const uint32_t layer = (fi < L.n_faces ? __ldg(L.faces + fi) : 0u) & 0xFFFFu;
+  float u, v;
+  face_uv(nid, local, &u, &v);
+  const float4 tx = atlas_sample(L, u, v, layer, lod);
+  const F3 tint = {tx.x, tx.y, tx.z};
+  const F3 ro2 = hit + rd * VM_SURFACE_EPS;
+  const float reach = fmaxf(VM_GLASS_TRANSMIT_DIST, f.far_);
+  const WorldHit h2 = trace_world<false, false, true>(w, f, ro2, rd, reach, nullptr);
+  F3 through = sky_color(f, L, ro2, rd, t, 1.0f);
+  if (h2.hit) {
+    const F3 p2 = ro2 + rd * h2.t;
+    const Chunk c2 = ld_chunk(w, h2.ci);
+    if (block_at(w, c2, h2.vx, h2.vy, h2.vz) == VM_WATER)
+      through = shade_water(w, f, L, h2.ci, h2.vx, h2.vy, h2.vz, h2.normal, p2, rd, t + h2.t);
+    else
+      through = shade_leg(w, f, L, h2, p2, rd, t + h2.t, GLASS_SHADOW_DIST);
+    through = mix3(through, sky_base(f, L, rd, 1.0f), 1.0f - transmittance_from(f, hit.y, h2.t, rd));
+  }
+  const F3 mirror = reflect(rd, n);
+  F3 refl = sky_color(f, L, hit, mirror, t, 1.0f);
+  if ((L.spec_hi & HI_GLASS_REFLECT) != 0u) {
+    const F3 origin = hit + n * VM_SURFACE_EPS;
+    const WorldHit r = trace_world<false, false, true>(w, f, origin, mirror, reach, nullptr);
+    if (r.hit) {
+      const F3 point = origin + mirror * r.t;
+      const Chunk c3 = ld_chunk(w, r.ci);
+      if (block_at(w, c3, r.vx, r.vy, r.vz) == VM_WATER)
+        refl = shade_water(w, f, L, r.ci, r.vx, r.vy, r.vz, r.normal, point, mirror, t + r.t);
+      else
+        refl = shade_leg(w, f, L, r, point, mirror, t + r.t, GLASS_SHADOW_DIST);
+      refl = mix3(refl, sky_base(f, L, mirror, 1.0f), 1.0f - transmittance_from(f, hit.y, r.t, mirror));
+    }
+  }
+  return mix3(through * tint, refl, schlick_f0(0.0426f, fmaxf(-dot(rd, n), 1e-3f)));
+}
+
 }  // namespace vmd
 
 namespace vmk {
@@ -212,25 +473,106 @@ __device__ __forceinline__ float sun_visibility(const float* mask, const float* 
   return floorf(clampf(m, 0.0f, 1.0f) * 255.0f + 0.5f) / 255.0f;
 }
 
-// SKY: the pass over the sky pixels (sky_color with clouds and the sun
-// shafts), else the pass over the opaque surfaces.  Two launches over the
-// frame instead of one with both paths: each kernel's code is half the size
-// (the single kernel stalled on instruction fetch) and a warp runs one path.
-template <bool SKY>
+// The engine's rgba16float water_sec targets: binary16, round to nearest even.
+__device__ __forceinline__ ushort4 to_half4(float4 v) {
+  return make_ushort4(__half_as_ushort(__float2half_rn(v.x)), __half_as_ushort(__float2half_rn(v.y)),
+                      __half_as_ushort(__float2half_rn(v.z)), __half_as_ushort(__float2half_rn(v.w)));
+}
+__device__ __forceinline__ float4 from_half4(ushort4 h) {
+  return make_float4(__half2float(__ushort_as_half(h.x)), __half2float(__ushort_as_half(h.y)),
+                     __half2float(__ushort_as_half(h.z)), __half2float(__ushort_as_half(h.w)));
+}
+
+// The colour pass of water_sec (resolve.wgsl:1468-1535): per (2^shift)^2
+// block the water pixel of least hit distance (first in x-major order on
+// ties), its water_ctx and both legs shaded, stored as the engine's
+// rgba16float targets (refract: colour and depth; reflect: colour, 1 if hit).
+__global__ void __launch_bounds__(128) k_water_legs(const __grid_constant__ vm_frame f, const __grid_constant__ DevWorld w,
+                                                    const __grid_constant__ Look L,
+                                                    const unsigned long long* __restrict__ vis, uint32_t shift,
+                                                    ushort4* __restrict__ refr, ushort4* __restrict__ refl) {
+  const uint32_t span = 1u << shift;
+  const uint32_t hw = (f.res[0] + span - 1u) >> shift, hh = (f.res[1] + span - 1u) >> shift;
+  const uint32_t hx = blockIdx.x * 16u + threadIdx.x, hy = blockIdx.y * 8u + threadIdx.y;
+  if (hx >= hw || hy >= hh) return;
+  float4 leg_r = make_float4(0.0f, 0.0f, 0.0f, VM_WATER_REFRACT_DIST), leg_m = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float best_t = 3.4e38f;
+  bool has = false;
+  KeyParts best = {};
+  uint32_t bpx = 0, bpy = 0;
+  for (uint32_t i = 0; i < span; ++i)
+    for (uint32_t j = 0; j < span; ++j) {
+      const uint32_t pxs = span * hx + i, pys = span * hy + j;
+      if (pxs >= f.res[0] || pys >= f.res[1]) continue;
+      const unsigned long long key = vis[(uint64_t)pys * f.res[0] + pxs];
+      if (key == 0ull) continue;
+      const KeyParts k = split_key(key);
+      const Chunk c = ld_chunk(w, k.ci);
+      if (block_at(w, c, k.vx, k.vy, k.vz) != VM_WATER) continue;
+      const F3 rd0 = ray_dir(f, (float)pxs + 0.5f, (float)pys + 0.5f);
+      const float ts = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd0);
+      if (ts < best_t) { best_t = ts; best = k; bpx = pxs; bpy = pys; has = true; }
+    }
+  if (has) {
+    const F3 rd = ray_dir(f, (float)bpx + 0.5f, (float)bpy + 0.5f);
+    const F3 hit = ld3(f.cam_pos) + rd * best_t;
+    const WaterCtx x = water_ctx(w, f, L, best.ci, best.vx, best.vy, best.vz, best.nid, hit, rd, best_t);
+    if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && x.refract_detail > 0.0f)
+      leg_r = water_refract_leg(w, f, L, hit, x.n, rd, best_t);
+    if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f)
+      leg_m = water_reflect_leg(w, f, L, hit, x.n, x.mirror_t, best_t);
+  }
+  const uint64_t h = (uint64_t)hy * hw + hx;
+  refr[h] = to_half4(leg_r);
+  refl[h] = to_half4(leg_m);
+}
+
+// water_share_safe: resolve.wgsl:1223-1245: the block's pixels all hit flat
+// water on the same +Y plane, close in distance
+__device__ __noinline__ bool water_share_safe(const vm_frame& f, const DevWorld& w, const unsigned long long* vis,
+                                              uint32_t shift, uint32_t px, uint32_t py, uint32_t nid, F3 hit, float t) {
+  if (nid != VM_NORMAL_PY) return false;
+  const uint32_t span = 1u << shift;
+  const uint32_t bx = (px >> shift) * span, by = (py >> shift) * span;
+  for (uint32_t y = 0; y < span; ++y)
+    for (uint32_t x = 0; x < span; ++x) {
+      const uint32_t qx = bx + x, qy = by + y;
+      if (qx >= f.res[0] || qy >= f.res[1]) continue;
+      const unsigned long long key = vis[(uint64_t)qy * f.res[0] + qx];
+      if (key == 0ull) return false;
+      const KeyParts k = split_key(key);
+      if (k.nid != nid) return false;
+      const Chunk c = ld_chunk(w, k.ci);
+      if (block_at(w, c, k.vx, k.vy, k.vz) != VM_WATER) return false;
+      const F3 rd = ray_dir(f, (float)qx + 0.5f, (float)qy + 0.5f);
+      const float td = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+      const F3 hd = ld3(f.cam_pos) + rd * td;
+      if (fabsf(hd.y - hit.y) > 0.01f || fabsf(td - t) > fmaxf(0.1f, fminf(1.0f, t * 0.02f))) return false;
+    }
+  return true;
+}
+
+struct WaterSec { const ushort4* refr; const ushort4* refl; uint32_t shift, hw; };
+
+// PART 0: the opaque surfaces, 1: the sky, 2: water and glass.  Three
+// launches over the frame instead of one kernel with every path: each
+// kernel carries a third of the code (one kernel stalled on instruction
+// fetch) and its warps run one path.
+template <int PART>
 __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_frame f, const __grid_constant__ DevWorld w,
                                                     const __grid_constant__ Look L,
                                                     const unsigned long long* __restrict__ vis,
                                                     const float* __restrict__ mask, const float* __restrict__ dist,
-                                                    bool soft, float4* __restrict__ out) {
+                                                    bool soft, WaterSec ws, float4* __restrict__ out) {
   const uint32_t px = blockIdx.x * 32u + threadIdx.x, py = blockIdx.y * 4u + threadIdx.y;
   if (px >= f.res[0] || py >= f.res[1]) return;
   const uint64_t pix = (uint64_t)py * f.res[0] + px;
   const unsigned long long key = vis[pix];
-  if ((key == 0ull) != SKY) return;
+  if ((key == 0ull) != (PART == 1)) return;
   const F3 cam = ld3(f.cam_pos);
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   F3 color;
-  if (SKY) {
+  if (PART == 1) {
     const float shaft = sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
     color = sky_color(f, L, cam, rd, 0.0f, shaft);
   } else {
@@ -243,11 +585,24 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
     const float t = hit_t(f, c, vx, vy, vz, mx, my, mz, nid, rd);
     const F3 hit = cam + rd * t;
     const uint32_t id = block_at(w, c, vx, vy, vz);
-    if (id == VM_WATER || ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS)) {
-      out[pix] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);   // the water and glass lanes' pixels
-      return;
+    const bool lane2 = id == VM_WATER || ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS);
+    if (lane2 != (PART == 2)) return;
+    if (PART == 0) {
+      color = shade_surface(w, f, L, ci, vx, vy, vz, id, nid, hit, rd, t, f.shadow_dist, true, true,
+                            sun_visibility(mask, dist, soft, pix));
+    } else if (id == VM_WATER) {
+      if (ws.refr != nullptr &&
+          !((w.spec & VM_SPEC_WATER_REPAIR) != 0u && !water_share_safe(f, w, vis, ws.shift, px, py, nid, hit, t))) {
+        // shade_water_sec (resolve.wgsl:1247-1259): the block's legs
+        const WaterCtx x = water_ctx(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
+        const uint64_t h = (uint64_t)(py >> ws.shift) * ws.hw + (px >> ws.shift);
+        color = water_compose(f, L, x, from_half4(ws.refr[h]), from_half4(ws.refl[h]));
+      } else {
+        color = shade_water(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
+      }
+    } else {
+      color = shade_glass(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
     }
-    color = shade_surface(w, f, L, ci, vx, vy, vz, id, nid, hit, rd, t, sun_visibility(mask, dist, soft, pix));
     const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
     const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
     color = mix3(color, sky_base(f, L, rd, shaft), alpha);
@@ -256,10 +611,20 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
 }
 
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
-                           const float* mask, const float* dist, bool soft_rays, float4* out, cudaStream_t s) {
+                           const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
+                           uint16_t* leg_refr, uint16_t* leg_refl, float4* out, cudaStream_t s) {
+  WaterSec ws{nullptr, nullptr, water_sec_shift, 0u};
+  if (leg_refr != nullptr) {
+    const uint32_t span = 1u << water_sec_shift;
+    const uint32_t hw = (f.res[0] + span - 1u) >> water_sec_shift, hh = (f.res[1] + span - 1u) >> water_sec_shift;
+    k_water_legs<<<dim3((hw + 15) / 16, (hh + 7) / 8), dim3(16, 8), 0, s>>>(
+        f, w, L, vis, water_sec_shift, (ushort4*)leg_refr, (ushort4*)leg_refl);
+    ws = {(const ushort4*)leg_refr, (const ushort4*)leg_refl, water_sec_shift, hw};
+  }
   const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
-  k_resolve<false><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, out);
-  k_resolve<true><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, out);
+  k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
+  k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
+  k_resolve<2><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
   return cudaGetLastError();
 }
 

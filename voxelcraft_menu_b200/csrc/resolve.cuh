@@ -628,9 +628,13 @@ __device__ __forceinline__ float face_shade(uint32_t nid) {
 }
 
 // ---------------------------------------------------------------------------
-// shade_hit_legacy_cached: resolve.wgsl:1537-1788 (smooth_light and do_spec
-// on, the sun visibility read from the frame's shadow mask)
-__device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx, uint32_t vy,
-                            uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist, float lit_in);
+// shade_hit_legacy (resolve.wgsl:289-585) and its cached form
+// (resolve.wgsl:1537-1788): lit_in >= 0 is the frame's sun visibility of a
+// primary hit (the cached form), lit_in < 0 traces shadow_ray from the hit
+// over shadow_dist (the secondary legs).  smooth: the 3x3 smooth light with
+// AO, else the single light sample of the voxel in front of the face.
+__device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx,
+                                         uint32_t vy, uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist,
+                                         float shadow_dist, bool smooth, bool do_spec, float lit_in);
 
 }  // namespace vmd

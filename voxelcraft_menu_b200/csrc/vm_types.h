@@ -181,6 +181,7 @@ static_assert(sizeof(vm_tree_l1) == 24, "vm_tree_l1 layout");
 #define VM_FLAG_TINT 128u
 #define VM_FLAG_FOLIAGE 256u
 #define VM_FLAG_TERRAIN_SHAFTS 8192u
+#define VM_FLAG_FLAT_SECONDARY 1048576u
 #define VM_FLAG_TEX_VARIATION 16384u
 #define VM_FLAG_DISTANT_SHADOWS 32768u
 #define VM_FLAG_PROBE_TAP 16777216u

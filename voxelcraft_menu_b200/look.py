@@ -27,6 +27,7 @@ FLAG_FOLIAGE = 256
 FLAG_TERRAIN_SHAFTS = 8192
 FLAG_TEX_VARIATION = 16384
 FLAG_DISTANT_SHADOWS = 32768
+FLAG_FLAT_SECONDARY = 1048576
 FLAG_PROBE_TAP = 16777216
 FLAG_PROBE_AMBIENT = 33554432
 FLAG_PROBE_CUBE = 67108864
@@ -37,15 +38,20 @@ FLAG_PROBE_SUN_HIGH = 1073741824
 FLAG_SKY_TINT = 2147483648
 # the engine's default configuration's resolve flags (src/scene.rs:422-520 with
 # src/config.rs:276-380: AO, tint + biomes, terrain shafts, texture variation,
-# distant shadows, probe cube / bounce / sun, RGB light, sky tint)
+# distant shadows, flat secondary light, probe cube / bounce / sun, RGB light,
+# sky tint)
 LOOK_FLAGS = (FLAG_AO | FLAG_TINT | FLAG_TERRAIN_SHAFTS | FLAG_TEX_VARIATION | FLAG_DISTANT_SHADOWS |
-              FLAG_PROBE_CUBE | FLAG_PROBE_BOUNCE | FLAG_LIGHT_RGB | FLAG_PROBE_SUN | FLAG_SKY_TINT)
+              FLAG_FLAT_SECONDARY | FLAG_PROBE_CUBE | FLAG_PROBE_BOUNCE | FLAG_LIGHT_RGB | FLAG_PROBE_SUN |
+              FLAG_SKY_TINT)
 
 # spec_hi bits (FLAG_HI_*, src/render/mod.rs:196-300) the resolve reads
-HI_SKY_SPECULAR, HI_SHORE_WET, HI_CAUSTICS, HI_TINT_BALANCE = 1, 8, 64, 512
+HI_SKY_SPECULAR, HI_SHORE_WET, HI_SHORE_FOAM, HI_WATER_SEC, HI_CAUSTICS = 1, 8, 16, 32, 64
+HI_GLASS_REFLECT, HI_TINT_BALANCE, HI_WATER_LOOK = 128, 512, 4096
 HI_SKY_LOOK, HI_SKY_COOL, HI_FOLIAGE_RICH, HI_CANOPY_RELIEF = 1024, 2048, 8192, 16384
 HI_COMPACT_SHADE_HIT, HI_LEGACY_LIGHTING = 131072, 1048576
-HI_DEFAULT = HI_SKY_SPECULAR | HI_SHORE_WET     # src/scene.rs:341-411 with the default configuration
+# src/scene.rs:341-411 with the default configuration and a sea: sky specular,
+# shore wetting and foam, the half-resolution water legs
+HI_DEFAULT = HI_SKY_SPECULAR | HI_SHORE_WET | HI_SHORE_FOAM | HI_WATER_SEC
 
 
 def atlas(seed: int = 1) -> np.ndarray:
