@@ -108,6 +108,55 @@ def test_static_scratch_tile_lists_longer_than_its_capacity():
         assert np.array_equal(got_sh, sh), f"call {call}: shadow differs from the oracle"
 
 
+def test_static_scratch_replays_from_a_cuda_graph():
+    """The entry point's reason to exist: recorded into a stream capture the
+    caller owns (here a torch CUDA graph) and replayed, it writes the same
+    frame as the context path."""
+    import torch
+    w = W.World.generate(W.recipe_small_terrain())
+    inners, leaves, bricks = w.pools()
+    v = w.view(W.small_terrain_camera(width=320, height=180))
+    m = Marcher(320, 180)
+    m.upload_world(inners, leaves, bricks)
+    m.upload_view(v)
+    m.render()
+    want_vis, want_sh = m.read_vis(), m.read_shadow()
+    m.close()
+    L = native.lib()
+    d_ch, d_grid = _dev(v.chunks, torch), _dev(v.grid.astype(np.uint32), torch)
+    d_in, d_le, d_br = _dev(inners, torch), _dev(leaves, torch), _dev(bricks, torch)
+    npix = v.n_pixels
+    d_vis = torch.full((npix,), -1, dtype=torch.int64, device="cuda")
+    d_sh = torch.full((npix,), -1.0, dtype=torch.float32, device="cuda")
+    d_err = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def call(stream):
+        return L.vm_render_static(C.byref(v.frame), C.c_void_p(d_ch.data_ptr()), len(v.chunks),
+                                  C.c_void_p(d_grid.data_ptr()), v.grid.size, C.c_void_p(d_in.data_ptr()),
+                                  inners.shape[0], C.c_void_p(d_le.data_ptr()), leaves.shape[0],
+                                  C.c_void_p(d_br.data_ptr()), bricks.size, C.c_void_p(d_vis.data_ptr()),
+                                  C.c_void_p(d_sh.data_ptr()), C.c_void_p(d_err.data_ptr()), C.c_void_p(stream))
+
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        assert call(side.cuda_stream) == 0, L.vm_static_last_error().decode()   # warm-up outside the capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, capture_error_mode="thread_local"):
+        rc = call(torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, L.vm_static_last_error().decode()
+    d_vis.fill_(-1)
+    d_sh.fill_(-1.0)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(d_vis.cpu().numpy().view(np.uint64), want_vis)
+        assert np.array_equal(d_sh.cpu().numpy(), want_sh)
+        assert int(d_err.item()) == 0
+    del g
+
+
 def test_static_scratch_rejects_oversized_frames():
     import torch
     w = W.World.generate(W.recipe_small_terrain())

@@ -554,9 +554,9 @@ __device__ __noinline__ bool water_share_safe(const vm_frame& f, const DevWorld&
 
 struct WaterSec { const ushort4* refr; const ushort4* refl; uint32_t shift, hw; };
 
-// PART 0: the opaque surfaces, 1: the sky, 2: water and glass.  Three
+// PART 0: the opaque surfaces, 1: the sky, 2: water, 3: glass.  Four
 // launches over the frame instead of one kernel with every path: each
-// kernel carries a third of the code (one kernel stalled on instruction
+// kernel carries a part of the code (one kernel stalled on instruction
 // fetch) and its warps run one path.
 template <int PART>
 __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_frame f, const __grid_constant__ DevWorld w,
@@ -585,12 +585,12 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
     const float t = hit_t(f, c, vx, vy, vz, mx, my, mz, nid, rd);
     const F3 hit = cam + rd * t;
     const uint32_t id = block_at(w, c, vx, vy, vz);
-    const bool lane2 = id == VM_WATER || ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS);
-    if (lane2 != (PART == 2)) return;
+    const int part = id == VM_WATER ? 2 : ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS ? 3 : 0);
+    if (part != PART) return;
     if (PART == 0) {
       color = shade_surface(w, f, L, ci, vx, vy, vz, id, nid, hit, rd, t, f.shadow_dist, true, true,
                             sun_visibility(mask, dist, soft, pix));
-    } else if (id == VM_WATER) {
+    } else if (PART == 2) {
       if (ws.refr != nullptr &&
           !((w.spec & VM_SPEC_WATER_REPAIR) != 0u && !water_share_safe(f, w, vis, ws.shift, px, py, nid, hit, t))) {
         // shade_water_sec (resolve.wgsl:1247-1259): the block's legs
@@ -625,6 +625,7 @@ cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, 
   k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
   k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
   k_resolve<2><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
+  k_resolve<3><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
   return cudaGetLastError();
 }
 
