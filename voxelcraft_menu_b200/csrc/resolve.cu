@@ -554,6 +554,75 @@ __device__ __noinline__ bool water_share_safe(const vm_frame& f, const DevWorld&
 
 struct WaterSec { const ushort4* refr; const ushort4* refl; uint32_t shift, hw; };
 
+// The water pixels (lane 2 with SPEC_WATER_SEC and WATER_SEC_SHIFT 1).
+// water_share_safe compares a pixel with the three others of its 2x2 block;
+// the block lies in one 32x4 thread block, so each thread decodes its own
+// pixel once (hit distance, hit height, normal, water or not) into shared
+// memory and the comparisons read it there: the same values the per-pixel
+// test recomputes, with a quarter of the chunk and tree loads.
+__global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant__ vm_frame f,
+                                                          const __grid_constant__ DevWorld w,
+                                                          const __grid_constant__ Look L,
+                                                          const unsigned long long* __restrict__ vis, WaterSec ws,
+                                                          float4* __restrict__ out) {
+  __shared__ float s_hy[4][32], s_t[4][32];
+  __shared__ uint8_t s_code[4][32];   // bit 0 in the frame, 1 a key, 2 water, bits 3-5 the normal
+  const uint32_t tx = threadIdx.x, ty = threadIdx.y;
+  const uint32_t px = blockIdx.x * 32u + tx, py = blockIdx.y * 4u + ty;
+  const bool inside = px < f.res[0] && py < f.res[1];
+  const F3 cam = ld3(f.cam_pos);
+  F3 rd = {0.0f, 0.0f, 1.0f}, hit = {0.0f, 0.0f, 0.0f};
+  float t = 0.0f;
+  uint32_t code = 0u, ci = 0u, vx = 0u, vy = 0u, vz = 0u, nid = 0u;
+  if (inside) {
+    code = 1u;
+    const unsigned long long key = vis[(uint64_t)py * f.res[0] + px];
+    if (key != 0ull) {
+      rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+      nid = (uint32_t)(key >> 37) & 7u;
+      ci = (uint32_t)(key >> 24) & 0x1FFFu;
+      const uint32_t low = (uint32_t)(key & 0xFFFFFFull);
+      vx = (low >> 16) & 63u; vy = (low >> 8) & 63u; vz = low & 63u;
+      const uint32_t mx = (low >> 22) & 3u, my = (low >> 14) & 3u, mz = (low >> 6) & 3u;
+      const Chunk c = ld_chunk(w, ci);
+      t = hit_t(f, c, vx, vy, vz, mx, my, mz, nid, rd);
+      hit = cam + rd * t;
+      code |= 2u | (nid << 3);
+      if (block_at(w, c, vx, vy, vz) == VM_WATER) code |= 4u;
+    }
+  }
+  s_hy[ty][tx] = hit.y;
+  s_t[ty][tx] = t;
+  s_code[ty][tx] = (uint8_t)code;
+  __syncthreads();
+  if ((code & 4u) == 0u) return;
+  // water_share_safe: resolve.wgsl:1223-1245
+  bool safe = nid == VM_NORMAL_PY;
+  const uint32_t bx = tx & ~1u, by = ty & ~1u;
+  for (uint32_t y = 0; y < 2u && safe; ++y)
+    for (uint32_t x = 0; x < 2u && safe; ++x) {
+      const uint32_t q = s_code[by + y][bx + x];
+      if ((q & 1u) == 0u) continue;
+      if ((q & 2u) == 0u || ((q >> 3) & 7u) != nid || (q & 4u) == 0u) { safe = false; break; }
+      if (fabsf(s_hy[by + y][bx + x] - hit.y) > 0.01f ||
+          fabsf(s_t[by + y][bx + x] - t) > fmaxf(0.1f, fminf(1.0f, t * 0.02f)))
+        safe = false;
+    }
+  F3 color;
+  if (safe || (w.spec & VM_SPEC_WATER_REPAIR) == 0u) {
+    // shade_water_sec (resolve.wgsl:1247-1259): the block's legs
+    const WaterCtx x = water_ctx(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
+    const uint64_t h = (uint64_t)(py >> 1) * ws.hw + (px >> 1);
+    color = water_compose(f, L, x, from_half4(ws.refr[h]), from_half4(ws.refl[h]));
+  } else {
+    color = shade_water(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
+  }
+  const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
+  const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
+  color = mix3(color, sky_base(f, L, rd, shaft), alpha);
+  out[(uint64_t)py * f.res[0] + px] = make_float4(color.x, color.y, color.z, 1.0f);
+}
+
 // PART 0: the opaque surfaces, 1: the sky, 2: water, 3: glass.  Four
 // launches over the frame instead of one kernel with every path: each
 // kernel carries a part of the code (one kernel stalled on instruction
@@ -624,7 +693,8 @@ cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, 
   const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
   k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
   k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
-  k_resolve<2><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
+  if (ws.refr != nullptr && water_sec_shift == 1u) k_resolve_water<<<grid, block, 0, s>>>(f, w, L, vis, ws, out);
+  else k_resolve<2><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
   k_resolve<3><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
   return cudaGetLastError();
 }

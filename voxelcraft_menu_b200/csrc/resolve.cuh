@@ -130,7 +130,7 @@ __device__ __forceinline__ float cloud_noise(float px, float py) {
 
 static __device__ __noinline__ float cloud_fbm(float px, float py, float fp) {
   float freq = 1.0f, amp = 1.0f, sum = 0.0f, norm = 0.0f;
-#pragma unroll
+#pragma unroll 1
   for (int i = 0; i < 4; ++i) {
     const float w = amp * (1.0f - smoothstep(0.25f, 0.5f, fp * freq));
     if (w > 0.0f) {

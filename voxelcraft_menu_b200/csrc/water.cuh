@@ -34,36 +34,35 @@ __device__ __forceinline__ F3 wave_octave(float px_, float pz_, float dx, float 
   return {dx * s, dz * s, 0.5f * slope * slope * (1.0f - fade * fade)};
 }
 
-// wave_field: the sum of the octaves (8 with FLAG_WAVE_FILL, else 4)
+// the octaves of wave_field (resolve.wgsl:944-965): direction x, z, the
+// wavelength divisor, the amplitude share and the phase rate; FLAG_WAVE_FILL's
+// eight, else the base four
+static __constant__ float WAVE_FILL_OCTAVES[8][5] = {
+    {-0.438371f, 0.898794f, 1.0f, 0.3086f, 1.0000f},    {-0.927184f, 0.374607f, 1.3934f, 0.2584f, 1.1804f},
+    {-0.190809f, 0.981627f, 1.9417f, 0.2163f, 1.3934f}, {-0.669131f, 0.743145f, 2.7056f, 0.1810f, 1.6449f},
+    {0.121869f, 0.992546f, 3.7700f, 0.1515f, 1.9417f},  {0.694658f, 0.719340f, 5.2533f, 0.1269f, 2.2920f},
+    {0.970296f, 0.241922f, 7.3201f, 0.1062f, 2.7056f},  {0.438371f, 0.898794f, 10.2000f, 0.0889f, 3.1937f}};
+static __constant__ float WAVE_BASE_OCTAVES[4][5] = {{0.913089f, 0.407760f, 1.0f, 0.42f, 1.0000f},
+                                                     {-0.388685f, 0.921371f, 2.17f, 0.27f, 1.4731f},
+                                                     {-0.980382f, -0.197108f, 4.71f, 0.19f, 2.1703f},
+                                                     {0.477328f, -0.878725f, 10.20f, 0.12f, 3.1937f}};
+
+// wave_field: the sum of the octaves (8 with FLAG_WAVE_FILL, else 4).  The
+// loop stays rolled: unrolled, its transcendentals made the kernels that
+// shade water outgrow the instruction cache.
 __device__ __forceinline__ F3 wave_field(const vm_frame& f, float x, float z, float px, float vhx, float vhz, float kk,
                                          bool aniso, float shoal) {
   const float l0 = f.wave_scale;
   const float a = f.wave_amp * shoal;
   const float ph = f.time * f.wave_speed * WAVE_TAU;
+  const bool fill = (f.flags & VM_FLAG_WAVE_FILL) != 0u;
+  const float (*tab)[5] = fill ? WAVE_FILL_OCTAVES : WAVE_BASE_OCTAVES;
+  const int n = fill ? 8 : 4;
   F3 s = {0.0f, 0.0f, 0.0f};
-  if ((f.flags & VM_FLAG_WAVE_FILL) != 0u) {
-    const float dir[8][2] = {{-0.438371f, 0.898794f}, {-0.927184f, 0.374607f}, {-0.190809f, 0.981627f},
-                             {-0.669131f, 0.743145f}, {0.121869f, 0.992546f},  {0.694658f, 0.719340f},
-                             {0.970296f, 0.241922f},  {0.438371f, 0.898794f}};
-    const float div[8] = {1.0f, 1.3934f, 1.9417f, 2.7056f, 3.7700f, 5.2533f, 7.3201f, 10.2000f};
-    const float amp[8] = {0.3086f, 0.2584f, 0.2163f, 0.1810f, 0.1515f, 0.1269f, 0.1062f, 0.0889f};
-    const float phm[8] = {1.0000f, 1.1804f, 1.3934f, 1.6449f, 1.9417f, 2.2920f, 2.7056f, 3.1937f};
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const float lambda = i == 0 ? l0 : l0 / div[i];
-      s = s + wave_octave(x, z, dir[i][0], dir[i][1], lambda, a * amp[i], ph * phm[i], px, vhx, vhz, kk, aniso);
-    }
-    return s;
-  }
-  const float dir[4][2] = {{0.913089f, 0.407760f}, {-0.388685f, 0.921371f}, {-0.980382f, -0.197108f},
-                           {0.477328f, -0.878725f}};
-  const float div[4] = {1.0f, 2.17f, 4.71f, 10.20f};
-  const float amp[4] = {0.42f, 0.27f, 0.19f, 0.12f};
-  const float phm[4] = {1.0000f, 1.4731f, 2.1703f, 3.1937f};
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float lambda = i == 0 ? l0 : l0 / div[i];
-    s = s + wave_octave(x, z, dir[i][0], dir[i][1], lambda, a * amp[i], ph * phm[i], px, vhx, vhz, kk, aniso);
+#pragma unroll 1
+  for (int i = 0; i < n; ++i) {
+    const float lambda = i == 0 ? l0 : l0 / tab[i][2];
+    s = s + wave_octave(x, z, tab[i][0], tab[i][1], lambda, a * tab[i][3], ph * tab[i][4], px, vhx, vhz, kk, aniso);
   }
   return s;
 }
