@@ -588,12 +588,12 @@ def bench_reflect(m, w, stream, flush, steps, warmup):
 
 
 def bench_resolve(m, w, pools, stream, flush, steps, warmup, cpu=True):
-    """Lane 0 of the resolve (vm_resolve: sky and opaque surfaces with the
-    engine's default look, probe field and shaft envelope) over the timed
-    1080p frame.  Algorithmic bytes per launch: 28 per pixel (8 key + 4 shadow
-    read, 16 RGBA written); the material gathers (chunk records, light, tree
-    nodes, atlas, probes, shaft) are L2-resident.  The oracle is timed on a
-    bounded sample of rows and compared there."""
+    """The resolve (vm_resolve: sky, opaque surfaces, water with its shared
+    legs and glass, with the engine's default look, probe field and shaft
+    envelope) over the timed 1080p frame.  Algorithmic bytes per call: 28 per
+    pixel (8 key + 4 shadow read, 16 RGBA written); the material gathers
+    (chunk records, light, tree nodes, atlas, probes, shaft) are L2-resident.
+    The oracle is timed on a bounded sample of rows and compared there."""
     import torch
     from oracle.oracle import Oracle
     from voxelcraft_menu_b200 import look as LK

@@ -133,7 +133,7 @@ cudaError_t launch_soften(const vm_frame& f, const vmd::DevWorld& w, const unsig
 // (2^shift)^2 block; null: every water pixel traces its own legs).
 cudaError_t launch_resolve(const vm_frame& f, const vmd::DevWorld& w, const vmd::Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
-                           uint16_t* leg_refr, uint16_t* leg_refl, float4* out, cudaStream_t s);
+                           uint16_t* leg_refr, uint16_t* leg_refl, float* light_ao, float4* out, cudaStream_t s);
 cudaError_t launch_expand(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                           int32_t wx, int32_t wy, int32_t wz, uint32_t dx, uint32_t dy, uint32_t dz,
                           uint32_t* voxel, uint8_t* face, float* t, cudaStream_t s);

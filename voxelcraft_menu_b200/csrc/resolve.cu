@@ -11,62 +11,24 @@
 
 namespace vmd {
 
-__device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx,
-                                         uint32_t vy, uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist,
-                                         float shadow_dist, bool smooth, bool do_spec, float lit_in) {
+// The light terms of a surface hit (resolve.wgsl:617-747 of shade_hit), from
+// the light word of a foliage voxel, the one voxel in front of the face (flat
+// secondaries) or the 3x3 gather with AO (smooth light).
+static __device__ __noinline__ LightTerms surface_light_terms(const DevWorld& w, const vm_frame& f, const Look& L,
+                                                              uint32_t ci, uint32_t vx, uint32_t vy, uint32_t vz,
+                                                              uint32_t nid, F3 n, F3 hit, bool smooth) {
   const Chunk c = ld_chunk(w, ci);
   const float vs = c.vs;
   const bool foliage = nid >= VM_NORMAL_CROSS_A;
-  F3 n = normal_of(nid);
-  if (foliage && dot(n, rd) > 0.0f) n = neg(n);
-  const F3 sun = ld3(f.sun_dir);
-  F3 spec_pre = {0.0f, 0.0f, 0.0f};
-  if ((L.spec_hi & HI_SKY_SPECULAR) != 0u && do_spec)
-    spec_pre = sky_base(f, L, reflect(rd, n), 1.0f) * schlick_ground(clampf(dot(n, neg(rd)), 0.0f, 1.0f));
   const uint32_t axis = nid >> 1u;
   const F3 box_min = ld3(c.origin) + f3((float)vx, (float)vy, (float)vz) * vs;
   const F3 lq = (hit - box_min) / vs;
   const F3 local = {clampf(lq.x, 0.0f, 1.0f), clampf(lq.y, 0.0f, 1.0f), clampf(lq.z, 0.0f, 1.0f)};
-  const uint32_t fi = id * 8u + nid;
-  const uint32_t face_word = fi < L.n_faces ? __ldg(L.faces + fi) : 0u;
-  const uint32_t layer = face_word & 0xFFFFu;
-  float u, v;
-  face_uv(nid, local, &u, &v);
-  if ((f.flags & VM_FLAG_TEX_VARIATION) != 0u) permute_uv(&u, &v, face_word >> 16u, perm_key(box_min, nid));
   float fa, fb;
   int32_t ta[3] = {0, 0, 0}, tb[3] = {0, 0, 0};
   if (axis == 0u) { fa = local.y; fb = local.z; ta[1] = 1; tb[2] = 1; }
   else if (axis == 1u) { fa = local.x; fb = local.z; ta[0] = 1; tb[2] = 1; }
   else { fa = local.x; fb = local.y; ta[0] = 1; tb[1] = 1; }
-  const float grazing = fmaxf(fabsf(dot(n, rd)), 0.25f);
-  const float footprint = fmaxf(dist, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs / grazing;
-  const float lod = clampf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f, 3.0f);
-  const float4 texel = atlas_sample(L, u, v, layer, lod);
-  F3 albedo = {texel.x, texel.y, texel.z};
-  const float tint_mask = foliage ? 1.0f : texel.w;
-  if ((f.flags & VM_FLAG_TINT) != 0u && tint_mask > 0.0f) {
-    const float k = tint_mask * f.tint_strength;
-    albedo = albedo * mix3(f3(1.0f, 1.0f, 1.0f), biome_tint(f, L, hit.x, hit.z), k);
-  }
-  if ((L.spec_hi & HI_SHORE_WET) != 0u && id == VM_SAND) {
-    const float wet = 1.0f - smoothstep(f.sea_level, f.sea_level + 1.5f, hit.y);
-    albedo = albedo * mixf(1.0f, 0.62f, wet);
-  }
-  if ((L.spec_hi & HI_FOLIAGE_RICH) != 0u && (foliage || ((id == VM_GRASS || id == VM_MEADOW) && nid == VM_NORMAL_PY))) {
-    const float hr = hash_alpha(box_min);
-    const float hv = hash_alpha(box_min + f3(17.31f, 7.77f, 3.03f));
-    F3 rich = {1.0f, 1.0f, 1.0f};
-    if (hr < 0.16f) rich = f3(1.30f, 1.10f, 0.55f);
-    else if (hr > 0.97f) rich = f3(1.35f, 0.72f, 0.95f);
-    albedo = albedo * rich * mixf(0.88f, 1.10f, hv);
-  }
-  if ((L.spec_hi & HI_CANOPY_RELIEF) != 0u && is_cutout_id(id)) {
-    const float clump = cloud_noise(box_min.x * 0.21f + box_min.y * 0.313f, box_min.z * 0.21f + box_min.y * 0.173f);
-    const float relief = mixf(0.72f, 1.34f, clump * clump);
-    const float micro = mixf(0.92f, 1.08f, hash_alpha(box_min));
-    const float toward_sun = clampf(dot(n, sun) * 0.5f + 0.5f, 0.0f, 1.0f);
-    albedo = albedo * relief * micro * mixf(0.84f, 1.0f, toward_sun);
-  }
   const F3 sky_tint = surface_sky_fill(f, L, n);
   const bool light_rgb = (f.flags & VM_FLAG_LIGHT_RGB) != 0u;
   const bool gather = (w.spec & VM_SPEC_EMITTER_GATHER) != 0u;
@@ -165,6 +127,65 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
     sky_sm = mixf(mixf(sky_c[0], sky_c[1], fa), mixf(sky_c[2], sky_c[3], fa), fb);
     amb = mix3(mix3(amb_c[0], amb_c[1], fa), mix3(amb_c[2], amb_c[3], fa), fb);
   }
+  return {amb, sky_sm, ao};
+}
+
+__device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx,
+                                         uint32_t vy, uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist,
+                                         float shadow_dist, bool smooth, bool do_spec, float lit_in,
+                                         const LightTerms* pre) {
+  const Chunk c = ld_chunk(w, ci);
+  const float vs = c.vs;
+  const bool foliage = nid >= VM_NORMAL_CROSS_A;
+  F3 n = normal_of(nid);
+  if (foliage && dot(n, rd) > 0.0f) n = neg(n);
+  const F3 sun = ld3(f.sun_dir);
+  F3 spec_pre = {0.0f, 0.0f, 0.0f};
+  if ((L.spec_hi & HI_SKY_SPECULAR) != 0u && do_spec)
+    spec_pre = sky_base(f, L, reflect(rd, n), 1.0f) * schlick_ground(clampf(dot(n, neg(rd)), 0.0f, 1.0f));
+  const F3 box_min = ld3(c.origin) + f3((float)vx, (float)vy, (float)vz) * vs;
+  const F3 lq = (hit - box_min) / vs;
+  const F3 local = {clampf(lq.x, 0.0f, 1.0f), clampf(lq.y, 0.0f, 1.0f), clampf(lq.z, 0.0f, 1.0f)};
+  const uint32_t fi = id * 8u + nid;
+  const uint32_t face_word = fi < L.n_faces ? __ldg(L.faces + fi) : 0u;
+  const uint32_t layer = face_word & 0xFFFFu;
+  float u, v;
+  face_uv(nid, local, &u, &v);
+  if ((f.flags & VM_FLAG_TEX_VARIATION) != 0u) permute_uv(&u, &v, face_word >> 16u, perm_key(box_min, nid));
+  const float grazing = fmaxf(fabsf(dot(n, rd)), 0.25f);
+  const float footprint = fmaxf(dist, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * 16.0f / vs / grazing;
+  const float lod = clampf(log2f(fmaxf(footprint, 1e-4f)) + f.mip_bias, 0.0f, 3.0f);
+  const float4 texel = atlas_sample(L, u, v, layer, lod);
+  F3 albedo = {texel.x, texel.y, texel.z};
+  const float tint_mask = foliage ? 1.0f : texel.w;
+  if ((f.flags & VM_FLAG_TINT) != 0u && tint_mask > 0.0f) {
+    const float k = tint_mask * f.tint_strength;
+    albedo = albedo * mix3(f3(1.0f, 1.0f, 1.0f), biome_tint(f, L, hit.x, hit.z), k);
+  }
+  if ((L.spec_hi & HI_SHORE_WET) != 0u && id == VM_SAND) {
+    const float wet = 1.0f - smoothstep(f.sea_level, f.sea_level + 1.5f, hit.y);
+    albedo = albedo * mixf(1.0f, 0.62f, wet);
+  }
+  if ((L.spec_hi & HI_FOLIAGE_RICH) != 0u && (foliage || ((id == VM_GRASS || id == VM_MEADOW) && nid == VM_NORMAL_PY))) {
+    const float hr = hash_alpha(box_min);
+    const float hv = hash_alpha(box_min + f3(17.31f, 7.77f, 3.03f));
+    F3 rich = {1.0f, 1.0f, 1.0f};
+    if (hr < 0.16f) rich = f3(1.30f, 1.10f, 0.55f);
+    else if (hr > 0.97f) rich = f3(1.35f, 0.72f, 0.95f);
+    albedo = albedo * rich * mixf(0.88f, 1.10f, hv);
+  }
+  if ((L.spec_hi & HI_CANOPY_RELIEF) != 0u && is_cutout_id(id)) {
+    const float clump = cloud_noise(box_min.x * 0.21f + box_min.y * 0.313f, box_min.z * 0.21f + box_min.y * 0.173f);
+    const float relief = mixf(0.72f, 1.34f, clump * clump);
+    const float micro = mixf(0.92f, 1.08f, hash_alpha(box_min));
+    const float toward_sun = clampf(dot(n, sun) * 0.5f + 0.5f, 0.0f, 1.0f);
+    albedo = albedo * relief * micro * mixf(0.84f, 1.0f, toward_sun);
+  }
+  LightTerms lt;
+  if (pre != nullptr) lt = *pre;
+  else lt = surface_light_terms(w, f, L, ci, vx, vy, vz, nid, n, hit, smooth);
+  const F3 amb = lt.amb;
+  const float sky_sm = lt.sky_sm, ao = lt.ao;
   float direct = 0.0f;
   const float ndl = dot(n, sun);
   if (ndl > 0.0f && f.daylight > 0.01f) {
@@ -325,7 +346,7 @@ static __device__ __noinline__ F3 shade_leg(const DevWorld& w, const vm_frame& f
   const Chunk c = ld_chunk(w, h.ci);
   const uint32_t id = block_at(w, c, h.vx, h.vy, h.vz);
   return shade_surface(w, f, L, h.ci, h.vx, h.vy, h.vz, id, h.normal, p, d, dist, shadow_dist, secondary_smooth(f),
-                       false, -1.0f);
+                       false, -1.0f, nullptr);
 }
 
 // water_refract_leg / water_reflect_leg: resolve.wgsl:1029-1058, as
@@ -623,6 +644,39 @@ __global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant_
   out[(uint64_t)py * f.res[0] + px] = make_float4(color.x, color.y, color.z, 1.0f);
 }
 
+// The light terms of every opaque-surface pixel, ahead of k_resolve<0>: the
+// 3x3 light and AO gather (tree walks, light bricks, the neighbour chunks)
+// in a kernel of its own, so that the shading kernel's code stays small.
+// Writes (amb, sky_sm) into the pixel's colour, which k_resolve<0> reads and
+// overwrites, and the AO into light_ao.
+__global__ void __launch_bounds__(128, 8) k_resolve_light(const __grid_constant__ vm_frame f,
+                                                          const __grid_constant__ DevWorld w,
+                                                          const __grid_constant__ Look L,
+                                                          const unsigned long long* __restrict__ vis,
+                                                          float4* __restrict__ out, float* __restrict__ light_ao) {
+  const uint32_t px = blockIdx.x * 32u + threadIdx.x, py = blockIdx.y * 4u + threadIdx.y;
+  if (px >= f.res[0] || py >= f.res[1]) return;
+  const uint64_t pix = (uint64_t)py * f.res[0] + px;
+  const unsigned long long key = vis[pix];
+  if (key == 0ull) return;
+  const uint32_t nid = (uint32_t)(key >> 37) & 7u;
+  const uint32_t ci = (uint32_t)(key >> 24) & 0x1FFFu;
+  const uint32_t low = (uint32_t)(key & 0xFFFFFFull);
+  const uint32_t vx = (low >> 16) & 63u, vy = (low >> 8) & 63u, vz = low & 63u;
+  const uint32_t mx = (low >> 22) & 3u, my = (low >> 14) & 3u, mz = (low >> 6) & 3u;
+  const Chunk c = ld_chunk(w, ci);
+  const uint32_t id = block_at(w, c, vx, vy, vz);
+  if (id == VM_WATER || ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS)) return;
+  const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+  const float t = hit_t(f, c, vx, vy, vz, mx, my, mz, nid, rd);
+  const F3 hit = ld3(f.cam_pos) + rd * t;
+  F3 n = normal_of(nid);
+  if (nid >= VM_NORMAL_CROSS_A && dot(n, rd) > 0.0f) n = neg(n);
+  const LightTerms lt = surface_light_terms(w, f, L, ci, vx, vy, vz, nid, n, hit, true);
+  out[pix] = make_float4(lt.amb.x, lt.amb.y, lt.amb.z, lt.sky_sm);
+  light_ao[pix] = lt.ao;
+}
+
 // PART 0: the opaque surfaces, 1: the sky, 2: water, 3: glass.  Four
 // launches over the frame instead of one kernel with every path: each
 // kernel carries a part of the code (one kernel stalled on instruction
@@ -632,7 +686,8 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
                                                     const __grid_constant__ Look L,
                                                     const unsigned long long* __restrict__ vis,
                                                     const float* __restrict__ mask, const float* __restrict__ dist,
-                                                    bool soft, WaterSec ws, float4* __restrict__ out) {
+                                                    bool soft, WaterSec ws, const float* __restrict__ light_ao,
+                                                    float4* __restrict__ out) {
   const uint32_t px = blockIdx.x * 32u + threadIdx.x, py = blockIdx.y * 4u + threadIdx.y;
   if (px >= f.res[0] || py >= f.res[1]) return;
   const uint64_t pix = (uint64_t)py * f.res[0] + px;
@@ -657,8 +712,13 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
     const int part = id == VM_WATER ? 2 : ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS ? 3 : 0);
     if (part != PART) return;
     if (PART == 0) {
+      LightTerms lt;
+      if (light_ao != nullptr) {
+        const float4 a = out[pix];
+        lt = {f3(a.x, a.y, a.z), a.w, light_ao[pix]};
+      }
       color = shade_surface(w, f, L, ci, vx, vy, vz, id, nid, hit, rd, t, f.shadow_dist, true, true,
-                            sun_visibility(mask, dist, soft, pix));
+                            sun_visibility(mask, dist, soft, pix), light_ao != nullptr ? &lt : nullptr);
     } else if (PART == 2) {
       if (ws.refr != nullptr &&
           !((w.spec & VM_SPEC_WATER_REPAIR) != 0u && !water_share_safe(f, w, vis, ws.shift, px, py, nid, hit, t))) {
@@ -681,7 +741,7 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
 
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
-                           uint16_t* leg_refr, uint16_t* leg_refl, float4* out, cudaStream_t s) {
+                           uint16_t* leg_refr, uint16_t* leg_refl, float* light_ao, float4* out, cudaStream_t s) {
   WaterSec ws{nullptr, nullptr, water_sec_shift, 0u};
   if (leg_refr != nullptr) {
     const uint32_t span = 1u << water_sec_shift;
@@ -691,11 +751,12 @@ cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, 
     ws = {(const ushort4*)leg_refr, (const ushort4*)leg_refl, water_sec_shift, hw};
   }
   const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
-  k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
-  k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
+  if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, out, light_ao);
+  k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, light_ao, out);
+  k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
   if (ws.refr != nullptr && water_sec_shift == 1u) k_resolve_water<<<grid, block, 0, s>>>(f, w, L, vis, ws, out);
-  else k_resolve<2><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
-  k_resolve<3><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, out);
+  else k_resolve<2><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
+  k_resolve<3><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
   return cudaGetLastError();
 }
 
