@@ -52,6 +52,10 @@ struct vm_ctx {
   bool chunks_foliage = false;   // a chunk of the uploaded list holds tufts (VM_ATTR_HAS_FOLIAGE)
   bool batch_foliage = false;    // the same for the batch's chunk lists
   bool have_probes = false, have_shaft = false, color_done = false;
+  // the resolve's water and glass lanes run beside the sky / opaque lanes:
+  // two streams forked from the context's stream and joined back by events
+  cudaStream_t lane_stream[2] = {nullptr, nullptr};
+  cudaEvent_t lane_event[3] = {nullptr, nullptr, nullptr};
   DevBuf shadow16;      // vm_read_async_r16f staging, sized on first use
   DevBuf refl_key, refl_t;   // reflect legs of water hits, sized by the first FLAG_WATER_REFLECT frame
   DevBuf ws_refr_key, ws_refr_t, ws_refl_key, ws_refl_t;   // vm_water_sec cells, sized by its first call
@@ -339,6 +343,10 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->atlas_alpha, &ctx->leg_refr, &ctx->leg_refl, &ctx->light_ao};
   for (DevBuf* b : all) release(*b);
   if (ctx->rendered) cudaEventDestroy(ctx->rendered);
+  for (cudaEvent_t e : ctx->lane_event)
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t ls : ctx->lane_stream)
+    if (ls) cudaStreamDestroy(ls);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
 }
@@ -1098,6 +1106,12 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
                 "are not built", spec_hi & HI_UNBUILT);
   CK(cudaSetDevice(ctx->device));
   if ((rc = ensure(ctx, ctx->color, npix * 16)) || (rc = ensure(ctx, ctx->light_ao, npix * 4))) return rc;
+  if (!ctx->lane_stream[0]) {
+    int least = 0, greatest = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    for (cudaStream_t& ls : ctx->lane_stream) CK(cudaStreamCreateWithPriority(&ls, cudaStreamNonBlocking, greatest));
+    for (cudaEvent_t& e : ctx->lane_event) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
   vmd::Look L;
   L.atlas = (const float4*)ctx->atlas.p; L.atlas_layers = ctx->atlas_layers;
   L.faces = (const uint32_t*)ctx->faces.p; L.n_faces = ctx->n_faces;
@@ -1116,7 +1130,8 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
   }
   CK(vmk::launch_resolve(f, dev_world(ctx), L, (const unsigned long long*)ctx->vis.p, mask,
                          (const float*)ctx->shadow.p, (ctx->spec & VM_SPEC_SOFT_RAYS) != 0u, WATER_SEC_SHIFT, refr,
-                         refl, (float*)ctx->light_ao.p, (float4*)ctx->color.p, ctx->stream));
+                         refl, (float*)ctx->light_ao.p, (float4*)ctx->color.p, ctx->stream, ctx->lane_stream,
+                         ctx->lane_event));
   ctx->color_done = true;
   return VM_OK;
 }

@@ -741,23 +741,40 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
 
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
-                           uint16_t* leg_refr, uint16_t* leg_refl, float* light_ao, float4* out, cudaStream_t s) {
+                           uint16_t* leg_refr, uint16_t* leg_refl, float* light_ao, float4* out, cudaStream_t s,
+                           const cudaStream_t lane_stream[2], const cudaEvent_t lane_event[3]) {
+  // The lanes write disjoint pixels.  The water lane (its legs, then the
+  // pixels) and the glass lane cover a few clustered pixels with long serial
+  // traces, which leave most SMs idle: they run on two streams of their own,
+  // forked from s and joined back into it, beside the sky / opaque lanes.
+  cudaError_t e;
+  if ((e = cudaEventRecord(lane_event[0], s)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(lane_stream[0], lane_event[0], 0)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(lane_stream[1], lane_event[0], 0)) != cudaSuccess)
+    return e;
+  const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
+  k_resolve<3><<<grid, block, 0, lane_stream[1]>>>(f, w, L, vis, mask, dist, soft_rays, WaterSec{nullptr, nullptr, 0u, 0u},
+                                                   nullptr, out);
   WaterSec ws{nullptr, nullptr, water_sec_shift, 0u};
+  const cudaStream_t sw = lane_stream[0];
   if (leg_refr != nullptr) {
     const uint32_t span = 1u << water_sec_shift;
     const uint32_t hw = (f.res[0] + span - 1u) >> water_sec_shift, hh = (f.res[1] + span - 1u) >> water_sec_shift;
-    k_water_legs<<<dim3((hw + 15) / 16, (hh + 7) / 8), dim3(16, 8), 0, s>>>(
+    k_water_legs<<<dim3((hw + 15) / 16, (hh + 7) / 8), dim3(16, 8), 0, sw>>>(
         f, w, L, vis, water_sec_shift, (ushort4*)leg_refr, (ushort4*)leg_refl);
     ws = {(const ushort4*)leg_refr, (const ushort4*)leg_refl, water_sec_shift, hw};
   }
-  const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
+  if (ws.refr != nullptr && water_sec_shift == 1u) k_resolve_water<<<grid, block, 0, sw>>>(f, w, L, vis, ws, out);
+  else k_resolve<2><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
   if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, out, light_ao);
   k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, light_ao, out);
   k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
-  if (ws.refr != nullptr && water_sec_shift == 1u) k_resolve_water<<<grid, block, 0, s>>>(f, w, L, vis, ws, out);
-  else k_resolve<2><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
-  k_resolve<3><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
-  return cudaGetLastError();
+  if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaEventRecord(lane_event[1], lane_stream[0])) != cudaSuccess ||
+      (e = cudaEventRecord(lane_event[2], lane_stream[1])) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(s, lane_event[1], 0)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(s, lane_event[2], 0)) != cudaSuccess)
+    return e;
+  return cudaSuccess;
 }
 
 }  // namespace vmk
