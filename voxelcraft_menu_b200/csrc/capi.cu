@@ -53,9 +53,9 @@ struct vm_ctx {
   bool batch_foliage = false;    // the same for the batch's chunk lists
   bool have_probes = false, have_shaft = false, color_done = false;
   // the resolve's water and glass lanes run beside the sky / opaque lanes:
-  // two streams forked from the context's stream and joined back by events
-  cudaStream_t lane_stream[2] = {nullptr, nullptr};
-  cudaEvent_t lane_event[3] = {nullptr, nullptr, nullptr};
+  // three streams forked from the context's stream and joined back by events
+  cudaStream_t lane_stream[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t lane_event[4] = {nullptr, nullptr, nullptr, nullptr};
   DevBuf shadow16;      // vm_read_async_r16f staging, sized on first use
   DevBuf refl_key, refl_t;   // reflect legs of water hits, sized by the first FLAG_WATER_REFLECT frame
   DevBuf ws_refr_key, ws_refr_t, ws_refl_key, ws_refl_t;   // vm_water_sec cells, sized by its first call

@@ -581,6 +581,12 @@ struct WaterSec { const ushort4* refr; const ushort4* refl; uint32_t shift, hw; 
 // pixel once (hit distance, hit height, normal, water or not) into shared
 // memory and the comparisons read it there: the same values the per-pixel
 // test recomputes, with a quarter of the chunk and tree loads.
+// OWN = false: the pixels that compose the block's shared legs (run after
+// k_water_legs); OWN = true: the pixels that water_share_safe sends to their
+// own legs under SPEC_WATER_REPAIR (independent of k_water_legs, so they
+// start with the other lanes: their two legs per pixel are the lane's
+// longest threads).
+template <bool OWN>
 __global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant__ vm_frame f,
                                                           const __grid_constant__ DevWorld w,
                                                           const __grid_constant__ Look L,
@@ -629,8 +635,10 @@ __global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant_
           fabsf(s_t[by + y][bx + x] - t) > fmaxf(0.1f, fminf(1.0f, t * 0.02f)))
         safe = false;
     }
+  const bool shared = safe || (w.spec & VM_SPEC_WATER_REPAIR) == 0u;
+  if (shared == OWN) return;
   F3 color;
-  if (safe || (w.spec & VM_SPEC_WATER_REPAIR) == 0u) {
+  if (!OWN) {
     // shade_water_sec (resolve.wgsl:1247-1259): the block's legs
     const WaterCtx x = water_ctx(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
     const uint64_t h = (uint64_t)(py >> 1) * ws.hw + (px >> 1);
@@ -742,17 +750,18 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
                            uint16_t* leg_refr, uint16_t* leg_refl, float* light_ao, float4* out, cudaStream_t s,
-                           const cudaStream_t lane_stream[2], const cudaEvent_t lane_event[3]) {
+                           const cudaStream_t lane_stream[3], const cudaEvent_t lane_event[4]) {
   // The lanes write disjoint pixels.  The water lane (its legs, then the
   // pixels) and the glass lane cover a few clustered pixels with long serial
-  // traces, which leave most SMs idle: they run on two streams of their own,
+  // traces, which leave most SMs idle: they run on streams of their own,
   // forked from s and joined back into it, beside the sky / opaque lanes.
-  cudaError_t e;
-  if ((e = cudaEventRecord(lane_event[0], s)) != cudaSuccess ||
-      (e = cudaStreamWaitEvent(lane_stream[0], lane_event[0], 0)) != cudaSuccess ||
-      (e = cudaStreamWaitEvent(lane_stream[1], lane_event[0], 0)) != cudaSuccess)
-    return e;
+  cudaError_t e = cudaEventRecord(lane_event[0], s);
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(lane_stream[i], lane_event[0], 0);
+  if (e != cudaSuccess) return e;
   const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
+  const bool split_water = leg_refr != nullptr && water_sec_shift == 1u;
+  if (split_water && (w.spec & VM_SPEC_WATER_REPAIR) != 0u)
+    k_resolve_water<true><<<grid, block, 0, lane_stream[2]>>>(f, w, L, vis, WaterSec{nullptr, nullptr, 1u, 0u}, out);
   k_resolve<3><<<grid, block, 0, lane_stream[1]>>>(f, w, L, vis, mask, dist, soft_rays, WaterSec{nullptr, nullptr, 0u, 0u},
                                                    nullptr, out);
   WaterSec ws{nullptr, nullptr, water_sec_shift, 0u};
@@ -764,17 +773,17 @@ cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, 
         f, w, L, vis, water_sec_shift, (ushort4*)leg_refr, (ushort4*)leg_refl);
     ws = {(const ushort4*)leg_refr, (const ushort4*)leg_refl, water_sec_shift, hw};
   }
-  if (ws.refr != nullptr && water_sec_shift == 1u) k_resolve_water<<<grid, block, 0, sw>>>(f, w, L, vis, ws, out);
+  if (split_water) k_resolve_water<false><<<grid, block, 0, sw>>>(f, w, L, vis, ws, out);
   else k_resolve<2><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
   if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, out, light_ao);
   k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, light_ao, out);
   k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
-  if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaEventRecord(lane_event[1], lane_stream[0])) != cudaSuccess ||
-      (e = cudaEventRecord(lane_event[2], lane_stream[1])) != cudaSuccess ||
-      (e = cudaStreamWaitEvent(s, lane_event[1], 0)) != cudaSuccess ||
-      (e = cudaStreamWaitEvent(s, lane_event[2], 0)) != cudaSuccess)
-    return e;
-  return cudaSuccess;
+  e = cudaGetLastError();
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+    e = cudaEventRecord(lane_event[1 + i], lane_stream[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, lane_event[1 + i], 0);
+  }
+  return e;
 }
 
 }  // namespace vmk
