@@ -4,9 +4,11 @@ and the half-resolution water_sec legs or per-pixel legs, glass with its
 transmission and reflection; the fog blend with sun shafts, sky_color with
 clouds) against the oracle's restatement.
 
-The kernel and the oracle share the float contract but not the
-transcendental functions (CUDA's expf / powf / log2f / logf / exp2f against
-the host's), so colours are compared within a tolerance: 2e-4 absolute plus
+The kernel and the oracle share the float contract of the march but not
+the colour arithmetic: the kernel divides, exponentiates and takes logs and
+powers at the accuracy WGSL specifies for the engine's shaders (approximate
+reciprocal, exp2 and log2 units), the oracle with IEEE division and the
+host's libm, so colours are compared within a tolerance: 2e-4 absolute plus
 1e-3 relative at 99.9% of the pixels, and 0.05 absolute at every pixel (a
 last-bit difference can move a texture-level or a smoothstep edge, or a
 water_sec leg across a binary16 rounding step).

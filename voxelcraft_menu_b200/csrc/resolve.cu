@@ -43,7 +43,7 @@ static __device__ __noinline__ LightTerms surface_light_terms(const DevWorld& w,
       amb = block_ambient(light_curve3(light_block_rgb(packed)), sk, sky_tint);
     } else {
       const float bk = light_curve(light_block_level(packed));
-      amb = mix3(sky_tint, block_tint(), bk / fmaxf(sk + bk, 1e-4f)) * fmaxf(sk, bk);
+      amb = mix3(sky_tint, block_tint(), wdiv(bk, fmaxf(sk + bk, 1e-4f))) * fmaxf(sk, bk);
     }
   } else if (!smooth) {
     // one light sample: the voxel in front of the face, in this chunk or
@@ -60,7 +60,7 @@ static __device__ __noinline__ LightTerms surface_light_terms(const DevWorld& w,
       amb = block_ambient(light_curve3(light_block_rgb(packed1)), sk1, sky_tint);
     } else {
       const float bk1 = light_curve(light_block_level(packed1));
-      amb = mix3(sky_tint, block_tint(), bk1 / fmaxf(sk1 + bk1, 1e-4f)) * fmaxf(sk1, bk1);
+      amb = mix3(sky_tint, block_tint(), wdiv(bk1, fmaxf(sk1 + bk1, 1e-4f))) * fmaxf(sk1, bk1);
     }
   } else {
     const F3 air_c = box_min + f3(0.5f * vs, 0.5f * vs, 0.5f * vs) + n * vs;
@@ -101,7 +101,7 @@ static __device__ __noinline__ LightTerms surface_light_terms(const DevWorld& w,
       const int ia = 4 + ((k & 1) * 2 - 1);
       const int ib = 4 + ((k >> 1) * 2 - 1) * 3;
       const int ic = ia + ib - 4;
-      const float inv = 1.0f / (1.0f + open_n[ia] + open_n[ib] + open_n[ic]);
+      const float inv = wdiv(1.0f, 1.0f + open_n[ia] + open_n[ib] + open_n[ic]);
       const float sk = (sky_n[4] + sky_n[ia] * open_n[ia] + sky_n[ib] * open_n[ib] + sky_n[ic] * open_n[ic]) * inv;
       sky_c[k] = sk;
       if (light_rgb) {
@@ -116,7 +116,7 @@ static __device__ __noinline__ LightTerms surface_light_terms(const DevWorld& w,
         }
       } else {
         const float bk = (blk_n[4] + blk_n[ia] * open_n[ia] + blk_n[ib] * open_n[ib] + blk_n[ic] * open_n[ic]) * inv;
-        amb_c[k] = mix3(sky_tint, block_tint(), bk / fmaxf(sk + bk, 1e-4f)) * fmaxf(sk, bk);
+        amb_c[k] = mix3(sky_tint, block_tint(), wdiv(bk, fmaxf(sk + bk, 1e-4f))) * fmaxf(sk, bk);
       }
       const float s1 = 1.0f - open_n[ia];
       const float s2 = 1.0f - open_n[ib];
@@ -203,7 +203,7 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
     if ((L.spec_hi & HI_CAUSTICS) != 0u) {
       const float cdepth = f.sea_level - hit.y;
       if (cdepth > 0.0f && cdepth < 8.0f && direct > 0.0f) {
-        const float k = cdepth / fmaxf(sun.y, 1e-3f);
+        const float k = wdiv(cdepth, fmaxf(sun.y, 1e-3f));
         const float spx = hit.x - sun.x * k, spz = hit.z - sun.z * k;
         const float a = f.wave_amp, l0 = f.wave_scale, ph = f.time * f.wave_speed * WAVE_TAU;
         const F3 g0 = wave_octave(spx, spz, 0.913089f, 0.407760f, l0, a * 0.42f, ph, 0.35f, 0.0f, 0.0f, 0.0f, false);
@@ -212,7 +212,7 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
         const float r0 = g0.x * g0.x + g0.y * g0.y;
         const float r1 = g1.x * g1.x + g1.y * g1.y;
         const float sheets = r0 * r1 * 4000.0f;
-        direct = direct * (1.0f + sheets * expf(-cdepth * 0.30f));
+        direct = direct * (1.0f + sheets * wexp(-cdepth * 0.30f));
       }
     }
   }
@@ -258,8 +258,8 @@ __device__ __forceinline__ float medium_light(const vm_frame& f, uint32_t packed
 // water_medium: common.wgsl:1262-1265 (WATER_EXT per channel)
 __device__ __forceinline__ F3 water_medium(const vm_frame& f, F3 c, float d, F3 body) {
   const float dd = fmaxf(d, 0.0f);
-  const F3 tr = {expf(-0.280f * f.water_absorb * dd), expf(-0.055f * f.water_absorb * dd),
-                 expf(-0.020f * f.water_absorb * dd)};
+  const F3 tr = {wexp(-0.280f * f.water_absorb * dd), wexp(-0.055f * f.water_absorb * dd),
+                 wexp(-0.020f * f.water_absorb * dd)};
   return c * tr + body * f3(1.0f - tr.x, 1.0f - tr.y, 1.0f - tr.z);
 }
 __device__ __forceinline__ float schlick_f0(float f0, float cos_i) {   // schlick / schlick_glass
@@ -326,9 +326,9 @@ static __device__ __noinline__ WaterCtx water_ctx(const DevWorld& w, const vm_fr
     const float gl = sqrtf(wf.x * wf.x + wf.y * wf.y);
     const float lim = fminf(1.0f, f.wave_reflect_slope / fmaxf(gl, 1e-6f));
     nt = unit(f3(-(wf.x * lim), 1.0f, -(wf.y * lim)));
-    gloss = 1.0f / (1.0f + 0.5f * 320.0f * wf.z);
+    gloss = wdiv(1.0f, 1.0f + 0.5f * 320.0f * wf.z);
   }
-  const float rough = clampf(1.0f - expf(-8.0f * unresolved), 0.0f, 1.0f);
+  const float rough = clampf(1.0f - wexp(-8.0f * unresolved), 0.0f, 1.0f);
   nw = unit(nw * (1.0f - rough) + n * rough);
   nt = unit(nt * (1.0f - rough) + n * rough);
   x.n = n; x.nw = nw; x.nt = nt; x.gloss = gloss; x.waved = waved;
@@ -410,7 +410,7 @@ static __device__ __noinline__ F3 water_compose(const vm_frame& f, const Look& L
   const F3 sun = ld3(f.sun_dir);
   F3 refl = sky_color(f, L, x.hit, x.mirror, x.t, 1.0f) +
             f3(1.0000f, 0.8469f, 0.5647f) *
-                (powf(fmaxf(dot(x.mirror, sun), 0.0f), 320.0f * x.gloss) * 2.5f * x.gloss * f.daylight);
+                (wpow(fmaxf(dot(x.mirror, sun), 0.0f), 320.0f * x.gloss) * 2.5f * x.gloss * f.daylight);
   if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f && leg_m.w > 0.0f)
     refl = mix3(refl, f3(leg_m.x, leg_m.y, leg_m.z), x.reflect_detail);
   refl = mix3(refl, sky_base(f, L, x.n, 1.0f), x.roughness * 0.65f);

@@ -14,7 +14,11 @@
 // agree up to the last bits of the transcendental functions.
 //
 // Compiled with the march's float contract (--fmad=false): block lookups
-// and voxel indices must match the march exactly.  The larger helpers (sky,
+// and voxel indices must match the march exactly.  The colour arithmetic
+// (fog, sky, clouds, shafts, light curves, shading) runs at the accuracy
+// WGSL specifies for the engine's own shaders instead (wdiv / wexp / wlog /
+// wpow below), on the SM's approximate reciprocal, exp2 and log2 units.
+// The larger helpers (sky,
 // cloud octaves, biome noise, light samples, texture filters, shafts) stay
 // out of line: inlined at every call site the kernel's code outgrew the
 // instruction cache and its warps stalled on instruction fetch.
@@ -35,6 +39,19 @@ struct Look {
   uint32_t spec_hi;                             // the engine's FLAG_HI_* word (the resolve's overrides)
 };
 
+// WGSL's accuracy for the engine's shader arithmetic: x / y within 2.5 ULP
+// (__fdividef: an approximate reciprocal and a multiply, 2 ULP for |y| below
+// 2^126), exp within 3 + 2|x| ULP (__expf), log within 2^-21 absolute on
+// [0.5, 2] and 3 ULP elsewhere (__logf), and pow inheriting its accuracy
+// from exp2(y * log2(x)) (__powf computes exactly that).  IEEE division and
+// CUDA's expf / logf / powf are several times the instructions and buy no
+// accuracy the engine's own colours have.
+__device__ __forceinline__ float wdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ F3 wdiv3(F3 a, float b) { return {wdiv(a.x, b), wdiv(a.y, b), wdiv(a.z, b)}; }
+__device__ __forceinline__ float wexp(float x) { return __expf(x); }
+__device__ __forceinline__ float wlog(float x) { return __logf(x); }
+__device__ __forceinline__ float wpow(float x, float y) { return __powf(x, y); }
+
 constexpr uint32_t ATLAS_SIZE = VM_ATLAS_SIZE, ATLAS_MIPS = VM_ATLAS_MIPS;
 constexpr uint32_t PROBE_NX = VM_PROBE_NX, PROBE_NY = VM_PROBE_NY, PROBE_NZ = VM_PROBE_NZ;
 
@@ -52,9 +69,9 @@ __device__ __forceinline__ float transmittance_from(const vm_frame& f, float y0,
   const float lambda = f.fog_falloff;
   const float x = clampf(lambda * s * rd.y, -60.0f, 60.0f);
   float path = s;
-  if (fabsf(x) > 1e-4f) path = s * (1.0f - expf(-x)) / x;
-  const float rho = f.fog_density * expf(-clampf(lambda * (y0 - f.fog_height), -60.0f, 60.0f));
-  return expf(-clampf(rho * path, 0.0f, 60.0f));
+  if (fabsf(x) > 1e-4f) path = wdiv(s * (1.0f - wexp(-x)), x);
+  const float rho = f.fog_density * wexp(-clampf(lambda * (y0 - f.fog_height), -60.0f, 60.0f));
+  return wexp(-clampf(rho * path, 0.0f, 60.0f));
 }
 
 __device__ __forceinline__ F3 scatter_tint() { return {1.0000f, 0.4770f, 0.1474f}; }
@@ -62,7 +79,7 @@ __device__ __forceinline__ F3 scatter_tint() { return {1.0000f, 0.4770f, 0.1474f
 __device__ __forceinline__ float hg_gain(float cos_t, float g) {
   const float g2 = g * g;
   const float d = 1.0f + g2 - 2.0f * g * cos_t;
-  return (1.0f - g2) / powf(fmaxf(d, 1e-4f), 1.5f);
+  return wdiv(1.0f - g2, wpow(fmaxf(d, 1e-4f), 1.5f));
 }
 
 __device__ __forceinline__ F3 scatter_lobe(const vm_frame& f, F3 rd) {
@@ -88,18 +105,18 @@ static __device__ __noinline__ F3 sky_base(const vm_frame& f, const Look& L, F3 
   const float up = clampf(rd.y, 0.0f, 1.0f);
   const F3 horizon = sky_horizon(L, day);
   const F3 zenith = sky_zenith(L, day);
-  F3 c = mix3(horizon, zenith, powf(up, 0.55f));
+  F3 c = mix3(horizon, zenith, wpow(up, 0.55f));
   const float sd = dot(rd, ld3(f.sun_dir));
   c = c + f3(1.0f, 0.8276f, 0.5225f) * smoothstep(0.9975f, 0.9990f, sd) * fmaxf(day, 0.2f);
   c = c + scatter_lobe(f, rd) * shaft;
   const bool look = (L.spec_hi & HI_SKY_LOOK) != 0u;
   if (look && f.haze_warm > 0.0f) {
-    const float band = powf(1.0f - up, 3.0f);
-    const float toward = 0.35f + 0.65f * powf(fmaxf(sd, 0.0f), 4.0f);
+    const float band = wpow(1.0f - up, 3.0f);
+    const float toward = 0.35f + 0.65f * wpow(fmaxf(sd, 0.0f), 4.0f);
     c = c + scatter_tint() * (band * toward * f.haze_warm * day * 0.22f);
   }
   if (look && f.zenith_deep > 0.0f) {
-    const float z = powf(up, 0.55f);
+    const float z = wpow(up, 0.55f);
     c = c * mix3(f3(1.0f, 1.0f, 1.0f), f3(0.80f, 0.90f, 1.16f), f.zenith_deep * z * day);
   }
   return mix3(c, horizon * 0.26f, smoothstep(0.0f, -0.35f, rd.y));
@@ -141,19 +158,19 @@ static __device__ __noinline__ float cloud_fbm(float px, float py, float fp) {
     amp *= 0.5f;
   }
   if (norm <= 0.0f) return 0.5f;
-  return sum / norm;
+  return wdiv(sum, norm);
 }
 
 __device__ __forceinline__ float cloud_shade(const vm_frame& f, F3 p, float fp) {
   if (f.cloud_shadow <= 0.0f || f.cloud_cover <= 0.0f) return 1.0f;
   const float dy = f.cloud_height - p.y;
   if (dy * f.sun_dir[1] <= 0.0f) return 1.0f;
-  const float t = dy / f.sun_dir[1];
+  const float t = wdiv(dy, f.sun_dir[1]);
   if (t > CLOUD_MAX) return 1.0f;
   const float qx = p.x + f.sun_dir[0] * t, qz = p.z + f.sun_dir[2] * t;
   const float drift = f.time * f.cloud_speed;
-  const float n = cloud_fbm((qx + 0.94f * drift) / f.cloud_scale, (qz + 0.34f * drift) / f.cloud_scale,
-                            fmaxf(fp, t * SUN_ANGLE) / f.cloud_scale);
+  const float n = cloud_fbm(wdiv(qx + 0.94f * drift, f.cloud_scale), wdiv(qz + 0.34f * drift, f.cloud_scale),
+                            wdiv(fmaxf(fp, t * SUN_ANGLE), f.cloud_scale));
   const float thr = 1.0f - f.cloud_cover;
   return 1.0f - smoothstep(thr, thr + CLOUD_SOFT, n) * f.cloud_shadow;
 }
@@ -176,19 +193,19 @@ static __device__ __noinline__ F3 sky_color(const vm_frame& f, const Look& L, F3
   if (f.cloud_cover <= 0.0f) return base;
   const float dy = f.cloud_height - ro.y;
   if (dy * rd.y <= 0.0f) return base;
-  const float t = dy / rd.y;
+  const float t = wdiv(dy, rd.y);
   if (t > CLOUD_MAX) return base;
   const float px = ro.x + rd.x * t, pz = ro.z + rd.z * t;
   const float px_angle = 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
-  const float fp = (travelled + t) * px_angle / (fabsf(rd.y) * f.cloud_scale);
+  const float fp = wdiv((travelled + t) * px_angle, fabsf(rd.y) * f.cloud_scale);
   const float drift = f.time * f.cloud_speed;
   const float qx = px + 0.94f * drift, qz = pz + 0.34f * drift;
-  const float n = cloud_fbm(qx / f.cloud_scale, qz / f.cloud_scale, fp);
+  const float n = cloud_fbm(wdiv(qx, f.cloud_scale), wdiv(qz, f.cloud_scale), fp);
   float thr = 1.0f - f.cloud_cover;
   const bool look = (L.spec_hi & HI_SKY_LOOK) != 0u;
   if (look && f.cloud_patch > 0.0f) {
     const float span = f.cloud_scale * CLOUD_PATCH_SPAN;
-    const float m = cloud_fbm(qx / span, qz / span, fp / CLOUD_PATCH_SPAN);
+    const float m = cloud_fbm(wdiv(qx, span), wdiv(qz, span), wdiv(fp, CLOUD_PATCH_SPAN));
     thr = clampf(thr + (m - 0.5f) * f.cloud_patch, 0.0f, 0.99f);
   }
   const float dens = smoothstep(thr, thr + CLOUD_SOFT, n);
@@ -197,9 +214,9 @@ static __device__ __noinline__ F3 sky_color(const vm_frame& f, const Look& L, F3
   if (look && f.cloud_relief > 0.0f) {
     const float ax0 = f.sun_dir[0] + 1.0e-3f, az0 = f.sun_dir[2];
     const float al = sqrtf(ax0 * ax0 + az0 * az0);
-    const float ax = ax0 / al, az = az0 / al;
-    const float step = (8.0f + f.sun_dir[1] * 48.0f) / f.cloud_scale;
-    const float ns = cloud_fbm(qx / f.cloud_scale + ax * step, qz / f.cloud_scale + az * step, fp);
+    const float ax = wdiv(ax0, al), az = wdiv(az0, al);
+    const float step = wdiv(8.0f + f.sun_dir[1] * 48.0f, f.cloud_scale);
+    const float ns = cloud_fbm(wdiv(qx, f.cloud_scale) + ax * step, wdiv(qz, f.cloud_scale) + az * step, fp);
     depth = clampf(depth + (ns - n) * (2.2f * f.cloud_relief), 0.0f, 1.0f);
   }
   const float reach = 1.0f - smoothstep(CLOUD_FADE, CLOUD_MAX, t);
@@ -216,8 +233,8 @@ __device__ __forceinline__ float shaft_at(const Look& L, uint32_t x, uint32_t y)
 
 static __device__ __noinline__ float terrain_shade(const vm_frame& f, const Look& L, F3 p) {
   if (L.shaft == nullptr) return 1.0f;
-  const float tx = (p.x - f.shaft_origin[0]) / f.shaft_texel - 0.5f;
-  const float tz = (p.z - f.shaft_origin[1]) / f.shaft_texel - 0.5f;
+  const float tx = wdiv(p.x - f.shaft_origin[0], f.shaft_texel) - 0.5f;
+  const float tz = wdiv(p.z - f.shaft_origin[1], f.shaft_texel) - 0.5f;
   const float hi = (float)VM_SHAFT_DIM - 1.0f;
   const float cx = clampf(tx, 0.0f, hi), cz = clampf(tz, 0.0f, hi);
   const float f0x = floorf(cx), f0z = floorf(cz);
@@ -250,28 +267,28 @@ static __device__ __noinline__ float sun_shaft(const vm_frame& f, const Look& L,
   const float opac = 1.0f - transmittance_from(f, ro.y, d, rd);
   if (opac <= 1e-6f) return 1.0f;
   const float lambda = f.fog_falloff;
-  const float rho0 = f.fog_density * expf(-clampf(lambda * (ro.y - f.fog_height), -60.0f, 60.0f));
+  const float rho0 = f.fog_density * wexp(-clampf(lambda * (ro.y - f.fog_height), -60.0f, 60.0f));
   const float k = lambda * rd.y;
   const float off = dither(f, px, py);
   const float px_angle = 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
   float sum = 0.0f;
   for (uint32_t i = 0; i < f.godray_steps; ++i) {
-    const float u = ((float)i + off) / (float)f.godray_steps;
-    const float path = -logf(1.0f - u * opac) / rho0;
+    const float u = wdiv((float)i + off, (float)f.godray_steps);
+    const float path = wdiv(-wlog(1.0f - u * opac), rho0);
     float s = path;
     const float kp = k * path;
-    if (fabsf(kp) > 1e-4f) s = -logf(fmaxf(1.0f - kp, 1e-6f)) / k;
+    if (fabsf(kp) > 1e-4f) s = wdiv(-wlog(fmaxf(1.0f - kp, 1e-6f)), k);
     s = clampf(s, 0.0f, d);
     const F3 p = ro + rd * s;
     float v = cloud_shade(f, p, s * px_angle);
     if (terrain) v = v * terrain_shade(f, L, p);
     sum += v;
   }
-  const float vis = sum / (float)f.godray_steps;
+  const float vis = wdiv(sum, (float)f.godray_steps);
   float covered = 1.0f;
   if (d < dist) {
     const float full = 1.0f - transmittance_from(f, ro.y, dist, rd);
-    if (full > 1e-6f) covered = fminf(opac / full, 1.0f);
+    if (full > 1e-6f) covered = fminf(wdiv(opac, full), 1.0f);
   }
   return fmaxf(mixf(1.0f, vis, imp * f.godray_strength * covered), 0.0f);
 }
@@ -390,17 +407,17 @@ __device__ __forceinline__ float light_block_level(uint32_t p) {
   return fmaxf(c.x, fmaxf(c.y, c.z));
 }
 __device__ __forceinline__ float light_curve(float level) {
-  const float l = level / 15.0f;
+  const float l = wdiv(level, 15.0f);
   return l * l * (0.6f + 0.4f * l);
 }
 __device__ __forceinline__ F3 light_curve3(F3 level) {
-  const F3 l = level / 15.0f;
+  const F3 l = wdiv3(level, 15.0f);
   return l * l * add_s(l * 0.4f, 0.6f);
 }
 __device__ __forceinline__ F3 block_ambient(F3 blk, float sk, F3 sky) {
   const float bk = fmaxf(blk.x, fmaxf(blk.y, blk.z));
-  const F3 tint = blk / fmaxf(bk, 1e-4f);
-  return mix3(sky, tint, bk / fmaxf(sk + bk, 1e-4f)) * fmaxf(sk, bk);
+  const F3 tint = wdiv3(blk, fmaxf(bk, 1e-4f));
+  return mix3(sky, tint, wdiv(bk, fmaxf(sk + bk, 1e-4f))) * fmaxf(sk, bk);
 }
 __device__ __forceinline__ F3 block_tint() { return {1.0000f, 0.6500f, 0.3200f}; }
 
@@ -416,9 +433,10 @@ __device__ __forceinline__ F3 sky_ambient_tint(const vm_frame& f, const Look& L,
   F3 c = mix3(horizon, zenith, wgt);
   c = c + scatter_tint() * (f.fog_scatter * day * 4.0f * fmaxf(dot(n, ld3(f.sun_dir)), 0.0f));
   const F3 ref = {0.14658824f, 0.30178431f, 0.84105882f};
-  const F3 t = sky_tint * f3(powf(c.x / ref.x, 2.5f), powf(c.y / ref.y, 2.5f), powf(c.z / ref.z, 2.5f));
+  const F3 t = sky_tint * f3(wpow(wdiv(c.x, ref.x), 2.5f), wpow(wdiv(c.y, ref.y), 2.5f),
+                             wpow(wdiv(c.z, ref.z), 2.5f));
   const float luma = 0.2126f * t.x + 0.7152f * t.y + 0.0722f * t.z;
-  return t * (0.70721556f / fmaxf(luma, 1e-6f));
+  return t * wdiv(0.70721556f, fmaxf(luma, 1e-6f));
 }
 __device__ __forceinline__ bool lighting_repair(const Look& L) { return (L.spec_hi & HI_LEGACY_LIGHTING) == 0u; }
 static __device__ __noinline__ F3 surface_sky_fill(const vm_frame& f, const Look& L, F3 n) {
