@@ -163,7 +163,7 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
     albedo = albedo * mix3(f3(1.0f, 1.0f, 1.0f), biome_tint(f, L, hit.x, hit.z), k);
   }
   if ((L.spec_hi & HI_SHORE_WET) != 0u && id == VM_SAND) {
-    const float wet = 1.0f - smoothstep(f.sea_level, f.sea_level + 1.5f, hit.y);
+    const float wet = 1.0f - wsmooth(f.sea_level, f.sea_level + 1.5f, hit.y);
     albedo = albedo * mixf(1.0f, 0.62f, wet);
   }
   if ((L.spec_hi & HI_FOLIAGE_RICH) != 0u && (foliage || ((id == VM_GRASS || id == VM_MEADOW) && nid == VM_NORMAL_PY))) {
@@ -402,9 +402,9 @@ static __device__ __noinline__ F3 water_compose(const vm_frame& f, const Look& L
     column_depth = leg_r.w;
   }
   if ((L.spec_hi & HI_SHORE_FOAM) != 0u && x.refract_detail > 0.0f && column_depth < 2.5f) {
-    const float shall = 1.0f - smoothstep(0.0f, 2.5f, column_depth);
+    const float shall = 1.0f - wsmooth(0.0f, 2.5f, column_depth);
     const float m = foam_mottle(x.hit.x, x.hit.z, f.time * f.wave_speed);
-    const float foam = shall * smoothstep(0.45f, 0.75f, m) * x.refract_detail;
+    const float foam = shall * wsmooth(0.45f, 0.75f, m) * x.refract_detail;
     refr = mix3(refr, f3(0.92f, 0.97f, 1.0f) * x.ml, clampf(foam, 0.0f, 1.0f) * 0.85f);
   }
   const F3 sun = ld3(f.sun_dir);

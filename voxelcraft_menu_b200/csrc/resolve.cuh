@@ -51,6 +51,12 @@ __device__ __forceinline__ F3 wdiv3(F3 a, float b) { return {wdiv(a.x, b), wdiv(
 __device__ __forceinline__ float wexp(float x) { return __expf(x); }
 __device__ __forceinline__ float wlog(float x) { return __logf(x); }
 __device__ __forceinline__ float wpow(float x, float y) { return __powf(x, y); }
+// smoothstep with WGSL's division (the march's smoothstep stays IEEE: its
+// results decide which legs are traced)
+__device__ __forceinline__ float wsmooth(float e0, float e1, float x) {
+  const float t = fminf(fmaxf(wdiv(x - e0, e1 - e0), 0.0f), 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
 
 constexpr uint32_t ATLAS_SIZE = VM_ATLAS_SIZE, ATLAS_MIPS = VM_ATLAS_MIPS;
 constexpr uint32_t PROBE_NX = VM_PROBE_NX, PROBE_NY = VM_PROBE_NY, PROBE_NZ = VM_PROBE_NZ;
@@ -107,7 +113,7 @@ static __device__ __noinline__ F3 sky_base(const vm_frame& f, const Look& L, F3 
   const F3 zenith = sky_zenith(L, day);
   F3 c = mix3(horizon, zenith, wpow(up, 0.55f));
   const float sd = dot(rd, ld3(f.sun_dir));
-  c = c + f3(1.0f, 0.8276f, 0.5225f) * smoothstep(0.9975f, 0.9990f, sd) * fmaxf(day, 0.2f);
+  c = c + f3(1.0f, 0.8276f, 0.5225f) * wsmooth(0.9975f, 0.9990f, sd) * fmaxf(day, 0.2f);
   c = c + scatter_lobe(f, rd) * shaft;
   const bool look = (L.spec_hi & HI_SKY_LOOK) != 0u;
   if (look && f.haze_warm > 0.0f) {
@@ -119,7 +125,7 @@ static __device__ __noinline__ F3 sky_base(const vm_frame& f, const Look& L, F3 
     const float z = wpow(up, 0.55f);
     c = c * mix3(f3(1.0f, 1.0f, 1.0f), f3(0.80f, 0.90f, 1.16f), f.zenith_deep * z * day);
   }
-  return mix3(c, horizon * 0.26f, smoothstep(0.0f, -0.35f, rd.y));
+  return mix3(c, horizon * 0.26f, wsmooth(0.0f, -0.35f, rd.y));
 }
 
 // ---------------------------------------------------------------------------
@@ -149,7 +155,7 @@ static __device__ __noinline__ float cloud_fbm(float px, float py, float fp) {
   float freq = 1.0f, amp = 1.0f, sum = 0.0f, norm = 0.0f;
 #pragma unroll 1
   for (int i = 0; i < 4; ++i) {
-    const float w = amp * (1.0f - smoothstep(0.25f, 0.5f, fp * freq));
+    const float w = amp * (1.0f - wsmooth(0.25f, 0.5f, fp * freq));
     if (w > 0.0f) {
       sum += w * cloud_noise(px * freq, py * freq);
       norm += w;
@@ -172,13 +178,13 @@ __device__ __forceinline__ float cloud_shade(const vm_frame& f, F3 p, float fp) 
   const float n = cloud_fbm(wdiv(qx + 0.94f * drift, f.cloud_scale), wdiv(qz + 0.34f * drift, f.cloud_scale),
                             wdiv(fmaxf(fp, t * SUN_ANGLE), f.cloud_scale));
   const float thr = 1.0f - f.cloud_cover;
-  return 1.0f - smoothstep(thr, thr + CLOUD_SOFT, n) * f.cloud_shadow;
+  return 1.0f - wsmooth(thr, thr + CLOUD_SOFT, n) * f.cloud_shadow;
 }
 
 __device__ __forceinline__ F3 cloud_radiance(const vm_frame& f, const Look& L, float dens, float depth, F3 rd) {
   const float day = f.daylight;
   const float thick = rd.y < 0.0f ? 0.0f : depth;
-  const float warm = 1.0f - smoothstep(0.02f, 0.30f, f.sun_dir[1]);
+  const float warm = 1.0f - wsmooth(0.02f, 0.30f, f.sun_dir[1]);
   const F3 sun_tint = mix3(f3(1.0f, 1.0f, 1.0f), scatter_tint(), warm * 0.72f);
   const bool cool = (L.spec_hi & HI_SKY_COOL) != 0u;
   const F3 lit = cool ? f3(1.0f, 1.0f, 1.0f) : f3(1.0000f, 0.9575f, 0.8963f);
@@ -208,9 +214,9 @@ static __device__ __noinline__ F3 sky_color(const vm_frame& f, const Look& L, F3
     const float m = cloud_fbm(wdiv(qx, span), wdiv(qz, span), wdiv(fp, CLOUD_PATCH_SPAN));
     thr = clampf(thr + (m - 0.5f) * f.cloud_patch, 0.0f, 0.99f);
   }
-  const float dens = smoothstep(thr, thr + CLOUD_SOFT, n);
+  const float dens = wsmooth(thr, thr + CLOUD_SOFT, n);
   if (dens <= 0.0f) return base;
-  float depth = smoothstep(thr, thr + CLOUD_DEEP, n);
+  float depth = wsmooth(thr, thr + CLOUD_DEEP, n);
   if (look && f.cloud_relief > 0.0f) {
     const float ax0 = f.sun_dir[0] + 1.0e-3f, az0 = f.sun_dir[2];
     const float al = sqrtf(ax0 * ax0 + az0 * az0);
@@ -219,7 +225,7 @@ static __device__ __noinline__ F3 sky_color(const vm_frame& f, const Look& L, F3
     const float ns = cloud_fbm(wdiv(qx, f.cloud_scale) + ax * step, wdiv(qz, f.cloud_scale) + az * step, fp);
     depth = clampf(depth + (ns - n) * (2.2f * f.cloud_relief), 0.0f, 1.0f);
   }
-  const float reach = 1.0f - smoothstep(CLOUD_FADE, CLOUD_MAX, t);
+  const float reach = 1.0f - wsmooth(CLOUD_FADE, CLOUD_MAX, t);
   const float a = dens * reach * transmittance_from(f, ro.y, t, rd);
   return mix3(base, cloud_radiance(f, L, dens, depth, rd), a);
 }
@@ -244,7 +250,7 @@ static __device__ __noinline__ float terrain_shade(const vm_frame& f, const Look
   const float a = shaft_at(L, i0x, i0z), b = shaft_at(L, i1x, i0z);
   const float c0 = shaft_at(L, i0x, i1z), d = shaft_at(L, i1x, i1z);
   const float e = mixf(mixf(a, b, frx), mixf(c0, d, frx), frz);
-  return smoothstep(e - f.shaft_soft, e + f.shaft_soft, p.y);
+  return wsmooth(e - f.shaft_soft, e + f.shaft_soft, p.y);
 }
 
 __device__ __forceinline__ float dither(const vm_frame& f, uint32_t px, uint32_t py) {
@@ -260,7 +266,7 @@ static __device__ __noinline__ float sun_shaft(const vm_frame& f, const Look& L,
   if (f.godray_strength <= 0.0f) return 1.0f;
   if (!deck && !terrain) return 1.0f;
   const F3 lobe = scatter_lobe(f, rd);
-  const float imp = smoothstep(0.0040f, 0.0120f, fmaxf(fmaxf(lobe.x, lobe.y), lobe.z) * alpha);
+  const float imp = wsmooth(0.0040f, 0.0120f, fmaxf(fmaxf(lobe.x, lobe.y), lobe.z) * alpha);
   if (imp <= 0.0f) return 1.0f;
   const float d = fminf(dist, f.godray_dist);
   if (d <= 0.0f) return 1.0f;
@@ -611,8 +617,8 @@ static __device__ __noinline__ float biome_noise(const Look& L, int32_t seed_i, 
   return (n0 + n1 + n2) * 99.83685446303647f;
 }
 __device__ __forceinline__ F3 biome_band_weights(float n) {
-  const float hot = smoothstep(0.22f - 0.18f, 0.22f + 0.18f, n);
-  const float cold = 1.0f - smoothstep(-0.22f - 0.18f, -0.22f + 0.18f, n);
+  const float hot = wsmooth(0.22f - 0.18f, 0.22f + 0.18f, n);
+  const float cold = 1.0f - wsmooth(-0.22f - 0.18f, -0.22f + 0.18f, n);
   return {cold, 1.0f - cold - hot, hot};
 }
 __device__ __forceinline__ F3 biome_tint(const vm_frame& f, const Look& L, float x, float z) {
