@@ -504,13 +504,17 @@ __device__ __forceinline__ float4 from_half4(ushort4 h) {
                      __half2float(__ushort_as_half(h.z)), __half2float(__ushort_as_half(h.w)));
 }
 
+// the resolve's lanes, as k_resolve's PART
+constexpr uint8_t LANE_OPAQUE = 0, LANE_SKY = 1, LANE_WATER = 2, LANE_GLASS = 3;
+
 // The colour pass of water_sec (resolve.wgsl:1468-1535): per (2^shift)^2
 // block the water pixel of least hit distance (first in x-major order on
 // ties), its water_ctx and both legs shaded, stored as the engine's
 // rgba16float targets (refract: colour and depth; reflect: colour, 1 if hit).
 __global__ void __launch_bounds__(128) k_water_legs(const __grid_constant__ vm_frame f, const __grid_constant__ DevWorld w,
                                                     const __grid_constant__ Look L,
-                                                    const unsigned long long* __restrict__ vis, uint32_t shift,
+                                                    const unsigned long long* __restrict__ vis,
+                                                    const uint8_t* __restrict__ lane, uint32_t shift,
                                                     ushort4* __restrict__ refr, ushort4* __restrict__ refl) {
   const uint32_t span = 1u << shift;
   const uint32_t hw = (f.res[0] + span - 1u) >> shift, hh = (f.res[1] + span - 1u) >> shift;
@@ -525,11 +529,10 @@ __global__ void __launch_bounds__(128) k_water_legs(const __grid_constant__ vm_f
     for (uint32_t j = 0; j < span; ++j) {
       const uint32_t pxs = span * hx + i, pys = span * hy + j;
       if (pxs >= f.res[0] || pys >= f.res[1]) continue;
-      const unsigned long long key = vis[(uint64_t)pys * f.res[0] + pxs];
-      if (key == 0ull) continue;
-      const KeyParts k = split_key(key);
+      const uint64_t pix = (uint64_t)pys * f.res[0] + pxs;
+      if (lane[pix] != LANE_WATER) continue;
+      const KeyParts k = split_key(vis[pix]);
       const Chunk c = ld_chunk(w, k.ci);
-      if (block_at(w, c, k.vx, k.vy, k.vz) != VM_WATER) continue;
       const F3 rd0 = ray_dir(f, (float)pxs + 0.5f, (float)pys + 0.5f);
       const float ts = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd0);
       if (ts < best_t) { best_t = ts; best = k; bpx = pxs; bpy = pys; has = true; }
@@ -590,7 +593,8 @@ template <bool OWN>
 __global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant__ vm_frame f,
                                                           const __grid_constant__ DevWorld w,
                                                           const __grid_constant__ Look L,
-                                                          const unsigned long long* __restrict__ vis, WaterSec ws,
+                                                          const unsigned long long* __restrict__ vis,
+                                                          const uint8_t* __restrict__ lane, WaterSec ws,
                                                           float4* __restrict__ out) {
   __shared__ float s_hy[4][32], s_t[4][32];
   __shared__ uint8_t s_code[4][32];   // bit 0 in the frame, 1 a key, 2 water, bits 3-5 the normal
@@ -603,8 +607,13 @@ __global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant_
   uint32_t code = 0u, ci = 0u, vx = 0u, vy = 0u, vz = 0u, nid = 0u;
   if (inside) {
     code = 1u;
-    const unsigned long long key = vis[(uint64_t)py * f.res[0] + px];
-    if (key != 0ull) {
+    const uint64_t pix = (uint64_t)py * f.res[0] + px;
+    const uint32_t ln = lane[pix];
+    // a pixel of another lane with a key makes its block unsafe whatever its
+    // normal, distance or height: only water pixels are decoded
+    if (ln != LANE_SKY) code |= 2u;
+    if (ln == LANE_WATER) {
+      const unsigned long long key = vis[pix];
       rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
       nid = (uint32_t)(key >> 37) & 7u;
       ci = (uint32_t)(key >> 24) & 0x1FFFu;
@@ -614,8 +623,7 @@ __global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant_
       const Chunk c = ld_chunk(w, ci);
       t = hit_t(f, c, vx, vy, vz, mx, my, mz, nid, rd);
       hit = cam + rd * t;
-      code |= 2u | (nid << 3);
-      if (block_at(w, c, vx, vy, vz) == VM_WATER) code |= 4u;
+      code |= 4u | (nid << 3);
     }
   }
   s_hy[ty][tx] = hit.y;
@@ -652,6 +660,26 @@ __global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant_
   out[(uint64_t)py * f.res[0] + px] = make_float4(color.x, color.y, color.z, 1.0f);
 }
 
+// The lane of every pixel: the engine's resolve picks a pixel's shading by
+// its hit's block (resolve.wgsl:1378-1466).  Decided once per pixel, a byte
+// each, so that every lane's kernel passes over the other lanes' pixels with
+// one byte load instead of a chunk record load and a tree walk.
+__global__ void __launch_bounds__(256) k_resolve_lanes(const __grid_constant__ vm_frame f,
+                                                       const __grid_constant__ DevWorld w,
+                                                       const unsigned long long* __restrict__ vis,
+                                                       uint8_t* __restrict__ lane) {
+  const uint64_t pix = (uint64_t)blockIdx.x * 256u + threadIdx.x;
+  if (pix >= (uint64_t)f.res[0] * f.res[1]) return;
+  const unsigned long long key = vis[pix];
+  uint8_t ln = LANE_SKY;
+  if (key != 0ull) {
+    const KeyParts k = split_key(key);
+    const uint32_t id = block_at(w, ld_chunk(w, k.ci), k.vx, k.vy, k.vz);
+    ln = id == VM_WATER ? LANE_WATER : ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS ? LANE_GLASS : LANE_OPAQUE);
+  }
+  lane[pix] = ln;
+}
+
 // The light terms of every opaque-surface pixel, ahead of k_resolve<0>: the
 // 3x3 light and AO gather (tree walks, light bricks, the neighbour chunks)
 // in a kernel of its own, so that the shading kernel's code stays small.
@@ -661,20 +689,19 @@ __global__ void __launch_bounds__(128, 8) k_resolve_light(const __grid_constant_
                                                           const __grid_constant__ DevWorld w,
                                                           const __grid_constant__ Look L,
                                                           const unsigned long long* __restrict__ vis,
+                                                          const uint8_t* __restrict__ lane,
                                                           float4* __restrict__ out, float* __restrict__ light_ao) {
   const uint32_t px = blockIdx.x * 32u + threadIdx.x, py = blockIdx.y * 4u + threadIdx.y;
   if (px >= f.res[0] || py >= f.res[1]) return;
   const uint64_t pix = (uint64_t)py * f.res[0] + px;
+  if (lane[pix] != LANE_OPAQUE) return;
   const unsigned long long key = vis[pix];
-  if (key == 0ull) return;
   const uint32_t nid = (uint32_t)(key >> 37) & 7u;
   const uint32_t ci = (uint32_t)(key >> 24) & 0x1FFFu;
   const uint32_t low = (uint32_t)(key & 0xFFFFFFull);
   const uint32_t vx = (low >> 16) & 63u, vy = (low >> 8) & 63u, vz = low & 63u;
   const uint32_t mx = (low >> 22) & 3u, my = (low >> 14) & 3u, mz = (low >> 6) & 3u;
   const Chunk c = ld_chunk(w, ci);
-  const uint32_t id = block_at(w, c, vx, vy, vz);
-  if (id == VM_WATER || ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS)) return;
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   const float t = hit_t(f, c, vx, vy, vz, mx, my, mz, nid, rd);
   const F3 hit = ld3(f.cam_pos) + rd * t;
@@ -694,13 +721,13 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
                                                     const __grid_constant__ Look L,
                                                     const unsigned long long* __restrict__ vis,
                                                     const float* __restrict__ mask, const float* __restrict__ dist,
-                                                    bool soft, WaterSec ws, const float* __restrict__ light_ao,
-                                                    float4* __restrict__ out) {
+                                                    const uint8_t* __restrict__ lane, bool soft, WaterSec ws,
+                                                    const float* __restrict__ light_ao, float4* __restrict__ out) {
   const uint32_t px = blockIdx.x * 32u + threadIdx.x, py = blockIdx.y * 4u + threadIdx.y;
   if (px >= f.res[0] || py >= f.res[1]) return;
   const uint64_t pix = (uint64_t)py * f.res[0] + px;
+  if (lane[pix] != (uint8_t)PART) return;
   const unsigned long long key = vis[pix];
-  if ((key == 0ull) != (PART == 1)) return;
   const F3 cam = ld3(f.cam_pos);
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   F3 color;
@@ -716,10 +743,8 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
     const Chunk c = ld_chunk(w, ci);
     const float t = hit_t(f, c, vx, vy, vz, mx, my, mz, nid, rd);
     const F3 hit = cam + rd * t;
-    const uint32_t id = block_at(w, c, vx, vy, vz);
-    const int part = id == VM_WATER ? 2 : ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS ? 3 : 0);
-    if (part != PART) return;
     if (PART == 0) {
+      const uint32_t id = block_at(w, c, vx, vy, vz);
       LightTerms lt;
       if (light_ao != nullptr) {
         const float4 a = out[pix];
@@ -749,35 +774,38 @@ __global__ void __launch_bounds__(128, 8) k_resolve(const __grid_constant__ vm_f
 
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
-                           uint16_t* leg_refr, uint16_t* leg_refl, float* light_ao, float4* out, cudaStream_t s,
-                           const cudaStream_t lane_stream[3], const cudaEvent_t lane_event[4]) {
+                           uint16_t* leg_refr, uint16_t* leg_refl, uint8_t* lane, float* light_ao, float4* out,
+                           cudaStream_t s, const cudaStream_t lane_stream[3], const cudaEvent_t lane_event[4]) {
   // The lanes write disjoint pixels.  The water lane (its legs, then the
   // pixels) and the glass lane cover a few clustered pixels with long serial
   // traces, which leave most SMs idle: they run on streams of their own,
   // forked from s and joined back into it, beside the sky / opaque lanes.
+  const uint64_t npix = (uint64_t)f.res[0] * f.res[1];
+  k_resolve_lanes<<<(unsigned)((npix + 255u) / 256u), 256, 0, s>>>(f, w, vis, lane);
   cudaError_t e = cudaEventRecord(lane_event[0], s);
   for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(lane_stream[i], lane_event[0], 0);
   if (e != cudaSuccess) return e;
   const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
   const bool split_water = leg_refr != nullptr && water_sec_shift == 1u;
   if (split_water && (w.spec & VM_SPEC_WATER_REPAIR) != 0u)
-    k_resolve_water<true><<<grid, block, 0, lane_stream[2]>>>(f, w, L, vis, WaterSec{nullptr, nullptr, 1u, 0u}, out);
-  k_resolve<3><<<grid, block, 0, lane_stream[1]>>>(f, w, L, vis, mask, dist, soft_rays, WaterSec{nullptr, nullptr, 0u, 0u},
-                                                   nullptr, out);
+    k_resolve_water<true><<<grid, block, 0, lane_stream[2]>>>(f, w, L, vis, lane, WaterSec{nullptr, nullptr, 1u, 0u},
+                                                              out);
+  k_resolve<3><<<grid, block, 0, lane_stream[1]>>>(f, w, L, vis, mask, dist, lane, soft_rays,
+                                                   WaterSec{nullptr, nullptr, 0u, 0u}, nullptr, out);
   WaterSec ws{nullptr, nullptr, water_sec_shift, 0u};
   const cudaStream_t sw = lane_stream[0];
   if (leg_refr != nullptr) {
     const uint32_t span = 1u << water_sec_shift;
     const uint32_t hw = (f.res[0] + span - 1u) >> water_sec_shift, hh = (f.res[1] + span - 1u) >> water_sec_shift;
     k_water_legs<<<dim3((hw + 15) / 16, (hh + 7) / 8), dim3(16, 8), 0, sw>>>(
-        f, w, L, vis, water_sec_shift, (ushort4*)leg_refr, (ushort4*)leg_refl);
+        f, w, L, vis, lane, water_sec_shift, (ushort4*)leg_refr, (ushort4*)leg_refl);
     ws = {(const ushort4*)leg_refr, (const ushort4*)leg_refl, water_sec_shift, hw};
   }
-  if (split_water) k_resolve_water<false><<<grid, block, 0, sw>>>(f, w, L, vis, ws, out);
-  else k_resolve<2><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
-  if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, out, light_ao);
-  k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, light_ao, out);
-  k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, soft_rays, ws, nullptr, out);
+  if (split_water) k_resolve_water<false><<<grid, block, 0, sw>>>(f, w, L, vis, lane, ws, out);
+  else k_resolve<2><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
+  if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, lane, out, light_ao);
+  k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, light_ao, out);
+  k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
   e = cudaGetLastError();
   for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
     e = cudaEventRecord(lane_event[1 + i], lane_stream[i]);
