@@ -505,7 +505,7 @@ __device__ __forceinline__ float4 from_half4(ushort4 h) {
 }
 
 // the resolve's lanes, as k_resolve's PART
-constexpr uint8_t LANE_OPAQUE = 0, LANE_SKY = 1, LANE_WATER = 2, LANE_GLASS = 3;
+constexpr uint8_t LANE_OPAQUE = 0, LANE_SKY = 1, LANE_WATER = 2, LANE_GLASS = 3, LANE_WATER_OWN = 4;
 
 // The colour pass of water_sec (resolve.wgsl:1468-1535): per (2^shift)^2
 // block the water pixel of least hit distance (first in x-major order on
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(128) k_water_legs(const __grid_constant__ vm_f
       const uint32_t pxs = span * hx + i, pys = span * hy + j;
       if (pxs >= f.res[0] || pys >= f.res[1]) continue;
       const uint64_t pix = (uint64_t)pys * f.res[0] + pxs;
-      if (lane[pix] != LANE_WATER) continue;
+      if (lane[pix] != LANE_WATER && lane[pix] != LANE_WATER_OWN) continue;
       const KeyParts k = split_key(vis[pix]);
       const Chunk c = ld_chunk(w, k.ci);
       const F3 rd0 = ray_dir(f, (float)pxs + 0.5f, (float)pys + 0.5f);
@@ -576,108 +576,118 @@ __device__ __noinline__ bool water_share_safe(const vm_frame& f, const DevWorld&
   return true;
 }
 
-struct WaterSec { const ushort4* refr; const ushort4* refl; uint32_t shift, hw; };
+// the water_sec targets; decided: k_resolve_lanes sent the pixels of unsafe
+// blocks to LANE_WATER_OWN, so every LANE_WATER pixel composes its block's legs
+struct WaterSec { const ushort4* refr; const ushort4* refl; uint32_t shift, hw; bool decided; };
 
-// The water pixels (lane 2 with SPEC_WATER_SEC and WATER_SEC_SHIFT 1).
-// water_share_safe compares a pixel with the three others of its 2x2 block;
-// the block lies in one 32x4 thread block, so each thread decodes its own
-// pixel once (hit distance, hit height, normal, water or not) into shared
-// memory and the comparisons read it there: the same values the per-pixel
-// test recomputes, with a quarter of the chunk and tree loads.
-// OWN = false: the pixels that compose the block's shared legs (run after
-// k_water_legs); OWN = true: the pixels that water_share_safe sends to their
-// own legs under SPEC_WATER_REPAIR (independent of k_water_legs, so they
-// start with the other lanes: their two legs per pixel are the lane's
-// longest threads).
-template <bool OWN>
-__global__ void __launch_bounds__(128, 8) k_resolve_water(const __grid_constant__ vm_frame f,
-                                                          const __grid_constant__ DevWorld w,
-                                                          const __grid_constant__ Look L,
-                                                          const unsigned long long* __restrict__ vis,
-                                                          const uint8_t* __restrict__ lane, WaterSec ws,
-                                                          float4* __restrict__ out) {
-  __shared__ float s_hy[4][32], s_t[4][32];
-  __shared__ uint8_t s_code[4][32];   // bit 0 in the frame, 1 a key, 2 water, bits 3-5 the normal
-  const uint32_t tx = threadIdx.x, ty = threadIdx.y;
-  const uint32_t px = blockIdx.x * 32u + tx, py = blockIdx.y * 4u + ty;
-  const bool inside = px < f.res[0] && py < f.res[1];
-  const F3 cam = ld3(f.cam_pos);
-  F3 rd = {0.0f, 0.0f, 1.0f}, hit = {0.0f, 0.0f, 0.0f};
-  float t = 0.0f;
-  uint32_t code = 0u, ci = 0u, vx = 0u, vy = 0u, vz = 0u, nid = 0u;
-  if (inside) {
-    code = 1u;
-    const uint64_t pix = (uint64_t)py * f.res[0] + px;
-    const uint32_t ln = lane[pix];
-    // a pixel of another lane with a key makes its block unsafe whatever its
-    // normal, distance or height: only water pixels are decoded
-    if (ln != LANE_SKY) code |= 2u;
-    if (ln == LANE_WATER) {
-      const unsigned long long key = vis[pix];
-      rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
-      nid = (uint32_t)(key >> 37) & 7u;
-      ci = (uint32_t)(key >> 24) & 0x1FFFu;
-      const uint32_t low = (uint32_t)(key & 0xFFFFFFull);
-      vx = (low >> 16) & 63u; vy = (low >> 8) & 63u; vz = low & 63u;
-      const uint32_t mx = (low >> 22) & 3u, my = (low >> 14) & 3u, mz = (low >> 6) & 3u;
-      const Chunk c = ld_chunk(w, ci);
-      t = hit_t(f, c, vx, vy, vz, mx, my, mz, nid, rd);
-      hit = cam + rd * t;
-      code |= 4u | (nid << 3);
-    }
-  }
-  s_hy[ty][tx] = hit.y;
-  s_t[ty][tx] = t;
-  s_code[ty][tx] = (uint8_t)code;
-  __syncthreads();
-  if ((code & 4u) == 0u) return;
-  // water_share_safe: resolve.wgsl:1223-1245
-  bool safe = nid == VM_NORMAL_PY;
-  const uint32_t bx = tx & ~1u, by = ty & ~1u;
-  for (uint32_t y = 0; y < 2u && safe; ++y)
-    for (uint32_t x = 0; x < 2u && safe; ++x) {
-      const uint32_t q = s_code[by + y][bx + x];
-      if ((q & 1u) == 0u) continue;
-      if ((q & 2u) == 0u || ((q >> 3) & 7u) != nid || (q & 4u) == 0u) { safe = false; break; }
-      if (fabsf(s_hy[by + y][bx + x] - hit.y) > 0.01f ||
-          fabsf(s_t[by + y][bx + x] - t) > fmaxf(0.1f, fminf(1.0f, t * 0.02f)))
-        safe = false;
-    }
-  const bool shared = safe || (w.spec & VM_SPEC_WATER_REPAIR) == 0u;
-  if (shared == OWN) return;
-  F3 color;
-  if (!OWN) {
-    // shade_water_sec (resolve.wgsl:1247-1259): the block's legs
-    const WaterCtx x = water_ctx(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
-    const uint64_t h = (uint64_t)(py >> 1) * ws.hw + (px >> 1);
-    color = water_compose(f, L, x, from_half4(ws.refr[h]), from_half4(ws.refl[h]));
-  } else {
-    color = shade_water(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
-  }
-  const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
-  const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
-  color = mix3(color, sky_base(f, L, rd, shaft), alpha);
-  out[(uint64_t)py * f.res[0] + px] = make_float4(color.x, color.y, color.z, 1.0f);
+// A warp's pixels of one kind appended to a compact list (one atomic per
+// warp; the lanes of a 32-wide row stay together in the list).
+__device__ __forceinline__ void append_pixel(bool mine, uint32_t* list, uint32_t* count, uint32_t pix) {
+  const uint32_t bal = __ballot_sync(FULLMASK, mine);
+  if (bal == 0u) return;
+  uint32_t base = 0u;
+  if ((threadIdx.x & 31u) == 0u) base = atomicAdd(count, (uint32_t)__popc(bal));
+  base = __shfl_sync(FULLMASK, base, 0);
+  if (mine) list[base + (uint32_t)__popc(bal & lanemask_lt())] = pix;
 }
 
 // The lane of every pixel: the engine's resolve picks a pixel's shading by
 // its hit's block (resolve.wgsl:1378-1466).  Decided once per pixel, a byte
 // each, so that every lane's kernel passes over the other lanes' pixels with
-// one byte load instead of a chunk record load and a tree walk.
-__global__ void __launch_bounds__(256) k_resolve_lanes(const __grid_constant__ vm_frame f,
+// one byte load instead of a chunk record load and a tree walk.  With the
+// half-resolution legs under SPEC_WATER_REPAIR (DECIDE), water_share_safe
+// (resolve.wgsl:1223-1245) is decided here as well: a 32x4 tile holds whole
+// 2x2 blocks, so each thread decodes its own pixel (hit distance, hit
+// height, normal, water or not) into shared memory and the test reads its
+// block there; water pixels of unsafe blocks take LANE_WATER_OWN.  The glass
+// pixels and those, few and clustered, each tracing long legs, also go to
+// compact lists, so that their kernels run full warps over them instead of
+// the frame's grid with a few live lanes per warp.
+template <bool DECIDE>
+__global__ void __launch_bounds__(128) k_resolve_lanes(const __grid_constant__ vm_frame f,
                                                        const __grid_constant__ DevWorld w,
                                                        const unsigned long long* __restrict__ vis,
-                                                       uint8_t* __restrict__ lane) {
-  const uint64_t pix = (uint64_t)blockIdx.x * 256u + threadIdx.x;
-  if (pix >= (uint64_t)f.res[0] * f.res[1]) return;
-  const unsigned long long key = vis[pix];
-  uint8_t ln = LANE_SKY;
-  if (key != 0ull) {
-    const KeyParts k = split_key(key);
-    const uint32_t id = block_at(w, ld_chunk(w, k.ci), k.vx, k.vy, k.vz);
-    ln = id == VM_WATER ? LANE_WATER : ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS ? LANE_GLASS : LANE_OPAQUE);
+                                                       uint8_t* __restrict__ lane, uint32_t* __restrict__ glass_list,
+                                                       uint32_t* __restrict__ own_list, uint32_t* __restrict__ counts) {
+  __shared__ float s_hy[4][32], s_t[4][32];
+  __shared__ uint8_t s_code[4][32];   // bit 0 in the frame, 1 a key, 2 water, bits 3-5 the normal
+  const uint32_t tx = threadIdx.x, ty = threadIdx.y;
+  const uint32_t px = blockIdx.x * 32u + tx, py = blockIdx.y * 4u + ty;
+  const bool inside = px < f.res[0] && py < f.res[1];
+  const uint32_t pix = inside ? py * f.res[0] + px : 0u;
+  uint32_t ln = LANE_SKY, code = 0u, nid = 0u;
+  float hy = 0.0f, t = 0.0f;
+  if (inside) {
+    code = 1u;
+    const unsigned long long key = vis[pix];
+    if (key != 0ull) {
+      const KeyParts k = split_key(key);
+      const Chunk c = ld_chunk(w, k.ci);
+      const uint32_t id = block_at(w, c, k.vx, k.vy, k.vz);
+      ln = id == VM_WATER ? LANE_WATER : ((w.spec & VM_SPEC_GLASS) != 0u && id == VM_GLASS ? LANE_GLASS : LANE_OPAQUE);
+      code |= 2u;
+      if (DECIDE && ln == LANE_WATER) {
+        const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+        t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+        hy = (ld3(f.cam_pos) + rd * t).y;
+        nid = k.nid;
+        code |= 4u | (nid << 3);
+      }
+    }
   }
-  lane[pix] = ln;
+  if (DECIDE) {
+    s_hy[ty][tx] = hy;
+    s_t[ty][tx] = t;
+    s_code[ty][tx] = (uint8_t)code;
+    __syncthreads();
+    if (ln == LANE_WATER) {
+      bool safe = nid == VM_NORMAL_PY;
+      const uint32_t bx = tx & ~1u, by = ty & ~1u;
+      for (uint32_t y = 0; y < 2u && safe; ++y)
+        for (uint32_t x = 0; x < 2u && safe; ++x) {
+          const uint32_t q = s_code[by + y][bx + x];
+          if ((q & 1u) == 0u) continue;
+          if ((q & 2u) == 0u || ((q >> 3) & 7u) != nid || (q & 4u) == 0u) { safe = false; break; }
+          if (fabsf(s_hy[by + y][bx + x] - hy) > 0.01f ||
+              fabsf(s_t[by + y][bx + x] - t) > fmaxf(0.1f, fminf(1.0f, t * 0.02f)))
+            safe = false;
+        }
+      if (!safe) ln = LANE_WATER_OWN;
+    }
+  }
+  append_pixel(ln == LANE_GLASS, glass_list, counts, pix);
+  append_pixel(ln == LANE_WATER_OWN, own_list, counts + 1, pix);
+  if (inside) lane[pix] = (uint8_t)ln;
+}
+
+// The pixels of a compact list: glass (WHICH 0, shade_glass,
+// resolve.wgsl:1261-1319) or water with its own legs (WHICH 1, shade_water),
+// then the fog blend; a thread per pixel over a grid of resident blocks.
+template <int WHICH>
+__global__ void __launch_bounds__(128, 8) k_resolve_list(const __grid_constant__ vm_frame f,
+                                                         const __grid_constant__ DevWorld w,
+                                                         const __grid_constant__ Look L,
+                                                         const unsigned long long* __restrict__ vis,
+                                                         const uint32_t* __restrict__ list,
+                                                         const uint32_t* __restrict__ count,
+                                                         float4* __restrict__ out) {
+  const uint32_t n = *count;
+  const F3 cam = ld3(f.cam_pos);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t pix = list[i];
+    const uint32_t px = pix % f.res[0], py = pix / f.res[0];
+    const KeyParts k = split_key(vis[pix]);
+    const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+    const Chunk c = ld_chunk(w, k.ci);
+    const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+    const F3 hit = cam + rd * t;
+    F3 color = WHICH == 0 ? shade_glass(w, f, L, k.ci, k.vx, k.vy, k.vz, k.nid, hit, rd, t)
+                          : shade_water(w, f, L, k.ci, k.vx, k.vy, k.vz, k.nid, hit, rd, t);
+    const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
+    const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
+    color = mix3(color, sky_base(f, L, rd, shaft), alpha);
+    out[pix] = make_float4(color.x, color.y, color.z, 1.0f);
+  }
 }
 
 // The light terms of every opaque-surface pixel, ahead of k_resolve<0>: the
@@ -712,9 +722,10 @@ __global__ void __launch_bounds__(128, 12) k_resolve_light(const __grid_constant
   light_ao[pix] = lt.ao;
 }
 
-// PART 0: the opaque surfaces, 1: the sky, 2: water, 3: glass.  Four
-// launches over the frame instead of one kernel with every path: each
-// kernel carries a part of the code (one kernel stalled on instruction
+// PART 0: the opaque surfaces, 1: the sky, 2: water (the glass pixels and the
+// water pixels with their own legs run from compact lists, k_resolve_list).
+// A launch per lane over the frame instead of one kernel with every path:
+// each kernel carries a part of the code (one kernel stalled on instruction
 // fetch) and its warps run one path.
 // 12 blocks of 4 warps per SM (40 registers, a few bytes spilled): more
 // warps hide the L2 gathers of the issue-bound lanes (8 blocks: 2% slower).
@@ -755,8 +766,8 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
       color = shade_surface(w, f, L, ci, vx, vy, vz, id, nid, hit, rd, t, f.shadow_dist, true, true,
                             sun_visibility(mask, dist, soft, pix), light_ao != nullptr ? &lt : nullptr);
     } else if (PART == 2) {
-      if (ws.refr != nullptr &&
-          !((w.spec & VM_SPEC_WATER_REPAIR) != 0u && !water_share_safe(f, w, vis, ws.shift, px, py, nid, hit, t))) {
+      if (ws.refr != nullptr && (ws.decided || (w.spec & VM_SPEC_WATER_REPAIR) == 0u ||
+                                 water_share_safe(f, w, vis, ws.shift, px, py, nid, hit, t))) {
         // shade_water_sec (resolve.wgsl:1247-1259): the block's legs
         const WaterCtx x = water_ctx(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
         const uint64_t h = (uint64_t)(py >> ws.shift) * ws.hw + (px >> ws.shift);
@@ -764,8 +775,6 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
       } else {
         color = shade_water(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
       }
-    } else {
-      color = shade_glass(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
     }
     const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
     const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
@@ -776,35 +785,41 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
 
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
-                           uint16_t* leg_refr, uint16_t* leg_refl, uint8_t* lane, float* light_ao, float4* out,
-                           cudaStream_t s, const cudaStream_t lane_stream[3], const cudaEvent_t lane_event[4]) {
+                           uint16_t* leg_refr, uint16_t* leg_refl, uint8_t* lane, uint32_t* lists, float* light_ao,
+                           float4* out, int sms, cudaStream_t s, const cudaStream_t lane_stream[3],
+                           const cudaEvent_t lane_event[4]) {
   // The lanes write disjoint pixels.  The water lane (its legs, then the
   // pixels) and the glass lane cover a few clustered pixels with long serial
   // traces, which leave most SMs idle: they run on streams of their own,
   // forked from s and joined back into it, beside the sky / opaque lanes.
-  const uint64_t npix = (uint64_t)f.res[0] * f.res[1];
-  k_resolve_lanes<<<(unsigned)((npix + 255u) / 256u), 256, 0, s>>>(f, w, vis, lane);
-  cudaError_t e = cudaEventRecord(lane_event[0], s);
-  for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(lane_stream[i], lane_event[0], 0);
-  if (e != cudaSuccess) return e;
+  const uint32_t npix = f.res[0] * f.res[1];
+  uint32_t* glass_list = lists;
+  uint32_t* own_list = lists + npix;
+  uint32_t* counts = lists + 2u * (uint64_t)npix;
   const dim3 block(32, 4), grid((f.res[0] + 31u) / 32u, (f.res[1] + 3u) / 4u);
   const bool split_water = leg_refr != nullptr && water_sec_shift == 1u;
-  if (split_water && (w.spec & VM_SPEC_WATER_REPAIR) != 0u)
-    k_resolve_water<true><<<grid, block, 0, lane_stream[2]>>>(f, w, L, vis, lane, WaterSec{nullptr, nullptr, 1u, 0u},
-                                                              out);
-  k_resolve<3><<<grid, block, 0, lane_stream[1]>>>(f, w, L, vis, mask, dist, lane, soft_rays,
-                                                   WaterSec{nullptr, nullptr, 0u, 0u}, nullptr, out);
-  WaterSec ws{nullptr, nullptr, water_sec_shift, 0u};
+  const bool decide = split_water && (w.spec & VM_SPEC_WATER_REPAIR) != 0u;
+  cudaError_t e = cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), s);
+  if (e != cudaSuccess) return e;
+  if (decide) k_resolve_lanes<true><<<grid, block, 0, s>>>(f, w, vis, lane, glass_list, own_list, counts);
+  else k_resolve_lanes<false><<<grid, block, 0, s>>>(f, w, vis, lane, glass_list, own_list, counts);
+  if ((e = cudaEventRecord(lane_event[0], s)) != cudaSuccess) return e;
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(lane_stream[i], lane_event[0], 0);
+  if (e != cudaSuccess) return e;
+  const unsigned resident = (unsigned)max(sms, 1) * 8u;
+  if (decide) k_resolve_list<1><<<resident, 128, 0, lane_stream[2]>>>(f, w, L, vis, own_list, counts + 1, out);
+  if ((w.spec & VM_SPEC_GLASS) != 0u)
+    k_resolve_list<0><<<resident, 128, 0, lane_stream[1]>>>(f, w, L, vis, glass_list, counts, out);
+  WaterSec ws{nullptr, nullptr, water_sec_shift, 0u, decide};
   const cudaStream_t sw = lane_stream[0];
   if (leg_refr != nullptr) {
     const uint32_t span = 1u << water_sec_shift;
     const uint32_t hw = (f.res[0] + span - 1u) >> water_sec_shift, hh = (f.res[1] + span - 1u) >> water_sec_shift;
     k_water_legs<<<dim3((hw + 15) / 16, (hh + 7) / 8), dim3(16, 8), 0, sw>>>(
         f, w, L, vis, lane, water_sec_shift, (ushort4*)leg_refr, (ushort4*)leg_refl);
-    ws = {(const ushort4*)leg_refr, (const ushort4*)leg_refl, water_sec_shift, hw};
+    ws = {(const ushort4*)leg_refr, (const ushort4*)leg_refl, water_sec_shift, hw, decide};
   }
-  if (split_water) k_resolve_water<false><<<grid, block, 0, sw>>>(f, w, L, vis, lane, ws, out);
-  else k_resolve<2><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
+  k_resolve<2><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
   if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, lane, out, light_ao);
   k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, light_ao, out);
   k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
