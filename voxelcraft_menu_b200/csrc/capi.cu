@@ -45,7 +45,7 @@ struct vm_ctx {
   DevBuf shadow_mask;   // vm_soften_shadows output, sized on first use
   bool mask_valid = false;   // the mask belongs to the last rendered frame
   // the resolve's material inputs and output (vm_upload_atlas ... vm_resolve)
-  DevBuf atlas, faces, probes, shaft, grad, color, leg_refr, leg_refl, light_ao, lane, lane_lists;
+  DevBuf atlas, faces, probes, shaft, grad, color, leg_refr, leg_refl, light_ao, lane, lane_lists, fog;
   uint32_t atlas_layers = 0, n_faces = 0;
   DevBuf atlas_alpha;          // the atlas's alpha channel for the tuft quads of the march
   uint32_t tuft_layer[3] = {0, 0, 0};
@@ -341,7 +341,7 @@ void vm_destroy(vm_ctx* ctx) {
                    &ctx->shadow16, &ctx->ws_refr_key, &ctx->ws_refr_t, &ctx->ws_refl_key, &ctx->ws_refl_t,
                    &ctx->atlas, &ctx->faces, &ctx->probes, &ctx->shaft, &ctx->grad, &ctx->color,
                    &ctx->atlas_alpha, &ctx->leg_refr, &ctx->leg_refl, &ctx->light_ao, &ctx->lane,
-                   &ctx->lane_lists};
+                   &ctx->lane_lists, &ctx->fog};
   for (DevBuf* b : all) release(*b);
   if (ctx->rendered) cudaEventDestroy(ctx->rendered);
   for (cudaEvent_t e : ctx->lane_event)
@@ -1107,7 +1107,8 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
                 "are not built", spec_hi & HI_UNBUILT);
   CK(cudaSetDevice(ctx->device));
   if ((rc = ensure(ctx, ctx->color, npix * 16)) || (rc = ensure(ctx, ctx->light_ao, npix * 4)) ||
-      (rc = ensure(ctx, ctx->lane, npix)) || (rc = ensure(ctx, ctx->lane_lists, npix * 8 + 8)))
+      (rc = ensure(ctx, ctx->lane, npix)) || (rc = ensure(ctx, ctx->lane_lists, npix * 8 + 8)) ||
+      (rc = ensure(ctx, ctx->fog, npix * 16)))
     return rc;
   if (!ctx->lane_stream[0]) {
     // default priority: the lanes' long-latency threads are launched first and
@@ -1135,7 +1136,8 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
   CK(vmk::launch_resolve(f, dev_world(ctx), L, (const unsigned long long*)ctx->vis.p, mask,
                          (const float*)ctx->shadow.p, (ctx->spec & VM_SPEC_SOFT_RAYS) != 0u, WATER_SEC_SHIFT, refr,
                          refl, (uint8_t*)ctx->lane.p, (uint32_t*)ctx->lane_lists.p, (float*)ctx->light_ao.p,
-                         (float4*)ctx->color.p, ctx->sms, ctx->stream, ctx->lane_stream, ctx->lane_event));
+                         (float4*)ctx->fog.p, (float4*)ctx->color.p, ctx->sms, ctx->stream, ctx->lane_stream,
+                         ctx->lane_event));
   ctx->color_done = true;
   return VM_OK;
 }

@@ -134,7 +134,8 @@ cudaError_t launch_soften(const vm_frame& f, const vmd::DevWorld& w, const unsig
 // lane: one byte per pixel, each pixel's lane (sky, opaque, water, glass,
 // water with its own legs).  lists: 2 x pixels + 2 words, the compact lists
 // of the glass pixels and of the water pixels with their own legs, and their
-// counts.
+// counts.  fog: one float4 per pixel, the fog terms of the water and glass
+// pixels (sky colour behind, opacity), blended after their lanes.
 // light_ao: one float per pixel, the opaque lane's AO between its light stage
 // and its shading (null: one kernel does both).  The water lane (legs, then
 // the pixels that share them), the glass lane and the water pixels with
@@ -145,7 +146,7 @@ cudaError_t launch_soften(const vm_frame& f, const vmd::DevWorld& w, const unsig
 cudaError_t launch_resolve(const vm_frame& f, const vmd::DevWorld& w, const vmd::Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
                            uint16_t* leg_refr, uint16_t* leg_refl, uint8_t* lane, uint32_t* lists, float* light_ao,
-                           float4* out, int sms, cudaStream_t s, const cudaStream_t lane_stream[3],
+                           float4* fog, float4* out, int sms, cudaStream_t s, const cudaStream_t lane_stream[3],
                            const cudaEvent_t lane_event[4]);
 cudaError_t launch_expand(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                           int32_t wx, int32_t wy, int32_t wz, uint32_t dx, uint32_t dy, uint32_t dz,

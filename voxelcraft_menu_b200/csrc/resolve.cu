@@ -662,7 +662,7 @@ __global__ void __launch_bounds__(128) k_resolve_lanes(const __grid_constant__ v
 
 // The pixels of a compact list: glass (WHICH 0, shade_glass,
 // resolve.wgsl:1261-1319) or water with its own legs (WHICH 1, shade_water),
-// then the fog blend; a thread per pixel over a grid of resident blocks.
+// before the fog blend; a thread per pixel over a grid of resident blocks.
 template <int WHICH>
 __global__ void __launch_bounds__(128, 8) k_resolve_list(const __grid_constant__ vm_frame f,
                                                          const __grid_constant__ DevWorld w,
@@ -681,12 +681,9 @@ __global__ void __launch_bounds__(128, 8) k_resolve_list(const __grid_constant__
     const Chunk c = ld_chunk(w, k.ci);
     const float t = hit_t(f, c, k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
     const F3 hit = cam + rd * t;
-    F3 color = WHICH == 0 ? shade_glass(w, f, L, k.ci, k.vx, k.vy, k.vz, k.nid, hit, rd, t)
-                          : shade_water(w, f, L, k.ci, k.vx, k.vy, k.vz, k.nid, hit, rd, t);
-    const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
-    const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
-    color = mix3(color, sky_base(f, L, rd, shaft), alpha);
-    out[pix] = make_float4(color.x, color.y, color.z, 1.0f);
+    const F3 color = WHICH == 0 ? shade_glass(w, f, L, k.ci, k.vx, k.vy, k.vz, k.nid, hit, rd, t)
+                                : shade_water(w, f, L, k.ci, k.vx, k.vy, k.vz, k.nid, hit, rd, t);
+    out[pix] = make_float4(color.x, color.y, color.z, 1.0f);   // the fog blend follows (k_resolve_blend)
   }
 }
 
@@ -776,17 +773,55 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
         color = shade_water(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
       }
     }
-    const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
-    const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
-    color = mix3(color, sky_base(f, L, rd, shaft), alpha);
+    if (PART == 0) {   // water: the fog blend follows (k_resolve_blend)
+      const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
+      const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
+      color = mix3(color, sky_base(f, L, rd, shaft), alpha);
+    }
   }
+  out[pix] = make_float4(color.x, color.y, color.z, 1.0f);
+}
+
+// The fog terms of the water and glass pixels (the blend of every surface
+// lane, resolve.wgsl:1440-1466: fog opacity, sun shafts, sky behind), on the
+// issue-bound chain beside the water and glass lanes, so that their long
+// per-pixel chains end at the surface colour; k_resolve_blend applies them.
+__global__ void __launch_bounds__(128, 12) k_resolve_fog(const __grid_constant__ vm_frame f,
+                                                        const __grid_constant__ DevWorld w,
+                                                        const __grid_constant__ Look L,
+                                                        const unsigned long long* __restrict__ vis,
+                                                        const uint8_t* __restrict__ lane, float4* __restrict__ fog) {
+  const uint32_t px = blockIdx.x * 32u + threadIdx.x, py = blockIdx.y * 4u + threadIdx.y;
+  if (px >= f.res[0] || py >= f.res[1]) return;
+  const uint64_t pix = (uint64_t)py * f.res[0] + px;
+  const uint32_t ln = lane[pix];
+  if (ln != LANE_WATER && ln != LANE_GLASS && ln != LANE_WATER_OWN) return;
+  const KeyParts k = split_key(vis[pix]);
+  const F3 cam = ld3(f.cam_pos);
+  const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+  const float t = hit_t(f, ld_chunk(w, k.ci), k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+  const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
+  const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
+  const F3 sky = sky_base(f, L, rd, shaft);
+  fog[pix] = make_float4(sky.x, sky.y, sky.z, alpha);
+}
+
+// The fog blend of the water and glass pixels, once their lanes are done.
+__global__ void __launch_bounds__(256) k_resolve_blend(uint32_t npix, const uint8_t* __restrict__ lane,
+                                                       const float4* __restrict__ fog, float4* __restrict__ out) {
+  const uint32_t pix = blockIdx.x * 256u + threadIdx.x;
+  if (pix >= npix) return;
+  const uint32_t ln = lane[pix];
+  if (ln != LANE_WATER && ln != LANE_GLASS && ln != LANE_WATER_OWN) return;
+  const float4 c = out[pix], g = fog[pix];
+  const F3 color = mix3(f3(c.x, c.y, c.z), f3(g.x, g.y, g.z), g.w);
   out[pix] = make_float4(color.x, color.y, color.z, 1.0f);
 }
 
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
                            uint16_t* leg_refr, uint16_t* leg_refl, uint8_t* lane, uint32_t* lists, float* light_ao,
-                           float4* out, int sms, cudaStream_t s, const cudaStream_t lane_stream[3],
+                           float4* fog, float4* out, int sms, cudaStream_t s, const cudaStream_t lane_stream[3],
                            const cudaEvent_t lane_event[4]) {
   // The lanes write disjoint pixels.  The water lane (its legs, then the
   // pixels) and the glass lane cover a few clustered pixels with long serial
@@ -823,12 +858,15 @@ cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, 
   if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, lane, out, light_ao);
   k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, light_ao, out);
   k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
+  k_resolve_fog<<<grid, block, 0, s>>>(f, w, L, vis, lane, fog);
   e = cudaGetLastError();
   for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
     e = cudaEventRecord(lane_event[1 + i], lane_stream[i]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, lane_event[1 + i], 0);
   }
-  return e;
+  if (e != cudaSuccess) return e;
+  k_resolve_blend<<<(npix + 255u) / 256u, 256, 0, s>>>(npix, lane, fog, out);
+  return cudaGetLastError();
 }
 
 }  // namespace vmk
