@@ -317,6 +317,46 @@ def test_resolve_rejects_unbuilt_variants(small):
 
 
 @pytest.mark.gpu
+def test_resolve_replays_from_a_cuda_graph(small):
+    """vm_resolve forks its water and glass lanes onto streams of the context
+    with events and joins them back into the caller's stream: recorded into a
+    stream capture the caller owns (a torch CUDA graph) and replayed, it
+    writes the colours of a direct call, bit for bit."""
+    import torch
+    from voxelcraft_menu_b200.march import Marcher
+    w, pools = small
+    v = look_view(w, look_camera())
+    look = (LK.atlas(1), LK.block_faces(), LK.probe_field(5),
+            LK.shaft_envelope(w.recipe, v.frame.sun_dir, v.frame.shaft_origin, 4.0))
+    m = Marcher(v.res[0], v.res[1])
+    try:
+        side = torch.cuda.Stream()
+        m.set_stream(side.cuda_stream)
+        m.upload_world(*pools)
+        m.upload_view(v)
+        m.upload_look(*look)
+        m.render()
+        m.resolve(LK.HI_DEFAULT)          # sizes the resolve's buffers and streams outside the capture
+        want = m.read_color()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side, capture_error_mode="thread_local"):
+            m.resolve(LK.HI_DEFAULT)
+        torch.cuda.synchronize()
+        m.resolve(0)                      # another look over the colour buffer before each replay
+        plain = m.read_color()
+        assert not np.array_equal(plain, want)
+        for _ in range(2):
+            with torch.cuda.stream(side):     # the replay follows the direct calls on the caller's stream
+                g.replay()
+            assert np.array_equal(m.read_color(), want)
+            m.resolve(0)
+        del g
+    finally:
+        m.close()
+
+
+@pytest.mark.gpu
 def test_full_hd_frame_resolve_matches_the_oracle():
     rec = W.recipe_large_terrain()
     w = W.World.generate(rec)

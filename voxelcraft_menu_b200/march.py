@@ -115,6 +115,11 @@ class Marcher:
         override constants); None restores the engine's defaults."""
         self._ck(self._L.vm_set_spec(self._h, SPEC_DEFAULT if spec is None else spec))
 
+    def set_stream(self, stream: int = 0):
+        """The CUDA stream (a cudaStream_t as an int, e.g. a torch stream's
+        cuda_stream) the context's work is issued on; 0: its own stream."""
+        self._ck(self._L.vm_set_stream(self._h, C.c_void_p(stream or None)))
+
     # -- the engine's passes ------------------------------------------------------
     def select(self):
         self._ck(self._L.vm_select(self._h))
@@ -249,12 +254,12 @@ class Marcher:
         self._look = (a, fc, probes, shaft)
 
     def resolve(self, spec_hi: int):
-        """Lane 0 of the engine's resolve (sky and opaque surfaces) over the
+        """The engine's resolve (sky, opaque surfaces, water, glass) over the
         last frame: vm_resolve with the engine's FLAG_HI_* word."""
         self._ck(self._L.vm_resolve(self._h, spec_hi))
 
     def read_color(self) -> np.ndarray:
-        """RGBA float per pixel (alpha 0 for the water and glass pixels)."""
+        """RGBA float per pixel of the last vm_resolve (alpha 1)."""
         out = np.empty((self._npix(), 4), np.float32)
         self._ck(self._L.vm_read_color(self._h, ptr(out)))
         return out
