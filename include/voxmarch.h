@@ -203,6 +203,10 @@ int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* 
  * TERRAIN_SHAFTS, FLAT_SECONDARY, WAVES..., PROBE_CUBE / BOUNCE / SUN /
  * SUN_HIGH, LIGHT_RGB, SKY_TINT, WATER_REFRACT / REFLECT), as make_spec
  * derives them; WATER_SEC_SHIFT is 1 (the engine's water_sec_scale 2).
+ * vm_resolve issues its work on the context's stream (vm_set_stream); the
+ * water and glass lanes run on three streams of the context forked from it
+ * with events and joined back before the call returns, so the call can be
+ * recorded into a stream capture of the caller's stream.
  * vm_read_color: res.x * res.y RGBA float (alpha 1), the value the engine
  * stores into its rgba16float target. */
 int vm_upload_atlas(vm_ctx* ctx, const uint8_t* rgba, uint32_t layers, uint32_t size, uint32_t mips);
