@@ -196,8 +196,10 @@ int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* 
  * the engine's primary_sun texture), spec_hi = the engine's FLAG_HI_* word
  * (src/render/mod.rs:196-300; SKY_SPECULAR, SHORE_WET, SHORE_FOAM,
  * WATER_SEC, CAUSTICS, GLASS_REFLECT, TINT_BALANCE, SKY_LOOK, SKY_COOL,
- * FOLIAGE_RICH, CANOPY_RELIEF, LEGACY_LIGHTING are read; COMPACT_SHADE_HIT,
- * WATER_LOOK and the surface debug views return VM_E_INVALID, as do
+ * FOLIAGE_RICH, CANOPY_RELIEF, LEGACY_LIGHTING are read; COMPACT_SHADE_HIT
+ * is accepted and gives the same colours (the compact shade_hit reorders the
+ * legacy one's statements); WATER_LOOK and the surface debug views return
+ * VM_E_INVALID, as do
  * underwater, heat-map, probe-tap and probe-ambient frames).  The frame
  * flags give the rest (AO, TINT, TEX_VARIATION, DISTANT_SHADOWS,
  * TERRAIN_SHAFTS, FLAT_SECONDARY, WAVES..., PROBE_CUBE / BOUNCE / SUN /

@@ -199,9 +199,9 @@ class Oracle:
         return tuple(out)
 
     def resolve(self, vis, sun_vis, atlas, faces, probes=None, shaft=None, spec_hi: int = 0, pix=None):
-        """Lane 0 of the resolve (resolve.wgsl:1378-1466): RGBA float per pixel
-        of [pix[0], pix[1]) (default: all), alpha 0 for water and glass pixels.
-        sun_vis: the per-pixel sun visibility (the engine's primary_sun)."""
+        """The resolve (resolve.wgsl:1378-1466), every lane: RGBA float per
+        pixel of [pix[0], pix[1]) (default: all), alpha 1.  sun_vis: the
+        per-pixel sun visibility (the engine's primary_sun)."""
         b, e = (0, self.npix) if pix is None else pix
         keep = [np.ascontiguousarray(atlas, np.uint8), np.ascontiguousarray(faces, np.uint32)]
         pr = None if probes is None else np.ascontiguousarray(probes, np.uint16)

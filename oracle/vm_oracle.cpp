@@ -2334,7 +2334,14 @@ bool shadow_ray(const World& w, V3 ro, V3 rd, float max_dist) {
 
 // shade_hit_legacy (resolve.wgsl:289-585) and shade_hit_legacy_cached
 // (resolve.wgsl:1537-1788): lit_frame >= 0 is the cached sun visibility,
-// lit_frame < 0 traces shadow_ray over shadow_dist
+// lit_frame < 0 traces shadow_ray over shadow_dist.  The compact variants
+// (SPEC_COMPACT_SHADE_HIT: shade_hit_compact, resolve.wgsl:587-851, and
+// shade_hit_compact_cached, resolve.wgsl:1790-2054) run the same statements
+// with the material block after the light block: the same chunk's box_min
+// and local, canopy relief from material_ndl = ndl (the same dot(n, sun)),
+// and light_rgb * face_scale with face_scale = 1.0, which is exact; their
+// colours are the legacy variants' bit for bit, so this one restatement
+// serves both.
 V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint32_t nid, V3 hit, V3 rd, float dist,
              float shadow_dist, bool smooth_light, bool do_spec, float lit_frame) {
   const vm_frame& f = *w.f;

@@ -304,7 +304,7 @@ def test_resolve_rejects_unbuilt_variants(small):
         with pytest.raises(RuntimeError):
             m.read_color()                                # no resolve yet
         with pytest.raises(RuntimeError):
-            m.resolve(LK.HI_COMPACT_SHADE_HIT)
+            m.resolve(LK.HI_DEFAULT | LK.HI_WATER_LOOK)
         m.resolve(LK.HI_DEFAULT)
         assert m.read_color().shape == (64 * 36, 4)
         v.frame.flags |= LK.FLAG_PROBE_TAP
@@ -314,6 +314,25 @@ def test_resolve_rejects_unbuilt_variants(small):
             m.resolve(LK.HI_DEFAULT)
     finally:
         m.close()
+
+
+@pytest.mark.gpu
+def test_compact_shade_hit_gives_the_legacy_colours(small):
+    """SPEC_COMPACT_SHADE_HIT (FLAG_HI_COMPACT_SHADE_HIT): shade_hit_compact
+    and shade_hit_compact_cached (resolve.wgsl:587-851,1790-2054) run the
+    legacy variants' statements with the material block after the light
+    block, the light times face_scale = 1.0: the same colours, bit for bit."""
+    w, pools = small
+    v = look_view(w, look_camera())
+    v.frame.flags |= W.FLAG_WATER_REFLECT | W.FLAG_WAVES   # legs shade through the non-cached variant too
+    look = (LK.atlas(1), LK.block_faces(), LK.probe_field(5),
+            LK.shaft_envelope(w.recipe, v.frame.sun_dir, v.frame.shaft_origin, 4.0))
+    hi = LK.HI_DEFAULT | LK.HI_GLASS_REFLECT
+    _, _, _, legacy = gpu_resolve(v, pools, look, hi)
+    vis, sh, _, compact = gpu_resolve(v, pools, look, hi | LK.HI_COMPACT_SHADE_HIT)
+    assert np.array_equal(compact, legacy)
+    want = Oracle(v, *pools).resolve(vis, LK.sun_visibility(sh), *look, spec_hi=hi | LK.HI_COMPACT_SHADE_HIT)
+    within(compact, want, "compact")
 
 
 @pytest.mark.gpu

@@ -999,8 +999,11 @@ float srgb_decode(uint8_t u) {
   return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f);
 }
 
-constexpr uint32_t HI_UNBUILT = 131072u /* COMPACT_SHADE_HIT */ | 8388608u | 16777216u | 33554432u /* DEBUG */ |
-                               4096u /* WATER_LOOK */;
+// FLAG_HI_COMPACT_SHADE_HIT (131072) is accepted: shade_hit_compact(_cached)
+// runs shade_hit_legacy(_cached)'s statements with the material block after
+// the light block (the light times face_scale = 1.0, the canopy relief from
+// the same n . sun), so its colours are the legacy variant's bit for bit.
+constexpr uint32_t HI_UNBUILT = 8388608u | 16777216u | 33554432u /* DEBUG */ | 4096u /* WATER_LOOK */;
 constexpr uint32_t HI_WATER_SEC = 32u;
 constexpr uint32_t WATER_SEC_SHIFT = 1u;   // WATER_SEC_SHIFT of the engine's default water_sec_scale 2
 
@@ -1103,8 +1106,8 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
   if (f.flags & (VM_FLAG_UNDERWATER | VM_FLAG_HEATMAP | VM_FLAG_PROBE_TAP | VM_FLAG_PROBE_AMBIENT))
     return fail(ctx, VM_E_INVALID, "resolve of underwater, heat-map, probe-tap or probe-ambient frames is not built");
   if (spec_hi & HI_UNBUILT)
-    return fail(ctx, VM_E_INVALID, "spec_hi 0x%x: compact shade_hit, the water look and surface debug views "
-                "are not built", spec_hi & HI_UNBUILT);
+    return fail(ctx, VM_E_INVALID, "spec_hi 0x%x: the water look and surface debug views are not built",
+                spec_hi & HI_UNBUILT);
   CK(cudaSetDevice(ctx->device));
   if ((rc = ensure(ctx, ctx->color, npix * 16)) || (rc = ensure(ctx, ctx->light_ao, npix * 4)) ||
       (rc = ensure(ctx, ctx->lane, npix)) || (rc = ensure(ctx, ctx->lane_lists, npix * 8 + 8)) ||
