@@ -2187,6 +2187,31 @@ F4 probe_field(const Look& L, V3 p, uint32_t nid) {
   return mix4(s[0], s[1], az);
 }
 
+// probe_tap: resolve.wgsl:120-127 (PROBE_TAPS = 1): the probe texture
+// through the engine's linear sampler (mod.rs:1070-1077: linear filtering,
+// clamp to edge on every axis) at fract(p / (PROBE_DIM * PROBE_SPACING))
+F4 probe_texel_clamped(const Look& L, int32_t x, int32_t y, int32_t z) {
+  return probe_texel(L, std::min(std::max(x, 0), 127), y, std::min(std::max(z, 0), 127));
+}
+V3 probe_tap(const Look& L, V3 p) {
+  if (!L.probes) return v3(1.0f, 1.0f, 1.0f);
+  const float inv_span = 1.0f / (128.0f * 4.0f);
+  auto fract = [](float x) { return x - floorf(x); };
+  float u = fract(p.x * inv_span), v = fract(p.y * inv_span), wz = fract(p.z * inv_span + 0.0f);
+  float x = u * 128.0f - 0.5f, yy = v * 768.0f - 0.5f, z = wz * 128.0f - 0.5f;
+  float x0 = floorf(x), y0 = floorf(yy), z0 = floorf(z);
+  float ax = x - x0, ay = yy - y0, az = z - z0;
+  int32_t ix = f2i(x0), iy = f2i(y0), iz = f2i(z0);
+  F4 s[2];
+  for (int dz = 0; dz < 2; ++dz) {
+    F4 a = mix4(probe_texel_clamped(L, ix, iy, iz + dz), probe_texel_clamped(L, ix + 1, iy, iz + dz), ax);
+    F4 b = mix4(probe_texel_clamped(L, ix, iy + 1, iz + dz), probe_texel_clamped(L, ix + 1, iy + 1, iz + dz), ax);
+    s[dz] = mix4(a, b, ay);
+  }
+  F4 r = mix4(s[0], s[1], az);
+  return mul(v3(1.0f, 1.0f, 1.0f), v3(r.r, r.g, r.b));
+}
+
 // face_uv / perm_key / permute_uv: resolve.wgsl:129-164
 void face_uv(uint32_t nid, V3 local, float& u, float& v) {
   if (nid >= VM_NORMAL_CROSS_A) { u = local.x; v = 1.0f - local.y; return; }
@@ -2490,6 +2515,11 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
     sky_sm = mixs(mixs(sky_c[0], sky_c[1], fa), mixs(sky_c[2], sky_c[3], fa), fb);
     amb = mixv(mixv(amb_c[0], amb_c[1], fa), mixv(amb_c[2], amb_c[3], fa), fb);
   }
+  // SPEC_PROBE_AMBIENT / SPEC_PROBE_TAP (resolve.wgsl:500-505): the ambient
+  // from the probe tap alone (the light words' ambient unused), or scaled by it
+  const bool probe_ambient = (f.flags & VM_FLAG_PROBE_AMBIENT) != 0u;
+  if (probe_ambient) amb = probe_tap(L, hit);
+  else if ((f.flags & VM_FLAG_PROBE_TAP) != 0u) amb = mul(amb, probe_tap(L, hit));
   float direct = 0.0f;
   float ndl = dot(n, sun);
   if (ndl > 0.0f && f.daylight > 0.01f) {
@@ -2522,17 +2552,23 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
   }
   bool probe_cube = (f.flags & VM_FLAG_PROBE_CUBE) != 0u, probe_bounce = (f.flags & VM_FLAG_PROBE_BOUNCE) != 0u;
   F4 probe = {1.0f, 1.0f, 1.0f, 1.0f};
-  if (probe_cube || probe_bounce) probe = probe_field(L, add(hit, muls(n, 2.0f)), nid);
-  float shade = repair(L) ? 1.0f : face_shade(nid);
-  if (probe_cube) shade = shade * probe.a;
+  if (!probe_ambient && (probe_cube || probe_bounce)) probe = probe_field(L, add(hit, muls(n, 2.0f)), nid);
+  float shade = 1.0f;
+  if (!probe_ambient) {
+    shade = repair(L) ? 1.0f : face_shade(nid);
+    if (probe_cube) shade = shade * probe.a;
+  }
   V3 ambient_rgb = muls(amb, 0.50f);
   V3 sun_rgb = muls(v3(1.0000f, 0.8469f, 0.5647f), direct * (repair(L) ? 0.78f : 0.52f));
-  V3 floor_rgb = muls(v3(0.85f, 0.90f, 1.00f), f.ambient);
+  V3 floor_rgb = v3(0.0f, 0.0f, 0.0f);
   V3 prgb = v3(probe.r, probe.g, probe.b);
-  if (probe_bounce) floor_rgb = mul(floor_rgb, prgb);
-  if ((f.flags & VM_FLAG_PROBE_SUN) != 0u) {
-    float gain = (f.flags & VM_FLAG_PROBE_SUN_HIGH) != 0u ? 0.25f : 0.10f;
-    floor_rgb = add(floor_rgb, muls(mul(v3(0.85f, 0.90f, 1.00f), prgb), gain * sky_sm));
+  if (!probe_ambient) {
+    floor_rgb = muls(v3(0.85f, 0.90f, 1.00f), f.ambient);
+    if (probe_bounce) floor_rgb = mul(floor_rgb, prgb);
+    if ((f.flags & VM_FLAG_PROBE_SUN) != 0u) {
+      float gain = (f.flags & VM_FLAG_PROBE_SUN_HIGH) != 0u ? 0.25f : 0.10f;
+      floor_rgb = add(floor_rgb, muls(mul(v3(0.85f, 0.90f, 1.00f), prgb), gain * sky_sm));
+    }
   }
   V3 spec_rgb = muls(spec_pre, sky_sm * 0.5f);
   V3 light = repair(L) ? add(add(muls(muls(ambient_rgb, ao), shade), sun_rgb), floor_rgb)

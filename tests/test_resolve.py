@@ -235,7 +235,7 @@ def gpu_resolve(v, pools, look, spec_hi, soften=None, spec=None):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["default", "engine_atlas", "probes_shaft", "plain_flags", "legacy_lighting",
-                                  "reflect_legs", "per_pixel_legs"])
+                                  "reflect_legs", "per_pixel_legs", "probe_tap", "probe_ambient"])
 def test_resolve_matches_the_oracle(small, case):
     w, pools = small
     cam = look_camera()
@@ -257,6 +257,11 @@ def test_resolve_matches_the_oracle(small, case):
         v.frame.flags |= W.FLAG_WATER_REFLECT
         v.frame.flags &= ~LK.FLAG_FLAT_SECONDARY
         spec_hi = LK.HI_DEFAULT & ~LK.HI_WATER_SEC
+    elif case in ("probe_tap", "probe_ambient"):
+        # SPEC_PROBE_TAP / SPEC_PROBE_AMBIENT (resolve.wgsl:500-505): the probe
+        # field through the clamped linear sampler scales, or replaces, the ambient
+        probes = LK.probe_field(5)
+        v.frame.flags |= LK.FLAG_PROBE_TAP if case == "probe_tap" else LK.FLAG_PROBE_AMBIENT
     atlas = engine_atlas() if case == "engine_atlas" else LK.atlas(2)
     look = (atlas, LK.block_faces(), probes, shaft)
     vis, sh, _, got = gpu_resolve(v, pools, look, spec_hi)
@@ -307,7 +312,7 @@ def test_resolve_rejects_unbuilt_variants(small):
             m.resolve(LK.HI_DEFAULT | LK.HI_WATER_LOOK)
         m.resolve(LK.HI_DEFAULT)
         assert m.read_color().shape == (64 * 36, 4)
-        v.frame.flags |= LK.FLAG_PROBE_TAP
+        v.frame.flags |= W.FLAG_HEATMAP
         m.upload_view(v)
         m.render()
         with pytest.raises(RuntimeError):

@@ -184,8 +184,13 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
   LightTerms lt;
   if (pre != nullptr) lt = *pre;
   else lt = surface_light_terms(w, f, L, ci, vx, vy, vz, nid, n, hit, smooth);
-  const F3 amb = lt.amb;
+  F3 amb = lt.amb;
   const float sky_sm = lt.sky_sm, ao = lt.ao;
+  // SPEC_PROBE_AMBIENT / SPEC_PROBE_TAP (resolve.wgsl:500-505): the ambient
+  // from the probe tap alone (the light words' ambient unused), or scaled by it
+  const bool probe_ambient = (f.flags & VM_FLAG_PROBE_AMBIENT) != 0u;
+  if (probe_ambient) amb = probe_tap(L, hit);
+  else if ((f.flags & VM_FLAG_PROBE_TAP) != 0u) amb = amb * probe_tap(L, hit);
   float direct = 0.0f;
   const float ndl = dot(n, sun);
   if (ndl > 0.0f && f.daylight > 0.01f) {
@@ -218,18 +223,24 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
   }
   const bool probe_cube = (f.flags & VM_FLAG_PROBE_CUBE) != 0u, probe_bounce = (f.flags & VM_FLAG_PROBE_BOUNCE) != 0u;
   float4 probe = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-  if (probe_cube || probe_bounce) probe = probe_field(L, hit + n * 2.0f, nid);
+  if (!probe_ambient && (probe_cube || probe_bounce)) probe = probe_field(L, hit + n * 2.0f, nid);
   const bool repair = lighting_repair(L);
-  float shade = repair ? 1.0f : face_shade(nid);
-  if (probe_cube) shade = shade * probe.w;
+  float shade = 1.0f;
+  if (!probe_ambient) {
+    shade = repair ? 1.0f : face_shade(nid);
+    if (probe_cube) shade = shade * probe.w;
+  }
   const F3 ambient_rgb = amb * 0.50f;
   const F3 sun_rgb = f3(1.0000f, 0.8469f, 0.5647f) * (direct * (repair ? 0.78f : 0.52f));
-  F3 floor_rgb = f3(0.85f, 0.90f, 1.00f) * f.ambient;
-  const F3 probe_rgb = {probe.x, probe.y, probe.z};
-  if (probe_bounce) floor_rgb = floor_rgb * probe_rgb;
-  if ((f.flags & VM_FLAG_PROBE_SUN) != 0u) {
-    const float gain = (f.flags & VM_FLAG_PROBE_SUN_HIGH) != 0u ? 0.25f : 0.10f;
-    floor_rgb = floor_rgb + f3(0.85f, 0.90f, 1.00f) * probe_rgb * (gain * sky_sm);
+  F3 floor_rgb = {0.0f, 0.0f, 0.0f};
+  if (!probe_ambient) {
+    floor_rgb = f3(0.85f, 0.90f, 1.00f) * f.ambient;
+    const F3 probe_rgb = {probe.x, probe.y, probe.z};
+    if (probe_bounce) floor_rgb = floor_rgb * probe_rgb;
+    if ((f.flags & VM_FLAG_PROBE_SUN) != 0u) {
+      const float gain = (f.flags & VM_FLAG_PROBE_SUN_HIGH) != 0u ? 0.25f : 0.10f;
+      floor_rgb = floor_rgb + f3(0.85f, 0.90f, 1.00f) * probe_rgb * (gain * sky_sm);
+    }
   }
   const F3 spec_rgb = spec_pre * (sky_sm * 0.5f);
   // surface_light / surface_radiance: resolve.wgsl:7-17

@@ -531,6 +531,32 @@ static __device__ __noinline__ float4 probe_field(const Look& L, F3 p, uint32_t 
   return mix4(s[0], s[1], az);
 }
 
+// probe_tap (resolve.wgsl:120-127, PROBE_TAPS = 1): the probe field through
+// the engine's linear sampler (linear filtering, clamp to edge on every
+// axis) at fract(p / (PROBE_DIM * PROBE_SPACING)).
+__device__ __forceinline__ float4 probe_texel_clamped(const Look& L, int32_t x, int32_t y, int32_t z) {
+  return probe_texel(L, min(max(x, 0), (int32_t)PROBE_NX - 1), y, min(max(z, 0), (int32_t)PROBE_NZ - 1));
+}
+static __device__ __noinline__ F3 probe_tap(const Look& L, F3 p) {
+  if (L.probes == nullptr) return {1.0f, 1.0f, 1.0f};
+  const float inv_span = 1.0f / ((float)PROBE_NX * 4.0f);
+  const float u = fractf(p.x * inv_span), v = fractf(p.y * inv_span), w = fractf(p.z * inv_span + 0.0f);
+  const float x = u * (float)PROBE_NX - 0.5f, yy = v * (float)PROBE_NY - 0.5f, z = w * (float)PROBE_NZ - 0.5f;
+  const float x0 = floorf(x), y0 = floorf(yy), z0 = floorf(z);
+  const float ax = x - x0, ay = yy - y0, az = z - z0;
+  const int32_t ix = ffloor_i(x0), iy = ffloor_i(y0), iz = ffloor_i(z0);
+  float4 s[2];
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz) {
+    const float4 a = mix4(probe_texel_clamped(L, ix, iy, iz + dz), probe_texel_clamped(L, ix + 1, iy, iz + dz), ax);
+    const float4 b =
+        mix4(probe_texel_clamped(L, ix, iy + 1, iz + dz), probe_texel_clamped(L, ix + 1, iy + 1, iz + dz), ax);
+    s[dz] = mix4(a, b, ay);
+  }
+  const float4 r = mix4(s[0], s[1], az);
+  return f3(1.0f, 1.0f, 1.0f) * f3(r.x, r.y, r.z);
+}
+
 // ---------------------------------------------------------------------------
 // surface material: resolve.wgsl:129-165, 166-285
 
