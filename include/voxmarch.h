@@ -199,10 +199,10 @@ int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* 
  * FOLIAGE_RICH, CANOPY_RELIEF, LEGACY_LIGHTING are read; COMPACT_SHADE_HIT
  * is accepted and gives the same colours (the compact shade_hit reorders the
  * legacy one's statements); WATER_LOOK and the surface debug views return
- * VM_E_INVALID, as do underwater and heat-map frames).  The frame flags give
- * the rest (AO, TINT, TEX_VARIATION, DISTANT_SHADOWS, TERRAIN_SHAFTS,
- * FLAT_SECONDARY, WAVES..., PROBE_CUBE / BOUNCE / SUN / SUN_HIGH / TAP /
- * AMBIENT, LIGHT_RGB, SKY_TINT, WATER_REFRACT / REFLECT), as make_spec
+ * VM_E_INVALID, as do heat-map frames).  The frame flags give the rest
+ * (AO, TINT, TEX_VARIATION, DISTANT_SHADOWS, TERRAIN_SHAFTS, FLAT_SECONDARY,
+ * WAVES..., PROBE_CUBE / BOUNCE / SUN / SUN_HIGH / TAP / AMBIENT, LIGHT_RGB,
+ * SKY_TINT, WATER_REFRACT / REFLECT, UNDERWATER, SNELL), as make_spec
  * derives them; WATER_SEC_SHIFT is 1 (the engine's water_sec_scale 2).
  * vm_resolve issues its work on the context's stream (vm_set_stream); the
  * water and glass lanes run on three streams of the context forked from it

@@ -2871,6 +2871,53 @@ typedef struct or_look {
 // The resolve's colour (RGBA, alpha 1; water and glass pixels 0) of pixels
 // [pix_begin, pix_end) from the frame's keys and the sun visibility of each
 // pixel (the engine's primary_sun: r8unorm of the soft mask, or 1 - blocked).
+// ---- the underwater resolve: resolve.wgsl:1321-1376,1449-1464 ----------------
+constexpr uint32_t FLAG_SNELL = 8388608u;   // mod.rs FLAG_SNELL
+// water_path: common.wgsl:1293-1298
+float water_path(const vm_frame& f, float t, V3 rd) {
+  if (rd.y <= 0.0f) return t;
+  return clampf((f.sea_level - f.cam_pos[1]) / rd.y, 0.0f, t);
+}
+// underwater_body: resolve.wgsl:1321-1323 (WATER_BODY, resolve.wgsl:894)
+V3 underwater_body(const World& w) {
+  return muls(v3(0.0100f, 0.0947f, 0.1474f), medium_light(*w.f, world_sample(w, ld3(w.f->cam_pos)).x));
+}
+// surface_from_below: resolve.wgsl:1325-1376 (SNELL_MIN_DEPTH 3, WATER_DARK_DEPTH
+// 15, SNELL_DIM_MAX 0.9: common.wgsl:167-171)
+V3 surface_from_below(const World& w, V3 above, V3 rd, float dist) {
+  const vm_frame& f = *w.f;
+  if ((f.flags & FLAG_SNELL) == 0u) return above;
+  float depth = f.sea_level - f.cam_pos[1];
+  float s = smoothstep(3.0f, 15.0f, depth);
+  if (s <= 0.0f) return above;
+  if (rd.y <= 0.0f) return above;
+  float t_surf = (f.sea_level - f.cam_pos[1]) / rd.y;
+  if (t_surf >= dist || t_surf <= 0.0f) return above;
+  V3 surf = add(ld3(f.cam_pos), muls(rd, t_surf));
+  float mirror_detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, t_surf);
+  V3 nup = v3(0.0f, 1.0f, 0.0f);
+  if ((f.flags & VM_FLAG_WAVES) != 0u && mirror_detail > 0.0f) {
+    float px_world = fmaxf(t_surf, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1];
+    float kk = 0.0f, vhx = 0.0f, vhz = 0.0f;
+    bool aniso = (f.flags & VM_FLAG_WAVE_ANISO) != 0u;
+    if (aniso) {
+      float k = 1.0f / fmaxf(fabsf(rd.y), 1e-3f);
+      kk = k * k - 1.0f;
+      float r = 1.0f / sqrtf(fmaxf(rd.x * rd.x + rd.z * rd.z, 1e-12f));
+      vhx = rd.x * r; vhz = rd.z * r;
+    }
+    V3 wf = wave_field(f, surf.x, surf.z, px_world, vhx, vhz, kk, aniso, 1.0f);
+    nup = normalize(v3(-wf.x, 1.0f, -wf.y));   // wave_normal
+  }
+  float cos_i = clampf(dot(rd, nup), 1e-3f, 1.0f);
+  float sin2_t = VM_WATER_IOR * VM_WATER_IOR * (1.0f - cos_i * cos_i);
+  float fr = 1.0f;
+  if (sin2_t < 1.0f) fr = schlick_f0(0.02f, sqrtf(1.0f - sin2_t));
+  V3 below = underwater_body(w);
+  V3 transmitted = mixv(above, underwater_body(w), s * 0.9f);
+  return mixv(transmitted, below, fr * s);
+}
+
 int or_resolve(const or_world* o, const or_look* lk, const uint64_t* vis, const float* sun_vis, float* rgba,
                uint64_t pix_begin, uint64_t pix_end, int threads) {
   World w = mk(o);
@@ -2904,8 +2951,10 @@ int or_resolve(const or_world* o, const or_look* lk, const uint64_t* vis, const 
     uint64_t key = vis[pix];
     V3 color;
     float* out = rgba + 4 * (pix - pix_begin);
+    const bool underwater = (f.flags & VM_FLAG_UNDERWATER) != 0u;
+    float dist = f.far_;
     if (key == 0) {
-      float shaft = sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
+      float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
       color = sky_color(f, L, cam, rd, 0.0f, shaft);
     } else {
       uint32_t nid = key_nid(key), ci = key_ci(key);
@@ -2930,9 +2979,15 @@ int or_resolve(const or_world* o, const or_look* lk, const uint64_t* vis, const 
       } else {
         color = shade_hit(w, L, ci, v, id, nid, hit, rd, t, f.shadow_dist, true, true, sun_vis[pix]);
       }
-      float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
-      float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
+      dist = t;
+      float wet = underwater ? water_path(f, t, rd) : 0.0f;
+      float alpha = 1.0f - transmittance_from(f, cam.y + wet * rd.y, t - wet, rd);
+      float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, t, alpha, px, py);
       color = mixv(color, sky_base(f, L, rd, shaft), alpha);
+    }
+    if (underwater) {
+      color = surface_from_below(w, color, rd, dist);
+      color = water_medium(f, color, water_path(f, dist, rd), underwater_body(w));
     }
     out[0] = color.x; out[1] = color.y; out[2] = color.z; out[3] = 1.0f;
   }

@@ -321,6 +321,35 @@ def test_resolve_rejects_unbuilt_variants(small):
         m.close()
 
 
+FLAG_SNELL = 8388608   # the engine's FLAG_SNELL frame flag (src/render/mod.rs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("snell", [False, True])
+def test_underwater_resolve_matches_the_oracle(small, snell):
+    """An underwater frame (resolve.wgsl:1396-1464): the fog path starts at the
+    sea surface (water_path), no sun shafts, and every pixel ends with
+    surface_from_below (with FLAG_SNELL the waved sea surface seen from below,
+    Fresnel-weighted against the water body) and the camera ray's water
+    medium (resolve.wgsl:1321-1376)."""
+    w, pools = small
+    # the deepest sea floor away from the world's edge, the camera 4 above it
+    h, x, z = min((W.surface_height(w.recipe, x, z), x, z) for x in range(32, 224, 4) for z in range(32, 224, 4))
+    assert h + 4 < w.recipe.water_level - 3                 # deeper than SNELL_MIN_DEPTH
+    flags = (W.FLAG_SHADOWS | W.FLAG_WATER_REFRACT | W.FLAG_UNDERWATER | W.FLAG_WATER_FAR | W.FLAG_WAVES |
+             LK.LOOK_FLAGS | (FLAG_SNELL if snell else 0))
+    cam = W.Camera(pos=(x + 0.5, h + 4.0, z + 0.5), pitch=math.radians(25.0), width=320, height=200, flags=flags)
+    v = look_view(w, cam)
+    look = (LK.atlas(1), LK.block_faces(), LK.probe_field(5),
+            LK.shaft_envelope(w.recipe, v.frame.sun_dir, v.frame.shaft_origin, 4.0))
+    vis, sh, _, got = gpu_resolve(v, pools, look, LK.HI_DEFAULT)
+    o = Oracle(v, *pools)
+    assert np.array_equal(vis, o.frame_vis()[0])
+    want = o.resolve(vis, LK.sun_visibility(sh), *look, spec_hi=LK.HI_DEFAULT)
+    within(got, want, f"underwater, snell {snell}")
+    assert (vis == 0).any() and (vis != 0).any()
+
+
 @pytest.mark.gpu
 def test_compact_shade_hit_gives_the_legacy_colours(small):
     """SPEC_COMPACT_SHADE_HIT (FLAG_HI_COMPACT_SHADE_HIT): shade_hit_compact

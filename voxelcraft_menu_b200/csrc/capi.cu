@@ -1103,8 +1103,7 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
   if (!ctx->vis.p || ctx->vis.bytes < npix * 8 || !ctx->shadow.p)
     return fail(ctx, VM_E_NOT_READY, "no rendered frame to resolve");
   if (!ctx->atlas_layers || !ctx->n_faces) return fail(ctx, VM_E_NOT_READY, "no atlas / block faces uploaded");
-  if (f.flags & (VM_FLAG_UNDERWATER | VM_FLAG_HEATMAP))
-    return fail(ctx, VM_E_INVALID, "resolve of underwater or heat-map frames is not built");
+  if (f.flags & VM_FLAG_HEATMAP) return fail(ctx, VM_E_INVALID, "resolve of heat-map frames is not built");
   if (spec_hi & HI_UNBUILT)
     return fail(ctx, VM_E_INVALID, "spec_hi 0x%x: the water look and surface debug views are not built",
                 spec_hi & HI_UNBUILT);

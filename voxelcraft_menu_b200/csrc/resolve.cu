@@ -385,6 +385,62 @@ static __device__ __noinline__ float4 water_reflect_leg(const DevWorld& w, const
   return make_float4(lit.x, lit.y, lit.z, 1.0f);
 }
 
+// ---------------------------------------------------------------------------
+// the underwater resolve: resolve.wgsl:1321-1376,1449-1464
+
+constexpr uint32_t FLAG_SNELL = 8388608u;   // the engine's FLAG_SNELL frame flag
+
+// water_path: common.wgsl:1293-1298, the part of a camera ray under the sea
+__device__ __forceinline__ float water_path(const vm_frame& f, float t, F3 rd) {
+  if (rd.y <= 0.0f) return t;
+  return clampf((f.sea_level - f.cam_pos[1]) / rd.y, 0.0f, t);
+}
+// underwater_body: resolve.wgsl:1321-1323 (WATER_BODY, resolve.wgsl:894)
+static __device__ __noinline__ F3 underwater_body(const DevWorld& w, const vm_frame& f) {
+  return f3(0.0100f, 0.0947f, 0.1474f) * medium_light(f, world_sample(w, f, ld3(f.cam_pos)).x);
+}
+// surface_from_below: resolve.wgsl:1325-1376, the sea surface seen from
+// below (SNELL_MIN_DEPTH 3, WATER_DARK_DEPTH 15, SNELL_DIM_MAX 0.9:
+// common.wgsl:167-171)
+static __device__ __noinline__ F3 surface_from_below(const DevWorld& w, const vm_frame& f, F3 above, F3 rd,
+                                                     float dist) {
+  if ((f.flags & FLAG_SNELL) == 0u) return above;
+  const float depth = f.sea_level - f.cam_pos[1];
+  const float s = smoothstep(3.0f, 15.0f, depth);
+  if (s <= 0.0f) return above;
+  if (rd.y <= 0.0f) return above;
+  const float t_surf = (f.sea_level - f.cam_pos[1]) / rd.y;
+  if (t_surf >= dist || t_surf <= 0.0f) return above;
+  const F3 surf = ld3(f.cam_pos) + rd * t_surf;
+  const float mirror_detail = 1.0f - smoothstep(VM_WATER_REFRACT_NEAR, VM_WATER_REFRACT_FAR, t_surf);
+  F3 nup = {0.0f, 1.0f, 0.0f};
+  if ((f.flags & VM_FLAG_WAVES) != 0u && mirror_detail > 0.0f) {
+    const float px_world = fmaxf(t_surf, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1];
+    float kk = 0.0f, vhx = 0.0f, vhz = 0.0f;
+    const bool aniso = (f.flags & VM_FLAG_WAVE_ANISO) != 0u;
+    if (aniso) {
+      const float k = 1.0f / fmaxf(fabsf(rd.y), WAVE_GRAZE_MIN);
+      kk = k * k - 1.0f;
+      const float r = 1.0f / sqrtf(fmaxf(rd.x * rd.x + rd.z * rd.z, 1e-12f));
+      vhx = rd.x * r; vhz = rd.z * r;
+    }
+    const F3 wf = wave_field(f, surf.x, surf.z, px_world, vhx, vhz, kk, aniso, 1.0f);
+    nup = unit(f3(-wf.x, 1.0f, -wf.y));   // wave_normal
+  }
+  const float cos_i = clampf(dot(rd, nup), 1e-3f, 1.0f);
+  const float sin2_t = VM_WATER_IOR * VM_WATER_IOR * (1.0f - cos_i * cos_i);
+  float fr = 1.0f;
+  if (sin2_t < 1.0f) fr = schlick_f0(0.02f, sqrtf(1.0f - sin2_t));
+  const F3 below = underwater_body(w, f);
+  const F3 transmitted = mix3(above, underwater_body(w, f), s * 0.9f);
+  return mix3(transmitted, below, fr * s);
+}
+// the camera-ray tail of an underwater frame (resolve.wgsl:1460-1464)
+__device__ __forceinline__ F3 underwater_tail(const DevWorld& w, const vm_frame& f, F3 color, F3 rd, float dist) {
+  color = surface_from_below(w, f, color, rd, dist);
+  return water_medium(f, color, water_path(f, dist, rd), underwater_body(w, f));
+}
+
 // foam_hash / foam_mottle: resolve.wgsl:1011-1027
 __device__ __forceinline__ float foam_hash(float ix, float iy) {
   const int32_t qx = __float2int_rz(ix), qy = __float2int_rz(iy);
@@ -752,9 +808,11 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
   const F3 cam = ld3(f.cam_pos);
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   F3 color;
+  const bool underwater = (f.flags & VM_FLAG_UNDERWATER) != 0u;
   if (PART == 1) {
-    const float shaft = sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
+    const float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
     color = sky_color(f, L, cam, rd, 0.0f, shaft);
+    if (underwater) color = underwater_tail(w, f, color, rd, f.far_);
   } else {
     const uint32_t nid = (uint32_t)(key >> 37) & 7u;
     const uint32_t ci = (uint32_t)(key >> 24) & 0x1FFFu;
@@ -785,9 +843,11 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
       }
     }
     if (PART == 0) {   // water: the fog blend follows (k_resolve_blend)
-      const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
-      const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
+      const float wet = underwater ? water_path(f, t, rd) : 0.0f;
+      const float alpha = 1.0f - transmittance_from(f, cam.y + wet * rd.y, t - wet, rd);
+      const float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, t, alpha, px, py);
       color = mix3(color, sky_base(f, L, rd, shaft), alpha);
+      if (underwater) color = underwater_tail(w, f, color, rd, t);
     }
   }
   out[pix] = make_float4(color.x, color.y, color.z, 1.0f);
@@ -811,21 +871,34 @@ __global__ void __launch_bounds__(128, 12) k_resolve_fog(const __grid_constant__
   const F3 cam = ld3(f.cam_pos);
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   const float t = hit_t(f, ld_chunk(w, k.ci), k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
-  const float alpha = 1.0f - transmittance_from(f, cam.y, t, rd);
-  const float shaft = sun_shaft(f, L, cam, rd, t, alpha, px, py);
+  const bool underwater = (f.flags & VM_FLAG_UNDERWATER) != 0u;
+  const float wet = underwater ? water_path(f, t, rd) : 0.0f;
+  const float alpha = 1.0f - transmittance_from(f, cam.y + wet * rd.y, t - wet, rd);
+  const float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, t, alpha, px, py);
   const F3 sky = sky_base(f, L, rd, shaft);
   fog[pix] = make_float4(sky.x, sky.y, sky.z, alpha);
 }
 
-// The fog blend of the water and glass pixels, once their lanes are done.
-__global__ void __launch_bounds__(256) k_resolve_blend(uint32_t npix, const uint8_t* __restrict__ lane,
+// The fog blend of the water and glass pixels, once their lanes are done
+// (and, in an underwater frame, the camera ray's own tail).
+__global__ void __launch_bounds__(256) k_resolve_blend(const __grid_constant__ vm_frame f,
+                                                       const __grid_constant__ DevWorld w,
+                                                       const unsigned long long* __restrict__ vis,
+                                                       const uint8_t* __restrict__ lane,
                                                        const float4* __restrict__ fog, float4* __restrict__ out) {
   const uint32_t pix = blockIdx.x * 256u + threadIdx.x;
-  if (pix >= npix) return;
+  if (pix >= f.res[0] * f.res[1]) return;
   const uint32_t ln = lane[pix];
   if (ln != LANE_WATER && ln != LANE_GLASS && ln != LANE_WATER_OWN) return;
   const float4 c = out[pix], g = fog[pix];
-  const F3 color = mix3(f3(c.x, c.y, c.z), f3(g.x, g.y, g.z), g.w);
+  F3 color = mix3(f3(c.x, c.y, c.z), f3(g.x, g.y, g.z), g.w);
+  if ((f.flags & VM_FLAG_UNDERWATER) != 0u) {
+    const uint32_t px = pix % f.res[0], py = pix / f.res[0];
+    const KeyParts k = split_key(vis[pix]);
+    const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
+    const float t = hit_t(f, ld_chunk(w, k.ci), k.vx, k.vy, k.vz, k.mx, k.my, k.mz, k.nid, rd);
+    color = underwater_tail(w, f, color, rd, t);
+  }
   out[pix] = make_float4(color.x, color.y, color.z, 1.0f);
 }
 
@@ -876,7 +949,7 @@ cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, 
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, lane_event[1 + i], 0);
   }
   if (e != cudaSuccess) return e;
-  k_resolve_blend<<<(npix + 255u) / 256u, 256, 0, s>>>(npix, lane, fog, out);
+  k_resolve_blend<<<(npix + 255u) / 256u, 256, 0, s>>>(f, w, vis, lane, fog, out);
   return cudaGetLastError();
 }
 
