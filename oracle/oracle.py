@@ -84,6 +84,7 @@ def lib():
             "or_reflect": (C.c_int, [vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
             "or_water_sec": (C.c_int, [vp, vp, C.c_uint32, vp, vp, vp, vp, C.c_int]),
             "or_resolve": (C.c_int, [vp, vp, vp, vp, vp, C.c_uint64, C.c_uint64, C.c_int]),
+            "or_resolve_heat": (C.c_int, [vp, vp, vp, C.c_uint64, C.c_uint64]),
             "or_build_atlas": (None, [C.c_float, C.c_int, vp]),
             "or_pick_rows": (C.c_uint64, [vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, vp]),
             "or_f16_round": (None, [vp, vp, C.c_uint64]),
@@ -197,6 +198,15 @@ class Oracle:
         v = np.ascontiguousarray(vis, np.uint64)
         self._check(self.L.or_water_sec(C.byref(self.w), _p(v), shift, *(_p(a) for a in out), self.threads))
         return tuple(out)
+
+    def resolve_heat(self, dbg, pix=None):
+        """The heat-map view of a FLAG_HEATMAP frame (resolve.wgsl:36-44,
+        1389-1394): RGBA per pixel from the summed march iterations dbg."""
+        b, e = (0, self.npix) if pix is None else pix
+        d = np.ascontiguousarray(dbg, np.uint32)
+        out = np.zeros((e - b, 4), np.float32)
+        self._check(self.L.or_resolve_heat(C.byref(self.w), _p(d), _p(out), b, e))
+        return out
 
     def resolve(self, vis, sun_vis, atlas, faces, probes=None, shaft=None, spec_hi: int = 0, pix=None):
         """The resolve (resolve.wgsl:1378-1466), every lane: RGBA float per

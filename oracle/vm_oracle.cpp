@@ -2918,6 +2918,23 @@ V3 surface_from_below(const World& w, V3 above, V3 rd, float dist) {
   return mixv(transmitted, below, fr * s);
 }
 
+// heat: resolve.wgsl:36-44, the heat-map view of a FLAG_HEATMAP frame
+// (resolve.wgsl:1389-1394): every pixel's summed march iterations / 300
+int or_resolve_heat(const or_world* o, const uint32_t* dbg, float* rgba, uint64_t pix_begin, uint64_t pix_end) {
+  const vm_frame& f = *o->frame;
+  const uint64_t npix = (uint64_t)f.res[0] * f.res[1];
+  if (pix_end > npix) pix_end = npix;
+  for (uint64_t pix = pix_begin; pix < pix_end; ++pix) {
+    float t = clampf((float)dbg[pix] / 300.0f, 0.0f, 1.0f);
+    float c[3] = {smoothstep(0.35f, 0.85f, t), smoothstep(0.0f, 0.45f, t) - smoothstep(0.65f, 1.0f, t),
+                  1.0f - smoothstep(0.0f, 0.45f, t)};
+    float* out = rgba + 4 * (pix - pix_begin);
+    for (int ch = 0; ch < 3; ++ch) out[ch] = powf(c[ch], 2.2f);
+    out[3] = 1.0f;
+  }
+  return 0;
+}
+
 int or_resolve(const or_world* o, const or_look* lk, const uint64_t* vis, const float* sun_vis, float* rgba,
                uint64_t pix_begin, uint64_t pix_end, int threads) {
   World w = mk(o);

@@ -316,7 +316,7 @@ def test_resolve_rejects_unbuilt_variants(small):
         m.upload_view(v)
         m.render()
         with pytest.raises(RuntimeError):
-            m.resolve(LK.HI_DEFAULT)
+            m.resolve(LK.HI_DEFAULT)          # a heat map needs the engine passes' iteration counts
     finally:
         m.close()
 
@@ -348,6 +348,30 @@ def test_underwater_resolve_matches_the_oracle(small, snell):
     want = o.resolve(vis, LK.sun_visibility(sh), *look, spec_hi=LK.HI_DEFAULT)
     within(got, want, f"underwater, snell {snell}")
     assert (vis == 0).any() and (vis != 0).any()
+
+
+@pytest.mark.gpu
+def test_heat_map_view_matches_the_oracle(small):
+    """FLAG_HEATMAP (resolve.wgsl:36-44,1389-1394): after the engine passes
+    (tile_select, march), every pixel's colour is heat(iterations / 300)."""
+    from voxelcraft_menu_b200.march import Marcher
+    w, pools = small
+    v = w.view(W.small_terrain_camera(width=320, height=180, flags=W.FLAG_HEATMAP))
+    m = Marcher(320, 180)
+    try:
+        m.upload_world(*pools)
+        m.upload_view(v)
+        m.select()
+        m.march()
+        m.resolve(0)
+        got = m.read_color()
+        it = m.read_heatmap()
+    finally:
+        m.close()
+    o = Oracle(v, *pools)
+    assert np.array_equal(it, o.frame_vis(heat=True)[3])
+    assert it.max() > 0
+    within(got, o.resolve_heat(it), "heat map")
 
 
 @pytest.mark.gpu

@@ -52,6 +52,7 @@ struct vm_ctx {
   bool chunks_foliage = false;   // a chunk of the uploaded list holds tufts (VM_ATTR_HAS_FOLIAGE)
   bool batch_foliage = false;    // the same for the batch's chunk lists
   bool have_probes = false, have_shaft = false, color_done = false;
+  bool heat_valid = false;   // dbg holds the iteration counts of this frame's vm_select / vm_march
   // the resolve's water and glass lanes run beside the sky / opaque lanes:
   // three streams forked from the context's stream and joined back by events
   cudaStream_t lane_stream[3] = {nullptr, nullptr, nullptr};
@@ -227,6 +228,7 @@ int prepare_reflect(vm_ctx* ctx) {
 int enqueue_render(vm_ctx* ctx, bool count, const cudaEvent_t* ev = nullptr) {
   ctx->mask_valid = false;
   ctx->color_done = false;
+  ctx->heat_valid = false;
   const vm_frame& f = ctx->frame;
   // buffers are grown before any of their pointers is taken below
   int rc;
@@ -423,6 +425,7 @@ int vm_set_frame(vm_ctx* ctx, const vm_frame* frame) {
   if (!ctx || !frame) return VM_E_INVALID;
   ctx->frame = *frame;
   ctx->have_frame = true;
+  ctx->heat_valid = false;
   return VM_OK;
 }
 
@@ -468,6 +471,7 @@ int vm_select(vm_ctx* ctx) {
   if ((rc = ensure(ctx, ctx->pairs, (size_t)f.max_pairs * 2 * 4))) return rc;
   CK(cudaMemsetAsync(ctx->vis.p, 0, npix * 8, ctx->stream));
   CK(cudaMemsetAsync(ctx->counters.p, 0, 32, ctx->stream));
+  ctx->heat_valid = false;
   if (f.flags & VM_FLAG_HEATMAP) CK(cudaMemsetAsync(ctx->dbg.p, 0, npix * 4, ctx->stream));
   if (!(f.flags & VM_FLAG_HIZ)) CK(cudaMemsetAsync(ctx->hiz.p, 0, tiles * 4, ctx->stream));
   const vmd::DevWorld w = dev_world(ctx);
@@ -496,6 +500,7 @@ int vm_march(vm_ctx* ctx) {
     CK(vmk::launch_finalize(f, ctr, true, ctx->stream));
     CK(vmk::launch_march_pairs(f, w, pairs, ctr, vis, dbg, ctx->sms, ctx->stream));
   }
+  ctx->heat_valid = dbg != nullptr;
   return VM_OK;
 }
 
@@ -1102,8 +1107,18 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
   const size_t npix = (size_t)f.res[0] * f.res[1];
   if (!ctx->vis.p || ctx->vis.bytes < npix * 8 || !ctx->shadow.p)
     return fail(ctx, VM_E_NOT_READY, "no rendered frame to resolve");
+  if (f.flags & VM_FLAG_HEATMAP) {
+    // the engine's heat-map view (resolve.wgsl:1389-1394): the iteration
+    // counts its march summed per pixel, which vm_select / vm_march keep
+    if (!ctx->heat_valid)
+      return fail(ctx, VM_E_NOT_READY, "a heat-map frame resolves the iteration counts of vm_select / vm_march");
+    CK(cudaSetDevice(ctx->device));
+    if ((rc = ensure(ctx, ctx->color, npix * 16))) return rc;
+    CK(vmk::launch_resolve_heat(f, (const uint32_t*)ctx->dbg.p, (float4*)ctx->color.p, ctx->stream));
+    ctx->color_done = true;
+    return VM_OK;
+  }
   if (!ctx->atlas_layers || !ctx->n_faces) return fail(ctx, VM_E_NOT_READY, "no atlas / block faces uploaded");
-  if (f.flags & VM_FLAG_HEATMAP) return fail(ctx, VM_E_INVALID, "resolve of heat-map frames is not built");
   if (spec_hi & HI_UNBUILT)
     return fail(ctx, VM_E_INVALID, "spec_hi 0x%x: the water look and surface debug views are not built",
                 spec_hi & HI_UNBUILT);

@@ -148,6 +148,9 @@ cudaError_t launch_resolve(const vm_frame& f, const vmd::DevWorld& w, const vmd:
                            uint16_t* leg_refr, uint16_t* leg_refl, uint8_t* lane, uint32_t* lists, float* light_ao,
                            float4* fog, float4* out, int sms, cudaStream_t s, const cudaStream_t lane_stream[3],
                            const cudaEvent_t lane_event[4]);
+// the heat map of a FLAG_HEATMAP frame (resolve.wgsl:36-44,1389-1394) from
+// the iteration counts the engine passes' march summed per pixel
+cudaError_t launch_resolve_heat(const vm_frame& f, const uint32_t* dbg, float4* out, cudaStream_t s);
 cudaError_t launch_expand(const vm_frame& f, const vmd::DevWorld& w, const unsigned long long* vis,
                           int32_t wx, int32_t wy, int32_t wz, uint32_t dx, uint32_t dy, uint32_t dz,
                           uint32_t* voxel, uint8_t* face, float* t, cudaStream_t s);

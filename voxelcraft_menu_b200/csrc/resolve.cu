@@ -902,6 +902,24 @@ __global__ void __launch_bounds__(256) k_resolve_blend(const __grid_constant__ v
   out[pix] = make_float4(color.x, color.y, color.z, 1.0f);
 }
 
+// heat (resolve.wgsl:36-44): the iteration heat map of a FLAG_HEATMAP frame
+// (resolve.wgsl:1389-1394), every pixel's summed march iterations / 300.
+__global__ void __launch_bounds__(256) k_resolve_heat(const __grid_constant__ vm_frame f,
+                                                      const uint32_t* __restrict__ dbg, float4* __restrict__ out) {
+  const uint32_t pix = blockIdx.x * 256u + threadIdx.x;
+  if (pix >= f.res[0] * f.res[1]) return;
+  const float t = clampf((float)dbg[pix] / 300.0f, 0.0f, 1.0f);
+  const F3 c = {smoothstep(0.35f, 0.85f, t), smoothstep(0.0f, 0.45f, t) - smoothstep(0.65f, 1.0f, t),
+                1.0f - smoothstep(0.0f, 0.45f, t)};
+  out[pix] = make_float4(wpow(c.x, 2.2f), wpow(c.y, 2.2f), wpow(c.z, 2.2f), 1.0f);
+}
+
+cudaError_t launch_resolve_heat(const vm_frame& f, const uint32_t* dbg, float4* out, cudaStream_t s) {
+  const uint32_t npix = f.res[0] * f.res[1];
+  k_resolve_heat<<<(npix + 255u) / 256u, 256, 0, s>>>(f, dbg, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, const unsigned long long* vis,
                            const float* mask, const float* dist, bool soft_rays, uint32_t water_sec_shift,
                            uint16_t* leg_refr, uint16_t* leg_refl, uint8_t* lane, uint32_t* lists, float* light_ao,
