@@ -2578,7 +2578,23 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
 }
 
 // ---- the water and glass lanes: resolve.wgsl:896-1320 ----------------------
-constexpr uint32_t HI_SHORE_FOAM = 16u, HI_WATER_SEC = 32u, HI_GLASS_REFLECT = 128u;
+constexpr uint32_t HI_SHORE_FOAM = 16u, HI_WATER_SEC = 32u, HI_GLASS_REFLECT = 128u, HI_WATER_LOOK = 4096u;
+constexpr float WATER_LOOK_RIPPLE_AMP = 0.16f;
+
+// look_ripple: resolve.wgsl:995-1008
+void look_ripple(const World& w, float px, float pz, float time, float w1, float w2, float& gx, float& gz) {
+  const float d1x = 0.86f, d1z = 0.51f, d2x = -0.42f, d2z = 0.91f;
+  const float k1 = (float)(6.2832 / 1.15), k2 = (float)(6.2832 / 0.62);
+  float ph_x = 0.0f, ph_z = 0.0f;
+  if ((w.spec & VM_SPEC_WATER_REPAIR) != 0u) {
+    ph_x = sinf(px * 0.071f + pz * 0.113f) * 2.0f;
+    ph_z = sinf(px * -0.097f + pz * 0.053f + 1.9f) * 2.0f;
+  }
+  float a1 = cosf((px * d1x + pz * d1z) * k1 + time * 1.7f + ph_x) * w1;
+  float a2 = cosf((px * d2x + pz * d2z) * k2 - time * 2.3f + ph_z) * w2;
+  gx = d1x * a1 + d2x * a2;
+  gz = d1z * a1 + d2z * a2;
+}
 
 inline bool secondary_smooth(const vm_frame& f) { return (f.flags & VM_FLAG_FLAT_SECONDARY) == 0u; }
 float medium_light(const vm_frame& f, uint32_t packed) {
@@ -2652,6 +2668,17 @@ WaterCtx water_ctx(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t ni
     nt = normalize(v3(-(wf.x * lim), 1.0f, -(wf.y * lim)));
     gloss = 1.0f / (1.0f + 0.5f * 320.0f * wf.z);
   }
+  if ((L.spec_hi & HI_WATER_LOOK) != 0u && nid == VM_NORMAL_PY) {   // resolve.wgsl:1138-1153
+    float pix = px_world / fmaxf(fabsf(rd.y), 1e-3f);
+    float range_gate = (1.0f - smoothstep(48.0f, 96.0f, t)) * smoothstep(0.08f, 0.20f, fabsf(rd.y));
+    float fade_115 = range_gate * smoothstep(2.0f, 4.0f, 1.15f / fmaxf(pix, 1e-4f));
+    float fade_62 = range_gate * smoothstep(2.0f, 4.0f, 0.62f / fmaxf(pix, 1e-4f));
+    unresolved += WATER_LOOK_RIPPLE_AMP * WATER_LOOK_RIPPLE_AMP * 0.5f *
+                  (0.36f * (1.0f - fade_115 * fade_115) + 0.16f * (1.0f - fade_62 * fade_62));
+    float gx, gz;
+    look_ripple(w, hit.x, hit.z, f.time * f.wave_speed, 0.60f * fade_115, 0.40f * fade_62, gx, gz);
+    nw = normalize(add(nw, muls(v3(gx, 0.0f, gz), WATER_LOOK_RIPPLE_AMP)));
+  }
   float rough = clampf(1.0f - expf(-8.0f * unresolved), 0.0f, 1.0f);
   nw = normalize(add(muls(nw, 1.0f - rough), muls(n, rough)));
   nt = normalize(add(muls(nt, 1.0f - rough), muls(n, rough)));
@@ -2714,6 +2741,12 @@ V3 water_compose(const vm_frame& f, const Look& L, const WaterCtx& x, F4 leg_r, 
   if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && x.refract_detail > 0.0f) {
     refr = mixv(refr, water_medium(f, v3(leg_r.r, leg_r.g, leg_r.b), leg_r.a, x.body), x.refract_detail);
     column_depth = leg_r.a;
+  }
+  if ((L.spec_hi & HI_WATER_LOOK) != 0u && x.refract_detail > 0.0f) {   // resolve.wgsl:1178-1183
+    float depth_f = clampf(column_depth / 7.0f, 0.0f, 1.0f);
+    refr = mul(refr, mixv(v3(1.0f, 1.0f, 1.0f), v3(0.82f, 0.90f, 0.70f), depth_f));
+    float shall = 1.0f - smoothstep(0.0f, 2.0f, column_depth);
+    refr = mixv(refr, muls(v3(0.55f, 0.74f, 0.68f), x.ml), shall * 0.45f * x.refract_detail);
   }
   if ((L.spec_hi & HI_SHORE_FOAM) != 0u && x.refract_detail > 0.0f && column_depth < 2.5f) {
     float shall = 1.0f - smoothstep(0.0f, 2.5f, column_depth);

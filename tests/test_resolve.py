@@ -235,7 +235,7 @@ def gpu_resolve(v, pools, look, spec_hi, soften=None, spec=None):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["default", "engine_atlas", "probes_shaft", "plain_flags", "legacy_lighting",
-                                  "reflect_legs", "per_pixel_legs", "probe_tap", "probe_ambient"])
+                                  "reflect_legs", "per_pixel_legs", "probe_tap", "probe_ambient", "water_look"])
 def test_resolve_matches_the_oracle(small, case):
     w, pools = small
     cam = look_camera()
@@ -257,6 +257,11 @@ def test_resolve_matches_the_oracle(small, case):
         v.frame.flags |= W.FLAG_WATER_REFLECT
         v.frame.flags &= ~LK.FLAG_FLAT_SECONDARY
         spec_hi = LK.HI_DEFAULT & ~LK.HI_WATER_SEC
+    elif case == "water_look":
+        # SPEC_WATER_LOOK (resolve.wgsl:995-1008,1138-1153,1178-1183): ripples on
+        # the mirror normal, murk and a shallow tint in the refracted colour
+        v.frame.flags |= W.FLAG_WAVES
+        spec_hi = LK.HI_DEFAULT | LK.HI_WATER_LOOK
     elif case in ("probe_tap", "probe_ambient"):
         # SPEC_PROBE_TAP / SPEC_PROBE_AMBIENT (resolve.wgsl:500-505): the probe
         # field through the clamped linear sampler scales, or replaces, the ambient
@@ -309,7 +314,7 @@ def test_resolve_rejects_unbuilt_variants(small):
         with pytest.raises(RuntimeError):
             m.read_color()                                # no resolve yet
         with pytest.raises(RuntimeError):
-            m.resolve(LK.HI_DEFAULT | LK.HI_WATER_LOOK)
+            m.resolve(LK.HI_DEFAULT | (1 << 23))          # a surface debug view
         m.resolve(LK.HI_DEFAULT)
         assert m.read_color().shape == (64 * 36, 4)
         v.frame.flags |= W.FLAG_HEATMAP

@@ -254,7 +254,24 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
 // ---------------------------------------------------------------------------
 // the water and glass lanes: resolve.wgsl:896-1320
 
-constexpr uint32_t HI_SHORE_FOAM = 16u, HI_WATER_SEC = 32u, HI_GLASS_REFLECT = 128u;
+constexpr uint32_t HI_SHORE_FOAM = 16u, HI_WATER_SEC = 32u, HI_GLASS_REFLECT = 128u, HI_WATER_LOOK = 4096u;
+constexpr float WATER_LOOK_RIPPLE_AMP = 0.16f;
+
+// look_ripple: resolve.wgsl:995-1008, the water look's two short ripples
+// (gradient), phase-warped under SPEC_WATER_REPAIR
+static __device__ __noinline__ float2 look_ripple(const DevWorld& w, float px, float pz, float time, float w1,
+                                                  float w2) {
+  const float d1x = 0.86f, d1z = 0.51f, d2x = -0.42f, d2z = 0.91f;
+  const float k1 = (float)(6.2832 / 1.15), k2 = (float)(6.2832 / 0.62);   // abstract-float constants, folded first
+  float ph_x = 0.0f, ph_z = 0.0f;
+  if ((w.spec & VM_SPEC_WATER_REPAIR) != 0u) {
+    ph_x = sinf(px * 0.071f + pz * 0.113f) * 2.0f;
+    ph_z = sinf(px * -0.097f + pz * 0.053f + 1.9f) * 2.0f;
+  }
+  const float a1 = cosf((px * d1x + pz * d1z) * k1 + time * 1.7f + ph_x) * w1;
+  const float a2 = cosf((px * d2x + pz * d2z) * k2 - time * 2.3f + ph_z) * w2;
+  return make_float2(d1x * a1 + d2x * a2, d1z * a1 + d2z * a2);
+}
 constexpr float WATER_SHADOW_DIST = 16.0f;    // SPEC_WATER_SHADOW_DIST
 constexpr float GLASS_SHADOW_DIST = 48.0f;
 
@@ -338,6 +355,18 @@ static __device__ __noinline__ WaterCtx water_ctx(const DevWorld& w, const vm_fr
     const float lim = fminf(1.0f, f.wave_reflect_slope / fmaxf(gl, 1e-6f));
     nt = unit(f3(-(wf.x * lim), 1.0f, -(wf.y * lim)));
     gloss = wdiv(1.0f, 1.0f + 0.5f * 320.0f * wf.z);
+  }
+  if ((L.spec_hi & HI_WATER_LOOK) != 0u && nid == VM_NORMAL_PY) {
+    // SPEC_WATER_LOOK (resolve.wgsl:1138-1153): sub-pixel ripples on the
+    // mirror normal, their unresolved part added to the optical roughness
+    const float pix = px_world / fmaxf(fabsf(rd.y), WAVE_GRAZE_MIN);
+    const float range_gate = (1.0f - smoothstep(48.0f, 96.0f, t)) * smoothstep(0.08f, 0.20f, fabsf(rd.y));
+    const float fade_115 = range_gate * smoothstep(2.0f, 4.0f, 1.15f / fmaxf(pix, 1e-4f));
+    const float fade_62 = range_gate * smoothstep(2.0f, 4.0f, 0.62f / fmaxf(pix, 1e-4f));
+    unresolved += WATER_LOOK_RIPPLE_AMP * WATER_LOOK_RIPPLE_AMP * 0.5f *
+                  (0.36f * (1.0f - fade_115 * fade_115) + 0.16f * (1.0f - fade_62 * fade_62));
+    const float2 rp = look_ripple(w, hit.x, hit.z, f.time * f.wave_speed, 0.60f * fade_115, 0.40f * fade_62);
+    nw = unit(nw + f3(rp.x, 0.0f, rp.y) * WATER_LOOK_RIPPLE_AMP);
   }
   const float rough = clampf(1.0f - wexp(-8.0f * unresolved), 0.0f, 1.0f);
   nw = unit(nw * (1.0f - rough) + n * rough);
@@ -467,6 +496,13 @@ static __device__ __noinline__ F3 water_compose(const vm_frame& f, const Look& L
   if ((f.flags & VM_FLAG_WATER_REFRACT) != 0u && x.refract_detail > 0.0f) {
     refr = mix3(refr, water_medium(f, f3(leg_r.x, leg_r.y, leg_r.z), leg_r.w, x.body), x.refract_detail);
     column_depth = leg_r.w;
+  }
+  if ((L.spec_hi & HI_WATER_LOOK) != 0u && x.refract_detail > 0.0f) {
+    // SPEC_WATER_LOOK (resolve.wgsl:1178-1183): murk with depth, a shallow tint
+    const float depth_f = clampf(wdiv(column_depth, 7.0f), 0.0f, 1.0f);
+    refr = refr * mix3(f3(1.0f, 1.0f, 1.0f), f3(0.82f, 0.90f, 0.70f), depth_f);
+    const float shall = 1.0f - wsmooth(0.0f, 2.0f, column_depth);
+    refr = mix3(refr, f3(0.55f, 0.74f, 0.68f) * x.ml, shall * 0.45f * x.refract_detail);
   }
   if ((L.spec_hi & HI_SHORE_FOAM) != 0u && x.refract_detail > 0.0f && column_depth < 2.5f) {
     const float shall = 1.0f - wsmooth(0.0f, 2.5f, column_depth);
