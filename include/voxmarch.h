@@ -198,8 +198,9 @@ int vm_read_water_sec(vm_ctx* ctx, uint64_t* refr_key, float* refr_t, uint64_t* 
  * WATER_SEC, CAUSTICS, GLASS_REFLECT, TINT_BALANCE, SKY_LOOK, SKY_COOL,
  * FOLIAGE_RICH, CANOPY_RELIEF, LEGACY_LIGHTING are read; COMPACT_SHADE_HIT
  * is accepted and gives the same colours (the compact shade_hit reorders the
- * legacy one's statements); WATER_LOOK is read; the surface debug views
- * return VM_E_INVALID; a FLAG_HEATMAP frame resolves to the heat map of the
+ * legacy one's statements); WATER_LOOK and the surface debug views
+ * (DEBUG_A..C, SURFACE_DEBUG = spec_hi >> 23 & 7) are read; a FLAG_HEATMAP
+ * frame resolves to the heat map of the
  * iteration counts of vm_select / vm_march, VM_E_NOT_READY without them).
  * The frame flags give the rest
  * (AO, TINT, TEX_VARIATION, DISTANT_SHADOWS, TERRAIN_SHAFTS, FLAT_SECONDARY,

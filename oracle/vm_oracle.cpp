@@ -1832,6 +1832,8 @@ inline V3 mixv(V3 a, V3 b, float t) { return {mixs(a.x, b.x, t), mixs(a.y, b.y, 
 inline float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
 inline bool cool(const Look& L) { return (L.spec_hi & HI_SKY_COOL) != 0u; }
 inline bool repair(const Look& L) { return (L.spec_hi & HI_LEGACY_LIGHTING) == 0u; }
+// SURFACE_DEBUG = (spec_hi >> 23) & 7 (FLAG_HI_DEBUG_A..C, mod.rs make_spec)
+inline uint32_t surface_debug(const Look& L) { return (L.spec_hi >> 23) & 7u; }
 const V3 SCATTER_TINT = {1.0000f, 0.4770f, 0.1474f};
 
 // transmittance_from: common.wgsl:1332-1341
@@ -2520,7 +2522,7 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
   const bool probe_ambient = (f.flags & VM_FLAG_PROBE_AMBIENT) != 0u;
   if (probe_ambient) amb = probe_tap(L, hit);
   else if ((f.flags & VM_FLAG_PROBE_TAP) != 0u) amb = mul(amb, probe_tap(L, hit));
-  float direct = 0.0f;
+  float direct = 0.0f, visibility = 1.0f;
   float ndl = dot(n, sun);
   if (ndl > 0.0f && f.daylight > 0.01f) {
     float lit = 1.0f;
@@ -2533,6 +2535,7 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
       float cloud_fp = fmaxf(dist, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
       lit = lit * cloud_shade(f, hit, cloud_fp);
     }
+    visibility = lit;
     direct = lit * ndl * sky_sm;
     if ((L.spec_hi & HI_CAUSTICS) != 0u) {
       float cdepth = f.sea_level - hit.y;
@@ -2570,6 +2573,11 @@ V3 shade_hit(const World& w, const Look& L, uint32_t ci, U3 v, uint32_t id, uint
       floor_rgb = add(floor_rgb, muls(mul(v3(0.85f, 0.90f, 1.00f), prgb), gain * sky_sm));
     }
   }
+  uint32_t debug_view = surface_debug(L);   // resolve.wgsl:579-582
+  if (debug_view == 1u) return add(muls(n, 0.5f), v3(0.5f, 0.5f, 0.5f));
+  if (debug_view == 2u) return v3(visibility, visibility, visibility);
+  if (debug_view == 3u) return sun_rgb;
+  if (debug_view == 4u) return add(muls(ambient_rgb, ao), floor_rgb);
   V3 spec_rgb = muls(spec_pre, sky_sm * 0.5f);
   V3 light = repair(L) ? add(add(muls(muls(ambient_rgb, ao), shade), sun_rgb), floor_rgb)
                        : muls(add(muls(add(ambient_rgb, sun_rgb), ao), floor_rgb), shade);
@@ -2759,6 +2767,10 @@ V3 water_compose(const vm_frame& f, const Look& L, const WaterCtx& x, F4 leg_r, 
                      powf(fmaxf(dot(x.mirror, ld3(f.sun_dir)), 0.0f), 320.0f * x.gloss) * 2.5f * x.gloss * f.daylight));
   if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f && leg_m.a > 0.0f)
     refl = mixv(refl, v3(leg_m.r, leg_m.g, leg_m.b), x.reflect_detail);
+  uint32_t debug_view = surface_debug(L);   // resolve.wgsl:1200-1202
+  if (debug_view == 5u) return add(muls(x.n, 0.5f), v3(0.5f, 0.5f, 0.5f));
+  if (debug_view == 6u) return refl;
+  if (debug_view == 7u) return refr;
   refl = mixv(refl, sky_base(f, L, x.n, 1.0f), x.roughness * 0.65f);
   return mixv(refr, refl, schlick_f0(0.02f, fmaxf(-dot(x.rd, x.nw), 1e-3f)));
 }
@@ -3030,12 +3042,12 @@ int or_resolve(const or_world* o, const or_look* lk, const uint64_t* vis, const 
         color = shade_hit(w, L, ci, v, id, nid, hit, rd, t, f.shadow_dist, true, true, sun_vis[pix]);
       }
       dist = t;
-      float wet = underwater ? water_path(f, t, rd) : 0.0f;
+      float wet = underwater && surface_debug(L) == 0u ? water_path(f, t, rd) : 0.0f;
       float alpha = 1.0f - transmittance_from(f, cam.y + wet * rd.y, t - wet, rd);
       float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, t, alpha, px, py);
-      color = mixv(color, sky_base(f, L, rd, shaft), alpha);
+      if (surface_debug(L) == 0u) color = mixv(color, sky_base(f, L, rd, shaft), alpha);
     }
-    if (underwater) {
+    if (underwater && surface_debug(L) == 0u) {
       color = surface_from_below(w, color, rd, dist);
       color = water_medium(f, color, water_path(f, dist, rd), underwater_body(w));
     }

@@ -313,8 +313,6 @@ def test_resolve_rejects_unbuilt_variants(small):
         m.upload_look(LK.atlas(1), LK.block_faces())
         with pytest.raises(RuntimeError):
             m.read_color()                                # no resolve yet
-        with pytest.raises(RuntimeError):
-            m.resolve(LK.HI_DEFAULT | (1 << 23))          # a surface debug view
         m.resolve(LK.HI_DEFAULT)
         assert m.read_color().shape == (64 * 36, 4)
         v.frame.flags |= W.FLAG_HEATMAP
@@ -377,6 +375,24 @@ def test_heat_map_view_matches_the_oracle(small):
     assert np.array_equal(it, o.frame_vis(heat=True)[3])
     assert it.max() > 0
     within(got, o.resolve_heat(it), "heat map")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("view", range(1, 8))
+def test_surface_debug_views_match_the_oracle(small, view):
+    """SURFACE_DEBUG = (FLAG_HI_* >> 23) & 7 (resolve.wgsl:579-582,1200-1202,
+    1449-1464): 1 normal, 2 sun visibility, 3 sun, 4 ambient of the surface
+    lanes, 5 normal, 6 reflected, 7 refracted colour of the water lane, no
+    fog blend."""
+    w, pools = small
+    v = look_view(w, look_camera())
+    v.frame.flags |= W.FLAG_WAVES
+    look = (LK.atlas(1), LK.block_faces(), LK.probe_field(5),
+            LK.shaft_envelope(w.recipe, v.frame.sun_dir, v.frame.shaft_origin, 4.0))
+    hi = LK.HI_DEFAULT | (view << 23)
+    vis, sh, _, got = gpu_resolve(v, pools, look, hi)
+    want = Oracle(v, *pools).resolve(vis, LK.sun_visibility(sh), *look, spec_hi=hi)
+    within(got, want, f"debug view {view}")
 
 
 @pytest.mark.gpu

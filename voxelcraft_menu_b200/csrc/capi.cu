@@ -1008,7 +1008,6 @@ float srgb_decode(uint8_t u) {
 // runs shade_hit_legacy(_cached)'s statements with the material block after
 // the light block (the light times face_scale = 1.0, the canopy relief from
 // the same n . sun), so its colours are the legacy variant's bit for bit.
-constexpr uint32_t HI_UNBUILT = 8388608u | 16777216u | 33554432u;   // the surface debug views
 constexpr uint32_t HI_WATER_SEC = 32u;
 constexpr uint32_t WATER_SEC_SHIFT = 1u;   // WATER_SEC_SHIFT of the engine's default water_sec_scale 2
 
@@ -1119,9 +1118,7 @@ int vm_resolve(vm_ctx* ctx, uint32_t spec_hi) {
     return VM_OK;
   }
   if (!ctx->atlas_layers || !ctx->n_faces) return fail(ctx, VM_E_NOT_READY, "no atlas / block faces uploaded");
-  if (spec_hi & HI_UNBUILT)
-    return fail(ctx, VM_E_INVALID, "spec_hi 0x%x: the surface debug views are not built",
-                spec_hi & HI_UNBUILT);
+
   CK(cudaSetDevice(ctx->device));
   if ((rc = ensure(ctx, ctx->color, npix * 16)) || (rc = ensure(ctx, ctx->light_ao, npix * 4)) ||
       (rc = ensure(ctx, ctx->lane, npix)) || (rc = ensure(ctx, ctx->lane_lists, npix * 8 + 8)) ||

@@ -191,7 +191,7 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
   const bool probe_ambient = (f.flags & VM_FLAG_PROBE_AMBIENT) != 0u;
   if (probe_ambient) amb = probe_tap(L, hit);
   else if ((f.flags & VM_FLAG_PROBE_TAP) != 0u) amb = amb * probe_tap(L, hit);
-  float direct = 0.0f;
+  float direct = 0.0f, visibility = 1.0f;
   const float ndl = dot(n, sun);
   if (ndl > 0.0f && f.daylight > 0.01f) {
     float lit = 1.0f;
@@ -204,6 +204,7 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
       const float cloud_fp = fmaxf(dist, 1e-3f) * 2.0f * f.tan_half_fov / (float)f.res[1] * exp2f(f.mip_bias);
       lit = lit * cloud_shade(f, hit, cloud_fp);
     }
+    visibility = lit;
     direct = lit * ndl * sky_sm;
     if ((L.spec_hi & HI_CAUSTICS) != 0u) {
       const float cdepth = f.sea_level - hit.y;
@@ -242,6 +243,12 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
       floor_rgb = floor_rgb + f3(0.85f, 0.90f, 1.00f) * probe_rgb * (gain * sky_sm);
     }
   }
+  // SURFACE_DEBUG 1-4 (resolve.wgsl:579-582): normal, sun visibility, sun, ambient
+  const uint32_t debug_view = surface_debug(L);
+  if (debug_view == 1u) return add_s(n * 0.5f, 0.5f);
+  if (debug_view == 2u) return f3(visibility, visibility, visibility);
+  if (debug_view == 3u) return sun_rgb;
+  if (debug_view == 4u) return ambient_rgb * ao + floor_rgb;
   const F3 spec_rgb = spec_pre * (sky_sm * 0.5f);
   // surface_light / surface_radiance: resolve.wgsl:7-17
   const F3 light = repair ? ambient_rgb * ao * shade + sun_rgb + floor_rgb
@@ -516,6 +523,11 @@ static __device__ __noinline__ F3 water_compose(const vm_frame& f, const Look& L
                 (wpow(fmaxf(dot(x.mirror, sun), 0.0f), 320.0f * x.gloss) * 2.5f * x.gloss * f.daylight);
   if ((f.flags & VM_FLAG_WATER_REFLECT) != 0u && x.reflect_detail > 0.0f && leg_m.w > 0.0f)
     refl = mix3(refl, f3(leg_m.x, leg_m.y, leg_m.z), x.reflect_detail);
+  // SURFACE_DEBUG 5-7 (resolve.wgsl:1200-1202): water normal, reflected, refracted
+  const uint32_t debug_view = surface_debug(L);
+  if (debug_view == 5u) return add_s(x.n * 0.5f, 0.5f);
+  if (debug_view == 6u) return refl;
+  if (debug_view == 7u) return refr;
   refl = mix3(refl, sky_base(f, L, x.n, 1.0f), x.roughness * 0.65f);
   return mix3(refr, refl, schlick_f0(0.02f, fmaxf(-dot(x.rd, x.nw), 1e-3f)));
 }
@@ -848,7 +860,7 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
   if (PART == 1) {
     const float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
     color = sky_color(f, L, cam, rd, 0.0f, shaft);
-    if (underwater) color = underwater_tail(w, f, color, rd, f.far_);
+    if (underwater && surface_debug(L) == 0u) color = underwater_tail(w, f, color, rd, f.far_);
   } else {
     const uint32_t nid = (uint32_t)(key >> 37) & 7u;
     const uint32_t ci = (uint32_t)(key >> 24) & 0x1FFFu;
@@ -878,7 +890,7 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
         color = shade_water(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
       }
     }
-    if (PART == 0) {   // water: the fog blend follows (k_resolve_blend)
+    if (PART == 0 && surface_debug(L) == 0u) {   // water: the fog blend follows (k_resolve_blend)
       const float wet = underwater ? water_path(f, t, rd) : 0.0f;
       const float alpha = 1.0f - transmittance_from(f, cam.y + wet * rd.y, t - wet, rd);
       const float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, t, alpha, px, py);
@@ -996,14 +1008,15 @@ cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, 
   if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, lane, out, light_ao);
   k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, light_ao, out);
   k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
-  k_resolve_fog<<<grid, block, 0, s>>>(f, w, L, vis, lane, fog);
+  const bool blend = surface_debug(L) == 0u;   // the debug views skip the fog and the underwater tail
+  if (blend) k_resolve_fog<<<grid, block, 0, s>>>(f, w, L, vis, lane, fog);
   e = cudaGetLastError();
   for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
     e = cudaEventRecord(lane_event[1 + i], lane_stream[i]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, lane_event[1 + i], 0);
   }
   if (e != cudaSuccess) return e;
-  k_resolve_blend<<<(npix + 255u) / 256u, 256, 0, s>>>(f, w, vis, lane, fog, out);
+  if (blend) k_resolve_blend<<<(npix + 255u) / 256u, 256, 0, s>>>(f, w, vis, lane, fog, out);
   return cudaGetLastError();
 }
 

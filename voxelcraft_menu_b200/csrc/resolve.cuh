@@ -445,6 +445,8 @@ __device__ __forceinline__ F3 sky_ambient_tint(const vm_frame& f, const Look& L,
   return t * wdiv(0.70721556f, fmaxf(luma, 1e-6f));
 }
 __device__ __forceinline__ bool lighting_repair(const Look& L) { return (L.spec_hi & HI_LEGACY_LIGHTING) == 0u; }
+// SURFACE_DEBUG: (spec_hi >> 23) & 7 (FLAG_HI_DEBUG_A..C, mod.rs make_spec)
+__host__ __device__ __forceinline__ uint32_t surface_debug(const Look& L) { return (L.spec_hi >> 23) & 7u; }
 static __device__ __noinline__ F3 surface_sky_fill(const vm_frame& f, const Look& L, F3 n) {
   const F3 sky = sky_ambient_tint(f, L, n);
   if (!lighting_repair(L)) return sky;
