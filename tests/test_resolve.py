@@ -181,6 +181,30 @@ def test_oracle_sky_without_clouds_is_sky_base(small):
         assert np.allclose(c[pix, :3], col, rtol=2e-4, atol=2e-6), pix   # float32 rd . sun at the disk edge
 
 
+def test_oracle_heat_map_and_debug_view_properties(small):
+    """heat (resolve.wgsl:36-44): no iterations -> blue, 300 or more -> red;
+    SURFACE_DEBUG 1 (resolve.wgsl:579): n * 0.5 + 0.5 without the fog blend,
+    so a +Y face reads (0.5, 1, 0.5) and the sky keeps its colour."""
+    w, pools = small
+    v = look_view(w, look_camera(64, 36, pitch=math.radians(-30.0)))
+    o = Oracle(v, *pools)
+    heat = o.resolve_heat(np.array([0, 150, 300, 5000] + [0] * (o.npix - 4), np.uint32))
+    assert np.allclose(heat[0], [0.0, 0.0, 1.0, 1.0]) and np.allclose(heat[2], [1.0, 0.0, 0.0, 1.0])
+    assert np.array_equal(heat[2], heat[3]) and 0.0 < heat[1, 1] <= 1.0
+    vis = o.frame_vis()[0]
+    sv = np.ones(o.npix, np.float32)
+    look = (LK.atlas(1), LK.block_faces())
+    dbg = o.resolve(vis, sv, *look, spec_hi=LK.HI_DEFAULT | (1 << 23))
+    plain = o.resolve(vis, sv, *look, spec_hi=LK.HI_DEFAULT)
+    top = (vis != 0) & (((vis >> np.uint64(37)) & np.uint64(7)) == 3)    # +Y faces (NORMAL_PY)
+    blocks = np.array([o.block_at((int(k) >> 24) & 0x1FFF, [(int(k) >> 16) & 63, (int(k) >> 8) & 63, int(k) & 63])
+                       for k in vis[top]])
+    dry = np.flatnonzero(top)[(blocks != 13) & (blocks != 10)]
+    assert dry.size > 100
+    assert np.allclose(dbg[dry, :3], [0.5, 1.0, 0.5])
+    assert np.array_equal(dbg[vis == 0], plain[vis == 0])
+
+
 # ---------------------------------------------------------------- GPU -----
 
 def light_bricks(v, bricks, seed):
