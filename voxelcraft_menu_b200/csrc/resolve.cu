@@ -130,6 +130,7 @@ static __device__ __noinline__ LightTerms surface_light_terms(const DevWorld& w,
   return {amb, sky_sm, ao};
 }
 
+template <bool EXTRA>
 __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx,
                                          uint32_t vy, uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist,
                                          float shadow_dist, bool smooth, bool do_spec, float lit_in,
@@ -188,9 +189,9 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
   const float sky_sm = lt.sky_sm, ao = lt.ao;
   // SPEC_PROBE_AMBIENT / SPEC_PROBE_TAP (resolve.wgsl:500-505): the ambient
   // from the probe tap alone (the light words' ambient unused), or scaled by it
-  const bool probe_ambient = (f.flags & VM_FLAG_PROBE_AMBIENT) != 0u;
+  const bool probe_ambient = EXTRA && (f.flags & VM_FLAG_PROBE_AMBIENT) != 0u;
   if (probe_ambient) amb = probe_tap(L, hit);
-  else if ((f.flags & VM_FLAG_PROBE_TAP) != 0u) amb = amb * probe_tap(L, hit);
+  else if (EXTRA && (f.flags & VM_FLAG_PROBE_TAP) != 0u) amb = amb * probe_tap(L, hit);
   float direct = 0.0f, visibility = 1.0f;
   const float ndl = dot(n, sun);
   if (ndl > 0.0f && f.daylight > 0.01f) {
@@ -244,11 +245,13 @@ __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, c
     }
   }
   // SURFACE_DEBUG 1-4 (resolve.wgsl:579-582): normal, sun visibility, sun, ambient
-  const uint32_t debug_view = surface_debug(L);
-  if (debug_view == 1u) return add_s(n * 0.5f, 0.5f);
-  if (debug_view == 2u) return f3(visibility, visibility, visibility);
-  if (debug_view == 3u) return sun_rgb;
-  if (debug_view == 4u) return ambient_rgb * ao + floor_rgb;
+  if (EXTRA) {
+    const uint32_t debug_view = surface_debug(L);
+    if (debug_view == 1u) return add_s(n * 0.5f, 0.5f);
+    if (debug_view == 2u) return f3(visibility, visibility, visibility);
+    if (debug_view == 3u) return sun_rgb;
+    if (debug_view == 4u) return ambient_rgb * ao + floor_rgb;
+  }
   const F3 spec_rgb = spec_pre * (sky_sm * 0.5f);
   // surface_light / surface_radiance: resolve.wgsl:7-17
   const F3 light = repair ? ambient_rgb * ao * shade + sun_rgb + floor_rgb
@@ -392,7 +395,7 @@ static __device__ __noinline__ F3 shade_leg(const DevWorld& w, const vm_frame& f
                                             F3 p, F3 d, float dist, float shadow_dist) {
   const Chunk c = ld_chunk(w, h.ci);
   const uint32_t id = block_at(w, c, h.vx, h.vy, h.vz);
-  return shade_surface(w, f, L, h.ci, h.vx, h.vy, h.vz, id, h.normal, p, d, dist, shadow_dist, secondary_smooth(f),
+  return shade_surface<true>(w, f, L, h.ci, h.vx, h.vy, h.vz, id, h.normal, p, d, dist, shadow_dist, secondary_smooth(f),
                        false, -1.0f, nullptr);
 }
 
@@ -841,7 +844,9 @@ __global__ void __launch_bounds__(128, 12) k_resolve_light(const __grid_constant
 // fetch) and its warps run one path.
 // 12 blocks of 4 warps per SM (40 registers, a few bytes spilled): more
 // warps hide the L2 gathers of the issue-bound lanes (8 blocks: 2% slower).
-template <int PART>
+// EXTRA: the frame is underwater, uses the probe-tap / probe-ambient variants
+// or a surface debug view (their code is compiled out of the other launches).
+template <int PART, bool EXTRA>
 __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_frame f, const __grid_constant__ DevWorld w,
                                                     const __grid_constant__ Look L,
                                                     const unsigned long long* __restrict__ vis,
@@ -856,7 +861,7 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
   const F3 cam = ld3(f.cam_pos);
   const F3 rd = ray_dir(f, (float)px + 0.5f, (float)py + 0.5f);
   F3 color;
-  const bool underwater = (f.flags & VM_FLAG_UNDERWATER) != 0u;
+  const bool underwater = EXTRA && (f.flags & VM_FLAG_UNDERWATER) != 0u;
   if (PART == 1) {
     const float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, f.far_, 1.0f, px, py);
     color = sky_color(f, L, cam, rd, 0.0f, shaft);
@@ -877,7 +882,7 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
         const float4 a = out[pix];
         lt = {f3(a.x, a.y, a.z), a.w, light_ao[pix]};
       }
-      color = shade_surface(w, f, L, ci, vx, vy, vz, id, nid, hit, rd, t, f.shadow_dist, true, true,
+      color = shade_surface<EXTRA>(w, f, L, ci, vx, vy, vz, id, nid, hit, rd, t, f.shadow_dist, true, true,
                             sun_visibility(mask, dist, soft, pix), light_ao != nullptr ? &lt : nullptr);
     } else if (PART == 2) {
       if (ws.refr != nullptr && (ws.decided || (w.spec & VM_SPEC_WATER_REPAIR) == 0u ||
@@ -890,7 +895,7 @@ __global__ void __launch_bounds__(128, 12) k_resolve(const __grid_constant__ vm_
         color = shade_water(w, f, L, ci, vx, vy, vz, nid, hit, rd, t);
       }
     }
-    if (PART == 0 && surface_debug(L) == 0u) {   // water: the fog blend follows (k_resolve_blend)
+    if (PART == 0 && (!EXTRA || surface_debug(L) == 0u)) {   // water: the fog blend follows (k_resolve_blend)
       const float wet = underwater ? water_path(f, t, rd) : 0.0f;
       const float alpha = 1.0f - transmittance_from(f, cam.y + wet * rd.y, t - wet, rd);
       const float shaft = underwater ? 1.0f : sun_shaft(f, L, cam, rd, t, alpha, px, py);
@@ -1004,10 +1009,18 @@ cudaError_t launch_resolve(const vm_frame& f, const DevWorld& w, const Look& L, 
         f, w, L, vis, lane, water_sec_shift, (ushort4*)leg_refr, (ushort4*)leg_refl);
     ws = {(const ushort4*)leg_refr, (const ushort4*)leg_refl, water_sec_shift, hw, decide};
   }
-  k_resolve<2><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
+  const bool extra = (f.flags & (VM_FLAG_UNDERWATER | VM_FLAG_PROBE_TAP | VM_FLAG_PROBE_AMBIENT)) != 0u ||
+                     surface_debug(L) != 0u;
+  if (extra) k_resolve<2, true><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
+  else k_resolve<2, false><<<grid, block, 0, sw>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
   if (light_ao != nullptr) k_resolve_light<<<grid, block, 0, s>>>(f, w, L, vis, lane, out, light_ao);
-  k_resolve<0><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, light_ao, out);
-  k_resolve<1><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
+  if (extra) {
+    k_resolve<0, true><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, light_ao, out);
+    k_resolve<1, true><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
+  } else {
+    k_resolve<0, false><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, light_ao, out);
+    k_resolve<1, false><<<grid, block, 0, s>>>(f, w, L, vis, mask, dist, lane, soft_rays, ws, nullptr, out);
+  }
   const bool blend = surface_debug(L) == 0u;   // the debug views skip the fog and the underwater tail
   if (blend) k_resolve_fog<<<grid, block, 0, s>>>(f, w, L, vis, lane, fog);
   e = cudaGetLastError();

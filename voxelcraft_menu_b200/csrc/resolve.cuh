@@ -685,8 +685,11 @@ __device__ __forceinline__ float face_shade(uint32_t nid) {
 // primary hit (the cached form), lit_in < 0 traces shadow_ray from the hit
 // over shadow_dist (the secondary legs).  smooth: the 3x3 smooth light with
 // AO, else the single light sample of the voxel in front of the face.
-// pre: the hit's light terms when a stage computed them, else null.
+// pre: the hit's light terms when a stage computed them, else null.  EXTRA:
+// the frame may use the probe-tap / probe-ambient variants or a surface debug
+// view (without it their branches are compiled out).
 struct LightTerms { F3 amb; float sky_sm, ao; };   // ambient colour, smoothed sky light, AO
+template <bool EXTRA>
 __device__ __noinline__ F3 shade_surface(const DevWorld& w, const vm_frame& f, const Look& L, uint32_t ci, uint32_t vx,
                                          uint32_t vy, uint32_t vz, uint32_t id, uint32_t nid, F3 hit, F3 rd, float dist,
                                          float shadow_dist, bool smooth, bool do_spec, float lit_in,
